@@ -1,0 +1,196 @@
+/*
+ * powergrid_b200.h — C ABI of the B200 (sm_100a) implementation of PowerGrid's
+ * system-operator path: Gnufft, Gdft, TimeSegmentation, SENSE, pcSenseTimeSeg,
+ * QuadPenalty/TVPenalty and solve_pwls_pcg, plus a request server.
+ *
+ * Plain C: pointers, sizes and status codes only.  Complex vectors are
+ * interleaved single-precision pairs (re, im) — the memory layout of
+ * std::complex<float> / arma::cx_float.  Image vectors are y-fastest
+ * (index = y + Ny*x + Nx*Ny*z, reconSolve.cpp:40-53); coil data are
+ * coil-major [coil][sample] (SENSE.cpp:66, 86).
+ *
+ * Every entry point returns pg_status and never exits the process (the
+ * reference prints and calls exit(1), gridding.cpp:454-457; Gnufft.cpp:297-300).
+ * pg_last_error() gives a message for the calling thread's last failure.
+ *
+ * Reference citations are relative to the PowerGrid/ source directory.
+ */
+#ifndef POWERGRID_B200_H
+#define POWERGRID_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum pg_status {
+  PG_OK = 0,
+  PG_INVALID_ARG = 1,
+  PG_OUT_OF_MEMORY = 2,
+  PG_CUDA_ERROR = 3,
+  PG_TIMEOUT = 4,
+  PG_CANCELLED = 5,
+  PG_NOT_INITIALIZED = 6,
+  PG_CUFFT_ERROR = 7,
+  PG_REJECTED = 8,     /* admission control: request exceeds the HBM budget */
+  PG_NOT_READY = 9     /* pg_poll: request still running */
+} pg_status;
+
+/* Opaque handles. */
+typedef struct pg_op_s* pg_op;          /* any system operator */
+typedef struct pg_server_s* pg_server;  /* request server */
+
+/* ---- library ---------------------------------------------------------- */
+/* Select the CUDA device and create the library context.  Calling any other
+ * entry point first initialises device 0 implicitly. */
+pg_status pg_init(int device);
+pg_status pg_shutdown(void);
+const char* pg_status_string(pg_status s);
+const char* pg_last_error(void);
+/* Number of this library's kernel launches since pg_init (instrumentation). */
+uint64_t pg_kernel_launch_count(void);
+
+/* ---- operators -------------------------------------------------------- */
+/* Gnufft(dataLength, gridos, nx, ny, nz, kx, ky, kz, ix, iy, iz)
+ * replaces Gnufft<float>::Gnufft (Gnufft.h:51-53, Gnufft.cpp:34-122).
+ * k in cycles/FOV, host arrays of length dataLength (copied).  The image
+ * coordinates ix/iy/iz are stored but unused by the math in the reference
+ * (Gnufft.cpp:47-49), so they are not taken here.  2-D requires nx == ny
+ * (the reference mixes x/y-fastest conventions otherwise: zero_pad2d
+ * griddingSupport.cpp:488 vs gridding.cpp:100).  gridos must be 2 here. */
+pg_status pg_gnufft_create(pg_op* out, uint64_t data_length, float gridos, uint64_t nx, uint64_t ny,
+                           uint64_t nz, const float* kx, const float* ky, const float* kz);
+
+/* Gdft(nk, ni, kx, ky, kz, ix, iy, iz, FM_rad_per_s, t_s) replaces
+ * Gdft<float>::Gdft (Gdft.h:47-49, Gdft.cpp:33-49). */
+pg_status pg_gdft_create(pg_op* out, uint64_t nk, uint64_t ni, const float* kx, const float* ky,
+                         const float* kz, const float* ix, const float* iy, const float* iz,
+                         const float* field_map, const float* t);
+
+/* TimeSegmentation(G, fieldmap, tvec, n1 = data length, n2 = image length, L,
+ * interptype, shots) replaces TimeSegmentation<float, Tobj>::TimeSegmentation
+ * (TimeSegmentation.h:70-71, TimeSegmentation.cpp:37-221).  G is not owned
+ * and must outlive this operator (TimeSegmentation.cpp:53).  interptype 1 =
+ * Hanning (TimeSegmentation.cpp:80-93). */
+pg_status pg_timeseg_create(pg_op* out, pg_op G, const float* field_map, const float* tvec, uint64_t n1,
+                            uint64_t n2, uint64_t L, uint64_t interptype, uint64_t shots);
+
+/* SENSE(G, senseMap (complex, n2*nc, coil-major), n1, n2, nc) replaces
+ * SENSE<float, Tobj>::SENSE (SENSE.h:64, SENSE.cpp:33-44).  G not owned. */
+pg_status pg_sense_create(pg_op* out, pg_op G, const float* sense_map, uint64_t n1, uint64_t n2, uint64_t nc);
+
+/* pcSenseTimeSeg(kx, ky, kz, nx, ny, nz, nc, t, L, intType, SENSEmap,
+ * FieldMap, ShotPhaseMap) replaces pcSenseTimeSeg<float>::pcSenseTimeSeg
+ * (pcSenseTimeSeg.h:80-82, pcSenseTimeSeg.cpp:41-125).  nk = total samples
+ * (all shots); shots = n_shot_phase / (nx*ny*nz) (pcSenseTimeSeg.cpp:47). */
+pg_status pg_pcsense_timeseg_create(pg_op* out, const float* kx, const float* ky, const float* kz, uint64_t nk,
+                                    uint64_t nx, uint64_t ny, uint64_t nz, uint64_t nc, const float* t,
+                                    uint64_t L, uint64_t interptype, const float* sense_map,
+                                    const float* field_map, const float* shot_phase_map, uint64_t n_shot_phase);
+
+pg_status pg_op_destroy(pg_op op);
+/* Lengths of the data vector (operator* output) and image vector. */
+pg_status pg_op_shape(pg_op op, uint64_t* n_data, uint64_t* n_image);
+
+/* operator* (forward) and operator/ (adjoint) on HOST buffers: the
+ * Col<complex<float>> interface of every operator above (e.g.
+ * Gnufft.cpp:153-211, SENSE.cpp:51-97).  Synchronous. */
+pg_status pg_op_forward(pg_op op, const float* x, float* y);
+pg_status pg_op_adjoint(pg_op op, const float* y, float* x);
+
+/* The same on DEVICE buffers, stream-ordered (stream may be NULL = the
+ * library's default stream).  No host synchronisation. */
+pg_status pg_op_forward_device(pg_op op, const void* x_dev, void* y_dev, void* stream);
+pg_status pg_op_adjoint_device(pg_op op, const void* y_dev, void* x_dev, void* stream);
+
+/* ---- regularizers and solver ----------------------------------------- */
+typedef enum pg_penalty_kind { PG_PENALTY_QUAD = 0, PG_PENALTY_TV = 1 } pg_penalty_kind;
+
+/* QuadPenalty(nx, ny, nz, beta, dims2penalize) (QuadPenalty.h:43) and
+ * TVPenalty(nx, ny, nz, beta, delta, dims2penalize) (TVPenalty.h:42). */
+typedef struct pg_penalty {
+  int kind;                 /* pg_penalty_kind */
+  uint64_t nx, ny, nz;
+  float beta;
+  float delta;              /* TV only */
+  uint64_t dims2penalize;   /* 2 or 3; reference default 3 */
+} pg_penalty;
+
+/* solve_pwls_pcg(xInitial, A, W, yi, R, niter) (solve_pwls_pcg.hpp:48-51).
+ * Host buffers.  x0 may be NULL (zeros, as reconSolve.h:75-76); W may be
+ * NULL (ones, reconSolve.h:73-74).  Inner products, step sizes and the CG
+ * coefficient are accumulated in FP64 on the device; each iteration runs as
+ * one CUDA graph.  iters_done (may be NULL) receives the number of
+ * completed iterations (early exits as solve_pwls_pcg.hpp:88-91, 113-116,
+ * 137-145). */
+pg_status pg_pcg_solve(pg_op A, const float* x0, const float* W, const float* y, const pg_penalty* R,
+                       uint64_t niter, float* x_out, uint64_t* iters_done);
+
+/* The same on device buffers, stream-ordered; iters_done_dev (may be NULL)
+ * is a device uint32. */
+pg_status pg_pcg_solve_device(pg_op A, const void* x0_dev, const void* W_dev, const void* y_dev,
+                              const pg_penalty* R, uint64_t niter, void* x_out_dev, void* iters_done_dev,
+                              void* stream);
+
+/* reconSolve(data, Sg, R, kx, ky, kz, Nx, Ny, Nz, tvec, niter)
+ * (reconSolve.h:63-82): W = 1, x0 = 0. */
+pg_status pg_recon_solve(pg_op Sg, const pg_penalty* R, const float* data, uint64_t niter, float* image_out);
+
+/* Penalty pieces (Robject.cpp:143-193) on device buffers, for tests. */
+pg_status pg_penalty_gradient_device(const pg_penalty* R, const void* x_dev, void* g_dev, void* stream);
+pg_status pg_penalty_denom_device(const pg_penalty* R, const void* ddir_dev, const void* x_dev, double* out_host);
+
+/* ---- request server (continuous batching) ---------------------------- */
+typedef struct pg_server_config {
+  uint64_t hbm_budget_bytes;   /* admission limit on resident request state */
+  uint32_t max_inflight;       /* concurrent requests on the GPU */
+  uint32_t streams;            /* CUDA streams used for overlap */
+} pg_server_config;
+
+/* A 2-D/3-D time-segmented SENSE reconstruction request:
+ * SENSE<TimeSegmentation<Gnufft>> + QuadPenalty, reconSolve semantics. */
+typedef struct pg_request {
+  uint64_t nx, ny, nz, nc, n_samples, L, niter;
+  float beta;
+  const float* kx; const float* ky; const float* kz; const float* t;
+  const float* field_map;      /* nx*ny*nz, rad/s */
+  const float* sense_map;      /* complex, nx*ny*nz*nc, coil-major */
+  const float* data;           /* complex, n_samples*nc, coil-major */
+  float* image_out;            /* complex, nx*ny*nz; written when done */
+} pg_request;
+
+typedef struct pg_request_stats {
+  double t_submit_ms, t_start_ms, t_done_ms;   /* host steady-clock */
+  uint64_t iters_done;
+  uint64_t bytes_resident;
+  pg_status status;
+} pg_request_stats;
+
+pg_status pg_server_create(pg_server* out, const pg_server_config* cfg);
+pg_status pg_server_destroy(pg_server s);
+/* Request buffers must stay valid until pg_poll reports completion. */
+pg_status pg_submit(pg_server s, const pg_request* req, uint64_t* ticket);
+/* PG_OK when done (stats filled), PG_NOT_READY while queued/running. */
+pg_status pg_poll(pg_server s, uint64_t ticket, pg_request_stats* stats);
+pg_status pg_wait(pg_server s, uint64_t ticket, pg_request_stats* stats);
+pg_status pg_cancel(pg_server s, uint64_t ticket);
+/* Estimated device bytes a request holds while resident (admission metric). */
+uint64_t pg_request_footprint(const pg_request* req);
+
+/* ---- instrumentation and fault injection (host-side only) ------------ */
+/* Make the n-th device allocation from now fail with PG_OUT_OF_MEMORY
+ * (n = 0 disables). */
+void pg_debug_fail_allocation_after(uint64_t n);
+/* Kaiser-Bessel lookup table as built by Gnufft (griddingSupport.cpp:52-76;
+ * beta from Gnufft.cpp:84-88).  Returns its length. */
+uint64_t pg_util_kb_lut(float gridos, float* lut_out, uint64_t cap, float* beta_out);
+/* The adjoint's sample binning for a Gnufft operator: per-sample bin key in
+ * original order, and the stable sorted permutation. */
+pg_status pg_util_gnufft_binning(pg_op G, uint32_t* keys_out, uint32_t* perm_out, uint64_t* n_bins_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* POWERGRID_B200_H */

@@ -1,0 +1,240 @@
+"""ORACLE / TEST INFRASTRUCTURE ONLY — the checker, never the product.
+
+ctypes front end of the CPU oracle (oracle_capi.cpp over pg_oracle.hpp):
+a restatement of PowerGrid's system-operator path in float (the reference
+CPU path) and double (the FP64 oracle), optionally running Gnufft/Gdft on
+the reference's own kernels compiled from its sources (oracle/_ref/).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libpgref.so")
+
+F32, F64, C64, C128 = np.float32, np.float64, np.complex64, np.complex128
+P = C.c_void_p
+U64 = C.c_uint64
+
+_lib = None
+
+
+def build(ref: bool = False) -> None:
+    """Compile the restatement (and, where the reference tree exists, its kernels)."""
+    targets = ["all"] + (["ref"] if ref else [])
+    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        L.orc_last_error.restype = C.c_char_p
+        L.orc_gnufft_new.restype = P
+        L.orc_gnufft_new.argtypes = [C.c_int, U64, C.c_float, U64, U64, U64, P, P, P]
+        L.orc_gdft_new.restype = P
+        L.orc_gdft_new.argtypes = [C.c_int, U64, U64] + [P] * 8
+        L.orc_timeseg_new.restype = P
+        L.orc_timeseg_new.argtypes = [P, P, P, U64, U64, U64, U64, U64]
+        L.orc_sense_new.restype = P
+        L.orc_sense_new.argtypes = [P, P, U64, U64, U64]
+        L.orc_pcsense_ts_new.restype = P
+        L.orc_pcsense_ts_new.argtypes = [C.c_int, P, P, P, U64, U64, U64, U64, U64, P, U64, U64, P, P, P, U64]
+        L.orc_free.argtypes = [P]
+        L.orc_data_len.restype = U64
+        L.orc_data_len.argtypes = [P]
+        L.orc_image_len.restype = U64
+        L.orc_image_len.argtypes = [P]
+        L.orc_forward.argtypes = [P, P, P]
+        L.orc_adjoint.argtypes = [P, P, P]
+        L.orc_pcg.argtypes = [P, P, P, P, C.c_int, U64, U64, U64, C.c_double, C.c_double, U64, U64, P]
+        L.orc_penalty_gradient.argtypes = [C.c_int, C.c_int, U64, U64, U64, C.c_double, C.c_double, U64, P, P]
+        L.orc_penalty_denom.argtypes = [C.c_int, C.c_int, U64, U64, U64, C.c_double, C.c_double, U64, P, P, P]
+        L.orc_kb_lut.argtypes = [C.c_int, C.c_float, P, U64, P]
+        L.orc_timeseg_tables.argtypes = [P, P, P, P, P]
+        L.orc_fft.argtypes = [C.c_int, P, P, C.c_int, C.c_int]
+        L.orc_use_reference.argtypes = [C.c_char_p]
+        L.orc_set_threads.argtypes = [C.c_int]
+        _lib = L
+    return _lib
+
+
+def reference_available() -> bool:
+    return os.path.exists(REF_PATH)
+
+
+def use_reference(on: bool = True) -> None:
+    """Route Gnufft/Gdft (float, double) through the reference's compiled kernels."""
+    rc = lib().orc_use_reference(REF_PATH.encode() if on else None)
+    if rc != 0:
+        raise RuntimeError("oracle: " + lib().orc_last_error().decode())
+
+
+def set_threads(n: int) -> None:
+    lib().orc_set_threads(int(n))
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(P)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=F32)
+
+
+class Op:
+    """An oracle operator: forward = operator*, adjoint = operator/."""
+
+    def __init__(self, handle, prec: int, keep=()):
+        if not handle:
+            raise RuntimeError("oracle: " + lib().orc_last_error().decode())
+        self.h = handle
+        self.prec = prec
+        self._keep = list(keep)
+
+    @property
+    def cdtype(self):
+        return C64 if self.prec == 0 else C128
+
+    @property
+    def rdtype(self):
+        return F32 if self.prec == 0 else F64
+
+    @property
+    def n_data(self) -> int:
+        return int(lib().orc_data_len(self.h))
+
+    @property
+    def n_image(self) -> int:
+        return int(lib().orc_image_len(self.h))
+
+    def forward(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=self.cdtype)
+        y = np.zeros(self.n_data, dtype=self.cdtype)
+        lib().orc_forward(self.h, _p(x), _p(y))
+        return y
+
+    def adjoint(self, y: np.ndarray) -> np.ndarray:
+        y = np.ascontiguousarray(y, dtype=self.cdtype)
+        x = np.zeros(self.n_image, dtype=self.cdtype)
+        lib().orc_adjoint(self.h, _p(y), _p(x))
+        return x
+
+    __mul__ = forward
+    __truediv__ = adjoint
+
+    def pcg(self, y, penalty: str, nx, ny, nz, beta, delta=1.0, dims2pen=3, niter=10, x0=None, W=None):
+        y = np.ascontiguousarray(y, dtype=self.cdtype)
+        x = np.zeros(self.n_image, dtype=self.cdtype)
+        x0p = None if x0 is None else _p(np.ascontiguousarray(x0, dtype=self.cdtype))
+        Wa = None if W is None else np.ascontiguousarray(W, dtype=self.rdtype)
+        kind = {"quad": 0, "tv": 1}[penalty]
+        n = lib().orc_pcg(self.h, x0p, None if Wa is None else _p(Wa), _p(y), kind, nx, ny, nz, beta, delta,
+                          dims2pen, niter, _p(x))
+        return x, n
+
+    def timeseg_tables(self):
+        L = int(lib().orc_timeseg_tables(self.h, None, None, None, _p(np.zeros(2))))
+        n1, n2 = self.n_data, self.n_image
+        AA = np.zeros(n1 * L, self.cdtype)
+        Wo = np.zeros(n2 * (L + 1) if L > 1 else n2, self.cdtype)
+        WoH = np.zeros_like(Wo)
+        tt = np.zeros(2)
+        lib().orc_timeseg_tables(self.h, _p(AA), _p(Wo), _p(WoH), _p(tt))
+        return AA.reshape(L, n1), Wo, WoH, tt
+
+    def __del__(self):
+        try:
+            if _lib is not None and self.h:
+                _lib.orc_free(self.h)
+        except Exception:
+            pass
+
+
+def gnufft(prec, M, nx, ny, nz, kx, ky, kz, gridos=2.0) -> Op:
+    kx, ky, kz = _f32(kx), _f32(ky), _f32(kz)
+    return Op(lib().orc_gnufft_new(prec, M, gridos, nx, ny, nz, _p(kx), _p(ky), _p(kz)), prec)
+
+
+def gdft(prec, kx, ky, kz, ix, iy, iz, fm, t) -> Op:
+    a = [_f32(v) for v in (kx, ky, kz, ix, iy, iz, fm, t)]
+    return Op(lib().orc_gdft_new(prec, a[0].size, a[3].size, *[_p(v) for v in a]), prec)
+
+
+def timeseg(G: Op, fm, t, n1, n2, L, interptype=1, shots=1) -> Op:
+    fm, t = _f32(fm), _f32(t)
+    return Op(lib().orc_timeseg_new(G.h, _p(fm), _p(t), n1, n2, L, interptype, shots), G.prec, keep=[G])
+
+
+def sense(G: Op, smap, n1, n2, nc) -> Op:
+    s = np.ascontiguousarray(smap, dtype=C64)
+    return Op(lib().orc_sense_new(G.h, _p(s), n1, n2, nc), G.prec, keep=[G])
+
+
+def pcsense_timeseg(prec, kx, ky, kz, nx, ny, nz, nc, t, L, smap, fm, pmap, interptype=1) -> Op:
+    kx, ky, kz, t, fm, pm = (_f32(v) for v in (kx, ky, kz, t, fm, pmap))
+    s = np.ascontiguousarray(smap, dtype=C64)
+    return Op(lib().orc_pcsense_ts_new(prec, _p(kx), _p(ky), _p(kz), kx.size, nx, ny, nz, nc, _p(t), L, interptype,
+                                       _p(s), _p(fm), _p(pm), pm.size), prec)
+
+
+def kb_lut(prec: int, gridos: float = 2.0):
+    out = np.zeros(100000, dtype=F32 if prec == 0 else F64)
+    beta = np.zeros(1)
+    n = lib().orc_kb_lut(prec, gridos, _p(out), out.size, _p(beta))
+    return out[:n].copy(), float(beta[0])
+
+
+def fft(a: np.ndarray, sign: int) -> np.ndarray:
+    a = np.ascontiguousarray(a.copy())
+    prec = 0 if a.dtype == C64 else 1
+    dims = np.array(a.shape, dtype=np.uint64)
+    lib().orc_fft(prec, _p(a), _p(dims), a.ndim, sign)
+    return a
+
+
+def penalty_gradient(prec, kind, nx, ny, nz, beta, delta, dims2pen, x):
+    x = np.ascontiguousarray(x, dtype=C64 if prec == 0 else C128)
+    g = np.zeros_like(x)
+    lib().orc_penalty_gradient(prec, {"quad": 0, "tv": 1}[kind], nx, ny, nz, beta, delta, dims2pen, _p(x), _p(g))
+    return g
+
+
+def penalty_denom(prec, kind, nx, ny, nz, beta, delta, dims2pen, ddir, x):
+    ct = C64 if prec == 0 else C128
+    d = np.ascontiguousarray(ddir, dtype=ct)
+    x = np.ascontiguousarray(x, dtype=ct)
+    out = np.zeros(2)
+    lib().orc_penalty_denom(prec, {"quad": 0, "tv": 1}[kind], nx, ny, nz, beta, delta, dims2pen, _p(d), _p(x),
+                            _p(out))
+    return complex(out[0], out[1])
+
+
+def build_problem_op(prob, prec: int) -> Op:
+    """The operator a Problem describes, as the reference's drivers compose it
+    (PowerGridIsmrmrd.cpp:244-264, PowerGridPcSenseTimeSeg.cpp)."""
+    from powergrid_b200.synthetic import image_coords  # noqa: WPS433 (shared generator)
+    M = prob.kx.size
+    n = prob.nimg
+    if prob.op == "pcsense_ts":
+        return pcsense_timeseg(prec, prob.kx, prob.ky, prob.kz, prob.nx, prob.ny, prob.nz, prob.nc, prob.t, prob.L,
+                               prob.smap, prob.fm, prob.pmap)
+    if prob.op == "sense_gdft":
+        ix, iy, iz = image_coords(prob.nx, prob.ny, prob.nz)
+        G = gdft(prec, prob.kx, prob.ky, prob.kz, ix, iy, iz, prob.fm, prob.t)
+        return sense(G, prob.smap, M, n, prob.nc)
+    G = gnufft(prec, M, prob.nx, prob.ny, prob.nz, prob.kx, prob.ky, prob.kz)
+    if prob.op == "sense_ts_nufft":
+        A = timeseg(G, prob.fm, prob.t, M, n, prob.L)
+        return sense(A, prob.smap, M, n, prob.nc)
+    return sense(G, prob.smap, M, n, prob.nc)

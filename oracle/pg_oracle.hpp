@@ -1,0 +1,859 @@
+// ORACLE / TEST INFRASTRUCTURE ONLY — the checker, never the product.
+//
+// CPU restatement of PowerGrid's system-operator path, written for this
+// project from the cited reference lines (paths relative to PowerGrid/):
+//   Gnufft pipeline     computeFd_CPU_Grid / computeFH_CPU_Grid (gridding.cpp:584-727, 418-581),
+//                       gridding_{forward,adjoint}_{2D,3D} (gridding.cpp:31-415),
+//                       deapodization/zero_pad/crop/circshift (griddingSupport.cpp:210-627),
+//                       LUT + I0 (griddingSupport.cpp:33-76), beta (Gnufft.cpp:84-88)
+//   Gdft                ftCpu / iftCpu (ftCpu.cpp:95-215) in float, plus an exact FP64 variant
+//   TimeSegmentation    Hanning interpolator (TimeSegmentation.cpp:37-93, 213-218, 252-324)
+//   SENSE               SENSE.cpp:33-97
+//   pcSenseTimeSeg      pcSenseTimeSeg.cpp:41-171
+//   Robject/Quad/TV     Robject.cpp:49-193, QuadPenalty.cpp:45-64, TVPenalty.cpp:43-68
+//   solve_pwls_pcg      solve_pwls_pcg.hpp:34-167
+//
+// Expressions keep the reference's operand types and evaluation order, so
+// the float instantiation reproduces the reference CPU path bit for bit when
+// both use the same FFT (checked by tests against the reference compiled
+// from its own sources).  The double instantiation is the FP64 oracle; for
+// the DFT it evaluates sin/cos in double (ftCpu<double> itself calls
+// sinf/cosf, ftCpu.cpp:104, 129-130, 203-204).
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <stdexcept>
+#include <vector>
+
+#include "fft_engine.hpp"
+
+namespace pgo {
+
+using u64 = unsigned long long;
+
+// Single-precision build's pi literal (PGIncludes.h:69): used wherever the
+// reference writes MRI_PI, in both instantiations.
+constexpr float kPiF = 3.1415926535897932384626433832795029f;
+constexpr double kPiD = 3.141592653589793238462643383279502884;  // arma datum::pi
+
+// ---------------------------------------------------------------------------
+// Kaiser-Bessel support
+// ---------------------------------------------------------------------------
+
+// Modified Bessel I0 by the Abramowitz & Stegun 9.8.1 / 9.8.2 polynomial
+// approximations (as tabulated in Numerical Recipes in C, 2nd ed.), with the
+// operand types of griddingSupport.cpp:33-48 (double literals, T storage).
+template <typename T>
+T bessel_i0(T x) {
+  T ax = std::abs(x);
+  T y;
+  T r;
+  if (ax < 3.75) {
+    y = x / 3.75;
+    y = y * y;
+    r = 1.0 + y * (3.5156229 + y * (3.0899424 + y * (1.2067492 +
+        y * (0.2659732 + y * (0.360768e-1 + y * 0.45813e-2)))));
+  } else {
+    y = 3.75 / ax;
+    r = (std::exp(ax) / std::sqrt(ax)) *
+        (0.39894228 + y * (0.1328592e-1 + y * (0.225319e-2 + y * (-0.157565e-2 +
+        y * (0.916281e-2 + y * (-0.2057706e-1 + y * (0.2635537e-1 +
+        y * (-0.1647633e-1 + y * 0.392377e-2))))))));
+  }
+  return r;
+}
+
+// LUT[k] = I0(beta*sqrt(1 - k/size))/width, size = 10000*width
+// (griddingSupport.cpp:52-76).
+template <typename T>
+std::vector<T> kb_lut(T beta, T width) {
+  std::vector<T> lut;
+  if (width > 0) {
+    const u64 n = (u64)(10000 * width);
+    lut.resize(n);
+    for (int k = 0; k < (int)n; ++k) {
+      T v = static_cast<T>(k) / static_cast<T>(n);
+      lut[k] = bessel_i0<T>(beta * std::sqrt(1.0 - (v))) / width;
+    }
+  }
+  return lut;
+}
+
+// Gnufft.cpp:84-88: kernel width 4 and beta from the oversampling factor.
+template <typename T>
+T kb_beta(T gridos, T width) {
+  return kPiF * std::sqrt((gridos - 0.5) * (gridos - 0.5) * (width * width * 4.0) / (gridos * gridos) - 0.8);
+}
+
+// ---------------------------------------------------------------------------
+// Grid geometry (gridding.cpp:437-446, Gnufft.cpp:55-61)
+// ---------------------------------------------------------------------------
+template <typename T>
+struct Geom {
+  int Nx = 1, Ny = 1, Nz = 1;  // image size
+  int Gx = 1, Gy = 1, Gz = 1;  // oversampled grid size
+  T os = 2;                    // grid oversampling
+  T kw = 4;                    // kernel width
+  T beta = 0;
+  std::vector<T> lut;
+  bool is3d() const { return Nz != 1; }
+  u64 nimg() const { return (u64)Nx * Ny * Nz; }
+  u64 ngrid() const { return (u64)Gx * Gy * Gz; }
+
+  static Geom make(int nx, int ny, int nz, T gridos) {
+    Geom g;
+    g.Nx = nx; g.Ny = ny; g.Nz = nz; g.os = gridos; g.kw = (T)4.0;
+    g.Gx = (int)std::ceil(gridos * (T)nx);
+    g.Gy = (int)std::ceil(gridos * (T)ny);
+    if (g.Gx % 2) g.Gx += 1;
+    if (g.Gy % 2) g.Gy += 1;
+    g.Gz = (nz == 1) ? nz : (int)std::ceil(gridos * (T)nz);
+    g.beta = kb_beta<T>(gridos, g.kw);
+    g.lut = kb_lut<T>(g.beta, g.kw);
+    return g;
+  }
+};
+
+// Window bounds along one axis: clamped to the grid, not wrapped
+// (gridding.cpp:67-73).
+template <typename T>
+inline void window(T s, T kw, T os, int n_image, int& lo, int& hi) {
+  lo = (int)(std::max((T)0.0, std::ceil(s - kw * (os) / (T)2.0)));
+  hi = (int)(std::min((os * (T)n_image - (T)1.0), std::floor(s + kw * (os) / (T)2.0)));
+}
+
+// Nearest-lower LUT entry, zero past the end (gridding.cpp:78-84).
+template <typename T>
+inline T lut_weight(T s, int n, T os, T kw, const T* lut, u64 nlut) {
+  T dist = std::abs(s - ((T)n)) / (os);
+  int k0 = (int)((dist * dist * (T)4.0 / (kw * kw)) * (T)nlut);
+  if ((u64)k0 >= nlut) return (T)0.0;
+  return lut[k0];
+}
+
+// Forward interpolation: y_i = sum over the window of w * grid[ny + nx*Gy (+ nz*Gx*Gy)]
+// (gridding.cpp:217-415).
+template <typename T>
+void interp_forward(const Geom<T>& g, u64 M, const T* kx, const T* ky, const T* kz,
+                    const std::complex<T>* grid, std::complex<T>* y) {
+  const T* lut = g.lut.data();
+  const u64 nl = g.lut.size();
+  for (u64 i = 0; i < M; ++i) {
+    T acc_r = 0, acc_i = 0;
+    T sx = (g.os) * (kx[i] + ((T)g.Nx) / (T)2.0);
+    T sy = (g.os) * (ky[i] + ((T)g.Ny) / (T)2.0);
+    int xl, xh, yl, yh;
+    window(sx, g.kw, g.os, g.Nx, xl, xh);
+    window(sy, g.kw, g.os, g.Ny, yl, yh);
+    if (!g.is3d()) {
+      for (int nx = xl; nx <= xh; ++nx) {
+        T wx = lut_weight(sx, nx, g.os, g.kw, lut, nl);
+        for (int ny = yl; ny <= yh; ++ny) {
+          T wy = lut_weight(sy, ny, g.os, g.kw, lut, nl);
+          T w = wx * wy;
+          const std::complex<T> v = grid[(u64)ny + (u64)nx * g.Gy];
+          acc_r += w * v.real();
+          acc_i += w * v.imag();
+        }
+      }
+    } else {
+      T sz = (g.os) * (kz[i] + ((T)g.Nz) / (T)2.0);
+      int zl, zh;
+      window(sz, g.kw, g.os, g.Nz, zl, zh);
+      for (int nz = zl; nz <= zh; ++nz) {
+        T wz = lut_weight(sz, nz, g.os, g.kw, lut, nl);
+        for (int nx = xl; nx <= xh; ++nx) {
+          T wx = lut_weight(sx, nx, g.os, g.kw, lut, nl);
+          for (int ny = yl; ny <= yh; ++ny) {
+            T wy = lut_weight(sy, ny, g.os, g.kw, lut, nl);
+            T w = wx * wy * wz;
+            const std::complex<T> v = grid[(u64)ny + (u64)nx * g.Gy + (u64)nz * g.Gx * g.Gy];
+            acc_r += w * v.real();
+            acc_i += w * v.imag();
+          }
+        }
+      }
+    }
+    y[i] = std::complex<T>(acc_r, acc_i);
+  }
+}
+
+// Adjoint spreading in sample order: grid[idx] += w * d_i (gridding.cpp:31-214).
+template <typename T>
+void spread_adjoint(const Geom<T>& g, u64 M, const T* kx, const T* ky, const T* kz,
+                    const std::complex<T>* d, std::complex<T>* grid) {
+  const T* lut = g.lut.data();
+  const u64 nl = g.lut.size();
+  T* gr = reinterpret_cast<T*>(grid);
+  for (u64 i = 0; i < M; ++i) {
+    const T dr = d[i].real(), di = d[i].imag();
+    T sx = (g.os) * (kx[i] + ((T)g.Nx) / (T)2.0);
+    T sy = (g.os) * (ky[i] + ((T)g.Ny) / (T)2.0);
+    int xl, xh, yl, yh;
+    window(sx, g.kw, g.os, g.Nx, xl, xh);
+    window(sy, g.kw, g.os, g.Ny, yl, yh);
+    if (!g.is3d()) {
+      for (int nx = xl; nx <= xh; ++nx) {
+        T wx = lut_weight(sx, nx, g.os, g.kw, lut, nl);
+        for (int ny = yl; ny <= yh; ++ny) {
+          T wy = lut_weight(sy, ny, g.os, g.kw, lut, nl);
+          T w = wx * wy;
+          const u64 idx = 2 * ((u64)ny + (u64)nx * g.Gy);
+          gr[idx] += w * dr;
+          gr[idx + 1] += w * di;
+        }
+      }
+    } else {
+      T sz = (g.os) * (kz[i] + ((T)g.Nz) / (T)2.0);
+      int zl, zh;
+      window(sz, g.kw, g.os, g.Nz, zl, zh);
+      for (int nz = zl; nz <= zh; ++nz) {
+        T wz = lut_weight(sz, nz, g.os, g.kw, lut, nl);
+        for (int nx = xl; nx <= xh; ++nx) {
+          T wx = lut_weight(sx, nx, g.os, g.kw, lut, nl);
+          for (int ny = yl; ny <= yh; ++ny) {
+            T wy = lut_weight(sy, ny, g.os, g.kw, lut, nl);
+            T w = wx * wy * wz;
+            const u64 idx = (u64)ny + (u64)nx * g.Gy + (u64)nz * g.Gx * g.Gy;
+            gr[2 * idx] += w * dr;
+            gr[2 * idx + 1] += w * di;
+          }
+        }
+      }
+    }
+  }
+}
+
+// Reciprocal Kaiser-Bessel transform factor along one axis
+// (griddingSupport.cpp:249-260 in 2-D; :331-348 in 3-D, where the sinh branch
+// runs in double).
+template <typename T>
+inline T deapod_axis(T u, T kw, T beta, bool three_d) {
+  T c = (T)(kPiF * kPiF) * kw * kw * u * u - beta * beta;
+  if (c >= 0) return (T)(std::sin(std::sqrt(c)) / std::sqrt(c));
+  if (three_d) return (T)(std::sinh(std::sqrt(-1.0 * c)) / std::sqrt(-1.0 * c));
+  return std::sinh(std::sqrt((T)-1.0 * c)) / std::sqrt((T)-1.0 * c);
+}
+
+// deapodization2d/3d: out = in / Pi_axes g(u) / os^d; NaN factor -> 0
+// (griddingSupport.cpp:210-368).  In place on an image (y fastest).
+template <typename T>
+void deapodize(const Geom<T>& g, std::complex<T>* img) {
+  const int X = g.Nx, Y = g.Ny, Z = g.Nz;
+  if (!g.is3d()) {
+    for (int x = 0; x < X; ++x) {
+      for (int y = 0; y < Y; ++y) {
+        T uy = (T)(y - (Y / 2)) / (T)Y;
+        T ux = (T)(x - (X / 2)) / (T)X;
+        T k = deapod_axis(ux, g.kw, g.beta, false) * deapod_axis(uy, g.kw, g.beta, false);
+        const u64 p = (u64)y + (u64)x * Y;
+        if (k == k) {
+          T os2 = g.os * g.os;
+          img[p] = std::complex<T>(img[p].real() / k * ((T)1.0 / os2), img[p].imag() / k * ((T)1.0 / os2));
+        } else {
+          img[p] = std::complex<T>(0, 0);
+        }
+      }
+    }
+  } else {
+    for (int z = 0; z < Z; ++z)
+      for (int x = 0; x < X; ++x)
+        for (int y = 0; y < Y; ++y) {
+          T uz = (T)((z) - ((T)Z / 2.0)) / (T)Z;
+          T uy = (T)((y) - ((T)Y / 2.0)) / (T)Y;
+          T ux = (T)((x) - ((T)X / 2.0)) / (T)X;
+          T kx = deapod_axis(ux, g.kw, g.beta, true);
+          T ky = deapod_axis(uy, g.kw, g.beta, true);
+          T kz = deapod_axis(uz, g.kw, g.beta, true);
+          T k = kx * ky * kz;
+          const u64 p = (u64)z * Y * X + (u64)x * Y + y;
+          if (k == k) {
+            T os3 = g.os * g.os * g.os;
+            img[p] = std::complex<T>((T)((img[p].real()) / k * (1.0 / os3)),
+                                     (T)((img[p].imag()) / k * (1.0 / os3)));
+          } else {
+            img[p] = std::complex<T>(0, 0);
+          }
+        }
+  }
+}
+
+// Circular shift by (sa, sb, sc) of an array with a fastest (extent na)
+// (griddingSupport.cpp:552-593): out[(a+sa)%na, (b+sb)%nb, (c+sc)%nc] = in[a,b,c].
+template <typename T>
+void circshift(std::complex<T>* out, const std::complex<T>* in, int na, int nb, int nc, int sa, int sb, int sc) {
+  for (int c = 0; c < nc; ++c)
+    for (int b = 0; b < nb; ++b)
+      for (int a = 0; a < na; ++a) {
+        const u64 src = (u64)a + (u64)b * na + (u64)c * na * nb;
+        const u64 dst = (u64)((a + sa) % na) + (u64)((b + sb) % nb) * na + (u64)((c + sc) % nc) * na * nb;
+        out[dst] = in[src];
+      }
+}
+
+// fftshift: floor(n/2) per axis; ifftshift: ceil(n/2) in-plane, floor(n/2)
+// along z (griddingSupport.cpp:599-627).  Axes passed as (xdim, ydim, zdim) =
+// gridSize[0..2], with xdim the fastest index, as the reference does.
+template <typename T>
+void fftshift_grid(const Geom<T>& g, std::complex<T>* out, const std::complex<T>* in) {
+  circshift(out, in, g.Gx, g.Gy, g.Gz, (int)std::floor(g.Gx / 2.0), (int)std::floor(g.Gy / 2.0),
+            g.is3d() ? (int)std::floor(g.Gz / 2.0) : 0);
+}
+template <typename T>
+void ifftshift_grid(const Geom<T>& g, std::complex<T>* out, const std::complex<T>* in) {
+  circshift(out, in, g.Gx, g.Gy, g.Gz, (int)std::ceil(g.Gx / 2.0), (int)std::ceil(g.Gy / 2.0),
+            g.is3d() ? (int)std::floor(g.Gz / 2.0) : 0);
+}
+
+// zero_pad2d/3d (griddingSupport.cpp:457-547) and crop_center_region2d/3d
+// (griddingSupport.cpp:372-453): centre embed / extract.
+template <typename T>
+void zero_pad(const Geom<T>& g, std::complex<T>* grid, const std::complex<T>* img) {
+  std::fill(grid, grid + g.ngrid(), std::complex<T>(0, 0));
+  if (!g.is3d()) {
+    // zero_pad2d indexes the first image axis fastest (griddingSupport.cpp:488-489).
+    const int oy = (int)(((T)g.Ny * g.os / (T)2.0) - ((T)g.Ny / (T)2.0));
+    const int ox = (int)(((T)g.Nx * g.os / (T)2.0) - ((T)g.Nx / (T)2.0));
+    const int rowlen = (int)(g.Nx * g.os);
+    for (int b = 0; b < g.Ny; ++b)
+      for (int a = 0; a < g.Nx; ++a)
+        grid[(u64)(b + oy) * rowlen + (a + ox)] = img[(u64)b * g.Nx + a];
+  } else {
+    const int oy = (int)(((T)g.Ny * g.os / (T)2.0) - ((T)g.Ny / (T)2.0));
+    const int ox = (int)(((T)g.Nx * g.os / (T)2.0) - ((T)g.Nx / (T)2.0));
+    const int oz = (int)(((T)g.Nz * g.os / (T)2.0) - ((T)g.Nz / (T)2.0));
+    for (int z = 0; z < g.Nz; ++z)
+      for (int y = 0; y < g.Ny; ++y)
+        for (int x = 0; x < g.Nx; ++x) {
+          const u64 dst = (u64)(int)((z + oz) * g.Nx * g.Ny * g.os * g.os) + (u64)(x + ox) * (int)(g.Ny * g.os) + (y + oy);
+          grid[dst] = img[(u64)z * g.Nx * g.Ny + (u64)x * g.Ny + y];
+        }
+  }
+}
+template <typename T>
+void crop_center(const Geom<T>& g, std::complex<T>* img, const std::complex<T>* grid) {
+  const int oy = (int)(((T)g.Gy / (T)2.0) - ((T)g.Ny / (T)2.0));
+  const int ox = (int)(((T)g.Gx / (T)2.0) - ((T)g.Nx / (T)2.0));
+  const int oz = g.is3d() ? (int)(((T)g.Gz / (T)2.0) - ((T)g.Nz / (T)2.0)) : 0;
+  for (int z = 0; z < g.Nz; ++z)
+    for (int x = 0; x < g.Nx; ++x)
+      for (int y = 0; y < g.Ny; ++y)
+        img[(u64)z * g.Nx * g.Ny + (u64)x * g.Ny + y] =
+            grid[(u64)(z + oz) * g.Gx * g.Gy + (u64)(x + ox) * g.Gy + (y + oy)];
+}
+
+// In-place unnormalised FFT over the grid with the dimension order fftCPU.cpp
+// gives FFTW: plan_dft_2d(Gy, Gx), plan_dft_3d(Gz, Gy, Gx) (fftCPU.cpp:54, 84).
+template <typename T>
+void grid_fft(const Geom<T>& g, std::complex<T>* grid, int sign) {
+  if (!g.is3d()) {
+    const std::size_t dims[2] = {(std::size_t)g.Gy, (std::size_t)g.Gx};
+    fft_nd<T>(grid, dims, 2, sign);
+  } else {
+    const std::size_t dims[3] = {(std::size_t)g.Gz, (std::size_t)g.Gy, (std::size_t)g.Gx};
+    fft_nd<T>(grid, dims, 3, sign);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Backend hook: the composites below run either on the restated kernels or
+// on the reference's own compiled kernels (oracle/_ref/libpgref.so).
+// ---------------------------------------------------------------------------
+template <typename T>
+struct RefKernels {
+  // computeFd_CPU_Grid / computeFH_CPU_Grid wrappers
+  void (*fd)(int, const T*, const T*, const T*, const T*, int, int, int, T, T, T, const T*, u64, T*) = nullptr;
+  void (*fh)(int, const T*, const T*, const T*, const T*, int, int, int, T, T, T, const T*, u64, T*) = nullptr;
+  // ftCpu / iftCpu wrappers
+  void (*ft)(T*, T*, const T*, const T*, const T*, const T*, const T*, const T*, const T*, const T*,
+             const T*, const T*, int, int) = nullptr;
+  void (*ift)(T*, T*, const T*, const T*, const T*, const T*, const T*, const T*, const T*, const T*,
+              const T*, const T*, int, int) = nullptr;
+};
+template <typename T>
+RefKernels<T>& ref_kernels() {
+  static RefKernels<T> k;
+  return k;
+}
+
+// ---------------------------------------------------------------------------
+// Operators.  n1 = data length, n2 = image length (reference naming).
+// ---------------------------------------------------------------------------
+template <typename T>
+struct Op {
+  using C = std::complex<T>;
+  u64 n1 = 0, n2 = 0;
+  virtual ~Op() {}
+  virtual void forward(const C* x, C* y) const = 0;   // operator*
+  virtual void adjoint(const C* y, C* x) const = 0;   // operator/
+};
+
+// Gnufft (Gnufft.cpp:34-211).
+template <typename T>
+struct GnufftOp : Op<T> {
+  using C = std::complex<T>;
+  Geom<T> g;
+  std::vector<T> kx, ky, kz;
+  bool use_ref = false;
+
+  GnufftOp(u64 M, T gridos, int nx, int ny, int nz, const T* k1, const T* k2, const T* k3) {
+    this->n1 = (u64)nx * ny * nz;   // image (Gnufft names the image n1)
+    this->n2 = M;                   // samples
+    g = Geom<T>::make(nx, ny, nz, gridos);
+    kx.assign(k1, k1 + M); ky.assign(k2, k2 + M); kz.assign(k3, k3 + M);
+  }
+  u64 data_len() const { return this->n2; }
+  u64 image_len() const { return this->n1; }
+
+  // computeFd_CPU_Grid restated (gridding.cpp:584-727)
+  void forward(const C* x, C* y) const override {
+    const u64 M = this->n2;
+    if (use_ref && ref_kernels<T>().fd) {
+      ref_kernels<T>().fd((int)M, kx.data(), ky.data(), kz.data(), reinterpret_cast<const T*>(x), g.Nx, g.Ny,
+                          g.Nz, g.os, g.kw, g.beta, g.lut.data(), g.lut.size(), reinterpret_cast<T*>(y));
+      return;
+    }
+    std::vector<C> img(x, x + g.nimg());
+    deapodize(g, img.data());
+    std::vector<C> a(g.ngrid()), b(g.ngrid());
+    zero_pad(g, a.data(), img.data());
+    fftshift_grid(g, b.data(), a.data());
+    grid_fft(g, b.data(), -1);
+    ifftshift_grid(g, a.data(), b.data());
+    interp_forward(g, M, kx.data(), ky.data(), kz.data(), a.data(), y);
+  }
+  // computeFH_CPU_Grid restated (gridding.cpp:418-581)
+  void adjoint(const C* d, C* x) const override {
+    const u64 M = this->n2;
+    if (use_ref && ref_kernels<T>().fh) {
+      ref_kernels<T>().fh((int)M, kx.data(), ky.data(), kz.data(), reinterpret_cast<const T*>(d), g.Nx, g.Ny,
+                          g.Nz, g.os, g.kw, g.beta, g.lut.data(), g.lut.size(), reinterpret_cast<T*>(x));
+      return;
+    }
+    std::vector<C> a(g.ngrid(), C(0, 0)), b(g.ngrid());
+    spread_adjoint(g, M, kx.data(), ky.data(), kz.data(), d, a.data());
+    ifftshift_grid(g, b.data(), a.data());
+    grid_fft(g, b.data(), +1);
+    fftshift_grid(g, a.data(), b.data());
+    crop_center(g, x, a.data());
+    deapodize(g, x);
+  }
+};
+
+// Gdft (Gdft.cpp:33-136).  exact64 selects the FP64 oracle formula (double
+// sin/cos); otherwise the expression types of ftCpu / iftCpu are kept
+// (float sinf/cosf, ftCpu.cpp:104, 129-130, 203-204).
+template <typename T>
+struct GdftOp : Op<T> {
+  using C = std::complex<T>;
+  std::vector<T> kx, ky, kz, ix, iy, iz, fm, t;
+  bool exact64 = false;
+  bool use_ref = false;
+  GdftOp(u64 nk, u64 ni, const T* k1, const T* k2, const T* k3, const T* i1, const T* i2, const T* i3,
+         const T* f, const T* tt) {
+    this->n1 = nk; this->n2 = ni;
+    kx.assign(k1, k1 + nk); ky.assign(k2, k2 + nk); kz.assign(k3, k3 + nk);
+    ix.assign(i1, i1 + ni); iy.assign(i2, i2 + ni); iz.assign(i3, i3 + ni);
+    fm.assign(f, f + ni); t.assign(tt, tt + nk);
+  }
+  void forward(const C* x, C* y) const override {
+    const u64 nk = this->n1, ni = this->n2;
+    std::vector<T> xr(ni), xi(ni), yr(nk, 0), yi(nk, 0);
+    for (u64 j = 0; j < ni; ++j) { xr[j] = x[j].real(); xi[j] = x[j].imag(); }
+    if (use_ref && ref_kernels<T>().ft && !exact64) {
+      ref_kernels<T>().ft(yr.data(), yi.data(), xr.data(), xi.data(), kx.data(), ky.data(), kz.data(), ix.data(),
+                          iy.data(), iz.data(), fm.data(), t.data(), (int)nk, (int)ni);
+    } else if (exact64) {
+      const double tpi = 2.0 * kPiD;
+      for (u64 i = 0; i < nk; ++i) {
+        double sr = 0, si = 0;
+        for (u64 j = 0; j < ni; ++j) {
+          double ph = tpi * ((double)kx[i] * ix[j] + (double)ky[i] * iy[j] + (double)kz[i] * iz[j]) +
+                      (double)fm[j] * t[i];
+          double s = std::sin(ph), c = std::cos(ph);
+          sr += c * xr[j] + s * xi[j];
+          si += -s * xr[j] + c * xi[j];
+        }
+        yr[i] = (T)sr; yi[i] = (T)si;
+      }
+    } else {
+      // ftCpu.cpp:115-138
+      for (u64 i = 0; i < nk; ++i) {
+        T sr = 0.0, si = 0.0;
+        T a = kx[i] * 2 * kPiF, b = ky[i] * 2 * kPiF, c = kz[i] * 2 * kPiF;
+        T ti = t[i];
+        for (u64 j = 0; j < ni; ++j) {
+          T e = (a * ix[j] + b * iy[j] + c * iz[j] + (fm[j] * ti));
+          float s = sinf(e);
+          float co = cosf(e);
+          sr += (co * xr[j]) + (s * xi[j]);
+          si += (-s * xr[j]) + (co * xi[j]);
+        }
+        yr[i] = sr; yi[i] = si;
+      }
+    }
+    for (u64 i = 0; i < nk; ++i) y[i] = C(yr[i], yi[i]);
+  }
+  void adjoint(const C* y, C* x) const override {
+    const u64 nk = this->n1, ni = this->n2;
+    std::vector<T> yr(nk), yi(nk), xr(ni, 0), xi(ni, 0);
+    for (u64 i = 0; i < nk; ++i) { yr[i] = y[i].real(); yi[i] = y[i].imag(); }
+    if (use_ref && ref_kernels<T>().ift && !exact64) {
+      ref_kernels<T>().ift(xr.data(), xi.data(), yr.data(), yi.data(), kx.data(), ky.data(), kz.data(), ix.data(),
+                           iy.data(), iz.data(), fm.data(), t.data(), (int)nk, (int)ni);
+    } else if (exact64) {
+      const double tpi = 2.0 * kPiD;
+      for (u64 j = 0; j < ni; ++j) {
+        double sr = 0, si = 0;
+        for (u64 i = 0; i < nk; ++i) {
+          double ph = tpi * ((double)kx[i] * ix[j] + (double)ky[i] * iy[j] + (double)kz[i] * iz[j]) +
+                      (double)fm[j] * t[i];
+          double s = std::sin(ph), c = std::cos(ph);
+          sr += c * yr[i] - s * yi[i];
+          si += s * yr[i] + c * yi[i];
+        }
+        xr[j] = (T)sr; xi[j] = (T)si;
+      }
+    } else {
+      // iftCpu.cpp:164-212
+      T tpi = kPiF * 2.0;
+      for (u64 j = 0; j < ni; ++j) {
+        T sr = 0.0, si = 0.0;
+        T ax = ix[j] * tpi, ay = iy[j] * tpi, az = iz[j] * tpi;
+        T f = fm[j];
+        for (u64 i = 0; i < nk; ++i) {
+          T e = (kx[i] * ax + ky[i] * ay + kz[i] * az + (f * t[i]));
+          T s = sinf(e);
+          T co = cosf(e);
+          sr += (co * yr[i]) - (s * yi[i]);
+          si += (s * yr[i]) + (co * yi[i]);
+        }
+        xr[j] = sr; xi[j] = si;
+      }
+    }
+    for (u64 j = 0; j < ni; ++j) x[j] = C(xr[j], xi[j]);
+  }
+};
+
+template <typename T>
+struct SenseOp;
+
+// Data/image lengths of any operator: Gnufft names the image n1
+// (Gnufft.cpp:42-43) and SENSE's n1 is the per-coil data length
+// (SENSE.cpp:36, 42), so both need a translation.
+template <typename T>
+inline u64 op_data_len(const Op<T>& op);
+template <typename T>
+inline u64 op_image_len(const Op<T>& op) {
+  if (auto* g = dynamic_cast<const GnufftOp<T>*>(&op)) return g->image_len();
+  return op.n2;
+}
+
+// TimeSegmentation with the Hanning interpolator (TimeSegmentation.cpp:37-93,
+// 213-218) and its operators (:252-324).  Holds a non-owning pointer to G,
+// like the reference (TimeSegmentation.cpp:53).
+template <typename T>
+struct TimeSegOp : Op<T> {
+  using C = std::complex<T>;
+  const Op<T>* G;
+  int L;
+  u64 nshots;
+  T tau, tmin;
+  std::vector<C> AA;   // n1 x L, column-major (AA[m + n1*l])
+  std::vector<C> Wo;   // n2 x (L+1)
+  std::vector<C> WoH;
+
+  TimeSegOp(const Op<T>* g, const T* fieldmap, const T* tvec, u64 a, u64 b, u64 nsegs, u64 interptype, u64 shots)
+      : G(g) {
+    this->n1 = a; this->n2 = b;
+    L = (nsegs == 0 || nsegs == 1) ? 1 : (int)nsegs;
+    if (interptype != 1 && L > 1) throw std::runtime_error("oracle: only the Hanning interpolator (type 1) is restated");
+    nshots = shots;
+    std::vector<T> tv(tvec, tvec + a);
+    T mn = *std::min_element(tv.begin(), tv.end());
+    T mx = *std::max_element(tv.begin(), tv.end());
+    tmin = mn;
+    T rangt = mx - tmin;
+    tau = (rangt + std::numeric_limits<double>::epsilon()) / L;
+    for (auto& v : tv) v = v - tmin;
+    const u64 none = a / shots;
+    if (L <= 1) {
+      L = 1; tau = 0;
+      AA.assign(a * 2, C(1, 0));
+      Wo.assign(b, C(1, 0));
+      WoH.assign(b, C(1, 0));
+    } else {
+      std::vector<C> one(none * L);
+      for (unsigned int l = 0; l < (unsigned)L; ++l)
+        for (unsigned int m = 0; m < none; ++m) {
+          if ((std::abs(tv[m] - ((l) * tau))) <= tau)
+            one[m + none * l] = C(0.5 + 0.5 * std::cos((kPiD) * (tv[m] - ((l) * tau)) / tau), 0);
+          else
+            one[m + none * l] = C(0, 0);
+        }
+      AA.resize(a * L);
+      for (int l = 0; l < L; ++l)
+        for (u64 m = 0; m < a; ++m) AA[m + a * l] = one[(m % none) + none * l];
+      Wo.resize(b * (L + 1));
+      WoH.resize(b * (L + 1));
+      for (unsigned int l = 0; l < (unsigned)L + 1; ++l) {
+        T s = (l) * tau + tmin;
+        for (u64 p = 0; p < b; ++p) {
+          T v = fieldmap[p] * s;
+          Wo[p + b * l] = C(std::cos(v), -std::sin(v));
+          WoH[p + b * l] = C(std::cos(v), std::sin(v));
+        }
+      }
+    }
+  }
+  void forward(const C* x, C* y) const override {
+    const u64 n1 = this->n1, n2 = this->n2;
+    std::vector<C> tmp(n2), out(n1);
+    std::fill(y, y + n1, C(0, 0));
+    for (int l = 0; l < L; ++l) {
+      for (u64 p = 0; p < n2; ++p) tmp[p] = Wo[p + n2 * l] * x[p];
+      G->forward(tmp.data(), out.data());
+      for (u64 m = 0; m < n1; ++m) y[m] += out[m] * AA[m + n1 * l];
+    }
+  }
+  void adjoint(const C* d, C* x) const override {
+    const u64 n1 = this->n1, n2 = this->n2;
+    std::vector<C> tmp(n1), img(n2);
+    std::fill(x, x + n2, C(0, 0));
+    for (int l = 0; l < L; ++l) {
+      for (u64 m = 0; m < n1; ++m) tmp[m] = std::conj(AA[m + n1 * l]) * d[m];
+      G->adjoint(tmp.data(), img.data());
+      for (u64 p = 0; p < n2; ++p) x[p] += img[p] * WoH[p + n2 * l];
+    }
+  }
+};
+
+// SENSE coil loop (SENSE.cpp:33-97); non-owning pointer to G (SENSE.cpp:39).
+template <typename T>
+struct SenseOp : Op<T> {
+  using C = std::complex<T>;
+  const Op<T>* G;
+  u64 nc;
+  std::vector<C> S;  // n2 x nc
+  SenseOp(const Op<T>* g, const C* smap, u64 a, u64 b, u64 c) : G(g), nc(c) {
+    this->n1 = a; this->n2 = b;
+    S.assign(smap, smap + b * c);
+  }
+  void forward(const C* x, C* y) const override {
+    const u64 n1 = this->n1, n2 = this->n2;
+    std::vector<C> tmp(n2);
+    for (u64 c = 0; c < nc; ++c) {
+      for (u64 p = 0; p < n2; ++p) tmp[p] = S[p + n2 * c] * x[p];
+      G->forward(tmp.data(), y + n1 * c);
+    }
+  }
+  void adjoint(const C* d, C* x) const override {
+    const u64 n1 = this->n1, n2 = this->n2;
+    std::vector<C> img(n2);
+    std::fill(x, x + n2, C(0, 0));
+    for (u64 c = 0; c < nc; ++c) {
+      G->adjoint(d + n1 * c, img.data());
+      for (u64 p = 0; p < n2; ++p) x[p] += img[p] * std::conj(S[p + n2 * c]);
+    }
+  }
+};
+
+template <typename T>
+inline u64 op_data_len(const Op<T>& op) {
+  if (auto* g = dynamic_cast<const GnufftOp<T>*>(&op)) return g->data_len();
+  if (auto* s = dynamic_cast<const SenseOp<T>*>(&op)) return s->n1 * s->nc;
+  return op.n1;
+}
+
+// pcSenseTimeSeg (pcSenseTimeSeg.cpp:41-171): per-shot Gnufft + TimeSegmentation.
+template <typename T>
+struct PcSenseTimeSegOp : Op<T> {
+  using C = std::complex<T>;
+  u64 Ni, Nc, Ns, Nd;
+  std::vector<std::unique_ptr<GnufftOp<T>>> G;
+  std::vector<std::unique_ptr<TimeSegOp<T>>> A;
+  std::vector<C> M, Mc;  // Ni x (Nc*Ns), column s + c*Ns
+  PcSenseTimeSegOp(const T* kx, const T* ky, const T* kz, u64 nk, int nx, int ny, int nz, u64 nc, const T* t,
+                   u64 L, u64 type, const C* smap, const T* fmap, const T* pmap, u64 npmap, bool use_ref) {
+    Ni = (u64)nx * ny * nz; Nc = nc; Ns = npmap / Ni; Nd = nk / Ns;
+    this->n1 = Nd * Ns * Nc; this->n2 = Ni;
+    for (u64 s = 0; s < Ns; ++s) {
+      G.emplace_back(new GnufftOp<T>(Nd, (T)2.0, nx, ny, nz, kx + s * Nd, ky + s * Nd, kz + s * Nd));
+      G.back()->use_ref = use_ref;
+      A.emplace_back(new TimeSegOp<T>(G.back().get(), fmap, t + s * Nd, Nd, Ni, L, type, 1));
+    }
+    M.resize(Ni * Nc * Ns); Mc.resize(Ni * Nc * Ns);
+    for (u64 c = 0; c < Nc; ++c)
+      for (u64 s = 0; s < Ns; ++s)
+        for (u64 p = 0; p < Ni; ++p) {
+          T ph = pmap[p + Ni * s];
+          C e(std::cos(ph), -std::sin(ph));
+          M[p + Ni * (s + c * Ns)] = smap[p + Ni * c] * e;
+          Mc[p + Ni * (s + c * Ns)] = std::conj(smap[p + Ni * c]) * std::conj(e);
+        }
+  }
+  void forward(const C* x, C* y) const override {
+    std::vector<C> tmp(Ni);
+    for (u64 c = 0; c < Nc; ++c)
+      for (u64 s = 0; s < Ns; ++s) {
+        const C* m = M.data() + Ni * (s + c * Ns);
+        for (u64 p = 0; p < Ni; ++p) tmp[p] = x[p] * m[p];
+        A[s]->forward(tmp.data(), y + Nd * (s + c * Ns));
+      }
+  }
+  void adjoint(const C* d, C* x) const override {
+    std::vector<C> img(Ni);
+    std::fill(x, x + Ni, C(0, 0));
+    for (u64 c = 0; c < Nc; ++c)
+      for (u64 s = 0; s < Ns; ++s) {
+        A[s]->adjoint(d + Nd * (s + c * Ns), img.data());
+        const C* m = Mc.data() + Ni * (s + c * Ns);
+        for (u64 p = 0; p < Ni; ++p) x[p] += m[p] * img[p];
+      }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Regularizers (Robject.cpp:49-193, QuadPenalty.cpp:45-64, TVPenalty.cpp:43-68)
+// ---------------------------------------------------------------------------
+template <typename T>
+struct Penalty {
+  using C = std::complex<T>;
+  int kind = 0;  // 0 quadratic, 1 TV
+  u64 Nx = 1, Ny = 1, Nz = 1;
+  T beta = 0, delta = 1;
+  u64 dims2pen = 3;
+  u64 nd() const { return (Nz == 1 || dims2pen == 2) ? 2 : 3; }
+  u64 offset(u64 dim) const { return dim == 0 ? 1 : dim == 1 ? Ny : Nx * Ny; }
+
+  // Cd: out[i] = d[i] - d[i-off] for i >= off, else 0 (Robject.cpp:76-79).
+  void Cd(const C* d, u64 dim, C* out) const {
+    const u64 N = Nx * Ny * Nz, off = offset(dim);
+    std::fill(out, out + N, C(0, 0));
+    for (u64 i = off; i < N; ++i) out[i] = d[i] - d[i - off];
+  }
+  // Ctd exactly as Robject.cpp:111-117 (not the exact adjoint of Cd).
+  void Ctd(const C* d, u64 dim, C* out) const {
+    const u64 N = Nx * Ny * Nz, off = offset(dim);
+    std::fill(out, out + N, C(0, 0));
+    out[off - 1] = -d[off];
+    out[N - 1 - off] = d[N - 1 - off];
+    for (u64 i = off; i < N - 1; ++i) out[i - off] = d[i - off] - d[i];
+  }
+  C wpot(C d) const {
+    if (kind == 0) return C(1, 0);
+    T a = std::abs(d / delta);
+    return C((T)1 / std::sqrt((T)1 + a * a), 0);
+  }
+  C dpot(C d) const {
+    if (kind == 0) return d;
+    T a = std::abs(d / delta);
+    return d / std::sqrt((T)1 + a * a);
+  }
+  void Gradient(const C* x, C* g) const {
+    const u64 N = Nx * Ny * Nz;
+    std::vector<C> d(N), e(N);
+    std::fill(g, g + N, C(0, 0));
+    for (u64 dim = 0; dim < nd(); ++dim) {
+      Cd(x, dim, d.data());
+      for (u64 i = 0; i < N; ++i) d[i] = dpot(d[i]);
+      Ctd(d.data(), dim, e.data());
+      for (u64 i = 0; i < N; ++i) g[i] += e[i];
+    }
+    for (u64 i = 0; i < N; ++i) g[i] = beta * g[i];
+  }
+  C Denom(const C* ddir, const C* x) const {
+    const u64 N = Nx * Ny * Nz;
+    std::vector<C> cdir(N), cx(N);
+    C pen(0, 0);
+    for (u64 dim = 0; dim < nd(); ++dim) {
+      Cd(ddir, dim, cdir.data());
+      Cd(x, dim, cx.data());
+      C acc(0, 0);
+      for (u64 i = 0; i < N; ++i) acc += std::conj(cdir[i]) * (wpot(cx[i]) * cdir[i]);
+      pen += acc;
+    }
+    return pen * C(beta, 0);
+  }
+};
+
+template <typename T>
+inline std::complex<T> cdot(const std::complex<T>* a, const std::complex<T>* b, u64 n) {
+  std::complex<T> s(0, 0);
+  for (u64 i = 0; i < n; ++i) s += std::conj(a[i]) * b[i];
+  return s;
+}
+
+// solve_pwls_pcg (solve_pwls_pcg.hpp:48-167), scalars complex<T> as in the reference.
+// Returns the number of completed iterations.
+template <typename T>
+int pwls_pcg(const Op<T>& A, const std::complex<T>* x0, const T* W, const std::complex<T>* y,
+             const Penalty<T>& R, u64 niter, std::complex<T>* xout) {
+  using C = std::complex<T>;
+  const u64 nd = op_data_len(A), ni = op_image_len(A);
+  std::vector<C> x(x0, x0 + ni), Ax(nd), r(nd), ngrad(ni), ddir(ni, C(0, 0)), Adir(nd), pgrad(ni), xs(ni);
+  A.forward(x.data(), Ax.data());
+  C oldinprod = 0, gamma = 0;
+  // norm_grad denominator real(y' * (W % y)) (solve_pwls_pcg.hpp:42-46)
+  T ywy = 0;
+  {
+    C s(0, 0);
+    for (u64 m = 0; m < nd; ++m) s += std::conj(y[m]) * (W[m] * y[m]);
+    ywy = s.real();
+  }
+  int done = 0;
+  for (u64 it = 0; it < niter; ++it) {
+    for (u64 m = 0; m < nd; ++m) r[m] = W[m] * (y[m] - Ax[m]);
+    A.adjoint(r.data(), ngrad.data());
+    T gn = 0;
+    for (u64 j = 0; j < ni; ++j) gn += std::norm(ngrad[j]);
+    if (std::sqrt(gn) / ywy < 1e-10) break;
+    R.Gradient(x.data(), pgrad.data());
+    for (u64 j = 0; j < ni; ++j) ngrad[j] -= pgrad[j];
+    C newinprod = cdot(ngrad.data(), ngrad.data(), ni).real();
+    if (it == 0) {
+      ddir = ngrad;
+    } else {
+      gamma = (std::abs(oldinprod) < 1e-10) ? C(0, 0) : newinprod / oldinprod;
+      for (u64 j = 0; j < ni; ++j) ddir[j] = ngrad[j] + gamma * ddir[j];
+    }
+    oldinprod = newinprod;
+    if (cdot(ddir.data(), ngrad.data(), ni).real() < 0) break;
+    A.forward(ddir.data(), Adir.data());
+    C dAWAd = 0, dAWr = 0;
+    {
+      C s1(0, 0), s2(0, 0);
+      for (u64 m = 0; m < nd; ++m) {
+        s1 += std::conj(Adir[m]) * (W[m] * Adir[m]);
+        s2 += std::conj(Adir[m]) * (W[m] * (y[m] - Ax[m]));
+      }
+      dAWAd = s1.real();
+      dAWr = s2.real();
+    }
+    C step = 0;
+    bool stop = false;
+    for (int j = 0; j < 3; ++j) {
+      for (u64 p = 0; p < ni; ++p) xs[p] = x[p] + step * ddir[p];
+      C pdenom = R.Denom(ddir.data(), xs.data());
+      C denom = dAWAd + pdenom;
+      if (std::abs(denom) < 1e-20 || std::abs(denom) > 1e25) { stop = true; break; }
+      R.Gradient(xs.data(), pgrad.data());
+      C pdot = cdot(ddir.data(), pgrad.data(), ni).real();
+      step -= (-dAWr + step * dAWAd + pdot) / denom;
+    }
+    if (stop) break;
+    for (u64 m = 0; m < nd; ++m) Ax[m] += step * Adir[m];
+    for (u64 p = 0; p < ni; ++p) x[p] += step * ddir[p];
+    done = (int)it + 1;
+  }
+  std::copy(x.begin(), x.end(), xout);
+  return done;
+}
+
+}  // namespace pgo

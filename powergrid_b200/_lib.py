@@ -1,0 +1,109 @@
+"""ctypes binding of libpowergrid_b200.so (the C ABI in include/powergrid_b200.h).
+
+There is no CPU fallback: if the CUDA library is missing or no sm_100a GPU
+is present, every operator constructor raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libpowergrid_b200.so")
+
+P = C.c_void_p
+U64 = C.c_uint64
+F32 = C.c_float
+
+STATUS = {0: "PG_OK", 1: "PG_INVALID_ARG", 2: "PG_OUT_OF_MEMORY", 3: "PG_CUDA_ERROR", 4: "PG_TIMEOUT",
+          5: "PG_CANCELLED", 6: "PG_NOT_INITIALIZED", 7: "PG_CUFFT_ERROR", 8: "PG_REJECTED", 9: "PG_NOT_READY"}
+PG_OK, PG_NOT_READY = 0, 9
+
+
+class PGError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Penalty(C.Structure):
+    _fields_ = [("kind", C.c_int), ("nx", U64), ("ny", U64), ("nz", U64), ("beta", F32), ("delta", F32),
+                ("dims2penalize", U64)]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", U64), ("max_inflight", C.c_uint32), ("streams", C.c_uint32)]
+
+
+class Request(C.Structure):
+    _fields_ = [("nx", U64), ("ny", U64), ("nz", U64), ("nc", U64), ("n_samples", U64), ("L", U64), ("niter", U64),
+                ("beta", F32), ("kx", P), ("ky", P), ("kz", P), ("t", P), ("field_map", P), ("sense_map", P),
+                ("data", P), ("image_out", P)]
+
+
+class RequestStats(C.Structure):
+    _fields_ = [("t_submit_ms", C.c_double), ("t_start_ms", C.c_double), ("t_done_ms", C.c_double),
+                ("iters_done", U64), ("bytes_resident", U64), ("status", C.c_int)]
+
+
+_lib = None
+
+# Every symbol the header declares, with its ctypes signature.
+SIGNATURES = {
+    "pg_init": (C.c_int, [C.c_int]),
+    "pg_shutdown": (C.c_int, []),
+    "pg_status_string": (C.c_char_p, [C.c_int]),
+    "pg_last_error": (C.c_char_p, []),
+    "pg_kernel_launch_count": (U64, []),
+    "pg_gnufft_create": (C.c_int, [C.POINTER(P), U64, F32, U64, U64, U64, P, P, P]),
+    "pg_gdft_create": (C.c_int, [C.POINTER(P), U64, U64, P, P, P, P, P, P, P, P]),
+    "pg_timeseg_create": (C.c_int, [C.POINTER(P), P, P, P, U64, U64, U64, U64, U64]),
+    "pg_sense_create": (C.c_int, [C.POINTER(P), P, P, U64, U64, U64]),
+    "pg_pcsense_timeseg_create": (C.c_int, [C.POINTER(P), P, P, P, U64, U64, U64, U64, U64, P, U64, U64, P, P, P,
+                                            U64]),
+    "pg_op_destroy": (C.c_int, [P]),
+    "pg_op_shape": (C.c_int, [P, C.POINTER(U64), C.POINTER(U64)]),
+    "pg_op_forward": (C.c_int, [P, P, P]),
+    "pg_op_adjoint": (C.c_int, [P, P, P]),
+    "pg_op_forward_device": (C.c_int, [P, P, P, P]),
+    "pg_op_adjoint_device": (C.c_int, [P, P, P, P]),
+    "pg_pcg_solve": (C.c_int, [P, P, P, P, C.POINTER(Penalty), U64, P, C.POINTER(U64)]),
+    "pg_pcg_solve_device": (C.c_int, [P, P, P, P, C.POINTER(Penalty), U64, P, P, P]),
+    "pg_recon_solve": (C.c_int, [P, C.POINTER(Penalty), P, U64, P]),
+    "pg_penalty_gradient_device": (C.c_int, [C.POINTER(Penalty), P, P, P]),
+    "pg_penalty_denom_device": (C.c_int, [C.POINTER(Penalty), P, P, C.POINTER(C.c_double)]),
+    "pg_server_create": (C.c_int, [C.POINTER(P), C.POINTER(ServerConfig)]),
+    "pg_server_destroy": (C.c_int, [P]),
+    "pg_submit": (C.c_int, [P, C.POINTER(Request), C.POINTER(U64)]),
+    "pg_poll": (C.c_int, [P, U64, C.POINTER(RequestStats)]),
+    "pg_wait": (C.c_int, [P, U64, C.POINTER(RequestStats)]),
+    "pg_cancel": (C.c_int, [P, U64]),
+    "pg_request_footprint": (U64, [C.POINTER(Request)]),
+    "pg_debug_fail_allocation_after": (None, [U64]),
+    "pg_util_kb_lut": (U64, [F32, P, U64, C.POINTER(F32)]),
+    "pg_util_gnufft_binning": (C.c_int, [P, P, P, C.POINTER(U64)]),
+}
+
+
+def load() -> C.CDLL:
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"powergrid_b200: CUDA library missing at {LIB_PATH}; run __graft_entry__.build()")
+        lib = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != PG_OK:
+        raise PGError(status, load().pg_last_error().decode(errors="replace"))
+
+
+def launches() -> int:
+    return int(load().pg_kernel_launch_count())

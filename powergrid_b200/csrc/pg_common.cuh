@@ -1,0 +1,117 @@
+// Shared infrastructure of the sm_100a library: status/error plumbing,
+// device buffers with an allocation-failure hook, complex helpers and the
+// kernel-launch counter.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <atomic>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "powergrid_b200.h"
+
+namespace pg {
+
+pg_status set_error(pg_status s, const char* fmt, ...);
+pg_status ensure_init();
+cudaStream_t default_stream();
+int sm_count();
+
+// Counts this library's kernel launches (reported by bench.py).
+extern std::atomic<uint64_t> g_launches;
+inline void count_launch(uint64_t n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+// Host-side fault injection: the n-th allocation from the arm point fails.
+extern std::atomic<uint64_t> g_fail_alloc_countdown;
+
+pg_status dev_alloc(void** p, size_t bytes);
+void dev_free(void* p);
+
+#define PG_CUDA(call)                                                                              \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess)                                                                         \
+      return ::pg::set_error(PG_CUDA_ERROR, "%s:%d %s: %s", __FILE__, __LINE__, #call,            \
+                             cudaGetErrorString(e_));                                              \
+  } while (0)
+
+#define PG_CUFFT(call)                                                                             \
+  do {                                                                                             \
+    cufftResult r_ = (call);                                                                       \
+    if (r_ != CUFFT_SUCCESS)                                                                       \
+      return ::pg::set_error(PG_CUFFT_ERROR, "%s:%d %s: cufft error %d", __FILE__, __LINE__, #call, \
+                             (int)r_);                                                             \
+  } while (0)
+
+#define PG_TRY(call)                \
+  do {                              \
+    pg_status s_ = (call);          \
+    if (s_ != PG_OK) return s_;     \
+  } while (0)
+
+// Kernel launch followed by a launch-error check.
+#define PG_LAUNCH(kernel, grid, block, smem, stream, ...)                                          \
+  do {                                                                                             \
+    kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);                                    \
+    ::pg::count_launch();                                                                          \
+    cudaError_t e_ = cudaGetLastError();                                                           \
+    if (e_ != cudaSuccess)                                                                         \
+      return ::pg::set_error(PG_CUDA_ERROR, "%s:%d launch %s: %s", __FILE__, __LINE__, #kernel,    \
+                             cudaGetErrorString(e_));                                              \
+  } while (0)
+
+// Owning device buffer.
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) { reset(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    return *this;
+  }
+  ~DevBuf() { reset(); }
+  void reset() {
+    if (p) dev_free(p);
+    p = nullptr;
+    n = 0;
+  }
+  pg_status alloc(size_t count) {
+    if (count == n && p) return PG_OK;
+    reset();
+    if (count == 0) return PG_OK;
+    void* q = nullptr;
+    PG_TRY(dev_alloc(&q, count * sizeof(T)));
+    p = static_cast<T*>(q);
+    n = count;
+    return PG_OK;
+  }
+  pg_status upload(const T* host, size_t count, cudaStream_t s) {
+    PG_TRY(alloc(count));
+    if (count) PG_CUDA(cudaMemcpyAsync(p, host, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    return PG_OK;
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+// ---- complex helpers (float2 = interleaved complex64) ----------------------
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(__fsub_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)),
+                     __fadd_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+}
+__host__ __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+__host__ __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+
+inline unsigned ceil_div(uint64_t a, uint64_t b) { return (unsigned)((a + b - 1) / b); }
+
+}  // namespace pg

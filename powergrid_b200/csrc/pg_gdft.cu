@@ -1,0 +1,276 @@
+// Exact field-corrected DFT (Gdft) for sm_100a.
+//
+// Reference: ftCpu / iftCpu (ftCpu.cpp:95-215), called by Gdft (Gdft.cpp:53-136):
+//   forward  y_i = sum_j x_j exp(-i (2pi k_i . r_j + FM_j t_i))
+//   adjoint  x_j = sum_i y_i exp(+i (2pi k_i . r_j + FM_j t_i))
+// The reference evaluates the phase and sinf/cosf in FP32.  Here the phase
+// is formed with FP64 products and reduced mod 2pi in FP64, then one FP32
+// __sincosf serves every coil of the pair; the complex MACs are FP32 with a
+// two-level (per-tile, then running) sum.
+//
+// Layout: one thread per output (sample for forward, voxel for adjoint);
+// the other side is staged in shared-memory tiles of 128 entries.  When the
+// outputs alone do not fill the GPU the inner sum is split over blockIdx.y
+// and the partial sums are combined in a fixed order (deterministic).
+#include "pg_gdft.cuh"
+
+namespace pg {
+
+namespace {
+constexpr int kTile = 128;
+constexpr int kCoilChunk = 8;
+
+__device__ __forceinline__ void phase_sincos(double ph, float* s, float* c) {
+  const double inv2pi = 0.15915494309189533577;   // 1 / (2 pi)
+  const double twopi = 6.283185307179586476925;    // 2 pi (double)
+  const double n = rint(ph * inv2pi);
+  const float r = (float)fma(-n, twopi, ph);      // |r| <= pi
+  __sincosf(r, s, c);
+}
+}  // namespace
+
+// Forward partial sums.  ks[i] = (2pi kx, 2pi ky, 2pi kz, t); vs[j] = (ix, iy, iz, FM).
+// xin: nc x ni inputs (already multiplied by the coil maps).
+template <int NC>
+__global__ void __launch_bounds__(kTile) k_dft_forward(uint64_t nk, uint64_t ni, const double4* __restrict__ ks,
+                                                       const double4* __restrict__ vs,
+                                                       const float2* __restrict__ xin, uint64_t jchunk,
+                                                       float2* __restrict__ part) {
+  __shared__ double4 sv[kTile];
+  __shared__ float2 sx[NC][kTile];
+  const uint64_t i = (uint64_t)blockIdx.x * kTile + threadIdx.x;
+  const uint64_t j0 = (uint64_t)blockIdx.y * jchunk;
+  const uint64_t j1 = min(ni, j0 + jchunk);
+  double4 k = make_double4(0, 0, 0, 0);
+  if (i < nk) k = ks[i];
+  float2 tot[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) tot[c] = make_float2(0.f, 0.f);
+  for (uint64_t jt = j0; jt < j1; jt += kTile) {
+    const int n = (int)((j1 - jt) < (uint64_t)kTile ? (j1 - jt) : (uint64_t)kTile);
+    __syncthreads();
+    if (threadIdx.x < n) {
+      sv[threadIdx.x] = vs[jt + threadIdx.x];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) sx[c][threadIdx.x] = xin[(uint64_t)c * ni + jt + threadIdx.x];
+    }
+    __syncthreads();
+    float2 acc[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) acc[c] = make_float2(0.f, 0.f);
+    for (int j = 0; j < n; ++j) {
+      const double4 v = sv[j];
+      const double ph = fma(k.x, v.x, fma(k.y, v.y, fma(k.z, v.z, v.w * k.w)));
+      float s, co;
+      phase_sincos(ph, &s, &co);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const float2 x = sx[c][j];
+        acc[c].x = fmaf(co, x.x, fmaf(s, x.y, acc[c].x));
+        acc[c].y = fmaf(co, x.y, fmaf(-s, x.x, acc[c].y));
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < NC; ++c) { tot[c].x += acc[c].x; tot[c].y += acc[c].y; }
+  }
+  if (i < nk) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) part[((uint64_t)blockIdx.y * NC + c) * nk + i] = tot[c];
+  }
+}
+
+// Adjoint partial sums.  yin: nc x nk data (coil-major, stride dstride).
+template <int NC>
+__global__ void __launch_bounds__(kTile) k_dft_adjoint(uint64_t nk, uint64_t ni, const double4* __restrict__ ks,
+                                                       const double4* __restrict__ vs,
+                                                       const float2* __restrict__ yin, uint64_t dstride,
+                                                       uint64_t ichunk, float2* __restrict__ part) {
+  __shared__ double4 sk[kTile];
+  __shared__ float2 sy[NC][kTile];
+  const uint64_t j = (uint64_t)blockIdx.x * kTile + threadIdx.x;
+  const uint64_t i0 = (uint64_t)blockIdx.y * ichunk;
+  const uint64_t i1 = min(nk, i0 + ichunk);
+  double4 v = make_double4(0, 0, 0, 0);
+  if (j < ni) v = vs[j];
+  float2 tot[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) tot[c] = make_float2(0.f, 0.f);
+  for (uint64_t it = i0; it < i1; it += kTile) {
+    const int n = (int)((i1 - it) < (uint64_t)kTile ? (i1 - it) : (uint64_t)kTile);
+    __syncthreads();
+    if (threadIdx.x < n) {
+      sk[threadIdx.x] = ks[it + threadIdx.x];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) sy[c][threadIdx.x] = yin[(uint64_t)c * dstride + it + threadIdx.x];
+    }
+    __syncthreads();
+    float2 acc[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) acc[c] = make_float2(0.f, 0.f);
+    for (int q = 0; q < n; ++q) {
+      const double4 k = sk[q];
+      const double ph = fma(k.x, v.x, fma(k.y, v.y, fma(k.z, v.z, v.w * k.w)));
+      float s, co;
+      phase_sincos(ph, &s, &co);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const float2 y = sy[c][q];
+        acc[c].x = fmaf(co, y.x, fmaf(-s, y.y, acc[c].x));
+        acc[c].y = fmaf(s, y.x, fmaf(co, y.y, acc[c].y));
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < NC; ++c) { tot[c].x += acc[c].x; tot[c].y += acc[c].y; }
+  }
+  if (j < ni) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) part[((uint64_t)blockIdx.y * NC + c) * ni + j] = tot[c];
+  }
+}
+
+// x_c = S_c * x (SENSE.cpp:59-63), for coils [c0, c0+nc).
+__global__ void k_apply_maps(uint64_t ni, int nc, int c0, const float2* __restrict__ S, const float2* __restrict__ x,
+                             float2* __restrict__ out) {
+  const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ni) return;
+  const float2 xv = x[j];
+  for (int c = 0; c < nc; ++c) out[(uint64_t)c * ni + j] = S ? cmul(S[(uint64_t)(c0 + c) * ni + j], xv) : xv;
+}
+
+// Forward finalize: y_c[i] = sum over splits (fixed order).
+__global__ void k_forward_finish(uint64_t nk, int nc, int nsplit, int ncpad, const float2* __restrict__ part,
+                                 float2* __restrict__ y, uint64_t dstride) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nk) return;
+  for (int c = 0; c < nc; ++c) {
+    float2 s = part[(uint64_t)c * nk + i];
+    for (int q = 1; q < nsplit; ++q) s = cadd(s, part[((uint64_t)q * ncpad + c) * nk + i]);
+    y[(uint64_t)c * dstride + i] = s;
+  }
+}
+
+// Adjoint finalize: x_j (+)= sum_c img_c * conj(S_c) (SENSE.cpp:84-96).
+__global__ void k_adjoint_finish(uint64_t ni, int nc, int c0, int nsplit, int ncpad, const float2* __restrict__ part,
+                                 const float2* __restrict__ S, int accumulate, float2* __restrict__ x) {
+  const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ni) return;
+  float2 acc = accumulate ? x[j] : make_float2(0.f, 0.f);
+  for (int c = 0; c < nc; ++c) {
+    float2 s = part[(uint64_t)c * ni + j];
+    for (int q = 1; q < nsplit; ++q) s = cadd(s, part[((uint64_t)q * ncpad + c) * ni + j]);
+    if (S) s = cmul(s, cconj(S[(uint64_t)(c0 + c) * ni + j]));
+    acc = (c == 0 && !accumulate) ? s : cadd(acc, s);
+  }
+  x[j] = acc;
+}
+
+pg_status gdft_plan_create(std::unique_ptr<GdftPlan>* out, uint64_t nk, uint64_t ni, const float* kx, const float* ky,
+                           const float* kz, const float* ix, const float* iy, const float* iz, const float* fm,
+                           const float* t, cudaStream_t s) {
+  if (nk == 0 || ni == 0) return set_error(PG_INVALID_ARG, "Gdft: empty operator");
+  auto p = std::make_unique<GdftPlan>();
+  p->nk = nk;
+  p->ni = ni;
+  const double tpi = 6.283185307179586476925;
+  std::vector<double4> ks(nk), vs(ni);
+  for (uint64_t i = 0; i < nk; ++i) {
+    if (!(std::isfinite(kx[i]) && std::isfinite(ky[i]) && std::isfinite(kz[i]) && std::isfinite(t[i])))
+      return set_error(PG_INVALID_ARG, "Gdft: non-finite sample input at %llu", (unsigned long long)i);
+    ks[i] = make_double4(tpi * kx[i], tpi * ky[i], tpi * kz[i], (double)t[i]);
+  }
+  for (uint64_t j = 0; j < ni; ++j) {
+    if (!(std::isfinite(ix[j]) && std::isfinite(iy[j]) && std::isfinite(iz[j]) && std::isfinite(fm[j])))
+      return set_error(PG_INVALID_ARG, "Gdft: non-finite voxel input at %llu", (unsigned long long)j);
+    vs[j] = make_double4(ix[j], iy[j], iz[j], fm[j]);
+  }
+  PG_TRY(p->ks.upload(ks.data(), nk, s));
+  PG_TRY(p->vs.upload(vs.data(), ni, s));
+  PG_CUDA(cudaStreamSynchronize(s));
+  *out = std::move(p);
+  return PG_OK;
+}
+
+static int splits_for(uint64_t nout, uint64_t ninner) {
+  const uint64_t blocks = (nout + kTile - 1) / kTile;
+  const uint64_t want = (uint64_t)sm_count() * 8;
+  uint64_t ns = (want + blocks - 1) / blocks;
+  const uint64_t max_ns = (ninner + kTile - 1) / kTile;
+  if (ns > max_ns) ns = max_ns;
+  if (ns < 1) ns = 1;
+  if (ns > 64) ns = 64;
+  return (int)ns;
+}
+
+template <int NC>
+static pg_status launch_fwd(GdftPlan* p, int nsplit, uint64_t jchunk, const float2* xin, float2* part, cudaStream_t s) {
+  dim3 grid(ceil_div(p->nk, kTile), nsplit);
+  PG_LAUNCH(k_dft_forward<NC>, grid, kTile, 0, s, p->nk, p->ni, p->ks.p, p->vs.p, xin, jchunk, part);
+  return PG_OK;
+}
+template <int NC>
+static pg_status launch_adj(GdftPlan* p, int nsplit, uint64_t ichunk, const float2* yin, uint64_t dstride,
+                            float2* part, cudaStream_t s) {
+  dim3 grid(ceil_div(p->ni, kTile), nsplit);
+  PG_LAUNCH(k_dft_adjoint<NC>, grid, kTile, 0, s, p->nk, p->ni, p->ks.p, p->vs.p, yin, dstride, ichunk, part);
+  return PG_OK;
+}
+
+static int pad_coils(int nc) { return nc <= 1 ? 1 : nc <= 2 ? 2 : nc <= 4 ? 4 : 8; }
+
+pg_status gdft_forward(GdftPlan* p, int C, const float2* S, const float2* x, float2* y, uint64_t dstride,
+                       cudaStream_t s) {
+  const int nsplit = splits_for(p->nk, p->ni);
+  uint64_t jchunk = (p->ni + nsplit - 1) / nsplit;
+  jchunk = (jchunk + kTile - 1) / kTile * kTile;
+  for (int c0 = 0; c0 < C; c0 += kCoilChunk) {
+    const int nc = std::min(kCoilChunk, C - c0);
+    const int ncp = pad_coils(nc);
+    PG_TRY(p->xin.alloc(std::max<uint64_t>(p->xin.n, (uint64_t)ncp * p->ni)));
+    PG_TRY(p->part.alloc(std::max<uint64_t>(p->part.n, (uint64_t)nsplit * ncp * p->nk)));
+    PG_LAUNCH(k_apply_maps, ceil_div(p->ni, 256), 256, 0, s, p->ni, nc, c0, S, x, p->xin.p);
+    if (ncp > nc) PG_CUDA(cudaMemsetAsync(p->xin.p + (uint64_t)nc * p->ni, 0, (ncp - nc) * p->ni * sizeof(float2), s));
+    switch (ncp) {
+      case 1: PG_TRY(launch_fwd<1>(p, nsplit, jchunk, p->xin.p, p->part.p, s)); break;
+      case 2: PG_TRY(launch_fwd<2>(p, nsplit, jchunk, p->xin.p, p->part.p, s)); break;
+      case 4: PG_TRY(launch_fwd<4>(p, nsplit, jchunk, p->xin.p, p->part.p, s)); break;
+      default: PG_TRY(launch_fwd<8>(p, nsplit, jchunk, p->xin.p, p->part.p, s)); break;
+    }
+    PG_LAUNCH(k_forward_finish, ceil_div(p->nk, 256), 256, 0, s, p->nk, nc, nsplit, ncp, p->part.p,
+              y + (uint64_t)c0 * dstride, dstride);
+  }
+  return PG_OK;
+}
+
+pg_status gdft_adjoint(GdftPlan* p, int C, const float2* S, const float2* y, uint64_t dstride, float2* x,
+                       cudaStream_t s) {
+  const int nsplit = splits_for(p->ni, p->nk);
+  uint64_t ichunk = (p->nk + nsplit - 1) / nsplit;
+  ichunk = (ichunk + kTile - 1) / kTile * kTile;
+  for (int c0 = 0; c0 < C; c0 += kCoilChunk) {
+    const int nc = std::min(kCoilChunk, C - c0);
+    const int ncp = pad_coils(nc);
+    PG_TRY(p->part.alloc(std::max<uint64_t>(p->part.n, (uint64_t)nsplit * ncp * p->ni)));
+    // Coils past nc read the first coil's data (valid memory); their sums are discarded.
+    const float2* yc = y + (uint64_t)c0 * dstride;
+    if (ncp > nc) {
+      // stage the chunk contiguously so padded coils stay in bounds
+      PG_TRY(p->xin.alloc(std::max<uint64_t>(p->xin.n, (uint64_t)ncp * p->nk)));
+      for (int c = 0; c < ncp; ++c)
+        PG_CUDA(cudaMemcpyAsync(p->xin.p + (uint64_t)c * p->nk, yc + (uint64_t)std::min(c, nc - 1) * dstride,
+                                p->nk * sizeof(float2), cudaMemcpyDeviceToDevice, s));
+      yc = p->xin.p;
+    }
+    const uint64_t stride = (ncp > nc) ? p->nk : dstride;
+    switch (ncp) {
+      case 1: PG_TRY(launch_adj<1>(p, nsplit, ichunk, yc, stride, p->part.p, s)); break;
+      case 2: PG_TRY(launch_adj<2>(p, nsplit, ichunk, yc, stride, p->part.p, s)); break;
+      case 4: PG_TRY(launch_adj<4>(p, nsplit, ichunk, yc, stride, p->part.p, s)); break;
+      default: PG_TRY(launch_adj<8>(p, nsplit, ichunk, yc, stride, p->part.p, s)); break;
+    }
+    PG_LAUNCH(k_adjoint_finish, ceil_div(p->ni, 256), 256, 0, s, p->ni, nc, c0, nsplit, ncp, p->part.p, S,
+              c0 > 0 ? 1 : 0, x);
+  }
+  return PG_OK;
+}
+
+}  // namespace pg

@@ -1,0 +1,29 @@
+// Exact field-corrected DFT (Gdft) on sm_100a.
+#pragma once
+
+#include <cmath>
+#include <memory>
+
+#include "pg_common.cuh"
+
+namespace pg {
+
+struct GdftPlan {
+  uint64_t nk = 0, ni = 0;
+  DevBuf<double4> ks;    // per sample (2pi kx, 2pi ky, 2pi kz, t)
+  DevBuf<double4> vs;    // per voxel (ix, iy, iz, FM rad/s)
+  DevBuf<float2> xin;    // staged coil inputs
+  DevBuf<float2> part;   // split partial sums
+};
+
+pg_status gdft_plan_create(std::unique_ptr<GdftPlan>* out, uint64_t nk, uint64_t ni, const float* kx, const float* ky,
+                           const float* kz, const float* ix, const float* iy, const float* iz, const float* fm,
+                           const float* t, cudaStream_t s);
+// y_c = G (S_c x) for C coils; S may be null (C = 1).  y coil stride dstride.
+pg_status gdft_forward(GdftPlan* p, int C, const float2* S, const float2* x, float2* y, uint64_t dstride,
+                       cudaStream_t s);
+// x = sum_c conj(S_c) G^H y_c.
+pg_status gdft_adjoint(GdftPlan* p, int C, const float2* S, const float2* y, uint64_t dstride, float2* x,
+                       cudaStream_t s);
+
+}  // namespace pg

@@ -1,0 +1,95 @@
+// Gridding NUFFT on sm_100a: the device side of Gnufft (Gnufft.cpp,
+// gridding.cpp, griddingSupport.cpp), batched over coils and time segments.
+#pragma once
+
+#include <map>
+#include <memory>
+
+#include "pg_common.cuh"
+
+namespace pg {
+
+// Oversampled-grid geometry (gridding.cpp:437-446).  Image and grid are
+// y-fastest: image p = y + Ny*(x + Nx*z), grid g = gy + Gy*(gx + Gx*gz).
+struct NufftGeom {
+  int dim = 2;
+  int Nx = 1, Ny = 1, Nz = 1;
+  int Gx = 1, Gy = 1, Gz = 1;
+  float os = 2.f, kw = 4.f, beta = 0.f;
+  int nlut = 0;
+  // index shifts folded into the kernels (griddingSupport.cpp:372-627)
+  int pad_off[3];      // zero_pad offset per axis (x, y, z)
+  int crop_off[3];     // crop_center offset per axis
+  int fs[3];           // fftshift amount (floor(G/2))
+  int ifs[3];          // ifftshift amount (ceil(G/2) in-plane, floor along z)
+  __host__ __device__ uint64_t nimg() const { return (uint64_t)Nx * Ny * Nz; }
+  __host__ __device__ uint64_t ngrid() const { return (uint64_t)Gx * Gy * Gz; }
+};
+
+// Adjoint tile shape (grid cells per tile) and its padded shared-memory extent.
+struct TileShape {
+  int TX, TY, TZ;      // tile size
+  int PX, PY, PZ;      // padded smem extent (>= T + 8 along gridded axes)
+  int ntx, nty, ntz;   // tiles per axis
+};
+
+// Per-(trajectory, segmentation) sample binning used by both directions.
+// All per-sample arrays are in sorted order (stable by bin key).
+struct Binning {
+  int K = 1;                 // segment-window length per sample
+  int L = 1;                 // segments
+  uint64_t M = 0;            // samples
+  TileShape tile{};
+  DevBuf<uint32_t> perm;     // sorted -> original sample index
+  DevBuf<uint2> start;       // (sx | sy << 16, sz): first of 8 taps per axis
+  DevBuf<float> wxy;         // 16 per sample: wx[8], wy[8]
+  DevBuf<float> wz;          // 8 per sample (3-D)
+  DevBuf<int> l0;            // segment-window start per sample
+  DevBuf<float2> aa;         // K per sample: interpolator values AA(m, l0..l0+K-1)
+  DevBuf<int4> subprob;      // (tile index, l0, first sorted sample, count)
+  int nsub = 0;
+  uint64_t nkeys = 0;
+  std::vector<uint32_t> h_keys;   // bin key per original sample (tests)
+  std::vector<uint32_t> h_perm;
+};
+
+struct NufftPlan {
+  NufftGeom g;
+  uint64_t M = 0;
+  DevBuf<float> kx, ky, kz;      // original order
+  DevBuf<float> lut;
+  DevBuf<float> deap;            // Nx + Ny + Nz reciprocal-transform factors
+  std::unique_ptr<Binning> plain;  // binning without segmentation (L = 1)
+  // grid workspace and cuFFT plans, keyed by batch size
+  DevBuf<float2> grids;
+  std::map<int, cufftHandle> ffts;
+  DevBuf<char> fft_work;
+  size_t budget_bytes = 8ull << 30;  // grid workspace limit per plan
+  ~NufftPlan();
+};
+
+// What surrounds the gridding in one batched application.
+struct NufftBatch {
+  int C = 1;                     // coils in this call
+  const float2* S = nullptr;     // C x N coil maps (coil-major) or null
+  const float2* E = nullptr;     // N extra image factor (shot phase) or null
+  const float2* Wo = nullptr;    // L x N segment phases (forward)
+  const float2* WoH = nullptr;   // L x N (adjoint)
+  const Binning* bin = nullptr;  // segmentation binning (L, K, AA) or plan->plain
+  uint64_t data_stride = 0;      // elements between coils in the data vector
+  bool accumulate = false;       // adjoint: add into x instead of overwrite
+};
+
+pg_status nufft_plan_create(std::unique_ptr<NufftPlan>* out, uint64_t M, float gridos, int nx, int ny, int nz,
+                            const float* kx, const float* ky, const float* kz, cudaStream_t s);
+// Binning for a segmentation: l0_host/aa_host (K per sample, original order)
+// or null for the unsegmented case.
+pg_status nufft_build_binning(NufftPlan* p, int L, int K, const int* l0_host, const float2* aa_host,
+                              std::unique_ptr<Binning>* out, cudaStream_t s);
+pg_status nufft_forward(NufftPlan* p, const NufftBatch& b, const float2* x, float2* y, cudaStream_t s);
+pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, float2* x, cudaStream_t s);
+
+// Host copies of the LUT and beta exactly as Gnufft builds them.
+void kb_table(float gridos, std::vector<float>* lut, float* beta);
+
+}  // namespace pg

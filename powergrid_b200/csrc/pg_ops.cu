@@ -1,0 +1,492 @@
+// Operators and their C ABI.  A composite recognises the operator under it
+// and runs the whole composition as one batched device pipeline:
+//   SENSE<TimeSegmentation<Gnufft>>  -> one NUFFT pass over coils x segments
+//   SENSE<Gnufft>, TimeSegmentation<Gnufft>, Gnufft -> the same pass, fewer factors
+//   SENSE<Gdft>, Gdft                -> one coil-batched DFT pass
+// Any other nesting falls back to composing the inner operator's device
+// calls with element-wise kernels (still on the GPU).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+
+#include "pg_ops.cuh"
+
+namespace pg {
+
+// ---- element-wise kernels for the generic composition path ----------------
+__global__ void k_cmul(uint64_t n, const float2* __restrict__ a, const float2* __restrict__ b, int conj_a,
+                       float2* __restrict__ out) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float2 av = conj_a ? cconj(a[i]) : a[i];
+  out[i] = cmul(av, b[i]);
+}
+// out (+)= a (.) b  (conj_b selects conj(b))
+__global__ void k_cmul_acc(uint64_t n, const float2* __restrict__ a, const float2* __restrict__ b, int conj_b,
+                           int accumulate, float2* __restrict__ out) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float2 bv = conj_b ? cconj(b[i]) : b[i];
+  const float2 v = cmul(a[i], bv);
+  out[i] = accumulate ? cadd(out[i], v) : v;
+}
+
+// ---- time-segmentation tables ---------------------------------------------
+pg_status build_ts_tables(const float* field_map, const float* tvec, uint64_t n1, uint64_t n2, uint64_t Lin,
+                          uint64_t interptype, uint64_t shots, TsTables* out) {
+  TsTables& T = *out;
+  if (n1 == 0 || n2 == 0) return set_error(PG_INVALID_ARG, "TimeSegmentation: empty sizes");
+  if (shots == 0 || n1 % shots) return set_error(PG_INVALID_ARG, "TimeSegmentation: n1 not divisible by shots");
+  for (uint64_t m = 0; m < n1; ++m)
+    if (!std::isfinite(tvec[m])) return set_error(PG_INVALID_ARG, "TimeSegmentation: non-finite time at %llu",
+                                                  (unsigned long long)m);
+  for (uint64_t p = 0; p < n2; ++p)
+    if (!std::isfinite(field_map[p])) return set_error(PG_INVALID_ARG, "TimeSegmentation: non-finite field map");
+  // TimeSegmentation.cpp:46-50: L in {0,1} means no segmentation.
+  int L = (Lin == 0 || Lin == 1) ? 1 : (int)Lin;
+  if (L > 64) return set_error(PG_INVALID_ARG, "TimeSegmentation: L=%d exceeds 64", L);
+  if (L > 1 && interptype != 1)
+    return set_error(PG_INVALID_ARG, "TimeSegmentation: interptype %llu is not implemented (Hanning = 1)",
+                     (unsigned long long)interptype);
+  std::vector<float> tv(tvec, tvec + n1);
+  float mn = tv[0], mx = tv[0];
+  for (float v : tv) { mn = std::min(mn, v); mx = std::max(mx, v); }
+  T.tmin = mn;
+  const float rangt = mx - T.tmin;
+  T.tau = (rangt + std::numeric_limits<double>::epsilon()) / L;  // :66-68 (datum::eps is double eps)
+  for (auto& v : tv) v = v - T.tmin;
+  T.L = L;
+  if (L <= 1) {
+    T.L = 1; T.tau = 0; T.K = 1;
+    return PG_OK;
+  }
+  const uint64_t none = n1 / shots;
+  const double kPi = 3.141592653589793238462643383279502884;  // arma datum::pi
+  // Hanning interpolator (:83-92), repeated over shots.
+  std::vector<float2> one(none * L);
+  for (unsigned int l = 0; l < (unsigned)L; ++l)
+    for (unsigned int m = 0; m < none; ++m) {
+      float v = 0.f;
+      if ((std::abs(tv[m] - ((l) * T.tau))) <= T.tau)
+        v = (float)(0.5 + 0.5 * std::cos((kPi) * (tv[m] - ((l) * T.tau)) / T.tau));
+      one[m + none * l] = make_float2(v, 0.f);
+    }
+  T.AA.resize(n1 * L);
+  for (int l = 0; l < L; ++l)
+    for (uint64_t m = 0; m < n1; ++m) T.AA[m + n1 * l] = one[(m % none) + none * l];
+  // Segment window per sample: the span of nonzero AA entries.
+  std::vector<int> first(n1, 0), last(n1, -1);
+  int K = 1;
+  for (uint64_t m = 0; m < n1; ++m) {
+    for (int l = 0; l < L; ++l) {
+      const float2 a = T.AA[m + n1 * l];
+      if (a.x != 0.f || a.y != 0.f) {
+        if (last[m] < 0) first[m] = l;
+        last[m] = l;
+      }
+    }
+    if (last[m] >= 0) K = std::max(K, last[m] - first[m] + 1);
+  }
+  T.K = K;
+  T.l0.resize(n1);
+  T.aa_win.resize(n1 * (uint64_t)K);
+  for (uint64_t m = 0; m < n1; ++m) {
+    const int s = std::min(first[m], L - K);
+    T.l0[m] = s;
+    for (int q = 0; q < K; ++q) T.aa_win[m * K + q] = T.AA[m + n1 * (s + q)];
+  }
+  // Wo / WoH (:213-218): exp(-/+ i * fieldMap * (l*tau + T_min)).
+  T.Wo.resize(n2 * (uint64_t)L);
+  T.WoH.resize(n2 * (uint64_t)L);
+  for (unsigned int l = 0; l < (unsigned)L; ++l) {
+    const float sft = (l) * T.tau + T.tmin;
+    for (uint64_t p = 0; p < n2; ++p) {
+      const float v = field_map[p] * sft;
+      const float c = std::cos(v), sn = std::sin(v);
+      T.Wo[p + n2 * l] = make_float2(c, -sn);
+      T.WoH[p + n2 * l] = make_float2(c, sn);
+    }
+  }
+  return PG_OK;
+}
+
+// ---- Gnufft ------------------------------------------------------------------
+pg_status GnufftOp::forward(const float2* x, float2* y, cudaStream_t s) {
+  NufftBatch b;
+  b.C = 1;
+  b.data_stride = plan->M;
+  return nufft_forward(plan.get(), b, x, y, s);
+}
+pg_status GnufftOp::adjoint(const float2* y, float2* x, cudaStream_t s) {
+  NufftBatch b;
+  b.C = 1;
+  b.data_stride = plan->M;
+  return nufft_adjoint(plan.get(), b, y, x, s);
+}
+uint64_t GnufftOp::resident_bytes() const {
+  return plan->M * (3 * 4 + 8 + 64 + 4 + 4) + plan->grids.bytes();
+}
+
+// ---- Gdft ------------------------------------------------------------------
+pg_status GdftOp::forward(const float2* x, float2* y, cudaStream_t s) {
+  return gdft_forward(plan.get(), 1, nullptr, x, y, plan->nk, s);
+}
+pg_status GdftOp::adjoint(const float2* y, float2* x, cudaStream_t s) {
+  return gdft_adjoint(plan.get(), 1, nullptr, y, plan->nk, x, s);
+}
+
+// ---- TimeSegmentation --------------------------------------------------------
+pg_status TimeSegOp::forward(const float2* x, float2* y, cudaStream_t s) {
+  if (tab.L == 1) return inner->forward(x, y, s);  // AA = Wo = 1
+  if (inner->kind == PG_OP_GNUFFT) {
+    auto* g = static_cast<GnufftOp*>(inner);
+    NufftBatch b;
+    b.C = 1;
+    b.Wo = Wo.p;
+    b.bin = bin.get();
+    b.data_stride = n_data;
+    return nufft_forward(g->plan.get(), b, x, y, s);
+  }
+  // generic: y = sum_l AA_l (.) G(Wo_l (.) x)   (TimeSegmentation.cpp:266-295)
+  PG_TRY(tmp_img.alloc(n_image));
+  PG_TRY(tmp_data.alloc(n_data));
+  for (int l = 0; l < tab.L; ++l) {
+    PG_LAUNCH(k_cmul, ceil_div(n_image, 256), 256, 0, s, n_image, Wo.p + (uint64_t)l * n_image, x, 0, tmp_img.p);
+    PG_TRY(inner->forward(tmp_img.p, tmp_data.p, s));
+    PG_LAUNCH(k_cmul_acc, ceil_div(n_data, 256), 256, 0, s, n_data, tmp_data.p, AAfull.p + (uint64_t)l * n_data, 0,
+              l > 0 ? 1 : 0, y);
+  }
+  return PG_OK;
+}
+pg_status TimeSegOp::adjoint(const float2* y, float2* x, cudaStream_t s) {
+  if (tab.L == 1) return inner->adjoint(y, x, s);
+  if (inner->kind == PG_OP_GNUFFT) {
+    auto* g = static_cast<GnufftOp*>(inner);
+    NufftBatch b;
+    b.C = 1;
+    b.WoH = WoH.p;
+    b.bin = bin.get();
+    b.data_stride = n_data;
+    return nufft_adjoint(g->plan.get(), b, y, x, s);
+  }
+  // generic: x = sum_l WoH_l (.) G^H(conj(AA_l) (.) y)   (TimeSegmentation.cpp:304-323)
+  PG_TRY(tmp_img.alloc(n_image));
+  PG_TRY(tmp_data.alloc(n_data));
+  for (int l = 0; l < tab.L; ++l) {
+    PG_LAUNCH(k_cmul, ceil_div(n_data, 256), 256, 0, s, n_data, AAfull.p + (uint64_t)l * n_data, y, 1, tmp_data.p);
+    PG_TRY(inner->adjoint(tmp_data.p, tmp_img.p, s));
+    PG_LAUNCH(k_cmul_acc, ceil_div(n_image, 256), 256, 0, s, n_image, tmp_img.p, WoH.p + (uint64_t)l * n_image, 0,
+              l > 0 ? 1 : 0, x);
+  }
+  return PG_OK;
+}
+
+// ---- SENSE -------------------------------------------------------------------
+static bool nufft_under(pg_op_s* inner, NufftPlan** plan, const TimeSegOp** ts) {
+  *ts = nullptr;
+  if (inner->kind == PG_OP_GNUFFT) {
+    *plan = static_cast<GnufftOp*>(inner)->plan.get();
+    return true;
+  }
+  if (inner->kind == PG_OP_TIMESEG) {
+    auto* t = static_cast<TimeSegOp*>(inner);
+    if (t->inner->kind == PG_OP_GNUFFT) {
+      *plan = static_cast<GnufftOp*>(t->inner)->plan.get();
+      *ts = t->tab.L > 1 ? t : nullptr;
+      return true;
+    }
+  }
+  return false;
+}
+
+pg_status SenseOp::forward(const float2* x, float2* y, cudaStream_t s) {
+  NufftPlan* plan = nullptr;
+  const TimeSegOp* ts = nullptr;
+  if (nufft_under(inner, &plan, &ts)) {
+    NufftBatch b;
+    b.C = (int)nc;
+    b.S = S.p;
+    b.data_stride = n_data;
+    if (ts) { b.Wo = ts->Wo.p; b.bin = ts->bin.get(); }
+    return nufft_forward(plan, b, x, y, s);
+  }
+  if (inner->kind == PG_OP_GDFT)
+    return gdft_forward(static_cast<GdftOp*>(inner)->plan.get(), (int)nc, S.p, x, y, n_data, s);
+  // generic (SENSE.cpp:59-70)
+  PG_TRY(tmp_img.alloc(n_image));
+  for (uint64_t c = 0; c < nc; ++c) {
+    PG_LAUNCH(k_cmul, ceil_div(n_image, 256), 256, 0, s, n_image, S.p + c * n_image, x, 0, tmp_img.p);
+    PG_TRY(inner->forward(tmp_img.p, y + c * n_data, s));
+  }
+  return PG_OK;
+}
+
+pg_status SenseOp::adjoint(const float2* y, float2* x, cudaStream_t s) {
+  NufftPlan* plan = nullptr;
+  const TimeSegOp* ts = nullptr;
+  if (nufft_under(inner, &plan, &ts)) {
+    NufftBatch b;
+    b.C = (int)nc;
+    b.S = S.p;
+    b.data_stride = n_data;
+    if (ts) { b.WoH = ts->WoH.p; b.bin = ts->bin.get(); }
+    return nufft_adjoint(plan, b, y, x, s);
+  }
+  if (inner->kind == PG_OP_GDFT)
+    return gdft_adjoint(static_cast<GdftOp*>(inner)->plan.get(), (int)nc, S.p, y, n_data, x, s);
+  // generic (SENSE.cpp:84-96)
+  PG_TRY(tmp_img.alloc(n_image));
+  for (uint64_t c = 0; c < nc; ++c) {
+    PG_TRY(inner->adjoint(y + c * n_data, tmp_img.p, s));
+    PG_LAUNCH(k_cmul_acc, ceil_div(n_image, 256), 256, 0, s, n_image, tmp_img.p, S.p + c * n_image, 1,
+              c > 0 ? 1 : 0, x);
+  }
+  return PG_OK;
+}
+
+// ---- pcSenseTimeSeg ----------------------------------------------------------
+pg_status PcSenseTsOp::forward(const float2* x, float2* y, cudaStream_t s) {
+  for (uint64_t sh = 0; sh < Ns; ++sh) {
+    NufftBatch b;
+    b.C = (int)Nc;
+    b.S = S.p;
+    b.E = E.p + sh * Ni;
+    b.data_stride = Ns * Nd;
+    if (tabs[sh].L > 1) { b.Wo = Wo[sh].p; b.bin = bins[sh].get(); }
+    PG_TRY(nufft_forward(plans[sh].get(), b, x, y + sh * Nd, s));
+  }
+  return PG_OK;
+}
+pg_status PcSenseTsOp::adjoint(const float2* y, float2* x, cudaStream_t s) {
+  for (uint64_t sh = 0; sh < Ns; ++sh) {
+    NufftBatch b;
+    b.C = (int)Nc;
+    b.S = S.p;
+    b.E = E.p + sh * Ni;
+    b.data_stride = Ns * Nd;
+    b.accumulate = sh > 0;
+    if (tabs[sh].L > 1) { b.WoH = WoH[sh].p; b.bin = bins[sh].get(); }
+    PG_TRY(nufft_adjoint(plans[sh].get(), b, y + sh * Nd, x, s));
+  }
+  return PG_OK;
+}
+uint64_t PcSenseTsOp::resident_bytes() const {
+  uint64_t b = S.bytes() + E.bytes();
+  for (auto& p : plans) b += p->grids.bytes() + p->M * 100;
+  return b;
+}
+
+static pg_status make_binning_for(NufftPlan* plan, const TsTables& tab, std::unique_ptr<Binning>* out,
+                                  cudaStream_t s) {
+  return nufft_build_binning(plan, tab.L, tab.K, tab.l0.data(), tab.aa_win.data(), out, s);
+}
+
+}  // namespace pg
+
+using namespace pg;
+
+// ---- C ABI -------------------------------------------------------------------
+extern "C" {
+
+pg_status pg_gnufft_create(pg_op* out, uint64_t data_length, float gridos, uint64_t nx, uint64_t ny, uint64_t nz,
+                           const float* kx, const float* ky, const float* kz) {
+  if (!out || !kx || !ky) return set_error(PG_INVALID_ARG, "Gnufft: null argument");
+  if (nz > 1 && !kz) return set_error(PG_INVALID_ARG, "Gnufft: kz required for 3-D");
+  PG_TRY(ensure_init());
+  auto op = std::make_unique<GnufftOp>();
+  op->kind = PG_OP_GNUFFT;
+  PG_TRY(nufft_plan_create(&op->plan, data_length, gridos, (int)nx, (int)ny, (int)nz, kx, ky, kz, default_stream()));
+  op->n_data = data_length;
+  op->n_image = nx * ny * nz;
+  *out = op.release();
+  return PG_OK;
+}
+
+pg_status pg_gdft_create(pg_op* out, uint64_t nk, uint64_t ni, const float* kx, const float* ky, const float* kz,
+                         const float* ix, const float* iy, const float* iz, const float* field_map, const float* t) {
+  if (!out || !kx || !ky || !kz || !ix || !iy || !iz || !field_map || !t)
+    return set_error(PG_INVALID_ARG, "Gdft: null argument");
+  PG_TRY(ensure_init());
+  auto op = std::make_unique<GdftOp>();
+  op->kind = PG_OP_GDFT;
+  PG_TRY(gdft_plan_create(&op->plan, nk, ni, kx, ky, kz, ix, iy, iz, field_map, t, default_stream()));
+  op->n_data = nk;
+  op->n_image = ni;
+  *out = op.release();
+  return PG_OK;
+}
+
+pg_status pg_timeseg_create(pg_op* out, pg_op G, const float* field_map, const float* tvec, uint64_t n1, uint64_t n2,
+                            uint64_t L, uint64_t interptype, uint64_t shots) {
+  if (!out || !G || !field_map || !tvec) return set_error(PG_INVALID_ARG, "TimeSegmentation: null argument");
+  PG_TRY(ensure_init());
+  if (G->n_data != n1 || G->n_image != n2)
+    return set_error(PG_INVALID_ARG, "TimeSegmentation: sizes (%llu, %llu) do not match the inner operator (%llu, %llu)",
+                     (unsigned long long)n1, (unsigned long long)n2, (unsigned long long)G->n_data,
+                     (unsigned long long)G->n_image);
+  auto op = std::make_unique<TimeSegOp>();
+  op->kind = PG_OP_TIMESEG;
+  op->inner = G;
+  op->n_data = n1;
+  op->n_image = n2;
+  PG_TRY(build_ts_tables(field_map, tvec, n1, n2, L, interptype, shots, &op->tab));
+  cudaStream_t s = default_stream();
+  if (op->tab.L > 1) {
+    PG_TRY(op->Wo.upload(op->tab.Wo.data(), op->tab.Wo.size(), s));
+    PG_TRY(op->WoH.upload(op->tab.WoH.data(), op->tab.WoH.size(), s));
+    if (G->kind == PG_OP_GNUFFT) {
+      PG_TRY(make_binning_for(static_cast<GnufftOp*>(G)->plan.get(), op->tab, &op->bin, s));
+    } else {
+      PG_TRY(op->AAfull.upload(op->tab.AA.data(), op->tab.AA.size(), s));
+    }
+  }
+  PG_CUDA(cudaStreamSynchronize(s));
+  *out = op.release();
+  return PG_OK;
+}
+
+pg_status pg_sense_create(pg_op* out, pg_op G, const float* sense_map, uint64_t n1, uint64_t n2, uint64_t nc) {
+  if (!out || !G || !sense_map) return set_error(PG_INVALID_ARG, "SENSE: null argument");
+  PG_TRY(ensure_init());
+  if (nc == 0) return set_error(PG_INVALID_ARG, "SENSE: nc = 0");
+  if (G->n_data != n1 || G->n_image != n2)
+    return set_error(PG_INVALID_ARG, "SENSE: sizes do not match the inner operator");
+  auto op = std::make_unique<SenseOp>();
+  op->kind = PG_OP_SENSE;
+  op->inner = G;
+  op->nc = nc;
+  op->n_data = n1 * nc;
+  op->n_image = n2;
+  PG_TRY(op->S.upload(reinterpret_cast<const float2*>(sense_map), n2 * nc, default_stream()));
+  PG_CUDA(cudaStreamSynchronize(default_stream()));
+  *out = op.release();
+  return PG_OK;
+}
+
+pg_status pg_pcsense_timeseg_create(pg_op* out, const float* kx, const float* ky, const float* kz, uint64_t nk,
+                                    uint64_t nx, uint64_t ny, uint64_t nz, uint64_t nc, const float* t, uint64_t L,
+                                    uint64_t interptype, const float* sense_map, const float* field_map,
+                                    const float* shot_phase_map, uint64_t n_shot_phase) {
+  if (!out || !kx || !ky || !kz || !t || !sense_map || !field_map || !shot_phase_map)
+    return set_error(PG_INVALID_ARG, "pcSenseTimeSeg: null argument");
+  PG_TRY(ensure_init());
+  const uint64_t Ni = nx * ny * nz;
+  if (Ni == 0 || n_shot_phase % Ni) return set_error(PG_INVALID_ARG, "pcSenseTimeSeg: phase map size");
+  const uint64_t Ns = n_shot_phase / Ni;  // pcSenseTimeSeg.cpp:47
+  if (Ns == 0 || nk % Ns) return set_error(PG_INVALID_ARG, "pcSenseTimeSeg: samples not divisible by shots");
+  const uint64_t Nd = nk / Ns;            // :48
+  auto op = std::make_unique<PcSenseTsOp>();
+  op->kind = PG_OP_PCSENSE_TS;
+  op->Ni = Ni; op->Nc = nc; op->Ns = Ns; op->Nd = Nd;
+  op->n_data = Nd * Ns * nc;
+  op->n_image = Ni;
+  cudaStream_t s = default_stream();
+  op->Wo.resize(Ns);
+  op->WoH.resize(Ns);
+  op->tabs.resize(Ns);
+  op->bins.resize(Ns);
+  for (uint64_t sh = 0; sh < Ns; ++sh) {
+    std::unique_ptr<NufftPlan> plan;
+    PG_TRY(nufft_plan_create(&plan, Nd, 2.0f, (int)nx, (int)ny, (int)nz, kx + sh * Nd, ky + sh * Nd, kz + sh * Nd, s));
+    PG_TRY(build_ts_tables(field_map, t + sh * Nd, Nd, Ni, L, interptype, 1, &op->tabs[sh]));
+    if (op->tabs[sh].L > 1) {
+      PG_TRY(op->Wo[sh].upload(op->tabs[sh].Wo.data(), op->tabs[sh].Wo.size(), s));
+      PG_TRY(op->WoH[sh].upload(op->tabs[sh].WoH.data(), op->tabs[sh].WoH.size(), s));
+      PG_TRY(make_binning_for(plan.get(), op->tabs[sh], &op->bins[sh], s));
+      op->tabs[sh].AA.clear();
+      op->tabs[sh].AA.shrink_to_fit();
+    }
+    // share the grid workspace budget across shots: each plan sizes its own
+    op->plans.push_back(std::move(plan));
+  }
+  PG_TRY(op->S.upload(reinterpret_cast<const float2*>(sense_map), Ni * nc, s));
+  // E_s = exp(-i P_s) (pcSenseTimeSeg.cpp:107)
+  std::vector<float2> E(Ni * Ns);
+  for (uint64_t i = 0; i < Ni * Ns; ++i) {
+    const float ph = shot_phase_map[i];
+    if (!std::isfinite(ph)) return set_error(PG_INVALID_ARG, "pcSenseTimeSeg: non-finite phase map");
+    E[i] = make_float2(std::cos(ph), -std::sin(ph));
+  }
+  PG_TRY(op->E.upload(E.data(), E.size(), s));
+  PG_CUDA(cudaStreamSynchronize(s));
+  *out = op.release();
+  return PG_OK;
+}
+
+pg_status pg_op_destroy(pg_op op) {
+  if (!op) return PG_OK;
+  cudaStreamSynchronize(default_stream());
+  delete op;
+  return PG_OK;
+}
+
+pg_status pg_op_shape(pg_op op, uint64_t* n_data, uint64_t* n_image) {
+  if (!op) return set_error(PG_INVALID_ARG, "null operator");
+  if (n_data) *n_data = op->n_data;
+  if (n_image) *n_image = op->n_image;
+  return PG_OK;
+}
+
+pg_status pg_op_forward_device(pg_op op, const void* x, void* y, void* stream) {
+  if (!op || !x || !y) return set_error(PG_INVALID_ARG, "forward: null argument");
+  PG_TRY(ensure_init());
+  cudaStream_t s = stream ? (cudaStream_t)stream : default_stream();
+  return op->forward((const float2*)x, (float2*)y, s);
+}
+
+pg_status pg_op_adjoint_device(pg_op op, const void* y, void* x, void* stream) {
+  if (!op || !x || !y) return set_error(PG_INVALID_ARG, "adjoint: null argument");
+  PG_TRY(ensure_init());
+  cudaStream_t s = stream ? (cudaStream_t)stream : default_stream();
+  return op->adjoint((const float2*)y, (float2*)x, s);
+}
+
+pg_status pg_op_forward(pg_op op, const float* x, float* y) {
+  if (!op || !x || !y) return set_error(PG_INVALID_ARG, "forward: null argument");
+  PG_TRY(ensure_init());
+  cudaStream_t s = default_stream();
+  PG_TRY(op->hx.alloc(op->n_image));
+  PG_TRY(op->hy.alloc(op->n_data));
+  PG_CUDA(cudaMemcpyAsync(op->hx.p, x, op->n_image * sizeof(float2), cudaMemcpyHostToDevice, s));
+  PG_TRY(op->forward(op->hx.p, op->hy.p, s));
+  PG_CUDA(cudaMemcpyAsync(y, op->hy.p, op->n_data * sizeof(float2), cudaMemcpyDeviceToHost, s));
+  PG_CUDA(cudaStreamSynchronize(s));
+  return PG_OK;
+}
+
+pg_status pg_op_adjoint(pg_op op, const float* y, float* x) {
+  if (!op || !x || !y) return set_error(PG_INVALID_ARG, "adjoint: null argument");
+  PG_TRY(ensure_init());
+  cudaStream_t s = default_stream();
+  PG_TRY(op->hx.alloc(op->n_image));
+  PG_TRY(op->hy.alloc(op->n_data));
+  PG_CUDA(cudaMemcpyAsync(op->hy.p, y, op->n_data * sizeof(float2), cudaMemcpyHostToDevice, s));
+  PG_TRY(op->adjoint(op->hy.p, op->hx.p, s));
+  PG_CUDA(cudaMemcpyAsync(x, op->hx.p, op->n_image * sizeof(float2), cudaMemcpyDeviceToHost, s));
+  PG_CUDA(cudaStreamSynchronize(s));
+  return PG_OK;
+}
+
+uint64_t pg_util_kb_lut(float gridos, float* lut_out, uint64_t cap, float* beta_out) {
+  std::vector<float> lut;
+  float beta = 0.f;
+  kb_table(gridos, &lut, &beta);
+  if (beta_out) *beta_out = beta;
+  if (lut_out) std::memcpy(lut_out, lut.data(), std::min<uint64_t>(cap, lut.size()) * sizeof(float));
+  return lut.size();
+}
+
+pg_status pg_util_gnufft_binning(pg_op G, uint32_t* keys_out, uint32_t* perm_out, uint64_t* n_bins_out) {
+  if (!G) return set_error(PG_INVALID_ARG, "null operator");
+  const Binning* b = nullptr;
+  if (G->kind == PG_OP_GNUFFT) b = static_cast<GnufftOp*>(G)->plan->plain.get();
+  else if (G->kind == PG_OP_TIMESEG && static_cast<TimeSegOp*>(G)->bin) b = static_cast<TimeSegOp*>(G)->bin.get();
+  if (!b) return set_error(PG_INVALID_ARG, "operator has no sample binning");
+  if (keys_out) std::memcpy(keys_out, b->h_keys.data(), b->h_keys.size() * sizeof(uint32_t));
+  if (perm_out) std::memcpy(perm_out, b->h_perm.data(), b->h_perm.size() * sizeof(uint32_t));
+  if (n_bins_out) *n_bins_out = b->nkeys;
+  return PG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,84 @@
+// Operator objects behind the pg_op handle.
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "pg_gdft.cuh"
+#include "pg_nufft.cuh"
+
+enum pg_op_kind { PG_OP_GNUFFT = 1, PG_OP_GDFT = 2, PG_OP_TIMESEG = 3, PG_OP_SENSE = 4, PG_OP_PCSENSE_TS = 5 };
+
+struct pg_op_s {
+  int kind = 0;
+  uint64_t n_data = 0, n_image = 0;
+  // staging for the host-buffer entry points
+  pg::DevBuf<float2> hx, hy;
+  virtual ~pg_op_s() {}
+  virtual pg_status forward(const float2* x, float2* y, cudaStream_t s) = 0;
+  virtual pg_status adjoint(const float2* y, float2* x, cudaStream_t s) = 0;
+  // Device bytes held by the operator (admission accounting).
+  virtual uint64_t resident_bytes() const { return 0; }
+};
+
+namespace pg {
+
+// Time-segmentation tables built on the host with the reference's operand
+// types (TimeSegmentation.cpp:59-93, 213-218).
+struct TsTables {
+  int L = 1;
+  float tau = 0.f, tmin = 0.f;
+  int K = 1;
+  std::vector<float2> AA;       // n1 x L (column l contiguous) — full table
+  std::vector<int> l0;          // per sample window start
+  std::vector<float2> aa_win;   // per sample K values
+  std::vector<float2> Wo, WoH;  // L x n2
+};
+pg_status build_ts_tables(const float* field_map, const float* tvec, uint64_t n1, uint64_t n2, uint64_t L,
+                          uint64_t interptype, uint64_t shots, TsTables* out);
+
+struct GnufftOp : pg_op_s {
+  std::unique_ptr<NufftPlan> plan;
+  pg_status forward(const float2* x, float2* y, cudaStream_t s) override;
+  pg_status adjoint(const float2* y, float2* x, cudaStream_t s) override;
+  uint64_t resident_bytes() const override;
+};
+
+struct GdftOp : pg_op_s {
+  std::unique_ptr<GdftPlan> plan;
+  pg_status forward(const float2* x, float2* y, cudaStream_t s) override;
+  pg_status adjoint(const float2* y, float2* x, cudaStream_t s) override;
+};
+
+struct TimeSegOp : pg_op_s {
+  pg_op_s* inner = nullptr;  // not owned (TimeSegmentation.cpp:53)
+  TsTables tab;
+  DevBuf<float2> Wo, WoH, AAfull;
+  std::unique_ptr<Binning> bin;  // when inner is Gnufft
+  DevBuf<float2> tmp_img, tmp_data, acc;
+  pg_status forward(const float2* x, float2* y, cudaStream_t s) override;
+  pg_status adjoint(const float2* y, float2* x, cudaStream_t s) override;
+};
+
+struct SenseOp : pg_op_s {
+  pg_op_s* inner = nullptr;  // not owned (SENSE.cpp:39)
+  uint64_t nc = 0;
+  DevBuf<float2> S;
+  DevBuf<float2> tmp_img, acc;
+  pg_status forward(const float2* x, float2* y, cudaStream_t s) override;
+  pg_status adjoint(const float2* y, float2* x, cudaStream_t s) override;
+};
+
+struct PcSenseTsOp : pg_op_s {
+  uint64_t Ni = 0, Nc = 0, Ns = 0, Nd = 0;
+  std::vector<std::unique_ptr<NufftPlan>> plans;
+  std::vector<std::unique_ptr<Binning>> bins;
+  std::vector<TsTables> tabs;
+  std::vector<DevBuf<float2>> Wo, WoH;
+  DevBuf<float2> S, E;
+  pg_status forward(const float2* x, float2* y, cudaStream_t s) override;
+  pg_status adjoint(const float2* y, float2* x, cudaStream_t s) override;
+  uint64_t resident_bytes() const override;
+};
+
+}  // namespace pg

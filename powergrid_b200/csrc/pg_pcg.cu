@@ -1,0 +1,513 @@
+// PWLS-PCG on the device (solve_pwls_pcg.hpp:48-167) with the Robject
+// regularizers (Robject.cpp:49-193, QuadPenalty.cpp:45-64, TVPenalty.cpp:43-68).
+//
+// Every vector op of an iteration is a kernel; inner products are
+// accumulated in FP64 (per-block partials, then a fixed-order sum in a
+// one-warp scalar kernel, so results are deterministic); the CG coefficient,
+// the three Newton steps and every early-exit test run on the device, so an
+// iteration needs no host synchronisation and is replayed as one CUDA graph.
+// Early exits set a device flag that turns the remaining kernels into
+// no-ops, which returns the x of the exit point as the reference does.
+//
+// The regularizer is fused: Gradient = beta * sum_dims Ctd(dpot(Cd x)) is a
+// 3-point stencil per dimension evaluated on the fly (no Cd/Ctd vectors),
+// with the reference's boundary rules: Cd is zero below the offset and
+// differences across row/slice boundaries (Robject.cpp:76-79); Ctd is
+// d[j]-d[j+off] up to N-2-off, d[N-1-off] at N-1-off, zero above
+// (Robject.cpp:111-117).
+#include <cmath>
+#include <vector>
+
+#include "pg_ops.cuh"
+
+namespace pg {
+
+namespace {
+
+struct PenDev {
+  int kind;          // 0 quad, 1 TV
+  int nd;            // dimensions penalised
+  uint64_t N;
+  uint64_t off[3];
+  float beta, delta;
+};
+
+enum Scal { S_YWY = 0, S_OLD, S_GAMMA, S_DAWAD, S_DAWR, S_STEP, S_NEW, S_DIRDOT, S_NSCAL };
+enum Flag { F_DONE = 0, F_IT, F_COMPLETED, F_REASON, F_NFLAG };
+
+constexpr int kRed = 256;  // threads per reduction block
+
+__device__ __forceinline__ float2 dpot(const PenDev& R, float2 d) {
+  if (R.kind == 0) return d;
+  const float a = hypotf(d.x / R.delta, d.y / R.delta);
+  const float s = sqrtf(1.f + a * a);
+  return make_float2(d.x / s, d.y / s);
+}
+__device__ __forceinline__ float wpot(const PenDev& R, float2 d) {
+  if (R.kind == 0) return 1.f;
+  const float a = hypotf(d.x / R.delta, d.y / R.delta);
+  return 1.f / sqrtf(1.f + a * a);
+}
+
+__device__ __forceinline__ float2 zval(const float2* __restrict__ x, const float2* __restrict__ d, float st,
+                                       uint64_t i) {
+  const float2 a = x[i];
+  if (!d) return a;
+  const float2 b = d[i];
+  return make_float2(a.x + st * b.x, a.y + st * b.y);
+}
+
+// beta * sum_dims Ctd(dpot(Cd z))[j], z = x + st*d.
+__device__ __forceinline__ float2 grad_at(const PenDev& R, const float2* __restrict__ x, const float2* __restrict__ d,
+                                          float st, uint64_t j) {
+  float2 g = make_float2(0.f, 0.f);
+  const float2 zj = zval(x, d, st, j);
+  for (int dim = 0; dim < R.nd; ++dim) {
+    const uint64_t off = R.off[dim];
+    if (off >= R.N) continue;
+    const uint64_t last = R.N - 1 - off;
+    if (j > last) continue;
+    float2 vj = make_float2(0.f, 0.f);
+    if (j >= off) vj = dpot(R, csub(zj, zval(x, d, st, j - off)));
+    if (j < last) {
+      const float2 vn = dpot(R, csub(zval(x, d, st, j + off), zj));
+      g = cadd(g, csub(vj, vn));
+    } else {
+      g = cadd(g, vj);
+    }
+  }
+  return make_float2(R.beta * g.x, R.beta * g.y);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block reduction of up to 2 values; thread 0 writes part[k*nb + blockIdx.x].
+__device__ __forceinline__ void block_store2(double a, double b, double* part, int nb) {
+  __shared__ double sa[kRed / 32], sb[kRed / 32];
+  a = warp_sum(a);
+  b = warp_sum(b);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { sa[w] = a; sb[w] = b; }
+  __syncthreads();
+  if (w == 0) {
+    a = (l < (int)(blockDim.x >> 5)) ? sa[l] : 0.0;
+    b = (l < (int)(blockDim.x >> 5)) ? sb[l] : 0.0;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    if (l == 0) { part[blockIdx.x] = a; part[nb + blockIdx.x] = b; }
+  }
+}
+
+// Fixed-order sum of part[k*nb .. k*nb+nb) by one warp.
+__device__ __forceinline__ double part_sum(const double* part, int nb, int k) {
+  double v = 0.0;
+  for (int i = threadIdx.x; i < nb; i += 32) v += part[k * nb + i];
+  return warp_sum(v);
+}
+
+// ---- kernels ------------------------------------------------------------------
+__global__ void k_fill_ones(uint64_t n, float* w) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) w[i] = 1.f;
+}
+
+// sum W |y|^2 (norm_grad denominator, solve_pwls_pcg.hpp:42-46)
+__global__ void k_ywy(uint64_t n, const float2* __restrict__ y, const float* __restrict__ W, double* part, int nb) {
+  double a = 0.0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const float2 v = y[i];
+    a += (double)W[i] * ((double)v.x * v.x + (double)v.y * v.y);
+  }
+  block_store2(a, 0.0, part, nb);
+}
+
+__global__ void k_scalar_init(const double* part, int nb, double* sc, uint32_t* fl) {
+  const double ywy = part_sum(part, nb, 0);
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < S_NSCAL; ++i) sc[i] = 0.0;
+    sc[S_YWY] = ywy;
+    fl[F_DONE] = 0; fl[F_IT] = 0; fl[F_COMPLETED] = 0; fl[F_REASON] = 0;
+  }
+}
+
+// r = W (.) (y - Ax)
+__global__ void k_residual(uint64_t n, const float2* __restrict__ y, const float2* __restrict__ Ax,
+                           const float* __restrict__ W, float2* __restrict__ r, const uint32_t* fl) {
+  if (fl[F_DONE]) return;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const float2 d = csub(y[i], Ax[i]);
+    const float w = W[i];
+    r[i] = make_float2(w * d.x, w * d.y);
+  }
+}
+
+// ngrad = A'r - R.Gradient(x); partials |A'r|^2 and |ngrad|^2.
+__global__ void k_ngrad(PenDev R, const float2* __restrict__ x, float2* __restrict__ ngrad, double* part, int nb,
+                        const uint32_t* fl) {
+  if (fl[F_DONE]) return;
+  double a = 0.0, b = 0.0;
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < R.N; j += (uint64_t)gridDim.x * blockDim.x) {
+    const float2 raw = ngrad[j];
+    a += (double)raw.x * raw.x + (double)raw.y * raw.y;
+    const float2 g = grad_at(R, x, nullptr, 0.f, j);
+    const float2 v = csub(raw, g);
+    ngrad[j] = v;
+    b += (double)v.x * v.x + (double)v.y * v.y;
+  }
+  block_store2(a, b, part, nb);
+}
+
+// Early exit on a vanishing gradient (:88-91) and the CG coefficient (:95-110).
+__global__ void k_scalar_dir(const double* part, int nb, double* sc, uint32_t* fl) {
+  if (fl[F_DONE]) return;
+  const double gn = part_sum(part, nb, 0);
+  const double nw = part_sum(part, nb, 1);
+  if (threadIdx.x == 0) {
+    if (sqrt(gn) / sc[S_YWY] < 1e-10) { fl[F_DONE] = 1; fl[F_REASON] = 1; return; }
+    double gamma = 0.0;
+    if (fl[F_IT] > 0) gamma = (fabs(sc[S_OLD]) < 1e-10) ? 0.0 : nw / sc[S_OLD];
+    sc[S_GAMMA] = gamma;
+    sc[S_OLD] = nw;
+  }
+}
+
+// ddir = ngrad + gamma ddir; partial Re<ddir, ngrad>.
+__global__ void k_ddir(uint64_t n, const float2* __restrict__ ngrad, float2* __restrict__ ddir, const double* sc,
+                       double* part, int nb, const uint32_t* fl) {
+  if (fl[F_DONE]) return;
+  const float gm = (float)sc[S_GAMMA];
+  double a = 0.0;
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x) {
+    const float2 g = ngrad[j];
+    float2 d = ddir[j];
+    d = make_float2(g.x + gm * d.x, g.y + gm * d.y);
+    ddir[j] = d;
+    a += (double)d.x * g.x + (double)d.y * g.y;
+  }
+  block_store2(a, 0.0, part, nb);
+}
+
+// Descent check (:113-116).
+__global__ void k_scalar_descent(const double* part, int nb, double* sc, uint32_t* fl) {
+  if (fl[F_DONE]) return;
+  const double v = part_sum(part, nb, 0);
+  if (threadIdx.x == 0) {
+    sc[S_DIRDOT] = v;
+    if (v < 0) { fl[F_DONE] = 1; fl[F_REASON] = 2; }
+  }
+}
+
+// dAWAd = Re<Adir, W Adir>, dAWr = Re(Adir' r) (:123-125).
+__global__ void k_daw(uint64_t n, const float2* __restrict__ Adir, const float* __restrict__ W,
+                      const float2* __restrict__ r, double* part, int nb, const uint32_t* fl) {
+  if (fl[F_DONE]) return;
+  double a = 0.0, b = 0.0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const float2 v = Adir[i];
+    const float2 q = r[i];
+    a += (double)W[i] * ((double)v.x * v.x + (double)v.y * v.y);
+    b += (double)v.x * q.x + (double)v.y * q.y;
+  }
+  block_store2(a, b, part, nb);
+}
+
+__global__ void k_scalar_daw(const double* part, int nb, double* sc, uint32_t* fl) {
+  if (fl[F_DONE]) return;
+  const double a = part_sum(part, nb, 0);
+  const double b = part_sum(part, nb, 1);
+  if (threadIdx.x == 0) { sc[S_DAWAD] = a; sc[S_DAWR] = b; sc[S_STEP] = 0.0; }
+}
+
+// One Newton step's penalty terms at z = x + step*ddir (:132-150):
+// pdenom = sum_dims sum wpot(Cd z) |Cd ddir|^2, pdot = Re<ddir, Gradient(z)>.
+__global__ void k_newton(PenDev R, const float2* __restrict__ x, const float2* __restrict__ ddir, const double* sc,
+                         double* part, int nb, const uint32_t* fl) {
+  if (fl[F_DONE]) return;
+  const float st = (float)sc[S_STEP];
+  double a = 0.0, b = 0.0;
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < R.N; j += (uint64_t)gridDim.x * blockDim.x) {
+    const float2 dj = ddir[j];
+    const float2 zj = zval(x, ddir, st, j);
+    for (int dim = 0; dim < R.nd; ++dim) {
+      const uint64_t off = R.off[dim];
+      if (j < off || off >= R.N) continue;
+      const float2 cd = csub(dj, ddir[j - off]);
+      const float2 cz = csub(zj, zval(x, ddir, st, j - off));
+      a += (double)wpot(R, cz) * ((double)cd.x * cd.x + (double)cd.y * cd.y);
+    }
+    const float2 g = grad_at(R, x, ddir, st, j);
+    b += (double)dj.x * g.x + (double)dj.y * g.y;
+  }
+  block_store2(a, b, part, nb);
+}
+
+__global__ void k_scalar_newton(const double* part, int nb, double beta, double* sc, uint32_t* fl) {
+  if (fl[F_DONE]) return;
+  const double pden = part_sum(part, nb, 0);
+  const double pdot = part_sum(part, nb, 1);
+  if (threadIdx.x == 0) {
+    const double denom = sc[S_DAWAD] + beta * pden;
+    if (fabs(denom) < 1e-20 || fabs(denom) > 1e25 || denom != denom) { fl[F_DONE] = 1; fl[F_REASON] = 3; return; }
+    const double step = sc[S_STEP];
+    sc[S_STEP] = step - (-sc[S_DAWR] + step * sc[S_DAWAD] + pdot) / denom;
+  }
+}
+
+// x += step ddir; Ax += step Adir (:160-161).
+__global__ void k_update(uint64_t ni, uint64_t nd, float2* __restrict__ x, const float2* __restrict__ ddir,
+                         float2* __restrict__ Ax, const float2* __restrict__ Adir, const double* sc,
+                         const uint32_t* fl) {
+  if (fl[F_DONE]) return;
+  const float st = (float)sc[S_STEP];
+  const uint64_t n = ni > nd ? ni : nd;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    if (i < ni) { const float2 d = ddir[i]; float2 v = x[i]; v.x += st * d.x; v.y += st * d.y; x[i] = v; }
+    if (i < nd) { const float2 d = Adir[i]; float2 v = Ax[i]; v.x += st * d.x; v.y += st * d.y; Ax[i] = v; }
+  }
+}
+
+__global__ void k_scalar_end(uint32_t* fl) {
+  if (fl[F_DONE]) return;
+  fl[F_IT] += 1;
+  fl[F_COMPLETED] = fl[F_IT];
+}
+
+__global__ void k_copy_iters(const uint32_t* fl, uint32_t* out) { *out = fl[F_COMPLETED]; }
+
+int red_blocks(uint64_t n) {
+  uint64_t b = (n + 4 * kRed - 1) / (4 * kRed);
+  if (b > 592) b = 592;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+PenDev make_pen(const pg_penalty& R) {
+  PenDev p{};
+  p.kind = R.kind;
+  p.N = R.nx * R.ny * R.nz;
+  p.nd = (R.nz == 1 || R.dims2penalize == 2) ? 2 : 3;  // Robject.cpp:128-132
+  p.off[0] = 1;
+  p.off[1] = R.ny;
+  p.off[2] = R.nx * R.ny;
+  p.beta = R.beta;
+  p.delta = R.delta;
+  return p;
+}
+
+struct Solver {
+  pg_op A;
+  uint64_t nd, ni;
+  PenDev R;
+  double beta;
+  DevBuf<float2> x, Ax, r, ngrad, ddir, Adir;
+  DevBuf<float> Wones;
+  DevBuf<double> part, sc;
+  DevBuf<uint32_t> fl;
+  const float2* y;
+  const float* W;
+  int nbd, nbi;
+
+  pg_status iteration(cudaStream_t s) {
+    const unsigned gd = (unsigned)nbd, gi = (unsigned)nbi;
+    PG_LAUNCH(k_residual, gd, kRed, 0, s, nd, y, Ax.p, W, r.p, fl.p);
+    PG_TRY(A->adjoint(r.p, ngrad.p, s));
+    PG_LAUNCH(k_ngrad, gi, kRed, 0, s, R, x.p, ngrad.p, part.p, nbi, fl.p);
+    PG_LAUNCH(k_scalar_dir, 1, 32, 0, s, part.p, nbi, sc.p, fl.p);
+    PG_LAUNCH(k_ddir, gi, kRed, 0, s, ni, ngrad.p, ddir.p, sc.p, part.p, nbi, fl.p);
+    PG_LAUNCH(k_scalar_descent, 1, 32, 0, s, part.p, nbi, sc.p, fl.p);
+    PG_TRY(A->forward(ddir.p, Adir.p, s));
+    PG_LAUNCH(k_daw, gd, kRed, 0, s, nd, Adir.p, W, r.p, part.p, nbd, fl.p);
+    PG_LAUNCH(k_scalar_daw, 1, 32, 0, s, part.p, nbd, sc.p, fl.p);
+    for (int k = 0; k < 3; ++k) {
+      PG_LAUNCH(k_newton, gi, kRed, 0, s, R, x.p, ddir.p, sc.p, part.p, nbi, fl.p);
+      PG_LAUNCH(k_scalar_newton, 1, 32, 0, s, part.p, nbi, beta, sc.p, fl.p);
+    }
+    PG_LAUNCH(k_update, (unsigned)red_blocks(std::max(nd, ni)), kRed, 0, s, ni, nd, x.p, ddir.p, Ax.p, Adir.p, sc.p,
+              fl.p);
+    PG_LAUNCH(k_scalar_end, 1, 1, 0, s, fl.p);
+    return PG_OK;
+  }
+};
+
+bool graphs_enabled() {
+  const char* e = getenv("PG_NO_GRAPH");
+  return !(e && e[0] == '1');
+}
+
+}  // namespace
+
+pg_status pcg_solve_device(pg_op A, const float2* x0, const float* W, const float2* y, const pg_penalty& Rh,
+                           uint64_t niter, float2* xout, uint32_t* iters_dev, cudaStream_t s) {
+  Solver S;
+  S.A = A;
+  S.nd = A->n_data;
+  S.ni = A->n_image;
+  if (Rh.nx * Rh.ny * Rh.nz != S.ni)
+    return set_error(PG_INVALID_ARG, "penalty size %llux%llux%llu does not match the image length %llu",
+                     (unsigned long long)Rh.nx, (unsigned long long)Rh.ny, (unsigned long long)Rh.nz,
+                     (unsigned long long)S.ni);
+  if (Rh.kind != PG_PENALTY_QUAD && Rh.kind != PG_PENALTY_TV) return set_error(PG_INVALID_ARG, "unknown penalty");
+  if (Rh.kind == PG_PENALTY_TV && !(Rh.delta > 0)) return set_error(PG_INVALID_ARG, "TV penalty needs delta > 0");
+  S.R = make_pen(Rh);
+  S.beta = Rh.beta;
+  S.y = y;
+  S.nbd = red_blocks(S.nd);
+  S.nbi = red_blocks(S.ni);
+  const int nb = std::max(S.nbd, S.nbi);
+  PG_TRY(S.x.alloc(S.ni));
+  PG_TRY(S.Ax.alloc(S.nd));
+  PG_TRY(S.r.alloc(S.nd));
+  PG_TRY(S.ngrad.alloc(S.ni));
+  PG_TRY(S.ddir.alloc(S.ni));
+  PG_TRY(S.Adir.alloc(S.nd));
+  PG_TRY(S.part.alloc(2 * (uint64_t)nb));
+  PG_TRY(S.sc.alloc(S_NSCAL));
+  PG_TRY(S.fl.alloc(F_NFLAG));
+  if (!W) {
+    PG_TRY(S.Wones.alloc(S.nd));
+    PG_LAUNCH(k_fill_ones, ceil_div(S.nd, 256), 256, 0, s, S.nd, S.Wones.p);
+    S.W = S.Wones.p;
+  } else {
+    S.W = W;
+  }
+  if (x0) PG_CUDA(cudaMemcpyAsync(S.x.p, x0, S.ni * sizeof(float2), cudaMemcpyDeviceToDevice, s));
+  else PG_CUDA(cudaMemsetAsync(S.x.p, 0, S.ni * sizeof(float2), s));
+  PG_CUDA(cudaMemsetAsync(S.ddir.p, 0, S.ni * sizeof(float2), s));
+  // Ax = A * xInitial (:55)
+  PG_TRY(A->forward(S.x.p, S.Ax.p, s));
+  PG_LAUNCH(k_ywy, (unsigned)S.nbd, kRed, 0, s, S.nd, y, S.W, S.part.p, S.nbd);
+  PG_LAUNCH(k_scalar_init, 1, 32, 0, s, S.part.p, S.nbd, S.sc.p, S.fl.p);
+
+  if (niter > 0) {
+    // first iteration eagerly: allocates every workspace the graph will use
+    PG_TRY(S.iteration(s));
+  }
+  if (niter > 1) {
+    if (graphs_enabled()) {
+      cudaGraph_t graph = nullptr;
+      cudaGraphExec_t exec = nullptr;
+      const uint64_t before = g_launches.load();
+      PG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      pg_status st = S.iteration(s);
+      cudaError_t ce = cudaStreamEndCapture(s, &graph);
+      if (st != PG_OK) { if (graph) cudaGraphDestroy(graph); return st; }
+      if (ce != cudaSuccess) return set_error(PG_CUDA_ERROR, "graph capture: %s", cudaGetErrorString(ce));
+      const uint64_t per_iter = g_launches.load() - before;
+      ce = cudaGraphInstantiate(&exec, graph, 0);
+      if (ce != cudaSuccess) { cudaGraphDestroy(graph); return set_error(PG_CUDA_ERROR, "graph instantiate: %s", cudaGetErrorString(ce)); }
+      for (uint64_t it = 1; it < niter; ++it) {
+        ce = cudaGraphLaunch(exec, s);
+        if (ce != cudaSuccess) break;
+        // replays launch the captured kernels; the capture itself launched none
+        count_launch(per_iter);
+      }
+      // the capture pass counted launches that never ran
+      g_launches.fetch_sub(per_iter);
+      cudaGraphExecDestroy(exec);
+      cudaGraphDestroy(graph);
+      if (ce != cudaSuccess) return set_error(PG_CUDA_ERROR, "graph launch: %s", cudaGetErrorString(ce));
+    } else {
+      for (uint64_t it = 1; it < niter; ++it) PG_TRY(S.iteration(s));
+    }
+  }
+  PG_CUDA(cudaMemcpyAsync(xout, S.x.p, S.ni * sizeof(float2), cudaMemcpyDeviceToDevice, s));
+  if (iters_dev) PG_LAUNCH(k_copy_iters, 1, 1, 0, s, S.fl.p, iters_dev);
+  // buffers are freed on return; make sure the stream is done with them
+  PG_CUDA(cudaStreamSynchronize(s));
+  return PG_OK;
+}
+
+// Gradient / Denom as stand-alone kernels (tests).
+__global__ void k_grad_only(PenDev R, const float2* __restrict__ x, float2* __restrict__ g) {
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < R.N; j += (uint64_t)gridDim.x * blockDim.x)
+    g[j] = grad_at(R, x, nullptr, 0.f, j);
+}
+__global__ void k_denom_only(PenDev R, const float2* __restrict__ ddir, const float2* __restrict__ x, double* part,
+                             int nb) {
+  double a = 0.0;
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < R.N; j += (uint64_t)gridDim.x * blockDim.x) {
+    for (int dim = 0; dim < R.nd; ++dim) {
+      const uint64_t off = R.off[dim];
+      if (j < off || off >= R.N) continue;
+      const float2 cd = csub(ddir[j], ddir[j - off]);
+      const float2 cz = csub(x[j], x[j - off]);
+      a += (double)wpot(R, cz) * ((double)cd.x * cd.x + (double)cd.y * cd.y);
+    }
+  }
+  block_store2(a, 0.0, part, nb);
+}
+
+}  // namespace pg
+
+using namespace pg;
+
+extern "C" {
+
+pg_status pg_pcg_solve_device(pg_op A, const void* x0, const void* W, const void* y, const pg_penalty* R,
+                              uint64_t niter, void* x_out, void* iters_done_dev, void* stream) {
+  if (!A || !y || !R || !x_out) return set_error(PG_INVALID_ARG, "pcg: null argument");
+  PG_TRY(ensure_init());
+  cudaStream_t s = stream ? (cudaStream_t)stream : default_stream();
+  return pcg_solve_device(A, (const float2*)x0, (const float*)W, (const float2*)y, *R, niter, (float2*)x_out,
+                          (uint32_t*)iters_done_dev, s);
+}
+
+pg_status pg_pcg_solve(pg_op A, const float* x0, const float* W, const float* y, const pg_penalty* R, uint64_t niter,
+                       float* x_out, uint64_t* iters_done) {
+  if (!A || !y || !R || !x_out) return set_error(PG_INVALID_ARG, "pcg: null argument");
+  PG_TRY(ensure_init());
+  cudaStream_t s = default_stream();
+  DevBuf<float2> dx0, dy, dx;
+  DevBuf<float> dW;
+  DevBuf<uint32_t> it;
+  PG_TRY(dy.upload(reinterpret_cast<const float2*>(y), A->n_data, s));
+  if (x0) PG_TRY(dx0.upload(reinterpret_cast<const float2*>(x0), A->n_image, s));
+  if (W) PG_TRY(dW.upload(W, A->n_data, s));
+  PG_TRY(dx.alloc(A->n_image));
+  PG_TRY(it.alloc(1));
+  PG_TRY(pcg_solve_device(A, x0 ? dx0.p : nullptr, W ? dW.p : nullptr, dy.p, *R, niter, dx.p, it.p, s));
+  PG_CUDA(cudaMemcpyAsync(x_out, dx.p, A->n_image * sizeof(float2), cudaMemcpyDeviceToHost, s));
+  uint32_t n = 0;
+  PG_CUDA(cudaMemcpyAsync(&n, it.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  PG_CUDA(cudaStreamSynchronize(s));
+  if (iters_done) *iters_done = n;
+  return PG_OK;
+}
+
+pg_status pg_recon_solve(pg_op Sg, const pg_penalty* R, const float* data, uint64_t niter, float* image_out) {
+  // reconSolve.h:63-82: W = ones, x0 = zeros.
+  return pg_pcg_solve(Sg, nullptr, nullptr, data, R, niter, image_out, nullptr);
+}
+
+pg_status pg_penalty_gradient_device(const pg_penalty* R, const void* x, void* g, void* stream) {
+  if (!R || !x || !g) return set_error(PG_INVALID_ARG, "penalty: null argument");
+  PG_TRY(ensure_init());
+  cudaStream_t s = stream ? (cudaStream_t)stream : default_stream();
+  PenDev P = make_pen(*R);
+  PG_LAUNCH(k_grad_only, (unsigned)red_blocks(P.N), kRed, 0, s, P, (const float2*)x, (float2*)g);
+  return PG_OK;
+}
+
+pg_status pg_penalty_denom_device(const pg_penalty* R, const void* ddir, const void* x, double* out_host) {
+  if (!R || !x || !ddir || !out_host) return set_error(PG_INVALID_ARG, "penalty: null argument");
+  PG_TRY(ensure_init());
+  cudaStream_t s = default_stream();
+  PenDev P = make_pen(*R);
+  const int nb = red_blocks(P.N);
+  DevBuf<double> part;
+  PG_TRY(part.alloc(2 * (uint64_t)nb));
+  PG_LAUNCH(k_denom_only, (unsigned)nb, kRed, 0, s, P, (const float2*)ddir, (const float2*)x, part.p, nb);
+  std::vector<double> h(nb);
+  PG_CUDA(cudaMemcpyAsync(h.data(), part.p, nb * sizeof(double), cudaMemcpyDeviceToHost, s));
+  PG_CUDA(cudaStreamSynchronize(s));
+  double a = 0;
+  for (double v : h) a += v;
+  *out_host = a * R->beta;
+  return PG_OK;
+}
+
+}  // extern "C"

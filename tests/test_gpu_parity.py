@@ -1,0 +1,207 @@
+"""GPU parity: the sm_100a path through the C ABI against the reference CPU
+path (golden fixtures from the reference's own kernels, and the live
+oracle) and against the FP64 oracle.
+
+Tolerances (relative L2):
+  * one operator application     <= 1e-5 vs the reference CPU path
+  * a PCG solve (5-10 iterations) <= 1e-4 vs the reference CPU path
+  * every case also states its error vs FP64 (printed, and bounded)
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OP_TOL = 1e-5
+PCG_TOL = 1e-4
+
+
+def _case(name):
+    d = np.load(os.path.join(HERE, "golden", name + ".npz"))
+    c = {k: d[k] for k in d.files}
+    for k in ("nx", "ny", "nz", "L", "nc", "niter"):
+        if k in c:
+            c[k] = int(c[k])
+    for k in ("beta", "delta"):
+        if k in c:
+            c[k] = float(c[k])
+    return c
+
+
+def _gpu_op(pg, name, c):
+    from powergrid_b200 import synthetic as S
+    M = c["kx"].size
+    n = c["nx"] * c["ny"] * c["nz"]
+    if name.startswith("nufft"):
+        return pg.Gnufft(M, 2.0, c["nx"], c["ny"], c["nz"], c["kx"], c["ky"], c["kz"])
+    if name == "gdft3d":
+        ix, iy, iz = S.image_coords(c["nx"], c["ny"], c["nz"])
+        G = pg.Gdft(M, n, c["kx"], c["ky"], c["kz"], ix, iy, iz, c["fm"], c["t"])
+        return pg.SENSE(G, c["smap"], M, n, c["nc"])
+    if name == "pcsense3d":
+        return pg.pcSenseTimeSeg(c["kx"], c["ky"], c["kz"], c["nx"], c["ny"], c["nz"], c["nc"], c["t"], c["L"], 1,
+                                 c["smap"], c["fm"], c["pmap"])
+    G = pg.Gnufft(M, 2.0, c["nx"], c["ny"], c["nz"], c["kx"], c["ky"], c["kz"])
+    A = pg.TimeSegmentation(G, c["fm"], c["t"], M, n, c["L"], 1, 1)
+    return pg.SENSE(A, c["smap"], M, n, c["nc"])
+
+
+@pytest.mark.parametrize("name", ["nufft2d", "nufft3d", "gdft3d", "tssense2d", "pcsense3d"])
+def test_operator_vs_reference_fixture(pg, name):
+    c = _case(name)
+    op = _gpu_op(pg, name, c)
+    y = op * c["x"]
+    x = op / c["y_f32"]
+    ey, ex = rel_l2(y, c["y_f32"]), rel_l2(x, c["x_adj_f32"])
+    ey64, ex64 = rel_l2(y, c["y_f64"]), rel_l2(x, c["x_adj_f64"])
+    ref64y, ref64x = rel_l2(c["y_f32"], c["y_f64"]), rel_l2(c["x_adj_f32"], c["x_adj_f64"])
+    print(f"{name}: fwd {ey:.2e} (fp64 {ey64:.2e}, ref-vs-fp64 {ref64y:.2e}); "
+          f"adj {ex:.2e} (fp64 {ex64:.2e}, ref-vs-fp64 {ref64x:.2e})")
+    assert ey <= OP_TOL and ex <= OP_TOL
+    assert ey64 <= OP_TOL and ex64 <= OP_TOL
+
+
+@pytest.mark.parametrize("name", ["pcg2d", "pcgtv2d"])
+def test_pcg_vs_reference_fixture(pg, name):
+    c = _case(name)
+    op = _gpu_op(pg, name, c)
+    if name == "pcgtv2d":
+        R = pg.TVPenalty(c["nx"], c["ny"], c["nz"], c["beta"], c["delta"])
+    else:
+        R = pg.QuadPenalty(c["nx"], c["ny"], c["nz"], c["beta"])
+    x, it = pg.solve_pwls_pcg(None, op, None, c["y_f32"], R, c["niter"])
+    e, e64 = rel_l2(x, c["x_pcg_f32"]), rel_l2(x, c["x_pcg_f64"])
+    print(f"{name}: pcg {e:.2e} vs reference, {e64:.2e} vs fp64, iterations {it}")
+    assert it == int(c["iters_f32"])
+    assert e <= PCG_TOL and e64 <= PCG_TOL
+
+
+def test_binning_is_a_stable_cpu_sort(pg):
+    """The adjoint's counting sort equals numpy's stable argsort of the bin keys, bit for bit."""
+    c = _case("nufft2d")
+    G = _gpu_op(pg, "nufft2d", c)
+    keys, perm, nb = G.binning()
+    assert keys.max() < nb
+    assert np.array_equal(perm, np.argsort(keys, kind="stable").astype(np.uint32))
+
+
+@pytest.mark.parametrize("name", ["nufft2d", "nufft3d", "tssense2d"])
+def test_adjointness(pg, name):
+    """<A x, y> = <x, A^H y> (even grid sizes make fftshift = ifftshift)."""
+    c = _case(name)
+    op = _gpu_op(pg, name, c)
+    rng = np.random.default_rng(5)
+    x = (rng.standard_normal(op.n_image) + 1j * rng.standard_normal(op.n_image)).astype(np.complex64)
+    y = (rng.standard_normal(op.n_data) + 1j * rng.standard_normal(op.n_data)).astype(np.complex64)
+    a = np.vdot((op * x).astype(np.complex128), y)
+    b = np.vdot(x.astype(np.complex128), (op / y).astype(np.complex128))
+    assert abs(a - b) <= 1e-5 * abs(a)
+
+
+def test_linearity_and_repeatability(pg):
+    c = _case("tssense2d")
+    op = _gpu_op(pg, "tssense2d", c)
+    x = c["x"]
+    y1 = op * x
+    y2 = op * (2.0 * x)
+    assert rel_l2(y2, 2 * y1) < 1e-6
+    a1 = op / c["y_f32"]
+    a2 = op / c["y_f32"]
+    assert rel_l2(a1, a2) < 1e-6   # shared-memory atomics reorder sums only
+
+
+def test_config1_full_size_vs_oracle(pg, oracle):
+    """Config 1 (64x64, 4096 samples, SENSE with one coil): fwd, adj and 10 PCG iterations."""
+    from powergrid_b200 import synthetic as S
+    p = S.config1()
+    M, n = p.kx.size, p.nimg
+    G = pg.Gnufft(M, 2.0, p.nx, p.ny, 1, p.kx, p.ky, p.kz)
+    Sg = pg.SENSE(G, p.smap, M, n, 1)
+    o32 = oracle.build_problem_op(p, 0)
+    o64 = oracle.build_problem_op(p, 2)
+    y = Sg * p.x_true
+    assert rel_l2(y, o32.forward(p.x_true)) <= OP_TOL
+    y64 = o64.forward(p.x_true.astype(np.complex128)).astype(np.complex64)
+    xa = Sg / y64
+    assert rel_l2(xa, o32.adjoint(y64)) <= OP_TOL
+    R = pg.QuadPenalty(p.nx, p.ny, 1, p.beta)
+    x = pg.reconSolve(y64, Sg, R, niter=10)
+    xr, _ = o32.pcg(y64, "quad", p.nx, p.ny, 1, p.beta, niter=10)
+    x64, _ = o64.pcg(y64, "quad", p.nx, p.ny, 1, p.beta, niter=10)
+    print(f"cfg1 pcg: {rel_l2(x, xr):.2e} vs reference, {rel_l2(x, x64):.2e} vs fp64")
+    assert rel_l2(x, xr) <= PCG_TOL and rel_l2(x, x64) <= PCG_TOL
+
+
+def test_config2_operator_full_size_vs_oracle(pg, oracle):
+    """Config 2 (128x128, 131072 samples, L=8, 4 coils): one forward and one adjoint."""
+    from powergrid_b200 import synthetic as S
+    p = S.config2()
+    M, n = p.kx.size, p.nimg
+    G = pg.Gnufft(M, 2.0, p.nx, p.ny, 1, p.kx, p.ky, p.kz)
+    A = pg.TimeSegmentation(G, p.fm, p.t, M, n, p.L, 1, 1)
+    Sg = pg.SENSE(A, p.smap, M, n, p.nc)
+    oracle.set_threads(os.cpu_count() or 1)
+    o32 = oracle.build_problem_op(p, 0)
+    y = Sg * p.x_true
+    yr = o32.forward(p.x_true)
+    e1 = rel_l2(y, yr)
+    xa = Sg / yr
+    e2 = rel_l2(xa, o32.adjoint(yr))
+    oracle.set_threads(1)
+    print(f"cfg2: fwd {e1:.2e}, adj {e2:.2e} vs reference CPU path")
+    assert e1 <= OP_TOL and e2 <= OP_TOL
+
+
+def test_gdft_config3_sampled_outputs(pg, oracle):
+    """Config 3 at full size (64x64x32, 131072 samples, 8 coils): sampled outputs vs FP64 DFT."""
+    from powergrid_b200 import synthetic as S
+    p = S.config3()
+    M, n = p.kx.size, p.nimg
+    ix, iy, iz = S.image_coords(p.nx, p.ny, p.nz)
+    G = pg.Gdft(M, n, p.kx, p.ky, p.kz, ix, iy, iz, p.fm, p.t)
+    Sg = pg.SENSE(G, p.smap, M, n, p.nc)
+    y = Sg * p.x_true
+    rng = np.random.default_rng(0)
+    idx = np.sort(rng.choice(M, 48, replace=False))
+    # FP64 DFT of coil 0 and 5 at the sampled rows
+    sm = p.smap.reshape(p.nc, n)
+    for c in (0, 5):
+        sub = oracle.gdft(2, p.kx[idx], p.ky[idx], p.kz[idx], ix, iy, iz, p.fm, p.t[idx])
+        ref = sub.forward((sm[c] * p.x_true).astype(np.complex128))
+        got = y[c * M + idx]
+        e = rel_l2(got, ref)
+        print(f"cfg3 coil {c}: sampled fwd vs fp64 {e:.2e}")
+        assert e <= OP_TOL
+
+
+def test_invalid_inputs_are_rejected(pg):
+    from powergrid_b200._lib import PGError
+    k = np.zeros(16, np.float32)
+    bad = k.copy()
+    bad[3] = np.nan
+    with pytest.raises(PGError, match="INVALID_ARG"):
+        pg.Gnufft(16, 2.0, 16, 16, 1, bad, k, k)
+    far = k.copy()
+    far[0] = 100.0
+    with pytest.raises(PGError, match="INVALID_ARG"):
+        pg.Gnufft(16, 2.0, 16, 16, 1, far, k, k)
+    with pytest.raises(PGError, match="INVALID_ARG"):
+        pg.Gnufft(16, 2.0, 16, 8, 1, k, k, k)   # non-square in-plane
+
+
+def test_allocation_failure_is_reported_and_recoverable(pg):
+    from powergrid_b200 import _lib
+    from powergrid_b200._lib import PGError
+    c = _case("nufft2d")
+    _lib.load().pg_debug_fail_allocation_after(1)
+    with pytest.raises(PGError, match="OUT_OF_MEMORY"):
+        _gpu_op(pg, "nufft2d", c)
+    _lib.load().pg_debug_fail_allocation_after(0)
+    op = _gpu_op(pg, "nufft2d", c)
+    assert rel_l2(op * c["x"], c["y_f32"]) <= OP_TOL

@@ -1,0 +1,150 @@
+"""The oracle, pinned: restatement vs the reference's own compiled kernels and
+vs the committed golden fixtures (which those kernels produced).  CPU only."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = sorted(glob.glob(os.path.join(HERE, "golden", "*.npz")))
+
+
+def _case(path):
+    d = np.load(path)
+    c = {k: d[k] for k in d.files}
+    for k in ("nx", "ny", "nz", "L", "nc", "niter"):
+        if k in c:
+            c[k] = int(c[k])
+    for k in ("beta", "delta"):
+        if k in c:
+            c[k] = float(c[k])
+    return c
+
+
+def test_fixtures_present():
+    names = {os.path.basename(p)[:-4] for p in GOLDEN}
+    assert {"nufft2d", "nufft3d", "gdft3d", "tssense2d", "pcsense3d", "pcg2d", "pcgtv2d"} <= names
+
+
+@pytest.mark.parametrize("shape", [(16,), (12,), (30,), (7,), (8, 6), (4, 6, 10), (64, 64)])
+@pytest.mark.parametrize("sign", [-1, 1])
+def test_project_fft_matches_numpy(oracle, shape, sign):
+    rng = np.random.default_rng(1)
+    a = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    got = oracle.fft(a.astype(np.complex128), sign)
+    ref = np.fft.fftn(a) if sign == -1 else np.fft.ifftn(a) * a.size
+    assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=lambda p: os.path.basename(p)[:-4])
+def test_restatement_reproduces_reference_fixtures(oracle, path):
+    """The restated float path equals the reference CPU path bit for bit."""
+    import make_golden as MG
+    name = os.path.basename(path)[:-4]
+    c = _case(path)
+    for prec, tag in ((0, "f32"), (2, "f64")):
+        out = MG.compute(name, c, prec)
+        for k, v in out.items():
+            ref = c[f"{k}_{tag}"]
+            if k == "iters":
+                assert int(v) == int(ref)
+                continue
+            if tag == "f32":
+                assert np.array_equal(v, ref), f"{name} {k}: max |diff| {np.abs(v - ref).max()}"
+            else:
+                assert rel_l2(v, ref) < 1e-13, f"{name} {k} fp64 rel {rel_l2(v, ref)}"
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(HERE), "oracle", "_ref", "libpgref.so")),
+                    reason="reference kernels are compiled only where the reference tree exists")
+@pytest.mark.parametrize("seed", [7, 8])
+def test_restatement_matches_reference_kernels_live(oracle, seed):
+    """Fresh seeded cases (other sizes): Gnufft fwd/adj and ftCpu/iftCpu, bit for bit."""
+    from powergrid_b200 import synthetic as S
+    n = 24 + 8 * (seed % 2)
+    kx, ky, _ = S.spiral(n, 3, 300, 1e-3)
+    kz = np.zeros_like(kx)
+    x = S.image(S.Rng(seed), n * n)
+    outs = []
+    for use_ref in (False, True):
+        oracle.use_reference(use_ref)
+        G = oracle.gnufft(0, kx.size, n, n, 1, kx, ky, kz)
+        y = G.forward(x)
+        outs.append((y, G.adjoint(y)))
+    oracle.use_reference(False)
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])
+    kx, ky, kz, t = S.stack_of_spirals(6, 4, 1, 40, 2e-2)
+    ix, iy, iz = S.image_coords(6, 6, 4)
+    fm = S.field_map(S.Rng(seed), 6, 6, 4, 120.0)
+    xi = S.image(S.Rng(seed + 1), 144)
+    res = []
+    for use_ref in (False, True):
+        oracle.use_reference(use_ref)
+        G = oracle.gdft(0, kx, ky, kz, ix, iy, iz, fm, t)
+        y = G.forward(xi)
+        res.append((y, G.adjoint(y)))
+    oracle.use_reference(False)
+    assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
+
+
+def test_kb_lut_matches_reference_values(oracle):
+    """LUT endpoints and beta as Gnufft.cpp:84-88 / griddingSupport.cpp:52-76 define them."""
+    lut, beta = oracle.kb_lut(0)
+    assert lut.size == 40000
+    assert abs(beta - np.pi * np.sqrt(1.5 ** 2 * 64 / 4 - 0.8)) < 1e-5
+    assert np.all(np.diff(lut) <= 0)  # I0(beta*sqrt(1-v)) decreases in v
+    assert abs(lut[-1] - 0.25) < 1e-3  # I0(~0)/W at the edge
+
+
+def _np_gradient(x, nx, ny, nz, beta, kind, delta, dims2pen):
+    """Independent numpy statement of Robject::Gradient (Robject.cpp:49-165)."""
+    N = x.size
+    nd = 2 if (nz == 1 or dims2pen == 2) else 3
+    offs = [1, ny, nx * ny][:nd]
+    g = np.zeros(N, np.complex128)
+    for off in offs:
+        d = np.zeros(N, np.complex128)
+        d[off:] = x[off:] - x[:-off]
+        if kind == "tv":
+            d = d / np.sqrt(1 + np.abs(d / delta) ** 2)
+        o = np.zeros(N, np.complex128)
+        o[off - 1] = -d[off]
+        o[N - 1 - off] = d[N - 1 - off]
+        o[: N - 1 - off] = d[: N - 1 - off] - d[off: N - 1]
+        g += o
+    return beta * g
+
+
+@pytest.mark.parametrize("kind", ["quad", "tv"])
+@pytest.mark.parametrize("dims", [(8, 8, 1), (6, 6, 4)])
+def test_penalty_gradient_quirks(oracle, kind, dims):
+    nx, ny, nz = dims
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(nx * ny * nz) + 1j * rng.standard_normal(nx * ny * nz)
+    g = oracle.penalty_gradient(2, kind, nx, ny, nz, 0.7, 0.3, 3, x)
+    ref = _np_gradient(x, nx, ny, nz, 0.7, kind, 0.3, 3)
+    assert rel_l2(g, ref) < 1e-12
+
+
+def test_timeseg_hanning_tail(oracle):
+    """Sum of the Hanning weights is 1 inside the readout and < 1 in the last interval."""
+    from powergrid_b200 import synthetic as S
+    kx, ky, t = S.spiral(32, 1, 400, 10e-3)
+    G = oracle.gnufft(0, kx.size, 32, 32, 1, kx, ky, np.zeros_like(kx))
+    A = oracle.timeseg(G, np.zeros(1024, np.float32), t, kx.size, 1024, 5)
+    AA, Wo, WoH, (tau, tmin) = A.timeseg_tables()
+    s = AA.real.sum(axis=0)
+    inner = t <= (5 - 1) * tau
+    assert np.allclose(s[inner], 1.0, atol=1e-6)
+    assert np.all(s[~inner] < 1.0)
+    assert np.all((AA.real >= 0) & (AA.real <= 1)) and np.all(AA.imag == 0)
+
+
+def test_oracle_pcg_float_vs_fp64(oracle):
+    """The float reference path and the FP64 oracle agree on a 5-iteration solve."""
+    c = _case(os.path.join(HERE, "golden", "pcg2d.npz"))
+    assert rel_l2(c["x_pcg_f32"], c["x_pcg_f64"]) < 1e-4
