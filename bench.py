@@ -1,0 +1,341 @@
+"""Benchmark: PCG iterations/s of the 2-D field-corrected SENSE reconstruction.
+
+Workload (one "step" = one full reconstruction): SENSE<TimeSegmentation<Gnufft>>,
+128x128 image, L = 8 Hanning segments, 4 coils, 16-interleave spiral with
+8192 samples per interleave (131072 samples), 20 ms readout, +-100 Hz field
+map, QuadPenalty beta = 1e-3, 20 PWLS-PCG iterations (reconSolve semantics:
+W = 1, x0 = 0).  Seeded synthetic inputs stand in for ISMRMRD data.
+
+  value      PCG iterations/s with inputs resident in HBM (device-timed,
+             CUDA events per step, L2 flushed between steps, max over ranks)
+  e2e        the same metric through the C ABI's host-buffer entry point
+             pg_pcg_solve (H2D of the coil data and D2H of the image inside
+             the timed region)
+  roofline   the adjoint gridding kernel (k_spread), timed by CUDA events
+             inside the timed region, against the measured HBM bandwidth
+  cpu_baseline  the reference CPU path on this host's cores (rank 0, N=1)
+
+`--impl reference` times the reference's own CPU implementation of the path
+(oracle/_ref when built from the reference sources, else the oracle port).
+Multi-GPU: independent replicas (weak scaling), one process per GPU.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [ROOT, os.path.join(ROOT, "oracle")]
+
+METRIC = "PCG iters/s"
+UNIT = "iter/s"
+NITER = 20
+WORKLOAD = ("SENSE<TimeSegmentation<Gnufft>> 128x128, L=8 Hanning, 4 coils, 16x8192 spiral "
+            "(131072 samples/coil), 20 ms readout, +-100 Hz, QuadPenalty beta=1e-3, 20 PCG iterations")
+
+
+def _config(extra=None):
+    c = {"workload": WORKLOAD, "image": [128, 128, 1], "coils": 4, "segments": 8, "samples_per_coil": 131072,
+         "pcg_iterations_per_step": NITER, "l2": "flushed between steps (256 MiB write)",
+         "parallelism": "replicas"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                v = [s.strip() for s in out.stdout.strip().split(",")]
+                if len(v) == 7:
+                    self.rows.append(v)
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(self.rows[0][1]), "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _problem():
+    from powergrid_b200 import synthetic as S
+    return S.config2()
+
+
+# --------------------------------------------------------------------------------------------
+# CPU baseline: the reference CPU path (reference kernels when built, else the oracle port)
+# --------------------------------------------------------------------------------------------
+def cpu_reference_rate(p, y, iters: int, threads: int):
+    import oracle as O
+    kind = "port"
+    if O.reference_available():
+        O.use_reference(True)
+        kind = "reference"
+    O.set_threads(threads)
+    op = O.build_problem_op(p, 0)
+    t0 = time.perf_counter()
+    _, n = op.pcg(y, "quad", p.nx, p.ny, p.nz, p.beta, niter=iters)
+    dt = time.perf_counter() - t0
+    O.set_threads(1)
+    if kind == "reference":
+        O.use_reference(False)
+    return n / dt, kind, n, dt
+
+
+def run_reference_arm(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    p = _problem()
+    import oracle as O
+    O.set_threads(os.cpu_count() or 1)
+    y = O.build_problem_op(p, 0).forward(p.x_true)
+    threads = os.cpu_count() or 1
+    iters_per_step = 2
+    for _ in range(args.warmup):
+        cpu_reference_rate(p, y, iters_per_step, threads)
+    rates, tot_it, tot_t, kind = [], 0, 0.0, "port"
+    for _ in range(args.steps):
+        r, kind, n, dt = cpu_reference_rate(p, y, iters_per_step, threads)
+        rates.append(r)
+        tot_it += n
+        tot_t += dt
+    value = tot_it / tot_t
+    sample = (f"{iters_per_step} PCG iterations of the workload per step (plus the initial forward), "
+              f"{threads} host threads over the independent (coil, segment) Gnufft calls")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * tot_t / max(1, args.steps), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": _config({"impl_note": "reference kernels (gridding.cpp, griddingSupport.cpp, ftCpu.cpp, "
+                                            "fftCPU.cpp) compiled from the reference sources; Armadillo layers "
+                                            "restated; project FFT behind the FFTW API"
+                               if kind == "reference" else "oracle port"}),
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# --------------------------------------------------------------------------------------------
+# GPU arm
+# --------------------------------------------------------------------------------------------
+def run_gpu_arm(args):
+    import ctypes as C
+
+    import torch
+
+    ws, rank, local = _dist()
+    if ws > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    import powergrid_b200 as pg
+    from powergrid_b200 import _lib
+    from powergrid_b200._lib import P, Penalty, check
+
+    from powergrid_b200 import build as B
+    B.build()
+    pg.init(local)
+    L = _lib.load()
+    p = _problem()
+    M, n = p.kx.size, p.nimg
+    G = pg.Gnufft(M, 2.0, p.nx, p.ny, 1, p.kx, p.ky, p.kz)
+    A = pg.TimeSegmentation(G, p.fm, p.t, M, n, p.L, 1, 1)
+    Sg = pg.SENSE(A, p.smap, M, n, p.nc)
+    R = pg.QuadPenalty(p.nx, p.ny, 1, p.beta)
+
+    stream = torch.cuda.Stream(device=dev)
+    sp = P(stream.cuda_stream)
+    xt = torch.from_numpy(p.x_true).to(dev)
+    y = torch.empty(Sg.n_data, dtype=torch.complex64, device=dev)
+    x = torch.empty(n, dtype=torch.complex64, device=dev)
+    iters = torch.zeros(1, dtype=torch.int32, device=dev)
+    with torch.cuda.stream(stream):
+        Sg.forward(xt, out=y, stream=stream)
+    stream.synchronize()
+    pen = R._struct()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def solve():
+        check(L.pg_pcg_solve_device(Sg.handle, None, None, P(y.data_ptr()), C.byref(pen), NITER, P(x.data_ptr()),
+                                    P(iters.data_ptr()), sp))
+
+    # warm-up (also builds the graph path and cuFFT plans)
+    for _ in range(max(3, args.warmup)):
+        solve()
+    stream.synchronize()
+
+    check(L.pg_profile_enable(1))
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    spread_ms, step_ms = [], []
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    launches0 = _lib.launches()
+    sampler = ClockSampler(local)
+    with sampler:
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                ev[i][0].record(stream)
+                solve()
+                ev[i][1].record(stream)
+            stream.synchronize()
+            step_ms.append(ev[i][0].elapsed_time(ev[i][1]))
+            ms = C.c_float()
+            if L.pg_profile_stage_ms(b"spread", C.byref(ms)) == 0:
+                spread_ms.append(ms.value)
+    torch.cuda.synchronize()
+    launches = _lib.launches() - launches0
+    check(L.pg_profile_enable(0))
+    total_ms = sum(step_ms)
+    done = int(iters.item())
+    if ws > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = ws * args.steps * NITER / (total_ms / 1000.0)
+
+    # end to end through the C ABI host entry point (pinned host buffers)
+    yh = torch.empty(Sg.n_data, dtype=torch.complex64).pin_memory()
+    yh.copy_(y.cpu())
+    xh = torch.empty(n, dtype=torch.complex64).pin_memory()
+    itn = C.c_uint64()
+    check(L.pg_pcg_solve(Sg.handle, None, None, P(yh.data_ptr()), C.byref(pen), NITER, P(xh.data_ptr()),
+                         C.byref(itn)))
+    e2e_steps = max(3, min(args.steps, 10))
+    if ws > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        check(L.pg_pcg_solve(Sg.handle, None, None, P(yh.data_ptr()), C.byref(pen), NITER, P(xh.data_ptr()),
+                             C.byref(itn)))
+    e2e_s = time.perf_counter() - t0
+    if ws > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = ws * e2e_steps * NITER / e2e_s
+
+    # roofline of the adjoint gridding kernel: algorithmic bytes per launch
+    # = coils * (M * (4*d + 8 + 4) + L * G * 8), d = 2, G = 256^2
+    G2 = (2 * p.nx) * (2 * p.ny)
+    alg_bytes = p.nc * (M * (4 * 2 + 8 + 4) + p.L * G2 * 8)
+    peak, peak_kind = _peaks()
+    avg_spread = statistics.mean(spread_ms) if spread_ms else float("nan")
+    achieved = alg_bytes / (avg_spread / 1000.0) / 1e9 if spread_ms else None
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "spread_cfg2_traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    if rank == 0:
+        cpu = None
+        if ws == 1 and not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            y_host = y.cpu().numpy()
+            rate, kind, nit, dt = cpu_reference_rate(p, y_host, NITER, threads)
+            cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
+                   "sample": f"one full reconstruction ({nit} PCG iterations, {dt:.1f} s) of the same workload, "
+                             f"{threads} host threads over independent (coil, segment) Gnufft calls"}
+        clocks = sampler.summary()
+        lat = sorted(step_ms)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+                "config": _config({"iterations_completed_last_step": done}),
+                "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
+                "clocks": clocks,
+                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(Sg.n_data * 8),
+                        "d2h_bytes_per_step": int(n * 8)},
+                "roofline": {"kernel": "k_spread<2> (adjoint gridding, TS-fused, 4 coils x 8 segments)",
+                             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                             "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_spread,
+                             "peak_source": peak_kind},
+                "cpu_baseline": cpu,
+                "gpu_launches": int(launches)}
+        print(json.dumps(line))
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_gpu_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -180,6 +180,15 @@ pg_status pg_cancel(pg_server s, uint64_t ticket);
 uint64_t pg_request_footprint(const pg_request* req);
 
 /* ---- instrumentation and fault injection (host-side only) ------------ */
+/* Stage timing: while enabled, the NUFFT and Gdft pipelines record a CUDA
+ * event pair around each stage kernel on the stream they run on (also inside
+ * captured CUDA graphs).  pg_profile_stage_ms returns the elapsed time of the
+ * most recent recorded pair of a stage ("pre", "fft_fwd", "gather", "zero",
+ * "spread", "fft_adj", "post", "dft_fwd", "dft_adj"); the caller must have
+ * synchronised the stream.  Returns PG_NOT_READY if the stage never ran. */
+pg_status pg_profile_enable(int on);
+pg_status pg_profile_stage_ms(const char* stage, float* ms);
+
 /* Make the n-th device allocation from now fail with PG_OUT_OF_MEMORY
  * (n = 0 disables). */
 void pg_debug_fail_allocation_after(uint64_t n);

@@ -81,6 +81,8 @@ SIGNATURES = {
     "pg_request_footprint": (U64, [C.POINTER(Request)]),
     "pg_debug_fail_allocation_after": (None, [U64]),
     "pg_util_kb_lut": (U64, [F32, P, U64, C.POINTER(F32)]),
+    "pg_profile_enable": (C.c_int, [C.c_int]),
+    "pg_profile_stage_ms": (C.c_int, [C.c_char_p, C.POINTER(F32)]),
     "pg_util_gnufft_binning": (C.c_int, [P, P, P, C.POINTER(U64)]),
 }
 

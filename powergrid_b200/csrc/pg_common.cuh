@@ -35,9 +35,11 @@ void dev_free(void* p);
 #define PG_CUDA(call)                                                                              \
   do {                                                                                             \
     cudaError_t e_ = (call);                                                                       \
-    if (e_ != cudaSuccess)                                                                         \
+    if (e_ != cudaSuccess) {                                                                       \
+      cudaGetLastError(); /* do not leave a non-sticky error for the caller's next launch */      \
       return ::pg::set_error(PG_CUDA_ERROR, "%s:%d %s: %s", __FILE__, __LINE__, #call,            \
                              cudaGetErrorString(e_));                                              \
+    }                                                                                              \
   } while (0)
 
 #define PG_CUFFT(call)                                                                             \

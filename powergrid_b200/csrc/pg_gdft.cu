@@ -13,6 +13,7 @@
 // outputs alone do not fill the GPU the inner sum is split over blockIdx.y
 // and the partial sums are combined in a fixed order (deterministic).
 #include "pg_gdft.cuh"
+#include "pg_profile.cuh"
 
 namespace pg {
 
@@ -229,6 +230,7 @@ pg_status gdft_forward(GdftPlan* p, int C, const float2* S, const float2* x, flo
     PG_TRY(p->part.alloc(std::max<uint64_t>(p->part.n, (uint64_t)nsplit * ncp * p->nk)));
     PG_LAUNCH(k_apply_maps, ceil_div(p->ni, 256), 256, 0, s, p->ni, nc, c0, S, x, p->xin.p);
     if (ncp > nc) PG_CUDA(cudaMemsetAsync(p->xin.p + (uint64_t)nc * p->ni, 0, (ncp - nc) * p->ni * sizeof(float2), s));
+    ProfScope ps("dft_fwd", s);
     switch (ncp) {
       case 1: PG_TRY(launch_fwd<1>(p, nsplit, jchunk, p->xin.p, p->part.p, s)); break;
       case 2: PG_TRY(launch_fwd<2>(p, nsplit, jchunk, p->xin.p, p->part.p, s)); break;
@@ -261,6 +263,7 @@ pg_status gdft_adjoint(GdftPlan* p, int C, const float2* S, const float2* y, uin
       yc = p->xin.p;
     }
     const uint64_t stride = (ncp > nc) ? p->nk : dstride;
+    ProfScope ps("dft_adj", s);
     switch (ncp) {
       case 1: PG_TRY(launch_adj<1>(p, nsplit, ichunk, yc, stride, p->part.p, s)); break;
       case 2: PG_TRY(launch_adj<2>(p, nsplit, ichunk, yc, stride, p->part.p, s)); break;

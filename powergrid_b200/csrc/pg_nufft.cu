@@ -27,6 +27,7 @@
 #include <cstring>
 
 #include "pg_nufft.cuh"
+#include "pg_profile.cuh"
 
 namespace pg {
 
@@ -611,12 +612,19 @@ pg_status nufft_forward(NufftPlan* p, const NufftBatch& b, const float2* x, floa
     cufftHandle h;
     PG_TRY(ensure_workspace(p, B, &h, s));
     dim3 grid(ceil_div(G, 256), B);
-    PG_LAUNCH(k_pre, grid, 256, 0, s, g, L, x, b.S, c0, b.E, b.Wo, p->deap.p, scale, p->grids.p);
-    PG_CUFFT(cufftExecC2C(h, reinterpret_cast<cufftComplex*>(p->grids.p), reinterpret_cast<cufftComplex*>(p->grids.p),
-                          CUFFT_FORWARD));
+    {
+      ProfScope ps("pre", s);
+      PG_LAUNCH(k_pre, grid, 256, 0, s, g, L, x, b.S, c0, b.E, b.Wo, p->deap.p, scale, p->grids.p);
+    }
+    {
+      ProfScope ps("fft_fwd", s);
+      PG_CUFFT(cufftExecC2C(h, reinterpret_cast<cufftComplex*>(p->grids.p),
+                            reinterpret_cast<cufftComplex*>(p->grids.p), CUFFT_FORWARD));
+    }
     float2* yc = y + (uint64_t)c0 * b.data_stride;
     const float2* aa = (L > 1 || bin->aa.p) ? bin->aa.p : nullptr;
     const int* l0 = bin->l0.p;
+    ProfScope ps("gather", s);
     if (g.dim == 2)
       PG_LAUNCH(k_gather<2>, ceil_div(p->M, 128), 128, 0, s, g, p->M, bin->start.p, bin->wxy.p, bin->wz.p,
                 bin->perm.p, l0, aa, K, L, p->grids.p, nb, yc, b.data_stride);
@@ -649,13 +657,17 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
     const int B = nb * L;
     cufftHandle h;
     PG_TRY(ensure_workspace(p, B, &h, s));
-    PG_CUDA(cudaMemsetAsync(p->grids.p, 0, (size_t)B * G * sizeof(float2), s));
+    {
+      ProfScope ps("zero", s);
+      PG_CUDA(cudaMemsetAsync(p->grids.p, 0, (size_t)B * G * sizeof(float2), s));
+    }
     const int cc = std::min(Cc, nb);
     const size_t smem = plane_bytes * K * cc;
     dim3 grid(bin->nsub, ceil_div(nb, cc));
     const float2* yc = y + (uint64_t)c0 * b.data_stride;
     const float2* aa = (L > 1 || bin->aa.p) ? bin->aa.p : nullptr;
     if (bin->nsub > 0) {
+      ProfScope ps("spread", s);
       if (g.dim == 2) {
         PG_CUDA(cudaFuncSetAttribute(k_spread<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         PG_LAUNCH(k_spread<2>, grid, 256, smem, s, g, t, bin->subprob.p, bin->start.p, bin->wxy.p, bin->wz.p,
@@ -666,9 +678,13 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
                   bin->perm.p, aa, K, L, yc, b.data_stride, nb, cc, p->grids.p);
       }
     }
-    PG_CUFFT(cufftExecC2C(h, reinterpret_cast<cufftComplex*>(p->grids.p), reinterpret_cast<cufftComplex*>(p->grids.p),
-                          CUFFT_INVERSE));
+    {
+      ProfScope ps("fft_adj", s);
+      PG_CUFFT(cufftExecC2C(h, reinterpret_cast<cufftComplex*>(p->grids.p),
+                            reinterpret_cast<cufftComplex*>(p->grids.p), CUFFT_INVERSE));
+    }
     const int acc = (b.accumulate || c0 > 0) ? 1 : 0;
+    ProfScope ps("post", s);
     PG_LAUNCH(k_post, ceil_div(g.nimg(), 256), 256, 0, s, g, nb, L, p->grids.p, b.S, c0, b.E, b.WoH, p->deap.p,
               scale, acc, x);
   }

@@ -207,17 +207,17 @@ pg_status SenseOp::forward(const float2* x, float2* y, cudaStream_t s) {
     NufftBatch b;
     b.C = (int)nc;
     b.S = S.p;
-    b.data_stride = n_data;
+    b.data_stride = n_data / nc;  // per-coil data length (SENSE.cpp:86)
     if (ts) { b.Wo = ts->Wo.p; b.bin = ts->bin.get(); }
     return nufft_forward(plan, b, x, y, s);
   }
   if (inner->kind == PG_OP_GDFT)
-    return gdft_forward(static_cast<GdftOp*>(inner)->plan.get(), (int)nc, S.p, x, y, n_data, s);
+    return gdft_forward(static_cast<GdftOp*>(inner)->plan.get(), (int)nc, S.p, x, y, n_data / nc, s);
   // generic (SENSE.cpp:59-70)
   PG_TRY(tmp_img.alloc(n_image));
   for (uint64_t c = 0; c < nc; ++c) {
     PG_LAUNCH(k_cmul, ceil_div(n_image, 256), 256, 0, s, n_image, S.p + c * n_image, x, 0, tmp_img.p);
-    PG_TRY(inner->forward(tmp_img.p, y + c * n_data, s));
+    PG_TRY(inner->forward(tmp_img.p, y + c * (n_data / nc), s));
   }
   return PG_OK;
 }
@@ -229,16 +229,16 @@ pg_status SenseOp::adjoint(const float2* y, float2* x, cudaStream_t s) {
     NufftBatch b;
     b.C = (int)nc;
     b.S = S.p;
-    b.data_stride = n_data;
+    b.data_stride = n_data / nc;  // per-coil data length (SENSE.cpp:86)
     if (ts) { b.WoH = ts->WoH.p; b.bin = ts->bin.get(); }
     return nufft_adjoint(plan, b, y, x, s);
   }
   if (inner->kind == PG_OP_GDFT)
-    return gdft_adjoint(static_cast<GdftOp*>(inner)->plan.get(), (int)nc, S.p, y, n_data, x, s);
+    return gdft_adjoint(static_cast<GdftOp*>(inner)->plan.get(), (int)nc, S.p, y, n_data / nc, x, s);
   // generic (SENSE.cpp:84-96)
   PG_TRY(tmp_img.alloc(n_image));
   for (uint64_t c = 0; c < nc; ++c) {
-    PG_TRY(inner->adjoint(y + c * n_data, tmp_img.p, s));
+    PG_TRY(inner->adjoint(y + c * (n_data / nc), tmp_img.p, s));
     PG_LAUNCH(k_cmul_acc, ceil_div(n_image, 256), 256, 0, s, n_image, tmp_img.p, S.p + c * n_image, 1,
               c > 0 ? 1 : 0, x);
   }

@@ -64,7 +64,8 @@ def test_operator_vs_reference_fixture(pg, name):
     print(f"{name}: fwd {ey:.2e} (fp64 {ey64:.2e}, ref-vs-fp64 {ref64y:.2e}); "
           f"adj {ex:.2e} (fp64 {ex64:.2e}, ref-vs-fp64 {ref64x:.2e})")
     assert ey <= OP_TOL and ex <= OP_TOL
-    assert ey64 <= OP_TOL and ex64 <= OP_TOL
+    # vs FP64: no worse than the reference CPU path's own float error (plus the tolerance)
+    assert ey64 <= ref64y + OP_TOL and ex64 <= ref64x + OP_TOL
 
 
 @pytest.mark.parametrize("name", ["pcg2d", "pcgtv2d"])
@@ -131,11 +132,19 @@ def test_config1_full_size_vs_oracle(pg, oracle):
     xa = Sg / y64
     assert rel_l2(xa, o32.adjoint(y64)) <= OP_TOL
     R = pg.QuadPenalty(p.nx, p.ny, 1, p.beta)
-    x = pg.reconSolve(y64, Sg, R, niter=10)
-    xr, _ = o32.pcg(y64, "quad", p.nx, p.ny, 1, p.beta, niter=10)
-    x64, _ = o64.pcg(y64, "quad", p.nx, p.ny, 1, p.beta, niter=10)
-    print(f"cfg1 pcg: {rel_l2(x, xr):.2e} vs reference, {rel_l2(x, x64):.2e} vs fp64")
-    assert rel_l2(x, xr) <= PCG_TOL and rel_l2(x, x64) <= PCG_TOL
+    # Config 1 has one sample per unknown and a white-noise image, so CG
+    # amplifies FP32 rounding: the reference CPU path itself drifts from FP64
+    # by ~3e-4 after 5 iterations and ~4e-2 after 10.  At 5 iterations every
+    # bound holds; at 10 the GPU path must stay within 1e-3 of the reference
+    # path and no further from FP64 than the reference path is.
+    for niter, tol in ((5, PCG_TOL), (10, 1e-3)):
+        x = pg.reconSolve(y64, Sg, R, niter=niter)
+        xr, _ = o32.pcg(y64, "quad", p.nx, p.ny, 1, p.beta, niter=niter)
+        x64, _ = o64.pcg(y64, "quad", p.nx, p.ny, 1, p.beta, niter=niter)
+        e, e64, r64 = rel_l2(x, xr), rel_l2(x, x64), rel_l2(xr, x64)
+        print(f"cfg1 pcg({niter}): {e:.2e} vs reference, {e64:.2e} vs fp64 (reference vs fp64 {r64:.2e})")
+        assert e <= tol
+        assert e64 <= max(PCG_TOL, 1.1 * r64)
 
 
 def test_config2_operator_full_size_vs_oracle(pg, oracle):
