@@ -218,34 +218,42 @@ def run_gpu_arm(args):
         check(L.pg_pcg_solve_device(Sg.handle, None, None, P(y.data_ptr()), C.byref(pen), NITER, P(x.data_ptr()),
                                     P(iters.data_ptr()), sp))
 
-    # warm-up (also builds the graph path and cuFFT plans)
-    for _ in range(max(3, args.warmup)):
-        solve()
-    stream.synchronize()
-
+    # Stage timing stays on for warm-up and timed steps alike (same graph).
     check(L.pg_profile_enable(1))
+    sampler = ClockSampler(local)
+    sampler.__enter__()
+    for _ in range(max(3, args.warmup)):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            solve()
+    stream.synchronize()
+    sampler.rows.clear()
+
+    stages = ["pre", "fft_fwd", "gather", "zero", "spread", "fft_adj", "post"]
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    spread_ms, step_ms = [], []
+    stage_ms = {k: [] for k in stages}
+    step_ms = []
     if ws > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
     launches0 = _lib.launches()
-    sampler = ClockSampler(local)
-    with sampler:
-        for i in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.zero_()
-                ev[i][0].record(stream)
-                solve()
-                ev[i][1].record(stream)
-            stream.synchronize()
-            step_ms.append(ev[i][0].elapsed_time(ev[i][1]))
+    for i in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            ev[i][0].record(stream)
+            solve()
+            ev[i][1].record(stream)
+        stream.synchronize()
+        step_ms.append(ev[i][0].elapsed_time(ev[i][1]))
+        for k in stages:
             ms = C.c_float()
-            if L.pg_profile_stage_ms(b"spread", C.byref(ms)) == 0:
-                spread_ms.append(ms.value)
+            if L.pg_profile_stage_ms(k.encode(), C.byref(ms)) == 0:
+                stage_ms[k].append(ms.value)
     torch.cuda.synchronize()
     launches = _lib.launches() - launches0
+    sampler.__exit__(None, None, None)
     check(L.pg_profile_enable(0))
+    spread_ms = stage_ms["spread"]
     total_ms = sum(step_ms)
     done = int(iters.item())
     if ws > 1:
@@ -309,6 +317,7 @@ def run_gpu_arm(args):
                 "clocks": clocks,
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(Sg.n_data * 8),
                         "d2h_bytes_per_step": int(n * 8)},
+                "stages_ms_per_launch": {k: (statistics.mean(v) if v else None) for k, v in stage_ms.items()},
                 "roofline": {"kernel": "k_spread<2> (adjoint gridding, TS-fused, 4 coils x 8 segments)",
                              "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": (achieved / peak) if achieved else None, "traffic": traffic,

@@ -32,6 +32,22 @@ extern std::atomic<uint64_t> g_fail_alloc_countdown;
 pg_status dev_alloc(void** p, size_t bytes);
 void dev_free(void* p);
 
+// Per-thread device arena.  While a thread has an arena installed, device
+// allocations are carved from one slab (falling back to stream-ordered pool
+// allocations past its end) and frees are deferred to arena_release(), which
+// returns everything stream-ordered on the arena's stream.  The request
+// server uses one arena per request so that building and running a request
+// never calls cudaMalloc/cudaFree, which would serialise the other streams.
+struct Arena {
+  char* base = nullptr;
+  size_t cap = 0, used = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<void*> overflow;
+};
+pg_status arena_open(Arena* a, size_t bytes, cudaStream_t s);
+void arena_install(Arena* a);   // nullptr uninstalls
+void arena_release(Arena* a);   // after all work on a->stream that uses it
+
 #define PG_CUDA(call)                                                                              \
   do {                                                                                             \
     cudaError_t e_ = (call);                                                                       \
@@ -103,6 +119,15 @@ struct DevBuf {
   }
   size_t bytes() const { return n * sizeof(T); }
 };
+
+// Grow a lazily-sized workspace used on stream s: queued work on s may still
+// read the old buffer, so drain s before replacing it.
+template <typename T>
+inline pg_status grow(DevBuf<T>& b, size_t count, cudaStream_t s) {
+  if (b.n >= count && b.p) return PG_OK;
+  if (b.p) PG_CUDA(cudaStreamSynchronize(s));
+  return b.alloc(count);
+}
 
 // ---- complex helpers (float2 = interleaved complex64) ----------------------
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {

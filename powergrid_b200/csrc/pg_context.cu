@@ -49,6 +49,14 @@ pg_status ensure_init() {
     return set_error(PG_CUDA_ERROR, "device %d is sm_%d%d; this library is built for sm_100a", g_device, prop.major,
                      prop.minor);
   g_sms = prop.multiProcessorCount;
+  {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, g_device) == cudaSuccess) {
+      uint64_t thr = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    cudaGetLastError();
+  }
   PG_CUDA(cudaStreamCreateWithFlags(&g_stream, cudaStreamNonBlocking));
   g_inited = true;
   return PG_OK;
@@ -57,7 +65,58 @@ pg_status ensure_init() {
 cudaStream_t default_stream() { return g_stream; }
 int sm_count() { return g_sms; }
 
+namespace {
+thread_local Arena* t_arena = nullptr;
+}
+
+void arena_install(Arena* a) { t_arena = a; }
+
+pg_status arena_open(Arena* a, size_t bytes, cudaStream_t s) {
+  a->stream = s;
+  a->cap = bytes;
+  a->used = 0;
+  a->overflow.clear();
+  a->base = nullptr;
+  if (bytes == 0) return PG_OK;
+  cudaError_t e = cudaMallocAsync((void**)&a->base, bytes, s);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    a->base = nullptr;
+    return set_error(e == cudaErrorMemoryAllocation ? PG_OUT_OF_MEMORY : PG_CUDA_ERROR,
+                     "arena of %zu bytes: %s", bytes, cudaGetErrorString(e));
+  }
+  // make the slab usable from every stream before anything is carved from it
+  e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) { cudaGetLastError(); return set_error(PG_CUDA_ERROR, "arena sync: %s", cudaGetErrorString(e)); }
+  return PG_OK;
+}
+
+void arena_release(Arena* a) {
+  if (a->base) cudaFreeAsync(a->base, a->stream);
+  for (void* p : a->overflow) cudaFreeAsync(p, a->stream);
+  a->base = nullptr;
+  a->overflow.clear();
+  a->cap = a->used = 0;
+}
+
 pg_status dev_alloc(void** p, size_t bytes) {
+  if (t_arena) {
+    Arena* a = t_arena;
+    const size_t off = (a->used + 255) & ~size_t(255);
+    if (a->base && off + bytes <= a->cap) {
+      *p = a->base + off;
+      a->used = off + bytes;
+      return PG_OK;
+    }
+    cudaError_t e = cudaMallocAsync(p, bytes, a->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(a->stream);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return set_error(PG_OUT_OF_MEMORY, "arena overflow allocation of %zu bytes failed", bytes);
+    }
+    a->overflow.push_back(*p);
+    return PG_OK;
+  }
   uint64_t c = g_fail_alloc_countdown.load();
   while (c > 0) {
     if (g_fail_alloc_countdown.compare_exchange_weak(c, c - 1)) {
@@ -74,7 +133,15 @@ pg_status dev_alloc(void** p, size_t bytes) {
   return PG_OK;
 }
 
-void dev_free(void* p) { cudaFree(p); }
+void dev_free(void* p) {
+  if (Arena* a = t_arena) {
+    // arena memory is returned by arena_release
+    if (a->base && (char*)p >= a->base && (char*)p < a->base + a->cap) return;
+    for (void* q : a->overflow)
+      if (q == p) return;
+  }
+  cudaFree(p);
+}
 
 }  // namespace pg
 

@@ -226,8 +226,8 @@ pg_status gdft_forward(GdftPlan* p, int C, const float2* S, const float2* x, flo
   for (int c0 = 0; c0 < C; c0 += kCoilChunk) {
     const int nc = std::min(kCoilChunk, C - c0);
     const int ncp = pad_coils(nc);
-    PG_TRY(p->xin.alloc(std::max<uint64_t>(p->xin.n, (uint64_t)ncp * p->ni)));
-    PG_TRY(p->part.alloc(std::max<uint64_t>(p->part.n, (uint64_t)nsplit * ncp * p->nk)));
+    PG_TRY(grow(p->xin, (uint64_t)ncp * p->ni, s));
+    PG_TRY(grow(p->part, (uint64_t)nsplit * ncp * p->nk, s));
     PG_LAUNCH(k_apply_maps, ceil_div(p->ni, 256), 256, 0, s, p->ni, nc, c0, S, x, p->xin.p);
     if (ncp > nc) PG_CUDA(cudaMemsetAsync(p->xin.p + (uint64_t)nc * p->ni, 0, (ncp - nc) * p->ni * sizeof(float2), s));
     ProfScope ps("dft_fwd", s);
@@ -251,12 +251,12 @@ pg_status gdft_adjoint(GdftPlan* p, int C, const float2* S, const float2* y, uin
   for (int c0 = 0; c0 < C; c0 += kCoilChunk) {
     const int nc = std::min(kCoilChunk, C - c0);
     const int ncp = pad_coils(nc);
-    PG_TRY(p->part.alloc(std::max<uint64_t>(p->part.n, (uint64_t)nsplit * ncp * p->ni)));
+    PG_TRY(grow(p->part, (uint64_t)nsplit * ncp * p->ni, s));
     // Coils past nc read the first coil's data (valid memory); their sums are discarded.
     const float2* yc = y + (uint64_t)c0 * dstride;
     if (ncp > nc) {
       // stage the chunk contiguously so padded coils stay in bounds
-      PG_TRY(p->xin.alloc(std::max<uint64_t>(p->xin.n, (uint64_t)ncp * p->nk)));
+      PG_TRY(grow(p->xin, (uint64_t)ncp * p->nk, s));
       for (int c = 0; c < ncp; ++c)
         PG_CUDA(cudaMemcpyAsync(p->xin.p + (uint64_t)c * p->nk, yc + (uint64_t)std::min(c, nc - 1) * dstride,
                                 p->nk * sizeof(float2), cudaMemcpyDeviceToDevice, s));

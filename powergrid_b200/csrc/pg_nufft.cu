@@ -489,9 +489,14 @@ pg_status nufft_plan_create(std::unique_ptr<NufftPlan>* out, uint64_t M, float g
   PG_TRY(p->lut.upload(lut.data(), lut.size(), s));
   PG_TRY(p->deap.upload(deap.data(), deap.size(), s));
   PG_CUDA(cudaStreamSynchronize(s));
-  PG_TRY(nufft_build_binning(p.get(), 1, 1, nullptr, nullptr, &p->plain, s));
+  // the unsegmented binning is built on first use (time-segmented operators never need it)
   *out = std::move(p);
   return PG_OK;
+}
+
+pg_status nufft_plain_binning(NufftPlan* p, cudaStream_t s) {
+  if (p->plain) return PG_OK;
+  return nufft_build_binning(p, 1, 1, nullptr, nullptr, &p->plain, s);
 }
 
 pg_status nufft_build_binning(NufftPlan* p, int L, int K, const int* l0_host, const float2* aa_host,
@@ -570,7 +575,10 @@ pg_status nufft_build_binning(NufftPlan* p, int L, int K, const int* l0_host, co
 // ---------------------------------------------------------------------------
 static pg_status ensure_workspace(NufftPlan* p, int B, cufftHandle* h, cudaStream_t s) {
   const uint64_t G = p->g.ngrid();
-  if (p->grids.n < (uint64_t)B * G) PG_TRY(p->grids.alloc((uint64_t)B * G));
+  if (p->grids.n < (uint64_t)B * G) {
+    PG_CUDA(cudaStreamSynchronize(s));  // queued work may still use the old workspace
+    PG_TRY(p->grids.alloc((uint64_t)B * G));
+  }
   auto it = p->ffts.find(B);
   if (it == p->ffts.end()) {
     cufftHandle hh;
@@ -580,13 +588,20 @@ static pg_status ensure_workspace(NufftPlan* p, int B, cufftHandle* h, cudaStrea
     if (p->g.dim == 2) { rank = 2; n[0] = p->g.Gx; n[1] = p->g.Gy; }
     else { rank = 3; n[0] = p->g.Gz; n[1] = p->g.Gx; n[2] = p->g.Gy; }
     size_t work = 0;
+    PG_CUFFT(cufftSetAutoAllocation(hh, 0));
     cufftResult r = cufftMakePlanMany(hh, rank, n, nullptr, 1, (int)G, nullptr, 1, (int)G, CUFFT_C2C, B, &work);
     if (r != CUFFT_SUCCESS) {
       cufftDestroy(hh);
       return set_error(r == CUFFT_ALLOC_FAILED ? PG_OUT_OF_MEMORY : PG_CUFFT_ERROR, "cufftMakePlanMany: %d", (int)r);
     }
+    if (work > p->fft_work.n) {
+      // the old area may still be in use by queued transforms of this plan
+      PG_CUDA(cudaStreamSynchronize(s));
+      PG_TRY(p->fft_work.alloc(work));
+    }
     it = p->ffts.emplace(B, hh).first;
   }
+  PG_CUFFT(cufftSetWorkArea(it->second, p->fft_work.p));
   PG_CUFFT(cufftSetStream(it->second, s));
   *h = it->second;
   return PG_OK;
@@ -601,6 +616,7 @@ static int batch_coils(const NufftPlan* p, int C, int L) {
 
 pg_status nufft_forward(NufftPlan* p, const NufftBatch& b, const float2* x, float2* y, cudaStream_t s) {
   const NufftGeom& g = p->g;
+  if (!b.bin) PG_TRY(nufft_plain_binning(p, s));
   const Binning* bin = b.bin ? b.bin : p->plain.get();
   const int L = bin->L, K = bin->K;
   const int Cb = batch_coils(p, b.C, L);
@@ -637,6 +653,7 @@ pg_status nufft_forward(NufftPlan* p, const NufftBatch& b, const float2* x, floa
 
 pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, float2* x, cudaStream_t s) {
   const NufftGeom& g = p->g;
+  if (!b.bin) PG_TRY(nufft_plain_binning(p, s));
   const Binning* bin = b.bin ? b.bin : p->plain.get();
   const int L = bin->L, K = bin->K;
   const int Cb = batch_coils(p, b.C, L);

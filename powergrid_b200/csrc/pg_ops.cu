@@ -149,8 +149,8 @@ pg_status TimeSegOp::forward(const float2* x, float2* y, cudaStream_t s) {
     return nufft_forward(g->plan.get(), b, x, y, s);
   }
   // generic: y = sum_l AA_l (.) G(Wo_l (.) x)   (TimeSegmentation.cpp:266-295)
-  PG_TRY(tmp_img.alloc(n_image));
-  PG_TRY(tmp_data.alloc(n_data));
+  PG_TRY(grow(tmp_img, n_image, s));
+  PG_TRY(grow(tmp_data, n_data, s));
   for (int l = 0; l < tab.L; ++l) {
     PG_LAUNCH(k_cmul, ceil_div(n_image, 256), 256, 0, s, n_image, Wo.p + (uint64_t)l * n_image, x, 0, tmp_img.p);
     PG_TRY(inner->forward(tmp_img.p, tmp_data.p, s));
@@ -171,8 +171,8 @@ pg_status TimeSegOp::adjoint(const float2* y, float2* x, cudaStream_t s) {
     return nufft_adjoint(g->plan.get(), b, y, x, s);
   }
   // generic: x = sum_l WoH_l (.) G^H(conj(AA_l) (.) y)   (TimeSegmentation.cpp:304-323)
-  PG_TRY(tmp_img.alloc(n_image));
-  PG_TRY(tmp_data.alloc(n_data));
+  PG_TRY(grow(tmp_img, n_image, s));
+  PG_TRY(grow(tmp_data, n_data, s));
   for (int l = 0; l < tab.L; ++l) {
     PG_LAUNCH(k_cmul, ceil_div(n_data, 256), 256, 0, s, n_data, AAfull.p + (uint64_t)l * n_data, y, 1, tmp_data.p);
     PG_TRY(inner->adjoint(tmp_data.p, tmp_img.p, s));
@@ -214,7 +214,7 @@ pg_status SenseOp::forward(const float2* x, float2* y, cudaStream_t s) {
   if (inner->kind == PG_OP_GDFT)
     return gdft_forward(static_cast<GdftOp*>(inner)->plan.get(), (int)nc, S.p, x, y, n_data / nc, s);
   // generic (SENSE.cpp:59-70)
-  PG_TRY(tmp_img.alloc(n_image));
+  PG_TRY(grow(tmp_img, n_image, s));
   for (uint64_t c = 0; c < nc; ++c) {
     PG_LAUNCH(k_cmul, ceil_div(n_image, 256), 256, 0, s, n_image, S.p + c * n_image, x, 0, tmp_img.p);
     PG_TRY(inner->forward(tmp_img.p, y + c * (n_data / nc), s));
@@ -236,7 +236,7 @@ pg_status SenseOp::adjoint(const float2* y, float2* x, cudaStream_t s) {
   if (inner->kind == PG_OP_GDFT)
     return gdft_adjoint(static_cast<GdftOp*>(inner)->plan.get(), (int)nc, S.p, y, n_data / nc, x, s);
   // generic (SENSE.cpp:84-96)
-  PG_TRY(tmp_img.alloc(n_image));
+  PG_TRY(grow(tmp_img, n_image, s));
   for (uint64_t c = 0; c < nc; ++c) {
     PG_TRY(inner->adjoint(y + c * (n_data / nc), tmp_img.p, s));
     PG_LAUNCH(k_cmul_acc, ceil_div(n_image, 256), 256, 0, s, n_image, tmp_img.p, S.p + c * n_image, 1,
@@ -282,6 +282,67 @@ static pg_status make_binning_for(NufftPlan* plan, const TsTables& tab, std::uni
   return nufft_build_binning(plan, tab.L, tab.K, tab.l0.data(), tab.aa_win.data(), out, s);
 }
 
+pg_status make_gnufft(std::unique_ptr<GnufftOp>* out, uint64_t data_length, float gridos, uint64_t nx, uint64_t ny,
+                      uint64_t nz, const float* kx, const float* ky, const float* kz, cudaStream_t s) {
+  if (!kx || !ky) return set_error(PG_INVALID_ARG, "Gnufft: null argument");
+  if (nz > 1 && !kz) return set_error(PG_INVALID_ARG, "Gnufft: kz required for 3-D");
+  auto op = std::make_unique<GnufftOp>();
+  op->kind = PG_OP_GNUFFT;
+  PG_TRY(nufft_plan_create(&op->plan, data_length, gridos, (int)nx, (int)ny, (int)nz, kx, ky, kz, s));
+  op->n_data = data_length;
+  op->n_image = nx * ny * nz;
+  *out = std::move(op);
+  return PG_OK;
+}
+
+pg_status make_timeseg(std::unique_ptr<TimeSegOp>* out, pg_op_s* G, const float* field_map, const float* tvec,
+                       uint64_t n1, uint64_t n2, uint64_t L, uint64_t interptype, uint64_t shots, cudaStream_t s) {
+  if (!G || !field_map || !tvec) return set_error(PG_INVALID_ARG, "TimeSegmentation: null argument");
+  if (G->n_data != n1 || G->n_image != n2)
+    return set_error(PG_INVALID_ARG, "TimeSegmentation: sizes (%llu, %llu) do not match the inner operator (%llu, %llu)",
+                     (unsigned long long)n1, (unsigned long long)n2, (unsigned long long)G->n_data,
+                     (unsigned long long)G->n_image);
+  auto op = std::make_unique<TimeSegOp>();
+  op->kind = PG_OP_TIMESEG;
+  op->inner = G;
+  op->n_data = n1;
+  op->n_image = n2;
+  PG_TRY(build_ts_tables(field_map, tvec, n1, n2, L, interptype, shots, &op->tab));
+  if (op->tab.L > 1) {
+    PG_TRY(op->Wo.upload(op->tab.Wo.data(), op->tab.Wo.size(), s));
+    PG_TRY(op->WoH.upload(op->tab.WoH.data(), op->tab.WoH.size(), s));
+    if (G->kind == PG_OP_GNUFFT) {
+      PG_TRY(make_binning_for(static_cast<GnufftOp*>(G)->plan.get(), op->tab, &op->bin, s));
+    } else {
+      PG_TRY(op->AAfull.upload(op->tab.AA.data(), op->tab.AA.size(), s));
+    }
+  }
+  PG_CUDA(cudaStreamSynchronize(s));
+  // host tables are only needed to build the device ones
+  op->tab.AA.clear(); op->tab.AA.shrink_to_fit();
+  op->tab.Wo.clear(); op->tab.Wo.shrink_to_fit();
+  op->tab.WoH.clear(); op->tab.WoH.shrink_to_fit();
+  *out = std::move(op);
+  return PG_OK;
+}
+
+pg_status make_sense(std::unique_ptr<SenseOp>* out, pg_op_s* G, const float* sense_map, uint64_t n1, uint64_t n2,
+                     uint64_t nc, cudaStream_t s) {
+  if (!G || !sense_map) return set_error(PG_INVALID_ARG, "SENSE: null argument");
+  if (nc == 0) return set_error(PG_INVALID_ARG, "SENSE: nc = 0");
+  if (G->n_data != n1 || G->n_image != n2) return set_error(PG_INVALID_ARG, "SENSE: sizes do not match the inner operator");
+  auto op = std::make_unique<SenseOp>();
+  op->kind = PG_OP_SENSE;
+  op->inner = G;
+  op->nc = nc;
+  op->n_data = n1 * nc;
+  op->n_image = n2;
+  PG_TRY(op->S.upload(reinterpret_cast<const float2*>(sense_map), n2 * nc, s));
+  PG_CUDA(cudaStreamSynchronize(s));
+  *out = std::move(op);
+  return PG_OK;
+}
+
 }  // namespace pg
 
 using namespace pg;
@@ -291,14 +352,10 @@ extern "C" {
 
 pg_status pg_gnufft_create(pg_op* out, uint64_t data_length, float gridos, uint64_t nx, uint64_t ny, uint64_t nz,
                            const float* kx, const float* ky, const float* kz) {
-  if (!out || !kx || !ky) return set_error(PG_INVALID_ARG, "Gnufft: null argument");
-  if (nz > 1 && !kz) return set_error(PG_INVALID_ARG, "Gnufft: kz required for 3-D");
+  if (!out) return set_error(PG_INVALID_ARG, "Gnufft: null argument");
   PG_TRY(ensure_init());
-  auto op = std::make_unique<GnufftOp>();
-  op->kind = PG_OP_GNUFFT;
-  PG_TRY(nufft_plan_create(&op->plan, data_length, gridos, (int)nx, (int)ny, (int)nz, kx, ky, kz, default_stream()));
-  op->n_data = data_length;
-  op->n_image = nx * ny * nz;
+  std::unique_ptr<GnufftOp> op;
+  PG_TRY(make_gnufft(&op, data_length, gridos, nx, ny, nz, kx, ky, kz, default_stream()));
   *out = op.release();
   return PG_OK;
 }
@@ -319,47 +376,19 @@ pg_status pg_gdft_create(pg_op* out, uint64_t nk, uint64_t ni, const float* kx, 
 
 pg_status pg_timeseg_create(pg_op* out, pg_op G, const float* field_map, const float* tvec, uint64_t n1, uint64_t n2,
                             uint64_t L, uint64_t interptype, uint64_t shots) {
-  if (!out || !G || !field_map || !tvec) return set_error(PG_INVALID_ARG, "TimeSegmentation: null argument");
+  if (!out) return set_error(PG_INVALID_ARG, "TimeSegmentation: null argument");
   PG_TRY(ensure_init());
-  if (G->n_data != n1 || G->n_image != n2)
-    return set_error(PG_INVALID_ARG, "TimeSegmentation: sizes (%llu, %llu) do not match the inner operator (%llu, %llu)",
-                     (unsigned long long)n1, (unsigned long long)n2, (unsigned long long)G->n_data,
-                     (unsigned long long)G->n_image);
-  auto op = std::make_unique<TimeSegOp>();
-  op->kind = PG_OP_TIMESEG;
-  op->inner = G;
-  op->n_data = n1;
-  op->n_image = n2;
-  PG_TRY(build_ts_tables(field_map, tvec, n1, n2, L, interptype, shots, &op->tab));
-  cudaStream_t s = default_stream();
-  if (op->tab.L > 1) {
-    PG_TRY(op->Wo.upload(op->tab.Wo.data(), op->tab.Wo.size(), s));
-    PG_TRY(op->WoH.upload(op->tab.WoH.data(), op->tab.WoH.size(), s));
-    if (G->kind == PG_OP_GNUFFT) {
-      PG_TRY(make_binning_for(static_cast<GnufftOp*>(G)->plan.get(), op->tab, &op->bin, s));
-    } else {
-      PG_TRY(op->AAfull.upload(op->tab.AA.data(), op->tab.AA.size(), s));
-    }
-  }
-  PG_CUDA(cudaStreamSynchronize(s));
+  std::unique_ptr<TimeSegOp> op;
+  PG_TRY(make_timeseg(&op, G, field_map, tvec, n1, n2, L, interptype, shots, default_stream()));
   *out = op.release();
   return PG_OK;
 }
 
 pg_status pg_sense_create(pg_op* out, pg_op G, const float* sense_map, uint64_t n1, uint64_t n2, uint64_t nc) {
-  if (!out || !G || !sense_map) return set_error(PG_INVALID_ARG, "SENSE: null argument");
+  if (!out) return set_error(PG_INVALID_ARG, "SENSE: null argument");
   PG_TRY(ensure_init());
-  if (nc == 0) return set_error(PG_INVALID_ARG, "SENSE: nc = 0");
-  if (G->n_data != n1 || G->n_image != n2)
-    return set_error(PG_INVALID_ARG, "SENSE: sizes do not match the inner operator");
-  auto op = std::make_unique<SenseOp>();
-  op->kind = PG_OP_SENSE;
-  op->inner = G;
-  op->nc = nc;
-  op->n_data = n1 * nc;
-  op->n_image = n2;
-  PG_TRY(op->S.upload(reinterpret_cast<const float2*>(sense_map), n2 * nc, default_stream()));
-  PG_CUDA(cudaStreamSynchronize(default_stream()));
+  std::unique_ptr<SenseOp> op;
+  PG_TRY(make_sense(&op, G, sense_map, n1, n2, nc, default_stream()));
   *out = op.release();
   return PG_OK;
 }
@@ -416,7 +445,8 @@ pg_status pg_pcsense_timeseg_create(pg_op* out, const float* kx, const float* ky
 
 pg_status pg_op_destroy(pg_op op) {
   if (!op) return PG_OK;
-  cudaStreamSynchronize(default_stream());
+  // the operator may have been used on any stream; its buffers must be idle
+  cudaDeviceSynchronize();
   delete op;
   return PG_OK;
 }
@@ -480,7 +510,10 @@ uint64_t pg_util_kb_lut(float gridos, float* lut_out, uint64_t cap, float* beta_
 pg_status pg_util_gnufft_binning(pg_op G, uint32_t* keys_out, uint32_t* perm_out, uint64_t* n_bins_out) {
   if (!G) return set_error(PG_INVALID_ARG, "null operator");
   const Binning* b = nullptr;
-  if (G->kind == PG_OP_GNUFFT) b = static_cast<GnufftOp*>(G)->plan->plain.get();
+  if (G->kind == PG_OP_GNUFFT) {
+    PG_TRY(nufft_plain_binning(static_cast<GnufftOp*>(G)->plan.get(), default_stream()));
+    b = static_cast<GnufftOp*>(G)->plan->plain.get();
+  }
   else if (G->kind == PG_OP_TIMESEG && static_cast<TimeSegOp*>(G)->bin) b = static_cast<TimeSegOp*>(G)->bin.get();
   if (!b) return set_error(PG_INVALID_ARG, "operator has no sample binning");
   if (keys_out) std::memcpy(keys_out, b->h_keys.data(), b->h_keys.size() * sizeof(uint32_t));

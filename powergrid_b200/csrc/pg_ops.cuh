@@ -1,6 +1,7 @@
 // Operator objects behind the pg_op handle.
 #pragma once
 
+#include <atomic>
 #include <memory>
 #include <vector>
 
@@ -9,8 +10,15 @@
 
 enum pg_op_kind { PG_OP_GNUFFT = 1, PG_OP_GDFT = 2, PG_OP_TIMESEG = 3, PG_OP_SENSE = 4, PG_OP_PCSENSE_TS = 5 };
 
+// Per-operator PWLS-PCG state kept between solves (buffers + the captured
+// per-iteration graph), defined in pg_pcg.cu.
+struct pg_pcg_cache_base {
+  virtual ~pg_pcg_cache_base() {}
+};
+
 struct pg_op_s {
   int kind = 0;
+  std::unique_ptr<pg_pcg_cache_base> pcg_cache;
   uint64_t n_data = 0, n_image = 0;
   // staging for the host-buffer entry points
   pg::DevBuf<float2> hx, hy;
@@ -80,5 +88,16 @@ struct PcSenseTsOp : pg_op_s {
   pg_status adjoint(const float2* y, float2* x, cudaStream_t s) override;
   uint64_t resident_bytes() const override;
 };
+
+pg_status make_gnufft(std::unique_ptr<GnufftOp>* out, uint64_t data_length, float gridos, uint64_t nx, uint64_t ny,
+                      uint64_t nz, const float* kx, const float* ky, const float* kz, cudaStream_t s);
+pg_status make_timeseg(std::unique_ptr<TimeSegOp>* out, pg_op_s* G, const float* field_map, const float* tvec,
+                       uint64_t n1, uint64_t n2, uint64_t L, uint64_t interptype, uint64_t shots, cudaStream_t s);
+pg_status make_sense(std::unique_ptr<SenseOp>* out, pg_op_s* G, const float* sense_map, uint64_t n1, uint64_t n2,
+                     uint64_t nc, cudaStream_t s);
+// Device PWLS-PCG (pg_pcg.cu).  cancel (may be null) is polled between iterations.
+pg_status pcg_solve_device(pg_op_s* A, const float2* x0, const float* W, const float2* y, const pg_penalty& R,
+                           uint64_t niter, float2* xout, uint32_t* iters_dev, cudaStream_t s,
+                           const std::atomic<bool>* cancel = nullptr);
 
 }  // namespace pg

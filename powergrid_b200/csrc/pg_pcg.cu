@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "pg_ops.cuh"
+#include "pg_profile.cuh"
 
 namespace pg {
 
@@ -340,21 +341,39 @@ bool graphs_enabled() {
 
 }  // namespace
 
-pg_status pcg_solve_device(pg_op A, const float2* x0, const float* W, const float2* y, const pg_penalty& Rh,
-                           uint64_t niter, float2* xout, uint32_t* iters_dev, cudaStream_t s) {
+namespace {
+
+// Solver buffers and the instantiated per-iteration graph, cached on the
+// operator.  The graph reads y and W from ybuf / wbuf, so a new solve only
+// copies its inputs there and replays the graph.
+struct PcgCache : pg_pcg_cache_base {
   Solver S;
+  DevBuf<float2> ybuf;
+  DevBuf<float> wbuf;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint64_t per_iter = 0;
+  pg_penalty R{};
+  bool prof = false;
+  bool w_ones = true;
+  ~PcgCache() override {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+  }
+  bool matches(const pg_penalty& r, bool ones) const {
+    return R.kind == r.kind && R.nx == r.nx && R.ny == r.ny && R.nz == r.nz && R.beta == r.beta &&
+           R.delta == r.delta && R.dims2penalize == r.dims2penalize && prof == g_profile && w_ones == ones;
+  }
+};
+
+pg_status make_cache(pg_op_s* A, const pg_penalty& Rh, bool w_ones, std::unique_ptr<PcgCache>* out, cudaStream_t s) {
+  auto c = std::make_unique<PcgCache>();
+  Solver& S = c->S;
   S.A = A;
   S.nd = A->n_data;
   S.ni = A->n_image;
-  if (Rh.nx * Rh.ny * Rh.nz != S.ni)
-    return set_error(PG_INVALID_ARG, "penalty size %llux%llux%llu does not match the image length %llu",
-                     (unsigned long long)Rh.nx, (unsigned long long)Rh.ny, (unsigned long long)Rh.nz,
-                     (unsigned long long)S.ni);
-  if (Rh.kind != PG_PENALTY_QUAD && Rh.kind != PG_PENALTY_TV) return set_error(PG_INVALID_ARG, "unknown penalty");
-  if (Rh.kind == PG_PENALTY_TV && !(Rh.delta > 0)) return set_error(PG_INVALID_ARG, "TV penalty needs delta > 0");
   S.R = make_pen(Rh);
   S.beta = Rh.beta;
-  S.y = y;
   S.nbd = red_blocks(S.nd);
   S.nbi = red_blocks(S.ni);
   const int nb = std::max(S.nbd, S.nbi);
@@ -367,57 +386,104 @@ pg_status pcg_solve_device(pg_op A, const float2* x0, const float* W, const floa
   PG_TRY(S.part.alloc(2 * (uint64_t)nb));
   PG_TRY(S.sc.alloc(S_NSCAL));
   PG_TRY(S.fl.alloc(F_NFLAG));
-  if (!W) {
-    PG_TRY(S.Wones.alloc(S.nd));
-    PG_LAUNCH(k_fill_ones, ceil_div(S.nd, 256), 256, 0, s, S.nd, S.Wones.p);
-    S.W = S.Wones.p;
-  } else {
-    S.W = W;
+  PG_TRY(c->ybuf.alloc(S.nd));
+  PG_TRY(c->wbuf.alloc(S.nd));
+  if (w_ones) PG_LAUNCH(k_fill_ones, ceil_div(S.nd, 256), 256, 0, s, S.nd, c->wbuf.p);
+  S.y = c->ybuf.p;
+  S.W = c->wbuf.p;
+  c->R = Rh;
+  c->prof = g_profile;
+  c->w_ones = w_ones;
+  *out = std::move(c);
+  return PG_OK;
+}
+
+}  // namespace
+
+pg_status pcg_solve_device(pg_op_s* A, const float2* x0, const float* W, const float2* y, const pg_penalty& Rh,
+                           uint64_t niter, float2* xout, uint32_t* iters_dev, cudaStream_t s,
+                           const std::atomic<bool>* cancel) {
+  const uint64_t ni = A->n_image, nd = A->n_data;
+  if (Rh.nx * Rh.ny * Rh.nz != ni)
+    return set_error(PG_INVALID_ARG, "penalty size %llux%llux%llu does not match the image length %llu",
+                     (unsigned long long)Rh.nx, (unsigned long long)Rh.ny, (unsigned long long)Rh.nz,
+                     (unsigned long long)ni);
+  if (Rh.kind != PG_PENALTY_QUAD && Rh.kind != PG_PENALTY_TV) return set_error(PG_INVALID_ARG, "unknown penalty");
+  if (Rh.kind == PG_PENALTY_TV && !(Rh.delta > 0)) return set_error(PG_INVALID_ARG, "TV penalty needs delta > 0");
+
+  auto* cache = dynamic_cast<PcgCache*>(A->pcg_cache.get());
+  if (!cache || !cache->matches(Rh, W == nullptr)) {
+    A->pcg_cache.reset();
+    std::unique_ptr<PcgCache> c;
+    PG_TRY(make_cache(A, Rh, W == nullptr, &c, s));
+    cache = c.get();
+    A->pcg_cache = std::move(c);
   }
-  if (x0) PG_CUDA(cudaMemcpyAsync(S.x.p, x0, S.ni * sizeof(float2), cudaMemcpyDeviceToDevice, s));
-  else PG_CUDA(cudaMemsetAsync(S.x.p, 0, S.ni * sizeof(float2), s));
-  PG_CUDA(cudaMemsetAsync(S.ddir.p, 0, S.ni * sizeof(float2), s));
+  Solver& S = cache->S;
+  // inputs into the buffers the graph reads
+  PG_CUDA(cudaMemcpyAsync(cache->ybuf.p, y, nd * sizeof(float2), cudaMemcpyDeviceToDevice, s));
+  if (W) PG_CUDA(cudaMemcpyAsync(cache->wbuf.p, W, nd * sizeof(float), cudaMemcpyDeviceToDevice, s));
+  if (x0) PG_CUDA(cudaMemcpyAsync(S.x.p, x0, ni * sizeof(float2), cudaMemcpyDeviceToDevice, s));
+  else PG_CUDA(cudaMemsetAsync(S.x.p, 0, ni * sizeof(float2), s));
+  PG_CUDA(cudaMemsetAsync(S.ddir.p, 0, ni * sizeof(float2), s));
   // Ax = A * xInitial (:55)
-  PG_TRY(A->forward(S.x.p, S.Ax.p, s));
-  PG_LAUNCH(k_ywy, (unsigned)S.nbd, kRed, 0, s, S.nd, y, S.W, S.part.p, S.nbd);
+  pg_status st = A->forward(S.x.p, S.Ax.p, s);
+  if (st != PG_OK) { A->pcg_cache.reset(); return st; }
+  PG_LAUNCH(k_ywy, (unsigned)S.nbd, kRed, 0, s, nd, S.y, S.W, S.part.p, S.nbd);
   PG_LAUNCH(k_scalar_init, 1, 32, 0, s, S.part.p, S.nbd, S.sc.p, S.fl.p);
 
-  if (niter > 0) {
+  uint64_t it = 0;
+  if (!cache->exec && niter > 0) {
     // first iteration eagerly: allocates every workspace the graph will use
-    PG_TRY(S.iteration(s));
-  }
-  if (niter > 1) {
-    if (graphs_enabled()) {
-      cudaGraph_t graph = nullptr;
-      cudaGraphExec_t exec = nullptr;
+    st = S.iteration(s);
+    if (st != PG_OK) { A->pcg_cache.reset(); return st; }
+    it = 1;
+    if (graphs_enabled() && niter > 1) {
       const uint64_t before = g_launches.load();
       PG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-      pg_status st = S.iteration(s);
+      st = S.iteration(s);
+      cudaGraph_t graph = nullptr;
       cudaError_t ce = cudaStreamEndCapture(s, &graph);
-      if (st != PG_OK) { if (graph) cudaGraphDestroy(graph); return st; }
-      if (ce != cudaSuccess) return set_error(PG_CUDA_ERROR, "graph capture: %s", cudaGetErrorString(ce));
-      const uint64_t per_iter = g_launches.load() - before;
-      ce = cudaGraphInstantiate(&exec, graph, 0);
-      if (ce != cudaSuccess) { cudaGraphDestroy(graph); return set_error(PG_CUDA_ERROR, "graph instantiate: %s", cudaGetErrorString(ce)); }
-      for (uint64_t it = 1; it < niter; ++it) {
-        ce = cudaGraphLaunch(exec, s);
-        if (ce != cudaSuccess) break;
-        // replays launch the captured kernels; the capture itself launched none
-        count_launch(per_iter);
-      }
       // the capture pass counted launches that never ran
-      g_launches.fetch_sub(per_iter);
-      cudaGraphExecDestroy(exec);
-      cudaGraphDestroy(graph);
-      if (ce != cudaSuccess) return set_error(PG_CUDA_ERROR, "graph launch: %s", cudaGetErrorString(ce));
-    } else {
-      for (uint64_t it = 1; it < niter; ++it) PG_TRY(S.iteration(s));
+      cache->per_iter = g_launches.load() - before;
+      g_launches.fetch_sub(cache->per_iter);
+      if (st != PG_OK || ce != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        A->pcg_cache.reset();
+        return st != PG_OK ? st : set_error(PG_CUDA_ERROR, "graph capture: %s", cudaGetErrorString(ce));
+      }
+      ce = cudaGraphInstantiate(&cache->exec, graph, 0);
+      if (ce != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        cudaGetLastError();
+        A->pcg_cache.reset();
+        return set_error(PG_CUDA_ERROR, "graph instantiate: %s", cudaGetErrorString(ce));
+      }
+      cache->graph = graph;
     }
   }
-  PG_CUDA(cudaMemcpyAsync(xout, S.x.p, S.ni * sizeof(float2), cudaMemcpyDeviceToDevice, s));
+  for (; it < niter; ++it) {
+    if (cancel && cancel->load()) break;
+    if (cache->exec) {
+      cudaError_t ce = cudaGraphLaunch(cache->exec, s);
+      if (ce != cudaSuccess) {
+        cudaGetLastError();
+        A->pcg_cache.reset();
+        return set_error(PG_CUDA_ERROR, "graph launch: %s", cudaGetErrorString(ce));
+      }
+      count_launch(cache->per_iter);
+    } else {
+      st = S.iteration(s);
+      if (st != PG_OK) { A->pcg_cache.reset(); return st; }
+    }
+  }
+  PG_CUDA(cudaMemcpyAsync(xout, S.x.p, ni * sizeof(float2), cudaMemcpyDeviceToDevice, s));
   if (iters_dev) PG_LAUNCH(k_copy_iters, 1, 1, 0, s, S.fl.p, iters_dev);
-  // buffers are freed on return; make sure the stream is done with them
-  PG_CUDA(cudaStreamSynchronize(s));
+  if (cancel && cancel->load()) {
+    PG_CUDA(cudaStreamSynchronize(s));
+    return set_error(PG_CANCELLED, "solve cancelled");
+  }
   return PG_OK;
 }
 
