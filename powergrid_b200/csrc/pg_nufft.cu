@@ -121,7 +121,11 @@ __device__ __forceinline__ int wrap(int v, int n) {
   return v < 0 ? v + n : v;
 }
 
-// Per-sample preparation (original order): tap starts, separable weights and bin key.
+// Per-sample preparation (original order): tap starts, weights and bin key.
+// The stored weights carry the +-1 checkerboard that replaces the shifts:
+// for even G, ifftshift(FFT(fftshift(u))) = c (-1)^k FFT((-1)^n u) with
+// c = prod_d (-1)^(G_d/2), so the gather and spread work on the unshifted
+// (centred) grid, where the reference's clamped windows never wrap.
 __global__ void k_prepare(NufftGeom g, uint64_t M, const float* __restrict__ kx, const float* __restrict__ ky,
                           const float* __restrict__ kz, const float* __restrict__ lut, TileShape t,
                           const int* __restrict__ l0, uint2* __restrict__ start, float* __restrict__ wxy,
@@ -129,17 +133,18 @@ __global__ void k_prepare(NufftGeom g, uint64_t M, const float* __restrict__ kx,
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= M) return;
   float w[8];
+  const float c = g.sign_c;
   const int sx = axis_taps(kx[i], g.Nx, g.os, g.kw, lut, g.nlut, w);
 #pragma unroll
-  for (int a = 0; a < 8; ++a) wxy[i * 16 + a] = w[a];
+  for (int a = 0; a < 8; ++a) wxy[i * 16 + a] = ((sx + a) & 1) ? -c * w[a] : c * w[a];
   const int sy = axis_taps(ky[i], g.Ny, g.os, g.kw, lut, g.nlut, w);
 #pragma unroll
-  for (int a = 0; a < 8; ++a) wxy[i * 16 + 8 + a] = w[a];
+  for (int a = 0; a < 8; ++a) wxy[i * 16 + 8 + a] = ((sy + a) & 1) ? -w[a] : w[a];
   int sz = 0;
   if (g.dim == 3) {
     sz = axis_taps(kz[i], g.Nz, g.os, g.kw, lut, g.nlut, w);
 #pragma unroll
-    for (int a = 0; a < 8; ++a) wz[i * 8 + a] = w[a];
+    for (int a = 0; a < 8; ++a) wz[i * 8 + a] = ((sz + a) & 1) ? -w[a] : w[a];
   }
   start[i] = make_uint2((uint32_t)sx | ((uint32_t)sy << 16), (uint32_t)sz);
   const int tx = sx / t.TX, ty = sy / t.TY, tz = sz / t.TZ;
@@ -167,8 +172,11 @@ __global__ void k_permute(uint64_t M, int dim, int K, const uint32_t* __restrict
   }
 }
 
+__device__ __forceinline__ int parity3(int a, int b, int c) { return (a + b + c) & 1; }
+
 // ---------------------------------------------------------------------------
-// Forward: pre-kernel (deapodize + maps + phases + zero-pad + fftshift)
+// Forward pre-kernel: deapodize, coil map, shot phase, segment phase and
+// zero-pad into the centred grid, times the (-1)^(x+y+z) checkerboard.
 // ---------------------------------------------------------------------------
 __global__ void k_pre(NufftGeom g, int L, const float2* __restrict__ x, const float2* __restrict__ S, int c0,
                       const float2* __restrict__ E, const float2* __restrict__ Wo, const float* __restrict__ deap,
@@ -178,12 +186,12 @@ __global__ void k_pre(NufftGeom g, int L, const float2* __restrict__ x, const fl
   if (q >= G) return;
   const int b = blockIdx.y;           // grid within the batch
   const int cl = b / L, l = b % L;
-  const int fy = (int)(q % g.Gy);
-  const int fx = (int)((q / g.Gy) % g.Gx);
-  const int fz = (int)(q / ((uint64_t)g.Gy * g.Gx));
-  const int iy = wrap(fy - g.fs[1], g.Gy) - g.pad_off[1];
-  const int ix = wrap(fx - g.fs[0], g.Gx) - g.pad_off[0];
-  const int iz = (g.dim == 3) ? wrap(fz - g.fs[2], g.Gz) - g.pad_off[2] : 0;
+  const int my = (int)(q % g.Gy);
+  const int mx = (int)((q / g.Gy) % g.Gx);
+  const int mz = (int)(q / ((uint64_t)g.Gy * g.Gx));
+  const int iy = my - g.pad_off[1];
+  const int ix = mx - g.pad_off[0];
+  const int iz = (g.dim == 3) ? mz - g.pad_off[2] : 0;
   float2 v = make_float2(0.f, 0.f);
   if (iy >= 0 && iy < g.Ny && ix >= 0 && ix < g.Nx && iz >= 0 && iz < g.Nz) {
     const uint64_t N = g.nimg();
@@ -198,98 +206,199 @@ __global__ void k_pre(NufftGeom g, int L, const float2* __restrict__ x, const fl
     if (g.dim == 3) k = k * deap[g.Nx + g.Ny + iz];
     v = (k == k) ? make_float2(__fmul_rn(__fdiv_rn(v.x, k), scale), __fmul_rn(__fdiv_rn(v.y, k), scale))
                  : make_float2(0.f, 0.f);
+    if (parity3(mx, my, mz)) v = make_float2(-v.x, -v.y);
   }
   grids[(uint64_t)b * G + q] = v;
 }
 
 // ---------------------------------------------------------------------------
-// Forward: interpolation (gather) with ifftshift folded into the reads and
-// the segment interpolator applied per sample.  One thread per sample.
+// Warp butterfly reduce-scatter of V = 2^p floats per lane: afterwards lane L
+// holds the warp-wide sum of value index (L >> (5 - p)) & (V - 1).
 // ---------------------------------------------------------------------------
-template <int DIM>
-__global__ void __launch_bounds__(128) k_gather(NufftGeom g, uint64_t M, const uint2* __restrict__ start,
-                                                const float* __restrict__ wxy, const float* __restrict__ wz,
-                                                const uint32_t* __restrict__ perm, const int* __restrict__ l0,
+template <int V>
+__device__ __forceinline__ float warp_reduce_scatter(float (&v)[V], int lane) {
+  int n = V;
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) {
+    if (n > 1) {
+      const bool upper = (lane & o) != 0;
+#pragma unroll
+      for (int i = 0; i < V / 2; ++i) {
+        if (i < n / 2) {
+          const float send = upper ? v[i] : v[i + n / 2];
+          const float keep = upper ? v[i + n / 2] : v[i];
+          v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+      }
+      n >>= 1;
+    } else {
+      v[0] += __shfl_xor_sync(0xffffffffu, v[0], o);
+    }
+  }
+  return v[0];
+}
+
+template <int V>
+__host__ __device__ constexpr int log2c() {
+  return V <= 1 ? 0 : V <= 2 ? 1 : V <= 4 ? 2 : V <= 8 ? 3 : V <= 16 ? 4 : 5;
+}
+
+// ---------------------------------------------------------------------------
+// Forward interpolation, tiled: one block per (subproblem, coil chunk).
+// The padded tiles of the subproblem's KP segment grids for CC coils are
+// staged in shared memory ([c][j][re|im][PZ][PX][PY], PY = 8 mod 32).  A
+// warp interpolates 4 samples at a time: lane = (y-tap, sample), each lane
+// walks its sample's 8 x-taps (x 8 z-taps in 3-D) for every (coil, segment)
+// plane, then the 8 lanes of a sample combine their partial sums with a
+// 3-level butterfly and the segment interpolator AA is applied per coil.
+// ---------------------------------------------------------------------------
+template <int V>
+__device__ __forceinline__ void group8_reduce_scatter(float (&v)[V], int lane) {
+  int n = V;
+#pragma unroll
+  for (int o = 4; o >= 1; o >>= 1) {
+    if (n > 1) {
+      const bool upper = (lane & o) != 0;
+#pragma unroll
+      for (int i = 0; i < V / 2; ++i) {
+        if (i < n / 2) {
+          const float send = upper ? v[i] : v[i + n / 2];
+          const float keep = upper ? v[i + n / 2] : v[i];
+          v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+      }
+      n >>= 1;
+    } else {
+      v[0] += __shfl_xor_sync(0xffffffffu, v[0], o);
+    }
+  }
+}
+
+template <int DIM, int CC, int KP>
+__global__ void __launch_bounds__(256) k_gather(NufftGeom g, TileShape t, const int4* __restrict__ sub,
+                                                const uint2* __restrict__ start, const float* __restrict__ wxy,
+                                                const float* __restrict__ wz, const uint32_t* __restrict__ perm,
                                                 const float2* __restrict__ aa, int K, int L,
                                                 const float2* __restrict__ grids, int Cb,
                                                 float2* __restrict__ data, uint64_t dstride) {
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= M) return;
-  const uint2 st = start[i];
-  const int sx = st.x & 0xffff, sy = st.x >> 16, sz = st.y;
-  float wx[8], wy[8], wzz[8];
-  {
-    const float4* w4 = reinterpret_cast<const float4*>(wxy + i * 16);
-    float4 a = w4[0], b = w4[1], c = w4[2], d = w4[3];
-    wx[0] = a.x; wx[1] = a.y; wx[2] = a.z; wx[3] = a.w; wx[4] = b.x; wx[5] = b.y; wx[6] = b.z; wx[7] = b.w;
-    wy[0] = c.x; wy[1] = c.y; wy[2] = c.z; wy[3] = c.w; wy[4] = d.x; wy[5] = d.y; wy[6] = d.z; wy[7] = d.w;
-    if (DIM == 3) {
-      const float4* z4 = reinterpret_cast<const float4*>(wz + i * 8);
-      float4 e = z4[0], f = z4[1];
-      wzz[0] = e.x; wzz[1] = e.y; wzz[2] = e.z; wzz[3] = e.w; wzz[4] = f.x; wzz[5] = f.y; wzz[6] = f.z; wzz[7] = f.w;
-    }
-  }
-  int py[8], px[8], pz[8];
-#pragma unroll
-  for (int a = 0; a < 8; ++a) {
-    py[a] = wrap(sy + a - g.ifs[1], g.Gy);
-    px[a] = wrap(sx + a - g.ifs[0], g.Gx) * g.Gy;
-    if (DIM == 3) pz[a] = wrap(sz + a - g.ifs[2], g.Gz) * g.Gx * g.Gy;
-  }
+  constexpr int V = 2 * CC * KP;                 // accumulators per sample
+  constexpr int PER = (V >= 8) ? V / 8 : 1;      // values a lane holds after the group butterfly
+  extern __shared__ float sm[];
+  __shared__ float red[8][4][V];
+  const int4 sp = sub[blockIdx.x];
+  const int cfirst = blockIdx.y * CC;
+  const int ncl = min(CC, Cb - cfirst);
+  const int tile = sp.x, lseg = sp.y, first = sp.z, count = sp.w;
+  const int ty = tile % t.nty;
+  const int txz = tile / t.nty;
+  const int tx = txz % t.ntx;
+  const int tz = txz / t.ntx;
+  const int x0 = tx * t.TX, y0 = ty * t.TY, z0 = tz * t.TZ;
+  const int cells = t.PX * t.PY * t.PZ;
   const uint64_t G = g.ngrid();
-  const int lbase = l0 ? l0[i] : 0;
-  const uint32_t orig = perm[i];
-  for (int c = 0; c < Cb; ++c) {
-    float2 out = make_float2(0.f, 0.f);
-    for (int j = 0; j < K; ++j) {
-      const float2* gr = grids + ((uint64_t)c * L + lbase + j) * G;
-      float ar = 0.f, ai = 0.f;
+  for (int q = threadIdx.x; q < cells; q += blockDim.x) {
+    const int pyy = q % t.PY;
+    const int pxx = (q / t.PY) % t.PX;
+    const int pzz = q / (t.PY * t.PX);
+    const int gy = y0 + pyy, gx = x0 + pxx, gz = z0 + pzz;
+    const bool in = gy < g.Gy && gx < g.Gx && gz < g.Gz;
+    const uint64_t idx = (uint64_t)gy + (uint64_t)g.Gy * ((uint64_t)gx + (uint64_t)g.Gx * gz);
+#pragma unroll
+    for (int c = 0; c < CC; ++c)
+#pragma unroll
+      for (int j = 0; j < KP; ++j) {
+        float2 v = make_float2(0.f, 0.f);
+        if (in && c < ncl && j < K) v = grids[((uint64_t)(cfirst + c) * L + lseg + j) * G + idx];
+        float* pr = sm + ((c * KP + j) * 2) * cells;
+        pr[q] = v.x;
+        pr[cells + q] = v.y;
+      }
+  }
+  __syncthreads();
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int dy = lane & 7, grp = lane >> 3;
+  const int plane = t.PX * t.PY;
+  const int end = first + count;
+  for (int s0 = first + 4 * warp; s0 < end; s0 += 4 * nw) {
+    const int s = s0 + grp;
+    float acc[V];
+#pragma unroll
+    for (int i = 0; i < V; ++i) acc[i] = 0.f;
+    if (s < end) {
+      const uint2 st = start[s];
+      const int ox = (int)(st.x & 0xffff) - x0, oy = (int)(st.x >> 16) - y0;
+      const float* w = wxy + (uint64_t)s * 16;
+      const float wyv = w[8 + dy];
       if (DIM == 2) {
 #pragma unroll
-        for (int a = 0; a < 8; ++a) {
-          if (wx[a] == 0.f) continue;
-          const float2* row = gr + px[a];
+        for (int r = 0; r < 8; ++r) {
+          const float wr = w[r] * wyv;
+          const int a = (ox + r) * t.PY + oy + dy;
 #pragma unroll
-          for (int b = 0; b < 8; ++b) {
-            if (wy[b] == 0.f) continue;
-            const float w = wx[a] * wy[b];
-            const float2 v = __ldg(row + py[b]);
-            ar = fmaf(w, v.x, ar);
-            ai = fmaf(w, v.y, ai);
+          for (int cj = 0; cj < CC * KP; ++cj) {
+            const float* pr = sm + (cj * 2) * cells;
+            acc[2 * cj] = fmaf(wr, pr[a], acc[2 * cj]);
+            acc[2 * cj + 1] = fmaf(wr, pr[cells + a], acc[2 * cj + 1]);
           }
         }
       } else {
+        const int oz = (int)st.y - z0;
+        const float* wzz = wz + (uint64_t)s * 8;
         for (int e = 0; e < 8; ++e) {
-          if (wzz[e] == 0.f) continue;
-          const float2* pl = gr + pz[e];
+          const float wze = wzz[e];
+          const int zo = (oz + e) * plane;
 #pragma unroll
-          for (int a = 0; a < 8; ++a) {
-            if (wx[a] == 0.f) continue;
-            const float2* row = pl + px[a];
+          for (int r = 0; r < 8; ++r) {
+            const float wr = w[r] * wyv * wze;
+            const int a = zo + (ox + r) * t.PY + oy + dy;
 #pragma unroll
-            for (int b = 0; b < 8; ++b) {
-              if (wy[b] == 0.f) continue;
-              const float w = wx[a] * wy[b] * wzz[e];
-              const float2 v = __ldg(row + py[b]);
-              ar = fmaf(w, v.x, ar);
-              ai = fmaf(w, v.y, ai);
+            for (int cj = 0; cj < CC * KP; ++cj) {
+              const float* pr = sm + (cj * 2) * cells;
+              acc[2 * cj] = fmaf(wr, pr[a], acc[2 * cj]);
+              acc[2 * cj + 1] = fmaf(wr, pr[cells + a], acc[2 * cj + 1]);
             }
           }
         }
       }
-      const float2 acc = make_float2(ar, ai);
-      out = aa ? cadd(out, cmul(acc, aa[i * K + j])) : acc;
     }
-    data[(uint64_t)c * dstride + orig] = out;
+    group8_reduce_scatter<V>(acc, lane);
+    // lane dy of a group now holds values [PER*dy', PER*dy'+PER) (dy' = dy for
+    // V >= 8; for V < 8 the low lanes hold the V values)
+    if (V >= 8) {
+#pragma unroll
+      for (int i = 0; i < PER; ++i) red[warp][grp][PER * dy + i] = acc[i];
+    } else {
+      constexpr int sh = (V >= 8) ? 0 : 3 - log2c<V>();
+      if ((dy & ((1 << sh) - 1)) == 0) red[warp][grp][(dy >> sh) & (V - 1)] = acc[0];
+    }
+    __syncwarp();
+    const int og = lane >> 3, oc = lane & 7;
+    const int so = s0 + og;
+    if (oc < ncl && so < end) {
+      float2 out = make_float2(0.f, 0.f);
+      for (int j = 0; j < K; ++j) {
+        const float2 a = make_float2(red[warp][og][2 * (oc * KP + j)], red[warp][og][2 * (oc * KP + j) + 1]);
+        out = aa ? cadd(out, cmul(a, aa[(uint64_t)so * K + j])) : a;
+      }
+      data[(uint64_t)(cfirst + oc) * dstride + perm[so]] = out;
+    }
+    __syncwarp();
   }
 }
 
 // ---------------------------------------------------------------------------
-// Adjoint: spread one subproblem (a bin's samples, one segment window) into
-// a padded shared-memory tile with shared atomics; flush each nonzero tile
-// cell to the ifftshifted grid position with one vector atomic.
-// Shared layout: [coil][segment][re|im][PZ][PX][PY], PY = 8 (mod 32) so a
-// warp's 32 lanes (8 y-taps x 4 x-taps) hit 32 distinct banks.
+// Adjoint spread: one block per (subproblem, coil chunk) into a padded
+// shared-memory tile, then each nonzero tile cell is flushed to the centred
+// grid with one vector atomic.  Shared accumulation is 32-bit fixed point
+// with native integer atomics (float shared atomics are compare-and-swap
+// loops): each (coil, segment) plane gets a power-of-two scale 2^e from the
+// bound B = wmax^d * sum_s |v_s| (|v| <= |re| + |im|) on any cell's
+// magnitude, with 2^30 headroom, so no partial sum can overflow and the
+// tile sums do not depend on the order of the atomics.  The quantisation
+// step is <= B / 2^29 per contribution.
+// Layout [coil][segment][re|im][PZ][PX][PY], PY = 8 (mod 32): a warp's 32
+// lanes (8 y-taps x 4 x-taps) hit 32 distinct banks.
 // ---------------------------------------------------------------------------
 template <int DIM>
 __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const int4* __restrict__ sub,
@@ -297,10 +406,12 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
                                                 const float* __restrict__ wz, const uint32_t* __restrict__ perm,
                                                 const float2* __restrict__ aa, int K, int L,
                                                 const float2* __restrict__ data, uint64_t dstride, int Cb,
-                                                int Cc, float2* __restrict__ grids) {
-  extern __shared__ float sm[];
+                                                int Cc, float wmax, float2* __restrict__ grids) {
+  extern __shared__ int smi[];
+  __shared__ float bound[16];
+  __shared__ float scale[16], inv_scale[16];
   const int4 sp = sub[blockIdx.x];
-  const int cfirst = blockIdx.y * Cc;            // first coil (within batch) of this block
+  const int cfirst = blockIdx.y * Cc;
   const int ncl = min(Cc, Cb - cfirst);
   const int tile = sp.x, lseg = sp.y, first = sp.z, count = sp.w;
   const int ty = tile % t.nty;
@@ -309,12 +420,52 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
   const int tz = txz / t.ntx;
   const int x0 = tx * t.TX, y0 = ty * t.TY, z0 = tz * t.TZ;
   const int cells = t.PX * t.PY * t.PZ;
-  const int nplanes = ncl * K * 2;
-  for (int q = threadIdx.x; q < nplanes * cells; q += blockDim.x) sm[q] = 0.f;
+  const int nplane = ncl * K;          // complex planes in use (<= 16)
+  for (int q = threadIdx.x; q < nplane * 2 * cells; q += blockDim.x) smi[q] = 0;
+  if (threadIdx.x < 16) bound[threadIdx.x] = 0.f;
+  __syncthreads();
+
+  // per-plane bound: sum over the subproblem's samples of |v| (<= |re|+|im|)
+  {
+    float loc[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) loc[i] = 0.f;
+    for (int s = first + threadIdx.x; s < first + count; s += blockDim.x) {
+      const uint32_t orig = perm[s];
+      for (int c = 0; c < ncl; ++c) {
+        const float2 d = data[(uint64_t)(cfirst + c) * dstride + orig];
+        const float m = fabsf(d.x) + fabsf(d.y);
+        for (int j = 0; j < K; ++j) {
+          const float2 a = aa ? aa[(uint64_t)s * K + j] : make_float2(1.f, 0.f);
+          loc[c * K + j] += m * (fabsf(a.x) + fabsf(a.y));
+        }
+      }
+    }
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      float v = loc[i];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0 && i < nplane && v > 0.f) atomicAdd(&bound[i], v);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 16) {
+    const float B = bound[threadIdx.x] * wmax * 1.0001f;
+    int e = 0;
+    if (B > 0.f) {
+      frexpf(B, &e);                       // B < 2^e
+      e = 30 - e;                          // B * 2^e' < 2^30
+    }
+    scale[threadIdx.x] = ldexpf(1.f, e);
+    inv_scale[threadIdx.x] = ldexpf(1.f, -e);
+  }
   __syncthreads();
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int dy = lane & 7, dx = lane >> 3;
+  const int plane = t.PX * t.PY;
   for (int s = first + warp; s < first + count; s += nw) {
     const uint2 st = start[s];
     const int ox = (int)(st.x & 0xffff) - x0, oy = (int)(st.x >> 16) - y0;
@@ -328,23 +479,31 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
     for (int c = 0; c < ncl; ++c) {
       const float2 d = data[(uint64_t)(cfirst + c) * dstride + orig];
       for (int j = 0; j < K; ++j) {
-        const float2 v = aa ? cmul(cconj(aa[(uint64_t)s * K + j]), d) : d;
-        float* pr = sm + ((c * K + j) * 2) * cells;
-        float* pi = pr + cells;
+        const int pl = c * K + j;
+        const float sc = scale[pl];
+        float2 v = aa ? cmul(cconj(aa[(uint64_t)s * K + j]), d) : d;
+        v = make_float2(v.x * sc, v.y * sc);
+        int* pr = smi + (pl * 2) * cells;
+        int* pi = pr + cells;
         if (DIM == 2) {
           const float w0 = wx0 * wyv, w1 = wx1 * wyv;
-          if (w0 != 0.f) { atomicAdd(pr + a0, w0 * v.x); atomicAdd(pi + a0, w0 * v.y); }
-          if (w1 != 0.f) { atomicAdd(pr + a1, w1 * v.x); atomicAdd(pi + a1, w1 * v.y); }
+          if (w0 != 0.f) { atomicAdd(pr + a0, __float2int_rn(w0 * v.x)); atomicAdd(pi + a0, __float2int_rn(w0 * v.y)); }
+          if (w1 != 0.f) { atomicAdd(pr + a1, __float2int_rn(w1 * v.x)); atomicAdd(pi + a1, __float2int_rn(w1 * v.y)); }
         } else {
-          const int plane = t.PX * t.PY;
 #pragma unroll 2
           for (int e = 0; e < 8; ++e) {
             const float wzv = wz[(uint64_t)s * 8 + e];
             if (wzv == 0.f) continue;
             const int zo = (oz + e) * plane;
             const float w0 = wx0 * wyv * wzv, w1 = wx1 * wyv * wzv;
-            if (w0 != 0.f) { atomicAdd(pr + zo + a0, w0 * v.x); atomicAdd(pi + zo + a0, w0 * v.y); }
-            if (w1 != 0.f) { atomicAdd(pr + zo + a1, w1 * v.x); atomicAdd(pi + zo + a1, w1 * v.y); }
+            if (w0 != 0.f) {
+              atomicAdd(pr + zo + a0, __float2int_rn(w0 * v.x));
+              atomicAdd(pi + zo + a0, __float2int_rn(w0 * v.y));
+            }
+            if (w1 != 0.f) {
+              atomicAdd(pr + zo + a1, __float2int_rn(w1 * v.x));
+              atomicAdd(pi + zo + a1, __float2int_rn(w1 * v.y));
+            }
           }
         }
       }
@@ -359,22 +518,22 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
     const int pzz = q / (t.PY * t.PX);
     const int gy = y0 + pyy, gx = x0 + pxx, gz = z0 + pzz;
     if (gy >= g.Gy || gx >= g.Gx || gz >= g.Gz) continue;
-    const int sy = (gy + g.ifs[1]) % g.Gy;
-    const int sx = (gx + g.ifs[0]) % g.Gx;
-    const int sz = (DIM == 3) ? (gz + g.ifs[2]) % g.Gz : 0;
-    const uint64_t idx = (uint64_t)sy + (uint64_t)g.Gy * ((uint64_t)sx + (uint64_t)g.Gx * sz);
+    const uint64_t idx = (uint64_t)gy + (uint64_t)g.Gy * ((uint64_t)gx + (uint64_t)g.Gx * gz);
     for (int c = 0; c < ncl; ++c)
       for (int j = 0; j < K; ++j) {
-        const float* pr = sm + ((c * K + j) * 2) * cells;
-        const float re = pr[q], im = pr[cells + q];
-        if (re != 0.f || im != 0.f)
-          atomicAdd(grids + ((uint64_t)(cfirst + c) * L + lseg + j) * G + idx, make_float2(re, im));
+        const int pl = c * K + j;
+        const int* pr = smi + (pl * 2) * cells;
+        const int re = pr[q], im = pr[cells + q];
+        if (re != 0 || im != 0)
+          atomicAdd(grids + ((uint64_t)(cfirst + c) * L + lseg + j) * G + idx,
+                    make_float2((float)re * inv_scale[pl], (float)im * inv_scale[pl]));
       }
   }
 }
 
 // ---------------------------------------------------------------------------
-// Adjoint: post-kernel (fftshift + crop + deapodize + WoH + coil combine)
+// Adjoint post-kernel: crop the centred grid, undo the checkerboard,
+// deapodize, apply WoH, combine segments and coils.
 // ---------------------------------------------------------------------------
 __global__ void k_post(NufftGeom g, int Cb, int L, const float2* __restrict__ grids, const float2* __restrict__ S,
                        int c0, const float2* __restrict__ E, const float2* __restrict__ WoH,
@@ -385,19 +544,21 @@ __global__ void k_post(NufftGeom g, int Cb, int L, const float2* __restrict__ gr
   const int iy = (int)(p % g.Ny);
   const int ix = (int)((p / g.Ny) % g.Nx);
   const int iz = (int)(p / ((uint64_t)g.Ny * g.Nx));
-  const int gy = wrap(iy + g.crop_off[1] - g.fs[1], g.Gy);
-  const int gx = wrap(ix + g.crop_off[0] - g.fs[0], g.Gx);
-  const int gz = (g.dim == 3) ? wrap(iz + g.crop_off[2] - g.fs[2], g.Gz) : 0;
+  const int gy = iy + g.crop_off[1];
+  const int gx = ix + g.crop_off[0];
+  const int gz = (g.dim == 3) ? iz + g.crop_off[2] : 0;
   const uint64_t q = (uint64_t)gy + (uint64_t)g.Gy * ((uint64_t)gx + (uint64_t)g.Gx * gz);
   const uint64_t G = g.ngrid();
   float k = deap[ix] * deap[g.Nx + iy];
   if (g.dim == 3) k = k * deap[g.Nx + g.Ny + iz];
   const bool ok = (k == k);
+  const float sgn = parity3(gx, gy, gz) ? -1.f : 1.f;
   float2 acc = accumulate ? x[p] : make_float2(0.f, 0.f);
   for (int c = 0; c < Cb; ++c) {
     float2 img = make_float2(0.f, 0.f);
     for (int l = 0; l < L; ++l) {
       float2 v = grids[((uint64_t)c * L + l) * G + q];
+      v = make_float2(sgn * v.x, sgn * v.y);
       v = ok ? make_float2(__fmul_rn(__fdiv_rn(v.x, k), scale), __fmul_rn(__fdiv_rn(v.y, k), scale))
              : make_float2(0.f, 0.f);
       if (WoH) v = cmul(v, WoH[(uint64_t)l * N + p]);
@@ -419,14 +580,37 @@ NufftPlan::~NufftPlan() {
   for (auto& kv : ffts) cufftDestroy(kv.second);
 }
 
-static TileShape choose_tiles(const NufftGeom& g) {
+NufftTune NufftTune::defaults() {
+  NufftTune t;
+  auto env = [](const char* n, int d) {
+    const char* v = getenv(n);
+    return (v && *v) ? atoi(v) : d;
+  };
+  t.tile2d = env("PG_TILE2D", t.tile2d);
+  t.tile3d = env("PG_TILE3D", t.tile3d);
+  t.submax2d = env("PG_SUBMAX2D", t.submax2d);
+  t.submax3d = env("PG_SUBMAX3D", t.submax3d);
+  t.spread_cc = env("PG_SPREAD_CC", t.spread_cc);
+  t.gather_cc = env("PG_GATHER_CC", t.gather_cc);
+  return t;
+}
+
+// Padded extent along y (the fastest axis) such that 4 x-rows of 8 y-taps
+// land in 32 distinct banks: PY = 8 or 24 (mod 32).
+static int padded_y(int T) {
+  int py = T + 8;
+  while ((py % 32) != 8 && (py % 32) != 24) ++py;
+  return py;
+}
+
+static TileShape choose_tiles(const NufftGeom& g, const NufftTune& tu) {
   TileShape t{};
   if (g.dim == 2) {
-    t.TX = 32; t.TY = 32; t.TZ = 1;
-    t.PX = t.TX + 8; t.PY = t.TY + 8; t.PZ = 1;     // PY = 40 = 8 (mod 32)
+    t.TX = t.TY = tu.tile2d; t.TZ = 1;
+    t.PX = t.TX + 8; t.PY = padded_y(t.TY); t.PZ = 1;
   } else {
-    t.TX = 8; t.TY = 8; t.TZ = 8;
-    t.PX = 16; t.PY = 24; t.PZ = 16;                // PY = 24: 4 x-taps hit 4 distinct bank groups
+    t.TX = t.TY = t.TZ = tu.tile3d;
+    t.PX = t.TX + 8; t.PY = padded_y(t.TY); t.PZ = t.TZ + 8;
   }
   t.ntx = (g.Gx + t.TX - 1) / t.TX;
   t.nty = (g.Gy + t.TY - 1) / t.TY;
@@ -452,6 +636,7 @@ pg_status nufft_plan_create(std::unique_ptr<NufftPlan>* out, uint64_t M, float g
                        (unsigned long long)i);
   }
   auto p = std::make_unique<NufftPlan>();
+  p->tune = NufftTune::defaults();
   NufftGeom& g = p->g;
   g.dim = (nz == 1) ? 2 : 3;
   g.Nx = nx; g.Ny = ny; g.Nz = nz;
@@ -468,8 +653,11 @@ pg_status nufft_plan_create(std::unique_ptr<NufftPlan>* out, uint64_t M, float g
   g.nlut = (int)lut.size();
   const int N3[3] = {nx, ny, nz};
   const int G3[3] = {g.Gx, g.Gy, g.Gz};
+  g.sign_c = 1.0f;
   for (int a = 0; a < 3; ++a) {
     const bool used = (a < 2) || g.dim == 3;
+    if (used && (G3[a] % 2)) return set_error(PG_INVALID_ARG, "Gnufft: oversampled grid must be even");
+    if (used && ((G3[a] / 2) % 2)) g.sign_c = -g.sign_c;
     g.pad_off[a] = used ? (int)(((float)N3[a] * gridos / 2.0f) - ((float)N3[a] / 2.0f)) : 0;
     g.crop_off[a] = used ? (int)(((float)G3[a] / 2.0f) - ((float)N3[a] / 2.0f)) : 0;
     g.fs[a] = used ? (int)std::floor(G3[a] / 2.0) : 0;
@@ -487,6 +675,7 @@ pg_status nufft_plan_create(std::unique_ptr<NufftPlan>* out, uint64_t M, float g
   if (!kz) zeros.assign(M, 0.f);
   PG_TRY(p->kz.upload(kz ? kz : zeros.data(), M, s));
   PG_TRY(p->lut.upload(lut.data(), lut.size(), s));
+  p->lut_max = *std::max_element(lut.begin(), lut.end());
   PG_TRY(p->deap.upload(deap.data(), deap.size(), s));
   PG_CUDA(cudaStreamSynchronize(s));
   // the unsegmented binning is built on first use (time-segmented operators never need it)
@@ -505,7 +694,7 @@ pg_status nufft_build_binning(NufftPlan* p, int L, int K, const int* l0_host, co
   const uint64_t M = p->M;
   auto b = std::make_unique<Binning>();
   b->L = L; b->K = K; b->M = M;
-  b->tile = choose_tiles(g);
+  b->tile = choose_tiles(g, p->tune);
   const TileShape& t = b->tile;
   const uint64_t ntiles = (uint64_t)t.ntx * t.nty * t.ntz;
   b->nkeys = ntiles * (uint64_t)L;
@@ -535,7 +724,7 @@ pg_status nufft_build_binning(NufftPlan* p, int L, int K, const int* l0_host, co
   for (uint64_t i = 0; i < M; ++i) b->h_perm[pos[b->h_keys[i]]++] = (uint32_t)i;
 
   // Subproblems: each (segment window, tile) bin split into chunks.
-  const int kMaxPerSub = (g.dim == 2) ? 512 : 256;
+  const int kMaxPerSub = (g.dim == 2) ? p->tune.submax2d : p->tune.submax3d;
   std::vector<int4> subs;
   for (uint64_t k = 0; k < b->nkeys; ++k) {
     const uint64_t a = cnt[k], e = cnt[k + 1];
@@ -614,11 +803,63 @@ static int batch_coils(const NufftPlan* p, int C, int L) {
   return (int)std::min<uint64_t>(cb, (uint64_t)C);
 }
 
+// Tiled gather launch: choose the padded segment count KP and the coils per
+// block CC so that the staged tiles fit in shared memory and 2*CC*KP <= 32.
+template <int DIM, int CC, int KP>
+static pg_status gather_launch_one(NufftPlan* p, const Binning* bin, const float2* aa, int nb, float2* y,
+                                   uint64_t dstride, cudaStream_t s) {
+  const TileShape& t = bin->tile;
+  const size_t smem = (size_t)CC * KP * 2 * t.PX * t.PY * t.PZ * sizeof(float);
+  PG_CUDA(cudaFuncSetAttribute(k_gather<DIM, CC, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid(bin->nsub, ceil_div(nb, CC));
+  PG_LAUNCH((k_gather<DIM, CC, KP>), grid, 256, smem, s, p->g, t, bin->subprob.p, bin->start.p, bin->wxy.p,
+            bin->wz.p, bin->perm.p, aa, bin->K, bin->L, p->grids.p, nb, y, dstride);
+  return PG_OK;
+}
+
+static int smem_optin_bytes() {
+  static int v = -1;
+  if (v < 0) {
+    int dev = 0, a = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&a, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    v = a;
+  }
+  return v;
+}
+
+template <int DIM>
+static pg_status launch_gather(NufftPlan* p, const Binning* bin, const float2* aa, int nb, float2* y, uint64_t dstride,
+                               cudaStream_t s) {
+  const int K = bin->K;
+  const int KP = K <= 1 ? 1 : K <= 2 ? 2 : K <= 4 ? 4 : 8;
+  const size_t pair = (size_t)bin->tile.PX * bin->tile.PY * bin->tile.PZ * 2 * sizeof(float);
+  const size_t limit = (size_t)smem_optin_bytes() - 6144;  // static reduction buffer + margin
+  int CC = std::max(1, std::min(4, p->tune.gather_cc));
+  while (CC > 1 && (CC >= 2 * nb || 2 * CC * KP > 32 || (size_t)CC * KP * pair > limit)) CC >>= 1;
+  if ((size_t)CC * KP * pair > limit || 2 * CC * KP > 32)
+    return set_error(PG_INVALID_ARG, "forward: segment window K=%d too wide for shared memory", K);
+  switch (KP * 10 + CC) {
+    case 11: return gather_launch_one<DIM, 1, 1>(p, bin, aa, nb, y, dstride, s);
+    case 12: return gather_launch_one<DIM, 2, 1>(p, bin, aa, nb, y, dstride, s);
+    case 14: return gather_launch_one<DIM, 4, 1>(p, bin, aa, nb, y, dstride, s);
+    case 21: return gather_launch_one<DIM, 1, 2>(p, bin, aa, nb, y, dstride, s);
+    case 22: return gather_launch_one<DIM, 2, 2>(p, bin, aa, nb, y, dstride, s);
+    case 24: return gather_launch_one<DIM, 4, 2>(p, bin, aa, nb, y, dstride, s);
+    case 41: return gather_launch_one<DIM, 1, 4>(p, bin, aa, nb, y, dstride, s);
+    case 42: return gather_launch_one<DIM, 2, 4>(p, bin, aa, nb, y, dstride, s);
+    case 44: return gather_launch_one<DIM, 4, 4>(p, bin, aa, nb, y, dstride, s);
+    case 81: return gather_launch_one<DIM, 1, 8>(p, bin, aa, nb, y, dstride, s);
+    case 82: return gather_launch_one<DIM, 2, 8>(p, bin, aa, nb, y, dstride, s);
+  }
+  return set_error(PG_INVALID_ARG, "forward: unsupported tiling (K=%d)", K);
+}
+
 pg_status nufft_forward(NufftPlan* p, const NufftBatch& b, const float2* x, float2* y, cudaStream_t s) {
   const NufftGeom& g = p->g;
   if (!b.bin) PG_TRY(nufft_plain_binning(p, s));
   const Binning* bin = b.bin ? b.bin : p->plain.get();
-  const int L = bin->L, K = bin->K;
+  const int L = bin->L;
   const int Cb = batch_coils(p, b.C, L);
   const float scale = (g.dim == 2) ? (1.0f / (g.os * g.os)) : (float)(1.0 / (double)(g.os * g.os * g.os));
   const uint64_t G = g.ngrid();
@@ -639,14 +880,13 @@ pg_status nufft_forward(NufftPlan* p, const NufftBatch& b, const float2* x, floa
     }
     float2* yc = y + (uint64_t)c0 * b.data_stride;
     const float2* aa = (L > 1 || bin->aa.p) ? bin->aa.p : nullptr;
-    const int* l0 = bin->l0.p;
     ProfScope ps("gather", s);
-    if (g.dim == 2)
-      PG_LAUNCH(k_gather<2>, ceil_div(p->M, 128), 128, 0, s, g, p->M, bin->start.p, bin->wxy.p, bin->wz.p,
-                bin->perm.p, l0, aa, K, L, p->grids.p, nb, yc, b.data_stride);
-    else
-      PG_LAUNCH(k_gather<3>, ceil_div(p->M, 128), 128, 0, s, g, p->M, bin->start.p, bin->wxy.p, bin->wz.p,
-                bin->perm.p, l0, aa, K, L, p->grids.p, nb, yc, b.data_stride);
+    if (bin->nsub > 0) {
+      if (g.dim == 2)
+        PG_TRY(launch_gather<2>(p, bin, aa, nb, yc, b.data_stride, s));
+      else
+        PG_TRY(launch_gather<3>(p, bin, aa, nb, yc, b.data_stride, s));
+    }
   }
   return PG_OK;
 }
@@ -661,14 +901,13 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
   const uint64_t G = g.ngrid();
   const TileShape& t = bin->tile;
   const size_t plane_bytes = (size_t)t.PX * t.PY * t.PZ * 2 * sizeof(float);
-  static int smem_optin = -1;
-  if (smem_optin < 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  }
-  int Cc = (int)std::min<size_t>(4, (size_t)smem_optin / (plane_bytes * K));
-  if (Cc < 1) return set_error(PG_INVALID_ARG, "adjoint: segment window K=%d too wide for shared memory", K);
+  const int smem_optin = smem_optin_bytes();
+  int Cc = (int)std::min<size_t>((size_t)std::max(1, std::min(4, p->tune.spread_cc)),
+                                  (size_t)(smem_optin - 2048) / (plane_bytes * K));
+  while (Cc > 1 && Cc * K > 16) --Cc;
+  if (Cc < 1 || K > 16) return set_error(PG_INVALID_ARG, "adjoint: segment window K=%d too wide for shared memory", K);
+  const float w1 = p->lut_max;
+  const float wmax = (g.dim == 2) ? w1 * w1 : w1 * w1 * w1;
   for (int c0 = 0; c0 < b.C; c0 += Cb) {
     const int nb = std::min(Cb, b.C - c0);
     const int B = nb * L;
@@ -688,11 +927,11 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
       if (g.dim == 2) {
         PG_CUDA(cudaFuncSetAttribute(k_spread<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         PG_LAUNCH(k_spread<2>, grid, 256, smem, s, g, t, bin->subprob.p, bin->start.p, bin->wxy.p, bin->wz.p,
-                  bin->perm.p, aa, K, L, yc, b.data_stride, nb, cc, p->grids.p);
+                  bin->perm.p, aa, K, L, yc, b.data_stride, nb, cc, wmax, p->grids.p);
       } else {
         PG_CUDA(cudaFuncSetAttribute(k_spread<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         PG_LAUNCH(k_spread<3>, grid, 256, smem, s, g, t, bin->subprob.p, bin->start.p, bin->wxy.p, bin->wz.p,
-                  bin->perm.p, aa, K, L, yc, b.data_stride, nb, cc, p->grids.p);
+                  bin->perm.p, aa, K, L, yc, b.data_stride, nb, cc, wmax, p->grids.p);
       }
     }
     {

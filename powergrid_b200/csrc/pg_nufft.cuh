@@ -22,6 +22,7 @@ struct NufftGeom {
   int crop_off[3];     // crop_center offset per axis
   int fs[3];           // fftshift amount (floor(G/2))
   int ifs[3];          // ifftshift amount (ceil(G/2) in-plane, floor along z)
+  float sign_c = 1.f;  // prod over gridded axes of (-1)^(G/2): checkerboard constant
   __host__ __device__ uint64_t nimg() const { return (uint64_t)Nx * Ny * Nz; }
   __host__ __device__ uint64_t ngrid() const { return (uint64_t)Gx * Gy * Gz; }
 };
@@ -31,6 +32,16 @@ struct TileShape {
   int TX, TY, TZ;      // tile size
   int PX, PY, PZ;      // padded smem extent (>= T + 8 along gridded axes)
   int ntx, nty, ntz;   // tiles per axis
+};
+
+// Tunable gridding parameters (tile edge, samples per subproblem, coils per
+// block).  Defaults can be overridden with PG_TILE2D, PG_TILE3D, PG_SUBMAX2D,
+// PG_SUBMAX3D, PG_SPREAD_CC, PG_GATHER_CC.
+struct NufftTune {
+  int tile2d = 16, tile3d = 8;        // measured best on cfg2 (B200): 16 > 32 > 64
+  int submax2d = 256, submax3d = 256;
+  int spread_cc = 2, gather_cc = 2;
+  static NufftTune defaults();
 };
 
 // Per-(trajectory, segmentation) sample binning used by both directions.
@@ -55,9 +66,11 @@ struct Binning {
 
 struct NufftPlan {
   NufftGeom g;
+  NufftTune tune;
   uint64_t M = 0;
   DevBuf<float> kx, ky, kz;      // original order
   DevBuf<float> lut;
+  float lut_max = 0.f;           // largest per-axis tap weight
   DevBuf<float> deap;            // Nx + Ny + Nz reciprocal-transform factors
   std::unique_ptr<Binning> plain;  // binning without segmentation (L = 1)
   // grid workspace and cuFFT plans, keyed by batch size
