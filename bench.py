@@ -325,11 +325,69 @@ def run_gpu_arm(args):
                              "peak_source": peak_kind},
                 "cpu_baseline": cpu,
                 "gpu_launches": int(launches)}
+        if ws == 1 and not args.no_serving:
+            line["serving"] = run_serving()
         print(json.dumps(line))
     if ws > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     return 0
+
+
+def run_serving(n_requests: int = 16, rate_hz: float = 20.0, inflight: int = 8, seed: int = 4):
+    """Config 4: a seeded Poisson stream of time-segmented SENSE reconstructions of
+    uneven size, served one request at a time (max_inflight = 1) and with
+    continuous batching (max_inflight = `inflight`).  Returns a summary dict."""
+    import numpy as np
+
+    import powergrid_b200 as pg
+    from powergrid_b200 import synthetic as S
+    from powergrid_b200.serve import ReconRequest, Server
+
+    items = S.serving_stream(seed=seed, n_requests=n_requests, rate_hz=rate_hz)
+    reqs = []
+    for it in items:
+        M, n = it.kx.size, it.nimg
+        G = pg.Gnufft(M, 2.0, it.nx, it.ny, it.nz, it.kx, it.ky, it.kz)
+        A = pg.TimeSegmentation(G, it.fm, it.t, M, n, it.L, 1, 1)
+        Sg = pg.SENSE(A, it.smap, M, n, it.nc)
+        y = Sg * it.x_true
+        del Sg, A, G
+        reqs.append(ReconRequest(it.nx, it.ny, it.nz, it.nc, it.L, it.niter, it.beta, it.kx, it.ky, it.kz, it.t,
+                                 np.tile(it.fm, it.n_slices), np.tile(it.smap, it.n_slices),
+                                 np.tile(y, it.n_slices), it.n_slices))
+    budget = 120 << 30
+
+    def serve(slots):
+        srv = Server(hbm_budget_bytes=budget, max_inflight=slots)
+        t0 = time.perf_counter()
+        tickets = []
+        for it, r in zip(items, reqs):
+            delay = it.arrival_s - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            tickets.append(srv.submit(r))
+        lat, iters, done = [], 0, 0.0
+        for t in tickets:
+            _, st = srv.wait(t)
+            assert st["status"] == "PG_OK", st
+            lat.append(st["t_done_ms"] - st["t_submit_ms"])
+            iters += st["iters_done"]
+            done = max(done, st["t_done_ms"])
+        makespan = time.perf_counter() - t0
+        srv.close()
+        lat.sort()
+        return {"iters_per_s": iters / makespan, "makespan_s": makespan, "iterations": iters,
+                "latency_ms_p50": lat[len(lat) // 2], "latency_ms_p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]}
+
+    serve(inflight)  # warm-up: module loading, pool growth
+    plain = serve(1)
+    served = serve(inflight)
+    return {"workload": f"config 4 stream: {n_requests} seeded requests, Poisson {rate_hz}/s, "
+                        "64-256 in-plane (or 3-D 64-128 x 16-32), 1-32 slices, 4-32 coils, 8k-200k samples, "
+                        f"L=4-12, 10 PCG iterations, QuadPenalty; {sum(r.n_slices for r in reqs)} slice jobs",
+            "plain_one_at_a_time": plain, "served": served, "inflight": inflight,
+            "speedup_iters_per_s": served["iters_per_s"] / plain["iters_per_s"]}
 
 
 def main():
@@ -339,7 +397,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="skip the config-4 serving stream")
+    ap.add_argument("--serving-only", action="store_true", help="only the config-4 serving stream")
     args = ap.parse_args()
+    if args.serving_only:
+        import powergrid_b200 as pg
+        pg.init(0)
+        print(json.dumps({"serving": run_serving()}))
+        return 0
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         return run_reference_arm(args)

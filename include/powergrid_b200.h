@@ -144,27 +144,35 @@ pg_status pg_penalty_denom_device(const pg_penalty* R, const void* ddir_dev, con
 
 /* ---- request server (continuous batching) ---------------------------- */
 typedef struct pg_server_config {
-  uint64_t hbm_budget_bytes;   /* admission limit on resident request state */
-  uint32_t max_inflight;       /* concurrent requests on the GPU */
-  uint32_t streams;            /* CUDA streams used for overlap */
+  uint64_t hbm_budget_bytes;   /* admission limit on the summed footprint of resident jobs */
+  uint32_t max_inflight;       /* jobs on the GPU at once: one worker thread and stream each */
+  uint32_t reserved;           /* must be 0 */
 } pg_server_config;
 
-/* A 2-D/3-D time-segmented SENSE reconstruction request:
- * SENSE<TimeSegmentation<Gnufft>> + QuadPenalty, reconSolve semantics. */
+/* A time-segmented SENSE reconstruction request:
+ * SENSE<TimeSegmentation<Gnufft>> + QuadPenalty with reconSolve semantics
+ * (reconSolve.h:63-82), for n_slices independent images that share one
+ * trajectory (the slice loop of PowerGridIsmrmrd.cpp:191-264).  Each slice is
+ * scheduled as its own job.  Arrays (host memory, valid until completion):
+ *   kx, ky, kz, t   n_samples                  (k in cycles/FOV, t in s)
+ *   field_map       n_slices * nx*ny*nz        (rad/s)
+ *   sense_map       n_slices * nx*ny*nz*nc     (complex, coil-major per slice)
+ *   data            n_slices * n_samples*nc    (complex, coil-major per slice)
+ *   image_out       n_slices * nx*ny*nz        (complex, written on completion) */
 typedef struct pg_request {
-  uint64_t nx, ny, nz, nc, n_samples, L, niter;
+  uint64_t nx, ny, nz, n_slices, nc, n_samples, L, niter;
   float beta;
   const float* kx; const float* ky; const float* kz; const float* t;
-  const float* field_map;      /* nx*ny*nz, rad/s */
-  const float* sense_map;      /* complex, nx*ny*nz*nc, coil-major */
-  const float* data;           /* complex, n_samples*nc, coil-major */
-  float* image_out;            /* complex, nx*ny*nz; written when done */
+  const float* field_map;
+  const float* sense_map;
+  const float* data;
+  float* image_out;
 } pg_request;
 
 typedef struct pg_request_stats {
-  double t_submit_ms, t_start_ms, t_done_ms;   /* host steady-clock */
-  uint64_t iters_done;
-  uint64_t bytes_resident;
+  double t_submit_ms, t_start_ms, t_done_ms;   /* host steady clock; start = first slice admitted */
+  uint64_t iters_done;                         /* PCG iterations completed, all slices */
+  uint64_t bytes_resident;                     /* admission footprint of one slice job */
   pg_status status;
 } pg_request_stats;
 
@@ -176,7 +184,8 @@ pg_status pg_submit(pg_server s, const pg_request* req, uint64_t* ticket);
 pg_status pg_poll(pg_server s, uint64_t ticket, pg_request_stats* stats);
 pg_status pg_wait(pg_server s, uint64_t ticket, pg_request_stats* stats);
 pg_status pg_cancel(pg_server s, uint64_t ticket);
-/* Estimated device bytes a request holds while resident (admission metric). */
+/* Device bytes one slice job of the request holds while resident (the
+ * admission metric; an upper bound of what the job allocates). */
 uint64_t pg_request_footprint(const pg_request* req);
 
 /* ---- instrumentation and fault injection (host-side only) ------------ */

@@ -32,13 +32,13 @@ class Penalty(C.Structure):
 
 
 class ServerConfig(C.Structure):
-    _fields_ = [("hbm_budget_bytes", U64), ("max_inflight", C.c_uint32), ("streams", C.c_uint32)]
+    _fields_ = [("hbm_budget_bytes", U64), ("max_inflight", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class Request(C.Structure):
-    _fields_ = [("nx", U64), ("ny", U64), ("nz", U64), ("nc", U64), ("n_samples", U64), ("L", U64), ("niter", U64),
-                ("beta", F32), ("kx", P), ("ky", P), ("kz", P), ("t", P), ("field_map", P), ("sense_map", P),
-                ("data", P), ("image_out", P)]
+    _fields_ = [("nx", U64), ("ny", U64), ("nz", U64), ("n_slices", U64), ("nc", U64), ("n_samples", U64),
+                ("L", U64), ("niter", U64), ("beta", F32), ("kx", P), ("ky", P), ("kz", P), ("t", P),
+                ("field_map", P), ("sense_map", P), ("data", P), ("image_out", P)]
 
 
 class RequestStats(C.Structure):

@@ -818,13 +818,12 @@ static pg_status gather_launch_one(NufftPlan* p, const Binning* bin, const float
 }
 
 static int smem_optin_bytes() {
-  static int v = -1;
-  if (v < 0) {
+  static const int v = [] {
     int dev = 0, a = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&a, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    v = a;
-  }
+    return a;
+  }();
   return v;
 }
 

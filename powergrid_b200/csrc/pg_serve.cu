@@ -1,17 +1,293 @@
-// Request server: placeholder until the continuous-batching loop lands.
+// Request server: continuous batching of time-segmented SENSE reconstructions.
+//
+// The reference drivers reconstruct one slice/echo/repetition after another
+// (PowerGridIsmrmrd.cpp:191-264), each with its own Gnufft, TimeSegmentation,
+// SENSE and reconSolve.  Here each slice of a request is a job; jobs are
+// admitted in FIFO order whenever a worker slot is free and the summed
+// device footprint of resident jobs stays within the HBM budget.  Every
+// worker owns a CUDA stream, so admitted jobs overlap on the GPU, and a job
+// that finishes frees its slot and memory for the next arrival.  A job keeps
+// its trajectory, maps and PCG state resident in a private device arena
+// (stream-ordered pool allocations, no cudaMalloc/cudaFree on the hot path)
+// until its image is copied out.
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+
 #include "pg_ops.cuh"
+
+namespace pg {
+namespace {
+
+double now_ms() {
+  using namespace std::chrono;
+  return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+struct Ticket {
+  uint64_t id = 0;
+  pg_request req{};
+  uint64_t footprint = 0;
+  int jobs_total = 0;
+  int jobs_left = 0;
+  int jobs_started = 0;
+  std::atomic<bool> cancel{false};
+  pg_request_stats st{};
+  bool done = false;
+};
+
+struct Job {
+  std::shared_ptr<Ticket> t;
+  uint64_t slice = 0;
+};
+
+uint64_t grid_cells(const pg_request& r) {
+  const uint64_t gx = 2 * r.nx, gy = 2 * r.ny, gz = (r.nz == 1) ? 1 : 2 * r.nz;
+  return gx * gy * gz;
+}
+
+// Per-job grid workspace cap: keeps one job from monopolising the device.
+constexpr uint64_t kJobGridBytes = 2ull << 30;
+
+}  // namespace
+
+uint64_t request_footprint(const pg_request& r) {
+  const uint64_t M = r.n_samples, N = r.nx * r.ny * r.nz, C = r.nc;
+  const uint64_t L = r.L <= 1 ? 1 : r.L;
+  const uint64_t G = grid_cells(r);
+  const bool d3 = r.nz > 1;
+  uint64_t b = 0;
+  b += 3 * M * 4 + 40000 * 4 + (r.nx + r.ny + r.nz) * 4;          // trajectory, LUT, deapodization
+  b += M * (8 + 64 + (d3 ? 32 : 0) + 4 + 4);                        // binning temporaries
+  b += M * (4 + 8 + 64 + (d3 ? 32 : 0) + 4 + 3 * 8) + (M / 64 + 4096 * L) * 16;  // binning
+  uint64_t grids = C * L * G * 8;
+  if (grids > kJobGridBytes) grids = std::max<uint64_t>(L * G * 8, (kJobGridBytes / (L * G * 8)) * L * G * 8);
+  b += 2 * grids;                                                   // grids + cuFFT work area
+  b += 2 * L * N * 8 + C * N * 8;                                   // Wo, WoH, coil maps
+  b += 3 * N * 8 + 3 * C * M * 8 + C * M * 8 + C * M * 4 + 64 * 1024;  // PCG state
+  b += C * M * 8 + N * 8;                                           // job input / output
+  return b + b / 4 + (32ull << 20);
+}
+
+}  // namespace pg
 
 using namespace pg;
 
+struct pg_server_s {
+  pg_server_config cfg{};
+  int device = 0;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<Job> pending;
+  std::unordered_map<uint64_t, std::shared_ptr<Ticket>> tickets;
+  uint64_t used = 0;
+  uint32_t running = 0;
+  bool stop = false;
+  uint64_t next = 1;
+  std::vector<std::thread> workers;
+
+  bool head_fits() const {
+    if (pending.empty()) return false;
+    const uint64_t f = pending.front().t->footprint;
+    return used + f <= cfg.hbm_budget_bytes || running == 0;
+  }
+
+  pg_status run_job(const Job& j, cudaStream_t s, uint64_t* iters) {
+    const pg_request& r = j.t->req;
+    const uint64_t N = r.nx * r.ny * r.nz, M = r.n_samples, C = r.nc;
+    const uint64_t sl = j.slice;
+    Arena arena;
+    PG_TRY(arena_open(&arena, j.t->footprint, s));
+    arena_install(&arena);
+    pg_status st = PG_OK;
+    {
+      std::unique_ptr<GnufftOp> G;
+      std::unique_ptr<TimeSegOp> A;
+      std::unique_ptr<SenseOp> S;
+      DevBuf<float2> y, x;
+      DevBuf<uint32_t> it;
+      do {
+        st = make_gnufft(&G, M, 2.0f, r.nx, r.ny, r.nz, r.kx, r.ky, r.kz, s);
+        if (st != PG_OK) break;
+        G->plan->budget_bytes = kJobGridBytes;
+        st = make_timeseg(&A, G.get(), r.field_map + sl * N, r.t, M, N, r.L, 1, 1, s);
+        if (st != PG_OK) break;
+        st = make_sense(&S, A.get(), r.sense_map + 2 * sl * N * C, M, N, C, s);
+        if (st != PG_OK) break;
+        st = y.upload(reinterpret_cast<const float2*>(r.data) + sl * M * C, M * C, s);
+        if (st != PG_OK) break;
+        if ((st = x.alloc(N)) != PG_OK) break;
+        if ((st = it.alloc(1)) != PG_OK) break;
+        pg_penalty R{PG_PENALTY_QUAD, r.nx, r.ny, r.nz, r.beta, 1.0f, 3};
+        st = pcg_solve_device(S.get(), nullptr, nullptr, y.p, R, r.niter, x.p, it.p, s, &j.t->cancel);
+        if (st != PG_OK) break;
+        uint32_t n = 0;
+        cudaError_t e = cudaMemcpyAsync(r.image_out + 2 * sl * N, x.p, N * sizeof(float2), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&n, it.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) { cudaGetLastError(); st = set_error(PG_CUDA_ERROR, "job copy-out: %s", cudaGetErrorString(e)); break; }
+        *iters = n;
+      } while (0);
+      cudaStreamSynchronize(s);
+      // operators and buffers release into the arena (no-ops) before it is returned
+    }
+    arena_install(nullptr);
+    arena_release(&arena);
+    cudaStreamSynchronize(s);
+    return st;
+  }
+
+  void worker() {
+    cudaSetDevice(device);
+    cudaStream_t s = nullptr;
+    cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    for (;;) {
+      Job job;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv_work.wait(lk, [&] { return stop || head_fits(); });
+        if (stop) break;
+        job = pending.front();
+        pending.pop_front();
+        used += job.t->footprint;
+        ++running;
+        if (job.t->jobs_started++ == 0) job.t->st.t_start_ms = now_ms();
+      }
+      uint64_t iters = 0;
+      pg_status st = job.t->cancel.load() ? PG_CANCELLED : run_job(job, s, &iters);
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        used -= job.t->footprint;
+        --running;
+        Ticket& t = *job.t;
+        t.st.iters_done += iters;
+        if (st != PG_OK && t.st.status == PG_OK) t.st.status = st;
+        if (--t.jobs_left == 0) {
+          t.st.t_done_ms = now_ms();
+          if (t.cancel.load() && t.st.status == PG_OK) t.st.status = PG_CANCELLED;
+          t.done = true;
+          cv_done.notify_all();
+        }
+      }
+      cv_work.notify_all();
+    }
+    if (s) cudaStreamDestroy(s);
+  }
+};
+
 extern "C" {
-pg_status pg_server_create(pg_server* out, const pg_server_config*) {
-  if (out) *out = nullptr;
-  return set_error(PG_INVALID_ARG, "server not built yet");
+
+uint64_t pg_request_footprint(const pg_request* req) { return req ? request_footprint(*req) : 0; }
+
+pg_status pg_server_create(pg_server* out, const pg_server_config* cfg) {
+  if (!out || !cfg) return set_error(PG_INVALID_ARG, "server: null argument");
+  if (cfg->max_inflight == 0 || cfg->max_inflight > 64) return set_error(PG_INVALID_ARG, "server: max_inflight in 1..64");
+  if (cfg->hbm_budget_bytes == 0) return set_error(PG_INVALID_ARG, "server: zero HBM budget");
+  PG_TRY(ensure_init());
+  auto* sv = new pg_server_s;
+  sv->cfg = *cfg;
+  cudaGetDevice(&sv->device);
+  for (uint32_t i = 0; i < cfg->max_inflight; ++i) sv->workers.emplace_back([sv] { sv->worker(); });
+  *out = sv;
+  return PG_OK;
 }
-pg_status pg_server_destroy(pg_server) { return PG_OK; }
-pg_status pg_submit(pg_server, const pg_request*, uint64_t*) { return set_error(PG_INVALID_ARG, "server not built yet"); }
-pg_status pg_poll(pg_server, uint64_t, pg_request_stats*) { return set_error(PG_INVALID_ARG, "server not built yet"); }
-pg_status pg_wait(pg_server, uint64_t, pg_request_stats*) { return set_error(PG_INVALID_ARG, "server not built yet"); }
-pg_status pg_cancel(pg_server, uint64_t) { return set_error(PG_INVALID_ARG, "server not built yet"); }
-uint64_t pg_request_footprint(const pg_request*) { return 0; }
+
+pg_status pg_server_destroy(pg_server sv) {
+  if (!sv) return PG_OK;
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    for (auto& kv : sv->tickets) kv.second->cancel.store(true);
+    // queued jobs are dropped; running ones stop at their next iteration
+    for (auto& j : sv->pending) {
+      Ticket& t = *j.t;
+      if (t.st.status == PG_OK) t.st.status = PG_CANCELLED;
+      if (--t.jobs_left == 0) { t.done = true; t.st.t_done_ms = now_ms(); }
+    }
+    sv->pending.clear();
+    sv->stop = true;
+  }
+  sv->cv_work.notify_all();
+  for (auto& w : sv->workers) w.join();
+  delete sv;
+  return PG_OK;
 }
+
+pg_status pg_submit(pg_server sv, const pg_request* r, uint64_t* ticket) {
+  if (!sv || !r || !ticket) return set_error(PG_INVALID_ARG, "submit: null argument");
+  if (!r->kx || !r->ky || !r->t || !r->field_map || !r->sense_map || !r->data || !r->image_out)
+    return set_error(PG_INVALID_ARG, "submit: null array");
+  if (r->nz > 1 && !r->kz) return set_error(PG_INVALID_ARG, "submit: kz required for 3-D");
+  if (r->nx == 0 || r->ny == 0 || r->nz == 0 || r->nc == 0 || r->n_samples == 0)
+    return set_error(PG_INVALID_ARG, "submit: empty request");
+  auto t = std::make_shared<Ticket>();
+  t->req = *r;
+  if (t->req.n_slices == 0) t->req.n_slices = 1;
+  t->footprint = request_footprint(t->req);
+  t->st.bytes_resident = t->footprint;
+  t->st.status = PG_OK;
+  if (t->footprint > sv->cfg.hbm_budget_bytes)
+    return set_error(PG_REJECTED, "request needs %llu bytes per slice, budget is %llu",
+                     (unsigned long long)t->footprint, (unsigned long long)sv->cfg.hbm_budget_bytes);
+  t->jobs_total = t->jobs_left = (int)t->req.n_slices;
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    if (sv->stop) return set_error(PG_CANCELLED, "server is shutting down");
+    t->id = sv->next++;
+    t->st.t_submit_ms = now_ms();
+    sv->tickets[t->id] = t;
+    for (uint64_t sl = 0; sl < t->req.n_slices; ++sl) sv->pending.push_back(Job{t, sl});
+    *ticket = t->id;
+  }
+  sv->cv_work.notify_all();
+  return PG_OK;
+}
+
+pg_status pg_poll(pg_server sv, uint64_t ticket, pg_request_stats* stats) {
+  if (!sv) return set_error(PG_INVALID_ARG, "poll: null server");
+  std::lock_guard<std::mutex> lk(sv->mu);
+  auto it = sv->tickets.find(ticket);
+  if (it == sv->tickets.end()) return set_error(PG_INVALID_ARG, "poll: unknown ticket %llu", (unsigned long long)ticket);
+  if (!it->second->done) return PG_NOT_READY;
+  if (stats) *stats = it->second->st;
+  return PG_OK;
+}
+
+pg_status pg_wait(pg_server sv, uint64_t ticket, pg_request_stats* stats) {
+  if (!sv) return set_error(PG_INVALID_ARG, "wait: null server");
+  std::unique_lock<std::mutex> lk(sv->mu);
+  auto it = sv->tickets.find(ticket);
+  if (it == sv->tickets.end()) return set_error(PG_INVALID_ARG, "wait: unknown ticket %llu", (unsigned long long)ticket);
+  auto t = it->second;
+  sv->cv_done.wait(lk, [&] { return t->done; });
+  if (stats) *stats = t->st;
+  return PG_OK;
+}
+
+pg_status pg_cancel(pg_server sv, uint64_t ticket) {
+  if (!sv) return set_error(PG_INVALID_ARG, "cancel: null server");
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    auto it = sv->tickets.find(ticket);
+    if (it == sv->tickets.end()) return set_error(PG_INVALID_ARG, "cancel: unknown ticket %llu", (unsigned long long)ticket);
+    auto t = it->second;
+    t->cancel.store(true);
+    // drop this request's queued jobs; running ones stop at their next iteration
+    for (auto i = sv->pending.begin(); i != sv->pending.end();) {
+      if (i->t == t) {
+        if (--t->jobs_left == 0) { t->done = true; t->st.t_done_ms = now_ms(); }
+        i = sv->pending.erase(i);
+      } else {
+        ++i;
+      }
+    }
+    t->st.status = PG_CANCELLED;
+  }
+  sv->cv_done.notify_all();
+  sv->cv_work.notify_all();
+  return PG_OK;
+}
+
+}  // extern "C"

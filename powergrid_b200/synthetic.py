@@ -222,3 +222,79 @@ def config5(seed: int = 5, n: int = 128, nz: int = 64, shots: int = 16, per: int
     return Problem("cfg5", n, n, nz, np.concatenate(kxs), np.concatenate(kys), np.concatenate(kzs),
                    np.concatenate(ts), fm, sm, nc, L, image(rng, n * n * nz), op="pcsense_ts", shots=shots,
                    pmap=pm, penalty="tv", beta=1e-3, delta=0.1, niter=30)
+
+
+@dataclasses.dataclass
+class StreamItem:
+    """One request of a serving stream (config 4) before its data are formed."""
+    arrival_s: float
+    nx: int
+    ny: int
+    nz: int
+    n_slices: int
+    nc: int
+    L: int
+    niter: int
+    beta: float
+    kx: np.ndarray
+    ky: np.ndarray
+    kz: np.ndarray
+    t: np.ndarray
+    fm: np.ndarray        # N, rad/s (shared by the request's slices)
+    smap: np.ndarray      # complex64 N*nc (shared by the request's slices)
+    x_true: np.ndarray    # complex64 N
+
+    @property
+    def nimg(self) -> int:
+        return self.nx * self.ny * self.nz
+
+
+def serving_stream(seed: int = 4, n_requests: int = 16, rate_hz: float = 4.0, small: bool = False,
+                   niter: int = 10):
+    """Seeded config-4 stream: Poisson arrivals at rate_hz; per request an
+    in-plane matrix 64-256 (square), 1-32 slices (2-D) or a 3-D volume, 4-32
+    coils, 8k-200k samples, L = 4-12.  `small=True` shrinks every range (for
+    tests).  Slices of one request share maps and image content."""
+    rng = Rng(seed, 77)
+    items = []
+    t_arr = 0.0
+    for _ in range(n_requests):
+        t_arr += float(-np.log1p(-rng.uniform(1)[0]) / rate_hz)
+        u = rng.uniform(8)
+        three_d = (u[0] < 0.25) and not small
+        if small:
+            n = int(32 + 16 * int(u[1] * 2))            # 32 or 48
+            nz = 1
+            slices = 1 + int(u[2] * 2)
+            nc = 2 + int(u[3] * 3)
+            M = 2048 + int(u[4] * 6144)
+            L = 3 + int(u[5] * 2)
+        elif three_d:
+            n = int(64 + 32 * int(u[1] * 3))            # 64, 96, 128
+            nz = 16 * (1 + int(u[2] * 2))               # 16 or 32
+            slices = 1
+            nc = 4 + int(u[3] * 29)
+            M = 8192 + int(u[4] * (200000 - 8192))
+            L = 4 + int(u[5] * 9)
+        else:
+            n = int(64 + 16 * int(u[1] * 13))           # 64 .. 256
+            nz = 1
+            slices = 1 + int(u[2] * 32)
+            nc = 4 + int(u[3] * 29)
+            M = 8192 + int(u[4] * (200000 - 8192))
+            L = 4 + int(u[5] * 9)
+        t_read = 5e-3 + 20e-3 * float(u[6])
+        amp = 50.0 + 150.0 * float(u[7])
+        if nz == 1:
+            inter = max(1, int(round(M / 8192)))
+            per = max(256, M // inter)
+            kx, ky, t = spiral(n, inter, per, t_read)
+            kz = np.zeros_like(kx)
+        else:
+            per = max(256, M // nz)
+            kx, ky, kz, t = stack_of_spirals(n, nz, 1, per, t_read)
+        fm = field_map(rng, n, n, nz, amp)
+        sm = coil_maps(rng, n, n, nz, nc)
+        x = image(rng, n * n * nz)
+        items.append(StreamItem(t_arr, n, n, nz, slices, nc, L, niter, 1e-3, kx, ky, kz, t, fm, sm, x))
+    return items

@@ -1,0 +1,118 @@
+"""Request server: continuous batching with HBM-footprint admission.
+
+GPU tests check that a request's result is the same whether it runs alone
+or overlapped with others (within the operator tolerance), that requests
+exceeding the budget are rejected, and that cancellation ends a request.
+The footprint model is host-only and tested on CPU.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+MIX_TOL = 1e-5
+
+
+def _requests(pg_mod, items):
+    """Form each request's data with the GPU forward operator of its own geometry."""
+    from powergrid_b200.serve import ReconRequest
+    reqs = []
+    for it in items:
+        M, n = it.kx.size, it.nimg
+        G = pg_mod.Gnufft(M, 2.0, it.nx, it.ny, it.nz, it.kx, it.ky, it.kz)
+        A = pg_mod.TimeSegmentation(G, it.fm, it.t, M, n, it.L, 1, 1)
+        S = pg_mod.SENSE(A, it.smap, M, n, it.nc)
+        y = S * it.x_true
+        reqs.append(ReconRequest(it.nx, it.ny, it.nz, it.nc, it.L, it.niter, it.beta, it.kx, it.ky, it.kz, it.t,
+                                 np.tile(it.fm, it.n_slices), np.tile(it.smap, it.n_slices),
+                                 np.tile(y, it.n_slices), it.n_slices))
+    return reqs
+
+
+def test_footprint_model_is_monotone():
+    from powergrid_b200 import build as B
+    B.build()
+    from powergrid_b200.serve import ReconRequest, Server
+    z = np.zeros(1, np.float32)
+
+    def req(n, nc, M, L):
+        k = np.zeros(M, np.float32)
+        return ReconRequest(n, n, 1, nc, L, 10, 1e-3, k, k, k, k, np.zeros(n * n, np.float32),
+                            np.zeros(n * n * nc, np.complex64), np.zeros(M * nc, np.complex64))
+
+    base = Server.footprint(req(64, 4, 8192, 4))
+    assert base > 0
+    assert Server.footprint(req(128, 4, 8192, 4)) > base
+    assert Server.footprint(req(64, 8, 8192, 4)) > base
+    assert Server.footprint(req(64, 4, 65536, 4)) > base
+    assert Server.footprint(req(64, 4, 8192, 8)) > base
+    _ = z
+
+
+@pytest.mark.gpu
+def test_alone_equals_in_mix(pg):
+    from powergrid_b200 import synthetic as S
+    from powergrid_b200.serve import Server
+    items = S.serving_stream(seed=11, n_requests=6, small=True, niter=5)
+    reqs = _requests(pg, items)
+    alone = []
+    srv1 = Server(hbm_budget_bytes=8 << 30, max_inflight=1)
+    for r in reqs:
+        img, st = srv1.wait(srv1.submit(r))
+        assert st["status"] == "PG_OK" and st["iters_done"] == 5 * r.n_slices
+        alone.append(img.copy())
+    srv1.close()
+    srv = Server(hbm_budget_bytes=8 << 30, max_inflight=6)
+    tickets = [srv.submit(r) for r in reqs]
+    for r, t, a in zip(reqs, tickets, alone):
+        img, st = srv.wait(t)
+        assert st["status"] == "PG_OK"
+        for s in range(r.n_slices):
+            e = rel_l2(img[s], a[s])
+            assert e <= MIX_TOL, e
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_results_match_direct_api(pg):
+    """A served slice equals reconSolve through the operator API."""
+    from powergrid_b200 import synthetic as S
+    from powergrid_b200.serve import Server
+    it = S.serving_stream(seed=12, n_requests=1, small=True, niter=5)[0]
+    r = _requests(pg, [it])[0]
+    srv = Server(hbm_budget_bytes=8 << 30, max_inflight=2)
+    img, st = srv.wait(srv.submit(r))
+    srv.close()
+    M, n = it.kx.size, it.nimg
+    G = pg.Gnufft(M, 2.0, it.nx, it.ny, it.nz, it.kx, it.ky, it.kz)
+    A = pg.TimeSegmentation(G, it.fm, it.t, M, n, it.L, 1, 1)
+    Sg = pg.SENSE(A, it.smap, M, n, it.nc)
+    x = pg.reconSolve(r.data[: M * it.nc], Sg, pg.QuadPenalty(it.nx, it.ny, it.nz, it.beta), niter=5)
+    assert rel_l2(img[0], x) <= MIX_TOL
+
+
+@pytest.mark.gpu
+def test_admission_rejects_oversized_request(pg):
+    from powergrid_b200 import synthetic as S
+    from powergrid_b200._lib import PGError
+    from powergrid_b200.serve import Server
+    r = _requests(pg, S.serving_stream(seed=13, n_requests=1, small=True))[0]
+    srv = Server(hbm_budget_bytes=Server.footprint(r) - 1, max_inflight=2)
+    with pytest.raises(PGError, match="REJECTED"):
+        srv.submit(r)
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_cancel_queued_request(pg):
+    from powergrid_b200 import synthetic as S
+    from powergrid_b200.serve import Server
+    reqs = _requests(pg, S.serving_stream(seed=14, n_requests=3, small=True, niter=20))
+    srv = Server(hbm_budget_bytes=8 << 30, max_inflight=1)
+    t = [srv.submit(r) for r in reqs]
+    srv.cancel(t[2])
+    _, st2 = srv.wait(t[2])
+    assert st2["status"] == "PG_CANCELLED"
+    _, st0 = srv.wait(t[0])
+    assert st0["status"] == "PG_OK"
+    srv.close()
