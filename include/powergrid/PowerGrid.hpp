@@ -1,0 +1,215 @@
+// PowerGrid operator API on the B200 library (header-only C++ over the C ABI
+// in powergrid_b200.h).  Drop-in for the reference's
+//   Gnufft<T1>            Gnufft.h:51-53
+//   Gdft<T1>              Gdft.h:47-49
+//   TimeSegmentation<T1, Tobj>   TimeSegmentation.h:70-71
+//   SENSE<T1, Tobj>       SENSE.h:64
+//   pcSenseTimeSeg<T1>    pcSenseTimeSeg.h:80-82
+//   QuadPenalty<T1>, TVPenalty<T1>   QuadPenalty.h:43, TVPenalty.h:42
+//   solve_pwls_pcg        solve_pwls_pcg.hpp:48-51
+//   reconSolve            reconSolve.h:63-66
+// with T1 = float.  Column types: any type with memptr() (or data()),
+// n_elem (or size()) and a size constructor — arma::Col<std::complex<float>>
+// and arma::Col<float> work unchanged; pg::Col<T> is provided for callers
+// without Armadillo.  operator* / operator/ return new columns.
+//
+// Lifetimes follow the reference: composites keep a non-owning pointer to the
+// operator they wrap (TimeSegmentation.cpp:53, SENSE.cpp:39).  Errors throw
+// pg::Error (the reference printed and called exit(1)).
+#pragma once
+
+#include <complex>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "../powergrid_b200.h"
+
+namespace pg {
+
+typedef unsigned long long uword;
+
+struct Error : std::runtime_error {
+  pg_status status;
+  Error(pg_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+inline void check(pg_status s) {
+  if (s != PG_OK) throw Error(s, std::string(pg_status_string(s)) + ": " + pg_last_error());
+}
+
+// Minimal column vector for callers without Armadillo.
+template <typename T>
+class Col {
+ public:
+  Col() = default;
+  explicit Col(uword n) : v_(n) {}
+  Col(uword n, const T& fill) : v_(n, fill) {}
+  T* memptr() { return v_.data(); }
+  const T* memptr() const { return v_.data(); }
+  uword n_elem_() const { return v_.size(); }
+  T& operator()(uword i) { return v_[i]; }
+  const T& operator()(uword i) const { return v_[i]; }
+  T& operator[](uword i) { return v_[i]; }
+  const T& operator[](uword i) const { return v_[i]; }
+  uword size() const { return v_.size(); }
+
+ private:
+  std::vector<T> v_;
+};
+
+namespace detail {
+template <typename C>
+auto ptr(const C& c) -> decltype(c.memptr()) { return c.memptr(); }
+template <typename C>
+auto mptr(C& c) -> decltype(c.memptr()) { return c.memptr(); }
+template <typename C>
+uword len(const C& c) { return (uword)c.size(); }
+}  // namespace detail
+
+// Common operator base: owns the handle, provides operator* and operator/.
+class Operator {
+ public:
+  Operator(const Operator&) = delete;
+  Operator& operator=(const Operator&) = delete;
+  virtual ~Operator() { if (h_) pg_op_destroy(h_); }
+  pg_op handle() const { return h_; }
+  uword n_data() const { return nd_; }
+  uword n_image() const { return ni_; }
+
+  template <typename CxCol>
+  CxCol operator*(const CxCol& d) const {
+    if (detail::len(d) != ni_) throw Error(PG_INVALID_ARG, "operator*: image length mismatch");
+    CxCol out(nd_);
+    check(pg_op_forward(h_, reinterpret_cast<const float*>(detail::ptr(d)),
+                        reinterpret_cast<float*>(detail::mptr(out))));
+    return out;
+  }
+  template <typename CxCol>
+  CxCol operator/(const CxCol& d) const {
+    if (detail::len(d) != nd_) throw Error(PG_INVALID_ARG, "operator/: data length mismatch");
+    CxCol out(ni_);
+    check(pg_op_adjoint(h_, reinterpret_cast<const float*>(detail::ptr(d)),
+                        reinterpret_cast<float*>(detail::mptr(out))));
+    return out;
+  }
+
+ protected:
+  Operator() = default;
+  void adopt(pg_op h) {
+    h_ = h;
+    uint64_t a = 0, b = 0;
+    check(pg_op_shape(h_, &a, &b));
+    nd_ = a;
+    ni_ = b;
+  }
+  pg_op h_ = nullptr;
+  uword nd_ = 0, ni_ = 0;
+};
+
+template <typename T1>
+class Gnufft : public Operator {
+  static_assert(std::is_same<T1, float>::value, "the B200 path computes in complex64");
+
+ public:
+  template <typename RCol>
+  Gnufft(uword dataLength, T1 gridos, uword nx, uword ny, uword nz, const RCol& k1, const RCol& k2, const RCol& k3,
+         const RCol& /*i1*/, const RCol& /*i2*/, const RCol& /*i3*/) {
+    pg_op h = nullptr;
+    check(pg_gnufft_create(&h, dataLength, gridos, nx, ny, nz, detail::ptr(k1), detail::ptr(k2), detail::ptr(k3)));
+    adopt(h);
+  }
+};
+
+template <typename T1>
+class Gdft : public Operator {
+ public:
+  template <typename RCol>
+  Gdft(uword nk, uword ni, const RCol& k1, const RCol& k2, const RCol& k3, const RCol& i1, const RCol& i2,
+       const RCol& i3, const RCol& FM, const RCol& t) {
+    pg_op h = nullptr;
+    check(pg_gdft_create(&h, nk, ni, detail::ptr(k1), detail::ptr(k2), detail::ptr(k3), detail::ptr(i1),
+                         detail::ptr(i2), detail::ptr(i3), detail::ptr(FM), detail::ptr(t)));
+    adopt(h);
+  }
+};
+
+template <typename T1, typename Tobj>
+class TimeSegmentation : public Operator {
+ public:
+  template <typename RCol>
+  TimeSegmentation(Tobj& G, const RCol& fieldMap, const RCol& timeVec, uword n1, uword n2, uword L,
+                   uword interptype = 1, uword shots = 1) {
+    pg_op h = nullptr;
+    check(pg_timeseg_create(&h, G.handle(), detail::ptr(fieldMap), detail::ptr(timeVec), n1, n2, L, interptype,
+                            shots));
+    adopt(h);
+  }
+};
+
+template <typename T1, typename Tobj>
+class SENSE : public Operator {
+ public:
+  template <typename CxCol>
+  SENSE(Tobj& G, const CxCol& senseMap, uword n1, uword n2, uword nc) {
+    pg_op h = nullptr;
+    check(pg_sense_create(&h, G.handle(), reinterpret_cast<const float*>(detail::ptr(senseMap)), n1, n2, nc));
+    adopt(h);
+  }
+};
+
+template <typename T1>
+class pcSenseTimeSeg : public Operator {
+ public:
+  template <typename RCol, typename CxCol>
+  pcSenseTimeSeg(const RCol& kx, const RCol& ky, const RCol& kz, uword nx, uword ny, uword nz, uword nc,
+                 const RCol& t, uword L, uword intType, const CxCol& SENSEmap, const RCol& FieldMap,
+                 const RCol& ShotPhaseMap) {
+    pg_op h = nullptr;
+    check(pg_pcsense_timeseg_create(&h, detail::ptr(kx), detail::ptr(ky), detail::ptr(kz), detail::len(kx), nx, ny,
+                                    nz, nc, detail::ptr(t), L, intType,
+                                    reinterpret_cast<const float*>(detail::ptr(SENSEmap)), detail::ptr(FieldMap),
+                                    detail::ptr(ShotPhaseMap), detail::len(ShotPhaseMap)));
+    adopt(h);
+  }
+};
+
+template <typename T1>
+struct QuadPenalty {
+  pg_penalty p;
+  QuadPenalty(uword nx, uword ny, uword nz, T1 beta, uword dims2penalize = 3)
+      : p{PG_PENALTY_QUAD, nx, ny, nz, (float)beta, 1.0f, dims2penalize} {}
+};
+
+template <typename T1>
+struct TVPenalty {
+  pg_penalty p;
+  TVPenalty(uword nx, uword ny, uword nz, T1 beta, T1 delta, uword dims2penalize = 3)
+      : p{PG_PENALTY_TV, nx, ny, nz, (float)beta, (float)delta, dims2penalize} {}
+};
+
+// solve_pwls_pcg(xInitial, A, W, yi, R, niter) on the device.
+template <typename T1, typename Tobj, typename Robj, typename CxCol, typename RCol>
+CxCol solve_pwls_pcg(const CxCol& xInitial, const Tobj& A, const RCol& W, const CxCol& yi, const Robj& R,
+                     uword niter) {
+  CxCol x(A.n_image());
+  uint64_t done = 0;
+  check(pg_pcg_solve(A.handle(), reinterpret_cast<const float*>(detail::ptr(xInitial)), detail::ptr(W),
+                     reinterpret_cast<const float*>(detail::ptr(yi)), &R.p, niter,
+                     reinterpret_cast<float*>(detail::mptr(x)), &done));
+  return x;
+}
+
+// reconSolve(data, Sg, R, kx, ky, kz, Nx, Ny, Nz, tvec, niter): W = 1, x0 = 0.
+template <typename T1, typename TObj, typename RObj, typename CxCol, typename RCol>
+CxCol reconSolve(const CxCol& data, TObj& Sg, RObj R, const RCol&, const RCol&, const RCol&, uword, uword, uword,
+                 const RCol&, uword niter) {
+  CxCol x(Sg.n_image());
+  check(pg_recon_solve(Sg.handle(), &R.p, reinterpret_cast<const float*>(detail::ptr(data)), niter,
+                       reinterpret_cast<float*>(detail::mptr(x))));
+  return x;
+}
+
+}  // namespace pg

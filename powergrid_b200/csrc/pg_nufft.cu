@@ -25,6 +25,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <tuple>
 
 #include "pg_nufft.cuh"
 #include "pg_profile.cuh"
@@ -576,8 +578,13 @@ __global__ void k_post(NufftGeom g, int Cb, int L, const float2* __restrict__ gr
 // ---------------------------------------------------------------------------
 // Plan construction
 // ---------------------------------------------------------------------------
+namespace {
+struct FftKey;
+}
+static void fft_release_plan(const NufftGeom& g, int B, cufftHandle h, size_t work);
+
 NufftPlan::~NufftPlan() {
-  for (auto& kv : ffts) cufftDestroy(kv.second);
+  for (auto& kv : ffts) fft_release_plan(g, kv.first, kv.second.first, kv.second.second);
 }
 
 NufftTune NufftTune::defaults() {
@@ -648,8 +655,15 @@ pg_status nufft_plan_create(std::unique_ptr<NufftPlan>* out, uint64_t M, float g
   if (g.Gx > 65535 || g.Gy > 65535 || g.Gz > 65535) return set_error(PG_INVALID_ARG, "Gnufft: grid too large");
   g.os = gridos;
   g.kw = 4.0f;
-  std::vector<float> lut;
-  kb_table(gridos, &lut, &g.beta);
+  // The table depends only on the oversampling factor (fixed at 2 here):
+  // build it once per process.
+  static const std::pair<std::vector<float>, float> kTable = [] {
+    std::pair<std::vector<float>, float> t;
+    kb_table(2.0f, &t.first, &t.second);
+    return t;
+  }();
+  const std::vector<float>& lut = kTable.first;
+  g.beta = kTable.second;
   g.nlut = (int)lut.size();
   const int N3[3] = {nx, ny, nz};
   const int G3[3] = {g.Gx, g.Gy, g.Gz};
@@ -762,6 +776,62 @@ pg_status nufft_build_binning(NufftPlan* p, int L, int K, const int* l0_host, co
 // ---------------------------------------------------------------------------
 // Execution
 // ---------------------------------------------------------------------------
+// Process-wide pool of cuFFT plans keyed by (grid shape, batch).  Plans are
+// created without an internal work area; a NufftPlan checks handles out on
+// first use, supplies its own work area and stream on every execution, and
+// returns them when destroyed, so serving many requests of recurring shapes
+// does not re-plan.
+namespace {
+struct FftKey {
+  int rank, n0, n1, n2, batch;
+  bool operator<(const FftKey& o) const {
+    return std::tie(rank, n0, n1, n2, batch) < std::tie(o.rank, o.n0, o.n1, o.n2, o.batch);
+  }
+};
+std::mutex g_fft_mu;
+std::map<FftKey, std::vector<std::pair<cufftHandle, size_t>>> g_fft_free;
+
+FftKey fft_key(const NufftGeom& g, int B) {
+  return g.dim == 2 ? FftKey{2, g.Gx, g.Gy, 0, B} : FftKey{3, g.Gz, g.Gx, g.Gy, B};
+}
+
+pg_status fft_acquire(const FftKey& k, cufftHandle* h, size_t* work) {
+  {
+    std::lock_guard<std::mutex> lk(g_fft_mu);
+    auto it = g_fft_free.find(k);
+    if (it != g_fft_free.end() && !it->second.empty()) {
+      *h = it->second.back().first;
+      *work = it->second.back().second;
+      it->second.pop_back();
+      return PG_OK;
+    }
+  }
+  cufftHandle hh;
+  PG_CUFFT(cufftCreate(&hh));
+  int n[3] = {k.n0, k.n1, k.n2};
+  const int G = k.n0 * k.n1 * (k.rank == 3 ? k.n2 : 1);
+  size_t w = 0;
+  cufftResult r = cufftSetAutoAllocation(hh, 0);
+  if (r == CUFFT_SUCCESS) r = cufftMakePlanMany(hh, k.rank, n, nullptr, 1, G, nullptr, 1, G, CUFFT_C2C, k.batch, &w);
+  if (r != CUFFT_SUCCESS) {
+    cufftDestroy(hh);
+    return set_error(r == CUFFT_ALLOC_FAILED ? PG_OUT_OF_MEMORY : PG_CUFFT_ERROR, "cufftMakePlanMany: %d", (int)r);
+  }
+  *h = hh;
+  *work = w;
+  return PG_OK;
+}
+
+void fft_release(const FftKey& k, cufftHandle h, size_t work) {
+  std::lock_guard<std::mutex> lk(g_fft_mu);
+  g_fft_free[k].emplace_back(h, work);
+}
+}  // namespace
+
+static void fft_release_plan(const NufftGeom& g, int B, cufftHandle h, size_t work) {
+  fft_release(fft_key(g, B), h, work);
+}
+
 static pg_status ensure_workspace(NufftPlan* p, int B, cufftHandle* h, cudaStream_t s) {
   const uint64_t G = p->g.ngrid();
   if (p->grids.n < (uint64_t)B * G) {
@@ -771,28 +841,19 @@ static pg_status ensure_workspace(NufftPlan* p, int B, cufftHandle* h, cudaStrea
   auto it = p->ffts.find(B);
   if (it == p->ffts.end()) {
     cufftHandle hh;
-    PG_CUFFT(cufftCreate(&hh));
-    int n[3];
-    int rank;
-    if (p->g.dim == 2) { rank = 2; n[0] = p->g.Gx; n[1] = p->g.Gy; }
-    else { rank = 3; n[0] = p->g.Gz; n[1] = p->g.Gx; n[2] = p->g.Gy; }
     size_t work = 0;
-    PG_CUFFT(cufftSetAutoAllocation(hh, 0));
-    cufftResult r = cufftMakePlanMany(hh, rank, n, nullptr, 1, (int)G, nullptr, 1, (int)G, CUFFT_C2C, B, &work);
-    if (r != CUFFT_SUCCESS) {
-      cufftDestroy(hh);
-      return set_error(r == CUFFT_ALLOC_FAILED ? PG_OUT_OF_MEMORY : PG_CUFFT_ERROR, "cufftMakePlanMany: %d", (int)r);
-    }
+    PG_TRY(fft_acquire(fft_key(p->g, B), &hh, &work));
     if (work > p->fft_work.n) {
       // the old area may still be in use by queued transforms of this plan
       PG_CUDA(cudaStreamSynchronize(s));
-      PG_TRY(p->fft_work.alloc(work));
+      pg_status st = p->fft_work.alloc(work);
+      if (st != PG_OK) { fft_release(fft_key(p->g, B), hh, work); return st; }
     }
-    it = p->ffts.emplace(B, hh).first;
+    it = p->ffts.emplace(B, std::make_pair(hh, work)).first;
   }
-  PG_CUFFT(cufftSetWorkArea(it->second, p->fft_work.p));
-  PG_CUFFT(cufftSetStream(it->second, s));
-  *h = it->second;
+  PG_CUFFT(cufftSetWorkArea(it->second.first, p->fft_work.p));
+  PG_CUFFT(cufftSetStream(it->second.first, s));
+  *h = it->second.first;
   return PG_OK;
 }
 

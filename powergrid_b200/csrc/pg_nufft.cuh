@@ -75,7 +75,7 @@ struct NufftPlan {
   std::unique_ptr<Binning> plain;  // binning without segmentation (L = 1)
   // grid workspace and cuFFT plans, keyed by batch size
   DevBuf<float2> grids;
-  std::map<int, cufftHandle> ffts;
+  std::map<int, std::pair<cufftHandle, size_t>> ffts;  // batch -> (pooled plan, work bytes)
   DevBuf<char> fft_work;
   size_t budget_bytes = 8ull << 30;  // grid workspace limit per plan
   ~NufftPlan();

@@ -96,18 +96,35 @@ pg_status build_ts_tables(const float* field_map, const float* tvec, uint64_t n1
     T.l0[m] = s;
     for (int q = 0; q < K; ++q) T.aa_win[m * K + q] = T.AA[m + n1 * (s + q)];
   }
-  // Wo / WoH (:213-218): exp(-/+ i * fieldMap * (l*tau + T_min)).
-  T.Wo.resize(n2 * (uint64_t)L);
-  T.WoH.resize(n2 * (uint64_t)L);
-  for (unsigned int l = 0; l < (unsigned)L; ++l) {
-    const float sft = (l) * T.tau + T.tmin;
-    for (uint64_t p = 0; p < n2; ++p) {
-      const float v = field_map[p] * sft;
-      const float c = std::cos(v), sn = std::sin(v);
-      T.Wo[p + n2 * l] = make_float2(c, -sn);
-      T.WoH[p + n2 * l] = make_float2(c, sn);
-    }
-  }
+  return PG_OK;
+}
+
+// Wo / WoH (TimeSegmentation.cpp:213-218): exp(-/+ i * fieldMap * (l*tau + T_min)),
+// l < L, evaluated on the device (the host loop over N x L sincos dominated
+// operator set-up).  sincosf is the accurate CUDA routine, not the fast
+// intrinsic; the argument is formed with the reference's float rounding.
+__global__ void k_ts_phases(uint64_t n2, int L, float tau, float tmin, const float* __restrict__ fm,
+                            float2* __restrict__ Wo, float2* __restrict__ WoH) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n2 * (uint64_t)L) return;
+  const unsigned int l = (unsigned int)(i / n2);
+  const uint64_t p = i % n2;
+  const float sft = __fadd_rn(__fmul_rn((float)l, tau), tmin);
+  const float v = __fmul_rn(fm[p], sft);
+  float sn, c;
+  sincosf(v, &sn, &c);
+  Wo[i] = make_float2(c, -sn);
+  WoH[i] = make_float2(c, sn);
+}
+
+pg_status build_ts_phases(const TsTables& T, const float* field_map, uint64_t n2, DevBuf<float2>* Wo,
+                          DevBuf<float2>* WoH, cudaStream_t s) {
+  DevBuf<float> fm;
+  PG_TRY(fm.upload(field_map, n2, s));
+  PG_TRY(Wo->alloc(n2 * (uint64_t)T.L));
+  PG_TRY(WoH->alloc(n2 * (uint64_t)T.L));
+  PG_LAUNCH(k_ts_phases, ceil_div(n2 * (uint64_t)T.L, 256), 256, 0, s, n2, T.L, T.tau, T.tmin, fm.p, Wo->p, WoH->p);
+  PG_CUDA(cudaStreamSynchronize(s));  // fm is released on return
   return PG_OK;
 }
 
@@ -309,8 +326,7 @@ pg_status make_timeseg(std::unique_ptr<TimeSegOp>* out, pg_op_s* G, const float*
   op->n_image = n2;
   PG_TRY(build_ts_tables(field_map, tvec, n1, n2, L, interptype, shots, &op->tab));
   if (op->tab.L > 1) {
-    PG_TRY(op->Wo.upload(op->tab.Wo.data(), op->tab.Wo.size(), s));
-    PG_TRY(op->WoH.upload(op->tab.WoH.data(), op->tab.WoH.size(), s));
+    PG_TRY(build_ts_phases(op->tab, field_map, n2, &op->Wo, &op->WoH, s));
     if (G->kind == PG_OP_GNUFFT) {
       PG_TRY(make_binning_for(static_cast<GnufftOp*>(G)->plan.get(), op->tab, &op->bin, s));
     } else {
@@ -320,8 +336,6 @@ pg_status make_timeseg(std::unique_ptr<TimeSegOp>* out, pg_op_s* G, const float*
   PG_CUDA(cudaStreamSynchronize(s));
   // host tables are only needed to build the device ones
   op->tab.AA.clear(); op->tab.AA.shrink_to_fit();
-  op->tab.Wo.clear(); op->tab.Wo.shrink_to_fit();
-  op->tab.WoH.clear(); op->tab.WoH.shrink_to_fit();
   *out = std::move(op);
   return PG_OK;
 }
@@ -420,8 +434,7 @@ pg_status pg_pcsense_timeseg_create(pg_op* out, const float* kx, const float* ky
     PG_TRY(nufft_plan_create(&plan, Nd, 2.0f, (int)nx, (int)ny, (int)nz, kx + sh * Nd, ky + sh * Nd, kz + sh * Nd, s));
     PG_TRY(build_ts_tables(field_map, t + sh * Nd, Nd, Ni, L, interptype, 1, &op->tabs[sh]));
     if (op->tabs[sh].L > 1) {
-      PG_TRY(op->Wo[sh].upload(op->tabs[sh].Wo.data(), op->tabs[sh].Wo.size(), s));
-      PG_TRY(op->WoH[sh].upload(op->tabs[sh].WoH.data(), op->tabs[sh].WoH.size(), s));
+      PG_TRY(build_ts_phases(op->tabs[sh], field_map, Ni, &op->Wo[sh], &op->WoH[sh], s));
       PG_TRY(make_binning_for(plan.get(), op->tabs[sh], &op->bins[sh], s));
       op->tabs[sh].AA.clear();
       op->tabs[sh].AA.shrink_to_fit();

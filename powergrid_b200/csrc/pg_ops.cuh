@@ -40,8 +40,10 @@ struct TsTables {
   std::vector<float2> AA;       // n1 x L (column l contiguous) — full table
   std::vector<int> l0;          // per sample window start
   std::vector<float2> aa_win;   // per sample K values
-  std::vector<float2> Wo, WoH;  // L x n2
 };
+// Segment phases Wo / WoH (L x n2) on the device.
+pg_status build_ts_phases(const TsTables& T, const float* field_map, uint64_t n2, DevBuf<float2>* Wo,
+                          DevBuf<float2>* WoH, cudaStream_t s);
 pg_status build_ts_tables(const float* field_map, const float* tvec, uint64_t n1, uint64_t n2, uint64_t L,
                           uint64_t interptype, uint64_t shots, TsTables* out);
 

@@ -1,0 +1,62 @@
+// Drives the C++ operator API (include/powergrid/PowerGrid.hpp) the way the
+// reference's PowerGridIsmrmrd driver does (PowerGridIsmrmrd.cpp:244-264):
+// Gnufft -> TimeSegmentation -> SENSE -> operator*, operator/, reconSolve.
+// Inputs and outputs are raw little-endian files in the directory argv[1]
+// (written and checked by tests/test_cpp_api.py).
+#include <complex>
+#include <cstdio>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "powergrid/PowerGrid.hpp"
+
+using cx = std::complex<float>;
+
+template <typename T>
+pg::Col<T> load(const std::string& path, pg::uword n) {
+  pg::Col<T> c(n);
+  std::ifstream f(path, std::ios::binary);
+  f.read(reinterpret_cast<char*>(c.memptr()), n * sizeof(T));
+  if (!f) throw std::runtime_error("cannot read " + path);
+  return c;
+}
+
+template <typename T>
+void save(const std::string& path, const pg::Col<T>& c) {
+  std::ofstream f(path, std::ios::binary);
+  f.write(reinterpret_cast<const char*>(c.memptr()), c.size() * sizeof(T));
+}
+
+int main(int argc, char** argv) {
+  if (argc < 2) return 2;
+  const std::string d = argv[1];
+  std::ifstream meta(d + "/meta.txt");
+  pg::uword nx, ny, nz, M, L, nc, niter;
+  float beta;
+  meta >> nx >> ny >> nz >> M >> L >> nc >> niter >> beta;
+  const pg::uword N = nx * ny * nz;
+  try {
+    auto kx = load<float>(d + "/kx.bin", M), ky = load<float>(d + "/ky.bin", M), kz = load<float>(d + "/kz.bin", M);
+    auto t = load<float>(d + "/t.bin", M);
+    auto fm = load<float>(d + "/fm.bin", N);
+    auto sm = load<cx>(d + "/smap.bin", N * nc);
+    auto x = load<cx>(d + "/x.bin", N);
+    auto data = load<cx>(d + "/data.bin", M * nc);
+    pg::Col<float> ix(N), iy(N), iz(N);
+    pg::Gnufft<float> G(M, 2.0f, nx, ny, nz, kx, ky, kz, ix, iy, iz);
+    pg::TimeSegmentation<float, pg::Gnufft<float>> A(G, fm, t, M, N, L, 1, 1);
+    pg::SENSE<float, pg::TimeSegmentation<float, pg::Gnufft<float>>> S(A, sm, M, N, nc);
+    pg::QuadPenalty<float> R(nx, ny, nz, beta);
+    pg::Col<cx> y = S * x;
+    pg::Col<cx> xa = S / data;
+    pg::Col<cx> img = pg::reconSolve<float>(data, S, R, kx, ky, kz, nx, ny, nz, t, niter);
+    save(d + "/y_out.bin", y);
+    save(d + "/xadj_out.bin", xa);
+    save(d + "/img_out.bin", img);
+  } catch (const pg::Error& e) {
+    std::fprintf(stderr, "pg error: %s\n", e.what());
+    return 1;
+  }
+  return 0;
+}

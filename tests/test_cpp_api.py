@@ -1,0 +1,47 @@
+"""The header-only C++ operator API, compiled here with g++ and run on the GPU."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+SRC = os.path.join(ROOT, "tests", "cpp", "recon_api.cpp")
+LIBDIR = os.path.join(ROOT, "powergrid_b200", "lib")
+
+
+def _build(outdir):
+    exe = os.path.join(outdir, "recon_api")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I" + os.path.join(ROOT, "include"), SRC, "-o", exe,
+                    "-L" + LIBDIR, "-lpowergrid_b200", "-Wl,-rpath," + LIBDIR], check=True)
+    return exe
+
+
+def test_cpp_api_compiles(tmp_path):
+    from powergrid_b200 import build as B
+    B.build()
+    assert os.path.exists(_build(str(tmp_path)))
+
+
+@pytest.mark.gpu
+def test_cpp_api_matches_reference_fixture(pg, tmp_path):
+    d = np.load(os.path.join(ROOT, "tests", "golden", "pcg2d.npz"))
+    c = {k: d[k] for k in d.files}
+    nx, ny, nz, L, nc, niter = (int(c[k]) for k in ("nx", "ny", "nz", "L", "nc", "niter"))
+    M = c["kx"].size
+    out = str(tmp_path)
+    with open(os.path.join(out, "meta.txt"), "w") as f:
+        f.write(f"{nx} {ny} {nz} {M} {L} {nc} {niter} {float(c['beta'])}\n")
+    for k, dt in (("kx", np.float32), ("ky", np.float32), ("kz", np.float32), ("t", np.float32),
+                  ("fm", np.float32), ("smap", np.complex64), ("x", np.complex64)):
+        np.ascontiguousarray(c[k], dtype=dt).tofile(os.path.join(out, k + ".bin"))
+    np.ascontiguousarray(c["y_f32"], dtype=np.complex64).tofile(os.path.join(out, "data.bin"))
+    exe = _build(out)
+    subprocess.run([exe, out], check=True)
+    y = np.fromfile(os.path.join(out, "y_out.bin"), np.complex64)
+    img = np.fromfile(os.path.join(out, "img_out.bin"), np.complex64)
+    t = np.load(os.path.join(ROOT, "tests", "golden", "tssense2d.npz"))
+    assert rel_l2(y, t["y_f32"]) <= 1e-5          # same geometry and image as the tssense2d fixture
+    assert rel_l2(img, c["x_pcg_f32"]) <= 1e-4    # reconSolve, 5 iterations
