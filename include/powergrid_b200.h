@@ -105,6 +105,23 @@ pg_status pg_op_adjoint(pg_op op, const float* y, float* x);
 pg_status pg_op_forward_device(pg_op op, const void* x_dev, void* y_dev, void* stream);
 pg_status pg_op_adjoint_device(pg_op op, const void* y_dev, void* x_dev, void* stream);
 
+/* y = Gdft * x for one coil, computed without allocating any device memory.
+ * No counterpart in the reference: it exists for callers that manage all
+ * device memory themselves (their own pool or a fixed budget) or that must
+ * not meet cudaMalloc's implicit synchronisation or an allocation failure
+ * mid-run.  Every pointer is a DEVICE pointer owned by the caller: the
+ * operator's inputs as for pg_gdft_create (nk samples, ni voxels), x (ni
+ * complex) and y (nk complex).  Scratch lives in a fixed 4 MiB device array
+ * held by every GPU that loads the library until exit, so nk is limited to
+ * 524288 samples (larger sizes return PG_INVALID_ARG).  The array is shared
+ * by all calls: calls whose work overlaps on the GPU race and must be
+ * ordered by the caller.  The first call on each device looks up the array's
+ * device address; make that first call before any stream capture.
+ * Stream-ordered on `stream` (NULL = the library's stream). */
+pg_status pg_gdft_forward_noalloc(uint64_t nk, uint64_t ni, const float* kx, const float* ky, const float* kz,
+                                  const float* ix, const float* iy, const float* iz, const float* field_map,
+                                  const float* t, const void* x_dev, void* y_dev, void* stream);
+
 /* ---- regularizers and solver ----------------------------------------- */
 typedef enum pg_penalty_kind { PG_PENALTY_QUAD = 0, PG_PENALTY_TV = 1 } pg_penalty_kind;
 

@@ -67,6 +67,7 @@ SIGNATURES = {
     "pg_op_adjoint": (C.c_int, [P, P, P]),
     "pg_op_forward_device": (C.c_int, [P, P, P, P]),
     "pg_op_adjoint_device": (C.c_int, [P, P, P, P]),
+    "pg_gdft_forward_noalloc": (C.c_int, [U64, U64, P, P, P, P, P, P, P, P, P, P, P]),
     "pg_pcg_solve": (C.c_int, [P, P, P, P, C.POINTER(Penalty), U64, P, C.POINTER(U64)]),
     "pg_pcg_solve_device": (C.c_int, [P, P, P, P, C.POINTER(Penalty), U64, P, P, P]),
     "pg_recon_solve": (C.c_int, [P, C.POINTER(Penalty), P, U64, P]),
