@@ -370,18 +370,22 @@ def run_serving(n_requests: int = 16, rate_hz: float = 20.0, inflight: int = 8, 
             if delay > 0:
                 time.sleep(delay)
             tickets.append(srv.submit(r))
-        lat, iters, done = [], 0, 0.0
+        lat, iters, done, setup, solve = [], 0, 0.0, 0.0, 0.0
         for t in tickets:
             _, st = srv.wait(t)
             assert st["status"] == "PG_OK", st
             lat.append(st["t_done_ms"] - st["t_submit_ms"])
             iters += st["iters_done"]
             done = max(done, st["t_done_ms"])
+            setup += st["setup_ms"]
+            solve += st["solve_ms"]
         makespan = time.perf_counter() - t0
         srv.close()
         lat.sort()
+        jobs = sum(r.n_slices for r in reqs)
         return {"iters_per_s": iters / makespan, "makespan_s": makespan, "iterations": iters,
-                "latency_ms_p50": lat[len(lat) // 2], "latency_ms_p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]}
+                "latency_ms_p50": lat[len(lat) // 2], "latency_ms_p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+                "mean_job_setup_ms": setup / jobs, "mean_job_solve_ms": solve / jobs}
 
     serve(inflight)  # warm-up: module loading, pool growth
     plain = serve(1)
@@ -395,6 +399,111 @@ def run_serving(n_requests: int = 16, rate_hz: float = 20.0, inflight: int = 8, 
             "speedup_iters_per_s": served["iters_per_s"] / plain["iters_per_s"]}
 
 
+def run_workload(name: str, steps: int, warmup: int):
+    """Secondary workloads, one JSON line each (parity cases elsewhere, measured here).
+
+    cfg3: SENSE<Gdft> 64x64x32, 8 coils, 131072 samples; per step one forward and
+          one adjoint; reports sample-voxel pairs/s per direction.
+    cfg5: pcSenseTimeSeg 128x128x64, 16 shots x 131072 samples, 32 coils, L=12,
+          TVPenalty; PCG iterations/s over one solve of `niter` iterations.
+    """
+    import ctypes as C
+
+    import torch
+
+    import powergrid_b200 as pg
+    from powergrid_b200 import _lib
+    from powergrid_b200 import synthetic as S
+    from powergrid_b200._lib import check
+
+    pg.init(0)
+    dev = torch.device("cuda", 0)
+    L = _lib.load()
+    stream = torch.cuda.Stream(device=dev)
+    sampler = ClockSampler(0)
+    if name == "cfg3":
+        p = S.config3()
+        M, n = p.kx.size, p.nimg
+        ix, iy, iz = S.image_coords(p.nx, p.ny, p.nz)
+        G = pg.Gdft(M, n, p.kx, p.ky, p.kz, ix, iy, iz, p.fm, p.t)
+        Sg = pg.SENSE(G, p.smap, M, n, p.nc)
+        x = torch.from_numpy(p.x_true).to(dev)
+        y = torch.empty(Sg.n_data, dtype=torch.complex64, device=dev)
+        xa = torch.empty(n, dtype=torch.complex64, device=dev)
+        torch.cuda.synchronize()
+        for _ in range(warmup):
+            Sg.forward(x, out=y, stream=stream)
+            Sg.adjoint(y, out=xa, stream=stream)
+        stream.synchronize()
+        fwd, adj = [], []
+        with sampler:
+            for _ in range(steps):
+                e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+                e[0].record(stream)
+                Sg.forward(x, out=y, stream=stream)
+                e[1].record(stream)
+                Sg.adjoint(y, out=xa, stream=stream)
+                e[2].record(stream)
+                stream.synchronize()
+                fwd.append(e[0].elapsed_time(e[1]))
+                adj.append(e[1].elapsed_time(e[2]))
+        pairs = float(M) * n
+        tf, ta = statistics.mean(fwd), statistics.mean(adj)
+        return {"workload": "cfg3 SENSE<Gdft> 64x64x32, 8 coils, 131072 samples, +-150 Hz, 0-25 ms readout",
+                "metric": "sample-voxel pairs/s per direction (8 coils per pair)", "steps": steps, "warmup": warmup,
+                "forward_ms": tf, "adjoint_ms": ta, "forward_pairs_per_s": pairs / (tf / 1e3),
+                "adjoint_pairs_per_s": pairs / (ta / 1e3), "clocks": sampler.summary()}
+    if name == "cfg5":
+        p = S.config5()
+        op = pg.pcSenseTimeSeg(p.kx, p.ky, p.kz, p.nx, p.ny, p.nz, p.nc, p.t, p.L, 1, p.smap, p.fm, p.pmap)
+        R = pg.TVPenalty(p.nx, p.ny, p.nz, p.beta, p.delta)
+        x = torch.from_numpy(p.x_true).to(dev)
+        y = torch.empty(op.n_data, dtype=torch.complex64, device=dev)
+        torch.cuda.synchronize()
+        op.forward(x, out=y, stream=stream)
+        stream.synchronize()
+        # The solver's |denominator| guard (1e25) is scale dependent and the
+        # unnormalised 3-D operator is large: scale the data so that the first
+        # line-search denominator ||A A' y||^2 is 1.
+        g = torch.empty(p.nimg, dtype=torch.complex64, device=dev)
+        op.adjoint(y, out=g, stream=stream)
+        Ag = torch.empty_like(y)
+        op.forward(g, out=Ag, stream=stream)
+        stream.synchronize()
+        y /= float(torch.sqrt(torch.sum(torch.abs(Ag).double() ** 2)))
+        del g, Ag
+        xo = torch.empty(p.nimg, dtype=torch.complex64, device=dev)
+        it = torch.zeros(1, dtype=torch.int32, device=dev)
+        torch.cuda.synchronize()
+        for _ in range(warmup):
+            pg.solve_pwls_pcg_device(op, y, R, 2, xo, iters=it, stream=stream)
+        stream.synchronize()
+        ms, done = [], 0
+        check(L.pg_profile_enable(1))
+        with sampler:
+            for _ in range(steps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                pg.solve_pwls_pcg_device(op, y, R, p.niter, xo, iters=it, stream=stream)
+                e1.record(stream)
+                stream.synchronize()
+                ms.append(e0.elapsed_time(e1))
+                done += int(it.item())
+        stages = {}
+        for k in ["pre", "fft_fwd", "gather", "zero", "spread", "fft_adj", "post"]:
+            v = C.c_float()
+            if L.pg_profile_stage_ms(k.encode(), C.byref(v)) == 0:
+                stages[k] = v.value
+        check(L.pg_profile_enable(0))
+        return {"workload": "cfg5 pcSenseTimeSeg 128x128x64, 16 shots x 131072 samples, 32 coils, L=12, "
+                            f"TVPenalty (beta {p.beta}, delta {p.delta}), data scaled so that the first "
+                            f"line-search denominator is 1, {p.niter} PCG iterations",
+                "metric": METRIC, "unit": UNIT, "value": done / (sum(ms) / 1e3), "iterations": done,
+                "ms_per_solve": statistics.mean(ms), "steps": steps, "warmup": warmup,
+                "stage_ms_last_launch": stages, "clocks": sampler.summary()}
+    raise SystemExit(f"unknown workload {name}")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -404,7 +513,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the config-4 serving stream")
     ap.add_argument("--serving-only", action="store_true", help="only the config-4 serving stream")
+    ap.add_argument("--workload", default=None, choices=["cfg3", "cfg5"], help="a secondary workload instead")
     args = ap.parse_args()
+    if args.workload:
+        print(json.dumps(run_workload(args.workload, args.steps, max(3, args.warmup))))
+        return 0
     if args.serving_only:
         import powergrid_b200 as pg
         pg.init(0)

@@ -191,6 +191,8 @@ typedef struct pg_request_stats {
   uint64_t iters_done;                         /* PCG iterations completed, all slices */
   uint64_t bytes_resident;                     /* admission footprint of one slice job */
   pg_status status;
+  double setup_ms;                             /* summed over slices: operator construction on the host */
+  double solve_ms;                             /* summed over slices: PCG solve and image copy-out */
 } pg_request_stats;
 
 pg_status pg_server_create(pg_server* out, const pg_server_config* cfg);

@@ -390,32 +390,50 @@ __global__ void __launch_bounds__(256) k_gather(NufftGeom g, TileShape t, const 
 }
 
 // ---------------------------------------------------------------------------
-// Adjoint spread: one block per (subproblem, coil chunk) into a padded
-// shared-memory tile, then each nonzero tile cell is flushed to the centred
-// grid with one vector atomic.  Shared accumulation is 32-bit fixed point
-// with native integer atomics (float shared atomics are compare-and-swap
-// loops): each (coil, segment) plane gets a power-of-two scale 2^e from the
-// bound B = wmax^d * sum_s |v_s| (|v| <= |re| + |im|) on any cell's
-// magnitude, with 2^30 headroom, so no partial sum can overflow and the
-// tile sums do not depend on the order of the atomics.  The quantisation
-// step is <= B / 2^29 per contribution.
-// Layout [coil][segment][re|im][PZ][PX][PY], PY = 8 (mod 32): a warp's 32
-// lanes (8 y-taps x 4 x-taps) hit 32 distinct banks.
+// Adjoint spread: one block per (subproblem, coil chunk).
+//  1. The subproblem's samples are staged in shared memory with coalesced
+//     loads: tap starts, tap weights and, per (coil, segment) plane, the value
+//     v = conj(AA) * y the sample spreads.
+//  2. Each plane gets a power-of-two scale 2^e from the largest |re| or |im|
+//     of its values, chosen so that every single contribution w * v * 2^e is
+//     below 2^22 in magnitude and the sum of all of them in one cell (at most
+//     one per sample, at most 256 << extra samples) stays below 2^30.
+//  3. A warp spreads one sample at a time into the padded tile, lane =
+//     (y-tap, x-tap pair), with 32-bit integer shared atomics (native, unlike
+//     float shared atomics).  The integer of a contribution is formed by one
+//     fma against the constant 1.5 * 2^23: for |x| < 2^22 the sum lands in
+//     [2^23, 2^24), where the float grid spacing is 1, so the fma rounds w*v
+//     to the nearest integer, held in the low mantissa bits.  Integer sums do
+//     not depend on the order of the atomics, so the result is deterministic.
+//  4. Each nonzero tile cell is flushed to the centred grid with one vector
+//     atomic, scaled back by 2^-e.
+// Tile layout [coil][segment][re|im][PZ][PX][PY], PY = 8 (mod 32): a warp's
+// 32 lanes (8 y-taps x 4 x-taps) hit 32 distinct banks.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ int fixed_point(float w, float v) {
+  constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23, float bits 0x4B400000
+  return __float_as_int(__fmaf_rn(w, v, kMagic)) - 0x4B400000;
+}
+
+// Staged weights per sample in the spread: wx[8], wy[8] and, in 3-D, wz[8].
+__host__ __device__ constexpr int spread_wrow(int dim) { return dim == 2 ? 16 : 24; }
+
 template <int DIM>
 __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const int4* __restrict__ sub,
                                                 const uint2* __restrict__ start, const float* __restrict__ wxy,
                                                 const float* __restrict__ wz, const uint32_t* __restrict__ perm,
                                                 const float2* __restrict__ aa, int K, int L,
                                                 const float2* __restrict__ data, uint64_t dstride, int Cb,
-                                                int Cc, float wmax, float2* __restrict__ grids) {
-  extern __shared__ int smi[];
-  __shared__ float bound[16];
+                                                int Cc, int smax, float wmax, float2* __restrict__ grids) {
+  constexpr int WROW = spread_wrow(DIM);   // staged weights per sample: wx[8] wy[8] (wz[8])
+  extern __shared__ __align__(16) int smi[];
+  __shared__ unsigned vmax[16];
   __shared__ float scale[16], inv_scale[16];
   const int4 sp = sub[blockIdx.x];
   const int cfirst = blockIdx.y * Cc;
   const int ncl = min(Cc, Cb - cfirst);
-  const int tile = sp.x, lseg = sp.y, first = sp.z, count = sp.w;
+  const int tile = sp.x, first = sp.z, count = sp.w;
+  const int lseg = sp.y;
   const int ty = tile % t.nty;
   const int txz = tile / t.nty;
   const int tx = txz % t.ntx;
@@ -423,98 +441,110 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
   const int x0 = tx * t.TX, y0 = ty * t.TY, z0 = tz * t.TZ;
   const int cells = t.PX * t.PY * t.PZ;
   const int nplane = ncl * K;          // complex planes in use (<= 16)
-  for (int q = threadIdx.x; q < nplane * 2 * cells; q += blockDim.x) smi[q] = 0;
-  if (threadIdx.x < 16) bound[threadIdx.x] = 0.f;
+  const int tid = threadIdx.x;
+  float* sw = reinterpret_cast<float*>(smi + (size_t)nplane * 2 * cells);
+  float2* sv = reinterpret_cast<float2*>(sw + (size_t)smax * WROW);
+  uint2* sst = reinterpret_cast<uint2*>(sv + (size_t)smax * nplane);
+
+  {
+    int4* z = reinterpret_cast<int4*>(smi);
+    for (int q = tid; q < (nplane * 2 * cells) / 4; q += blockDim.x) z[q] = make_int4(0, 0, 0, 0);
+  }
+  if (tid < 16) vmax[tid] = 0u;
   __syncthreads();
 
-  // per-plane bound: sum over the subproblem's samples of |v| (<= |re|+|im|)
-  {
-    float loc[16];
-#pragma unroll
-    for (int i = 0; i < 16; ++i) loc[i] = 0.f;
-    for (int s = first + threadIdx.x; s < first + count; s += blockDim.x) {
-      const uint32_t orig = perm[s];
-      for (int c = 0; c < ncl; ++c) {
-        const float2 d = data[(uint64_t)(cfirst + c) * dstride + orig];
-        const float m = fabsf(d.x) + fabsf(d.y);
-        for (int j = 0; j < K; ++j) {
-          const float2 a = aa ? aa[(uint64_t)s * K + j] : make_float2(1.f, 0.f);
-          loc[c * K + j] += m * (fabsf(a.x) + fabsf(a.y));
-        }
-      }
-    }
-    const int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      float v = loc[i];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-      if (lane == 0 && i < nplane && v > 0.f) atomicAdd(&bound[i], v);
-    }
+  // 1. staging
+  constexpr int R4 = WROW / 4;
+  for (int q = tid; q < count * R4; q += blockDim.x) {
+    const int i = q / R4, a = q % R4;
+    float4 val;
+    if (a < 4)
+      val = reinterpret_cast<const float4*>(wxy + (uint64_t)(first + i) * 16)[a];
+    else
+      val = reinterpret_cast<const float4*>(wz + (uint64_t)(first + i) * 8)[a - 4];
+    reinterpret_cast<float4*>(sw + i * WROW)[a] = val;
+  }
+  for (int i = tid; i < count; i += blockDim.x) sst[i] = start[first + i];
+  for (int q = tid; q < count * nplane; q += blockDim.x) {
+    const int i = q / nplane, pl = q % nplane;
+    const int c = pl / K, j = pl % K;
+    const int s = first + i;
+    const float2 d = data[(uint64_t)(cfirst + c) * dstride + perm[s]];
+    const float2 v = aa ? cmul(cconj(aa[(uint64_t)s * K + j]), d) : d;
+    sv[q] = v;
+    // non-negative floats order like their bit patterns
+    atomicMax(&vmax[pl], __float_as_uint(fmaxf(fabsf(v.x), fabsf(v.y))));
   }
   __syncthreads();
-  if (threadIdx.x < 16) {
-    const float B = bound[threadIdx.x] * wmax * 1.0001f;
+
+  // 2. per-plane scale
+  if (tid < 16) {
+    int extra = 0;
+    while (count > (256 << extra)) ++extra;
+    const float B = __uint_as_float(vmax[tid]) * wmax * 1.0001f;
     int e = 0;
     if (B > 0.f) {
       frexpf(B, &e);                       // B < 2^e
-      e = 30 - e;                          // B * 2^e' < 2^30
+      e = 22 - e - extra;                  // B * 2^e' < 2^(22 - extra)
     }
-    scale[threadIdx.x] = ldexpf(1.f, e);
-    inv_scale[threadIdx.x] = ldexpf(1.f, -e);
+    scale[tid] = ldexpf(1.f, e);
+    inv_scale[tid] = ldexpf(1.f, -e);
+  }
+  __syncthreads();
+  for (int q = tid; q < count * nplane; q += blockDim.x) {
+    const float sc = scale[q % nplane];
+    const float2 v = sv[q];
+    sv[q] = make_float2(v.x * sc, v.y * sc);
   }
   __syncthreads();
 
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  // 3. spread
+  const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
   const int dy = lane & 7, dx = lane >> 3;
   const int plane = t.PX * t.PY;
-  for (int s = first + warp; s < first + count; s += nw) {
-    const uint2 st = start[s];
+  for (int i = warp; i < count; i += nw) {
+    const uint2 st = sst[i];
     const int ox = (int)(st.x & 0xffff) - x0, oy = (int)(st.x >> 16) - y0;
-    const int oz = (DIM == 3) ? (int)st.y - z0 : 0;
-    const float wyv = wxy[(uint64_t)s * 16 + 8 + dy];
-    const float wx0 = wxy[(uint64_t)s * 16 + dx];
-    const float wx1 = wxy[(uint64_t)s * 16 + dx + 4];
-    const uint32_t orig = perm[s];
+    const float* w = sw + i * WROW;
+    const float wyv = w[8 + dy], wx0 = w[dx], wx1 = w[dx + 4];
     const int a0 = (ox + dx) * t.PY + oy + dy;
     const int a1 = a0 + 4 * t.PY;
-    for (int c = 0; c < ncl; ++c) {
-      const float2 d = data[(uint64_t)(cfirst + c) * dstride + orig];
-      for (int j = 0; j < K; ++j) {
-        const int pl = c * K + j;
-        const float sc = scale[pl];
-        float2 v = aa ? cmul(cconj(aa[(uint64_t)s * K + j]), d) : d;
-        v = make_float2(v.x * sc, v.y * sc);
+    const float2* vi = sv + i * nplane;
+    if (DIM == 2) {
+      const float w0 = wx0 * wyv, w1 = wx1 * wyv;
+      for (int pl = 0; pl < nplane; ++pl) {
+        const float2 v = vi[pl];
         int* pr = smi + (pl * 2) * cells;
         int* pi = pr + cells;
-        if (DIM == 2) {
-          const float w0 = wx0 * wyv, w1 = wx1 * wyv;
-          if (w0 != 0.f) { atomicAdd(pr + a0, __float2int_rn(w0 * v.x)); atomicAdd(pi + a0, __float2int_rn(w0 * v.y)); }
-          if (w1 != 0.f) { atomicAdd(pr + a1, __float2int_rn(w1 * v.x)); atomicAdd(pi + a1, __float2int_rn(w1 * v.y)); }
-        } else {
-#pragma unroll 2
-          for (int e = 0; e < 8; ++e) {
-            const float wzv = wz[(uint64_t)s * 8 + e];
-            if (wzv == 0.f) continue;
-            const int zo = (oz + e) * plane;
-            const float w0 = wx0 * wyv * wzv, w1 = wx1 * wyv * wzv;
-            if (w0 != 0.f) {
-              atomicAdd(pr + zo + a0, __float2int_rn(w0 * v.x));
-              atomicAdd(pi + zo + a0, __float2int_rn(w0 * v.y));
-            }
-            if (w1 != 0.f) {
-              atomicAdd(pr + zo + a1, __float2int_rn(w1 * v.x));
-              atomicAdd(pi + zo + a1, __float2int_rn(w1 * v.y));
-            }
-          }
+        atomicAdd(pr + a0, fixed_point(w0, v.x));
+        atomicAdd(pi + a0, fixed_point(w0, v.y));
+        atomicAdd(pr + a1, fixed_point(w1, v.x));
+        atomicAdd(pi + a1, fixed_point(w1, v.y));
+      }
+    } else {
+      const int oz = (int)st.y - z0;
+      for (int e = 0; e < 8; ++e) {
+        const float wzv = w[16 + e];
+        if (wzv == 0.f) continue;          // uniform across the warp
+        const int zo = (oz + e) * plane;
+        const float w0 = wx0 * wyv * wzv, w1 = wx1 * wyv * wzv;
+        for (int pl = 0; pl < nplane; ++pl) {
+          const float2 v = vi[pl];
+          int* pr = smi + (pl * 2) * cells + zo;
+          int* pi = pr + cells;
+          atomicAdd(pr + a0, fixed_point(w0, v.x));
+          atomicAdd(pi + a0, fixed_point(w0, v.y));
+          atomicAdd(pr + a1, fixed_point(w1, v.x));
+          atomicAdd(pi + a1, fixed_point(w1, v.y));
         }
       }
     }
   }
   __syncthreads();
 
+  // 4. flush
   const uint64_t G = g.ngrid();
-  for (int q = threadIdx.x; q < cells; q += blockDim.x) {
+  for (int q = tid; q < cells; q += blockDim.x) {
     const int pyy = q % t.PY;
     const int pxx = (q / t.PY) % t.PX;
     const int pzz = q / (t.PY * t.PX);
@@ -749,6 +779,7 @@ pg_status nufft_build_binning(NufftPlan* p, int L, int K, const int* l0_host, co
       subs.push_back(make_int4(tile, l, (int)f, (int)std::min<uint64_t>(kMaxPerSub, e - f)));
   }
   b->nsub = (int)subs.size();
+  b->submax = kMaxPerSub;
 
   PG_TRY(b->perm.upload(b->h_perm.data(), M, s));
   PG_TRY(b->subprob.upload(subs.data(), subs.size(), s));
@@ -834,24 +865,24 @@ static void fft_release_plan(const NufftGeom& g, int B, cufftHandle h, size_t wo
 
 static pg_status ensure_workspace(NufftPlan* p, int B, cufftHandle* h, cudaStream_t s) {
   const uint64_t G = p->g.ngrid();
-  if (p->grids.n < (uint64_t)B * G) {
+  if (p->work->grids.n < (uint64_t)B * G) {
     PG_CUDA(cudaStreamSynchronize(s));  // queued work may still use the old workspace
-    PG_TRY(p->grids.alloc((uint64_t)B * G));
+    PG_TRY(p->work->grids.alloc((uint64_t)B * G));
   }
   auto it = p->ffts.find(B);
   if (it == p->ffts.end()) {
     cufftHandle hh;
     size_t work = 0;
     PG_TRY(fft_acquire(fft_key(p->g, B), &hh, &work));
-    if (work > p->fft_work.n) {
+    if (work > p->work->fft_work.n) {
       // the old area may still be in use by queued transforms of this plan
       PG_CUDA(cudaStreamSynchronize(s));
-      pg_status st = p->fft_work.alloc(work);
+      pg_status st = p->work->fft_work.alloc(work);
       if (st != PG_OK) { fft_release(fft_key(p->g, B), hh, work); return st; }
     }
     it = p->ffts.emplace(B, std::make_pair(hh, work)).first;
   }
-  PG_CUFFT(cufftSetWorkArea(it->second.first, p->fft_work.p));
+  PG_CUFFT(cufftSetWorkArea(it->second.first, p->work->fft_work.p));
   PG_CUFFT(cufftSetStream(it->second.first, s));
   *h = it->second.first;
   return PG_OK;
@@ -874,7 +905,7 @@ static pg_status gather_launch_one(NufftPlan* p, const Binning* bin, const float
   PG_CUDA(cudaFuncSetAttribute(k_gather<DIM, CC, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid(bin->nsub, ceil_div(nb, CC));
   PG_LAUNCH((k_gather<DIM, CC, KP>), grid, 256, smem, s, p->g, t, bin->subprob.p, bin->start.p, bin->wxy.p,
-            bin->wz.p, bin->perm.p, aa, bin->K, bin->L, p->grids.p, nb, y, dstride);
+            bin->wz.p, bin->perm.p, aa, bin->K, bin->L, p->work->grids.p, nb, y, dstride);
   return PG_OK;
 }
 
@@ -931,12 +962,12 @@ pg_status nufft_forward(NufftPlan* p, const NufftBatch& b, const float2* x, floa
     dim3 grid(ceil_div(G, 256), B);
     {
       ProfScope ps("pre", s);
-      PG_LAUNCH(k_pre, grid, 256, 0, s, g, L, x, b.S, c0, b.E, b.Wo, p->deap.p, scale, p->grids.p);
+      PG_LAUNCH(k_pre, grid, 256, 0, s, g, L, x, b.S, c0, b.E, b.Wo, p->deap.p, scale, p->work->grids.p);
     }
     {
       ProfScope ps("fft_fwd", s);
-      PG_CUFFT(cufftExecC2C(h, reinterpret_cast<cufftComplex*>(p->grids.p),
-                            reinterpret_cast<cufftComplex*>(p->grids.p), CUFFT_FORWARD));
+      PG_CUFFT(cufftExecC2C(h, reinterpret_cast<cufftComplex*>(p->work->grids.p),
+                            reinterpret_cast<cufftComplex*>(p->work->grids.p), CUFFT_FORWARD));
     }
     float2* yc = y + (uint64_t)c0 * b.data_stride;
     const float2* aa = (L > 1 || bin->aa.p) ? bin->aa.p : nullptr;
@@ -961,11 +992,17 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
   const uint64_t G = g.ngrid();
   const TileShape& t = bin->tile;
   const size_t plane_bytes = (size_t)t.PX * t.PY * t.PZ * 2 * sizeof(float);
-  const int smem_optin = smem_optin_bytes();
-  int Cc = (int)std::min<size_t>((size_t)std::max(1, std::min(4, p->tune.spread_cc)),
-                                  (size_t)(smem_optin - 2048) / (plane_bytes * K));
-  while (Cc > 1 && Cc * K > 16) --Cc;
-  if (Cc < 1 || K > 16) return set_error(PG_INVALID_ARG, "adjoint: segment window K=%d too wide for shared memory", K);
+  const size_t smem_limit = (size_t)smem_optin_bytes() - 2048;   // static shared arrays + margin
+  const int smax = bin->submax;
+  // tile planes of cc coils x K segments, plus the staged samples
+  auto smem_for = [&](int cc) {
+    return plane_bytes * K * cc + (size_t)smax * (spread_wrow(g.dim) * sizeof(float) + sizeof(uint2) +
+                                                  (size_t)K * cc * sizeof(float2));
+  };
+  int Cc = std::max(1, std::min(4, p->tune.spread_cc));
+  while (Cc > 1 && (Cc * K > 16 || smem_for(Cc) > smem_limit)) --Cc;
+  if (K > 16 || smem_for(1) > smem_limit)
+    return set_error(PG_INVALID_ARG, "adjoint: segment window K=%d too wide for shared memory", K);
   const float w1 = p->lut_max;
   const float wmax = (g.dim == 2) ? w1 * w1 : w1 * w1 * w1;
   for (int c0 = 0; c0 < b.C; c0 += Cb) {
@@ -975,10 +1012,10 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
     PG_TRY(ensure_workspace(p, B, &h, s));
     {
       ProfScope ps("zero", s);
-      PG_CUDA(cudaMemsetAsync(p->grids.p, 0, (size_t)B * G * sizeof(float2), s));
+      PG_CUDA(cudaMemsetAsync(p->work->grids.p, 0, (size_t)B * G * sizeof(float2), s));
     }
     const int cc = std::min(Cc, nb);
-    const size_t smem = plane_bytes * K * cc;
+    const size_t smem = smem_for(cc);
     dim3 grid(bin->nsub, ceil_div(nb, cc));
     const float2* yc = y + (uint64_t)c0 * b.data_stride;
     const float2* aa = (L > 1 || bin->aa.p) ? bin->aa.p : nullptr;
@@ -987,21 +1024,21 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
       if (g.dim == 2) {
         PG_CUDA(cudaFuncSetAttribute(k_spread<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         PG_LAUNCH(k_spread<2>, grid, 256, smem, s, g, t, bin->subprob.p, bin->start.p, bin->wxy.p, bin->wz.p,
-                  bin->perm.p, aa, K, L, yc, b.data_stride, nb, cc, wmax, p->grids.p);
+                  bin->perm.p, aa, K, L, yc, b.data_stride, nb, cc, smax, wmax, p->work->grids.p);
       } else {
         PG_CUDA(cudaFuncSetAttribute(k_spread<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         PG_LAUNCH(k_spread<3>, grid, 256, smem, s, g, t, bin->subprob.p, bin->start.p, bin->wxy.p, bin->wz.p,
-                  bin->perm.p, aa, K, L, yc, b.data_stride, nb, cc, wmax, p->grids.p);
+                  bin->perm.p, aa, K, L, yc, b.data_stride, nb, cc, smax, wmax, p->work->grids.p);
       }
     }
     {
       ProfScope ps("fft_adj", s);
-      PG_CUFFT(cufftExecC2C(h, reinterpret_cast<cufftComplex*>(p->grids.p),
-                            reinterpret_cast<cufftComplex*>(p->grids.p), CUFFT_INVERSE));
+      PG_CUFFT(cufftExecC2C(h, reinterpret_cast<cufftComplex*>(p->work->grids.p),
+                            reinterpret_cast<cufftComplex*>(p->work->grids.p), CUFFT_INVERSE));
     }
     const int acc = (b.accumulate || c0 > 0) ? 1 : 0;
     ProfScope ps("post", s);
-    PG_LAUNCH(k_post, ceil_div(g.nimg(), 256), 256, 0, s, g, nb, L, p->grids.p, b.S, c0, b.E, b.WoH, p->deap.p,
+    PG_LAUNCH(k_post, ceil_div(g.nimg(), 256), 256, 0, s, g, nb, L, p->work->grids.p, b.S, c0, b.E, b.WoH, p->deap.p,
               scale, acc, x);
   }
   return PG_OK;

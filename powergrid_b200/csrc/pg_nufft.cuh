@@ -59,9 +59,17 @@ struct Binning {
   DevBuf<float2> aa;         // K per sample: interpolator values AA(m, l0..l0+K-1)
   DevBuf<int4> subprob;      // (tile index, l0, first sorted sample, count)
   int nsub = 0;
+  int submax = 0;            // most samples in one subproblem
   uint64_t nkeys = 0;
   std::vector<uint32_t> h_keys;   // bin key per original sample (tests)
   std::vector<uint32_t> h_perm;
+};
+
+// Grid workspace and cuFFT work area.  Plans of one geometry that run back
+// to back on one stream (the shots of pcSenseTimeSeg) share a single one.
+struct NufftWork {
+  DevBuf<float2> grids;
+  DevBuf<char> fft_work;
 };
 
 struct NufftPlan {
@@ -73,10 +81,9 @@ struct NufftPlan {
   float lut_max = 0.f;           // largest per-axis tap weight
   DevBuf<float> deap;            // Nx + Ny + Nz reciprocal-transform factors
   std::unique_ptr<Binning> plain;  // binning without segmentation (L = 1)
-  // grid workspace and cuFFT plans, keyed by batch size
-  DevBuf<float2> grids;
+  // grid workspace (possibly shared) and cuFFT plans, keyed by batch size
+  std::shared_ptr<NufftWork> work = std::make_shared<NufftWork>();
   std::map<int, std::pair<cufftHandle, size_t>> ffts;  // batch -> (pooled plan, work bytes)
-  DevBuf<char> fft_work;
   size_t budget_bytes = 8ull << 30;  // grid workspace limit per plan
   ~NufftPlan();
 };

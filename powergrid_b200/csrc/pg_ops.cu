@@ -142,7 +142,7 @@ pg_status GnufftOp::adjoint(const float2* y, float2* x, cudaStream_t s) {
   return nufft_adjoint(plan.get(), b, y, x, s);
 }
 uint64_t GnufftOp::resident_bytes() const {
-  return plan->M * (3 * 4 + 8 + 64 + 4 + 4) + plan->grids.bytes();
+  return plan->M * (3 * 4 + 8 + 64 + 4 + 4) + plan->work->grids.bytes();
 }
 
 // ---- Gdft ------------------------------------------------------------------
@@ -290,7 +290,8 @@ pg_status PcSenseTsOp::adjoint(const float2* y, float2* x, cudaStream_t s) {
 }
 uint64_t PcSenseTsOp::resident_bytes() const {
   uint64_t b = S.bytes() + E.bytes();
-  for (auto& p : plans) b += p->grids.bytes() + p->M * 100;
+  for (auto& p : plans) b += p->M * 100;
+  if (!plans.empty()) b += plans[0]->work->grids.bytes() + plans[0]->work->fft_work.bytes();
   return b;
 }
 
@@ -439,7 +440,8 @@ pg_status pg_pcsense_timeseg_create(pg_op* out, const float* kx, const float* ky
       op->tabs[sh].AA.clear();
       op->tabs[sh].AA.shrink_to_fit();
     }
-    // share the grid workspace budget across shots: each plan sizes its own
+    // the shots run one after another on one stream: one grid workspace serves all
+    if (sh > 0) plan->work = op->plans[0]->work;
     op->plans.push_back(std::move(plan));
   }
   PG_TRY(op->S.upload(reinterpret_cast<const float2*>(sense_map), Ni * nc, s));

@@ -95,10 +95,12 @@ struct pg_server_s {
     return used + f <= cfg.hbm_budget_bytes || running == 0;
   }
 
-  pg_status run_job(const Job& j, cudaStream_t s, uint64_t* iters) {
+  pg_status run_job(const Job& j, cudaStream_t s, uint64_t* iters, double* setup_ms, double* solve_ms) {
     const pg_request& r = j.t->req;
     const uint64_t N = r.nx * r.ny * r.nz, M = r.n_samples, C = r.nc;
     const uint64_t sl = j.slice;
+    const double t0 = now_ms();
+    double t1 = t0;
     Arena arena;
     PG_TRY(arena_open(&arena, j.t->footprint, s));
     arena_install(&arena);
@@ -122,6 +124,7 @@ struct pg_server_s {
         if ((st = x.alloc(N)) != PG_OK) break;
         if ((st = it.alloc(1)) != PG_OK) break;
         pg_penalty R{PG_PENALTY_QUAD, r.nx, r.ny, r.nz, r.beta, 1.0f, 3};
+        t1 = now_ms();
         st = pcg_solve_device(S.get(), nullptr, nullptr, y.p, R, r.niter, x.p, it.p, s, &j.t->cancel);
         if (st != PG_OK) break;
         uint32_t n = 0;
@@ -137,6 +140,8 @@ struct pg_server_s {
     arena_install(nullptr);
     arena_release(&arena);
     cudaStreamSynchronize(s);
+    *setup_ms = t1 - t0;
+    *solve_ms = now_ms() - t1;
     return st;
   }
 
@@ -157,13 +162,16 @@ struct pg_server_s {
         if (job.t->jobs_started++ == 0) job.t->st.t_start_ms = now_ms();
       }
       uint64_t iters = 0;
-      pg_status st = job.t->cancel.load() ? PG_CANCELLED : run_job(job, s, &iters);
+      double setup_ms = 0, solve_ms = 0;
+      pg_status st = job.t->cancel.load() ? PG_CANCELLED : run_job(job, s, &iters, &setup_ms, &solve_ms);
       {
         std::lock_guard<std::mutex> lk(mu);
         used -= job.t->footprint;
         --running;
         Ticket& t = *job.t;
         t.st.iters_done += iters;
+        t.st.setup_ms += setup_ms;
+        t.st.solve_ms += solve_ms;
         if (st != PG_OK && t.st.status == PG_OK) t.st.status = st;
         if (--t.jobs_left == 0) {
           t.st.t_done_ms = now_ms();
