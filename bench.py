@@ -11,8 +11,9 @@ W = 1, x0 = 0).  Seeded synthetic inputs stand in for ISMRMRD data.
   e2e        the same metric through the C ABI's host-buffer entry point
              pg_pcg_solve (H2D of the coil data and D2H of the image inside
              the timed region)
-  roofline   the adjoint gridding kernel (k_spread), timed by CUDA events
-             inside the timed region, against the measured HBM bandwidth
+  roofline   the adjoint gridding kernel (k_spread), timed by one CUDA event
+             pair per launch inside the timed region, against the measured
+             HBM bandwidth; the other stages are timed on extra steps
   cpu_baseline  the reference CPU path on this host's cores (rank 0, N=1)
 
 `--impl reference` times the reference's own CPU implementation of the path
@@ -218,8 +219,11 @@ def run_gpu_arm(args):
         check(L.pg_pcg_solve_device(Sg.handle, None, None, P(y.data_ptr()), C.byref(pen), NITER, P(x.data_ptr()),
                                     P(iters.data_ptr()), sp))
 
-    # Stage timing stays on for warm-up and timed steps alike (same graph).
+    # The timed steps carry one CUDA event pair per adjoint, around the spread
+    # kernel (the roofline kernel); the other stage times come from extra
+    # profiled steps after the timed region.
     check(L.pg_profile_enable(1))
+    check(L.pg_profile_only(b"spread"))
     sampler = ClockSampler(local)
     sampler.__enter__()
     for _ in range(max(3, args.warmup)):
@@ -229,10 +233,8 @@ def run_gpu_arm(args):
     stream.synchronize()
     sampler.rows.clear()
 
-    stages = ["pre", "fft_fwd", "gather", "zero", "spread", "fft_adj", "post"]
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    stage_ms = {k: [] for k in stages}
-    step_ms = []
+    step_ms, spread_ms = [], []
     if ws > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -245,15 +247,28 @@ def run_gpu_arm(args):
             ev[i][1].record(stream)
         stream.synchronize()
         step_ms.append(ev[i][0].elapsed_time(ev[i][1]))
+        ms = C.c_float()
+        if L.pg_profile_stage_ms(b"spread", C.byref(ms)) == 0:
+            spread_ms.append(ms.value)
+    torch.cuda.synchronize()
+    launches = _lib.launches() - launches0
+    sampler.__exit__(None, None, None)
+
+    stages = ["pre", "fft_fwd", "gather", "zero", "spread", "fft_adj", "post"]
+    stage_ms = {k: [] for k in stages}
+    check(L.pg_profile_only(None))
+    for i in range(4):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            solve()
+        stream.synchronize()
+        if i == 0:
+            continue                      # the first profiled solve re-captures the graph
         for k in stages:
             ms = C.c_float()
             if L.pg_profile_stage_ms(k.encode(), C.byref(ms)) == 0:
                 stage_ms[k].append(ms.value)
-    torch.cuda.synchronize()
-    launches = _lib.launches() - launches0
-    sampler.__exit__(None, None, None)
     check(L.pg_profile_enable(0))
-    spread_ms = stage_ms["spread"]
     total_ms = sum(step_ms)
     done = int(iters.item())
     if ws > 1:

@@ -216,6 +216,9 @@ uint64_t pg_request_footprint(const pg_request* req);
  * synchronised the stream.  Returns PG_NOT_READY if the stage never ran. */
 pg_status pg_profile_enable(int on);
 pg_status pg_profile_stage_ms(const char* stage, float* ms);
+/* Restrict recording to one stage (NULL or "" = every stage), so that a timed
+ * run carries only the event pair it needs. */
+pg_status pg_profile_only(const char* stage);
 
 /* Make the n-th device allocation from now fail with PG_OUT_OF_MEMORY
  * (n = 0 disables). */

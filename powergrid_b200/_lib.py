@@ -85,6 +85,7 @@ SIGNATURES = {
     "pg_util_kb_lut": (U64, [F32, P, U64, C.POINTER(F32)]),
     "pg_profile_enable": (C.c_int, [C.c_int]),
     "pg_profile_stage_ms": (C.c_int, [C.c_char_p, C.POINTER(F32)]),
+    "pg_profile_only": (C.c_int, [C.c_char_p]),
     "pg_util_gnufft_binning": (C.c_int, [P, P, P, C.POINTER(U64)]),
 }
 

@@ -177,40 +177,45 @@ __global__ void k_permute(uint64_t M, int dim, int K, const uint32_t* __restrict
 __device__ __forceinline__ int parity3(int a, int b, int c) { return (a + b + c) & 1; }
 
 // ---------------------------------------------------------------------------
-// Forward pre-kernel: deapodize, coil map, shot phase, segment phase and
-// zero-pad into the centred grid, times the (-1)^(x+y+z) checkerboard.
+// Forward pre-kernel: deapodize, coil map, shot phase and segment phase,
+// times the (-1)^(x+y+z) checkerboard, into the image region of the centred
+// forward-input grid.  The zero-pad border of that buffer is cleared once
+// when it is allocated and never written, so only N^d cells per grid move.
+// One thread per (pixel, grid of the batch).
 // ---------------------------------------------------------------------------
 __global__ void k_pre(NufftGeom g, int L, const float2* __restrict__ x, const float2* __restrict__ S, int c0,
                       const float2* __restrict__ E, const float2* __restrict__ Wo, const float* __restrict__ deap,
                       float scale, float2* __restrict__ grids) {
-  const uint64_t G = g.ngrid();
-  const uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= G) return;
+  const uint64_t N = g.nimg();
+  const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
   const int b = blockIdx.y;           // grid within the batch
-  const int cl = b / L, l = b % L;
-  const int my = (int)(q % g.Gy);
-  const int mx = (int)((q / g.Gy) % g.Gx);
-  const int mz = (int)(q / ((uint64_t)g.Gy * g.Gx));
-  const int iy = my - g.pad_off[1];
-  const int ix = mx - g.pad_off[0];
-  const int iz = (g.dim == 3) ? mz - g.pad_off[2] : 0;
-  float2 v = make_float2(0.f, 0.f);
-  if (iy >= 0 && iy < g.Ny && ix >= 0 && ix < g.Nx && iz >= 0 && iz < g.Nz) {
-    const uint64_t N = g.nimg();
-    const uint64_t p = (uint64_t)iy + (uint64_t)g.Ny * ((uint64_t)ix + (uint64_t)g.Nx * iz);
-    v = x[p];
-    if (S) {
-      const float2 s = S[(uint64_t)(c0 + cl) * N + p];
-      v = E ? cmul(v, cmul(s, E[p])) : cmul(s, v);
-    }
-    if (Wo) v = cmul(Wo[(uint64_t)l * N + p], v);
-    float k = deap[ix] * deap[g.Nx + iy];
-    if (g.dim == 3) k = k * deap[g.Nx + g.Ny + iz];
-    v = (k == k) ? make_float2(__fmul_rn(__fdiv_rn(v.x, k), scale), __fmul_rn(__fdiv_rn(v.y, k), scale))
-                 : make_float2(0.f, 0.f);
-    if (parity3(mx, my, mz)) v = make_float2(-v.x, -v.y);
+  const int c = b / L, l = b - c * L;
+  const int iy = (int)(p % g.Ny);
+  const int ix = (int)((p / g.Ny) % g.Nx);
+  const int iz = (int)(p / ((uint64_t)g.Ny * g.Nx));
+  const int my = iy + g.pad_off[1];
+  const int mx = ix + g.pad_off[0];
+  const int mz = (g.dim == 3) ? iz + g.pad_off[2] : 0;
+  const uint64_t q = (uint64_t)my + (uint64_t)g.Gy * ((uint64_t)mx + (uint64_t)g.Gx * mz);
+  float2 v = x[p];
+  if (S) {
+    const float2 sv = S[(uint64_t)(c0 + c) * N + p];
+    v = E ? cmul(v, cmul(sv, E[p])) : cmul(sv, v);
   }
-  grids[(uint64_t)b * G + q] = v;
+  if (Wo) v = cmul(Wo[(uint64_t)l * N + p], v);
+  float k = deap[ix] * deap[g.Nx + iy];
+  if (g.dim == 3) k = k * deap[g.Nx + g.Ny + iz];
+  v = (k == k) ? make_float2(__fmul_rn(__fdiv_rn(v.x, k), scale), __fmul_rn(__fdiv_rn(v.y, k), scale))
+               : make_float2(0.f, 0.f);
+  if (parity3(mx, my, mz)) v = make_float2(-v.x, -v.y);
+  grids[(uint64_t)b * g.ngrid() + q] = v;
+}
+
+// Zero n float4 words (the adjoint's grid batch before the spread).
+__global__ void k_zero(uint64_t n, float4* __restrict__ p) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    p[i] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
 // ---------------------------------------------------------------------------
@@ -276,16 +281,38 @@ __device__ __forceinline__ void group8_reduce_scatter(float (&v)[V], int lane) {
   }
 }
 
-template <int DIM, int CC, int KP>
+// Padded extent along y (the fastest axis) such that 4 x-rows of 8 y-taps
+// land in 32 distinct banks: PY = 8 or 24 (mod 32).
+__host__ __device__ constexpr int padded_y(int T) {
+  int py = T + 8;
+  while ((py % 32) != 8 && (py % 32) != 24) ++py;
+  return py;
+}
+
+// Compile-time tile geometry: every shared-memory address in the gridding
+// loops is a per-sample base plus an immediate offset.
+template <int DIM, int T>
+struct TileGeo {
+  static constexpr int TZ = (DIM == 3) ? T : 1;
+  static constexpr int PX = T + 8;
+  static constexpr int PY = padded_y(T);
+  static constexpr int PZ = (DIM == 3) ? T + 8 : 1;
+  static constexpr int PLANE = PX * PY;
+  static constexpr int CELLS = PLANE * PZ;
+};
+
+template <int DIM, int T, int CC, int KP>
 __global__ void __launch_bounds__(256) k_gather(NufftGeom g, TileShape t, const int4* __restrict__ sub,
                                                 const uint2* __restrict__ start, const float* __restrict__ wxy,
                                                 const float* __restrict__ wz, const uint32_t* __restrict__ perm,
                                                 const float2* __restrict__ aa, int K, int L,
                                                 const float2* __restrict__ grids, int Cb,
                                                 float2* __restrict__ data, uint64_t dstride) {
+  using TG = TileGeo<DIM, T>;
+  constexpr int CELLS = TG::CELLS, PY = TG::PY, PX = TG::PX, PLANE = TG::PLANE;
   constexpr int V = 2 * CC * KP;                 // accumulators per sample
   constexpr int PER = (V >= 8) ? V / 8 : 1;      // values a lane holds after the group butterfly
-  extern __shared__ float sm[];
+  extern __shared__ __align__(16) float sm[];
   __shared__ float red[8][4][V];
   const int4 sp = sub[blockIdx.x];
   const int cfirst = blockIdx.y * CC;
@@ -295,13 +322,12 @@ __global__ void __launch_bounds__(256) k_gather(NufftGeom g, TileShape t, const 
   const int txz = tile / t.nty;
   const int tx = txz % t.ntx;
   const int tz = txz / t.ntx;
-  const int x0 = tx * t.TX, y0 = ty * t.TY, z0 = tz * t.TZ;
-  const int cells = t.PX * t.PY * t.PZ;
+  const int x0 = tx * T, y0 = ty * T, z0 = tz * TG::TZ;
   const uint64_t G = g.ngrid();
-  for (int q = threadIdx.x; q < cells; q += blockDim.x) {
-    const int pyy = q % t.PY;
-    const int pxx = (q / t.PY) % t.PX;
-    const int pzz = q / (t.PY * t.PX);
+  for (int q = threadIdx.x; q < CELLS; q += blockDim.x) {
+    const int pyy = q % PY;
+    const int pxx = (q / PY) % PX;
+    const int pzz = q / PLANE;
     const int gy = y0 + pyy, gx = x0 + pxx, gz = z0 + pzz;
     const bool in = gy < g.Gy && gx < g.Gx && gz < g.Gz;
     const uint64_t idx = (uint64_t)gy + (uint64_t)g.Gy * ((uint64_t)gx + (uint64_t)g.Gx * gz);
@@ -311,18 +337,18 @@ __global__ void __launch_bounds__(256) k_gather(NufftGeom g, TileShape t, const 
       for (int j = 0; j < KP; ++j) {
         float2 v = make_float2(0.f, 0.f);
         if (in && c < ncl && j < K) v = grids[((uint64_t)(cfirst + c) * L + lseg + j) * G + idx];
-        float* pr = sm + ((c * KP + j) * 2) * cells;
+        float* pr = sm + ((c * KP + j) * 2) * CELLS;
         pr[q] = v.x;
-        pr[cells + q] = v.y;
+        pr[CELLS + q] = v.y;
       }
   }
   __syncthreads();
 
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int NW = 8;
   const int dy = lane & 7, grp = lane >> 3;
-  const int plane = t.PX * t.PY;
   const int end = first + count;
-  for (int s0 = first + 4 * warp; s0 < end; s0 += 4 * nw) {
+  for (int s0 = first + 4 * warp; s0 < end; s0 += 4 * NW) {
     const int s = s0 + grp;
     float acc[V];
 #pragma unroll
@@ -330,35 +356,35 @@ __global__ void __launch_bounds__(256) k_gather(NufftGeom g, TileShape t, const 
     if (s < end) {
       const uint2 st = start[s];
       const int ox = (int)(st.x & 0xffff) - x0, oy = (int)(st.x >> 16) - y0;
-      const float* w = wxy + (uint64_t)s * 16;
-      const float wyv = w[8 + dy];
+      const float4* w4 = reinterpret_cast<const float4*>(wxy + (uint64_t)s * 16);
+      const float4 wa = w4[0], wb = w4[1];
+      const float wxr[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
+      const float wyv = wxy[(uint64_t)s * 16 + 8 + dy];
+      const float* base = sm + ox * PY + oy + dy;
       if (DIM == 2) {
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
-          const float wr = w[r] * wyv;
-          const int a = (ox + r) * t.PY + oy + dy;
+          const float wr = wxr[r] * wyv;
 #pragma unroll
           for (int cj = 0; cj < CC * KP; ++cj) {
-            const float* pr = sm + (cj * 2) * cells;
-            acc[2 * cj] = fmaf(wr, pr[a], acc[2 * cj]);
-            acc[2 * cj + 1] = fmaf(wr, pr[cells + a], acc[2 * cj + 1]);
+            acc[2 * cj] = fmaf(wr, base[(2 * cj) * CELLS + r * PY], acc[2 * cj]);
+            acc[2 * cj + 1] = fmaf(wr, base[(2 * cj + 1) * CELLS + r * PY], acc[2 * cj + 1]);
           }
         }
       } else {
         const int oz = (int)st.y - z0;
         const float* wzz = wz + (uint64_t)s * 8;
-        for (int e = 0; e < 8; ++e) {
+        const float* bz = base + oz * PLANE;
+#pragma unroll 1
+        for (int e = 0; e < 8; ++e, bz += PLANE) {
           const float wze = wzz[e];
-          const int zo = (oz + e) * plane;
 #pragma unroll
           for (int r = 0; r < 8; ++r) {
-            const float wr = w[r] * wyv * wze;
-            const int a = zo + (ox + r) * t.PY + oy + dy;
+            const float wr = wxr[r] * wyv * wze;
 #pragma unroll
             for (int cj = 0; cj < CC * KP; ++cj) {
-              const float* pr = sm + (cj * 2) * cells;
-              acc[2 * cj] = fmaf(wr, pr[a], acc[2 * cj]);
-              acc[2 * cj + 1] = fmaf(wr, pr[cells + a], acc[2 * cj + 1]);
+              acc[2 * cj] = fmaf(wr, bz[(2 * cj) * CELLS + r * PY], acc[2 * cj]);
+              acc[2 * cj + 1] = fmaf(wr, bz[(2 * cj + 1) * CELLS + r * PY], acc[2 * cj + 1]);
             }
           }
         }
@@ -418,37 +444,38 @@ __device__ __forceinline__ int fixed_point(float w, float v) {
 // Staged weights per sample in the spread: wx[8], wy[8] and, in 3-D, wz[8].
 __host__ __device__ constexpr int spread_wrow(int dim) { return dim == 2 ? 16 : 24; }
 
-template <int DIM>
+template <int DIM, int T, int NP>
 __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const int4* __restrict__ sub,
                                                 const uint2* __restrict__ start, const float* __restrict__ wxy,
                                                 const float* __restrict__ wz, const uint32_t* __restrict__ perm,
                                                 const float2* __restrict__ aa, int K, int L,
-                                                const float2* __restrict__ data, uint64_t dstride, int Cb,
-                                                int Cc, int smax, float wmax, float2* __restrict__ grids) {
+                                                const float2* __restrict__ data, uint64_t dstride, int c0, int cc,
+                                                int smax, float wmax, float2* __restrict__ grids) {
+  using TG = TileGeo<DIM, T>;
+  constexpr int CELLS = TG::CELLS, PY = TG::PY, PX = TG::PX, PLANE = TG::PLANE;
   constexpr int WROW = spread_wrow(DIM);   // staged weights per sample: wx[8] wy[8] (wz[8])
   extern __shared__ __align__(16) int smi[];
   __shared__ unsigned vmax[16];
   __shared__ float scale[16], inv_scale[16];
+  // planes per block: NP when fixed at compile time, else cc x K
+  const int np = (NP > 0) ? NP : cc * K;
   const int4 sp = sub[blockIdx.x];
-  const int cfirst = blockIdx.y * Cc;
-  const int ncl = min(Cc, Cb - cfirst);
+  const int cfirst = c0 + blockIdx.y * cc;
   const int tile = sp.x, first = sp.z, count = sp.w;
   const int lseg = sp.y;
   const int ty = tile % t.nty;
   const int txz = tile / t.nty;
   const int tx = txz % t.ntx;
   const int tz = txz / t.ntx;
-  const int x0 = tx * t.TX, y0 = ty * t.TY, z0 = tz * t.TZ;
-  const int cells = t.PX * t.PY * t.PZ;
-  const int nplane = ncl * K;          // complex planes in use (<= 16)
+  const int x0 = tx * T, y0 = ty * T, z0 = tz * TG::TZ;
   const int tid = threadIdx.x;
-  float* sw = reinterpret_cast<float*>(smi + (size_t)nplane * 2 * cells);
+  float* sw = reinterpret_cast<float*>(smi + (size_t)np * 2 * CELLS);
   float2* sv = reinterpret_cast<float2*>(sw + (size_t)smax * WROW);
-  uint2* sst = reinterpret_cast<uint2*>(sv + (size_t)smax * nplane);
+  uint2* sst = reinterpret_cast<uint2*>(sv + (size_t)smax * np);
 
   {
     int4* z = reinterpret_cast<int4*>(smi);
-    for (int q = tid; q < (nplane * 2 * cells) / 4; q += blockDim.x) z[q] = make_int4(0, 0, 0, 0);
+    for (int q = tid; q < (np * 2 * CELLS) / 4; q += blockDim.x) z[q] = make_int4(0, 0, 0, 0);
   }
   if (tid < 16) vmax[tid] = 0u;
   __syncthreads();
@@ -465,9 +492,9 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
     reinterpret_cast<float4*>(sw + i * WROW)[a] = val;
   }
   for (int i = tid; i < count; i += blockDim.x) sst[i] = start[first + i];
-  for (int q = tid; q < count * nplane; q += blockDim.x) {
-    const int i = q / nplane, pl = q % nplane;
-    const int c = pl / K, j = pl % K;
+  for (int q = tid; q < count * np; q += blockDim.x) {
+    const int i = q / np, pl = q - i * np;
+    const int c = pl / K, j = pl - c * K;
     const int s = first + i;
     const float2 d = data[(uint64_t)(cfirst + c) * dstride + perm[s]];
     const float2 v = aa ? cmul(cconj(aa[(uint64_t)s * K + j]), d) : d;
@@ -491,51 +518,48 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
     inv_scale[tid] = ldexpf(1.f, -e);
   }
   __syncthreads();
-  for (int q = tid; q < count * nplane; q += blockDim.x) {
-    const float sc = scale[q % nplane];
+  for (int q = tid; q < count * np; q += blockDim.x) {
+    const float sc = scale[q % np];
     const float2 v = sv[q];
     sv[q] = make_float2(v.x * sc, v.y * sc);
   }
   __syncthreads();
 
   // 3. spread
-  const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+  const int warp = tid >> 5, lane = tid & 31;
+  constexpr int NW = 8;
   const int dy = lane & 7, dx = lane >> 3;
-  const int plane = t.PX * t.PY;
-  for (int i = warp; i < count; i += nw) {
+  for (int i = warp; i < count; i += NW) {
     const uint2 st = sst[i];
     const int ox = (int)(st.x & 0xffff) - x0, oy = (int)(st.x >> 16) - y0;
     const float* w = sw + i * WROW;
-    const float wyv = w[8 + dy], wx0 = w[dx], wx1 = w[dx + 4];
-    const int a0 = (ox + dx) * t.PY + oy + dy;
-    const int a1 = a0 + 4 * t.PY;
-    const float2* vi = sv + i * nplane;
+    const float wyv = w[8 + dy];
+    const float w0 = w[dx] * wyv, w1 = w[dx + 4] * wyv;
+    int* b = smi + (ox + dx) * PY + oy + dy;
+    const float2* vi = sv + i * np;
     if (DIM == 2) {
-      const float w0 = wx0 * wyv, w1 = wx1 * wyv;
-      for (int pl = 0; pl < nplane; ++pl) {
+#pragma unroll
+      for (int pl = 0; pl < np; ++pl) {
         const float2 v = vi[pl];
-        int* pr = smi + (pl * 2) * cells;
-        int* pi = pr + cells;
-        atomicAdd(pr + a0, fixed_point(w0, v.x));
-        atomicAdd(pi + a0, fixed_point(w0, v.y));
-        atomicAdd(pr + a1, fixed_point(w1, v.x));
-        atomicAdd(pi + a1, fixed_point(w1, v.y));
+        atomicAdd(b + (2 * pl) * CELLS, fixed_point(w0, v.x));
+        atomicAdd(b + (2 * pl + 1) * CELLS, fixed_point(w0, v.y));
+        atomicAdd(b + (2 * pl) * CELLS + 4 * PY, fixed_point(w1, v.x));
+        atomicAdd(b + (2 * pl + 1) * CELLS + 4 * PY, fixed_point(w1, v.y));
       }
     } else {
-      const int oz = (int)st.y - z0;
-      for (int e = 0; e < 8; ++e) {
+      b += ((int)st.y - z0) * PLANE;
+#pragma unroll 1
+      for (int e = 0; e < 8; ++e, b += PLANE) {
         const float wzv = w[16 + e];
         if (wzv == 0.f) continue;          // uniform across the warp
-        const int zo = (oz + e) * plane;
-        const float w0 = wx0 * wyv * wzv, w1 = wx1 * wyv * wzv;
-        for (int pl = 0; pl < nplane; ++pl) {
+        const float w0e = w0 * wzv, w1e = w1 * wzv;
+#pragma unroll
+        for (int pl = 0; pl < np; ++pl) {
           const float2 v = vi[pl];
-          int* pr = smi + (pl * 2) * cells + zo;
-          int* pi = pr + cells;
-          atomicAdd(pr + a0, fixed_point(w0, v.x));
-          atomicAdd(pi + a0, fixed_point(w0, v.y));
-          atomicAdd(pr + a1, fixed_point(w1, v.x));
-          atomicAdd(pi + a1, fixed_point(w1, v.y));
+          atomicAdd(b + (2 * pl) * CELLS, fixed_point(w0e, v.x));
+          atomicAdd(b + (2 * pl + 1) * CELLS, fixed_point(w0e, v.y));
+          atomicAdd(b + (2 * pl) * CELLS + 4 * PY, fixed_point(w1e, v.x));
+          atomicAdd(b + (2 * pl + 1) * CELLS + 4 * PY, fixed_point(w1e, v.y));
         }
       }
     }
@@ -544,65 +568,76 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
 
   // 4. flush
   const uint64_t G = g.ngrid();
-  for (int q = tid; q < cells; q += blockDim.x) {
-    const int pyy = q % t.PY;
-    const int pxx = (q / t.PY) % t.PX;
-    const int pzz = q / (t.PY * t.PX);
+  for (int q = tid; q < CELLS; q += blockDim.x) {
+    const int pyy = q % PY;
+    const int pxx = (q / PY) % PX;
+    const int pzz = q / PLANE;
     const int gy = y0 + pyy, gx = x0 + pxx, gz = z0 + pzz;
     if (gy >= g.Gy || gx >= g.Gx || gz >= g.Gz) continue;
     const uint64_t idx = (uint64_t)gy + (uint64_t)g.Gy * ((uint64_t)gx + (uint64_t)g.Gx * gz);
-    for (int c = 0; c < ncl; ++c)
-      for (int j = 0; j < K; ++j) {
-        const int pl = c * K + j;
-        const int* pr = smi + (pl * 2) * cells;
-        const int re = pr[q], im = pr[cells + q];
-        if (re != 0 || im != 0)
-          atomicAdd(grids + ((uint64_t)(cfirst + c) * L + lseg + j) * G + idx,
-                    make_float2((float)re * inv_scale[pl], (float)im * inv_scale[pl]));
-      }
+    for (int pl = 0; pl < np; ++pl) {
+      const int c = pl / K, j = pl - c * K;
+      const int* pr = smi + (pl * 2) * CELLS;
+      const int re = pr[q], im = pr[CELLS + q];
+      if (re != 0 || im != 0)
+        atomicAdd(grids + ((uint64_t)(cfirst + c) * L + lseg + j) * G + idx,
+                  make_float2((float)re * inv_scale[pl], (float)im * inv_scale[pl]));
+    }
   }
 }
 
 // ---------------------------------------------------------------------------
 // Adjoint post-kernel: crop the centred grid, undo the checkerboard,
-// deapodize, apply WoH, combine segments and coils.
+// deapodize, apply WoH, combine segments and coils.  CP lanes share one
+// pixel: lane c takes coils c, c+CP, ... and the lanes' images are added
+// with a fixed xor-butterfly (deterministic).
 // ---------------------------------------------------------------------------
+template <int CP>
 __global__ void k_post(NufftGeom g, int Cb, int L, const float2* __restrict__ grids, const float2* __restrict__ S,
                        int c0, const float2* __restrict__ E, const float2* __restrict__ WoH,
                        const float* __restrict__ deap, float scale, int accumulate, float2* __restrict__ x) {
   const uint64_t N = g.nimg();
-  const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= N) return;
-  const int iy = (int)(p % g.Ny);
-  const int ix = (int)((p / g.Ny) % g.Nx);
-  const int iz = (int)(p / ((uint64_t)g.Ny * g.Nx));
-  const int gy = iy + g.crop_off[1];
-  const int gx = ix + g.crop_off[0];
-  const int gz = (g.dim == 3) ? iz + g.crop_off[2] : 0;
-  const uint64_t q = (uint64_t)gy + (uint64_t)g.Gy * ((uint64_t)gx + (uint64_t)g.Gx * gz);
-  const uint64_t G = g.ngrid();
-  float k = deap[ix] * deap[g.Nx + iy];
-  if (g.dim == 3) k = k * deap[g.Nx + g.Ny + iz];
-  const bool ok = (k == k);
-  const float sgn = parity3(gx, gy, gz) ? -1.f : 1.f;
-  float2 acc = accumulate ? x[p] : make_float2(0.f, 0.f);
-  for (int c = 0; c < Cb; ++c) {
-    float2 img = make_float2(0.f, 0.f);
-    for (int l = 0; l < L; ++l) {
-      float2 v = grids[((uint64_t)c * L + l) * G + q];
-      v = make_float2(sgn * v.x, sgn * v.y);
-      v = ok ? make_float2(__fmul_rn(__fdiv_rn(v.x, k), scale), __fmul_rn(__fdiv_rn(v.y, k), scale))
-             : make_float2(0.f, 0.f);
-      if (WoH) v = cmul(v, WoH[(uint64_t)l * N + p]);
-      img = (l == 0) ? v : cadd(img, v);
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int cl = (int)(t % CP);
+  const uint64_t p = t / CP;
+  float2 acc = make_float2(0.f, 0.f);
+  if (p < N) {
+    const int iy = (int)(p % g.Ny);
+    const int ix = (int)((p / g.Ny) % g.Nx);
+    const int iz = (int)(p / ((uint64_t)g.Ny * g.Nx));
+    const int gy = iy + g.crop_off[1];
+    const int gx = ix + g.crop_off[0];
+    const int gz = (g.dim == 3) ? iz + g.crop_off[2] : 0;
+    const uint64_t q = (uint64_t)gy + (uint64_t)g.Gy * ((uint64_t)gx + (uint64_t)g.Gx * gz);
+    const uint64_t G = g.ngrid();
+    float k = deap[ix] * deap[g.Nx + iy];
+    if (g.dim == 3) k = k * deap[g.Nx + g.Ny + iz];
+    const bool ok = (k == k);
+    const float sgn = parity3(gx, gy, gz) ? -1.f : 1.f;
+    const float2 e = E ? cconj(E[p]) : make_float2(1.f, 0.f);
+    for (int c = cl; c < Cb; c += CP) {
+      float2 img = make_float2(0.f, 0.f);
+      for (int l = 0; l < L; ++l) {
+        float2 v = grids[((uint64_t)c * L + l) * G + q];
+        v = make_float2(sgn * v.x, sgn * v.y);
+        v = ok ? make_float2(__fmul_rn(__fdiv_rn(v.x, k), scale), __fmul_rn(__fdiv_rn(v.y, k), scale))
+               : make_float2(0.f, 0.f);
+        if (WoH) v = cmul(v, WoH[(uint64_t)l * N + p]);
+        img = (l == 0) ? v : cadd(img, v);
+      }
+      if (S) {
+        const float2 sv = S[(uint64_t)(c0 + c) * N + p];
+        img = E ? cmul(cmul(cconj(sv), e), img) : cmul(img, cconj(sv));
+      }
+      acc = cadd(acc, img);
     }
-    if (S) {
-      const float2 s = S[(uint64_t)(c0 + c) * N + p];
-      img = E ? cmul(cmul(cconj(s), cconj(E[p])), img) : cmul(img, cconj(s));
-    }
-    acc = cadd(acc, img);
   }
-  x[p] = acc;
+#pragma unroll
+  for (int o = CP / 2; o >= 1; o >>= 1) {
+    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+  }
+  if (p < N && cl == 0) x[p] = accumulate ? cadd(x[p], acc) : acc;
 }
 
 // ---------------------------------------------------------------------------
@@ -632,21 +667,16 @@ NufftTune NufftTune::defaults() {
   return t;
 }
 
-// Padded extent along y (the fastest axis) such that 4 x-rows of 8 y-taps
-// land in 32 distinct banks: PY = 8 or 24 (mod 32).
-static int padded_y(int T) {
-  int py = T + 8;
-  while ((py % 32) != 8 && (py % 32) != 24) ++py;
-  return py;
-}
+// Tile edges with compiled gridding kernels: 16 or 32 in 2-D, 8 in 3-D.
+static bool tile_supported(int dim, int T) { return dim == 2 ? (T == 16 || T == 32) : T == 8; }
 
 static TileShape choose_tiles(const NufftGeom& g, const NufftTune& tu) {
   TileShape t{};
   if (g.dim == 2) {
-    t.TX = t.TY = tu.tile2d; t.TZ = 1;
+    t.TX = t.TY = tile_supported(2, tu.tile2d) ? tu.tile2d : 16; t.TZ = 1;
     t.PX = t.TX + 8; t.PY = padded_y(t.TY); t.PZ = 1;
   } else {
-    t.TX = t.TY = t.TZ = tu.tile3d;
+    t.TX = t.TY = t.TZ = tile_supported(3, tu.tile3d) ? tu.tile3d : 8;
     t.PX = t.TX + 8; t.PY = padded_y(t.TY); t.PZ = t.TZ + 8;
   }
   t.ntx = (g.Gx + t.TX - 1) / t.TX;
@@ -888,25 +918,23 @@ static pg_status ensure_workspace(NufftPlan* p, int B, cufftHandle* h, cudaStrea
   return PG_OK;
 }
 
+// Forward input grids: the image region is rewritten by every forward, the
+// zero-pad border only here, when the buffer is (re)allocated.  cuFFT's
+// out-of-place C2C transform leaves its input unchanged.
+static pg_status ensure_forward_input(NufftPlan* p, int B, cudaStream_t s) {
+  const uint64_t n = (uint64_t)B * p->g.ngrid();
+  if (p->work->fin.n >= n && p->work->fin.p) return PG_OK;
+  if (p->work->fin.p) PG_CUDA(cudaStreamSynchronize(s));
+  PG_TRY(p->work->fin.alloc(n));
+  PG_CUDA(cudaMemsetAsync(p->work->fin.p, 0, n * sizeof(float2), s));
+  return PG_OK;
+}
+
 static int batch_coils(const NufftPlan* p, int C, int L) {
   const uint64_t per = (uint64_t)L * p->g.ngrid() * sizeof(float2);
   uint64_t cb = per ? p->budget_bytes / per : (uint64_t)C;
   if (cb < 1) cb = 1;
   return (int)std::min<uint64_t>(cb, (uint64_t)C);
-}
-
-// Tiled gather launch: choose the padded segment count KP and the coils per
-// block CC so that the staged tiles fit in shared memory and 2*CC*KP <= 32.
-template <int DIM, int CC, int KP>
-static pg_status gather_launch_one(NufftPlan* p, const Binning* bin, const float2* aa, int nb, float2* y,
-                                   uint64_t dstride, cudaStream_t s) {
-  const TileShape& t = bin->tile;
-  const size_t smem = (size_t)CC * KP * 2 * t.PX * t.PY * t.PZ * sizeof(float);
-  PG_CUDA(cudaFuncSetAttribute(k_gather<DIM, CC, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  dim3 grid(bin->nsub, ceil_div(nb, CC));
-  PG_LAUNCH((k_gather<DIM, CC, KP>), grid, 256, smem, s, p->g, t, bin->subprob.p, bin->start.p, bin->wxy.p,
-            bin->wz.p, bin->perm.p, aa, bin->K, bin->L, p->work->grids.p, nb, y, dstride);
-  return PG_OK;
 }
 
 static int smem_optin_bytes() {
@@ -919,31 +947,114 @@ static int smem_optin_bytes() {
   return v;
 }
 
-template <int DIM>
-static pg_status launch_gather(NufftPlan* p, const Binning* bin, const float2* aa, int nb, float2* y, uint64_t dstride,
-                               cudaStream_t s) {
+// Tiled gather launch: choose the padded segment count KP and the coils per
+// block CC so that the staged tiles fit in shared memory and 2*CC*KP <= 32.
+template <int DIM, int T, int CC, int KP>
+static pg_status gather_launch_one(NufftPlan* p, const Binning* bin, const float2* aa, int nb, float2* y,
+                                   uint64_t dstride, cudaStream_t s) {
+  const size_t smem = (size_t)CC * KP * 2 * TileGeo<DIM, T>::CELLS * sizeof(float);
+  PG_CUDA(cudaFuncSetAttribute(k_gather<DIM, T, CC, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid(bin->nsub, ceil_div(nb, CC));
+  PG_LAUNCH((k_gather<DIM, T, CC, KP>), grid, 256, smem, s, p->g, bin->tile, bin->subprob.p, bin->start.p,
+            bin->wxy.p, bin->wz.p, bin->perm.p, aa, bin->K, bin->L, p->work->grids.p, nb, y, dstride);
+  return PG_OK;
+}
+
+template <int DIM, int T>
+static pg_status launch_gather_t(NufftPlan* p, const Binning* bin, const float2* aa, int nb, float2* y,
+                                 uint64_t dstride, cudaStream_t s) {
   const int K = bin->K;
   const int KP = K <= 1 ? 1 : K <= 2 ? 2 : K <= 4 ? 4 : 8;
-  const size_t pair = (size_t)bin->tile.PX * bin->tile.PY * bin->tile.PZ * 2 * sizeof(float);
+  const size_t pair = (size_t)TileGeo<DIM, T>::CELLS * 2 * sizeof(float);
   const size_t limit = (size_t)smem_optin_bytes() - 6144;  // static reduction buffer + margin
   int CC = std::max(1, std::min(4, p->tune.gather_cc));
   while (CC > 1 && (CC >= 2 * nb || 2 * CC * KP > 32 || (size_t)CC * KP * pair > limit)) CC >>= 1;
   if ((size_t)CC * KP * pair > limit || 2 * CC * KP > 32)
     return set_error(PG_INVALID_ARG, "forward: segment window K=%d too wide for shared memory", K);
   switch (KP * 10 + CC) {
-    case 11: return gather_launch_one<DIM, 1, 1>(p, bin, aa, nb, y, dstride, s);
-    case 12: return gather_launch_one<DIM, 2, 1>(p, bin, aa, nb, y, dstride, s);
-    case 14: return gather_launch_one<DIM, 4, 1>(p, bin, aa, nb, y, dstride, s);
-    case 21: return gather_launch_one<DIM, 1, 2>(p, bin, aa, nb, y, dstride, s);
-    case 22: return gather_launch_one<DIM, 2, 2>(p, bin, aa, nb, y, dstride, s);
-    case 24: return gather_launch_one<DIM, 4, 2>(p, bin, aa, nb, y, dstride, s);
-    case 41: return gather_launch_one<DIM, 1, 4>(p, bin, aa, nb, y, dstride, s);
-    case 42: return gather_launch_one<DIM, 2, 4>(p, bin, aa, nb, y, dstride, s);
-    case 44: return gather_launch_one<DIM, 4, 4>(p, bin, aa, nb, y, dstride, s);
-    case 81: return gather_launch_one<DIM, 1, 8>(p, bin, aa, nb, y, dstride, s);
-    case 82: return gather_launch_one<DIM, 2, 8>(p, bin, aa, nb, y, dstride, s);
+    case 11: return gather_launch_one<DIM, T, 1, 1>(p, bin, aa, nb, y, dstride, s);
+    case 12: return gather_launch_one<DIM, T, 2, 1>(p, bin, aa, nb, y, dstride, s);
+    case 14: return gather_launch_one<DIM, T, 4, 1>(p, bin, aa, nb, y, dstride, s);
+    case 21: return gather_launch_one<DIM, T, 1, 2>(p, bin, aa, nb, y, dstride, s);
+    case 22: return gather_launch_one<DIM, T, 2, 2>(p, bin, aa, nb, y, dstride, s);
+    case 24: return gather_launch_one<DIM, T, 4, 2>(p, bin, aa, nb, y, dstride, s);
+    case 41: return gather_launch_one<DIM, T, 1, 4>(p, bin, aa, nb, y, dstride, s);
+    case 42: return gather_launch_one<DIM, T, 2, 4>(p, bin, aa, nb, y, dstride, s);
+    case 44: return gather_launch_one<DIM, T, 4, 4>(p, bin, aa, nb, y, dstride, s);
+    case 81: return gather_launch_one<DIM, T, 1, 8>(p, bin, aa, nb, y, dstride, s);
+    case 82: return gather_launch_one<DIM, T, 2, 8>(p, bin, aa, nb, y, dstride, s);
   }
   return set_error(PG_INVALID_ARG, "forward: unsupported tiling (K=%d)", K);
+}
+
+static pg_status launch_gather(NufftPlan* p, const Binning* bin, const float2* aa, int nb, float2* y,
+                               uint64_t dstride, cudaStream_t s) {
+  if (p->g.dim == 3) return launch_gather_t<3, 8>(p, bin, aa, nb, y, dstride, s);
+  if (bin->tile.TX == 32) return launch_gather_t<2, 32>(p, bin, aa, nb, y, dstride, s);
+  return launch_gather_t<2, 16>(p, bin, aa, nb, y, dstride, s);
+}
+
+// Spread launch arguments shared by every instantiation.
+struct SpreadArgs {
+  const float2* aa;
+  const float2* y;
+  uint64_t dstride;
+  int c0, cc, nchunks;
+  float wmax;
+  size_t smem;
+};
+
+template <int DIM, int T, int NP>
+static pg_status spread_launch_np(NufftPlan* p, const Binning* bin, const SpreadArgs& a, cudaStream_t s) {
+  PG_CUDA(cudaFuncSetAttribute(k_spread<DIM, T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.smem));
+  dim3 grid(bin->nsub, a.nchunks);
+  PG_LAUNCH((k_spread<DIM, T, NP>), grid, 256, a.smem, s, p->g, bin->tile, bin->subprob.p, bin->start.p,
+            bin->wxy.p, bin->wz.p, bin->perm.p, a.aa, bin->K, bin->L, a.y, a.dstride, a.c0, a.cc, bin->submax, a.wmax,
+            p->work->grids.p);
+  return PG_OK;
+}
+
+// Planes per block (coils x segments) with an unrolled kernel; others use the
+// runtime-loop instantiation (NP = 0).
+template <int DIM, int T>
+static pg_status spread_launch_t(NufftPlan* p, const Binning* bin, const SpreadArgs& a, cudaStream_t s) {
+  switch (a.cc * bin->K) {
+    case 1: return spread_launch_np<DIM, T, 1>(p, bin, a, s);
+    case 2: return spread_launch_np<DIM, T, 2>(p, bin, a, s);
+    case 3: return spread_launch_np<DIM, T, 3>(p, bin, a, s);
+    case 4: return spread_launch_np<DIM, T, 4>(p, bin, a, s);
+    case 6: return spread_launch_np<DIM, T, 6>(p, bin, a, s);
+    case 8: return spread_launch_np<DIM, T, 8>(p, bin, a, s);
+  }
+  return spread_launch_np<DIM, T, 0>(p, bin, a, s);
+}
+
+static pg_status launch_spread(NufftPlan* p, const Binning* bin, const SpreadArgs& a, cudaStream_t s) {
+  if (p->g.dim == 3) return spread_launch_t<3, 8>(p, bin, a, s);
+  if (bin->tile.TX == 32) return spread_launch_t<2, 32>(p, bin, a, s);
+  return spread_launch_t<2, 16>(p, bin, a, s);
+}
+
+// Post-kernel launch: CP coil lanes per pixel (a power of two, at most 8).
+static pg_status launch_post(NufftPlan* p, int nb, int L, const NufftBatch& b, int c0, float scale, int acc,
+                             float2* x, cudaStream_t s) {
+  const NufftGeom& g = p->g;
+  const uint64_t N = g.nimg();
+  const float2* grids = p->work->grids.p;
+  if (nb >= 8) {
+    PG_LAUNCH(k_post<8>, ceil_div(N * 8, 256), 256, 0, s, g, nb, L, grids, b.S, c0, b.E, b.WoH, p->deap.p, scale,
+              acc, x);
+  } else if (nb >= 4) {
+    PG_LAUNCH(k_post<4>, ceil_div(N * 4, 256), 256, 0, s, g, nb, L, grids, b.S, c0, b.E, b.WoH, p->deap.p, scale,
+              acc, x);
+  } else if (nb >= 2) {
+    PG_LAUNCH(k_post<2>, ceil_div(N * 2, 256), 256, 0, s, g, nb, L, grids, b.S, c0, b.E, b.WoH, p->deap.p, scale,
+              acc, x);
+  } else {
+    PG_LAUNCH(k_post<1>, ceil_div(N, 256), 256, 0, s, g, nb, L, grids, b.S, c0, b.E, b.WoH, p->deap.p, scale, acc,
+              x);
+  }
+  return PG_OK;
 }
 
 pg_status nufft_forward(NufftPlan* p, const NufftBatch& b, const float2* x, float2* y, cudaStream_t s) {
@@ -959,25 +1070,21 @@ pg_status nufft_forward(NufftPlan* p, const NufftBatch& b, const float2* x, floa
     const int B = nb * L;
     cufftHandle h;
     PG_TRY(ensure_workspace(p, B, &h, s));
-    dim3 grid(ceil_div(G, 256), B);
+    PG_TRY(ensure_forward_input(p, B, s));
     {
       ProfScope ps("pre", s);
-      PG_LAUNCH(k_pre, grid, 256, 0, s, g, L, x, b.S, c0, b.E, b.Wo, p->deap.p, scale, p->work->grids.p);
+      PG_LAUNCH(k_pre, dim3(ceil_div(g.nimg(), 256), B), 256, 0, s, g, L, x, b.S, c0, b.E, b.Wo, p->deap.p, scale,
+                p->work->fin.p);
     }
     {
       ProfScope ps("fft_fwd", s);
-      PG_CUFFT(cufftExecC2C(h, reinterpret_cast<cufftComplex*>(p->work->grids.p),
+      PG_CUFFT(cufftExecC2C(h, reinterpret_cast<cufftComplex*>(p->work->fin.p),
                             reinterpret_cast<cufftComplex*>(p->work->grids.p), CUFFT_FORWARD));
     }
     float2* yc = y + (uint64_t)c0 * b.data_stride;
     const float2* aa = (L > 1 || bin->aa.p) ? bin->aa.p : nullptr;
     ProfScope ps("gather", s);
-    if (bin->nsub > 0) {
-      if (g.dim == 2)
-        PG_TRY(launch_gather<2>(p, bin, aa, nb, yc, b.data_stride, s));
-      else
-        PG_TRY(launch_gather<3>(p, bin, aa, nb, yc, b.data_stride, s));
-    }
+    if (bin->nsub > 0) PG_TRY(launch_gather(p, bin, aa, nb, yc, b.data_stride, s));
   }
   return PG_OK;
 }
@@ -1012,23 +1119,22 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
     PG_TRY(ensure_workspace(p, B, &h, s));
     {
       ProfScope ps("zero", s);
-      PG_CUDA(cudaMemsetAsync(p->work->grids.p, 0, (size_t)B * G * sizeof(float2), s));
+      const uint64_t n4 = (uint64_t)B * G / 2;   // G is even: float2 pairs -> float4 words
+      PG_LAUNCH(k_zero, (unsigned)std::min<uint64_t>(ceil_div(n4, 256), 8ull * sm_count()), 256, 0, s, n4,
+                reinterpret_cast<float4*>(p->work->grids.p));
     }
-    const int cc = std::min(Cc, nb);
-    const size_t smem = smem_for(cc);
-    dim3 grid(bin->nsub, ceil_div(nb, cc));
     const float2* yc = y + (uint64_t)c0 * b.data_stride;
     const float2* aa = (L > 1 || bin->aa.p) ? bin->aa.p : nullptr;
     if (bin->nsub > 0) {
       ProfScope ps("spread", s);
-      if (g.dim == 2) {
-        PG_CUDA(cudaFuncSetAttribute(k_spread<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        PG_LAUNCH(k_spread<2>, grid, 256, smem, s, g, t, bin->subprob.p, bin->start.p, bin->wxy.p, bin->wz.p,
-                  bin->perm.p, aa, K, L, yc, b.data_stride, nb, cc, smax, wmax, p->work->grids.p);
-      } else {
-        PG_CUDA(cudaFuncSetAttribute(k_spread<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        PG_LAUNCH(k_spread<3>, grid, 256, smem, s, g, t, bin->subprob.p, bin->start.p, bin->wxy.p, bin->wz.p,
-                  bin->perm.p, aa, K, L, yc, b.data_stride, nb, cc, smax, wmax, p->work->grids.p);
+      // full chunks of cc coils, then the remaining coils in one chunk
+      const int cc = std::min(Cc, nb);
+      const int full = nb / cc, rest = nb - full * cc;
+      SpreadArgs a{aa, yc, b.data_stride, 0, cc, full, wmax, smem_for(cc)};
+      PG_TRY(launch_spread(p, bin, a, s));
+      if (rest > 0) {
+        SpreadArgs r{aa, yc, b.data_stride, full * cc, rest, 1, wmax, smem_for(rest)};
+        PG_TRY(launch_spread(p, bin, r, s));
       }
     }
     {
@@ -1038,8 +1144,7 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
     }
     const int acc = (b.accumulate || c0 > 0) ? 1 : 0;
     ProfScope ps("post", s);
-    PG_LAUNCH(k_post, ceil_div(g.nimg(), 256), 256, 0, s, g, nb, L, p->work->grids.p, b.S, c0, b.E, b.WoH, p->deap.p,
-              scale, acc, x);
+    PG_TRY(launch_post(p, nb, L, b, c0, scale, acc, x, s));
   }
   return PG_OK;
 }

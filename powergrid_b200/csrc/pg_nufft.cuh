@@ -68,7 +68,8 @@ struct Binning {
 // Grid workspace and cuFFT work area.  Plans of one geometry that run back
 // to back on one stream (the shots of pcSenseTimeSeg) share a single one.
 struct NufftWork {
-  DevBuf<float2> grids;
+  DevBuf<float2> grids;     // FFT output (forward) / spread target (adjoint)
+  DevBuf<float2> fin;       // forward FFT input; its zero-pad border stays zero
   DevBuf<char> fft_work;
 };
 

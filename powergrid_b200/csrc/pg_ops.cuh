@@ -20,8 +20,10 @@ struct pg_op_s {
   int kind = 0;
   std::unique_ptr<pg_pcg_cache_base> pcg_cache;
   uint64_t n_data = 0, n_image = 0;
-  // staging for the host-buffer entry points
-  pg::DevBuf<float2> hx, hy;
+  // staging for the host-buffer entry points (kept between calls)
+  pg::DevBuf<float2> hx, hy, hx0;
+  pg::DevBuf<float> hw;
+  pg::DevBuf<uint32_t> hit;
   virtual ~pg_op_s() {}
   virtual pg_status forward(const float2* x, float2* y, cudaStream_t s) = 0;
   virtual pg_status adjoint(const float2* y, float2* x, cudaStream_t s) = 0;

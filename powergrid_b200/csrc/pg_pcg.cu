@@ -2,10 +2,11 @@
 // regularizers (Robject.cpp:49-193, QuadPenalty.cpp:45-64, TVPenalty.cpp:43-68).
 //
 // Every vector op of an iteration is a kernel; inner products are
-// accumulated in FP64 (per-block partials, then a fixed-order sum in a
-// one-warp scalar kernel, so results are deterministic); the CG coefficient,
-// the three Newton steps and every early-exit test run on the device, so an
-// iteration needs no host synchronisation and is replayed as one CUDA graph.
+// accumulated in FP64: each block stores its partial sums and the block that
+// finishes last adds all partials in a fixed order (so results are
+// deterministic) and then evaluates the scalar step that follows (the CG
+// coefficient, a Newton step, an early-exit test) in the same launch.  No
+// step needs the host, so an iteration is replayed as one CUDA graph.
 // Early exits set a device flag that turns the remaining kernels into
 // no-ops, which returns the x of the exit point as the reference does.
 //
@@ -86,6 +87,27 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+// Block reduction of NV values; thread 0 writes part[k*nb + blockIdx.x].
+template <int NV>
+__device__ __forceinline__ void block_store(const double (&v)[NV], double* part, int nb) {
+  __shared__ double sv[NV][kRed / 32];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    const double t = warp_sum(v[k]);
+    if (l == 0) sv[k][w] = t;
+  }
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double t = (l < (int)(blockDim.x >> 5)) ? sv[k][l] : 0.0;
+      t = warp_sum(t);
+      if (l == 0) part[(size_t)k * nb + blockIdx.x] = t;
+    }
+  }
+}
+
 // Block reduction of up to 2 values; thread 0 writes part[k*nb + blockIdx.x].
 __device__ __forceinline__ void block_store2(double a, double b, double* part, int nb) {
   __shared__ double sa[kRed / 32], sb[kRed / 32];
@@ -135,10 +157,46 @@ __global__ void k_scalar_init(const double* part, int nb, double* sc, uint32_t* 
   }
 }
 
-// r = W (.) (y - Ax)
+// Last-block completion.  Every block has stored its partials (thread 0,
+// inside block_store2); the block whose ticket is the last one then sees all
+// of them.  The counter is reset for the next kernel of the stream.
+__device__ __forceinline__ bool last_block(unsigned* counter) {
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    if (last) *counter = 0u;
+  }
+  __syncthreads();
+  if (last) __threadfence();
+  return last;
+}
+
+// Fixed-order sum of part[k*nb .. k*nb+nb) by the whole (last) block.
+__device__ __forceinline__ double block_part_sum(const double* part, int nb, int k) {
+  __shared__ double red[kRed / 32];
+  __shared__ double out;
+  double v = 0.0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) v += __ldcg(part + (size_t)k * nb + i);
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    double r = (l < (int)(blockDim.x >> 5)) ? red[l] : 0.0;
+    r = warp_sum(r);
+    if (l == 0) out = r;
+  }
+  __syncthreads();
+  const double res = out;
+  __syncthreads();
+  return res;
+}
+
+// r = W (.) (y - Ax): the residual before the first iteration.
 __global__ void k_residual(uint64_t n, const float2* __restrict__ y, const float2* __restrict__ Ax,
-                           const float* __restrict__ W, float2* __restrict__ r, const uint32_t* fl) {
-  if (fl[F_DONE]) return;
+                           const float* __restrict__ W, float2* __restrict__ r) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     const float2 d = csub(y[i], Ax[i]);
     const float w = W[i];
@@ -146,9 +204,10 @@ __global__ void k_residual(uint64_t n, const float2* __restrict__ y, const float
   }
 }
 
-// ngrad = A'r - R.Gradient(x); partials |A'r|^2 and |ngrad|^2.
+// ngrad = A'r - R.Gradient(x); partials |A'r|^2 and |ngrad|^2; then the
+// early exit on a vanishing gradient (:88-91) and the CG coefficient (:95-110).
 __global__ void k_ngrad(PenDev R, const float2* __restrict__ x, float2* __restrict__ ngrad, double* part, int nb,
-                        const uint32_t* fl) {
+                        unsigned* counter, double* sc, uint32_t* fl) {
   if (fl[F_DONE]) return;
   double a = 0.0, b = 0.0;
   for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < R.N; j += (uint64_t)gridDim.x * blockDim.x) {
@@ -160,13 +219,9 @@ __global__ void k_ngrad(PenDev R, const float2* __restrict__ x, float2* __restri
     b += (double)v.x * v.x + (double)v.y * v.y;
   }
   block_store2(a, b, part, nb);
-}
-
-// Early exit on a vanishing gradient (:88-91) and the CG coefficient (:95-110).
-__global__ void k_scalar_dir(const double* part, int nb, double* sc, uint32_t* fl) {
-  if (fl[F_DONE]) return;
-  const double gn = part_sum(part, nb, 0);
-  const double nw = part_sum(part, nb, 1);
+  if (!last_block(counter)) return;
+  const double gn = block_part_sum(part, nb, 0);
+  const double nw = block_part_sum(part, nb, 1);
   if (threadIdx.x == 0) {
     if (sqrt(gn) / sc[S_YWY] < 1e-10) { fl[F_DONE] = 1; fl[F_REASON] = 1; return; }
     double gamma = 0.0;
@@ -176,9 +231,9 @@ __global__ void k_scalar_dir(const double* part, int nb, double* sc, uint32_t* f
   }
 }
 
-// ddir = ngrad + gamma ddir; partial Re<ddir, ngrad>.
-__global__ void k_ddir(uint64_t n, const float2* __restrict__ ngrad, float2* __restrict__ ddir, const double* sc,
-                       double* part, int nb, const uint32_t* fl) {
+// ddir = ngrad + gamma ddir; partial Re<ddir, ngrad>; then the descent check (:113-116).
+__global__ void k_ddir(uint64_t n, const float2* __restrict__ ngrad, float2* __restrict__ ddir, double* part, int nb,
+                       unsigned* counter, double* sc, uint32_t* fl) {
   if (fl[F_DONE]) return;
   const float gm = (float)sc[S_GAMMA];
   double a = 0.0;
@@ -190,12 +245,8 @@ __global__ void k_ddir(uint64_t n, const float2* __restrict__ ngrad, float2* __r
     a += (double)d.x * g.x + (double)d.y * g.y;
   }
   block_store2(a, 0.0, part, nb);
-}
-
-// Descent check (:113-116).
-__global__ void k_scalar_descent(const double* part, int nb, double* sc, uint32_t* fl) {
-  if (fl[F_DONE]) return;
-  const double v = part_sum(part, nb, 0);
+  if (!last_block(counter)) return;
+  const double v = block_part_sum(part, nb, 0);
   if (threadIdx.x == 0) {
     sc[S_DIRDOT] = v;
     if (v < 0) { fl[F_DONE] = 1; fl[F_REASON] = 2; }
@@ -204,7 +255,8 @@ __global__ void k_scalar_descent(const double* part, int nb, double* sc, uint32_
 
 // dAWAd = Re<Adir, W Adir>, dAWr = Re(Adir' r) (:123-125).
 __global__ void k_daw(uint64_t n, const float2* __restrict__ Adir, const float* __restrict__ W,
-                      const float2* __restrict__ r, double* part, int nb, const uint32_t* fl) {
+                      const float2* __restrict__ r, double* part, int nb, unsigned* counter, double* sc,
+                      const uint32_t* fl) {
   if (fl[F_DONE]) return;
   double a = 0.0, b = 0.0;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -214,19 +266,16 @@ __global__ void k_daw(uint64_t n, const float2* __restrict__ Adir, const float* 
     b += (double)v.x * q.x + (double)v.y * q.y;
   }
   block_store2(a, b, part, nb);
+  if (!last_block(counter)) return;
+  const double sa = block_part_sum(part, nb, 0);
+  const double sb = block_part_sum(part, nb, 1);
+  if (threadIdx.x == 0) { sc[S_DAWAD] = sa; sc[S_DAWR] = sb; sc[S_STEP] = 0.0; }
 }
 
-__global__ void k_scalar_daw(const double* part, int nb, double* sc, uint32_t* fl) {
-  if (fl[F_DONE]) return;
-  const double a = part_sum(part, nb, 0);
-  const double b = part_sum(part, nb, 1);
-  if (threadIdx.x == 0) { sc[S_DAWAD] = a; sc[S_DAWR] = b; sc[S_STEP] = 0.0; }
-}
-
-// One Newton step's penalty terms at z = x + step*ddir (:132-150):
-// pdenom = sum_dims sum wpot(Cd z) |Cd ddir|^2, pdot = Re<ddir, Gradient(z)>.
-__global__ void k_newton(PenDev R, const float2* __restrict__ x, const float2* __restrict__ ddir, const double* sc,
-                         double* part, int nb, const uint32_t* fl) {
+// One Newton step at z = x + step*ddir (:132-150): pdenom = sum_dims sum
+// wpot(Cd z) |Cd ddir|^2, pdot = Re<ddir, Gradient(z)>, then the step update.
+__global__ void k_newton(PenDev R, const float2* __restrict__ x, const float2* __restrict__ ddir, double beta,
+                         double* part, int nb, unsigned* counter, double* sc, uint32_t* fl) {
   if (fl[F_DONE]) return;
   const float st = (float)sc[S_STEP];
   double a = 0.0, b = 0.0;
@@ -244,12 +293,9 @@ __global__ void k_newton(PenDev R, const float2* __restrict__ x, const float2* _
     b += (double)dj.x * g.x + (double)dj.y * g.y;
   }
   block_store2(a, b, part, nb);
-}
-
-__global__ void k_scalar_newton(const double* part, int nb, double beta, double* sc, uint32_t* fl) {
-  if (fl[F_DONE]) return;
-  const double pden = part_sum(part, nb, 0);
-  const double pdot = part_sum(part, nb, 1);
+  if (!last_block(counter)) return;
+  const double pden = block_part_sum(part, nb, 0);
+  const double pdot = block_part_sum(part, nb, 1);
   if (threadIdx.x == 0) {
     const double denom = sc[S_DAWAD] + beta * pden;
     if (fabs(denom) < 1e-20 || fabs(denom) > 1e25 || denom != denom) { fl[F_DONE] = 1; fl[F_REASON] = 3; return; }
@@ -258,30 +304,85 @@ __global__ void k_scalar_newton(const double* part, int nb, double beta, double*
   }
 }
 
-// x += step ddir; Ax += step Adir (:160-161).
+// The three Newton steps for the quadratic penalty in one pass.  With
+// dpot(d) = d the gradient is linear, Gradient(x + s d) = Gradient(x) +
+// s Gradient(d), and wpot = 1, so pdenom does not depend on s and
+// pdot(s) = pdot(0) + s Re<ddir, Gradient(ddir)>; the last block runs the
+// reference's recurrence (:132-150) on these FP64 sums.
+__global__ void k_newton_quad(PenDev R, const float2* __restrict__ x, const float2* __restrict__ ddir, double beta,
+                              double* part, int nb, unsigned* counter, double* sc, uint32_t* fl) {
+  if (fl[F_DONE]) return;
+  double v[3] = {0.0, 0.0, 0.0};
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < R.N; j += (uint64_t)gridDim.x * blockDim.x) {
+    const float2 dj = ddir[j];
+    for (int dim = 0; dim < R.nd; ++dim) {
+      const uint64_t off = R.off[dim];
+      if (j < off || off >= R.N) continue;
+      const float2 cd = csub(dj, ddir[j - off]);
+      v[0] += (double)cd.x * cd.x + (double)cd.y * cd.y;
+    }
+    const float2 gx = grad_at(R, x, nullptr, 0.f, j);
+    const float2 gd = grad_at(R, ddir, nullptr, 0.f, j);
+    v[1] += (double)dj.x * gx.x + (double)dj.y * gx.y;
+    v[2] += (double)dj.x * gd.x + (double)dj.y * gd.y;
+  }
+  block_store<3>(v, part, nb);
+  if (!last_block(counter)) return;
+  const double pden = block_part_sum(part, nb, 0);
+  const double pdot0 = block_part_sum(part, nb, 1);
+  const double q1 = block_part_sum(part, nb, 2);
+  if (threadIdx.x == 0) {
+    const double denom = sc[S_DAWAD] + beta * pden;
+    double step = sc[S_STEP];
+    for (int k = 0; k < 3; ++k) {
+      if (fabs(denom) < 1e-20 || fabs(denom) > 1e25 || denom != denom) {
+        sc[S_STEP] = step;
+        fl[F_DONE] = 1;
+        fl[F_REASON] = 3;
+        return;
+      }
+      const double pdot = pdot0 + step * q1;
+      step = step - (-sc[S_DAWR] + step * sc[S_DAWAD] + pdot) / denom;
+    }
+    sc[S_STEP] = step;
+  }
+}
+
+// x += step ddir; Ax += step Adir (:160-161); the next residual
+// r = W (.) (y - Ax) in the same pass; then the iteration count.
 __global__ void k_update(uint64_t ni, uint64_t nd, float2* __restrict__ x, const float2* __restrict__ ddir,
-                         float2* __restrict__ Ax, const float2* __restrict__ Adir, const double* sc,
-                         const uint32_t* fl) {
+                         float2* __restrict__ Ax, const float2* __restrict__ Adir, const float2* __restrict__ y,
+                         const float* __restrict__ W, float2* __restrict__ r, unsigned* counter, const double* sc,
+                         uint32_t* fl) {
   if (fl[F_DONE]) return;
   const float st = (float)sc[S_STEP];
   const uint64_t n = ni > nd ? ni : nd;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     if (i < ni) { const float2 d = ddir[i]; float2 v = x[i]; v.x += st * d.x; v.y += st * d.y; x[i] = v; }
-    if (i < nd) { const float2 d = Adir[i]; float2 v = Ax[i]; v.x += st * d.x; v.y += st * d.y; Ax[i] = v; }
+    if (i < nd) {
+      const float2 d = Adir[i];
+      float2 v = Ax[i];
+      v.x += st * d.x; v.y += st * d.y;
+      Ax[i] = v;
+      const float2 e = csub(y[i], v);
+      const float w = W[i];
+      r[i] = make_float2(w * e.x, w * e.y);
+    }
   }
-}
-
-__global__ void k_scalar_end(uint32_t* fl) {
-  if (fl[F_DONE]) return;
-  fl[F_IT] += 1;
-  fl[F_COMPLETED] = fl[F_IT];
+  if (!last_block(counter)) return;
+  if (threadIdx.x == 0) {
+    fl[F_IT] += 1;
+    fl[F_COMPLETED] = fl[F_IT];
+  }
 }
 
 __global__ void k_copy_iters(const uint32_t* fl, uint32_t* out) { *out = fl[F_COMPLETED]; }
 
+// One element per thread up to 16 blocks per SM: small vectors still spread
+// over many SMs (these kernels are latency-bound at the usual sizes).
 int red_blocks(uint64_t n) {
-  uint64_t b = (n + 4 * kRed - 1) / (4 * kRed);
-  if (b > 592) b = 592;
+  uint64_t b = (n + kRed - 1) / kRed;
+  if (b > 2368) b = 2368;
   if (b < 1) b = 1;
   return (int)b;
 }
@@ -308,28 +409,27 @@ struct Solver {
   DevBuf<float> Wones;
   DevBuf<double> part, sc;
   DevBuf<uint32_t> fl;
+  DevBuf<unsigned> counter;   // last-block ticket, zero between kernels
   const float2* y;
   const float* W;
   int nbd, nbi;
 
+  // One PCG iteration; r = W (.) (y - Ax) holds on entry and on exit.
   pg_status iteration(cudaStream_t s) {
     const unsigned gd = (unsigned)nbd, gi = (unsigned)nbi;
-    PG_LAUNCH(k_residual, gd, kRed, 0, s, nd, y, Ax.p, W, r.p, fl.p);
     PG_TRY(A->adjoint(r.p, ngrad.p, s));
-    PG_LAUNCH(k_ngrad, gi, kRed, 0, s, R, x.p, ngrad.p, part.p, nbi, fl.p);
-    PG_LAUNCH(k_scalar_dir, 1, 32, 0, s, part.p, nbi, sc.p, fl.p);
-    PG_LAUNCH(k_ddir, gi, kRed, 0, s, ni, ngrad.p, ddir.p, sc.p, part.p, nbi, fl.p);
-    PG_LAUNCH(k_scalar_descent, 1, 32, 0, s, part.p, nbi, sc.p, fl.p);
+    PG_LAUNCH(k_ngrad, gi, kRed, 0, s, R, x.p, ngrad.p, part.p, nbi, counter.p, sc.p, fl.p);
+    PG_LAUNCH(k_ddir, gi, kRed, 0, s, ni, ngrad.p, ddir.p, part.p, nbi, counter.p, sc.p, fl.p);
     PG_TRY(A->forward(ddir.p, Adir.p, s));
-    PG_LAUNCH(k_daw, gd, kRed, 0, s, nd, Adir.p, W, r.p, part.p, nbd, fl.p);
-    PG_LAUNCH(k_scalar_daw, 1, 32, 0, s, part.p, nbd, sc.p, fl.p);
-    for (int k = 0; k < 3; ++k) {
-      PG_LAUNCH(k_newton, gi, kRed, 0, s, R, x.p, ddir.p, sc.p, part.p, nbi, fl.p);
-      PG_LAUNCH(k_scalar_newton, 1, 32, 0, s, part.p, nbi, beta, sc.p, fl.p);
+    PG_LAUNCH(k_daw, gd, kRed, 0, s, nd, Adir.p, W, r.p, part.p, nbd, counter.p, sc.p, fl.p);
+    if (R.kind == 0) {
+      PG_LAUNCH(k_newton_quad, gi, kRed, 0, s, R, x.p, ddir.p, beta, part.p, nbi, counter.p, sc.p, fl.p);
+    } else {
+      for (int k = 0; k < 3; ++k)
+        PG_LAUNCH(k_newton, gi, kRed, 0, s, R, x.p, ddir.p, beta, part.p, nbi, counter.p, sc.p, fl.p);
     }
-    PG_LAUNCH(k_update, (unsigned)red_blocks(std::max(nd, ni)), kRed, 0, s, ni, nd, x.p, ddir.p, Ax.p, Adir.p, sc.p,
-              fl.p);
-    PG_LAUNCH(k_scalar_end, 1, 1, 0, s, fl.p);
+    PG_LAUNCH(k_update, (unsigned)red_blocks(std::max(nd, ni)), kRed, 0, s, ni, nd, x.p, ddir.p, Ax.p, Adir.p, y, W,
+              r.p, counter.p, sc.p, fl.p);
     return PG_OK;
   }
 };
@@ -354,7 +454,7 @@ struct PcgCache : pg_pcg_cache_base {
   cudaGraphExec_t exec = nullptr;
   uint64_t per_iter = 0;
   pg_penalty R{};
-  bool prof = false;
+  uint64_t prof_epoch = 0;
   bool w_ones = true;
   ~PcgCache() override {
     if (exec) cudaGraphExecDestroy(exec);
@@ -362,7 +462,8 @@ struct PcgCache : pg_pcg_cache_base {
   }
   bool matches(const pg_penalty& r, bool ones) const {
     return R.kind == r.kind && R.nx == r.nx && R.ny == r.ny && R.nz == r.nz && R.beta == r.beta &&
-           R.delta == r.delta && R.dims2penalize == r.dims2penalize && prof == g_profile && w_ones == ones;
+           R.delta == r.delta && R.dims2penalize == r.dims2penalize && prof_epoch == g_profile_epoch &&
+           w_ones == ones;
   }
 };
 
@@ -383,16 +484,18 @@ pg_status make_cache(pg_op_s* A, const pg_penalty& Rh, bool w_ones, std::unique_
   PG_TRY(S.ngrad.alloc(S.ni));
   PG_TRY(S.ddir.alloc(S.ni));
   PG_TRY(S.Adir.alloc(S.nd));
-  PG_TRY(S.part.alloc(2 * (uint64_t)nb));
+  PG_TRY(S.part.alloc(3 * (uint64_t)nb));
   PG_TRY(S.sc.alloc(S_NSCAL));
   PG_TRY(S.fl.alloc(F_NFLAG));
+  PG_TRY(S.counter.alloc(1));
+  PG_CUDA(cudaMemsetAsync(S.counter.p, 0, sizeof(unsigned), s));
   PG_TRY(c->ybuf.alloc(S.nd));
   PG_TRY(c->wbuf.alloc(S.nd));
   if (w_ones) PG_LAUNCH(k_fill_ones, ceil_div(S.nd, 256), 256, 0, s, S.nd, c->wbuf.p);
   S.y = c->ybuf.p;
   S.W = c->wbuf.p;
   c->R = Rh;
-  c->prof = g_profile;
+  c->prof_epoch = g_profile_epoch;
   c->w_ones = w_ones;
   *out = std::move(c);
   return PG_OK;
@@ -431,6 +534,7 @@ pg_status pcg_solve_device(pg_op_s* A, const float2* x0, const float* W, const f
   if (st != PG_OK) { A->pcg_cache.reset(); return st; }
   PG_LAUNCH(k_ywy, (unsigned)S.nbd, kRed, 0, s, nd, S.y, S.W, S.part.p, S.nbd);
   PG_LAUNCH(k_scalar_init, 1, 32, 0, s, S.part.p, S.nbd, S.sc.p, S.fl.p);
+  PG_LAUNCH(k_residual, (unsigned)S.nbd, kRed, 0, s, nd, S.y, S.Ax.p, S.W, S.r.p);
 
   uint64_t it = 0;
   if (!cache->exec && niter > 0) {
@@ -527,18 +631,17 @@ pg_status pg_pcg_solve(pg_op A, const float* x0, const float* W, const float* y,
   if (!A || !y || !R || !x_out) return set_error(PG_INVALID_ARG, "pcg: null argument");
   PG_TRY(ensure_init());
   cudaStream_t s = default_stream();
-  DevBuf<float2> dx0, dy, dx;
-  DevBuf<float> dW;
-  DevBuf<uint32_t> it;
-  PG_TRY(dy.upload(reinterpret_cast<const float2*>(y), A->n_data, s));
-  if (x0) PG_TRY(dx0.upload(reinterpret_cast<const float2*>(x0), A->n_image, s));
-  if (W) PG_TRY(dW.upload(W, A->n_data, s));
-  PG_TRY(dx.alloc(A->n_image));
-  PG_TRY(it.alloc(1));
-  PG_TRY(pcg_solve_device(A, x0 ? dx0.p : nullptr, W ? dW.p : nullptr, dy.p, *R, niter, dx.p, it.p, s));
-  PG_CUDA(cudaMemcpyAsync(x_out, dx.p, A->n_image * sizeof(float2), cudaMemcpyDeviceToHost, s));
+  // the operator's staging buffers: no device allocation after the first call
+  PG_TRY(A->hy.upload(reinterpret_cast<const float2*>(y), A->n_data, s));
+  if (x0) PG_TRY(A->hx0.upload(reinterpret_cast<const float2*>(x0), A->n_image, s));
+  if (W) PG_TRY(A->hw.upload(W, A->n_data, s));
+  PG_TRY(A->hx.alloc(A->n_image));
+  PG_TRY(A->hit.alloc(1));
+  PG_TRY(pcg_solve_device(A, x0 ? A->hx0.p : nullptr, W ? A->hw.p : nullptr, A->hy.p, *R, niter, A->hx.p, A->hit.p,
+                          s));
+  PG_CUDA(cudaMemcpyAsync(x_out, A->hx.p, A->n_image * sizeof(float2), cudaMemcpyDeviceToHost, s));
   uint32_t n = 0;
-  PG_CUDA(cudaMemcpyAsync(&n, it.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  PG_CUDA(cudaMemcpyAsync(&n, A->hit.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   PG_CUDA(cudaStreamSynchronize(s));
   if (iters_done) *iters_done = n;
   return PG_OK;

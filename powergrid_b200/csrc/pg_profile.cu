@@ -8,6 +8,7 @@
 namespace pg {
 
 bool g_profile = false;
+uint64_t g_profile_epoch = 0;
 
 namespace {
 struct Pair {
@@ -16,6 +17,7 @@ struct Pair {
 };
 std::mutex g_mu;
 std::map<std::string, Pair> g_pairs;
+std::string g_only;   // record only this stage when non-empty
 
 Pair& get(const char* stage) {
   Pair& p = g_pairs[stage];
@@ -41,10 +43,12 @@ static void record(cudaEvent_t e, cudaStream_t s) {
 
 void prof_start(const char* stage, cudaStream_t s) {
   std::lock_guard<std::mutex> lk(g_mu);
+  if (!g_only.empty() && g_only != stage) return;
   record(get(stage).a, s);
 }
 void prof_stop(const char* stage, cudaStream_t s) {
   std::lock_guard<std::mutex> lk(g_mu);
+  if (!g_only.empty() && g_only != stage) return;
   Pair& p = get(stage);
   record(p.b, s);
   p.recorded = true;
@@ -57,6 +61,14 @@ extern "C" {
 pg_status pg_profile_enable(int on) {
   PG_TRY(pg::ensure_init());
   pg::g_profile = on != 0;
+  ++pg::g_profile_epoch;
+  return PG_OK;
+}
+
+pg_status pg_profile_only(const char* stage) {
+  std::lock_guard<std::mutex> lk(pg::g_mu);
+  pg::g_only = stage ? stage : "";
+  ++pg::g_profile_epoch;
   return PG_OK;
 }
 

@@ -6,6 +6,8 @@
 namespace pg {
 
 extern bool g_profile;
+// Changes whenever the recording set changes (captured graphs embed it).
+extern uint64_t g_profile_epoch;
 // Record the start / stop event of `stage` on stream s (no-op unless enabled).
 void prof_start(const char* stage, cudaStream_t s);
 void prof_stop(const char* stage, cudaStream_t s);
