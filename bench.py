@@ -254,7 +254,7 @@ def run_gpu_arm(args):
     launches = _lib.launches() - launches0
     sampler.__exit__(None, None, None)
 
-    stages = ["pre", "fft_fwd", "gather", "zero", "spread", "fft_adj", "post"]
+    stages = ["pre", "fft_fwd", "gather", "prep", "spread", "fft_adj", "post"]
     stage_ms = {k: [] for k in stages}
     check(L.pg_profile_only(None))
     for i in range(4):
@@ -505,7 +505,7 @@ def run_workload(name: str, steps: int, warmup: int):
                 ms.append(e0.elapsed_time(e1))
                 done += int(it.item())
         stages = {}
-        for k in ["pre", "fft_fwd", "gather", "zero", "spread", "fft_adj", "post"]:
+        for k in ["pre", "fft_fwd", "gather", "prep", "spread", "fft_adj", "post"]:
             v = C.c_float()
             if L.pg_profile_stage_ms(k.encode(), C.byref(v)) == 0:
                 stages[k] = v.value

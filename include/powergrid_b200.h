@@ -211,7 +211,7 @@ uint64_t pg_request_footprint(const pg_request* req);
 /* Stage timing: while enabled, the NUFFT and Gdft pipelines record a CUDA
  * event pair around each stage kernel on the stream they run on (also inside
  * captured CUDA graphs).  pg_profile_stage_ms returns the elapsed time of the
- * most recent recorded pair of a stage ("pre", "fft_fwd", "gather", "zero",
+ * most recent recorded pair of a stage ("pre", "fft_fwd", "gather", "prep",
  * "spread", "fft_adj", "post", "dft_fwd", "dft_adj"); the caller must have
  * synchronised the stream.  Returns PG_NOT_READY if the stage never ran. */
 pg_status pg_profile_enable(int on);

@@ -212,10 +212,24 @@ __global__ void k_pre(NufftGeom g, int L, const float2* __restrict__ x, const fl
   grids[(uint64_t)b * g.ngrid() + q] = v;
 }
 
-// Zero n float4 words (the adjoint's grid batch before the spread).
-__global__ void k_zero(uint64_t n, float4* __restrict__ p) {
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-    p[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+// Adjoint preparation in one launch: zero the batch's grids (n4 float4
+// words) and write, in binned sample order, the value each sample spreads
+// into each segment of its window, vs[c][s][j] = conj(AA(s, l0+j)) y_c[perm s].
+__global__ void k_adjoint_prep(uint64_t n4, float4* __restrict__ grids, int nb, uint64_t M, int K,
+                               const uint32_t* __restrict__ perm, const float2* __restrict__ aa,
+                               const float2* __restrict__ y, uint64_t dstride, float2* __restrict__ vs) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t t0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (uint64_t i = t0; i < n4; i += stride) grids[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int c = 0; c < nb; ++c)
+    for (uint64_t s = t0; s < M; s += stride) {
+      const float2 d = y[(uint64_t)c * dstride + perm[s]];
+      float2* o = vs + ((uint64_t)c * M + s) * K;
+      if (aa)
+        for (int j = 0; j < K; ++j) o[j] = cmul(cconj(aa[s * K + j]), d);
+      else
+        o[0] = d;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -312,7 +326,7 @@ __global__ void __launch_bounds__(256) k_gather(NufftGeom g, TileShape t, const 
   constexpr int CELLS = TG::CELLS, PY = TG::PY, PX = TG::PX, PLANE = TG::PLANE;
   constexpr int V = 2 * CC * KP;                 // accumulators per sample
   constexpr int PER = (V >= 8) ? V / 8 : 1;      // values a lane holds after the group butterfly
-  extern __shared__ __align__(16) float sm[];
+  extern __shared__ __align__(16) float2 sm2[];   // [c*KP + j][PZ][PX][PY] complex cells
   __shared__ float red[8][4][V];
   const int4 sp = sub[blockIdx.x];
   const int cfirst = blockIdx.y * CC;
@@ -337,9 +351,7 @@ __global__ void __launch_bounds__(256) k_gather(NufftGeom g, TileShape t, const 
       for (int j = 0; j < KP; ++j) {
         float2 v = make_float2(0.f, 0.f);
         if (in && c < ncl && j < K) v = grids[((uint64_t)(cfirst + c) * L + lseg + j) * G + idx];
-        float* pr = sm + ((c * KP + j) * 2) * CELLS;
-        pr[q] = v.x;
-        pr[CELLS + q] = v.y;
+        sm2[(c * KP + j) * CELLS + q] = v;
       }
   }
   __syncthreads();
@@ -350,9 +362,9 @@ __global__ void __launch_bounds__(256) k_gather(NufftGeom g, TileShape t, const 
   const int end = first + count;
   for (int s0 = first + 4 * warp; s0 < end; s0 += 4 * NW) {
     const int s = s0 + grp;
-    float acc[V];
+    float2 acc2[CC * KP];
 #pragma unroll
-    for (int i = 0; i < V; ++i) acc[i] = 0.f;
+    for (int i = 0; i < CC * KP; ++i) acc2[i] = make_float2(0.f, 0.f);
     if (s < end) {
       const uint2 st = start[s];
       const int ox = (int)(st.x & 0xffff) - x0, oy = (int)(st.x >> 16) - y0;
@@ -360,36 +372,35 @@ __global__ void __launch_bounds__(256) k_gather(NufftGeom g, TileShape t, const 
       const float4 wa = w4[0], wb = w4[1];
       const float wxr[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
       const float wyv = wxy[(uint64_t)s * 16 + 8 + dy];
-      const float* base = sm + ox * PY + oy + dy;
+      const float2* base = sm2 + ox * PY + oy + dy;
       if (DIM == 2) {
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
           const float wr = wxr[r] * wyv;
+          const float2 w2 = make_float2(wr, wr);
 #pragma unroll
-          for (int cj = 0; cj < CC * KP; ++cj) {
-            acc[2 * cj] = fmaf(wr, base[(2 * cj) * CELLS + r * PY], acc[2 * cj]);
-            acc[2 * cj + 1] = fmaf(wr, base[(2 * cj + 1) * CELLS + r * PY], acc[2 * cj + 1]);
-          }
+          for (int cj = 0; cj < CC * KP; ++cj) acc2[cj] = __ffma2_rn(w2, base[cj * CELLS + r * PY], acc2[cj]);
         }
       } else {
         const int oz = (int)st.y - z0;
         const float* wzz = wz + (uint64_t)s * 8;
-        const float* bz = base + oz * PLANE;
+        const float2* bz = base + oz * PLANE;
 #pragma unroll 1
         for (int e = 0; e < 8; ++e, bz += PLANE) {
           const float wze = wzz[e];
 #pragma unroll
           for (int r = 0; r < 8; ++r) {
             const float wr = wxr[r] * wyv * wze;
+            const float2 w2 = make_float2(wr, wr);
 #pragma unroll
-            for (int cj = 0; cj < CC * KP; ++cj) {
-              acc[2 * cj] = fmaf(wr, bz[(2 * cj) * CELLS + r * PY], acc[2 * cj]);
-              acc[2 * cj + 1] = fmaf(wr, bz[(2 * cj + 1) * CELLS + r * PY], acc[2 * cj + 1]);
-            }
+            for (int cj = 0; cj < CC * KP; ++cj) acc2[cj] = __ffma2_rn(w2, bz[cj * CELLS + r * PY], acc2[cj]);
           }
         }
       }
     }
+    float acc[V];
+#pragma unroll
+    for (int i = 0; i < CC * KP; ++i) { acc[2 * i] = acc2[i].x; acc[2 * i + 1] = acc2[i].y; }
     group8_reduce_scatter<V>(acc, lane);
     // lane dy of a group now holds values [PER*dy', PER*dy'+PER) (dy' = dy for
     // V >= 8; for V < 8 the low lanes hold the V values)
@@ -447,10 +458,9 @@ __host__ __device__ constexpr int spread_wrow(int dim) { return dim == 2 ? 16 : 
 template <int DIM, int T, int NP>
 __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const int4* __restrict__ sub,
                                                 const uint2* __restrict__ start, const float* __restrict__ wxy,
-                                                const float* __restrict__ wz, const uint32_t* __restrict__ perm,
-                                                const float2* __restrict__ aa, int K, int L,
-                                                const float2* __restrict__ data, uint64_t dstride, int c0, int cc,
-                                                int smax, float wmax, float2* __restrict__ grids) {
+                                                const float* __restrict__ wz, const float2* __restrict__ vs,
+                                                uint64_t M, int K, int L, int c0, int cc, int smax, float wmax,
+                                                float2* __restrict__ grids) {
   using TG = TileGeo<DIM, T>;
   constexpr int CELLS = TG::CELLS, PY = TG::PY, PX = TG::PX, PLANE = TG::PLANE;
   constexpr int WROW = spread_wrow(DIM);   // staged weights per sample: wx[8] wy[8] (wz[8])
@@ -492,15 +502,19 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
     reinterpret_cast<float4*>(sw + i * WROW)[a] = val;
   }
   for (int i = tid; i < count; i += blockDim.x) sst[i] = start[first + i];
-  for (int q = tid; q < count * np; q += blockDim.x) {
-    const int i = q / np, pl = q - i * np;
-    const int c = pl / K, j = pl - c * K;
-    const int s = first + i;
-    const float2 d = data[(uint64_t)(cfirst + c) * dstride + perm[s]];
-    const float2 v = aa ? cmul(cconj(aa[(uint64_t)s * K + j]), d) : d;
-    sv[q] = v;
-    // non-negative floats order like their bit patterns
-    atomicMax(&vmax[pl], __float_as_uint(fmaxf(fabsf(v.x), fabsf(v.y))));
+  // sv[i][c*K + j] = vs[cfirst + c][first + i][j]: for each coil of the block
+  // the block's samples are one contiguous run of count*K values
+  const int nk = count * K;
+  for (int c = 0; c < cc; ++c) {
+    const float2* src = vs + ((uint64_t)(cfirst + c) * M + first) * K;
+    for (int r = tid; r < nk; r += blockDim.x) {
+      const int i = (K == 1) ? r : (K == 2) ? (r >> 1) : r / K;
+      const int pl = c * K + (r - i * K);
+      const float2 v = src[r];
+      sv[i * np + pl] = v;
+      // non-negative floats order like their bit patterns
+      atomicMax(&vmax[pl], __float_as_uint(fmaxf(fabsf(v.x), fabsf(v.y))));
+    }
   }
   __syncthreads();
 
@@ -529,37 +543,87 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
   const int warp = tid >> 5, lane = tid & 31;
   constexpr int NW = 8;
   const int dy = lane & 7, dx = lane >> 3;
-  for (int i = warp; i < count; i += NW) {
-    const uint2 st = sst[i];
-    const int ox = (int)(st.x & 0xffff) - x0, oy = (int)(st.x >> 16) - y0;
-    const float* w = sw + i * WROW;
-    const float wyv = w[8 + dy];
-    const float w0 = w[dx] * wyv, w1 = w[dx + 4] * wyv;
-    int* b = smi + (ox + dx) * PY + oy + dy;
-    const float2* vi = sv + i * np;
-    if (DIM == 2) {
+  if (DIM == 2 && NP > 0) {
+    // Each warp walks a contiguous run of samples.  Samples are in readout
+    // order within a bin, so consecutive ones often share their window start;
+    // a lane then keeps hitting the same two cells, so it sums the run's
+    // contributions in registers (paired fp32 fma, fixed order) and issues
+    // the shared atomics once per run of equal starts, rounding the run sum
+    // to the integer grid.  Integer sums of the runs do not depend on the
+    // order of the atomics, so the result is deterministic.
+    constexpr int NPC = NP > 0 ? NP : 1;
+    const int per = (count + NW - 1) / NW;
+    const int i0 = warp * per, i1 = min(count, i0 + per);
+    float2 a0[NPC], a1[NPC];              // (re, im) at tap dx and dx + 4
+    uint32_t prev = 0xffffffffu;
+    int* b = smi;
+    bool open = false;
+    auto flush_run = [&]() {
 #pragma unroll
-      for (int pl = 0; pl < np; ++pl) {
-        const float2 v = vi[pl];
-        atomicAdd(b + (2 * pl) * CELLS, fixed_point(w0, v.x));
-        atomicAdd(b + (2 * pl + 1) * CELLS, fixed_point(w0, v.y));
-        atomicAdd(b + (2 * pl) * CELLS + 4 * PY, fixed_point(w1, v.x));
-        atomicAdd(b + (2 * pl + 1) * CELLS + 4 * PY, fixed_point(w1, v.y));
+      for (int pl = 0; pl < NPC; ++pl) {
+        atomicAdd(b + (2 * pl) * CELLS, __float2int_rn(a0[pl].x));
+        atomicAdd(b + (2 * pl + 1) * CELLS, __float2int_rn(a0[pl].y));
+        atomicAdd(b + (2 * pl) * CELLS + 4 * PY, __float2int_rn(a1[pl].x));
+        atomicAdd(b + (2 * pl + 1) * CELLS + 4 * PY, __float2int_rn(a1[pl].y));
       }
-    } else {
-      b += ((int)st.y - z0) * PLANE;
-#pragma unroll 1
-      for (int e = 0; e < 8; ++e, b += PLANE) {
-        const float wzv = w[16 + e];
-        if (wzv == 0.f) continue;          // uniform across the warp
-        const float w0e = w0 * wzv, w1e = w1 * wzv;
+    };
+    for (int i = i0; i < i1; ++i) {
+      const uint2 st = sst[i];
+      if (st.x != prev) {                  // uniform across the warp
+        if (open) flush_run();
+        open = true;
+        prev = st.x;
+        const int ox = (int)(st.x & 0xffff) - x0, oy = (int)(st.x >> 16) - y0;
+        b = smi + (ox + dx) * PY + oy + dy;
+#pragma unroll
+        for (int pl = 0; pl < NPC; ++pl) a0[pl] = a1[pl] = make_float2(0.f, 0.f);
+      }
+      const float* w = sw + i * WROW;
+      const float wyv = w[8 + dy];
+      const float w0 = w[dx] * wyv, w1 = w[dx + 4] * wyv;
+      const float2 w0v = make_float2(w0, w0), w1v = make_float2(w1, w1);
+      const float2* vi = sv + i * NPC;
+#pragma unroll
+      for (int pl = 0; pl < NPC; ++pl) {
+        const float2 v = vi[pl];
+        a0[pl] = __ffma2_rn(w0v, v, a0[pl]);
+        a1[pl] = __ffma2_rn(w1v, v, a1[pl]);
+      }
+    }
+    if (open) flush_run();
+  } else {
+    for (int i = warp; i < count; i += NW) {
+      const uint2 st = sst[i];
+      const int ox = (int)(st.x & 0xffff) - x0, oy = (int)(st.x >> 16) - y0;
+      const float* w = sw + i * WROW;
+      const float wyv = w[8 + dy];
+      const float w0 = w[dx] * wyv, w1 = w[dx + 4] * wyv;
+      int* b = smi + (ox + dx) * PY + oy + dy;
+      const float2* vi = sv + i * np;
+      if (DIM == 2) {
 #pragma unroll
         for (int pl = 0; pl < np; ++pl) {
           const float2 v = vi[pl];
-          atomicAdd(b + (2 * pl) * CELLS, fixed_point(w0e, v.x));
-          atomicAdd(b + (2 * pl + 1) * CELLS, fixed_point(w0e, v.y));
-          atomicAdd(b + (2 * pl) * CELLS + 4 * PY, fixed_point(w1e, v.x));
-          atomicAdd(b + (2 * pl + 1) * CELLS + 4 * PY, fixed_point(w1e, v.y));
+          atomicAdd(b + (2 * pl) * CELLS, fixed_point(w0, v.x));
+          atomicAdd(b + (2 * pl + 1) * CELLS, fixed_point(w0, v.y));
+          atomicAdd(b + (2 * pl) * CELLS + 4 * PY, fixed_point(w1, v.x));
+          atomicAdd(b + (2 * pl + 1) * CELLS + 4 * PY, fixed_point(w1, v.y));
+        }
+      } else {
+        b += ((int)st.y - z0) * PLANE;
+#pragma unroll 1
+        for (int e = 0; e < 8; ++e, b += PLANE) {
+          const float wzv = w[16 + e];
+          if (wzv == 0.f) continue;          // uniform across the warp
+          const float w0e = w0 * wzv, w1e = w1 * wzv;
+#pragma unroll
+          for (int pl = 0; pl < np; ++pl) {
+            const float2 v = vi[pl];
+            atomicAdd(b + (2 * pl) * CELLS, fixed_point(w0e, v.x));
+            atomicAdd(b + (2 * pl + 1) * CELLS, fixed_point(w0e, v.y));
+            atomicAdd(b + (2 * pl) * CELLS + 4 * PY, fixed_point(w1e, v.x));
+            atomicAdd(b + (2 * pl + 1) * CELLS + 4 * PY, fixed_point(w1e, v.y));
+          }
         }
       }
     }
@@ -575,14 +639,15 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
     const int gy = y0 + pyy, gx = x0 + pxx, gz = z0 + pzz;
     if (gy >= g.Gy || gx >= g.Gx || gz >= g.Gz) continue;
     const uint64_t idx = (uint64_t)gy + (uint64_t)g.Gy * ((uint64_t)gx + (uint64_t)g.Gx * gz);
-    for (int pl = 0; pl < np; ++pl) {
-      const int c = pl / K, j = pl - c * K;
-      const int* pr = smi + (pl * 2) * CELLS;
-      const int re = pr[q], im = pr[CELLS + q];
-      if (re != 0 || im != 0)
-        atomicAdd(grids + ((uint64_t)(cfirst + c) * L + lseg + j) * G + idx,
-                  make_float2((float)re * inv_scale[pl], (float)im * inv_scale[pl]));
-    }
+    int pl = 0;
+    for (int c = 0; c < cc; ++c)
+      for (int j = 0; j < K; ++j, ++pl) {
+        const int* pr = smi + (pl * 2) * CELLS;
+        const int re = pr[q], im = pr[CELLS + q];
+        if (re != 0 || im != 0)
+          atomicAdd(grids + ((uint64_t)(cfirst + c) * L + lseg + j) * G + idx,
+                    make_float2((float)re * inv_scale[pl], (float)im * inv_scale[pl]));
+      }
   }
 }
 
@@ -808,6 +873,9 @@ pg_status nufft_build_binning(NufftPlan* p, int L, int K, const int* l0_host, co
     for (uint64_t f = a; f < e; f += kMaxPerSub)
       subs.push_back(make_int4(tile, l, (int)f, (int)std::min<uint64_t>(kMaxPerSub, e - f)));
   }
+  // Largest subproblems first: blocks are dispatched roughly in index order,
+  // so the small ones fill the last wave instead of trailing it.
+  std::stable_sort(subs.begin(), subs.end(), [](const int4& a, const int4& c) { return a.w > c.w; });
   b->nsub = (int)subs.size();
   b->submax = kMaxPerSub;
 
@@ -996,9 +1064,7 @@ static pg_status launch_gather(NufftPlan* p, const Binning* bin, const float2* a
 
 // Spread launch arguments shared by every instantiation.
 struct SpreadArgs {
-  const float2* aa;
-  const float2* y;
-  uint64_t dstride;
+  const float2* vs;
   int c0, cc, nchunks;
   float wmax;
   size_t smem;
@@ -1009,8 +1075,7 @@ static pg_status spread_launch_np(NufftPlan* p, const Binning* bin, const Spread
   PG_CUDA(cudaFuncSetAttribute(k_spread<DIM, T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.smem));
   dim3 grid(bin->nsub, a.nchunks);
   PG_LAUNCH((k_spread<DIM, T, NP>), grid, 256, a.smem, s, p->g, bin->tile, bin->subprob.p, bin->start.p,
-            bin->wxy.p, bin->wz.p, bin->perm.p, a.aa, bin->K, bin->L, a.y, a.dstride, a.c0, a.cc, bin->submax, a.wmax,
-            p->work->grids.p);
+            bin->wxy.p, bin->wz.p, a.vs, bin->M, bin->K, bin->L, a.c0, a.cc, bin->submax, a.wmax, p->work->grids.p);
   return PG_OK;
 }
 
@@ -1117,23 +1182,26 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
     const int B = nb * L;
     cufftHandle h;
     PG_TRY(ensure_workspace(p, B, &h, s));
-    {
-      ProfScope ps("zero", s);
-      const uint64_t n4 = (uint64_t)B * G / 2;   // G is even: float2 pairs -> float4 words
-      PG_LAUNCH(k_zero, (unsigned)std::min<uint64_t>(ceil_div(n4, 256), 8ull * sm_count()), 256, 0, s, n4,
-                reinterpret_cast<float4*>(p->work->grids.p));
-    }
     const float2* yc = y + (uint64_t)c0 * b.data_stride;
     const float2* aa = (L > 1 || bin->aa.p) ? bin->aa.p : nullptr;
+    PG_TRY(grow(p->work->vs, (uint64_t)nb * bin->M * K, s));
+    {
+      ProfScope ps("prep", s);
+      const uint64_t n4 = (uint64_t)B * G / 2;   // G is even: float2 pairs -> float4 words
+      const uint64_t work = std::max<uint64_t>(n4, bin->M);
+      PG_LAUNCH(k_adjoint_prep, (unsigned)std::min<uint64_t>(ceil_div(work, 256), 8ull * sm_count()), 256, 0, s, n4,
+                reinterpret_cast<float4*>(p->work->grids.p), nb, bin->M, K, bin->perm.p, aa, yc, b.data_stride,
+                p->work->vs.p);
+    }
     if (bin->nsub > 0) {
       ProfScope ps("spread", s);
       // full chunks of cc coils, then the remaining coils in one chunk
       const int cc = std::min(Cc, nb);
       const int full = nb / cc, rest = nb - full * cc;
-      SpreadArgs a{aa, yc, b.data_stride, 0, cc, full, wmax, smem_for(cc)};
+      SpreadArgs a{p->work->vs.p, 0, cc, full, wmax, smem_for(cc)};
       PG_TRY(launch_spread(p, bin, a, s));
       if (rest > 0) {
-        SpreadArgs r{aa, yc, b.data_stride, full * cc, rest, 1, wmax, smem_for(rest)};
+        SpreadArgs r{p->work->vs.p, full * cc, rest, 1, wmax, smem_for(rest)};
         PG_TRY(launch_spread(p, bin, r, s));
       }
     }

@@ -40,7 +40,7 @@ struct TileShape {
 struct NufftTune {
   int tile2d = 16, tile3d = 8;        // measured best on cfg2 (B200): 16 > 32 > 64
   int submax2d = 256, submax3d = 256;
-  int spread_cc = 2, gather_cc = 2;
+  int spread_cc = 4, gather_cc = 2;
   static NufftTune defaults();
 };
 
@@ -70,6 +70,7 @@ struct Binning {
 struct NufftWork {
   DevBuf<float2> grids;     // FFT output (forward) / spread target (adjoint)
   DevBuf<float2> fin;       // forward FFT input; its zero-pad border stays zero
+  DevBuf<float2> vs;        // adjoint: per-sample segment values in binned order
   DevBuf<char> fft_work;
 };
 

@@ -34,7 +34,7 @@ struct PenDev {
   float beta, delta;
 };
 
-enum Scal { S_YWY = 0, S_OLD, S_GAMMA, S_DAWAD, S_DAWR, S_STEP, S_NEW, S_DIRDOT, S_NSCAL };
+enum Scal { S_YWY = 0, S_OLD, S_GAMMA, S_DAWAD, S_DAWR, S_STEP, S_NEW, S_DIRDOT, S_PDEN, S_PDOT0, S_Q1, S_NSCAL };
 enum Flag { F_DONE = 0, F_IT, F_COMPLETED, F_REASON, F_NFLAG };
 
 constexpr int kRed = 256;  // threads per reduction block
@@ -206,11 +206,15 @@ __global__ void k_residual(uint64_t n, const float2* __restrict__ y, const float
 
 // ngrad = A'r - R.Gradient(x); partials |A'r|^2 and |ngrad|^2; then the
 // early exit on a vanishing gradient (:88-91) and the CG coefficient (:95-110).
+// With ddir_prev set, the current direction is also copied there (the fused
+// quadratic k_ddir reads neighbours of the old direction while it rewrites it).
 __global__ void k_ngrad(PenDev R, const float2* __restrict__ x, float2* __restrict__ ngrad, double* part, int nb,
-                        unsigned* counter, double* sc, uint32_t* fl) {
+                        unsigned* counter, double* sc, uint32_t* fl, const float2* __restrict__ ddir,
+                        float2* __restrict__ ddir_prev) {
   if (fl[F_DONE]) return;
   double a = 0.0, b = 0.0;
   for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < R.N; j += (uint64_t)gridDim.x * blockDim.x) {
+    if (ddir_prev) ddir_prev[j] = ddir[j];
     const float2 raw = ngrad[j];
     a += (double)raw.x * raw.x + (double)raw.y * raw.y;
     const float2 g = grad_at(R, x, nullptr, 0.f, j);
@@ -253,10 +257,70 @@ __global__ void k_ddir(uint64_t n, const float2* __restrict__ ngrad, float2* __r
   }
 }
 
+// Quadratic penalty: ddir = ngrad + gamma ddir_prev, the descent product, and
+// the sums the three Newton steps need (see newton_quad_steps) in one pass.
+// Neighbour values of the new direction are formed from ngrad and ddir_prev,
+// which this kernel does not write.
+__global__ void k_ddir_quad(PenDev R, const float2* __restrict__ ngrad, const float2* __restrict__ ddir_prev,
+                            float2* __restrict__ ddir, const float2* __restrict__ x, double* part, int nb,
+                            unsigned* counter, double* sc, uint32_t* fl) {
+  if (fl[F_DONE]) return;
+  const float gm = (float)sc[S_GAMMA];
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < R.N; j += (uint64_t)gridDim.x * blockDim.x) {
+    const float2 g = ngrad[j];
+    const float2 dj = zval(ngrad, ddir_prev, gm, j);
+    ddir[j] = dj;
+    v[0] += (double)dj.x * g.x + (double)dj.y * g.y;
+    for (int dim = 0; dim < R.nd; ++dim) {
+      const uint64_t off = R.off[dim];
+      if (j < off || off >= R.N) continue;
+      const float2 cd = csub(dj, zval(ngrad, ddir_prev, gm, j - off));
+      v[1] += (double)cd.x * cd.x + (double)cd.y * cd.y;
+    }
+    const float2 gx = grad_at(R, x, nullptr, 0.f, j);
+    const float2 gd = grad_at(R, ngrad, ddir_prev, gm, j);
+    v[2] += (double)dj.x * gx.x + (double)dj.y * gx.y;
+    v[3] += (double)dj.x * gd.x + (double)dj.y * gd.y;
+  }
+  block_store<4>(v, part, nb);
+  if (!last_block(counter)) return;
+  const double dot = block_part_sum(part, nb, 0);
+  const double pden = block_part_sum(part, nb, 1);
+  const double pdot0 = block_part_sum(part, nb, 2);
+  const double q1 = block_part_sum(part, nb, 3);
+  if (threadIdx.x == 0) {
+    sc[S_DIRDOT] = dot;
+    sc[S_PDEN] = pden;
+    sc[S_PDOT0] = pdot0;
+    sc[S_Q1] = q1;
+    if (dot < 0) { fl[F_DONE] = 1; fl[F_REASON] = 2; }
+  }
+}
+
+// The three Newton steps of the quadratic penalty (:132-150) from the sums
+// k_ddir_quad stored: Gradient is linear and wpot = 1, so pdenom is fixed and
+// pdot(s) = pdot(0) + s Re<ddir, Gradient(ddir)>.
+__device__ __forceinline__ void newton_quad_steps(double beta, double* sc, uint32_t* fl) {
+  const double denom = sc[S_DAWAD] + beta * sc[S_PDEN];
+  double step = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    if (fabs(denom) < 1e-20 || fabs(denom) > 1e25 || denom != denom) {
+      sc[S_STEP] = step;
+      fl[F_DONE] = 1;
+      fl[F_REASON] = 3;
+      return;
+    }
+    const double pdot = sc[S_PDOT0] + step * sc[S_Q1];
+    step = step - (-sc[S_DAWR] + step * sc[S_DAWAD] + pdot) / denom;
+  }
+  sc[S_STEP] = step;
+}
+
 // dAWAd = Re<Adir, W Adir>, dAWr = Re(Adir' r) (:123-125).
 __global__ void k_daw(uint64_t n, const float2* __restrict__ Adir, const float* __restrict__ W,
                       const float2* __restrict__ r, double* part, int nb, unsigned* counter, double* sc,
-                      const uint32_t* fl) {
+                      uint32_t* fl, int quad, double beta) {
   if (fl[F_DONE]) return;
   double a = 0.0, b = 0.0;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -269,7 +333,12 @@ __global__ void k_daw(uint64_t n, const float2* __restrict__ Adir, const float* 
   if (!last_block(counter)) return;
   const double sa = block_part_sum(part, nb, 0);
   const double sb = block_part_sum(part, nb, 1);
-  if (threadIdx.x == 0) { sc[S_DAWAD] = sa; sc[S_DAWR] = sb; sc[S_STEP] = 0.0; }
+  if (threadIdx.x == 0) {
+    sc[S_DAWAD] = sa;
+    sc[S_DAWR] = sb;
+    sc[S_STEP] = 0.0;
+    if (quad) newton_quad_steps(beta, sc, fl);
+  }
 }
 
 // One Newton step at z = x + step*ddir (:132-150): pdenom = sum_dims sum
@@ -304,50 +373,6 @@ __global__ void k_newton(PenDev R, const float2* __restrict__ x, const float2* _
   }
 }
 
-// The three Newton steps for the quadratic penalty in one pass.  With
-// dpot(d) = d the gradient is linear, Gradient(x + s d) = Gradient(x) +
-// s Gradient(d), and wpot = 1, so pdenom does not depend on s and
-// pdot(s) = pdot(0) + s Re<ddir, Gradient(ddir)>; the last block runs the
-// reference's recurrence (:132-150) on these FP64 sums.
-__global__ void k_newton_quad(PenDev R, const float2* __restrict__ x, const float2* __restrict__ ddir, double beta,
-                              double* part, int nb, unsigned* counter, double* sc, uint32_t* fl) {
-  if (fl[F_DONE]) return;
-  double v[3] = {0.0, 0.0, 0.0};
-  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < R.N; j += (uint64_t)gridDim.x * blockDim.x) {
-    const float2 dj = ddir[j];
-    for (int dim = 0; dim < R.nd; ++dim) {
-      const uint64_t off = R.off[dim];
-      if (j < off || off >= R.N) continue;
-      const float2 cd = csub(dj, ddir[j - off]);
-      v[0] += (double)cd.x * cd.x + (double)cd.y * cd.y;
-    }
-    const float2 gx = grad_at(R, x, nullptr, 0.f, j);
-    const float2 gd = grad_at(R, ddir, nullptr, 0.f, j);
-    v[1] += (double)dj.x * gx.x + (double)dj.y * gx.y;
-    v[2] += (double)dj.x * gd.x + (double)dj.y * gd.y;
-  }
-  block_store<3>(v, part, nb);
-  if (!last_block(counter)) return;
-  const double pden = block_part_sum(part, nb, 0);
-  const double pdot0 = block_part_sum(part, nb, 1);
-  const double q1 = block_part_sum(part, nb, 2);
-  if (threadIdx.x == 0) {
-    const double denom = sc[S_DAWAD] + beta * pden;
-    double step = sc[S_STEP];
-    for (int k = 0; k < 3; ++k) {
-      if (fabs(denom) < 1e-20 || fabs(denom) > 1e25 || denom != denom) {
-        sc[S_STEP] = step;
-        fl[F_DONE] = 1;
-        fl[F_REASON] = 3;
-        return;
-      }
-      const double pdot = pdot0 + step * q1;
-      step = step - (-sc[S_DAWR] + step * sc[S_DAWAD] + pdot) / denom;
-    }
-    sc[S_STEP] = step;
-  }
-}
-
 // x += step ddir; Ax += step Adir (:160-161); the next residual
 // r = W (.) (y - Ax) in the same pass; then the iteration count.
 __global__ void k_update(uint64_t ni, uint64_t nd, float2* __restrict__ x, const float2* __restrict__ ddir,
@@ -378,11 +403,11 @@ __global__ void k_update(uint64_t ni, uint64_t nd, float2* __restrict__ x, const
 
 __global__ void k_copy_iters(const uint32_t* fl, uint32_t* out) { *out = fl[F_COMPLETED]; }
 
-// One element per thread up to 16 blocks per SM: small vectors still spread
-// over many SMs (these kernels are latency-bound at the usual sizes).
+// One element per thread up to 4 blocks per SM, then grid-stride: small
+// vectors still spread over many SMs, large ones keep the partial count low.
 int red_blocks(uint64_t n) {
   uint64_t b = (n + kRed - 1) / kRed;
-  if (b > 2368) b = 2368;
+  if (b > 592) b = 592;
   if (b < 1) b = 1;
   return (int)b;
 }
@@ -405,7 +430,7 @@ struct Solver {
   uint64_t nd, ni;
   PenDev R;
   double beta;
-  DevBuf<float2> x, Ax, r, ngrad, ddir, Adir;
+  DevBuf<float2> x, Ax, r, ngrad, ddir, Adir, ddir_prev;
   DevBuf<float> Wones;
   DevBuf<double> part, sc;
   DevBuf<uint32_t> fl;
@@ -417,17 +442,20 @@ struct Solver {
   // One PCG iteration; r = W (.) (y - Ax) holds on entry and on exit.
   pg_status iteration(cudaStream_t s) {
     const unsigned gd = (unsigned)nbd, gi = (unsigned)nbi;
+    const bool quad = R.kind == 0;
     PG_TRY(A->adjoint(r.p, ngrad.p, s));
-    PG_LAUNCH(k_ngrad, gi, kRed, 0, s, R, x.p, ngrad.p, part.p, nbi, counter.p, sc.p, fl.p);
-    PG_LAUNCH(k_ddir, gi, kRed, 0, s, ni, ngrad.p, ddir.p, part.p, nbi, counter.p, sc.p, fl.p);
+    PG_LAUNCH(k_ngrad, gi, kRed, 0, s, R, x.p, ngrad.p, part.p, nbi, counter.p, sc.p, fl.p, ddir.p,
+              quad ? ddir_prev.p : nullptr);
+    if (quad)
+      PG_LAUNCH(k_ddir_quad, gi, kRed, 0, s, R, ngrad.p, ddir_prev.p, ddir.p, x.p, part.p, nbi, counter.p, sc.p,
+                fl.p);
+    else
+      PG_LAUNCH(k_ddir, gi, kRed, 0, s, ni, ngrad.p, ddir.p, part.p, nbi, counter.p, sc.p, fl.p);
     PG_TRY(A->forward(ddir.p, Adir.p, s));
-    PG_LAUNCH(k_daw, gd, kRed, 0, s, nd, Adir.p, W, r.p, part.p, nbd, counter.p, sc.p, fl.p);
-    if (R.kind == 0) {
-      PG_LAUNCH(k_newton_quad, gi, kRed, 0, s, R, x.p, ddir.p, beta, part.p, nbi, counter.p, sc.p, fl.p);
-    } else {
+    PG_LAUNCH(k_daw, gd, kRed, 0, s, nd, Adir.p, W, r.p, part.p, nbd, counter.p, sc.p, fl.p, quad ? 1 : 0, beta);
+    if (!quad)
       for (int k = 0; k < 3; ++k)
         PG_LAUNCH(k_newton, gi, kRed, 0, s, R, x.p, ddir.p, beta, part.p, nbi, counter.p, sc.p, fl.p);
-    }
     PG_LAUNCH(k_update, (unsigned)red_blocks(std::max(nd, ni)), kRed, 0, s, ni, nd, x.p, ddir.p, Ax.p, Adir.p, y, W,
               r.p, counter.p, sc.p, fl.p);
     return PG_OK;
@@ -483,8 +511,9 @@ pg_status make_cache(pg_op_s* A, const pg_penalty& Rh, bool w_ones, std::unique_
   PG_TRY(S.r.alloc(S.nd));
   PG_TRY(S.ngrad.alloc(S.ni));
   PG_TRY(S.ddir.alloc(S.ni));
+  if (Rh.kind == PG_PENALTY_QUAD) PG_TRY(S.ddir_prev.alloc(S.ni));
   PG_TRY(S.Adir.alloc(S.nd));
-  PG_TRY(S.part.alloc(3 * (uint64_t)nb));
+  PG_TRY(S.part.alloc(4 * (uint64_t)nb));
   PG_TRY(S.sc.alloc(S_NSCAL));
   PG_TRY(S.fl.alloc(F_NFLAG));
   PG_TRY(S.counter.alloc(1));

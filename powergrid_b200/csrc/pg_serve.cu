@@ -66,6 +66,7 @@ uint64_t request_footprint(const pg_request& r) {
   uint64_t grids = C * L * G * 8;
   if (grids > kJobGridBytes) grids = std::max<uint64_t>(L * G * 8, (kJobGridBytes / (L * G * 8)) * L * G * 8);
   b += 3 * grids;                                                   // grids, forward input, cuFFT work area
+  b += C * M * 8 * std::min<uint64_t>(L, 3);                        // adjoint segment values (Hanning: K <= 3)
   b += 2 * L * N * 8 + C * N * 8;                                   // Wo, WoH, coil maps
   b += 3 * N * 8 + 3 * C * M * 8 + C * M * 8 + C * M * 4 + 64 * 1024;  // PCG state
   b += C * M * 8 + N * 8;                                           // job input / output
