@@ -46,6 +46,7 @@ struct Arena {
 };
 pg_status arena_open(Arena* a, size_t bytes, cudaStream_t s);
 void arena_install(Arena* a);   // nullptr uninstalls
+Arena* arena_current();
 void arena_release(Arena* a);   // after all work on a->stream that uses it
 
 #define PG_CUDA(call)                                                                              \
@@ -83,27 +84,40 @@ void arena_release(Arena* a);   // after all work on a->stream that uses it
                              cudaGetErrorString(e_));                                              \
   } while (0)
 
-// Owning device buffer.
+// Device buffer: owning, or a borrowed view of another buffer (borrow()),
+// which the owner must outlive.
 template <typename T>
 struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
+  bool owned = true;
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
-  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n), owned(o.owned) { o.p = nullptr; o.n = 0; o.owned = true; }
   DevBuf& operator=(DevBuf&& o) noexcept {
-    if (this != &o) { reset(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    if (this != &o) {
+      reset();
+      p = o.p; n = o.n; owned = o.owned;
+      o.p = nullptr; o.n = 0; o.owned = true;
+    }
     return *this;
   }
   ~DevBuf() { reset(); }
   void reset() {
-    if (p) dev_free(p);
+    if (p && owned) dev_free(p);
     p = nullptr;
     n = 0;
+    owned = true;
+  }
+  void borrow(const DevBuf& o) {
+    reset();
+    p = o.p;
+    n = o.n;
+    owned = false;
   }
   pg_status alloc(size_t count) {
-    if (count == n && p) return PG_OK;
+    if (count == n && p && owned) return PG_OK;
     reset();
     if (count == 0) return PG_OK;
     void* q = nullptr;
@@ -124,7 +138,7 @@ struct DevBuf {
 // read the old buffer, so drain s before replacing it.
 template <typename T>
 inline pg_status grow(DevBuf<T>& b, size_t count, cudaStream_t s) {
-  if (b.n >= count && b.p) return PG_OK;
+  if (b.n >= count && b.p && b.owned) return PG_OK;
   if (b.p) PG_CUDA(cudaStreamSynchronize(s));
   return b.alloc(count);
 }

@@ -70,6 +70,7 @@ thread_local Arena* t_arena = nullptr;
 }
 
 void arena_install(Arena* a) { t_arena = a; }
+Arena* arena_current() { return t_arena; }
 
 pg_status arena_open(Arena* a, size_t bytes, cudaStream_t s) {
   a->stream = s;

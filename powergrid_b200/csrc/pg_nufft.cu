@@ -822,6 +822,37 @@ pg_status nufft_plan_create(std::unique_ptr<NufftPlan>* out, uint64_t M, float g
   return PG_OK;
 }
 
+pg_status nufft_plan_share(const NufftPlan& src, std::unique_ptr<NufftPlan>* out) {
+  auto p = std::make_unique<NufftPlan>();
+  p->g = src.g;
+  p->tune = src.tune;
+  p->M = src.M;
+  p->lut_max = src.lut_max;
+  p->budget_bytes = src.budget_bytes;
+  p->kx.borrow(src.kx);
+  p->ky.borrow(src.ky);
+  p->kz.borrow(src.kz);
+  p->lut.borrow(src.lut);
+  p->deap.borrow(src.deap);
+  if (src.plain) p->plain = binning_share(*src.plain);
+  *out = std::move(p);
+  return PG_OK;
+}
+
+std::unique_ptr<Binning> binning_share(const Binning& b) {
+  auto o = std::make_unique<Binning>();
+  o->K = b.K; o->L = b.L; o->M = b.M; o->tile = b.tile;
+  o->nsub = b.nsub; o->submax = b.submax; o->nkeys = b.nkeys;
+  o->perm.borrow(b.perm);
+  o->start.borrow(b.start);
+  o->wxy.borrow(b.wxy);
+  o->wz.borrow(b.wz);
+  o->l0.borrow(b.l0);
+  o->aa.borrow(b.aa);
+  o->subprob.borrow(b.subprob);
+  return o;
+}
+
 pg_status nufft_plain_binning(NufftPlan* p, cudaStream_t s) {
   if (p->plain) return PG_OK;
   return nufft_build_binning(p, 1, 1, nullptr, nullptr, &p->plain, s);

@@ -109,6 +109,11 @@ pg_status nufft_plan_create(std::unique_ptr<NufftPlan>* out, uint64_t M, float g
 pg_status nufft_build_binning(NufftPlan* p, int L, int K, const int* l0_host, const float2* aa_host,
                               std::unique_ptr<Binning>* out, cudaStream_t s);
 pg_status nufft_plain_binning(NufftPlan* p, cudaStream_t s);
+// A plan that reads src's trajectory tables (src must outlive it) and has a
+// workspace of its own, so it can run concurrently with src on another stream.
+pg_status nufft_plan_share(const NufftPlan& src, std::unique_ptr<NufftPlan>* out);
+// A binning that views b's device arrays (b must outlive it).
+std::unique_ptr<Binning> binning_share(const Binning& b);
 pg_status nufft_forward(NufftPlan* p, const NufftBatch& b, const float2* x, float2* y, cudaStream_t s);
 pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, float2* x, cudaStream_t s);
 

@@ -342,6 +342,41 @@ pg_status make_timeseg(std::unique_ptr<TimeSegOp>* out, pg_op_s* G, const float*
   return PG_OK;
 }
 
+pg_status make_gnufft_shared(std::unique_ptr<GnufftOp>* out, const GnufftOp& src) {
+  auto op = std::make_unique<GnufftOp>();
+  op->kind = PG_OP_GNUFFT;
+  PG_TRY(nufft_plan_share(*src.plan, &op->plan));
+  op->n_data = src.n_data;
+  op->n_image = src.n_image;
+  *out = std::move(op);
+  return PG_OK;
+}
+
+pg_status make_timeseg_shared(std::unique_ptr<TimeSegOp>* out, pg_op_s* G, const TimeSegOp& src,
+                              const float* field_map, cudaStream_t s) {
+  if (!G || !field_map) return set_error(PG_INVALID_ARG, "TimeSegmentation: null argument");
+  if (G->n_data != src.n_data || G->n_image != src.n_image)
+    return set_error(PG_INVALID_ARG, "TimeSegmentation: shared tables do not match the inner operator");
+  for (uint64_t p = 0; p < src.n_image; ++p)
+    if (!std::isfinite(field_map[p])) return set_error(PG_INVALID_ARG, "TimeSegmentation: non-finite field map");
+  auto op = std::make_unique<TimeSegOp>();
+  op->kind = PG_OP_TIMESEG;
+  op->inner = G;
+  op->n_data = src.n_data;
+  op->n_image = src.n_image;
+  op->tab.L = src.tab.L;
+  op->tab.tau = src.tab.tau;
+  op->tab.tmin = src.tab.tmin;
+  op->tab.K = src.tab.K;
+  if (op->tab.L > 1) {
+    PG_TRY(build_ts_phases(op->tab, field_map, op->n_image, &op->Wo, &op->WoH, s));
+    if (src.bin) op->bin = binning_share(*src.bin);
+    if (src.AAfull.p) op->AAfull.borrow(src.AAfull);
+  }
+  *out = std::move(op);
+  return PG_OK;
+}
+
 pg_status make_sense(std::unique_ptr<SenseOp>* out, pg_op_s* G, const float* sense_map, uint64_t n1, uint64_t n2,
                      uint64_t nc, cudaStream_t s) {
   if (!G || !sense_map) return set_error(PG_INVALID_ARG, "SENSE: null argument");

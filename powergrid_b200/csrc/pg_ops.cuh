@@ -99,6 +99,12 @@ pg_status make_timeseg(std::unique_ptr<TimeSegOp>* out, pg_op_s* G, const float*
                        uint64_t n1, uint64_t n2, uint64_t L, uint64_t interptype, uint64_t shots, cudaStream_t s);
 pg_status make_sense(std::unique_ptr<SenseOp>* out, pg_op_s* G, const float* sense_map, uint64_t n1, uint64_t n2,
                      uint64_t nc, cudaStream_t s);
+// Operators that reuse the trajectory tables, time-segment windows and binning
+// of existing ones (which must outlive them) and own only their workspaces
+// and, for TimeSegmentation, the segment phases of their own field map.
+pg_status make_gnufft_shared(std::unique_ptr<GnufftOp>* out, const GnufftOp& src);
+pg_status make_timeseg_shared(std::unique_ptr<TimeSegOp>* out, pg_op_s* G, const TimeSegOp& src,
+                              const float* field_map, cudaStream_t s);
 // Device PWLS-PCG (pg_pcg.cu).  cancel (may be null) is polled between iterations.
 pg_status pcg_solve_device(pg_op_s* A, const float2* x0, const float* W, const float2* y, const pg_penalty& R,
                            uint64_t niter, float2* xout, uint32_t* iters_dev, cudaStream_t s,

@@ -11,6 +11,8 @@
 // (stream-ordered pool allocations, no cudaMalloc/cudaFree on the hot path)
 // until its image is copied out.
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <condition_variable>
 #include <deque>
 #include <mutex>
@@ -27,8 +29,33 @@ double now_ms() {
   return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
 }
 
+// What the slices of one request share: the trajectory tables, the
+// time-segment windows and the sample binning, built once by the request's
+// first job in an arena of their own and released with the request.
+struct SharedPlan {
+  Arena arena;
+  std::unique_ptr<GnufftOp> G;
+  std::unique_ptr<TimeSegOp> A;
+  // Runs after every job of the request has synchronised its stream.  The
+  // arena is returned on arena.stream, which the owner first points at a
+  // stream of the releasing thread: the builder's stream may be capturing a
+  // graph on another thread by then, and a free enqueued there would join
+  // that capture.
+  ~SharedPlan() {
+    Arena* prev = arena_current();
+    arena_install(&arena);
+    A.reset();
+    G.reset();
+    arena_install(prev);
+    arena_release(&arena);
+  }
+};
+
 struct Ticket {
   uint64_t id = 0;
+  std::once_flag shared_once;
+  pg_status shared_st = PG_OK;
+  std::unique_ptr<SharedPlan> shared;
   pg_request req{};
   uint64_t footprint = 0;
   int jobs_total = 0;
@@ -51,6 +78,19 @@ uint64_t grid_cells(const pg_request& r) {
 
 // Per-job grid workspace cap: keeps one job from monopolising the device.
 constexpr uint64_t kJobGridBytes = 2ull << 30;
+
+// Device bytes of a request's shared part (trajectory, binning with its
+// temporaries, segment phases of the first slice).
+uint64_t shared_footprint(const pg_request& r) {
+  const uint64_t M = r.n_samples, N = r.nx * r.ny * r.nz;
+  const uint64_t L = r.L <= 1 ? 1 : r.L;
+  uint64_t b = 3 * M * 4 + 40000 * 4 + (r.nx + r.ny + r.nz) * 4;
+  b += M * 2 * (8 + 64 + 32 + 4) + M * (4 + 4 + 3 * 8) + (M + 4096 * L) * 16;
+  b += 3 * L * N * 8;
+  return b + b / 4 + (4ull << 20);
+}
+
+void release_shared(std::unique_ptr<SharedPlan>& sp) { sp.reset(); }
 
 }  // namespace
 
@@ -89,11 +129,31 @@ struct pg_server_s {
   bool stop = false;
   uint64_t next = 1;
   std::vector<std::thread> workers;
+  bool log_errors = false;   // PG_SERVE_LOG=1: print failed jobs' messages to stderr
 
   bool head_fits() const {
     if (pending.empty()) return false;
     const uint64_t f = pending.front().t->footprint;
     return used + f <= cfg.hbm_budget_bytes || running == 0;
+  }
+
+  // The request's shared part, built by its first job (the others wait).
+  static pg_status build_shared(Ticket& T, cudaStream_t s) {
+    const pg_request& r = T.req;
+    const uint64_t N = r.nx * r.ny * r.nz, M = r.n_samples;
+    auto sp = std::make_unique<SharedPlan>();
+    PG_TRY(arena_open(&sp->arena, shared_footprint(r), s));
+    arena_install(&sp->arena);
+    pg_status st = make_gnufft(&sp->G, M, 2.0f, r.nx, r.ny, r.nz, r.kx, r.ky, r.kz, s);
+    if (st == PG_OK) st = make_timeseg(&sp->A, sp->G.get(), r.field_map, r.t, M, N, r.L, 1, 1, s);
+    if (st == PG_OK) {
+      cudaError_t e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) { cudaGetLastError(); st = set_error(PG_CUDA_ERROR, "shared plan: %s", cudaGetErrorString(e)); }
+    }
+    arena_install(nullptr);
+    T.shared = std::move(sp);
+    if (st != PG_OK) release_shared(T.shared);   // arena.stream is this thread's stream
+    return st;
   }
 
   pg_status run_job(const Job& j, cudaStream_t s, uint64_t* iters, double* setup_ms, double* solve_ms) {
@@ -102,6 +162,9 @@ struct pg_server_s {
     const uint64_t sl = j.slice;
     const double t0 = now_ms();
     double t1 = t0;
+    Ticket& T = *j.t;
+    std::call_once(T.shared_once, [&] { T.shared_st = build_shared(T, s); });
+    if (T.shared_st != PG_OK) return T.shared_st;
     Arena arena;
     PG_TRY(arena_open(&arena, j.t->footprint, s));
     arena_install(&arena);
@@ -113,10 +176,10 @@ struct pg_server_s {
       DevBuf<float2> y, x;
       DevBuf<uint32_t> it;
       do {
-        st = make_gnufft(&G, M, 2.0f, r.nx, r.ny, r.nz, r.kx, r.ky, r.kz, s);
+        st = make_gnufft_shared(&G, *T.shared->G);
         if (st != PG_OK) break;
         G->plan->budget_bytes = kJobGridBytes;
-        st = make_timeseg(&A, G.get(), r.field_map + sl * N, r.t, M, N, r.L, 1, 1, s);
+        st = make_timeseg_shared(&A, G.get(), *T.shared->A, r.field_map + sl * N, s);
         if (st != PG_OK) break;
         st = make_sense(&S, A.get(), r.sense_map + 2 * sl * N * C, M, N, C, s);
         if (st != PG_OK) break;
@@ -141,6 +204,8 @@ struct pg_server_s {
     arena_install(nullptr);
     arena_release(&arena);
     cudaStreamSynchronize(s);
+    if (cudaError_t e = cudaGetLastError())
+      if (log_errors) std::fprintf(stderr, "powergrid_b200 server: job teardown: %s\n", cudaGetErrorString(e));
     *setup_ms = t1 - t0;
     *solve_ms = now_ms() - t1;
     return st;
@@ -164,7 +229,14 @@ struct pg_server_s {
       }
       uint64_t iters = 0;
       double setup_ms = 0, solve_ms = 0;
+      std::unique_ptr<SharedPlan> done_shared;
+      if (cudaError_t stale = cudaGetLastError())   // never charge a new job with an earlier error
+        if (log_errors) std::fprintf(stderr, "powergrid_b200 server: stale error before a job: %s\n",
+                                     cudaGetErrorString(stale));
       pg_status st = job.t->cancel.load() ? PG_CANCELLED : run_job(job, s, &iters, &setup_ms, &solve_ms);
+      if (st != PG_OK && st != PG_CANCELLED && log_errors)
+        std::fprintf(stderr, "powergrid_b200 server: request %llu slice %llu: %s\n", (unsigned long long)job.t->id,
+                     (unsigned long long)job.slice, pg_last_error());
       {
         std::lock_guard<std::mutex> lk(mu);
         used -= job.t->footprint;
@@ -177,10 +249,17 @@ struct pg_server_s {
         if (--t.jobs_left == 0) {
           t.st.t_done_ms = now_ms();
           if (t.cancel.load() && t.st.status == PG_OK) t.st.status = PG_CANCELLED;
+          done_shared = std::move(t.shared);
           t.done = true;
           cv_done.notify_all();
         }
       }
+      // every job of the request has synchronised its stream
+      if (done_shared) done_shared->arena.stream = s;
+      release_shared(done_shared);
+      if (cudaError_t e = cudaGetLastError())
+        if (log_errors) std::fprintf(stderr, "powergrid_b200 server: releasing a request's shared plan: %s\n",
+                                     cudaGetErrorString(e));
       cv_work.notify_all();
     }
     if (s) cudaStreamDestroy(s);
@@ -199,6 +278,7 @@ pg_status pg_server_create(pg_server* out, const pg_server_config* cfg) {
   auto* sv = new pg_server_s;
   sv->cfg = *cfg;
   cudaGetDevice(&sv->device);
+  if (const char* e = getenv("PG_SERVE_LOG")) sv->log_errors = e[0] == '1';
   for (uint32_t i = 0; i < cfg->max_inflight; ++i) sv->workers.emplace_back([sv] { sv->worker(); });
   *out = sv;
   return PG_OK;
@@ -220,6 +300,9 @@ pg_status pg_server_destroy(pg_server sv) {
   }
   sv->cv_work.notify_all();
   for (auto& w : sv->workers) w.join();
+  // shared plans of cancelled requests: their builders' streams are gone
+  for (auto& kv : sv->tickets)
+    if (kv.second->shared) kv.second->shared->arena.stream = default_stream();
   delete sv;
   return PG_OK;
 }
