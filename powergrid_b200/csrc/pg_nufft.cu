@@ -28,6 +28,7 @@
 #include <mutex>
 #include <tuple>
 
+#include "pg_binsort.cuh"
 #include "pg_nufft.cuh"
 #include "pg_profile.cuh"
 
@@ -157,10 +158,15 @@ __global__ void k_prepare(NufftGeom g, uint64_t M, const float* __restrict__ kx,
 __global__ void k_permute(uint64_t M, int dim, int K, const uint32_t* __restrict__ perm,
                           const uint2* __restrict__ start_in, const float* __restrict__ wxy_in,
                           const float* __restrict__ wz_in, uint2* __restrict__ start_out,
-                          float* __restrict__ wxy_out, float* __restrict__ wz_out) {
+                          float* __restrict__ wxy_out, float* __restrict__ wz_out, const int* __restrict__ l0_in,
+                          const float2* __restrict__ aa_in, int* __restrict__ l0_out, float2* __restrict__ aa_out) {
   const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= M) return;
   const uint32_t i = perm[j];
+  if (l0_in) {
+    l0_out[j] = l0_in[i];
+    for (int q = 0; q < K; ++q) aa_out[j * K + q] = aa_in[(uint64_t)i * K + q];
+  }
   start_out[j] = start_in[i];
   const float4* src = reinterpret_cast<const float4*>(wxy_in + (uint64_t)i * 16);
   float4* dst = reinterpret_cast<float4*>(wxy_out + j * 16);
@@ -844,6 +850,7 @@ std::unique_ptr<Binning> binning_share(const Binning& b) {
   o->K = b.K; o->L = b.L; o->M = b.M; o->tile = b.tile;
   o->nsub = b.nsub; o->submax = b.submax; o->nkeys = b.nkeys;
   o->perm.borrow(b.perm);
+  o->keys.borrow(b.keys);
   o->start.borrow(b.start);
   o->wxy.borrow(b.wxy);
   o->wz.borrow(b.wz);
@@ -881,23 +888,21 @@ pg_status nufft_build_binning(NufftPlan* p, int L, int K, const int* l0_host, co
   if (l0_host) PG_TRY(l0d.upload(l0_host, M, s));
   PG_LAUNCH(k_prepare, ceil_div(M, 256), 256, 0, s, g, M, p->kx.p, p->ky.p, p->kz.p, p->lut.p, t,
             l0_host ? l0d.p : nullptr, st_o.p, wxy_o.p, g.dim == 3 ? wz_o.p : nullptr, key.p);
-  b->h_keys.resize(M);
-  PG_CUDA(cudaMemcpyAsync(b->h_keys.data(), key.p, M * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  PG_CUDA(cudaStreamSynchronize(s));
 
-  // Stable counting sort by key on the host (plan time, O(M + bins)).
-  std::vector<uint64_t> cnt(b->nkeys + 1, 0);
-  for (uint64_t i = 0; i < M; ++i) cnt[b->h_keys[i] + 1]++;
-  for (uint64_t k = 0; k < b->nkeys; ++k) cnt[k + 1] += cnt[k];
-  std::vector<uint64_t> pos(cnt.begin(), cnt.end() - 1);
-  b->h_perm.resize(M);
-  for (uint64_t i = 0; i < M; ++i) b->h_perm[pos[b->h_keys[i]]++] = (uint32_t)i;
+  // Stable counting sort by key on the device (bit-exact against a CPU one).
+  DevBuf<uint32_t> starts_d;
+  PG_TRY(b->perm.alloc(M));
+  PG_TRY(starts_d.alloc(b->nkeys));
+  PG_TRY(bin_sort(key.p, M, b->nkeys, b->perm.p, starts_d.p, s));
+  std::vector<uint32_t> starts(b->nkeys);
+  PG_CUDA(cudaMemcpyAsync(starts.data(), starts_d.p, b->nkeys * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  PG_CUDA(cudaStreamSynchronize(s));
 
   // Subproblems: each (segment window, tile) bin split into chunks.
   const int kMaxPerSub = (g.dim == 2) ? p->tune.submax2d : p->tune.submax3d;
   std::vector<int4> subs;
   for (uint64_t k = 0; k < b->nkeys; ++k) {
-    const uint64_t a = cnt[k], e = cnt[k + 1];
+    const uint64_t a = starts[k], e = (k + 1 < b->nkeys) ? starts[k + 1] : M;
     if (a == e) continue;
     const int l = (int)(k / ntiles);
     const int tile = (int)(k % ntiles);
@@ -910,24 +915,21 @@ pg_status nufft_build_binning(NufftPlan* p, int L, int K, const int* l0_host, co
   b->nsub = (int)subs.size();
   b->submax = kMaxPerSub;
 
-  PG_TRY(b->perm.upload(b->h_perm.data(), M, s));
   PG_TRY(b->subprob.upload(subs.data(), subs.size(), s));
   PG_TRY(b->start.alloc(M));
   PG_TRY(b->wxy.alloc(M * 16));
   if (g.dim == 3) PG_TRY(b->wz.alloc(M * 8));
-  PG_LAUNCH(k_permute, ceil_div(M, 256), 256, 0, s, M, g.dim, K, b->perm.p, st_o.p, wxy_o.p,
-            g.dim == 3 ? wz_o.p : nullptr, b->start.p, b->wxy.p, g.dim == 3 ? b->wz.p : nullptr);
+  DevBuf<float2> aa_d;
   if (l0_host) {
-    std::vector<int> l0s(M);
-    std::vector<float2> aas(M * (uint64_t)K);
-    for (uint64_t j = 0; j < M; ++j) {
-      const uint32_t i = b->h_perm[j];
-      l0s[j] = l0_host[i];
-      for (int q = 0; q < K; ++q) aas[j * K + q] = aa_host[(uint64_t)i * K + q];
-    }
-    PG_TRY(b->l0.upload(l0s.data(), M, s));
-    PG_TRY(b->aa.upload(aas.data(), aas.size(), s));
+    PG_TRY(aa_d.upload(aa_host, M * (uint64_t)K, s));
+    PG_TRY(b->l0.alloc(M));
+    PG_TRY(b->aa.alloc(M * (uint64_t)K));
   }
+  PG_LAUNCH(k_permute, ceil_div(M, 256), 256, 0, s, M, g.dim, K, b->perm.p, st_o.p, wxy_o.p,
+            g.dim == 3 ? wz_o.p : nullptr, b->start.p, b->wxy.p, g.dim == 3 ? b->wz.p : nullptr,
+            l0_host ? l0d.p : nullptr, l0_host ? aa_d.p : nullptr, l0_host ? b->l0.p : nullptr,
+            l0_host ? b->aa.p : nullptr);
+  b->keys = std::move(key);
   PG_CUDA(cudaStreamSynchronize(s));
   *out = std::move(b);
   return PG_OK;

@@ -58,11 +58,10 @@ struct Binning {
   DevBuf<int> l0;            // segment-window start per sample
   DevBuf<float2> aa;         // K per sample: interpolator values AA(m, l0..l0+K-1)
   DevBuf<int4> subprob;      // (tile index, l0, first sorted sample, count)
+  DevBuf<uint32_t> keys;     // bin key per original sample
   int nsub = 0;
   int submax = 0;            // most samples in one subproblem
   uint64_t nkeys = 0;
-  std::vector<uint32_t> h_keys;   // bin key per original sample (tests)
-  std::vector<uint32_t> h_perm;
 };
 
 // Grid workspace and cuFFT work area.  Plans of one geometry that run back

@@ -567,8 +567,12 @@ pg_status pg_util_gnufft_binning(pg_op G, uint32_t* keys_out, uint32_t* perm_out
   }
   else if (G->kind == PG_OP_TIMESEG && static_cast<TimeSegOp*>(G)->bin) b = static_cast<TimeSegOp*>(G)->bin.get();
   if (!b) return set_error(PG_INVALID_ARG, "operator has no sample binning");
-  if (keys_out) std::memcpy(keys_out, b->h_keys.data(), b->h_keys.size() * sizeof(uint32_t));
-  if (perm_out) std::memcpy(perm_out, b->h_perm.data(), b->h_perm.size() * sizeof(uint32_t));
+  cudaStream_t s = default_stream();
+  if (keys_out)
+    PG_CUDA(cudaMemcpyAsync(keys_out, b->keys.p, b->M * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  if (perm_out)
+    PG_CUDA(cudaMemcpyAsync(perm_out, b->perm.p, b->M * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  PG_CUDA(cudaStreamSynchronize(s));
   if (n_bins_out) *n_bins_out = b->nkeys;
   return PG_OK;
 }

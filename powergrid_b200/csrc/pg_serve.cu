@@ -86,6 +86,10 @@ uint64_t shared_footprint(const pg_request& r) {
   const uint64_t L = r.L <= 1 ? 1 : r.L;
   uint64_t b = 3 * M * 4 + 40000 * 4 + (r.nx + r.ny + r.nz) * 4;
   b += M * 2 * (8 + 64 + 32 + 4) + M * (4 + 4 + 3 * 8) + (M + 4096 * L) * 16;
+  // device bin sort: (key, chunk) table (at most 16 M entries), bin starts, keys
+  const uint64_t nkeys = (r.nz > 1 ? (r.nx / 4 + 1) * (r.ny / 4 + 1) * (r.nz / 4 + 1)
+                                   : (r.nx / 8 + 1) * (r.ny / 8 + 1)) * L;
+  b += std::min<uint64_t>(nkeys * ((M + 1023) / 1024), 16ull << 20) * 4 + nkeys * 4 + M * 4 + M * 3 * 8;
   b += 3 * L * N * 8;
   return b + b / 4 + (4ull << 20);
 }

@@ -125,6 +125,7 @@ class Gnufft(_Op):
         super().__init__(h)
 
     def binning(self):
+        """(bin key per sample, sorted order, number of bins) of the device binning."""
         keys = np.zeros(self.n_data, np.uint32)
         perm = np.zeros(self.n_data, np.uint32)
         nb = U64()
@@ -151,6 +152,9 @@ class TimeSegmentation(_Op):
         check(_lib.load().pg_timeseg_create(C.byref(h), G.handle, _ptr(fm), _ptr(tv), int(n1), int(n2), int(L),
                                              int(interptype), int(shots)))
         super().__init__(h, keep=[G])
+
+
+TimeSegmentation.binning = Gnufft.binning
 
 
 class SENSE(_Op):

@@ -92,6 +92,25 @@ def test_binning_is_a_stable_cpu_sort(pg):
     assert np.array_equal(perm, np.argsort(keys, kind="stable").astype(np.uint32))
 
 
+@pytest.mark.parametrize("three_d", [False, True])
+def test_device_binning_matches_stable_sort_at_size(pg, three_d):
+    """The device counting sort behind the time-segmented adjoint (segment
+    window x tile keys, 131072 samples; in 3-D a 64x64x32 stack of spirals)
+    equals numpy's stable argsort of the same keys, bit for bit."""
+    from powergrid_b200 import synthetic as S
+    if three_d:
+        p = S.config3()
+        p.L = 6
+    else:
+        p = S.config2()
+    M, n = p.kx.size, p.nimg
+    G = pg.Gnufft(M, 2.0, p.nx, p.ny, p.nz, p.kx, p.ky, p.kz)
+    A = pg.TimeSegmentation(G, p.fm, p.t, M, n, p.L, 1, 1)
+    keys, perm, nb = A.binning()
+    assert keys.max() < nb
+    assert np.array_equal(perm, np.argsort(keys, kind="stable").astype(np.uint32))
+
+
 @pytest.mark.parametrize("name", ["nufft2d", "nufft3d", "tssense2d"])
 def test_adjointness(pg, name):
     """<A x, y> = <x, A^H y> (even grid sizes make fftshift = ifftshift)."""
