@@ -433,6 +433,7 @@ def run_serving(n_requests: int = 16, rate_hz: float = 20.0, inflight: int = 8, 
                 "latency_ms_p50": lat[len(lat) // 2], "latency_ms_p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]}
 
     serve(inflight)  # warm-up: module loading, pool growth
+    direct()         # warm-up: per-shape gridding tunings are cached for both forms
     plain = direct()
     served_one = serve(1)
     served = serve(inflight)

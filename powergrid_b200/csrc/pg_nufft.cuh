@@ -117,11 +117,12 @@ pg_status nufft_forward(NufftPlan* p, const NufftBatch& b, const float2* x, floa
 pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, float2* x, cudaStream_t s);
 
 // Choose tile edge, bin size and coils per block for a batch of C coils by
-// timing candidates on stream s (cached per problem shape), and leave the
-// matching binning in *bin (kept if it already matches).  l0_host/aa_host as
-// for nufft_build_binning.
+// timing candidates on stream s (cached per problem shape; with search =
+// false only a cached choice or the defaults), and leave the matching
+// binning in *bin (kept if it already matches).  l0_host/aa_host as for
+// nufft_build_binning.
 pg_status nufft_autotune(NufftPlan* p, int L, int K, const int* l0_host, const float2* aa_host, int C,
-                         std::unique_ptr<Binning>* bin, cudaStream_t s);
+                         std::unique_ptr<Binning>* bin, bool search, cudaStream_t s);
 
 // Host copies of the LUT and beta exactly as Gnufft builds them.
 void kb_table(float gridos, std::vector<float>* lut, float* beta);

@@ -377,17 +377,18 @@ pg_status make_timeseg_shared(std::unique_ptr<TimeSegOp>* out, pg_op_s* G, const
   return PG_OK;
 }
 
-pg_status tune_for_coils(pg_op_s* G, int nc, cudaStream_t s) {
+pg_status tune_for_coils(pg_op_s* G, int nc, bool search, cudaStream_t s) {
   if (G->kind == PG_OP_GNUFFT) {
     NufftPlan* plan = static_cast<GnufftOp*>(G)->plan.get();
-    return nufft_autotune(plan, 1, 1, nullptr, nullptr, nc, &plan->plain, s);
+    return nufft_autotune(plan, 1, 1, nullptr, nullptr, nc, &plan->plain, search, s);
   }
   if (G->kind == PG_OP_TIMESEG) {
     auto* t = static_cast<TimeSegOp*>(G);
     // operators sharing another one's tables inherit its tuning
     if (t->inner->kind != PG_OP_GNUFFT || t->tab.L <= 1 || t->tab.l0.empty()) return PG_OK;
     NufftPlan* plan = static_cast<GnufftOp*>(t->inner)->plan.get();
-    return nufft_autotune(plan, t->tab.L, t->tab.K, t->tab.l0.data(), t->tab.aa_win.data(), nc, &t->bin, s);
+    return nufft_autotune(plan, t->tab.L, t->tab.K, t->tab.l0.data(), t->tab.aa_win.data(), nc, &t->bin, search,
+                          s);
   }
   return PG_OK;
 }
@@ -404,7 +405,7 @@ pg_status make_sense(std::unique_ptr<SenseOp>* out, pg_op_s* G, const float* sen
   op->n_data = n1 * nc;
   op->n_image = n2;
   PG_TRY(op->S.upload(reinterpret_cast<const float2*>(sense_map), n2 * nc, s));
-  PG_TRY(tune_for_coils(G, (int)nc, s));
+  PG_TRY(tune_for_coils(G, (int)nc, true, s));
   PG_CUDA(cudaStreamSynchronize(s));
   *out = std::move(op);
   return PG_OK;
@@ -489,7 +490,7 @@ pg_status pg_pcsense_timeseg_create(pg_op* out, const float* kx, const float* ky
     if (op->tabs[sh].L > 1) {
       PG_TRY(build_ts_phases(op->tabs[sh], field_map, Ni, &op->Wo[sh], &op->WoH[sh], s));
       PG_TRY(nufft_autotune(plan.get(), op->tabs[sh].L, op->tabs[sh].K, op->tabs[sh].l0.data(),
-                            op->tabs[sh].aa_win.data(), (int)nc, &op->bins[sh], s));
+                            op->tabs[sh].aa_win.data(), (int)nc, &op->bins[sh], true, s));
       op->tabs[sh].AA.clear();
       op->tabs[sh].AA.shrink_to_fit();
     }

@@ -100,8 +100,9 @@ pg_status make_timeseg(std::unique_ptr<TimeSegOp>* out, pg_op_s* G, const float*
 pg_status make_sense(std::unique_ptr<SenseOp>* out, pg_op_s* G, const float* sense_map, uint64_t n1, uint64_t n2,
                      uint64_t nc, cudaStream_t s);
 // Autotune the gridding under G (Gnufft or TimeSegmentation<Gnufft>) for
-// batches of nc coils; no-op for other operators.
-pg_status tune_for_coils(pg_op_s* G, int nc, cudaStream_t s);
+// batches of nc coils (search = false: cached choices only); no-op for other
+// operators.
+pg_status tune_for_coils(pg_op_s* G, int nc, bool search, cudaStream_t s);
 // Operators that reuse the trajectory tables, time-segment windows and binning
 // of existing ones (which must outlive them) and own only their workspaces
 // and, for TimeSegmentation, the segment phases of their own field map.

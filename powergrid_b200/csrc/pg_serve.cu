@@ -150,9 +150,8 @@ struct pg_server_s {
     arena_install(&sp->arena);
     pg_status st = make_gnufft(&sp->G, M, 2.0f, r.nx, r.ny, r.nz, r.kx, r.ky, r.kz, s);
     if (st == PG_OK) st = make_timeseg(&sp->A, sp->G.get(), r.field_map, r.t, M, N, r.L, 1, 1, s);
-    if (st == PG_OK) st = tune_for_coils(sp->A.get(), (int)r.nc, s);
-    // the tuning runs used a workspace the jobs never touch
-    if (st == PG_OK) sp->G->plan->work = std::make_shared<NufftWork>();
+    // a search per request would stall the slots: cached tunings only
+    if (st == PG_OK) st = tune_for_coils(sp->A.get(), (int)r.nc, false, s);
     if (st == PG_OK) {
       cudaError_t e = cudaStreamSynchronize(s);
       if (e != cudaSuccess) { cudaGetLastError(); st = set_error(PG_CUDA_ERROR, "shared plan: %s", cudaGetErrorString(e)); }

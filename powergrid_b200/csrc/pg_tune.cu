@@ -7,7 +7,9 @@
 // values), in two rounds: tile x bin size with the default coils per block,
 // then the coils per block for the winning binning.  Results are cached per
 // problem shape (dimension, image and sample counts, segments, window, coil
-// batch), so operators of a recurring shape are tuned once per process.
+// batch; the sample count by its power-of-two bucket), so operators of a
+// recurring shape are tuned once per process.  Callers that cannot afford a
+// search (the request server) only take cached results.
 // PG_AUTOTUNE=0 keeps the defaults (and the PG_TILE2D ... overrides).
 #include <map>
 #include <mutex>
@@ -19,14 +21,19 @@
 namespace pg {
 namespace {
 
+// Problem shape; the sample count enters as its power-of-two bucket, so
+// trajectories of similar length share a tuning.
 struct TuneKey {
-  int dim, nx, ny, nz;
-  uint64_t M;
-  int L, K, C;
+  int dim, nx, ny, nz, mlog, L, K, C;
   bool operator<(const TuneKey& o) const {
-    return std::tie(dim, nx, ny, nz, M, L, K, C) < std::tie(o.dim, o.nx, o.ny, o.nz, o.M, o.L, o.K, o.C);
+    return std::tie(dim, nx, ny, nz, mlog, L, K, C) < std::tie(o.dim, o.nx, o.ny, o.nz, o.mlog, o.L, o.K, o.C);
   }
 };
+int log2_bucket(uint64_t v) {
+  int b = 0;
+  while ((2ull << b) <= v) ++b;
+  return b;
+}
 std::mutex g_tune_mu;
 std::map<TuneKey, NufftTune> g_tuned;
 
@@ -64,10 +71,10 @@ float time_ms(F&& f, cudaStream_t s, int reps) {
 }  // namespace
 
 pg_status nufft_autotune(NufftPlan* p, int L, int K, const int* l0_host, const float2* aa_host, int C,
-                         std::unique_ptr<Binning>* bin, cudaStream_t s) {
+                         std::unique_ptr<Binning>* bin, bool search, cudaStream_t s) {
   const NufftGeom& g = p->g;
   const int Ct = std::max(1, std::min(C, 4));
-  const TuneKey key{g.dim, g.Nx, g.Ny, g.Nz, p->M, L, K, Ct};
+  const TuneKey key{g.dim, g.Nx, g.Ny, g.Nz, log2_bucket(p->M), L, K, Ct};
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tuned.find(key);
@@ -80,7 +87,7 @@ pg_status nufft_autotune(NufftPlan* p, int L, int K, const int* l0_host, const f
       return PG_OK;
     }
   }
-  if (!tuning_enabled()) {
+  if (!search || !tuning_enabled()) {
     if (!*bin) return nufft_build_binning(p, L, K, l0_host, aa_host, bin, s);
     return PG_OK;
   }
