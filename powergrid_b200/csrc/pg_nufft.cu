@@ -190,8 +190,8 @@ __device__ __forceinline__ int parity3(int a, int b, int c) { return (a + b + c)
 // One thread per (pixel, grid of the batch).
 // ---------------------------------------------------------------------------
 __global__ void k_pre(NufftGeom g, int L, const float2* __restrict__ x, const float2* __restrict__ S, int c0,
-                      const float2* __restrict__ E, const float2* __restrict__ Wo, const float* __restrict__ deap,
-                      float scale, float2* __restrict__ grids) {
+                      const float2* __restrict__ E, const float2* __restrict__ Wo, const float* __restrict__ deapf,
+                      float2* __restrict__ grids) {
   const uint64_t N = g.nimg();
   const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= N) return;
@@ -210,11 +210,8 @@ __global__ void k_pre(NufftGeom g, int L, const float2* __restrict__ x, const fl
     v = E ? cmul(v, cmul(sv, E[p])) : cmul(sv, v);
   }
   if (Wo) v = cmul(Wo[(uint64_t)l * N + p], v);
-  float k = deap[ix] * deap[g.Nx + iy];
-  if (g.dim == 3) k = k * deap[g.Nx + g.Ny + iz];
-  v = (k == k) ? make_float2(__fmul_rn(__fdiv_rn(v.x, k), scale), __fmul_rn(__fdiv_rn(v.y, k), scale))
-               : make_float2(0.f, 0.f);
-  if (parity3(mx, my, mz)) v = make_float2(-v.x, -v.y);
+  const float f = parity3(mx, my, mz) ? -deapf[p] : deapf[p];
+  v = make_float2(v.x * f, v.y * f);
   grids[(uint64_t)b * g.ngrid() + q] = v;
 }
 
@@ -659,18 +656,20 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
 
 // ---------------------------------------------------------------------------
 // Adjoint post-kernel: crop the centred grid, undo the checkerboard,
-// deapodize, apply WoH, combine segments and coils.  CP lanes share one
-// pixel: lane c takes coils c, c+CP, ... and the lanes' images are added
-// with a fixed xor-butterfly (deterministic).
+// deapodize, apply WoH, combine segments and coils.  CP x LP lanes share one
+// pixel: lane (c, h) takes coils c, c+CP, ... and segments h, h+LP, ...; the
+// lanes' images are added with a fixed xor-butterfly (deterministic).
 // ---------------------------------------------------------------------------
-template <int CP>
+template <int CP, int LP>
 __global__ void k_post(NufftGeom g, int Cb, int L, const float2* __restrict__ grids, const float2* __restrict__ S,
                        int c0, const float2* __restrict__ E, const float2* __restrict__ WoH,
-                       const float* __restrict__ deap, float scale, int accumulate, float2* __restrict__ x) {
+                       const float* __restrict__ deapf, int accumulate, float2* __restrict__ x) {
+  constexpr int LN = CP * LP;
   const uint64_t N = g.nimg();
   const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int cl = (int)(t % CP);
-  const uint64_t p = t / CP;
+  const int ln = (int)(t % LN);
+  const int cl = ln / LP, hl = ln % LP;
+  const uint64_t p = t / LN;
   float2 acc = make_float2(0.f, 0.f);
   if (p < N) {
     const int iy = (int)(p % g.Ny);
@@ -681,20 +680,16 @@ __global__ void k_post(NufftGeom g, int Cb, int L, const float2* __restrict__ gr
     const int gz = (g.dim == 3) ? iz + g.crop_off[2] : 0;
     const uint64_t q = (uint64_t)gy + (uint64_t)g.Gy * ((uint64_t)gx + (uint64_t)g.Gx * gz);
     const uint64_t G = g.ngrid();
-    float k = deap[ix] * deap[g.Nx + iy];
-    if (g.dim == 3) k = k * deap[g.Nx + g.Ny + iz];
-    const bool ok = (k == k);
-    const float sgn = parity3(gx, gy, gz) ? -1.f : 1.f;
+    const float f = parity3(gx, gy, gz) ? -deapf[p] : deapf[p];
     const float2 e = E ? cconj(E[p]) : make_float2(1.f, 0.f);
     for (int c = cl; c < Cb; c += CP) {
       float2 img = make_float2(0.f, 0.f);
-      for (int l = 0; l < L; ++l) {
+#pragma unroll 4
+      for (int l = hl; l < L; l += LP) {
         float2 v = grids[((uint64_t)c * L + l) * G + q];
-        v = make_float2(sgn * v.x, sgn * v.y);
-        v = ok ? make_float2(__fmul_rn(__fdiv_rn(v.x, k), scale), __fmul_rn(__fdiv_rn(v.y, k), scale))
-               : make_float2(0.f, 0.f);
+        v = make_float2(v.x * f, v.y * f);
         if (WoH) v = cmul(v, WoH[(uint64_t)l * N + p]);
-        img = (l == 0) ? v : cadd(img, v);
+        img = cadd(img, v);
       }
       if (S) {
         const float2 sv = S[(uint64_t)(c0 + c) * N + p];
@@ -704,11 +699,11 @@ __global__ void k_post(NufftGeom g, int Cb, int L, const float2* __restrict__ gr
     }
   }
 #pragma unroll
-  for (int o = CP / 2; o >= 1; o >>= 1) {
+  for (int o = LN / 2; o >= 1; o >>= 1) {
     acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
     acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
   }
-  if (p < N && cl == 0) x[p] = accumulate ? cadd(x[p], acc) : acc;
+  if (p < N && ln == 0) x[p] = accumulate ? cadd(x[p], acc) : acc;
 }
 
 // ---------------------------------------------------------------------------
@@ -822,6 +817,22 @@ pg_status nufft_plan_create(std::unique_ptr<NufftPlan>* out, uint64_t M, float g
   PG_TRY(p->lut.upload(lut.data(), lut.size(), s));
   p->lut_max = *std::max_element(lut.begin(), lut.end());
   PG_TRY(p->deap.upload(deap.data(), deap.size(), s));
+  // Per-voxel deapodization factor 1/(OS^d k), k the product of the axis
+  // factors in float as the reference forms it; 0 where k is NaN (the
+  // reference zeroes those voxels, griddingSupport.cpp:265-278).
+  {
+    const float scale = (g.dim == 2) ? (1.0f / (gridos * gridos)) : (float)(1.0 / (double)(gridos * gridos * gridos));
+    std::vector<float> f((uint64_t)nx * ny * nz);
+    for (int z = 0; z < nz; ++z)
+      for (int xx = 0; xx < nx; ++xx)
+        for (int yy = 0; yy < ny; ++yy) {
+          float k = deap[xx] * deap[nx + yy];
+          if (g.dim == 3) k = k * deap[nx + ny + z];
+          f[(uint64_t)yy + (uint64_t)ny * ((uint64_t)xx + (uint64_t)nx * z)] =
+              (k == k) ? (float)((double)scale / (double)k) : 0.f;
+        }
+    PG_TRY(p->deapf.upload(f.data(), f.size(), s));
+  }
   PG_CUDA(cudaStreamSynchronize(s));
   // the unsegmented binning is built on first use (time-segmented operators never need it)
   *out = std::move(p);
@@ -840,6 +851,7 @@ pg_status nufft_plan_share(const NufftPlan& src, std::unique_ptr<NufftPlan>* out
   p->kz.borrow(src.kz);
   p->lut.borrow(src.lut);
   p->deap.borrow(src.deap);
+  p->deapf.borrow(src.deapf);
   if (src.plain) p->plain = binning_share(*src.plain);
   *out = std::move(p);
   return PG_OK;
@@ -1133,26 +1145,32 @@ static pg_status launch_spread(NufftPlan* p, const Binning* bin, const SpreadArg
   return spread_launch_t<2, 16>(p, bin, a, s);
 }
 
-// Post-kernel launch: CP coil lanes per pixel (a power of two, at most 8).
-static pg_status launch_post(NufftPlan* p, int nb, int L, const NufftBatch& b, int c0, float scale, int acc,
-                             float2* x, cudaStream_t s) {
-  const NufftGeom& g = p->g;
-  const uint64_t N = g.nimg();
-  const float2* grids = p->work->grids.p;
-  if (nb >= 8) {
-    PG_LAUNCH(k_post<8>, ceil_div(N * 8, 256), 256, 0, s, g, nb, L, grids, b.S, c0, b.E, b.WoH, p->deap.p, scale,
-              acc, x);
-  } else if (nb >= 4) {
-    PG_LAUNCH(k_post<4>, ceil_div(N * 4, 256), 256, 0, s, g, nb, L, grids, b.S, c0, b.E, b.WoH, p->deap.p, scale,
-              acc, x);
-  } else if (nb >= 2) {
-    PG_LAUNCH(k_post<2>, ceil_div(N * 2, 256), 256, 0, s, g, nb, L, grids, b.S, c0, b.E, b.WoH, p->deap.p, scale,
-              acc, x);
-  } else {
-    PG_LAUNCH(k_post<1>, ceil_div(N, 256), 256, 0, s, g, nb, L, grids, b.S, c0, b.E, b.WoH, p->deap.p, scale, acc,
-              x);
-  }
+// Post-kernel launch: CP coil lanes x LP segment lanes per pixel (powers of
+// two, at most 8 lanes).
+template <int CP, int LP>
+static pg_status post_launch(NufftPlan* p, int nb, int L, const NufftBatch& b, int c0, int acc, float2* x,
+                             cudaStream_t s) {
+  const uint64_t N = p->g.nimg();
+  PG_LAUNCH((k_post<CP, LP>), ceil_div(N * CP * LP, 256), 256, 0, s, p->g, nb, L, p->work->grids.p, b.S, c0, b.E,
+            b.WoH, p->deapf.p, acc, x);
   return PG_OK;
+}
+
+static pg_status launch_post(NufftPlan* p, int nb, int L, const NufftBatch& b, int c0, int acc, float2* x,
+                             cudaStream_t s) {
+  const int cp = nb >= 8 ? 8 : nb >= 4 ? 4 : nb >= 2 ? 2 : 1;
+  const int lp = std::min(8 / cp, L >= 4 ? 4 : L >= 2 ? 2 : 1);
+  switch (cp * 10 + lp) {
+    case 81: return post_launch<8, 1>(p, nb, L, b, c0, acc, x, s);
+    case 42: return post_launch<4, 2>(p, nb, L, b, c0, acc, x, s);
+    case 41: return post_launch<4, 1>(p, nb, L, b, c0, acc, x, s);
+    case 24: return post_launch<2, 4>(p, nb, L, b, c0, acc, x, s);
+    case 22: return post_launch<2, 2>(p, nb, L, b, c0, acc, x, s);
+    case 21: return post_launch<2, 1>(p, nb, L, b, c0, acc, x, s);
+    case 14: return post_launch<1, 4>(p, nb, L, b, c0, acc, x, s);
+    case 12: return post_launch<1, 2>(p, nb, L, b, c0, acc, x, s);
+    default: return post_launch<1, 1>(p, nb, L, b, c0, acc, x, s);
+  }
 }
 
 pg_status nufft_forward(NufftPlan* p, const NufftBatch& b, const float2* x, float2* y, cudaStream_t s) {
@@ -1161,7 +1179,6 @@ pg_status nufft_forward(NufftPlan* p, const NufftBatch& b, const float2* x, floa
   const Binning* bin = b.bin ? b.bin : p->plain.get();
   const int L = bin->L;
   const int Cb = batch_coils(p, b.C, L);
-  const float scale = (g.dim == 2) ? (1.0f / (g.os * g.os)) : (float)(1.0 / (double)(g.os * g.os * g.os));
   const uint64_t G = g.ngrid();
   for (int c0 = 0; c0 < b.C; c0 += Cb) {
     const int nb = std::min(Cb, b.C - c0);
@@ -1171,7 +1188,7 @@ pg_status nufft_forward(NufftPlan* p, const NufftBatch& b, const float2* x, floa
     PG_TRY(ensure_forward_input(p, B, s));
     {
       ProfScope ps("pre", s);
-      PG_LAUNCH(k_pre, dim3(ceil_div(g.nimg(), 256), B), 256, 0, s, g, L, x, b.S, c0, b.E, b.Wo, p->deap.p, scale,
+      PG_LAUNCH(k_pre, dim3(ceil_div(g.nimg(), 256), B), 256, 0, s, g, L, x, b.S, c0, b.E, b.Wo, p->deapf.p,
                 p->work->fin.p);
     }
     {
@@ -1193,7 +1210,6 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
   const Binning* bin = b.bin ? b.bin : p->plain.get();
   const int L = bin->L, K = bin->K;
   const int Cb = batch_coils(p, b.C, L);
-  const float scale = (g.dim == 2) ? (1.0f / (g.os * g.os)) : (float)(1.0 / (double)(g.os * g.os * g.os));
   const uint64_t G = g.ngrid();
   const TileShape& t = bin->tile;
   const size_t plane_bytes = (size_t)t.PX * t.PY * t.PZ * 2 * sizeof(float);
@@ -1245,7 +1261,7 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
     }
     const int acc = (b.accumulate || c0 > 0) ? 1 : 0;
     ProfScope ps("post", s);
-    PG_TRY(launch_post(p, nb, L, b, c0, scale, acc, x, s));
+    PG_TRY(launch_post(p, nb, L, b, c0, acc, x, s));
   }
   return PG_OK;
 }

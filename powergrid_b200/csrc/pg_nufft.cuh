@@ -81,6 +81,7 @@ struct NufftPlan {
   DevBuf<float> lut;
   float lut_max = 0.f;           // largest per-axis tap weight
   DevBuf<float> deap;            // Nx + Ny + Nz reciprocal-transform factors
+  DevBuf<float> deapf;           // per voxel 1/(OS^d k), 0 where k is NaN
   std::unique_ptr<Binning> plain;  // binning without segmentation (L = 1)
   // grid workspace (possibly shared) and cuFFT plans, keyed by batch size
   std::shared_ptr<NufftWork> work = std::make_shared<NufftWork>();
