@@ -29,6 +29,7 @@
 #include <tuple>
 
 #include "pg_binsort.cuh"
+#include "pg_fft2d.cuh"
 #include "pg_nufft.cuh"
 #include "pg_profile.cuh"
 
@@ -817,6 +818,12 @@ pg_status nufft_plan_create(std::unique_ptr<NufftPlan>* out, uint64_t M, float g
   PG_TRY(p->lut.upload(lut.data(), lut.size(), s));
   p->lut_max = *std::max_element(lut.begin(), lut.end());
   PG_TRY(p->deap.upload(deap.data(), deap.size(), s));
+  // power-of-two 2-D grids run the pruned, fused FFT passes; PG_CUFFT=1 keeps cuFFT
+  {
+    const char* e = getenv("PG_CUFFT");
+    p->own_fft = fft2d_supported(g) && !(e && e[0] == '1');
+    if (p->own_fft) PG_TRY(fft2d_twiddles(g, &p->tw2d, s));
+  }
   // Per-voxel deapodization factor 1/(OS^d k), k the product of the axis
   // factors in float as the reference forms it; 0 where k is NaN (the
   // reference zeroes those voxels, griddingSupport.cpp:265-278).
@@ -852,6 +859,8 @@ pg_status nufft_plan_share(const NufftPlan& src, std::unique_ptr<NufftPlan>* out
   p->lut.borrow(src.lut);
   p->deap.borrow(src.deap);
   p->deapf.borrow(src.deapf);
+  p->own_fft = src.own_fft;
+  p->tw2d.borrow(src.tw2d);
   if (src.plain) p->plain = binning_share(*src.plain);
   *out = std::move(p);
   return PG_OK;
@@ -1006,12 +1015,15 @@ static void fft_release_plan(const NufftGeom& g, int B, cufftHandle h, size_t wo
   fft_release(fft_key(g, B), h, work);
 }
 
+// Grid workspace for B grids and, unless the plan runs its own FFT passes
+// (h == nullptr), the pooled cuFFT plan for a batch of B.
 static pg_status ensure_workspace(NufftPlan* p, int B, cufftHandle* h, cudaStream_t s) {
   const uint64_t G = p->g.ngrid();
   if (p->work->grids.n < (uint64_t)B * G) {
     PG_CUDA(cudaStreamSynchronize(s));  // queued work may still use the old workspace
     PG_TRY(p->work->grids.alloc((uint64_t)B * G));
   }
+  if (!h) return PG_OK;
   auto it = p->ffts.find(B);
   if (it == p->ffts.end()) {
     cufftHandle hh;
@@ -1183,6 +1195,13 @@ pg_status nufft_forward(NufftPlan* p, const NufftBatch& b, const float2* x, floa
   for (int c0 = 0; c0 < b.C; c0 += Cb) {
     const int nb = std::min(Cb, b.C - c0);
     const int B = nb * L;
+    if (p->own_fft) {
+      PG_TRY(ensure_workspace(p, B, nullptr, s));
+      PG_TRY(grow(p->work->fin, (uint64_t)B * G / 2, s));
+      ProfScope ps("fft_fwd", s);
+      PG_TRY(fft2d_forward(g, B, L, x, b.S, c0, b.E, b.Wo, p->deapf.p, p->tw2d.p, p->work->fin.p,
+                           p->work->grids.p, s));
+    } else {
     cufftHandle h;
     PG_TRY(ensure_workspace(p, B, &h, s));
     PG_TRY(ensure_forward_input(p, B, s));
@@ -1195,6 +1214,7 @@ pg_status nufft_forward(NufftPlan* p, const NufftBatch& b, const float2* x, floa
       ProfScope ps("fft_fwd", s);
       PG_CUFFT(cufftExecC2C(h, reinterpret_cast<cufftComplex*>(p->work->fin.p),
                             reinterpret_cast<cufftComplex*>(p->work->grids.p), CUFFT_FORWARD));
+    }
     }
     float2* yc = y + (uint64_t)c0 * b.data_stride;
     const float2* aa = (L > 1 || bin->aa.p) ? bin->aa.p : nullptr;
@@ -1229,8 +1249,8 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
   for (int c0 = 0; c0 < b.C; c0 += Cb) {
     const int nb = std::min(Cb, b.C - c0);
     const int B = nb * L;
-    cufftHandle h;
-    PG_TRY(ensure_workspace(p, B, &h, s));
+    cufftHandle h = 0;
+    PG_TRY(ensure_workspace(p, B, p->own_fft ? nullptr : &h, s));
     const float2* yc = y + (uint64_t)c0 * b.data_stride;
     const float2* aa = (L > 1 || bin->aa.p) ? bin->aa.p : nullptr;
     PG_TRY(grow(p->work->vs, (uint64_t)nb * bin->M * K, s));
@@ -1254,12 +1274,20 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
         PG_TRY(launch_spread(p, bin, r, s));
       }
     }
+    const int acc = (b.accumulate || c0 > 0) ? 1 : 0;
+    if (p->own_fft) {
+      PG_TRY(grow(p->work->fin, (uint64_t)B * G / 2, s));
+      PG_TRY(grow(p->work->rimg, (uint64_t)B * g.nimg(), s));
+      ProfScope ps("fft_adj", s);
+      PG_TRY(fft2d_adjoint(g, B, L, p->work->grids.p, b.S, c0, b.E, b.WoH, p->deapf.p, p->tw2d.p, p->work->fin.p,
+                           p->work->rimg.p, acc, x, s));
+      continue;
+    }
     {
       ProfScope ps("fft_adj", s);
       PG_CUFFT(cufftExecC2C(h, reinterpret_cast<cufftComplex*>(p->work->grids.p),
                             reinterpret_cast<cufftComplex*>(p->work->grids.p), CUFFT_INVERSE));
     }
-    const int acc = (b.accumulate || c0 > 0) ? 1 : 0;
     ProfScope ps("post", s);
     PG_TRY(launch_post(p, nb, L, b, c0, acc, x, s));
   }

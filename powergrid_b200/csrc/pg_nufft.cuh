@@ -70,6 +70,7 @@ struct NufftWork {
   DevBuf<float2> grids;     // FFT output (forward) / spread target (adjoint)
   DevBuf<float2> fin;       // forward FFT input; its zero-pad border stays zero
   DevBuf<float2> vs;        // adjoint: per-sample segment values in binned order
+  DevBuf<float2> rimg;      // adjoint with the plan's own FFT passes: one image per grid
   DevBuf<char> fft_work;
 };
 
@@ -82,6 +83,8 @@ struct NufftPlan {
   float lut_max = 0.f;           // largest per-axis tap weight
   DevBuf<float> deap;            // Nx + Ny + Nz reciprocal-transform factors
   DevBuf<float> deapf;           // per voxel 1/(OS^d k), 0 where k is NaN
+  bool own_fft = false;          // pruned fused 2-D FFT passes instead of cuFFT
+  DevBuf<float2> tw2d;           // their twiddle table
   std::unique_ptr<Binning> plain;  // binning without segmentation (L = 1)
   // grid workspace (possibly shared) and cuFFT plans, keyed by batch size
   std::shared_ptr<NufftWork> work = std::make_shared<NufftWork>();
