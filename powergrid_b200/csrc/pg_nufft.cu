@@ -319,6 +319,25 @@ struct TileGeo {
   static constexpr int CELLS = PLANE * PZ;
 };
 
+// Device work queue of the persistent spread launch: items are (subproblem,
+// coil chunk) pairs, subproblems largest first.  Each block takes the next
+// item until none is left; the block that finds the queue empty last resets
+// it for the next launch.  Returns the item, or -1.
+__device__ __forceinline__ int next_item(unsigned* q, int nitems) {
+  __shared__ int item;
+  __syncthreads();   // the previous item's shared memory is no longer in use
+  if (threadIdx.x == 0) {
+    int it = (int)atomicAdd(&q[0], 1u);
+    if (it >= nitems) {
+      it = -1;
+      if (atomicAdd(&q[1], 1u) == gridDim.x - 1) { q[0] = 0u; q[1] = 0u; }
+    }
+    item = it;
+  }
+  __syncthreads();
+  return item;
+}
+
 template <int DIM, int T, int CC, int KP>
 __global__ void __launch_bounds__(256) k_gather(NufftGeom g, TileShape t, const int4* __restrict__ sub,
                                                 const uint2* __restrict__ start, const float* __restrict__ wxy,
@@ -431,7 +450,8 @@ __global__ void __launch_bounds__(256) k_gather(NufftGeom g, TileShape t, const 
 }
 
 // ---------------------------------------------------------------------------
-// Adjoint spread: one block per (subproblem, coil chunk).
+// Adjoint spread, persistent: as many blocks as fit on the device take
+// (subproblem, coil chunk) items from a device work queue, largest first.
 //  1. The subproblem's samples are staged in shared memory with coalesced
 //     loads: tap starts, tap weights and, per (coil, segment) plane, the value
 //     v = conj(AA) * y the sample spreads.
@@ -464,7 +484,8 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
                                                 const uint2* __restrict__ start, const float* __restrict__ wxy,
                                                 const float* __restrict__ wz, const float2* __restrict__ vs,
                                                 uint64_t M, int K, int L, int c0, int cc, int smax, float wmax,
-                                                float2* __restrict__ grids) {
+                                                float2* __restrict__ grids, unsigned* __restrict__ queue,
+                                                int nchunks, int nitems) {
   using TG = TileGeo<DIM, T>;
   constexpr int CELLS = TG::CELLS, PY = TG::PY, PX = TG::PX, PLANE = TG::PLANE;
   constexpr int WROW = spread_wrow(DIM);   // staged weights per sample: wx[8] wy[8] (wz[8])
@@ -473,8 +494,9 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
   __shared__ float scale[16], inv_scale[16];
   // planes per block: NP when fixed at compile time, else cc x K
   const int np = (NP > 0) ? NP : cc * K;
-  const int4 sp = sub[blockIdx.x];
-  const int cfirst = c0 + blockIdx.y * cc;
+  for (int item; (item = next_item(queue, nitems)) >= 0;) {
+  const int4 sp = sub[item / nchunks];
+  const int cfirst = c0 + (item % nchunks) * cc;
   const int tile = sp.x, first = sp.z, count = sp.w;
   const int lseg = sp.y;
   const int ty = tile % t.nty;
@@ -652,6 +674,7 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
           atomicAdd(grids + ((uint64_t)(cfirst + c) * L + lseg + j) * G + idx,
                     make_float2((float)re * inv_scale[pl], (float)im * inv_scale[pl]));
       }
+  }
   }
 }
 
@@ -1072,6 +1095,36 @@ static int smem_optin_bytes() {
   return v;
 }
 
+// Blocks of a persistent launch: as many as fit on the device at
+// once (cached per kernel and shared-memory size), at most one per item.
+static int persistent_blocks(const void* kernel, size_t smem, int nitems) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, size_t>, int> cache;
+  int per_sm = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find({kernel, smem});
+    if (it != cache.end()) {
+      per_sm = it->second;
+    } else {
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, smem) != cudaSuccess) {
+        cudaGetLastError();
+        per_sm = 1;
+      }
+      cache[{kernel, smem}] = per_sm = std::max(1, per_sm);
+    }
+  }
+  return std::max(1, std::min(nitems, per_sm * sm_count()));
+}
+
+// The work-queue words of the plan's persistent spread launches (zero between launches).
+static pg_status ensure_queue(NufftPlan* p, cudaStream_t s) {
+  if (p->work->queue.p) return PG_OK;
+  PG_TRY(p->work->queue.alloc(2));
+  PG_CUDA(cudaMemsetAsync(p->work->queue.p, 0, 2 * sizeof(unsigned), s));
+  return PG_OK;
+}
+
 // Tiled gather launch: choose the padded segment count KP and the coils per
 // block CC so that the staged tiles fit in shared memory and 2*CC*KP <= 32.
 template <int DIM, int T, int CC, int KP>
@@ -1079,6 +1132,7 @@ static pg_status gather_launch_one(NufftPlan* p, const Binning* bin, const float
                                    uint64_t dstride, cudaStream_t s) {
   const size_t smem = (size_t)CC * KP * 2 * TileGeo<DIM, T>::CELLS * sizeof(float);
   PG_CUDA(cudaFuncSetAttribute(k_gather<DIM, T, CC, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // a static grid: the persistent work-queue form measured ~4 % slower here
   dim3 grid(bin->nsub, ceil_div(nb, CC));
   PG_LAUNCH((k_gather<DIM, T, CC, KP>), grid, 256, smem, s, p->g, bin->tile, bin->subprob.p, bin->start.p,
             bin->wxy.p, bin->wz.p, bin->perm.p, aa, bin->K, bin->L, p->work->grids.p, nb, y, dstride);
@@ -1130,9 +1184,12 @@ struct SpreadArgs {
 template <int DIM, int T, int NP>
 static pg_status spread_launch_np(NufftPlan* p, const Binning* bin, const SpreadArgs& a, cudaStream_t s) {
   PG_CUDA(cudaFuncSetAttribute(k_spread<DIM, T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.smem));
-  dim3 grid(bin->nsub, a.nchunks);
-  PG_LAUNCH((k_spread<DIM, T, NP>), grid, 256, a.smem, s, p->g, bin->tile, bin->subprob.p, bin->start.p,
-            bin->wxy.p, bin->wz.p, a.vs, bin->M, bin->K, bin->L, a.c0, a.cc, bin->submax, a.wmax, p->work->grids.p);
+  const int nitems = bin->nsub * a.nchunks;
+  PG_TRY(ensure_queue(p, s));
+  const int blocks = persistent_blocks((const void*)k_spread<DIM, T, NP>, a.smem, nitems);
+  PG_LAUNCH((k_spread<DIM, T, NP>), blocks, 256, a.smem, s, p->g, bin->tile, bin->subprob.p, bin->start.p,
+            bin->wxy.p, bin->wz.p, a.vs, bin->M, bin->K, bin->L, a.c0, a.cc, bin->submax, a.wmax, p->work->grids.p,
+            p->work->queue.p, a.nchunks, nitems);
   return PG_OK;
 }
 

@@ -71,6 +71,7 @@ struct NufftWork {
   DevBuf<float2> fin;       // forward FFT input; its zero-pad border stays zero
   DevBuf<float2> vs;        // adjoint: per-sample segment values in binned order
   DevBuf<float2> rimg;      // adjoint with the plan's own FFT passes: one image per grid
+  DevBuf<unsigned> queue;   // work-queue words of the persistent spread launches
   DevBuf<char> fft_work;
 };
 
