@@ -40,7 +40,7 @@ struct TileShape {
 struct NufftTune {
   int tile2d = 16, tile3d = 8;        // measured best on cfg2 (B200): 16 > 32 > 64
   int submax2d = 256, submax3d = 256;
-  int spread_cc = 4, gather_cc = 2;
+  int spread_cc = 2, gather_cc = 2;
   static NufftTune defaults();
 };
 
