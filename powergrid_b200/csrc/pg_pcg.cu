@@ -323,7 +323,21 @@ __global__ void k_daw(uint64_t n, const float2* __restrict__ Adir, const float* 
                       uint32_t* fl, int quad, double beta) {
   if (fl[F_DONE]) return;
   double a = 0.0, b = 0.0;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  // four elements per round with every load issued first (latency-bound at these sizes)
+  for (; i + 3 * stride < n; i += 4 * stride) {
+    float2 v[4], q[4];
+    float w[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) { v[u] = Adir[i + u * stride]; q[u] = r[i + u * stride]; w[u] = W[i + u * stride]; }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      a += (double)w[u] * ((double)v[u].x * v[u].x + (double)v[u].y * v[u].y);
+      b += (double)v[u].x * q[u].x + (double)v[u].y * q[u].y;
+    }
+  }
+  for (; i < n; i += stride) {
     const float2 v = Adir[i];
     const float2 q = r[i];
     a += (double)W[i] * ((double)v.x * v.x + (double)v.y * v.y);
@@ -377,8 +391,7 @@ __global__ void k_newton(PenDev R, const float2* __restrict__ x, const float2* _
 // r = W (.) (y - Ax) in the same pass; then the iteration count.
 __global__ void k_update(uint64_t ni, uint64_t nd, float2* __restrict__ x, const float2* __restrict__ ddir,
                          float2* __restrict__ Ax, const float2* __restrict__ Adir, const float2* __restrict__ y,
-                         const float* __restrict__ W, float2* __restrict__ r, unsigned* counter, const double* sc,
-                         uint32_t* fl) {
+                         const float* __restrict__ W, float2* __restrict__ r, const double* sc, uint32_t* fl) {
   if (fl[F_DONE]) return;
   const float st = (float)sc[S_STEP];
   const uint64_t n = ni > nd ? ni : nd;
@@ -394,8 +407,8 @@ __global__ void k_update(uint64_t ni, uint64_t nd, float2* __restrict__ x, const
       r[i] = make_float2(w * e.x, w * e.y);
     }
   }
-  if (!last_block(counter)) return;
-  if (threadIdx.x == 0) {
+  // the count needs no other block's data: block 0 takes it
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
     fl[F_IT] += 1;
     fl[F_COMPLETED] = fl[F_IT];
   }
@@ -457,7 +470,7 @@ struct Solver {
       for (int k = 0; k < 3; ++k)
         PG_LAUNCH(k_newton, gi, kRed, 0, s, R, x.p, ddir.p, beta, part.p, nbi, counter.p, sc.p, fl.p);
     PG_LAUNCH(k_update, (unsigned)red_blocks(std::max(nd, ni)), kRed, 0, s, ni, nd, x.p, ddir.p, Ax.p, Adir.p, y, W,
-              r.p, counter.p, sc.p, fl.p);
+              r.p, sc.p, fl.p);
     return PG_OK;
   }
 };
