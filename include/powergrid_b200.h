@@ -90,6 +90,16 @@ pg_status pg_pcsense_timeseg_create(pg_op* out, const float* kx, const float* ky
                                     uint64_t L, uint64_t interptype, const float* sense_map,
                                     const float* field_map, const float* shot_phase_map, uint64_t n_shot_phase);
 
+/* pcSENSE(kx, ky, kz, nx, ny, nz, nc, t, SENSEmap, FieldMap, ShotPhaseMap)
+ * replaces pcSENSE<float>::pcSENSE (pcSENSE.h:76-78, pcSENSE.cpp:40-104):
+ * multishot phase-corrected SENSE over one Gdft per shot.  nk = total samples
+ * (all shots); shots = n_shot_phase / (nx*ny*nz) (pcSENSE.cpp:44).  Like the
+ * reference, both directions weight by exp(+i*ShotPhaseMap) (pcSENSE.cpp:103,
+ * 123, 146), so the adjoint is not the exact adjoint of the forward. */
+pg_status pg_pcsense_create(pg_op* out, const float* kx, const float* ky, const float* kz, uint64_t nk, uint64_t nx,
+                            uint64_t ny, uint64_t nz, uint64_t nc, const float* t, const float* sense_map,
+                            const float* field_map, const float* shot_phase_map, uint64_t n_shot_phase);
+
 pg_status pg_op_destroy(pg_op op);
 /* Lengths of the data vector (operator* output) and image vector. */
 pg_status pg_op_shape(pg_op op, uint64_t* n_data, uint64_t* n_image);

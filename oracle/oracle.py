@@ -50,6 +50,8 @@ def lib() -> C.CDLL:
         L.orc_sense_new.argtypes = [P, P, U64, U64, U64]
         L.orc_pcsense_ts_new.restype = P
         L.orc_pcsense_ts_new.argtypes = [C.c_int, P, P, P, U64, U64, U64, U64, U64, P, U64, U64, P, P, P, U64]
+        L.orc_pcsense_new.restype = P
+        L.orc_pcsense_new.argtypes = [C.c_int, P, P, P, U64, U64, U64, U64, U64, P, P, P, P, U64]
         L.orc_free.argtypes = [P]
         L.orc_data_len.restype = U64
         L.orc_data_len.argtypes = [P]
@@ -186,6 +188,14 @@ def pcsense_timeseg(prec, kx, ky, kz, nx, ny, nz, nc, t, L, smap, fm, pmap, inte
     s = np.ascontiguousarray(smap, dtype=C64)
     return Op(lib().orc_pcsense_ts_new(prec, _p(kx), _p(ky), _p(kz), kx.size, nx, ny, nz, nc, _p(t), L, interptype,
                                        _p(s), _p(fm), _p(pm), pm.size), prec)
+
+
+def pcsense(prec, kx, ky, kz, nx, ny, nz, nc, t, smap, fm, pmap) -> Op:
+    """pcSENSE over per-shot Gdft (pcSENSE.cpp:40-153); prec 2 = FP64 DFT."""
+    kx, ky, kz, t, fm, pm = (_f32(v) for v in (kx, ky, kz, t, fm, pmap))
+    s = np.ascontiguousarray(smap, dtype=C64)
+    return Op(lib().orc_pcsense_new(prec, _p(kx), _p(ky), _p(kz), kx.size, nx, ny, nz, nc, _p(t), _p(s), _p(fm),
+                                    _p(pm), pm.size), prec)
 
 
 def kb_lut(prec: int, gridos: float = 2.0):

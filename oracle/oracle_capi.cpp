@@ -287,6 +287,29 @@ void* orc_pcsense_ts_new(int prec, const float* kx, const float* ky, const float
   });
 }
 
+// prec: 0 float, 1 double (reference DFT formula), 2 double with the FP64 DFT
+void* orc_pcsense_new(int prec, const float* kx, const float* ky, const float* kz, u64 nk, u64 nx, u64 ny, u64 nz,
+                      u64 nc, const float* t, const float* smap, const float* fmap, const float* pmap, u64 npmap) {
+  return guard([&]() -> void* {
+    auto* h = new Handle;
+    h->prec = prec;
+    const u64 ni = nx * ny * nz;
+    const std::complex<float>* s = reinterpret_cast<const std::complex<float>*>(smap);
+    if (prec == 0) {
+      h->f.reset(new pgo::PcSenseOp<float>(kx, ky, kz, nk, (int)nx, (int)ny, (int)nz, nc, t, s, fmap, pmap, npmap,
+                                           g_use_ref, false));
+    } else {
+      auto a = widen<double>(kx, nk), b = widen<double>(ky, nk), c = widen<double>(kz, nk);
+      auto tt = widen<double>(t, nk), fm = widen<double>(fmap, ni), pm = widen<double>(pmap, npmap);
+      std::vector<std::complex<double>> sd(ni * nc);
+      for (u64 i = 0; i < ni * nc; ++i) sd[i] = std::complex<double>(s[i].real(), s[i].imag());
+      h->d.reset(new pgo::PcSenseOp<double>(a.data(), b.data(), c.data(), nk, (int)nx, (int)ny, (int)nz, nc,
+                                            tt.data(), sd.data(), fm.data(), pm.data(), npmap, g_use_ref, prec == 2));
+    }
+    return h;
+  });
+}
+
 void orc_free(void* h) { delete (Handle*)h; }
 
 u64 orc_data_len(void* h) {

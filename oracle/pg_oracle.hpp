@@ -10,6 +10,7 @@
 //   TimeSegmentation    Hanning interpolator (TimeSegmentation.cpp:37-93, 213-218, 252-324)
 //   SENSE               SENSE.cpp:33-97
 //   pcSenseTimeSeg      pcSenseTimeSeg.cpp:41-171
+//   pcSENSE             pcSENSE.cpp:40-153
 //   Robject/Quad/TV     Robject.cpp:49-193, QuadPenalty.cpp:45-64, TVPenalty.cpp:43-68
 //   solve_pwls_pcg      solve_pwls_pcg.hpp:34-167
 //
@@ -715,6 +716,59 @@ struct PcSenseTimeSegOp : Op<T> {
         A[s]->adjoint(d + Nd * (s + c * Ns), img.data());
         const C* m = Mc.data() + Ni * (s + c * Ns);
         for (u64 p = 0; p < Ni; ++p) x[p] += m[p] * img[p];
+      }
+  }
+};
+
+// pcSENSE (pcSENSE.cpp:40-153): per-shot Gdft over one voxel table.  The
+// phase factor expiPMap = conj(exp(-i P)) = exp(+i P) (:103) weights both
+// directions; the adjoint multiplies by conj(S) (.) expiPMap (:146).
+template <typename T>
+struct PcSenseOp : Op<T> {
+  using C = std::complex<T>;
+  u64 Ni, Nc, Ns, Nd;
+  std::vector<T> ix, iy, iz;
+  std::vector<std::unique_ptr<GdftOp<T>>> A;
+  std::vector<C> S, E;  // Ni x Nc, Ni x Ns
+  PcSenseOp(const T* kx, const T* ky, const T* kz, u64 nk, int nx, int ny, int nz, u64 nc, const T* t,
+            const C* smap, const T* fmap, const T* pmap, u64 npmap, bool use_ref, bool exact64) {
+    Ni = (u64)nx * ny * nz; Nc = nc; Ns = npmap / Ni; Nd = nk / Ns;
+    this->n1 = Nd * Ns * Nc; this->n2 = Ni;
+    // :65-82, cube (Nx, Ny, Nz) with y as its first index
+    ix.resize(Ni); iy.resize(Ni); iz.resize(Ni);
+    for (int ii = 0; ii < ny; ++ii)
+      for (int jj = 0; jj < nx; ++jj)
+        for (int kk = 0; kk < nz; ++kk) {
+          const u64 j = (u64)ii + (u64)nx * jj + (u64)nx * ny * kk;
+          ix[j] = (T)(((T)jj - (T)nx / 2.0) / ((T)nx));
+          iy[j] = (T)(((T)ii - (T)ny / 2.0) / ((T)ny));
+          iz[j] = (T)(((T)kk - (T)nz / 2.0) / ((T)nz));
+        }
+    for (u64 s = 0; s < Ns; ++s) {
+      A.emplace_back(new GdftOp<T>(Nd, Ni, kx + s * Nd, ky + s * Nd, kz + s * Nd, ix.data(), iy.data(), iz.data(),
+                                   fmap, t + s * Nd));
+      A.back()->use_ref = use_ref;
+      A.back()->exact64 = exact64;
+    }
+    S.assign(smap, smap + Ni * Nc);
+    E.resize(Ni * Ns);
+    for (u64 i = 0; i < Ni * Ns; ++i) E[i] = std::conj(std::exp(C(0, -1) * pmap[i]));
+  }
+  void forward(const C* x, C* y) const override {
+    std::vector<C> tmp(Ni);
+    for (u64 c = 0; c < Nc; ++c)
+      for (u64 s = 0; s < Ns; ++s) {
+        for (u64 p = 0; p < Ni; ++p) tmp[p] = x[p] * (S[p + Ni * c] * E[p + Ni * s]);
+        A[s]->forward(tmp.data(), y + Nd * (s + c * Ns));
+      }
+  }
+  void adjoint(const C* d, C* x) const override {
+    std::vector<C> img(Ni);
+    std::fill(x, x + Ni, C(0, 0));
+    for (u64 c = 0; c < Nc; ++c)
+      for (u64 s = 0; s < Ns; ++s) {
+        A[s]->adjoint(d + Nd * (s + c * Ns), img.data());
+        for (u64 p = 0; p < Ni; ++p) x[p] += (std::conj(S[p + Ni * c]) * E[p + Ni * s]) * img[p];
       }
   }
 };

@@ -62,6 +62,7 @@ SIGNATURES = {
     "pg_sense_create": (C.c_int, [C.POINTER(P), P, P, U64, U64, U64]),
     "pg_pcsense_timeseg_create": (C.c_int, [C.POINTER(P), P, P, P, U64, U64, U64, U64, U64, P, U64, U64, P, P, P,
                                             U64]),
+    "pg_pcsense_create": (C.c_int, [C.POINTER(P), P, P, P, U64, U64, U64, U64, U64, P, P, P, P, U64]),
     "pg_op_destroy": (C.c_int, [P]),
     "pg_op_shape": (C.c_int, [P, C.POINTER(U64), C.POINTER(U64)]),
     "pg_op_forward": (C.c_int, [P, P, P]),

@@ -165,6 +165,9 @@ __global__ void k_adjoint_finish(uint64_t ni, int nc, int c0, int nsplit, int nc
   x[j] = acc;
 }
 
+static pg_status upload_samples(GdftPlan* p, uint64_t nk, const float* kx, const float* ky, const float* kz,
+                                const float* t, cudaStream_t s);
+
 pg_status gdft_plan_create(std::unique_ptr<GdftPlan>* out, uint64_t nk, uint64_t ni, const float* kx, const float* ky,
                            const float* kz, const float* ix, const float* iy, const float* iz, const float* fm,
                            const float* t, cudaStream_t s) {
@@ -172,21 +175,41 @@ pg_status gdft_plan_create(std::unique_ptr<GdftPlan>* out, uint64_t nk, uint64_t
   auto p = std::make_unique<GdftPlan>();
   p->nk = nk;
   p->ni = ni;
-  const double tpi = 6.283185307179586476925;
-  std::vector<double4> ks(nk), vs(ni);
-  for (uint64_t i = 0; i < nk; ++i) {
-    if (!(std::isfinite(kx[i]) && std::isfinite(ky[i]) && std::isfinite(kz[i]) && std::isfinite(t[i])))
-      return set_error(PG_INVALID_ARG, "Gdft: non-finite sample input at %llu", (unsigned long long)i);
-    ks[i] = make_double4(tpi * kx[i], tpi * ky[i], tpi * kz[i], (double)t[i]);
-  }
+  std::vector<double4> vs(ni);
   for (uint64_t j = 0; j < ni; ++j) {
     if (!(std::isfinite(ix[j]) && std::isfinite(iy[j]) && std::isfinite(iz[j]) && std::isfinite(fm[j])))
       return set_error(PG_INVALID_ARG, "Gdft: non-finite voxel input at %llu", (unsigned long long)j);
     vs[j] = make_double4(ix[j], iy[j], iz[j], fm[j]);
   }
-  PG_TRY(p->ks.upload(ks.data(), nk, s));
   PG_TRY(p->vs.upload(vs.data(), ni, s));
+  PG_TRY(upload_samples(p.get(), nk, kx, ky, kz, t, s));
+  *out = std::move(p);
+  return PG_OK;
+}
+
+static pg_status upload_samples(GdftPlan* p, uint64_t nk, const float* kx, const float* ky, const float* kz,
+                                const float* t, cudaStream_t s) {
+  const double tpi = 6.283185307179586476925;
+  std::vector<double4> ks(nk);
+  for (uint64_t i = 0; i < nk; ++i) {
+    if (!(std::isfinite(kx[i]) && std::isfinite(ky[i]) && std::isfinite(kz[i]) && std::isfinite(t[i])))
+      return set_error(PG_INVALID_ARG, "Gdft: non-finite sample input at %llu", (unsigned long long)i);
+    ks[i] = make_double4(tpi * kx[i], tpi * ky[i], tpi * kz[i], (double)t[i]);
+  }
+  PG_TRY(p->ks.upload(ks.data(), nk, s));
   PG_CUDA(cudaStreamSynchronize(s));
+  return PG_OK;
+}
+
+pg_status gdft_plan_same_voxels(std::unique_ptr<GdftPlan>* out, const GdftPlan& src, uint64_t nk, const float* kx,
+                                const float* ky, const float* kz, const float* t, cudaStream_t s) {
+  if (nk == 0) return set_error(PG_INVALID_ARG, "Gdft: empty operator");
+  auto p = std::make_unique<GdftPlan>();
+  p->nk = nk;
+  p->ni = src.ni;
+  p->vs.borrow(src.vs);
+  p->work = src.work;
+  PG_TRY(upload_samples(p.get(), nk, kx, ky, kz, t, s));
   *out = std::move(p);
   return PG_OK;
 }
@@ -226,18 +249,18 @@ pg_status gdft_forward(GdftPlan* p, int C, const float2* S, const float2* x, flo
   for (int c0 = 0; c0 < C; c0 += kCoilChunk) {
     const int nc = std::min(kCoilChunk, C - c0);
     const int ncp = pad_coils(nc);
-    PG_TRY(grow(p->xin, (uint64_t)ncp * p->ni, s));
-    PG_TRY(grow(p->part, (uint64_t)nsplit * ncp * p->nk, s));
-    PG_LAUNCH(k_apply_maps, ceil_div(p->ni, 256), 256, 0, s, p->ni, nc, c0, S, x, p->xin.p);
-    if (ncp > nc) PG_CUDA(cudaMemsetAsync(p->xin.p + (uint64_t)nc * p->ni, 0, (ncp - nc) * p->ni * sizeof(float2), s));
+    PG_TRY(grow(p->work->xin, (uint64_t)ncp * p->ni, s));
+    PG_TRY(grow(p->work->part, (uint64_t)nsplit * ncp * p->nk, s));
+    PG_LAUNCH(k_apply_maps, ceil_div(p->ni, 256), 256, 0, s, p->ni, nc, c0, S, x, p->work->xin.p);
+    if (ncp > nc) PG_CUDA(cudaMemsetAsync(p->work->xin.p + (uint64_t)nc * p->ni, 0, (ncp - nc) * p->ni * sizeof(float2), s));
     ProfScope ps("dft_fwd", s);
     switch (ncp) {
-      case 1: PG_TRY(launch_fwd<1>(p, nsplit, jchunk, p->xin.p, p->part.p, s)); break;
-      case 2: PG_TRY(launch_fwd<2>(p, nsplit, jchunk, p->xin.p, p->part.p, s)); break;
-      case 4: PG_TRY(launch_fwd<4>(p, nsplit, jchunk, p->xin.p, p->part.p, s)); break;
-      default: PG_TRY(launch_fwd<8>(p, nsplit, jchunk, p->xin.p, p->part.p, s)); break;
+      case 1: PG_TRY(launch_fwd<1>(p, nsplit, jchunk, p->work->xin.p, p->work->part.p, s)); break;
+      case 2: PG_TRY(launch_fwd<2>(p, nsplit, jchunk, p->work->xin.p, p->work->part.p, s)); break;
+      case 4: PG_TRY(launch_fwd<4>(p, nsplit, jchunk, p->work->xin.p, p->work->part.p, s)); break;
+      default: PG_TRY(launch_fwd<8>(p, nsplit, jchunk, p->work->xin.p, p->work->part.p, s)); break;
     }
-    PG_LAUNCH(k_forward_finish, ceil_div(p->nk, 256), 256, 0, s, p->nk, nc, nsplit, ncp, p->part.p,
+    PG_LAUNCH(k_forward_finish, ceil_div(p->nk, 256), 256, 0, s, p->nk, nc, nsplit, ncp, p->work->part.p,
               y + (uint64_t)c0 * dstride, dstride);
   }
   return PG_OK;
@@ -251,26 +274,26 @@ pg_status gdft_adjoint(GdftPlan* p, int C, const float2* S, const float2* y, uin
   for (int c0 = 0; c0 < C; c0 += kCoilChunk) {
     const int nc = std::min(kCoilChunk, C - c0);
     const int ncp = pad_coils(nc);
-    PG_TRY(grow(p->part, (uint64_t)nsplit * ncp * p->ni, s));
+    PG_TRY(grow(p->work->part, (uint64_t)nsplit * ncp * p->ni, s));
     // Coils past nc read the first coil's data (valid memory); their sums are discarded.
     const float2* yc = y + (uint64_t)c0 * dstride;
     if (ncp > nc) {
       // stage the chunk contiguously so padded coils stay in bounds
-      PG_TRY(grow(p->xin, (uint64_t)ncp * p->nk, s));
+      PG_TRY(grow(p->work->xin, (uint64_t)ncp * p->nk, s));
       for (int c = 0; c < ncp; ++c)
-        PG_CUDA(cudaMemcpyAsync(p->xin.p + (uint64_t)c * p->nk, yc + (uint64_t)std::min(c, nc - 1) * dstride,
+        PG_CUDA(cudaMemcpyAsync(p->work->xin.p + (uint64_t)c * p->nk, yc + (uint64_t)std::min(c, nc - 1) * dstride,
                                 p->nk * sizeof(float2), cudaMemcpyDeviceToDevice, s));
-      yc = p->xin.p;
+      yc = p->work->xin.p;
     }
     const uint64_t stride = (ncp > nc) ? p->nk : dstride;
     ProfScope ps("dft_adj", s);
     switch (ncp) {
-      case 1: PG_TRY(launch_adj<1>(p, nsplit, ichunk, yc, stride, p->part.p, s)); break;
-      case 2: PG_TRY(launch_adj<2>(p, nsplit, ichunk, yc, stride, p->part.p, s)); break;
-      case 4: PG_TRY(launch_adj<4>(p, nsplit, ichunk, yc, stride, p->part.p, s)); break;
-      default: PG_TRY(launch_adj<8>(p, nsplit, ichunk, yc, stride, p->part.p, s)); break;
+      case 1: PG_TRY(launch_adj<1>(p, nsplit, ichunk, yc, stride, p->work->part.p, s)); break;
+      case 2: PG_TRY(launch_adj<2>(p, nsplit, ichunk, yc, stride, p->work->part.p, s)); break;
+      case 4: PG_TRY(launch_adj<4>(p, nsplit, ichunk, yc, stride, p->work->part.p, s)); break;
+      default: PG_TRY(launch_adj<8>(p, nsplit, ichunk, yc, stride, p->work->part.p, s)); break;
     }
-    PG_LAUNCH(k_adjoint_finish, ceil_div(p->ni, 256), 256, 0, s, p->ni, nc, c0, nsplit, ncp, p->part.p, S,
+    PG_LAUNCH(k_adjoint_finish, ceil_div(p->ni, 256), 256, 0, s, p->ni, nc, c0, nsplit, ncp, p->work->part.p, S,
               c0 > 0 ? 1 : 0, x);
   }
   return PG_OK;

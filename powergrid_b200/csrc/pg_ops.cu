@@ -296,6 +296,33 @@ uint64_t PcSenseTsOp::resident_bytes() const {
   return b;
 }
 
+// ---- pcSENSE (over Gdft) --------------------------------------------------------
+// fwd column (s + c*Ns) = G_s (x (.) S_c (.) E_s)   (pcSENSE.cpp:113-126)
+pg_status PcSenseOp::forward(const float2* x, float2* y, cudaStream_t s) {
+  PG_TRY(grow(tmp, Ni, s));
+  for (uint64_t sh = 0; sh < Ns; ++sh) {
+    PG_LAUNCH(k_cmul, ceil_div(Ni, 256), 256, 0, s, Ni, E.p + sh * Ni, x, 0, tmp.p);
+    PG_TRY(gdft_forward(plans[sh].get(), (int)Nc, S.p, tmp.p, y + sh * Nd, Ns * Nd, s));
+  }
+  return PG_OK;
+}
+// adj = sum_{c,s} conj(S_c) (.) E_s (.) G_s^H d_{c,s}   (pcSENSE.cpp:131-150): the
+// phase factor is E_s in both directions, as in the reference.
+pg_status PcSenseOp::adjoint(const float2* y, float2* x, cudaStream_t s) {
+  PG_TRY(grow(tmp, Ni, s));
+  for (uint64_t sh = 0; sh < Ns; ++sh) {
+    PG_TRY(gdft_adjoint(plans[sh].get(), (int)Nc, S.p, y + sh * Nd, Ns * Nd, tmp.p, s));
+    PG_LAUNCH(k_cmul_acc, ceil_div(Ni, 256), 256, 0, s, Ni, tmp.p, E.p + sh * Ni, 0, sh > 0 ? 1 : 0, x);
+  }
+  return PG_OK;
+}
+uint64_t PcSenseOp::resident_bytes() const {
+  uint64_t b = S.bytes() + E.bytes() + tmp.bytes();
+  for (auto& p : plans) b += p->ks.bytes() + (p->vs.owned ? p->vs.bytes() : 0);
+  if (!plans.empty()) b += plans[0]->work->xin.bytes() + plans[0]->work->part.bytes();
+  return b;
+}
+
 static pg_status make_binning_for(NufftPlan* plan, const TsTables& tab, std::unique_ptr<Binning>* out,
                                   cudaStream_t s) {
   return nufft_build_binning(plan, tab.L, tab.K, tab.l0.data(), tab.aa_win.data(), out, s);
@@ -505,6 +532,57 @@ pg_status pg_pcsense_timeseg_create(pg_op* out, const float* kx, const float* ky
     const float ph = shot_phase_map[i];
     if (!std::isfinite(ph)) return set_error(PG_INVALID_ARG, "pcSenseTimeSeg: non-finite phase map");
     E[i] = make_float2(std::cos(ph), -std::sin(ph));
+  }
+  PG_TRY(op->E.upload(E.data(), E.size(), s));
+  PG_CUDA(cudaStreamSynchronize(s));
+  *out = op.release();
+  return PG_OK;
+}
+
+pg_status pg_pcsense_create(pg_op* out, const float* kx, const float* ky, const float* kz, uint64_t nk, uint64_t nx,
+                            uint64_t ny, uint64_t nz, uint64_t nc, const float* t, const float* sense_map,
+                            const float* field_map, const float* shot_phase_map, uint64_t n_shot_phase) {
+  if (!out || !kx || !ky || !kz || !t || !sense_map || !field_map || !shot_phase_map)
+    return set_error(PG_INVALID_ARG, "pcSENSE: null argument");
+  PG_TRY(ensure_init());
+  const uint64_t Ni = nx * ny * nz;
+  if (Ni == 0 || n_shot_phase % Ni) return set_error(PG_INVALID_ARG, "pcSENSE: phase map size");
+  const uint64_t Ns = n_shot_phase / Ni;  // pcSENSE.cpp:44
+  if (Ns == 0 || nk % Ns) return set_error(PG_INVALID_ARG, "pcSENSE: samples not divisible by shots");
+  if (nc == 0) return set_error(PG_INVALID_ARG, "pcSENSE: no coils");
+  const uint64_t Nd = nk / Ns;            // :45
+  auto op = std::make_unique<PcSenseOp>();
+  op->kind = PG_OP_PCSENSE;
+  op->Ni = Ni; op->Nc = nc; op->Ns = Ns; op->Nd = Nd;
+  op->n_data = Nd * Ns * nc;
+  op->n_image = Ni;
+  cudaStream_t s = default_stream();
+  // voxel coordinates (pcSENSE.cpp:65-82): ix = (x - Nx/2)/Nx evaluated with a
+  // double Nx/2, y fastest
+  std::vector<float> ix(Ni), iy(Ni), iz(Ni);
+  for (uint64_t z = 0; z < nz; ++z)
+    for (uint64_t xx = 0; xx < nx; ++xx)
+      for (uint64_t yy = 0; yy < ny; ++yy) {
+        const uint64_t j = yy + ny * (xx + nx * z);
+        ix[j] = (float)(((float)xx - (float)nx / 2.0) / ((float)nx));
+        iy[j] = (float)(((float)yy - (float)ny / 2.0) / ((float)ny));
+        iz[j] = (float)(((float)z - (float)nz / 2.0) / ((float)nz));
+      }
+  for (uint64_t sh = 0; sh < Ns; ++sh) {
+    std::unique_ptr<GdftPlan> plan;
+    if (sh == 0)
+      PG_TRY(gdft_plan_create(&plan, Nd, Ni, kx, ky, kz, ix.data(), iy.data(), iz.data(), field_map, t, s));
+    else
+      PG_TRY(gdft_plan_same_voxels(&plan, *op->plans[0], Nd, kx + sh * Nd, ky + sh * Nd, kz + sh * Nd, t + sh * Nd,
+                                   s));
+    op->plans.push_back(std::move(plan));
+  }
+  PG_TRY(op->S.upload(reinterpret_cast<const float2*>(sense_map), Ni * nc, s));
+  std::vector<float2> E(Ni * Ns);
+  for (uint64_t i = 0; i < Ni * Ns; ++i) {
+    const float ph = shot_phase_map[i];
+    if (!std::isfinite(ph)) return set_error(PG_INVALID_ARG, "pcSENSE: non-finite phase map");
+    E[i] = make_float2(std::cos(ph), std::sin(ph));
   }
   PG_TRY(op->E.upload(E.data(), E.size(), s));
   PG_CUDA(cudaStreamSynchronize(s));

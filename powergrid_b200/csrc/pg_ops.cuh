@@ -8,7 +8,9 @@
 #include "pg_gdft.cuh"
 #include "pg_nufft.cuh"
 
-enum pg_op_kind { PG_OP_GNUFFT = 1, PG_OP_GDFT = 2, PG_OP_TIMESEG = 3, PG_OP_SENSE = 4, PG_OP_PCSENSE_TS = 5 };
+enum pg_op_kind {
+  PG_OP_GNUFFT = 1, PG_OP_GDFT = 2, PG_OP_TIMESEG = 3, PG_OP_SENSE = 4, PG_OP_PCSENSE_TS = 5, PG_OP_PCSENSE = 6
+};
 
 // Per-operator PWLS-PCG state kept between solves (buffers + the captured
 // per-iteration graph), defined in pg_pcg.cu.
@@ -88,6 +90,19 @@ struct PcSenseTsOp : pg_op_s {
   std::vector<TsTables> tabs;
   std::vector<DevBuf<float2>> Wo, WoH;
   DevBuf<float2> S, E;
+  pg_status forward(const float2* x, float2* y, cudaStream_t s) override;
+  pg_status adjoint(const float2* y, float2* x, cudaStream_t s) override;
+  uint64_t resident_bytes() const override;
+};
+
+// pcSENSE over Gdft (pcSENSE.cpp:40-153): per shot its own Gdft on that shot's
+// samples and times, all over one voxel table.
+struct PcSenseOp : pg_op_s {
+  uint64_t Ni = 0, Nc = 0, Ns = 0, Nd = 0;
+  std::vector<std::unique_ptr<GdftPlan>> plans;
+  DevBuf<float2> S;     // Ni x Nc coil maps
+  DevBuf<float2> E;     // Ni x Ns: conj(exp(-i P_s)) = exp(+i P_s) (pcSENSE.cpp:103)
+  DevBuf<float2> tmp;
   pg_status forward(const float2* x, float2* y, cudaStream_t s) override;
   pg_status adjoint(const float2* y, float2* x, cudaStream_t s) override;
   uint64_t resident_bytes() const override;

@@ -23,7 +23,7 @@ import numpy as np
 from . import _lib
 from ._lib import P, U64, Penalty, check
 
-__all__ = ["Gnufft", "Gdft", "TimeSegmentation", "SENSE", "pcSenseTimeSeg", "QuadPenalty", "TVPenalty",
+__all__ = ["Gnufft", "Gdft", "TimeSegmentation", "SENSE", "pcSenseTimeSeg", "pcSENSE", "QuadPenalty", "TVPenalty",
            "solve_pwls_pcg", "reconSolve", "init"]
 
 
@@ -177,6 +177,21 @@ class pcSenseTimeSeg(_Op):
         check(_lib.load().pg_pcsense_timeseg_create(C.byref(h), _ptr(kx), _ptr(ky), _ptr(kz), kx.size, int(nx),
                                                      int(ny), int(nz), int(nc), _ptr(t), int(L), int(intType),
                                                      _ptr(sm), _ptr(fm), _ptr(pm), pm.size))
+        super().__init__(h)
+
+
+class pcSENSE(_Op):
+    """Multishot phase-corrected SENSE over one Gdft per shot (pcSENSE.cpp:40-153).
+
+    As in the reference, forward and adjoint both weight by exp(+i*ShotPhaseMap)
+    (pcSENSE.cpp:103, 123, 146)."""
+
+    def __init__(self, kx, ky, kz, nx, ny, nz, nc, t, SENSEmap, FieldMap, ShotPhaseMap):
+        kx, ky, kz, t, fm, pm = (_f32(v) for v in (kx, ky, kz, t, FieldMap, ShotPhaseMap))
+        sm = _c64(SENSEmap)
+        h = P()
+        check(_lib.load().pg_pcsense_create(C.byref(h), _ptr(kx), _ptr(ky), _ptr(kz), kx.size, int(nx), int(ny),
+                                             int(nz), int(nc), _ptr(t), _ptr(sm), _ptr(fm), _ptr(pm), pm.size))
         super().__init__(h)
 
 

@@ -8,7 +8,7 @@ Armadillo layers (TimeSegmentation, SENSE, pcSenseTimeSeg, PCG).  FP64
 outputs come from the reference's double instantiation (Gnufft) and the
 FP64 DFT restatement.
 
-Run where the reference tree exists:  python tests/golden/make_golden.py
+Run where the reference tree exists:  python tests/golden/make_golden.py [case ...]
 Inputs are seeded (powergrid_b200.synthetic), so the files are reproducible.
 """
 from __future__ import annotations
@@ -57,6 +57,16 @@ def small_cases():
                               fm=S.field_map(S.Rng(109), 16, 16, 4, 200.0),
                               smap=S.coil_maps(S.Rng(110), 16, 16, 4, 2),
                               pmap=S.shot_phase_maps(S.Rng(111), 16, 16, 4, 2), x=S.image(S.Rng(112), 1024))
+    # 3-D pcSENSE over Gdft, 8x8x4, 2 shots x 256 samples, 2 coils, +-150 Hz
+    kxs, kys, kzs, ts = [], [], [], []
+    for s in range(2):
+        a, b, c, d = S.stack_of_spirals(8, 4, 2, 64, 20e-3, which=[s])
+        kxs.append(a); kys.append(b); kzs.append(c); ts.append(d)
+    cases["pcsense_gdft3d"] = dict(nx=8, ny=8, nz=4, kx=np.concatenate(kxs), ky=np.concatenate(kys),
+                                   kz=np.concatenate(kzs), t=np.concatenate(ts), nc=2,
+                                   fm=S.field_map(S.Rng(113), 8, 8, 4, 150.0),
+                                   smap=S.coil_maps(S.Rng(114), 8, 8, 4, 2),
+                                   pmap=S.shot_phase_maps(S.Rng(115), 8, 8, 4, 2), x=S.image(S.Rng(116), 256))
     # 2-D PCG: SENSE<TimeSegmentation<Gnufft>> + QuadPenalty, 5 iterations
     c = dict(cases["tssense2d"])
     c["beta"] = 1e-3
@@ -83,6 +93,9 @@ def build_op(name, c, prec):
     if name == "pcsense3d":
         return O.pcsense_timeseg(prec, c["kx"], c["ky"], c["kz"], c["nx"], c["ny"], c["nz"], c["nc"], c["t"], c["L"],
                                  c["smap"], c["fm"], c["pmap"])
+    if name == "pcsense_gdft3d":
+        return O.pcsense(prec, c["kx"], c["ky"], c["kz"], c["nx"], c["ny"], c["nz"], c["nc"], c["t"], c["smap"],
+                         c["fm"], c["pmap"])
     G = O.gnufft(prec, M, c["nx"], c["ny"], c["nz"], c["kx"], c["ky"], c["kz"])
     A = O.timeseg(G, c["fm"], c["t"], M, n, c["L"])
     return O.sense(A, c["smap"], M, n, c["nc"])
@@ -109,10 +122,13 @@ def compute(name, c, prec):
     return out
 
 
-def main():
+def main(only=None):
+    """Write every fixture, or only the named ones."""
     O.build(ref=True)
     O.use_reference(True)
     for name, c in small_cases().items():
+        if only and name not in only:
+            continue
         rec = {k: (np.asarray(v) if not np.isscalar(v) else np.array(v)) for k, v in c.items()}
         for prec, tag in ((0, "f32"), (2, "f64")):
             for k, v in compute(name, c, prec).items():
@@ -123,4 +139,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or None)

@@ -47,12 +47,15 @@ def _gpu_op(pg, name, c):
     if name == "pcsense3d":
         return pg.pcSenseTimeSeg(c["kx"], c["ky"], c["kz"], c["nx"], c["ny"], c["nz"], c["nc"], c["t"], c["L"], 1,
                                  c["smap"], c["fm"], c["pmap"])
+    if name == "pcsense_gdft3d":
+        return pg.pcSENSE(c["kx"], c["ky"], c["kz"], c["nx"], c["ny"], c["nz"], c["nc"], c["t"], c["smap"], c["fm"],
+                          c["pmap"])
     G = pg.Gnufft(M, 2.0, c["nx"], c["ny"], c["nz"], c["kx"], c["ky"], c["kz"])
     A = pg.TimeSegmentation(G, c["fm"], c["t"], M, n, c["L"], 1, 1)
     return pg.SENSE(A, c["smap"], M, n, c["nc"])
 
 
-@pytest.mark.parametrize("name", ["nufft2d", "nufft3d", "gdft3d", "tssense2d", "pcsense3d"])
+@pytest.mark.parametrize("name", ["nufft2d", "nufft3d", "gdft3d", "tssense2d", "pcsense3d", "pcsense_gdft3d"])
 def test_operator_vs_reference_fixture(pg, name):
     c = _case(name)
     op = _gpu_op(pg, name, c)
@@ -236,3 +239,35 @@ def test_allocation_failure_is_reported_and_recoverable(pg):
     _lib.load().pg_debug_fail_allocation_after(0)
     op = _gpu_op(pg, "nufft2d", c)
     assert rel_l2(op * c["x"], c["y_f32"]) <= OP_TOL
+
+
+def test_pcsense_gdft_at_size_vs_oracle(pg, oracle):
+    """pcSENSE over Gdft, 16x16x8, 4 shots x 1024 samples, 4 coils, against the
+    restated reference path (float, the reference's ftCpu formula) and FP64."""
+    from powergrid_b200 import synthetic as S
+    nx = ny = 16
+    nz = 8
+    ns, nc = 4, 4
+    kxs, kys, kzs, ts = [], [], [], []
+    for s in range(ns):
+        a, b, c, d = S.stack_of_spirals(nx, nz, ns, 128, 20e-3, which=[s])
+        kxs.append(a); kys.append(b); kzs.append(c); ts.append(d)
+    kx, ky, kz, t = (np.concatenate(v) for v in (kxs, kys, kzs, ts))
+    fm = S.field_map(S.Rng(121), nx, ny, nz, 150.0)
+    sm = S.coil_maps(S.Rng(122), nx, ny, nz, nc)
+    pm = S.shot_phase_maps(S.Rng(123), nx, ny, nz, ns)
+    x = S.image(S.Rng(124), nx * ny * nz)
+    A = pg.pcSENSE(kx, ky, kz, nx, ny, nz, nc, t, sm, fm, pm)
+    R32 = oracle.pcsense(0, kx, ky, kz, nx, ny, nz, nc, t, sm, fm, pm)
+    R64 = oracle.pcsense(2, kx, ky, kz, nx, ny, nz, nc, t, sm, fm, pm)
+    y = A * x
+    y32 = R32.forward(x)
+    y64 = R64.forward(x.astype(np.complex128))
+    xa = A / y32
+    xa32 = R32.adjoint(y32)
+    xa64 = R64.adjoint(y32.astype(np.complex128))
+    ef, ea = rel_l2(y, y32), rel_l2(xa, xa32)
+    print(f"pcSENSE 16x16x8: fwd {ef:.2e} (fp64 {rel_l2(y, y64):.2e}, ref {rel_l2(y32, y64):.2e}); "
+          f"adj {ea:.2e} (fp64 {rel_l2(xa, xa64):.2e}, ref {rel_l2(xa32, xa64):.2e})")
+    assert ef <= OP_TOL and ea <= OP_TOL
+    assert rel_l2(y, y64) <= rel_l2(y32, y64) + OP_TOL
