@@ -59,7 +59,9 @@ uint64_t pg_kernel_launch_count(void);
  * coordinates ix/iy/iz are stored but unused by the math in the reference
  * (Gnufft.cpp:47-49), so they are not taken here.  2-D requires nx == ny
  * (the reference mixes x/y-fastest conventions otherwise: zero_pad2d
- * griddingSupport.cpp:488 vs gridding.cpp:100).  gridos must be 2 here. */
+ * griddingSupport.cpp:488 vs gridding.cpp:100).  Operator application
+ * needs gridos = 2; an operator made with another factor (up to 3.75) serves
+ * the spatial interpolation below only, as density compensation uses it. */
 pg_status pg_gnufft_create(pg_op* out, uint64_t data_length, float gridos, uint64_t nx, uint64_t ny,
                            uint64_t nz, const float* kx, const float* ky, const float* kz);
 
@@ -114,6 +116,32 @@ pg_status pg_op_adjoint(pg_op op, const float* y, float* x);
  * library's default stream).  No host synchronisation. */
 pg_status pg_op_forward_device(pg_op op, const void* x_dev, void* y_dev, void* stream);
 pg_status pg_op_adjoint_device(pg_op op, const void* y_dev, void* x_dev, void* stream);
+
+/* ---- interpolation without the FFT, and the direct reconstruction -------- */
+/* Cells of the operator's oversampled grid (Gnufft.cpp:56-61). */
+pg_status pg_gnufft_grid_length(pg_op G, uint64_t* n_cells);
+/* Gnufft::forwardSpatialInterp (Gnufft.cpp:213-258): grid (complex, n_cells,
+ * the reference's unshifted y-fastest layout, gridding.cpp:66) -> samples
+ * (complex, data_length).  Host buffers, synchronous. */
+pg_status pg_gnufft_forward_spatial_interp(pg_op G, const float* grid, float* samples);
+/* Gnufft::adjointSpatialInterp (Gnufft.cpp:261-330): samples -> grid (every
+ * cell written). */
+pg_status pg_gnufft_adjoint_spatial_interp(pg_op G, const float* samples, float* grid);
+/* The same on device buffers, stream-ordered. */
+pg_status pg_gnufft_forward_spatial_interp_device(pg_op G, const void* grid_dev, void* samples_dev, void* stream);
+pg_status pg_gnufft_adjoint_spatial_interp_device(pg_op G, const void* samples_dev, void* grid_dev, void* stream);
+/* calc3DDensityCompensation(kx, ky, kz, Ninplane, Nz)
+ * (reconSupport/directRecon.cpp:28-61): two Pipe iterations on a 3x
+ * oversampled grid, normalised to unit L2 norm; dcf = n floats. */
+pg_status pg_density_compensation(const float* kx, const float* ky, const float* kz, uint64_t n,
+                                  uint64_t n_inplane, uint64_t nz, float* dcf);
+/* The per-coil step of gridCoilImages (directRecon.cpp:108-133):
+ * images[c] = G / (dcf .* data[c]) for nc coils; data coil-major [c][sample],
+ * images coil-major [c][voxel] (complex). */
+pg_status pg_grid_coil_images(pg_op G, const float* dcf, const float* data, uint64_t nc, float* images);
+/* calcSumOfSquaresImage (directRecon.cpp:63-73): out[p] = sqrt(sum_c |img_c[p]|)
+ * (a sum of magnitudes, as the reference computes it). */
+pg_status pg_sum_of_squares_image(const float* coil_images, uint64_t n, uint64_t nc, float* out);
 
 /* y = Gdft * x for one coil, computed without allocating any device memory.
  * No counterpart in the reference: it exists for callers that manage all

@@ -52,6 +52,11 @@ def lib() -> C.CDLL:
         L.orc_pcsense_ts_new.argtypes = [C.c_int, P, P, P, U64, U64, U64, U64, U64, P, U64, U64, P, P, P, U64]
         L.orc_pcsense_new.restype = P
         L.orc_pcsense_new.argtypes = [C.c_int, P, P, P, U64, U64, U64, U64, U64, P, P, P, P, U64]
+        L.orc_gnufft_grid_len.restype = U64
+        L.orc_gnufft_grid_len.argtypes = [P]
+        L.orc_gnufft_interp_fwd.argtypes = [P, P, P]
+        L.orc_gnufft_interp_adj.argtypes = [P, P, P]
+        L.orc_density_compensation.argtypes = [C.c_int, P, P, P, U64, U64, U64, P]
         L.orc_free.argtypes = [P]
         L.orc_data_len.restype = U64
         L.orc_data_len.argtypes = [P]
@@ -196,6 +201,42 @@ def pcsense(prec, kx, ky, kz, nx, ny, nz, nc, t, smap, fm, pmap) -> Op:
     s = np.ascontiguousarray(smap, dtype=C64)
     return Op(lib().orc_pcsense_new(prec, _p(kx), _p(ky), _p(kz), kx.size, nx, ny, nz, nc, _p(t), _p(s), _p(fm),
                                     _p(pm), pm.size), prec)
+
+
+def forward_spatial_interp(G: Op, grid) -> np.ndarray:
+    """Gnufft::forwardSpatialInterp (Gnufft.cpp:213-258) of a Gnufft oracle handle."""
+    dt = C64 if G.prec == 0 else np.complex128
+    g = np.ascontiguousarray(grid, dtype=dt)
+    assert g.size == lib().orc_gnufft_grid_len(G.h)
+    out = np.zeros(lib().orc_data_len(G.h), dtype=dt)
+    lib().orc_gnufft_interp_fwd(G.h, _p(g), _p(out))
+    return out
+
+
+def adjoint_spatial_interp(G: Op, d) -> np.ndarray:
+    """Gnufft::adjointSpatialInterp (Gnufft.cpp:261-330) of a Gnufft oracle handle."""
+    dt = C64 if G.prec == 0 else np.complex128
+    v = np.ascontiguousarray(d, dtype=dt)
+    out = np.zeros(lib().orc_gnufft_grid_len(G.h), dtype=dt)
+    lib().orc_gnufft_interp_adj(G.h, _p(v), _p(out))
+    return out
+
+
+def density_compensation(prec, kx, ky, kz, ninplane, nz) -> np.ndarray:
+    """calc3DDensityCompensation (reconSupport/directRecon.cpp:28-61)."""
+    kx, ky, kz = (_f32(v) for v in (kx, ky, kz))
+    out = np.zeros(kx.size, dtype=F32 if prec == 0 else F64)
+    lib().orc_density_compensation(prec, _p(kx), _p(ky), _p(kz), kx.size, ninplane, nz, _p(out))
+    return out
+
+
+def sum_of_squares_image(coil_images, nc) -> np.ndarray:
+    """calcSumOfSquaresImage (directRecon.cpp:63-73): sqrt of the coil-ordered float sum of |img_c|."""
+    img = np.ascontiguousarray(coil_images, dtype=C64).reshape(nc, -1)
+    acc = np.zeros(img.shape[1], dtype=F32)
+    for c in range(nc):
+        acc = (acc + np.abs(img[c]).astype(F32)).astype(F32)
+    return np.sqrt(acc).astype(F32)
 
 
 def kb_lut(prec: int, gridos: float = 2.0):

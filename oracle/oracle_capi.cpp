@@ -161,7 +161,12 @@ int orc_use_reference(const char* so_path) {
   kd.fh = (decltype(kd.fh))dlsym(h, "pgref_fh_d");
   kd.ft = (decltype(kd.ft))dlsym(h, "pgref_ft_d");
   kd.ift = (decltype(kd.ift))dlsym(h, "pgref_ift_d");
-  if (!kf.fd || !kf.fh || !kf.ft || !kf.ift || !kd.fd || !kd.fh || !kd.ft || !kd.ift) {
+  kf.ifwd = (decltype(kf.ifwd))dlsym(h, "pgref_ifwd_f");
+  kf.iadj = (decltype(kf.iadj))dlsym(h, "pgref_iadj_f");
+  kd.ifwd = (decltype(kd.ifwd))dlsym(h, "pgref_ifwd_d");
+  kd.iadj = (decltype(kd.iadj))dlsym(h, "pgref_iadj_d");
+  if (!kf.fd || !kf.fh || !kf.ft || !kf.ift || !kd.fd || !kd.fh || !kd.ft || !kd.ift || !kf.ifwd || !kf.iadj ||
+      !kd.ifwd || !kd.iadj) {
     g_err = "libpgref.so lacks an expected symbol";
     return -1;
   }
@@ -335,6 +340,47 @@ int orc_adjoint(void* h, const void* y, void* x) {
     o->f->adjoint((const std::complex<float>*)y, (std::complex<float>*)x);
   else
     o->d->adjoint((const std::complex<double>*)y, (std::complex<double>*)x);
+  return 0;
+}
+
+// Spatial interpolation of a Gnufft handle (grid in the reference's layout).
+u64 orc_gnufft_grid_len(void* h) {
+  Handle* o = (Handle*)h;
+  if (o->prec == 0) return dynamic_cast<pgo::GnufftOp<float>&>(*o->f).g.ngrid();
+  return dynamic_cast<pgo::GnufftOp<double>&>(*o->d).g.ngrid();
+}
+int orc_gnufft_interp_fwd(void* h, const void* grid, void* y) {
+  Handle* o = (Handle*)h;
+  if (o->prec == 0)
+    dynamic_cast<pgo::GnufftOp<float>&>(*o->f).forward_interp((const std::complex<float>*)grid,
+                                                               (std::complex<float>*)y);
+  else
+    dynamic_cast<pgo::GnufftOp<double>&>(*o->d).forward_interp((const std::complex<double>*)grid,
+                                                                (std::complex<double>*)y);
+  return 0;
+}
+int orc_gnufft_interp_adj(void* h, const void* d, void* grid) {
+  Handle* o = (Handle*)h;
+  if (o->prec == 0)
+    dynamic_cast<pgo::GnufftOp<float>&>(*o->f).adjoint_interp((const std::complex<float>*)d,
+                                                               (std::complex<float>*)grid);
+  else
+    dynamic_cast<pgo::GnufftOp<double>&>(*o->d).adjoint_interp((const std::complex<double>*)d,
+                                                                (std::complex<double>*)grid);
+  return 0;
+}
+
+// calc3DDensityCompensation; out: n floats (prec 0) or doubles.
+int orc_density_compensation(int prec, const float* kx, const float* ky, const float* kz, u64 n, u64 ninplane,
+                             u64 nz, void* out) {
+  if (prec == 0) {
+    auto v = pgo::density_compensation<float>(kx, ky, kz, n, (int)ninplane, (int)nz, g_use_ref);
+    std::memcpy(out, v.data(), n * sizeof(float));
+  } else {
+    auto a = widen<double>(kx, n), b = widen<double>(ky, n), c = widen<double>(kz, n);
+    auto v = pgo::density_compensation<double>(a.data(), b.data(), c.data(), n, (int)ninplane, (int)nz, g_use_ref);
+    std::memcpy(out, v.data(), n * sizeof(double));
+  }
   return 0;
 }
 

@@ -11,6 +11,7 @@
 //   SENSE               SENSE.cpp:33-97
 //   pcSenseTimeSeg      pcSenseTimeSeg.cpp:41-171
 //   pcSENSE             pcSENSE.cpp:40-153
+//   spatial interpolation, density compensation   Gnufft.cpp:213-337, reconSupport/directRecon.cpp:28-73
 //   Robject/Quad/TV     Robject.cpp:49-193, QuadPenalty.cpp:45-64, TVPenalty.cpp:43-68
 //   solve_pwls_pcg      solve_pwls_pcg.hpp:34-167
 //
@@ -376,6 +377,9 @@ struct RefKernels {
              const T*, const T*, int, int) = nullptr;
   void (*ift)(T*, T*, const T*, const T*, const T*, const T*, const T*, const T*, const T*, const T*,
               const T*, const T*, int, int) = nullptr;
+  // forwardSpatialInterp / adjointSpatialInterp bodies
+  void (*ifwd)(int, const T*, const T*, const T*, const T*, u64, int, int, int, T, T, T, const T*, u64, T*) = nullptr;
+  void (*iadj)(int, const T*, const T*, const T*, const T*, u64, int, int, int, T, T, T, const T*, u64, T*) = nullptr;
 };
 template <typename T>
 RefKernels<T>& ref_kernels() {
@@ -445,7 +449,70 @@ struct GnufftOp : Op<T> {
     crop_center(g, x, a.data());
     deapodize(g, x);
   }
+  // Gnufft::forwardSpatialInterp (Gnufft.cpp:213-258): grid -> samples, no FFT
+  void forward_interp(const C* grid, C* y) const {
+    const u64 M = this->n2;
+    if (use_ref && ref_kernels<T>().ifwd) {
+      ref_kernels<T>().ifwd((int)M, kx.data(), ky.data(), kz.data(), reinterpret_cast<const T*>(grid), g.ngrid(),
+                            g.Nx, g.Ny, g.Nz, g.os, g.kw, g.beta, g.lut.data(), g.lut.size(), reinterpret_cast<T*>(y));
+      return;
+    }
+    interp_forward(g, M, kx.data(), ky.data(), kz.data(), grid, y);
+  }
+  // Gnufft::adjointSpatialInterp (Gnufft.cpp:261-330): samples -> zeroed grid + spread
+  void adjoint_interp(const C* d, C* grid) const {
+    const u64 M = this->n2;
+    if (use_ref && ref_kernels<T>().iadj) {
+      ref_kernels<T>().iadj((int)M, kx.data(), ky.data(), kz.data(), reinterpret_cast<const T*>(d), g.ngrid(), g.Nx,
+                            g.Ny, g.Nz, g.os, g.kw, g.beta, g.lut.data(), g.lut.size(), reinterpret_cast<T*>(grid));
+      return;
+    }
+    std::fill(grid, grid + g.ngrid(), C(0, 0));
+    spread_adjoint(g, M, kx.data(), ky.data(), kz.data(), d, grid);
+  }
 };
+
+// calc3DDensityCompensation (reconSupport/directRecon.cpp:28-61).  Armadillo
+// divides a complex column by a real one or by a scalar after promoting the
+// divisor to complex, so the divisions here are complex / complex.
+template <typename T>
+std::vector<T> density_compensation(const T* kx, const T* ky, const T* kz, u64 n, int ninplane, int nz,
+                                    bool use_ref) {
+  using C = std::complex<T>;
+  GnufftOp<T> G(n, (T)3.0, ninplane, ninplane, nz, kx, ky, kz);  // overSampling = 3 (:32-35)
+  G.use_ref = use_ref;
+  std::vector<C> dcf(n, C(1, 0));
+  const C den((T)n * (T)n);
+  for (auto& v : dcf) v /= den;                                  // :38-40
+  std::vector<C> c1(G.g.ngrid()), c2(n);
+  for (int it = 0; it < 2; ++it) {                               // Niter = 2 (:30), :49-55
+    G.adjoint_interp(dcf.data(), c1.data());
+    G.forward_interp(c1.data(), c2.data());
+    for (u64 i = 0; i < n; ++i) dcf[i] = dcf[i] / C(c2[i].real());
+  }
+  // normalise(dcf, 2) (:57): Armadillo's 2-norm of a complex column sums
+  // |v|^2 and, if that underflows or overflows, rescales by the largest |v|
+  T acc = 0;
+  for (const auto& v : dcf) {
+    const T a = std::abs(v);
+    acc += a * a;
+  }
+  T nrm = std::sqrt(acc);
+  if (nrm == (T)0 || !std::isfinite(nrm)) {
+    T mx = 0;
+    for (const auto& v : dcf) mx = std::max(mx, std::abs(v));
+    T alt = 0;
+    if (mx > (T)0 && std::isfinite(mx))
+      for (const auto& v : dcf) {
+        const T a = std::abs(v) / mx;
+        alt += a * a;
+      }
+    nrm = (mx > (T)0 && std::isfinite(mx)) ? std::sqrt(alt) * mx : nrm;
+  }
+  std::vector<T> out(n);
+  for (u64 i = 0; i < n; ++i) out[i] = std::abs(nrm != (T)0 ? dcf[i] / C(nrm) : dcf[i]);  // abs (:59)
+  return out;
+}
 
 // Gdft (Gdft.cpp:33-136).  exact64 selects the FP64 oracle formula (double
 // sin/cos); otherwise the expression types of ftCpu / iftCpu are kept

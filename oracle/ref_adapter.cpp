@@ -5,11 +5,14 @@
 // place by oracle/Makefile into oracle/_ref/libpgref.so).  Each wrapper
 // allocates the scratch buffers the way Gnufft's constructor does
 // (Gnufft.cpp:104-113) and calls the reference template exactly as
-// Gnufft::operator* / operator/ do (Gnufft.cpp:167-171, 203-207) and as
+// Gnufft::operator* / operator/ do (Gnufft.cpp:167-171, 203-207), as the
+// spatial interpolation methods do (Gnufft.cpp:238-253, 286-327) and as
 // Gdft does (Gdft.cpp:78-80, 120-122).  Nothing here re-implements the math.
 #include "gridding.h"
 #include "ftCpu.h"
 
+#include <cmath>
+#include <cstring>
 #include <vector>
 
 namespace {
@@ -44,9 +47,89 @@ void fh(int M, const T* kx, const T* ky, const T* kz, const T* d, int Nx, int Ny
   std::memcpy(x, g.data(), sizeof(T) * 2 * ni);
 }
 
+// parameters exactly as Gnufft::forwardSpatialInterp / adjointSpatialInterp
+// fill them (Gnufft.cpp:218-236, 266-284)
+template <typename T>
+parameters<T> interp_params(int M, int Nx, int Ny, int Nz, T gridos, T kw) {
+  parameters<T> p;
+  p.sync = 0;
+  p.binsize = 128;
+  p.useLUT = 1;
+  p.kernelWidth = kw;
+  p.gridOS = gridos;
+  p.imageSize[0] = Nx;
+  p.imageSize[1] = Ny;
+  p.imageSize[2] = Nz;
+  p.gridSize[0] = std::ceil(gridos * (T)Nx);
+  p.gridSize[1] = std::ceil(gridos * (T)Ny);
+  if (p.gridSize[0] % 2) p.gridSize[0] += 1;
+  if (p.gridSize[1] % 2) p.gridSize[1] += 1;
+  p.gridSize[2] = (Nz == 1) ? Nz : (std::ceil(gridos * (T)Nz));
+  p.numSamples = M;
+  return p;
+}
+
+// forwardSpatialInterp's body (Gnufft.cpp:238-253): samples zeroed, then
+// gridding_forward on the caller's grid.
+template <typename T>
+void ifwd(int M, const T* kx, const T* ky, const T* kz, const T* grid, unsigned long long ngrid, int Nx, int Ny,
+          int Nz, T gridos, T kw, T beta, const T* lut, unsigned long long nlut, T* y) {
+  parameters<T> p = interp_params<T>(M, Nx, Ny, Nz, gridos, kw);
+  std::vector<T> g(grid, grid + 2 * ngrid), s(2 * (size_t)M, (T)0.0);
+  if (Nz == 1)
+    gridding_forward_2D<T>(M, p, kx, ky, beta, s.data(), lut, nlut, g.data());
+  else
+    gridding_forward_3D<T>(M, p, kx, ky, kz, beta, s.data(), lut, nlut, g.data());
+  std::memcpy(y, s.data(), sizeof(T) * 2 * (size_t)M);
+}
+
+// adjointSpatialInterp's body (Gnufft.cpp:286-327): samples packed with
+// sdc = 1, grid zeroed, gridding_adjoint.
+template <typename T>
+void iadj(int M, const T* kx, const T* ky, const T* kz, const T* d, unsigned long long ngrid, int Nx, int Ny,
+          int Nz, T gridos, T kw, T beta, const T* lut, unsigned long long nlut, T* grid) {
+  parameters<T> p = interp_params<T>(M, Nx, Ny, Nz, gridos, kw);
+  std::vector<ReconstructionSample<T>> smp(M);
+  for (int i = 0; i < M; ++i) {
+    smp[i].kX = kx[i];
+    smp[i].kY = ky[i];
+    smp[i].kZ = kz[i];
+    smp[i].real = d[2 * i];
+    smp[i].imag = d[2 * i + 1];
+    smp[i].sdc = (T)1.0;
+  }
+  std::vector<T> g(2 * ngrid, (T)0.0);
+  if (Nz == 1)
+    gridding_adjoint_2D<T>(M, p, beta, smp.data(), lut, nlut, g.data());
+  else
+    gridding_adjoint_3D<T>(M, p, beta, smp.data(), lut, nlut, g.data());
+  std::memcpy(grid, g.data(), sizeof(T) * 2 * ngrid);
+}
+
 }  // namespace
 
 extern "C" {
+
+void pgref_ifwd_f(int M, const float* kx, const float* ky, const float* kz, const float* grid, unsigned long long ng,
+                  int Nx, int Ny, int Nz, float os, float kw, float beta, const float* lut, unsigned long long nlut,
+                  float* y) {
+  ifwd<float>(M, kx, ky, kz, grid, ng, Nx, Ny, Nz, os, kw, beta, lut, nlut, y);
+}
+void pgref_iadj_f(int M, const float* kx, const float* ky, const float* kz, const float* d, unsigned long long ng,
+                  int Nx, int Ny, int Nz, float os, float kw, float beta, const float* lut, unsigned long long nlut,
+                  float* grid) {
+  iadj<float>(M, kx, ky, kz, d, ng, Nx, Ny, Nz, os, kw, beta, lut, nlut, grid);
+}
+void pgref_ifwd_d(int M, const double* kx, const double* ky, const double* kz, const double* grid,
+                  unsigned long long ng, int Nx, int Ny, int Nz, double os, double kw, double beta, const double* lut,
+                  unsigned long long nlut, double* y) {
+  ifwd<double>(M, kx, ky, kz, grid, ng, Nx, Ny, Nz, os, kw, beta, lut, nlut, y);
+}
+void pgref_iadj_d(int M, const double* kx, const double* ky, const double* kz, const double* d,
+                  unsigned long long ng, int Nx, int Ny, int Nz, double os, double kw, double beta, const double* lut,
+                  unsigned long long nlut, double* grid) {
+  iadj<double>(M, kx, ky, kz, d, ng, Nx, Ny, Nz, os, kw, beta, lut, nlut, grid);
+}
 
 // calculateLUT (griddingSupport.cpp:52-76); caller frees with pgref_free.
 float* pgref_lut_f(float beta, float width, unsigned long long* n) {

@@ -63,6 +63,14 @@ SIGNATURES = {
     "pg_pcsense_timeseg_create": (C.c_int, [C.POINTER(P), P, P, P, U64, U64, U64, U64, U64, P, U64, U64, P, P, P,
                                             U64]),
     "pg_pcsense_create": (C.c_int, [C.POINTER(P), P, P, P, U64, U64, U64, U64, U64, P, P, P, P, U64]),
+    "pg_gnufft_grid_length": (C.c_int, [P, C.POINTER(U64)]),
+    "pg_gnufft_forward_spatial_interp": (C.c_int, [P, P, P]),
+    "pg_gnufft_adjoint_spatial_interp": (C.c_int, [P, P, P]),
+    "pg_gnufft_forward_spatial_interp_device": (C.c_int, [P, P, P, P]),
+    "pg_gnufft_adjoint_spatial_interp_device": (C.c_int, [P, P, P, P]),
+    "pg_density_compensation": (C.c_int, [P, P, P, U64, U64, U64, P]),
+    "pg_grid_coil_images": (C.c_int, [P, P, P, U64, P]),
+    "pg_sum_of_squares_image": (C.c_int, [P, U64, U64, P]),
     "pg_op_destroy": (C.c_int, [P]),
     "pg_op_shape": (C.c_int, [P, C.POINTER(U64), C.POINTER(U64)]),
     "pg_op_forward": (C.c_int, [P, P, P]),

@@ -30,6 +30,7 @@
 
 #include "pg_binsort.cuh"
 #include "pg_fft2d.cuh"
+#include "pg_kb.cuh"
 #include "pg_nufft.cuh"
 #include "pg_profile.cuh"
 
@@ -100,22 +101,14 @@ void kb_table(float gridos, std::vector<float>* lut, float* beta_out) {
 // 8 consecutive cells starting at `st`.  Cells outside [lo, hi] weigh 0.
 __device__ __forceinline__ int axis_taps(float k, int n_img, float os, float kw, const float* __restrict__ lut,
                                          int nlut, float* w) {
-  const float s = __fmul_rn(os, __fadd_rn(k, __fdiv_rn((float)n_img, 2.0f)));
-  const float half = __fdiv_rn(__fmul_rn(kw, os), 2.0f);
-  const int lo = (int)fmaxf(0.0f, ceilf(__fsub_rn(s, half)));
-  const int hi = (int)fminf(__fsub_rn(__fmul_rn(os, (float)n_img), 1.0f), floorf(__fadd_rn(s, half)));
+  int lo, hi;
+  const float s = kb_window(k, n_img, os, kw, &lo, &hi);
   const int st = (hi - lo == 8) ? lo + 1 : lo;
   const float kw2 = __fmul_rn(kw, kw);
 #pragma unroll
   for (int a = 0; a < 8; ++a) {
     const int c = st + a;
-    float wv = 0.0f;
-    if (c >= lo && c <= hi) {
-      const float dist = __fdiv_rn(fabsf(__fsub_rn(s, (float)c)), os);
-      const int k0 = (int)__fmul_rn(__fdiv_rn(__fmul_rn(__fmul_rn(dist, dist), 4.0f), kw2), (float)nlut);
-      wv = (k0 >= nlut || k0 < 0) ? 0.0f : lut[k0];
-    }
-    w[a] = wv;
+    w[a] = (c >= lo && c <= hi) ? kb_weight(s, c, os, kw2, lut, nlut) : 0.0f;
   }
   return st;
 }

@@ -129,19 +129,27 @@ pg_status build_ts_phases(const TsTables& T, const float* field_map, uint64_t n2
 }
 
 // ---- Gnufft ------------------------------------------------------------------
+static pg_status interp_only() {
+  return set_error(PG_INVALID_ARG, "Gnufft: operator application needs gridos = 2 (other factors: spatial "
+                                   "interpolation only)");
+}
+
 pg_status GnufftOp::forward(const float2* x, float2* y, cudaStream_t s) {
+  if (!plan) return interp_only();
   NufftBatch b;
   b.C = 1;
   b.data_stride = plan->M;
   return nufft_forward(plan.get(), b, x, y, s);
 }
 pg_status GnufftOp::adjoint(const float2* y, float2* x, cudaStream_t s) {
+  if (!plan) return interp_only();
   NufftBatch b;
   b.C = 1;
   b.data_stride = plan->M;
   return nufft_adjoint(plan.get(), b, y, x, s);
 }
 uint64_t GnufftOp::resident_bytes() const {
+  if (!plan) return interp ? interp->M * 16 + interp->lut.bytes() : 0;
   return plan->M * (3 * 4 + 8 + 64 + 4 + 4) + plan->work->grids.bytes() + plan->work->fin.bytes();
 }
 
@@ -204,14 +212,14 @@ static bool nufft_under(pg_op_s* inner, NufftPlan** plan, const TimeSegOp** ts) 
   *ts = nullptr;
   if (inner->kind == PG_OP_GNUFFT) {
     *plan = static_cast<GnufftOp*>(inner)->plan.get();
-    return true;
+    return *plan != nullptr;
   }
   if (inner->kind == PG_OP_TIMESEG) {
     auto* t = static_cast<TimeSegOp*>(inner);
     if (t->inner->kind == PG_OP_GNUFFT) {
       *plan = static_cast<GnufftOp*>(t->inner)->plan.get();
       *ts = t->tab.L > 1 ? t : nullptr;
-      return true;
+      return *plan != nullptr;
     }
   }
   return false;
@@ -334,7 +342,10 @@ pg_status make_gnufft(std::unique_ptr<GnufftOp>* out, uint64_t data_length, floa
   if (nz > 1 && !kz) return set_error(PG_INVALID_ARG, "Gnufft: kz required for 3-D");
   auto op = std::make_unique<GnufftOp>();
   op->kind = PG_OP_GNUFFT;
-  PG_TRY(nufft_plan_create(&op->plan, data_length, gridos, (int)nx, (int)ny, (int)nz, kx, ky, kz, s));
+  if (gridos != 2.0f)
+    PG_TRY(interp_plan_create(&op->interp, data_length, gridos, (int)nx, (int)ny, (int)nz, kx, ky, kz, s));
+  else
+    PG_TRY(nufft_plan_create(&op->plan, data_length, gridos, (int)nx, (int)ny, (int)nz, kx, ky, kz, s));
   op->n_data = data_length;
   op->n_image = nx * ny * nz;
   *out = std::move(op);
@@ -357,6 +368,7 @@ pg_status make_timeseg(std::unique_ptr<TimeSegOp>* out, pg_op_s* G, const float*
   if (op->tab.L > 1) {
     PG_TRY(build_ts_phases(op->tab, field_map, n2, &op->Wo, &op->WoH, s));
     if (G->kind == PG_OP_GNUFFT) {
+      if (!static_cast<GnufftOp*>(G)->plan) return interp_only();
       PG_TRY(make_binning_for(static_cast<GnufftOp*>(G)->plan.get(), op->tab, &op->bin, s));
     } else {
       PG_TRY(op->AAfull.upload(op->tab.AA.data(), op->tab.AA.size(), s));
@@ -372,6 +384,7 @@ pg_status make_timeseg(std::unique_ptr<TimeSegOp>* out, pg_op_s* G, const float*
 pg_status make_gnufft_shared(std::unique_ptr<GnufftOp>* out, const GnufftOp& src) {
   auto op = std::make_unique<GnufftOp>();
   op->kind = PG_OP_GNUFFT;
+  if (!src.plan) return interp_only();
   PG_TRY(nufft_plan_share(*src.plan, &op->plan));
   op->n_data = src.n_data;
   op->n_image = src.n_image;
@@ -407,6 +420,7 @@ pg_status make_timeseg_shared(std::unique_ptr<TimeSegOp>* out, pg_op_s* G, const
 pg_status tune_for_coils(pg_op_s* G, int nc, bool search, cudaStream_t s) {
   if (G->kind == PG_OP_GNUFFT) {
     NufftPlan* plan = static_cast<GnufftOp*>(G)->plan.get();
+    if (!plan) return PG_OK;
     return nufft_autotune(plan, 1, 1, nullptr, nullptr, nc, &plan->plain, search, s);
   }
   if (G->kind == PG_OP_TIMESEG) {
@@ -658,6 +672,7 @@ pg_status pg_util_gnufft_binning(pg_op G, uint32_t* keys_out, uint32_t* perm_out
   if (!G) return set_error(PG_INVALID_ARG, "null operator");
   const Binning* b = nullptr;
   if (G->kind == PG_OP_GNUFFT) {
+    if (!static_cast<GnufftOp*>(G)->plan) return interp_only();
     PG_TRY(nufft_plain_binning(static_cast<GnufftOp*>(G)->plan.get(), default_stream()));
     b = static_cast<GnufftOp*>(G)->plan->plain.get();
   }

@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "pg_gdft.cuh"
+#include "pg_interp.cuh"
 #include "pg_nufft.cuh"
 
 enum pg_op_kind {
@@ -52,7 +53,8 @@ pg_status build_ts_tables(const float* field_map, const float* tvec, uint64_t n1
                           uint64_t interptype, uint64_t shots, TsTables* out);
 
 struct GnufftOp : pg_op_s {
-  std::unique_ptr<NufftPlan> plan;
+  std::unique_ptr<NufftPlan> plan;           // null when gridos != 2 (spatial interpolation only)
+  std::unique_ptr<InterpPlan> interp;        // spatial-interpolation tables (Gnufft.cpp:213-337)
   pg_status forward(const float2* x, float2* y, cudaStream_t s) override;
   pg_status adjoint(const float2* y, float2* x, cudaStream_t s) override;
   uint64_t resident_bytes() const override;

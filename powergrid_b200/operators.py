@@ -24,7 +24,8 @@ from . import _lib
 from ._lib import P, U64, Penalty, check
 
 __all__ = ["Gnufft", "Gdft", "TimeSegmentation", "SENSE", "pcSenseTimeSeg", "pcSENSE", "QuadPenalty", "TVPenalty",
-           "solve_pwls_pcg", "reconSolve", "init"]
+           "calc3DDensityCompensation", "gridCoilImages", "calcSumOfSquaresImage", "solve_pwls_pcg", "reconSolve",
+           "init"]
 
 
 def init(device: int = 0) -> None:
@@ -132,6 +133,31 @@ class Gnufft(_Op):
         check(_lib.load().pg_util_gnufft_binning(self._h, _ptr(keys), _ptr(perm), C.byref(nb)))
         return keys, perm, int(nb.value)
 
+    @property
+    def grid_length(self) -> int:
+        """Cells of the oversampled grid (Gnufft.cpp:56-61)."""
+        n = U64()
+        check(_lib.load().pg_gnufft_grid_length(self._h, C.byref(n)))
+        return int(n.value)
+
+    def forwardSpatialInterp(self, grid):
+        """Samples interpolated from an oversampled grid in the reference's layout (Gnufft.cpp:213-258)."""
+        g = _c64(grid)
+        if g.size != self.grid_length:
+            raise ValueError(f"grid has {g.size} cells, expected {self.grid_length}")
+        out = np.empty(self.n_data, np.complex64)
+        check(_lib.load().pg_gnufft_forward_spatial_interp(self._h, _ptr(g), _ptr(out)))
+        return out
+
+    def adjointSpatialInterp(self, data):
+        """Samples spread onto the oversampled grid, no FFT (Gnufft.cpp:261-330)."""
+        d = _c64(data)
+        if d.size != self.n_data:
+            raise ValueError(f"data has {d.size} samples, expected {self.n_data}")
+        out = np.empty(self.grid_length, np.complex64)
+        check(_lib.load().pg_gnufft_adjoint_spatial_interp(self._h, _ptr(d), _ptr(out)))
+        return out
+
 
 class Gdft(_Op):
     """Exact field-corrected DFT (Gdft.cpp:33-136); FM in rad/s, t in s."""
@@ -193,6 +219,39 @@ class pcSENSE(_Op):
         check(_lib.load().pg_pcsense_create(C.byref(h), _ptr(kx), _ptr(ky), _ptr(kz), kx.size, int(nx), int(ny),
                                              int(nz), int(nc), _ptr(t), _ptr(sm), _ptr(fm), _ptr(pm), pm.size))
         super().__init__(h)
+
+
+def calc3DDensityCompensation(kx, ky, kz, Ninplane, Nz):
+    """Sample density compensation (reconSupport/directRecon.cpp:28-61): two Pipe
+    iterations on a 3x oversampled grid, |dcf| normalised to unit L2 norm."""
+    kx, ky, kz = _f32(kx), _f32(ky), _f32(kz)
+    out = np.empty(kx.size, np.float32)
+    check(_lib.load().pg_density_compensation(_ptr(kx), _ptr(ky), _ptr(kz), kx.size, int(Ninplane), int(Nz),
+                                              _ptr(out)))
+    return out
+
+
+def gridCoilImages(G: Gnufft, dcf, data, Ncoils):
+    """Per-coil gridded images G / (dcf .* data_c) (directRecon.cpp:108-133), coil-major."""
+    w = _f32(dcf)
+    d = _c64(data)
+    nc = int(Ncoils)
+    if w.size != G.n_data or d.size != G.n_data * nc:
+        raise ValueError("dcf / data sizes do not match the operator")
+    out = np.empty(G.n_image * nc, np.complex64)
+    check(_lib.load().pg_grid_coil_images(G.handle, _ptr(w), _ptr(d), nc, _ptr(out)))
+    return out
+
+
+def calcSumOfSquaresImage(coilImages, Ncoils):
+    """sqrt(sum_c |img_c|) per voxel (directRecon.cpp:63-73; a sum of magnitudes, as the reference has it)."""
+    img = _c64(coilImages)
+    nc = int(Ncoils)
+    if img.size % nc:
+        raise ValueError("coil images not divisible by Ncoils")
+    out = np.empty(img.size // nc, np.float32)
+    check(_lib.load().pg_sum_of_squares_image(_ptr(img), img.size // nc, nc, _ptr(out)))
+    return out
 
 
 class QuadPenalty:

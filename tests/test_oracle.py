@@ -148,3 +148,48 @@ def test_oracle_pcg_float_vs_fp64(oracle):
     """The float reference path and the FP64 oracle agree on a 5-iteration solve."""
     c = _case(os.path.join(HERE, "golden", "pcg2d.npz"))
     assert rel_l2(c["x_pcg_f32"], c["x_pcg_f64"]) < 1e-4
+
+
+def _interp_case(dim):
+    from powergrid_b200 import synthetic as S
+    if dim == 2:
+        kx, ky, _ = S.spiral(24, 3, 200, 1e-3)
+        return 24, 1, kx, ky, np.zeros_like(kx)
+    kx, ky, kz, _ = S.stack_of_spirals(12, 6, 2, 40, 1e-3)
+    return 12, 6, kx, ky, kz
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(HERE), "oracle", "_ref", "libpgref.so")),
+                    reason="reference kernels are compiled only where the reference tree exists")
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("gridos", [2.0, 3.0])
+def test_restated_spatial_interp_matches_reference_kernels(oracle, dim, gridos):
+    """forward/adjointSpatialInterp restated == the reference's gridding_forward/adjoint, bit for bit."""
+    from powergrid_b200 import synthetic as S
+    n, nz, kx, ky, kz = _interp_case(dim)
+    outs = []
+    for use_ref in (False, True):
+        oracle.use_reference(use_ref)
+        G = oracle.gnufft(0, kx.size, n, n, nz, kx, ky, kz, gridos=gridos)
+        ng = oracle.lib().orc_gnufft_grid_len(G.h)
+        g = S.image(S.Rng(31), ng)
+        outs.append((oracle.forward_spatial_interp(G, g), oracle.adjoint_spatial_interp(G, S.image(S.Rng(32), kx.size))))
+    oracle.use_reference(False)
+    assert np.array_equal(outs[0][0], outs[1][0], equal_nan=True)
+    assert np.array_equal(outs[0][1], outs[1][1], equal_nan=True)
+
+
+def test_density_compensation_oracle_float_vs_fp64(oracle):
+    """2-D: the float restatement agrees with FP64 to the float path's own error; 3-D at
+    gridos 3 the float arithmetic of the reference overflows (weights up to 1.2e22 per tap)."""
+    from powergrid_b200 import synthetic as S
+    kx, ky, _ = S.spiral(32, 4, 512, 1e-3)
+    z = np.zeros_like(kx)
+    d32 = oracle.density_compensation(0, kx, ky, z, 32, 1)
+    d64 = oracle.density_compensation(1, kx, ky, z, 32, 1)
+    assert rel_l2(d32, d64) < 1e-4
+    assert abs(np.linalg.norm(d64) - 1.0) < 1e-12
+    kx, ky, kz, _ = S.stack_of_spirals(16, 8, 2, 128, 1e-3)
+    d32 = oracle.density_compensation(0, kx, ky, kz, 16, 8)
+    d64 = oracle.density_compensation(1, kx, ky, kz, 16, 8)
+    assert np.all(np.isfinite(d64)) and not np.all(np.isfinite(d32))
