@@ -453,6 +453,8 @@ def run_workload(name: str, steps: int, warmup: int):
           one adjoint; reports sample-voxel pairs/s per direction.
     cfg5: pcSenseTimeSeg 128x128x64, 16 shots x 131072 samples, 32 coils, L=12,
           TVPenalty; PCG iterations/s over one solve of `niter` iterations.
+    direct: spatial interpolation at gridos 3, density compensation and coil
+          images on the cfg2 and cfg3 trajectories.
     """
     import ctypes as C
 
@@ -548,6 +550,61 @@ def run_workload(name: str, steps: int, warmup: int):
                 "metric": METRIC, "unit": UNIT, "value": done / (sum(ms) / 1e3), "iterations": done,
                 "ms_per_solve": statistics.mean(ms), "steps": steps, "warmup": warmup,
                 "stage_ms_last_launch": stages, "clocks": sampler.summary()}
+    if name == "direct":
+        res = {"workload": "direct reconstruction pieces on the cfg2 (128x128, 131072 samples) and cfg3 "
+                           "(64x64x32, 131072 samples) trajectories: spatial interpolation on the 3x oversampled "
+                           "grid (device buffers, CUDA events), density compensation and 4-coil gridded images "
+                           "through the host-buffer API (wall clock, set-up included)",
+               "steps": steps, "warmup": warmup}
+        with sampler:
+            for tag, p in (("2d", S.config2()), ("3d", S.config3())):
+                M = p.kx.size
+                G3 = pg.Gnufft(M, 3.0, p.nx, p.ny, p.nz, p.kx, p.ky, p.kz)
+                ng = G3.grid_length
+                d = torch.ones(M, dtype=torch.complex64, device=dev)
+                grid = torch.empty(ng, dtype=torch.complex64, device=dev)
+                yv = torch.empty(M, dtype=torch.complex64, device=dev)
+                sp = C.c_void_p(stream.cuda_stream)
+                args_a = (G3.handle, C.c_void_p(d.data_ptr()), C.c_void_p(grid.data_ptr()), sp)
+                args_f = (G3.handle, C.c_void_p(grid.data_ptr()), C.c_void_p(yv.data_ptr()), sp)
+                torch.cuda.synchronize()
+                for _ in range(warmup):
+                    check(L.pg_gnufft_adjoint_spatial_interp_device(*args_a))
+                    check(L.pg_gnufft_forward_spatial_interp_device(*args_f))
+                stream.synchronize()
+                ta, tf = [], []
+                for _ in range(steps):
+                    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+                    e[0].record(stream)
+                    check(L.pg_gnufft_adjoint_spatial_interp_device(*args_a))
+                    e[1].record(stream)
+                    check(L.pg_gnufft_forward_spatial_interp_device(*args_f))
+                    e[2].record(stream)
+                    stream.synchronize()
+                    ta.append(e[0].elapsed_time(e[1]))
+                    tf.append(e[1].elapsed_time(e[2]))
+                del G3
+                t0 = time.perf_counter()
+                dcf = pg.calc3DDensityCompensation(p.kx, p.ky, p.kz, p.nx, p.nz)
+                t_dcf = time.perf_counter() - t0
+                G2 = pg.Gnufft(M, 2.0, p.nx, p.ny, p.nz, p.kx, p.ky, p.kz)
+                data = S.image(S.Rng(9), M * 4)
+                pg.gridCoilImages(G2, dcf, data, 4)  # warm (plans, workspaces)
+                t0 = time.perf_counter()
+                imgs = pg.gridCoilImages(G2, dcf, data, 4)
+                t_img = time.perf_counter() - t0
+                pg.calcSumOfSquaresImage(imgs, 4)
+                del G2
+                dim = 3 if p.nz > 1 else 2
+                a_ms, f_ms = statistics.mean(ta), statistics.mean(tf)
+                res[tag] = {"samples": M, "grid_cells_os3": ng,
+                            "adjoint_interp_ms": a_ms, "forward_interp_ms": f_ms,
+                            "adjoint_interp_samples_per_s": M / (a_ms / 1e3),
+                            "adjoint_interp_algorithmic_GBps": (M * (4 * dim + 8) + ng * 8) / (a_ms / 1e3) / 1e9,
+                            "density_compensation_host_call_s": t_dcf,
+                            "coil_images_4_host_call_s": t_img}
+        res["clocks"] = sampler.summary()
+        return res
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -560,7 +617,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the config-4 serving stream")
     ap.add_argument("--serving-only", action="store_true", help="only the config-4 serving stream")
-    ap.add_argument("--workload", default=None, choices=["cfg3", "cfg5"], help="a secondary workload instead")
+    ap.add_argument("--workload", default=None, choices=["cfg3", "cfg5", "direct"],
+                    help="a secondary workload instead")
     args = ap.parse_args()
     if args.workload:
         print(json.dumps(run_workload(args.workload, args.steps, max(3, args.warmup))))

@@ -7,15 +7,20 @@
 // oversampling is any factor up to 3.75 (16 taps per axis), so these kernels
 // take the window bounds per sample instead of the fixed 8 taps of the
 // operator path.
-//   forward: one warp per sample, lanes over the window's cells (y fastest,
-//            so a warp's loads walk grid columns), butterfly sum.
+//   forward: one warp per sample; the per-axis window weights are computed
+//            once (lane a: cell a of each axis) and shuffled; half-warps walk
+//            alternate (z, x) rows with lane & 15 on the y cell, so a half
+//            warp reads one grid column; butterfly sum.
 //   adjoint: gather form, no atomics.  Samples are sorted (device counting
 //            sort, stable) by the 16-cell tile holding their window's low
-//            corner; a block owns one output tile and reads the samples of
-//            the tiles whose windows can reach it (2 per axis, since a window
-//            spans at most 16 cells), staged in shared memory.  Each cell is
-//            written once, so the sum for a cell is in a fixed order and no
-//            zeroing pass is needed.
+//            corner; the samples that can reach an output tile are those of
+//            its own bin and the previous bin along each axis (a window spans
+//            at most 16 cells).  They are cut into work items of at most 512
+//            samples; a block takes one item, stages its samples in shared
+//            memory and sums them into the tile's cells in registers.  A
+//            tile's first item stores the cells (so no zeroing pass is
+//            needed), further items store partial tiles that a second kernel
+//            adds in item order: every cell's sum has a fixed order.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -32,6 +37,7 @@ namespace {
 constexpr int kTileI = 16;     // adjoint tile edge (cells)
 constexpr int kMaxTaps = 16;   // cells per axis in one window
 constexpr int kChunk = 128;    // samples staged per round
+constexpr uint32_t kItemSamples = 512;  // samples per adjoint work item
 
 __global__ void k_interp_forward(InterpGeom g, uint64_t M, const float* __restrict__ kx, const float* __restrict__ ky,
                                  const float* __restrict__ kz, const float* __restrict__ lut,
@@ -46,19 +52,32 @@ __global__ void k_interp_forward(InterpGeom g, uint64_t M, const float* __restri
   float sz = 0.f;
   if (g.dim == 3) sz = kb_window(kz[i], g.Nz, g.os, g.kw, &zl, &zh);
   const int nxT = max(0, xh - xl + 1), nyT = max(0, yh - yl + 1), nzT = max(0, zh - zl + 1);
-  const int total = nxT * nyT * nzT;
+  // lane a holds the weights of window cell a along each axis
+  const float wxl = lane < nxT ? kb_weight(sx, xl + lane, g.os, kw2, lut, g.nlut) : 0.f;
+  const float wyl = lane < nyT ? kb_weight(sy, yl + lane, g.os, kw2, lut, g.nlut) : 0.f;
+  const float wzl = (g.dim == 3 && lane < nzT) ? kb_weight(sz, zl + lane, g.os, kw2, lut, g.nlut) : 0.f;
+  // half-warps take alternate (z, x) rows; lane & 15 is the y cell
+  const int ly = lane & 15;
+  const float wy = __shfl_sync(0xffffffffu, wyl, ly);
+  const int rows = nxT * nzT;
+  int ix = lane >> 4, iz = 0;
+  while (nxT > 0 && ix >= nxT) { ix -= nxT; ++iz; }
   float ar = 0.f, ai = 0.f;
-  for (int t = lane; t < total; t += 32) {
-    const int r = t / nyT;
-    const int cy = yl + (t - r * nyT);
-    const int cz = zl + r / nxT;
-    const int cx = xl + (r - (r / nxT) * nxT);
-    // w = kbX * kbY (* kbZ) as gridding.cpp:63, 100
-    float w = __fmul_rn(kb_weight(sx, cx, g.os, kw2, lut, g.nlut), kb_weight(sy, cy, g.os, kw2, lut, g.nlut));
-    if (g.dim == 3) w = __fmul_rn(w, kb_weight(sz, cz, g.os, kw2, lut, g.nlut));
-    const float2 v = grid[(uint64_t)cy + (uint64_t)g.Gy * ((uint64_t)cx + (uint64_t)g.Gx * cz)];
-    ar = __fadd_rn(ar, __fmul_rn(w, v.x));
-    ai = __fadd_rn(ai, __fmul_rn(w, v.y));
+  for (int r0 = 0; r0 < rows; r0 += 2) {  // warp-uniform trip count
+    const bool row_ok = r0 + (lane >> 4) < rows;
+    const float wx = __shfl_sync(0xffffffffu, wxl, row_ok ? ix : 0);
+    const float wz = __shfl_sync(0xffffffffu, wzl, row_ok ? iz : 0);
+    if (row_ok && ly < nyT) {
+      // w = kbX * kbY (* kbZ) as gridding.cpp:63, 100
+      float w = __fmul_rn(wx, wy);
+      if (g.dim == 3) w = __fmul_rn(w, wz);
+      const float2 v =
+          grid[(uint64_t)(yl + ly) + (uint64_t)g.Gy * ((uint64_t)(xl + ix) + (uint64_t)g.Gx * (uint64_t)(zl + iz))];
+      ar = __fadd_rn(ar, __fmul_rn(w, v.x));
+      ai = __fadd_rn(ai, __fmul_rn(w, v.y));
+    }
+    ix += 2;
+    while (nxT > 0 && ix >= nxT) { ix -= nxT; ++iz; }
   }
 #pragma unroll
   for (int o = 16; o; o >>= 1) {
@@ -82,20 +101,28 @@ __global__ void k_interp_keys(InterpGeom g, uint64_t M, const float* __restrict_
   key[i] = (uint32_t)(((uint64_t)bz * nbx + bx) * nby + by);
 }
 
-// One block per output tile (16 x 16 cells, x 16 z-planes in 3-D: TZ).
+// One block per work item: a piece (at most kItemSamples samples, in one or
+// more sorted ranges) of the samples that reach one output tile (16 x 16
+// cells, x 16 z-planes in 3-D: TZ).  A tile's first item stores the grid
+// cells; its further items store partial tiles that k_interp_fixup adds in
+// item order.
 template <int TZ>
-__global__ void __launch_bounds__(256) k_interp_adjoint(InterpGeom g, uint64_t M, const float* __restrict__ kx,
+__global__ void __launch_bounds__(256) k_interp_adjoint(InterpGeom g, const float* __restrict__ kx,
                                                         const float* __restrict__ ky, const float* __restrict__ kz,
                                                         const float* __restrict__ lut, const float2* __restrict__ d,
                                                         const uint32_t* __restrict__ perm,
-                                                        const uint32_t* __restrict__ starts, int nbx, int nby,
-                                                        int nbz, float2* __restrict__ grid) {
+                                                        const int4* __restrict__ items, const uint2* __restrict__ segs,
+                                                        int nbx, int nby, float2* __restrict__ grid,
+                                                        float2* __restrict__ partial) {
   // weights [axis][sample][tap], tap stride 17: a warp's 16 y-cells read 16 banks
   __shared__ float s_w[3][kChunk][kMaxTaps + 1];
   __shared__ int s_lo[3][kChunk];
   __shared__ int s_n[3][kChunk];
   __shared__ float2 s_v[kChunk];
-  const int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
+  const int4 it = items[blockIdx.x];   // (tile, first segment, segments, partial slot or -1)
+  const int by = it.x % nby;
+  const int bx = (it.x / nby) % nbx;
+  const int bz = it.x / (nby * nbx);
   const int gy = by * kTileI + (threadIdx.x & 15);
   const int gx = bx * kTileI + (threadIdx.x >> 4);
   const int gz0 = bz * TZ;
@@ -103,65 +130,89 @@ __global__ void __launch_bounds__(256) k_interp_adjoint(InterpGeom g, uint64_t M
   float2 acc[TZ];
 #pragma unroll
   for (int z = 0; z < TZ; ++z) acc[z] = make_float2(0.f, 0.f);
-  const uint64_t nkeys = (uint64_t)nbx * nby * nbz;
-  for (int dzb = (TZ > 1 ? -1 : 0); dzb <= 0; ++dzb)
-    for (int dxb = -1; dxb <= 0; ++dxb)
-      for (int dyb = -1; dyb <= 0; ++dyb) {
-        const int kbx = bx + dxb, kby = by + dyb, kbz = bz + dzb;
-        if (kbx < 0 || kby < 0 || kbz < 0) continue;  // block-uniform
-        const uint64_t key = ((uint64_t)kbz * nbx + kbx) * nby + kby;
-        const uint32_t b0 = starts[key];
-        const uint32_t b1 = (key + 1 < nkeys) ? starts[key + 1] : (uint32_t)M;
-        for (uint32_t c0 = b0; c0 < b1; c0 += kChunk) {
-          const int cn = (int)min((uint32_t)kChunk, b1 - c0);
-          __syncthreads();  // the previous round is consumed
-          if ((int)threadIdx.x < cn) {
-            const int q = threadIdx.x;
-            const uint32_t j = perm[c0 + q];
-            const float kk[3] = {kx[j], ky[j], g.dim == 3 ? kz[j] : 0.f};
-            const int nn[3] = {g.Nx, g.Ny, g.Nz};
-            for (int a = 0; a < (g.dim == 3 ? 3 : 2); ++a) {
-              int lo, hi;
-              const float sa = kb_window(kk[a], nn[a], g.os, g.kw, &lo, &hi);
-              const int n = max(0, hi - lo + 1);
-              s_lo[a][q] = lo;
-              s_n[a][q] = n;
-              for (int t = 0; t < n; ++t) s_w[a][q][t] = kb_weight(sa, lo + t, g.os, kw2, lut, g.nlut);
-            }
-            s_v[q] = d[j];
-          }
-          __syncthreads();
-          for (int q = 0; q < cn; ++q) {
-            const unsigned dx = (unsigned)(gx - s_lo[0][q]);
-            const unsigned dy = (unsigned)(gy - s_lo[1][q]);
-            if (dx < (unsigned)s_n[0][q] && dy < (unsigned)s_n[1][q]) {
-              const float wxy = __fmul_rn(s_w[0][q][dx], s_w[1][q][dy]);
-              const float2 v = s_v[q];
-              if (TZ == 1) {
-                acc[0].x = __fadd_rn(acc[0].x, __fmul_rn(wxy, v.x));
-                acc[0].y = __fadd_rn(acc[0].y, __fmul_rn(wxy, v.y));
-              } else {
-                const int lz = s_lo[2][q];
-                const unsigned nz = (unsigned)s_n[2][q];
+  for (int sg = 0; sg < it.z; ++sg) {
+    const uint2 seg = segs[it.y + sg];
+    for (uint32_t c0 = seg.x; c0 < seg.y; c0 += kChunk) {
+      const int cn = (int)min((uint32_t)kChunk, seg.y - c0);
+      __syncthreads();  // the previous round is consumed
+      if ((int)threadIdx.x < cn) {
+        const int q = threadIdx.x;
+        const uint32_t j = perm[c0 + q];
+        const float kk[3] = {kx[j], ky[j], g.dim == 3 ? kz[j] : 0.f};
+        const int nn[3] = {g.Nx, g.Ny, g.Nz};
+        for (int a = 0; a < (g.dim == 3 ? 3 : 2); ++a) {
+          int lo, hi;
+          const float sa = kb_window(kk[a], nn[a], g.os, g.kw, &lo, &hi);
+          const int n = max(0, hi - lo + 1);
+          s_lo[a][q] = lo;
+          s_n[a][q] = n;
+          for (int t = 0; t < n; ++t) s_w[a][q][t] = kb_weight(sa, lo + t, g.os, kw2, lut, g.nlut);
+        }
+        s_v[q] = d[j];
+      }
+      __syncthreads();
+      for (int q = 0; q < cn; ++q) {
+        const unsigned dx = (unsigned)(gx - s_lo[0][q]);
+        const unsigned dy = (unsigned)(gy - s_lo[1][q]);
+        if (dx < (unsigned)s_n[0][q] && dy < (unsigned)s_n[1][q]) {
+          const float wxy = __fmul_rn(s_w[0][q][dx], s_w[1][q][dy]);
+          const float2 v = s_v[q];
+          if (TZ == 1) {
+            acc[0].x = __fadd_rn(acc[0].x, __fmul_rn(wxy, v.x));
+            acc[0].y = __fadd_rn(acc[0].y, __fmul_rn(wxy, v.y));
+          } else {
+            const int lz = s_lo[2][q];
+            const unsigned nz = (unsigned)s_n[2][q];
 #pragma unroll
-                for (int z = 0; z < TZ; ++z) {
-                  const unsigned dz = (unsigned)(gz0 + z - lz);
-                  if (dz < nz) {
-                    const float w = __fmul_rn(wxy, s_w[2][q][dz]);
-                    acc[z].x = __fadd_rn(acc[z].x, __fmul_rn(w, v.x));
-                    acc[z].y = __fadd_rn(acc[z].y, __fmul_rn(w, v.y));
-                  }
-                }
+            for (int z = 0; z < TZ; ++z) {
+              const unsigned dz = (unsigned)(gz0 + z - lz);
+              if (dz < nz) {
+                const float w = __fmul_rn(wxy, s_w[2][q][dz]);
+                acc[z].x = __fadd_rn(acc[z].x, __fmul_rn(w, v.x));
+                acc[z].y = __fadd_rn(acc[z].y, __fmul_rn(w, v.y));
               }
             }
           }
         }
       }
+    }
+  }
+  if (it.w >= 0) {
+    float2* dst = partial + (uint64_t)it.w * (256 * TZ);
+#pragma unroll
+    for (int z = 0; z < TZ; ++z) dst[z * 256 + threadIdx.x] = acc[z];
+    return;
+  }
   if (gx >= g.Gx || gy >= g.Gy) return;
 #pragma unroll
   for (int z = 0; z < TZ; ++z) {
     const int gz = gz0 + z;
     if (gz < g.Gz) grid[(uint64_t)gy + (uint64_t)g.Gy * ((uint64_t)gx + (uint64_t)g.Gx * gz)] = acc[z];
+  }
+}
+
+// grid cell += the tile's partials in item order.  fix = (tile, first slot, slots).
+template <int TZ>
+__global__ void __launch_bounds__(256) k_interp_fixup(InterpGeom g, const int4* __restrict__ fix, int nbx, int nby,
+                                                      const float2* __restrict__ partial, float2* __restrict__ grid) {
+  const int4 f = fix[blockIdx.x];
+  const int by = f.x % nby;
+  const int bx = (f.x / nby) % nbx;
+  const int bz = f.x / (nby * nbx);
+  const int gy = by * kTileI + (threadIdx.x & 15);
+  const int gx = bx * kTileI + (threadIdx.x >> 4);
+  if (gx >= g.Gx || gy >= g.Gy) return;
+  for (int z = 0; z < TZ; ++z) {
+    const int gz = bz * TZ + z;
+    if (gz >= g.Gz) break;
+    const uint64_t cell = (uint64_t)gy + (uint64_t)g.Gy * ((uint64_t)gx + (uint64_t)g.Gx * gz);
+    float2 v = grid[cell];
+    for (int k = 0; k < f.z; ++k) {
+      const float2 q = partial[(uint64_t)(f.y + k) * (256 * TZ) + z * 256 + threadIdx.x];
+      v.x = __fadd_rn(v.x, q.x);
+      v.y = __fadd_rn(v.y, q.y);
+    }
+    grid[cell] = v;
   }
 }
 
@@ -256,7 +307,55 @@ static pg_status interp_plan_build(InterpPlan* p, cudaStream_t s) {
   PG_LAUNCH(k_interp_keys, ceil_div(p->M, 256), 256, 0, s, g, p->M, p->kx.p, p->ky.p, p->kz.p, p->nbx, p->nby,
             p->nbz, keys.p);
   PG_TRY(bin_sort(keys.p, p->M, nkeys, p->perm.p, p->starts.p, s));
+  std::vector<uint32_t> st(nkeys);
+  PG_CUDA(cudaMemcpyAsync(st.data(), p->starts.p, nkeys * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   PG_CUDA(cudaStreamSynchronize(s));  // keys is released on return
+  // Work items: per output tile the sorted ranges of the bins that reach it
+  // (the tile's own and the previous one along each axis), cut into pieces
+  // of at most kItemSamples samples so that dense k-space centres do not
+  // serialise in one block.
+  std::vector<int4> items, fix;
+  std::vector<uint2> segs;
+  int slots = 0;
+  for (int bz = 0; bz < p->nbz; ++bz)
+    for (int bx = 0; bx < p->nbx; ++bx)
+      for (int by = 0; by < p->nby; ++by) {
+        const int tile = (bz * p->nbx + bx) * p->nby + by;
+        const int first_item = (int)items.size();
+        int4 cur = make_int4(tile, (int)segs.size(), 0, -1);
+        uint32_t fill = 0;
+        for (int dzb = (g.dim == 3 ? -1 : 0); dzb <= 0; ++dzb)
+          for (int dxb = -1; dxb <= 0; ++dxb)
+            for (int dyb = -1; dyb <= 0; ++dyb) {
+              const int kbx = bx + dxb, kby = by + dyb, kbz = bz + dzb;
+              if (kbx < 0 || kby < 0 || kbz < 0) continue;
+              const uint64_t key = ((uint64_t)kbz * p->nbx + kbx) * p->nby + kby;
+              uint32_t b0 = st[key];
+              const uint32_t b1 = (key + 1 < nkeys) ? st[key + 1] : (uint32_t)p->M;
+              while (b0 < b1) {
+                if (fill == kItemSamples) {  // close the item, open the next (a partial slot)
+                  items.push_back(cur);
+                  cur = make_int4(tile, (int)segs.size(), 0, slots++);
+                  fill = 0;
+                }
+                const uint32_t take = std::min(b1 - b0, kItemSamples - fill);
+                segs.push_back(make_uint2(b0, b0 + take));
+                cur.z += 1;
+                fill += take;
+                b0 += take;
+              }
+            }
+        items.push_back(cur);
+        const int extra = (int)items.size() - first_item - 1;
+        if (extra > 0) fix.push_back(make_int4(tile, items[first_item + 1].w, extra, 0));
+      }
+  p->nitems = (int)items.size();
+  p->nfix = (int)fix.size();
+  p->nslots = slots;
+  PG_TRY(p->items.upload(items.data(), items.size(), s));
+  PG_TRY(p->segs.upload(segs.data(), std::max<size_t>(1, segs.size()), s));
+  if (!fix.empty()) PG_TRY(p->fix.upload(fix.data(), fix.size(), s));
+  PG_CUDA(cudaStreamSynchronize(s));
   return PG_OK;
 }
 
@@ -337,13 +436,21 @@ pg_status interp_forward(const InterpPlan* p, const float2* grid, float2* y, cud
 }
 
 pg_status interp_adjoint(const InterpPlan* p, const float2* d, float2* grid, cudaStream_t s) {
-  const dim3 blocks(p->nbx, p->nby, p->nbz);
-  if (p->g.dim == 3)
-    PG_LAUNCH(k_interp_adjoint<kTileI>, blocks, 256, 0, s, p->g, p->M, p->kx.p, p->ky.p, p->kz.p, p->lut.p, d,
-              p->perm.p, p->starts.p, p->nbx, p->nby, p->nbz, grid);
-  else
-    PG_LAUNCH(k_interp_adjoint<1>, blocks, 256, 0, s, p->g, p->M, p->kx.p, p->ky.p, p->kz.p, p->lut.p, d, p->perm.p,
-              p->starts.p, p->nbx, p->nby, p->nbz, grid);
+  const int tz = p->g.dim == 3 ? kTileI : 1;
+  float2* partial = nullptr;
+  if (p->nslots > 0) {
+    PG_TRY(grow(const_cast<InterpPlan*>(p)->partial, (uint64_t)p->nslots * 256 * tz, s));
+    partial = p->partial.p;
+  }
+  if (p->g.dim == 3) {
+    PG_LAUNCH(k_interp_adjoint<kTileI>, p->nitems, 256, 0, s, p->g, p->kx.p, p->ky.p, p->kz.p, p->lut.p, d, p->perm.p,
+              p->items.p, p->segs.p, p->nbx, p->nby, grid, partial);
+    if (p->nfix) PG_LAUNCH(k_interp_fixup<kTileI>, p->nfix, 256, 0, s, p->g, p->fix.p, p->nbx, p->nby, partial, grid);
+  } else {
+    PG_LAUNCH(k_interp_adjoint<1>, p->nitems, 256, 0, s, p->g, p->kx.p, p->ky.p, p->kz.p, p->lut.p, d, p->perm.p,
+              p->items.p, p->segs.p, p->nbx, p->nby, grid, partial);
+    if (p->nfix) PG_LAUNCH(k_interp_fixup<1>, p->nfix, 256, 0, s, p->g, p->fix.p, p->nbx, p->nby, partial, grid);
+  }
   return PG_OK;
 }
 

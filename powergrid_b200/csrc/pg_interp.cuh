@@ -30,6 +30,13 @@ struct InterpPlan {
   int nbx = 1, nby = 1, nbz = 1;   // 16-cell tiles per axis
   DevBuf<uint32_t> perm;       // samples sorted by the tile of their window's low corner
   DevBuf<uint32_t> starts;     // first sorted position per tile
+  // adjoint work items (tile, first range, ranges, partial slot or -1), their
+  // sorted-sample ranges, and per tile with several items (tile, first slot, slots)
+  DevBuf<int4> items;
+  DevBuf<uint2> segs;
+  DevBuf<int4> fix;
+  int nitems = 0, nfix = 0, nslots = 0;
+  DevBuf<float2> partial;      // partial tiles of the further items
   DevBuf<float2> tmp;          // density compensation: samples
   DevBuf<float2> grid;         // density compensation: grid
 };
