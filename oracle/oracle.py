@@ -45,7 +45,7 @@ def lib() -> C.CDLL:
         L.orc_gdft_new.restype = P
         L.orc_gdft_new.argtypes = [C.c_int, U64, U64] + [P] * 8
         L.orc_timeseg_new.restype = P
-        L.orc_timeseg_new.argtypes = [P, P, P, U64, U64, U64, U64, U64]
+        L.orc_timeseg_new.argtypes = [P, P, P, U64, U64, U64, U64, U64, C.c_int]
         L.orc_sense_new.restype = P
         L.orc_sense_new.argtypes = [P, P, U64, U64, U64]
         L.orc_pcsense_ts_new.restype = P
@@ -178,9 +178,12 @@ def gdft(prec, kx, ky, kz, ix, iy, iz, fm, t) -> Op:
     return Op(lib().orc_gdft_new(prec, a[0].size, a[3].size, *[_p(v) for v in a]), prec)
 
 
-def timeseg(G: Op, fm, t, n1, n2, L, interptype=1, shots=1) -> Op:
+def timeseg(G: Op, fm, t, n1, n2, L, interptype=1, shots=1, tables64=False) -> Op:
+    """TimeSegmentation over G; tables64 builds the min-max / histogram table in
+    double and rounds it (float G only)."""
     fm, t = _f32(fm), _f32(t)
-    return Op(lib().orc_timeseg_new(G.h, _p(fm), _p(t), n1, n2, L, interptype, shots), G.prec, keep=[G])
+    return Op(lib().orc_timeseg_new(G.h, _p(fm), _p(t), n1, n2, L, interptype, shots, int(tables64)), G.prec,
+              keep=[G])
 
 
 def sense(G: Op, smap, n1, n2, nc) -> Op:

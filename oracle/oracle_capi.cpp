@@ -234,14 +234,15 @@ void* orc_gdft_new(int prec, u64 nk, u64 ni, const float* kx, const float* ky, c
   });
 }
 
+// tables64: min-max / histogram tables built in double and rounded (float handles only)
 void* orc_timeseg_new(void* G, const float* fieldmap, const float* tvec, u64 n1, u64 n2, u64 L, u64 type,
-                      u64 shots) {
+                      u64 shots, int tables64) {
   return guard([&]() -> void* {
     Handle* g = (Handle*)G;
     auto* h = new Handle;
     h->prec = g->prec;
     if (g->prec == 0) {
-      h->f.reset(new pgo::TimeSegOp<float>(g->f.get(), fieldmap, tvec, n1, n2, L, type, shots));
+      h->f.reset(new pgo::TimeSegOp<float>(g->f.get(), fieldmap, tvec, n1, n2, L, type, shots, tables64 != 0));
     } else {
       auto fm = widen<double>(fieldmap, n2), tv = widen<double>(tvec, n1);
       h->d.reset(new pgo::TimeSegOp<double>(g->d.get(), fm.data(), tv.data(), n1, n2, L, type, shots));

@@ -623,6 +623,241 @@ inline u64 op_image_len(const Op<T>& op) {
   return op.n2;
 }
 
+// ---------------------------------------------------------------------------
+// Dense complex algebra in the operator's precision for the min-max
+// interpolators (Armadillo inv / pinv / cond / rcond over LAPACK in the
+// reference; restated: Gauss-Jordan with partial pivoting, one-sided Jacobi
+// SVD, pseudo-inverse with Armadillo's default tolerance n * max(s) * eps,
+// and the 1-norm reciprocal condition number that LAPACK's gecon estimates).
+// ---------------------------------------------------------------------------
+template <typename T>
+using CM = std::vector<std::complex<T>>;  // n x n row-major
+
+template <typename T>
+bool la_inverse(CM<T> A, int n, CM<T>* out) {
+  using C = std::complex<T>;
+  CM<T> I((size_t)n * n, C(0, 0));
+  for (int i = 0; i < n; ++i) I[(size_t)i * n + i] = C(1, 0);
+  for (int c = 0; c < n; ++c) {
+    int p = c;
+    for (int r = c + 1; r < n; ++r)
+      if (std::abs(A[(size_t)r * n + c]) > std::abs(A[(size_t)p * n + c])) p = r;
+    if (A[(size_t)p * n + c] == C(0, 0)) return false;
+    if (p != c)
+      for (int k = 0; k < n; ++k) {
+        std::swap(A[(size_t)p * n + k], A[(size_t)c * n + k]);
+        std::swap(I[(size_t)p * n + k], I[(size_t)c * n + k]);
+      }
+    const C inv = C(1, 0) / A[(size_t)c * n + c];
+    for (int k = 0; k < n; ++k) {
+      A[(size_t)c * n + k] *= inv;
+      I[(size_t)c * n + k] *= inv;
+    }
+    for (int r = 0; r < n; ++r) {
+      if (r == c) continue;
+      const C f = A[(size_t)r * n + c];
+      if (f == C(0, 0)) continue;
+      for (int k = 0; k < n; ++k) {
+        A[(size_t)r * n + k] -= f * A[(size_t)c * n + k];
+        I[(size_t)r * n + k] -= f * I[(size_t)c * n + k];
+      }
+    }
+  }
+  *out = I;
+  return true;
+}
+
+// A = U diag(s) V^H by one-sided (Hestenes) Jacobi rotations.
+template <typename T>
+void la_svd(const CM<T>& A, int n, std::vector<T>* s, CM<T>* U, CM<T>* V) {
+  using C = std::complex<T>;
+  CM<T> W = A, Vm((size_t)n * n, C(0, 0));
+  for (int i = 0; i < n; ++i) Vm[(size_t)i * n + i] = C(1, 0);
+  const T tol = std::numeric_limits<T>::epsilon();
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    T off = 0;
+    for (int p = 0; p < n - 1; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        T app = 0, aqq = 0;
+        C apq(0, 0);
+        for (int i = 0; i < n; ++i) {
+          app += std::norm(W[(size_t)i * n + p]);
+          aqq += std::norm(W[(size_t)i * n + q]);
+          apq += std::conj(W[(size_t)i * n + p]) * W[(size_t)i * n + q];
+        }
+        const T mag = std::abs(apq);
+        if (mag == (T)0 || mag <= tol * std::sqrt(app * aqq)) continue;
+        off = std::max(off, mag / std::sqrt(app * aqq));
+        const C ph = apq / mag;
+        const T zeta = (aqq - app) / ((T)2 * mag);
+        const T t = (zeta >= 0 ? (T)1 : (T)-1) / (std::abs(zeta) + std::sqrt((T)1 + zeta * zeta));
+        const T c = (T)1 / std::sqrt((T)1 + t * t), sn = c * t;
+        for (int i = 0; i < n; ++i) {
+          const C wp = W[(size_t)i * n + p], wq = W[(size_t)i * n + q];
+          W[(size_t)i * n + p] = c * wp - sn * std::conj(ph) * wq;
+          W[(size_t)i * n + q] = sn * ph * wp + c * wq;
+          const C vp = Vm[(size_t)i * n + p], vq = Vm[(size_t)i * n + q];
+          Vm[(size_t)i * n + p] = c * vp - sn * std::conj(ph) * vq;
+          Vm[(size_t)i * n + q] = sn * ph * vp + c * vq;
+        }
+      }
+    if (off < tol) break;
+  }
+  s->assign(n, (T)0);
+  CM<T> Um((size_t)n * n, C(0, 0));
+  for (int j = 0; j < n; ++j) {
+    T nr = 0;
+    for (int i = 0; i < n; ++i) nr += std::norm(W[(size_t)i * n + j]);
+    nr = std::sqrt(nr);
+    (*s)[j] = nr;
+    for (int i = 0; i < n; ++i) Um[(size_t)i * n + j] = nr > 0 ? W[(size_t)i * n + j] / nr : C(0, 0);
+  }
+  *U = Um;
+  *V = Vm;
+}
+
+template <typename T>
+CM<T> la_pinv(const CM<T>& A, int n) {
+  std::vector<T> s;
+  CM<T> U, V;
+  la_svd(A, n, &s, &U, &V);
+  const T smax = *std::max_element(s.begin(), s.end());
+  const T tol = (T)n * smax * std::numeric_limits<T>::epsilon();
+  CM<T> P((size_t)n * n, std::complex<T>(0, 0));
+  for (int k = 0; k < n; ++k) {
+    if (s[k] <= tol) continue;
+    for (int r = 0; r < n; ++r)
+      for (int c = 0; c < n; ++c)
+        P[(size_t)r * n + c] += V[(size_t)r * n + k] * ((T)1 / s[k]) * std::conj(U[(size_t)c * n + k]);
+  }
+  return P;
+}
+
+template <typename T>
+T la_cond(const CM<T>& A, int n) {
+  std::vector<T> s;
+  CM<T> U, V;
+  la_svd(A, n, &s, &U, &V);
+  const T smin = *std::min_element(s.begin(), s.end());
+  return smin > 0 ? *std::max_element(s.begin(), s.end()) / smin : std::numeric_limits<T>::infinity();
+}
+
+template <typename T>
+T la_norm1(const CM<T>& A, int n) {
+  T m = 0;
+  for (int c = 0; c < n; ++c) {
+    T sum = 0;
+    for (int r = 0; r < n; ++r) sum += std::abs(A[(size_t)r * n + c]);
+    m = std::max(m, sum);
+  }
+  return m;
+}
+
+// Min-max interpolator (TimeSegmentation.cpp:94-156) for one shot: AA(m, l),
+// m < none, l < L, column-major like tempAA.
+template <typename T>
+std::vector<std::complex<T>> aa_minmax(const T* fm, u64 n2, const std::vector<T>& tv, u64 none, int L, T tau) {
+  using C = std::complex<T>;
+  const C I(0, 1);
+  std::vector<C> gl(n2 * L);                                 // gl(j, ii) = gg_j^(ii+1)
+  for (u64 j = 0; j < n2; ++j) {
+    const C gg = std::exp(I * fm[j] * tau);
+    for (int ii = 0; ii < L; ++ii) gl[j + n2 * ii] = std::pow(gg, (T)(ii + 1));
+  }
+  std::vector<C> glsum(L, C(0, 0));                          // sum(gl.t(), 1)
+  for (int ii = 0; ii < L; ++ii)
+    for (u64 j = 0; j < n2; ++j) glsum[ii] += std::conj(gl[j + n2 * ii]);
+  CM<T> GTG((size_t)L * L, C(0, 0));
+  for (int d = 0; d < L; ++d) GTG[(size_t)d * L + d] += (T)n2;
+  for (int ii = 0; ii < L - 1; ++ii)
+    for (int d = 0; d + ii + 1 < L; ++d) {
+      GTG[(size_t)(d + ii + 1) * L + d] += glsum[ii];        // diag(-(ii+1))
+      GTG[(size_t)d * L + (d + ii + 1)] += std::conj(glsum[ii]);
+    }
+  const T rcn = (T)1 / la_cond(GTG, L);
+  CM<T> B;
+  if (!(rcn > (T)(10 * 2e-16) && la_inverse(GTG, L, &B))) B = la_pinv(GTG, L);
+  // iGTGGT = B * G^H, G columns: ones, then gl(:, 0 .. L-2)
+  std::vector<C> P((size_t)L * n2, C(0, 0));
+  for (int l = 0; l < L; ++l)
+    for (u64 j = 0; j < n2; ++j) {
+      C acc(0, 0);
+      for (int k = 0; k < L; ++k) acc += B[(size_t)l * L + k] * std::conj(k == 0 ? C(1, 0) : gl[j + n2 * (k - 1)]);
+      P[(size_t)l * n2 + j] = acc;
+    }
+  std::vector<C> AA(none * L), res(L);
+  for (u64 m = 0; m < none; ++m) {                           // res = iGTGGT * exp(i fm t_m) (:140-145)
+    std::fill(res.begin(), res.end(), C(0, 0));
+    for (u64 j = 0; j < n2; ++j) {
+      const C f = std::exp(I * fm[j] * tv[m]);
+      for (int l = 0; l < L; ++l) res[l] += P[(size_t)l * n2 + j] * f;
+    }
+    for (int l = 0; l < L; ++l) AA[m + none * l] = std::conj(res[l]);
+  }
+  return AA;
+}
+
+// Histogram interpolator (TimeSegmentation.cpp:157-211) for one shot; the
+// first L of its L+1 columns.  hist(X, 256) restates Armadillo 9.200's: bin
+// centres min + (max - min) * (b + 0.5) / 256, nearest centre, ties low.
+template <typename T>
+std::vector<std::complex<T>> aa_histogram(const T* fm, u64 n2, const std::vector<T>& tv, u64 none, int L, T tau) {
+  using C = std::complex<T>;
+  const C I(0, 1);
+  const int nbins = 256;
+  T mn = fm[0], mx = fm[0];
+  for (u64 j = 0; j < n2; ++j) { mn = std::min(mn, fm[j]); mx = std::max(mx, fm[j]); }
+  std::vector<T> ctr(nbins);
+  for (int b = 0; b < nbins; ++b) ctr[b] = (T)((0.5 + b) / (double)nbins);
+  for (int b = 0; b < nbins; ++b) ctr[b] = (mx - mn) * ctr[b] + mn;
+  std::vector<T> h(nbins, (T)0);
+  for (u64 j = 0; j < n2; ++j) {
+    int best = 0;
+    T bd = std::abs(fm[j] - ctr[0]);
+    for (int b = 1; b < nbins; ++b) {
+      const T d = std::abs(fm[j] - ctr[b]);
+      if (d < bd) { bd = d; best = b; } else { break; }
+    }
+    h[best] += (T)1;
+  }
+  const T rangeFM = mx - mn;
+  const int KK = (int)std::floor(2.0 * kPiD / ((rangeFM / (T)nbins) * tau));
+  if (KK < 2 * L + 1) throw std::runtime_error("oracle: histogram interpolator needs KK >= 2L+1");
+  const T dwn = 2 * kPiD / (KK * tau);
+  auto fft_k = [&](const std::vector<C>& in) {               // calcFFT1D(in, KK) (:225-242)
+    std::vector<C> d(KK, C(0, 0));
+    for (int b = 0; b < std::min(nbins, KK); ++b) d[b] = in[b];
+    const std::size_t dims[1] = {(std::size_t)KK};
+    fft_nd<T>(d.data(), dims, 1, -1);
+    return d;
+  };
+  std::vector<C> temp(nbins);
+  for (int b = 0; b < nbins; ++b) temp[b] = h[b] * std::exp(I * dwn * (T)b * tau * (T)L);
+  std::vector<C> ftwe = fft_k(temp);
+  for (int k = 0; k < KK; ++k) ftwe[k] = std::exp(-I * (mn + dwn / 2) * tau * ((T)k - (T)L)) * ftwe[k];
+  const int n = L + 1;
+  CM<T> At((size_t)n * n);                                   // GTGap_ap.st()
+  for (int r = 0; r < n; ++r)
+    for (int c = 0; c < n; ++c) At[(size_t)r * n + c] = ftwe[L + r - c];
+  CM<T> B;
+  bool use_inv = la_inverse(At, n, &B);
+  if (use_inv) use_inv = (T)1 / (la_norm1(At, n) * la_norm1(B, n)) > (T)(10 * std::numeric_limits<double>::epsilon());
+  if (!use_inv) B = la_pinv(At, n);
+  std::vector<C> AA(none * L);
+  for (u64 m = 0; m < none; ++m) {
+    for (int b = 0; b < nbins; ++b) temp[b] = h[b] * std::exp(I * (T)b * dwn * tv[m]);
+    std::vector<C> ftc = fft_k(temp);
+    for (int k = 0; k < n; ++k) ftc[k] = std::exp(I * (mn + dwn / 2) * (tv[m] - tau * (T)k)) * ftc[k];
+    for (int l = 0; l < L; ++l) {
+      C r(0, 0);
+      for (int k = 0; k < n; ++k) r += B[(size_t)l * n + k] * ftc[k];
+      AA[m + none * l] = std::conj(r);
+    }
+  }
+  return AA;
+}
+
+
 // TimeSegmentation with the Hanning interpolator (TimeSegmentation.cpp:37-93,
 // 213-218) and its operators (:252-324).  Holds a non-owning pointer to G,
 // like the reference (TimeSegmentation.cpp:53).
@@ -637,11 +872,12 @@ struct TimeSegOp : Op<T> {
   std::vector<C> Wo;   // n2 x (L+1)
   std::vector<C> WoH;
 
-  TimeSegOp(const Op<T>* g, const T* fieldmap, const T* tvec, u64 a, u64 b, u64 nsegs, u64 interptype, u64 shots)
+  TimeSegOp(const Op<T>* g, const T* fieldmap, const T* tvec, u64 a, u64 b, u64 nsegs, u64 interptype, u64 shots,
+            bool tables64 = false)
       : G(g) {
     this->n1 = a; this->n2 = b;
     L = (nsegs == 0 || nsegs == 1) ? 1 : (int)nsegs;
-    if (interptype != 1 && L > 1) throw std::runtime_error("oracle: only the Hanning interpolator (type 1) is restated");
+    if (L > 1 && (interptype < 1 || interptype > 3)) throw std::runtime_error("oracle: interptype 1, 2 or 3");
     nshots = shots;
     std::vector<T> tv(tvec, tvec + a);
     T mn = *std::min_element(tv.begin(), tv.end());
@@ -658,13 +894,26 @@ struct TimeSegOp : Op<T> {
       WoH.assign(b, C(1, 0));
     } else {
       std::vector<C> one(none * L);
-      for (unsigned int l = 0; l < (unsigned)L; ++l)
-        for (unsigned int m = 0; m < none; ++m) {
-          if ((std::abs(tv[m] - ((l) * tau))) <= tau)
-            one[m + none * l] = C(0.5 + 0.5 * std::cos((kPiD) * (tv[m] - ((l) * tau)) / tau), 0);
-          else
-            one[m + none * l] = C(0, 0);
-        }
+      if (interptype == 1) {
+        for (unsigned int l = 0; l < (unsigned)L; ++l)
+          for (unsigned int m = 0; m < none; ++m) {
+            if ((std::abs(tv[m] - ((l) * tau))) <= tau)
+              one[m + none * l] = C(0.5 + 0.5 * std::cos((kPiD) * (tv[m] - ((l) * tau)) / tau), 0);
+            else
+              one[m + none * l] = C(0, 0);
+          }
+      } else if (tables64) {
+        // the table built in double and rounded to T: the float gridding of
+        // the reference with the interpolator of the FP64 path
+        std::vector<double> fm64(fieldmap, fieldmap + b), tv64(tv.begin(), tv.end());
+        const auto d = interptype == 2 ? aa_minmax<double>(fm64.data(), b, tv64, none, L, (double)tau)
+                                       : aa_histogram<double>(fm64.data(), b, tv64, none, L, (double)tau);
+        for (u64 q = 0; q < d.size(); ++q) one[q] = C((T)d[q].real(), (T)d[q].imag());
+      } else if (interptype == 2) {
+        one = aa_minmax<T>(fieldmap, b, tv, none, L, tau);
+      } else {
+        one = aa_histogram<T>(fieldmap, b, tv, none, L, tau);
+      }
       AA.resize(a * L);
       for (int l = 0; l < L; ++l)
         for (u64 m = 0; m < a; ++m) AA[m + a * l] = one[(m % none) + none * l];

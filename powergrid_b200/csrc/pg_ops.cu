@@ -46,8 +46,8 @@ pg_status build_ts_tables(const float* field_map, const float* tvec, uint64_t n1
   // TimeSegmentation.cpp:46-50: L in {0,1} means no segmentation.
   int L = (Lin == 0 || Lin == 1) ? 1 : (int)Lin;
   if (L > 64) return set_error(PG_INVALID_ARG, "TimeSegmentation: L=%d exceeds 64", L);
-  if (L > 1 && interptype != 1)
-    return set_error(PG_INVALID_ARG, "TimeSegmentation: interptype %llu is not implemented (Hanning = 1)",
+  if (L > 1 && (interptype < 1 || interptype > 3))
+    return set_error(PG_INVALID_ARG, "TimeSegmentation: interptype %llu (1 Hanning, 2 min-max, 3 histogram)",
                      (unsigned long long)interptype);
   std::vector<float> tv(tvec, tvec + n1);
   float mn = tv[0], mx = tv[0];
@@ -63,15 +63,24 @@ pg_status build_ts_tables(const float* field_map, const float* tvec, uint64_t n1
   }
   const uint64_t none = n1 / shots;
   const double kPi = 3.141592653589793238462643383279502884;  // arma datum::pi
-  // Hanning interpolator (:83-92), repeated over shots.
   std::vector<float2> one(none * L);
-  for (unsigned int l = 0; l < (unsigned)L; ++l)
-    for (unsigned int m = 0; m < none; ++m) {
-      float v = 0.f;
-      if ((std::abs(tv[m] - ((l) * T.tau))) <= T.tau)
-        v = (float)(0.5 + 0.5 * std::cos((kPi) * (tv[m] - ((l) * T.tau)) / T.tau));
-      one[m + none * l] = make_float2(v, 0.f);
-    }
+  if (interptype == 1) {
+    // Hanning interpolator (:83-92), repeated over shots.
+    for (unsigned int l = 0; l < (unsigned)L; ++l)
+      for (unsigned int m = 0; m < none; ++m) {
+        float v = 0.f;
+        if ((std::abs(tv[m] - ((l) * T.tau))) <= T.tau)
+          v = (float)(0.5 + 0.5 * std::cos((kPi) * (tv[m] - ((l) * T.tau)) / T.tau));
+        one[m + none * l] = make_float2(v, 0.f);
+      }
+  } else {
+    // min-max (:94-156) or its histogram approximation (:157-211), over one shot's times
+    const std::vector<float> t1(tv.begin(), tv.begin() + none);
+    if (interptype == 2)
+      PG_TRY(ts_aa_minmax(field_map, n2, t1, L, T.tau, &one));
+    else
+      PG_TRY(ts_aa_histogram(field_map, n2, t1, L, T.tau, &one));
+  }
   T.AA.resize(n1 * L);
   for (int l = 0; l < L; ++l)
     for (uint64_t m = 0; m < n1; ++m) T.AA[m + n1 * l] = one[(m % none) + none * l];
@@ -164,7 +173,7 @@ pg_status GdftOp::adjoint(const float2* y, float2* x, cudaStream_t s) {
 // ---- TimeSegmentation --------------------------------------------------------
 pg_status TimeSegOp::forward(const float2* x, float2* y, cudaStream_t s) {
   if (tab.L == 1) return inner->forward(x, y, s);  // AA = Wo = 1
-  if (inner->kind == PG_OP_GNUFFT) {
+  if (inner->kind == PG_OP_GNUFFT && bin) {
     auto* g = static_cast<GnufftOp*>(inner);
     NufftBatch b;
     b.C = 1;
@@ -186,7 +195,7 @@ pg_status TimeSegOp::forward(const float2* x, float2* y, cudaStream_t s) {
 }
 pg_status TimeSegOp::adjoint(const float2* y, float2* x, cudaStream_t s) {
   if (tab.L == 1) return inner->adjoint(y, x, s);
-  if (inner->kind == PG_OP_GNUFFT) {
+  if (inner->kind == PG_OP_GNUFFT && bin) {
     auto* g = static_cast<GnufftOp*>(inner);
     NufftBatch b;
     b.C = 1;
@@ -217,6 +226,7 @@ static bool nufft_under(pg_op_s* inner, NufftPlan** plan, const TimeSegOp** ts) 
   if (inner->kind == PG_OP_TIMESEG) {
     auto* t = static_cast<TimeSegOp*>(inner);
     if (t->inner->kind == PG_OP_GNUFFT) {
+      if (t->tab.L > 1 && !t->bin) return false;  // segments applied one at a time
       *plan = static_cast<GnufftOp*>(t->inner)->plan.get();
       *ts = t->tab.L > 1 ? t : nullptr;
       return *plan != nullptr;
@@ -331,6 +341,12 @@ uint64_t PcSenseOp::resident_bytes() const {
   return b;
 }
 
+// The fused gridding stages K segment grids per tile in shared memory: up to
+// 8 in-plane (the forward's register budget), 3 in 3-D (8x8x8 tiles padded
+// to 16x24x16 complex cells, 48 KB each).  Wider windows (the dense min-max
+// interpolators) apply the segments one at a time, as the reference does.
+bool segment_window_fits(const NufftPlan& p, int K) { return p.g.dim == 2 ? K <= 8 : K <= 3; }
+
 static pg_status make_binning_for(NufftPlan* plan, const TsTables& tab, std::unique_ptr<Binning>* out,
                                   cudaStream_t s) {
   return nufft_build_binning(plan, tab.L, tab.K, tab.l0.data(), tab.aa_win.data(), out, s);
@@ -367,9 +383,10 @@ pg_status make_timeseg(std::unique_ptr<TimeSegOp>* out, pg_op_s* G, const float*
   PG_TRY(build_ts_tables(field_map, tvec, n1, n2, L, interptype, shots, &op->tab));
   if (op->tab.L > 1) {
     PG_TRY(build_ts_phases(op->tab, field_map, n2, &op->Wo, &op->WoH, s));
-    if (G->kind == PG_OP_GNUFFT) {
-      if (!static_cast<GnufftOp*>(G)->plan) return interp_only();
-      PG_TRY(make_binning_for(static_cast<GnufftOp*>(G)->plan.get(), op->tab, &op->bin, s));
+    NufftPlan* np = G->kind == PG_OP_GNUFFT ? static_cast<GnufftOp*>(G)->plan.get() : nullptr;
+    if (G->kind == PG_OP_GNUFFT && !np) return interp_only();
+    if (np && segment_window_fits(*np, op->tab.K)) {
+      PG_TRY(make_binning_for(np, op->tab, &op->bin, s));
     } else {
       PG_TRY(op->AAfull.upload(op->tab.AA.data(), op->tab.AA.size(), s));
     }
@@ -426,7 +443,7 @@ pg_status tune_for_coils(pg_op_s* G, int nc, bool search, cudaStream_t s) {
   if (G->kind == PG_OP_TIMESEG) {
     auto* t = static_cast<TimeSegOp*>(G);
     // operators sharing another one's tables inherit its tuning
-    if (t->inner->kind != PG_OP_GNUFFT || t->tab.L <= 1 || t->tab.l0.empty()) return PG_OK;
+    if (t->inner->kind != PG_OP_GNUFFT || t->tab.L <= 1 || t->tab.l0.empty() || !t->bin) return PG_OK;
     NufftPlan* plan = static_cast<GnufftOp*>(t->inner)->plan.get();
     return nufft_autotune(plan, t->tab.L, t->tab.K, t->tab.l0.data(), t->tab.aa_win.data(), nc, &t->bin, search,
                           s);
@@ -529,6 +546,9 @@ pg_status pg_pcsense_timeseg_create(pg_op* out, const float* kx, const float* ky
     PG_TRY(nufft_plan_create(&plan, Nd, 2.0f, (int)nx, (int)ny, (int)nz, kx + sh * Nd, ky + sh * Nd, kz + sh * Nd, s));
     PG_TRY(build_ts_tables(field_map, t + sh * Nd, Nd, Ni, L, interptype, 1, &op->tabs[sh]));
     if (op->tabs[sh].L > 1) {
+      if (!segment_window_fits(*plan, op->tabs[sh].K))
+        return set_error(PG_INVALID_ARG, "pcSenseTimeSeg: interpolator spans %d segments per sample; the fused "
+                                         "gridding takes at most %d here", op->tabs[sh].K, plan->g.dim == 2 ? 8 : 3);
       PG_TRY(build_ts_phases(op->tabs[sh], field_map, Ni, &op->Wo[sh], &op->WoH[sh], s));
       PG_TRY(nufft_autotune(plan.get(), op->tabs[sh].L, op->tabs[sh].K, op->tabs[sh].l0.data(),
                             op->tabs[sh].aa_win.data(), (int)nc, &op->bins[sh], true, s));

@@ -51,6 +51,14 @@ pg_status build_ts_phases(const TsTables& T, const float* field_map, uint64_t n2
                           DevBuf<float2>* WoH, cudaStream_t s);
 pg_status build_ts_tables(const float* field_map, const float* tvec, uint64_t n1, uint64_t n2, uint64_t L,
                           uint64_t interptype, uint64_t shots, TsTables* out);
+// Interpolator tables AA (none x L, column l contiguous) for one shot's times
+// tv (already shifted by T_min), pg_tsinterp.cu.
+pg_status ts_aa_minmax(const float* fm, uint64_t n2, const std::vector<float>& tv, int L, float tau,
+                       std::vector<float2>* aa);
+pg_status ts_aa_histogram(const float* fm, uint64_t n2, const std::vector<float>& tv, int L, float tau,
+                          std::vector<float2>* aa);
+// Whether the fused gridding can apply a segment window of K segments.
+bool segment_window_fits(const NufftPlan& p, int K);
 
 struct GnufftOp : pg_op_s {
   std::unique_ptr<NufftPlan> plan;           // null when gridos != 2 (spatial interpolation only)

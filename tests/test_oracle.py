@@ -193,3 +193,21 @@ def test_density_compensation_oracle_float_vs_fp64(oracle):
     d32 = oracle.density_compensation(0, kx, ky, kz, 16, 8)
     d64 = oracle.density_compensation(1, kx, ky, kz, 16, 8)
     assert np.all(np.isfinite(d64)) and not np.all(np.isfinite(d32))
+
+
+@pytest.mark.parametrize("typ", [2, 3])
+def test_minmax_interpolator_oracle_float_vs_fp64(oracle, typ):
+    """The restated min-max / histogram tables in float agree with FP64 where the
+    Gram matrix is well conditioned (L = 3, +-100 Hz)."""
+    from powergrid_b200 import synthetic as S
+    n = 16
+    kx, ky, t = S.spiral(n, 2, 512, 8e-3)
+    fm = S.field_map(S.Rng(5), n, n, 1, 100.0)
+    M = kx.size
+    ys = []
+    for prec in (0, 1):
+        G = oracle.gnufft(prec, M, n, n, 1, kx, ky, np.zeros_like(kx))
+        T = oracle.timeseg(G, fm, t, M, n * n, 3, typ, 1)
+        x = S.image(S.Rng(7), n * n)
+        ys.append(T.forward(x.astype(np.complex64 if prec == 0 else np.complex128)))
+    assert rel_l2(ys[0], ys[1]) < 1e-4
