@@ -121,6 +121,29 @@ class Gnufft : public Operator {
     check(pg_gnufft_create(&h, dataLength, gridos, nx, ny, nz, detail::ptr(k1), detail::ptr(k2), detail::ptr(k3)));
     adopt(h);
   }
+  // Gnufft::forwardSpatialInterp / adjointSpatialInterp (Gnufft.cpp:213-337):
+  // the oversampled grid in the reference's layout, no FFT.
+  uword grid_length() const {
+    uint64_t n = 0;
+    check(pg_gnufft_grid_length(h_, &n));
+    return n;
+  }
+  template <typename CxCol>
+  CxCol forwardSpatialInterp(const CxCol& grid) const {
+    if (detail::len(grid) != grid_length()) throw Error(PG_INVALID_ARG, "forwardSpatialInterp: grid length");
+    CxCol out(nd_);
+    check(pg_gnufft_forward_spatial_interp(h_, reinterpret_cast<const float*>(detail::ptr(grid)),
+                                           reinterpret_cast<float*>(detail::mptr(out))));
+    return out;
+  }
+  template <typename CxCol>
+  CxCol adjointSpatialInterp(const CxCol& d) const {
+    if (detail::len(d) != nd_) throw Error(PG_INVALID_ARG, "adjointSpatialInterp: data length");
+    CxCol out(grid_length());
+    check(pg_gnufft_adjoint_spatial_interp(h_, reinterpret_cast<const float*>(detail::ptr(d)),
+                                           reinterpret_cast<float*>(detail::mptr(out))));
+    return out;
+  }
 };
 
 template <typename T1>
@@ -175,6 +198,48 @@ class pcSenseTimeSeg : public Operator {
     adopt(h);
   }
 };
+
+template <typename T1>
+class pcSENSE : public Operator {
+ public:
+  template <typename RCol, typename CxCol>
+  pcSENSE(const RCol& kx, const RCol& ky, const RCol& kz, uword nx, uword ny, uword nz, uword nc, const RCol& t,
+          const CxCol& SENSEmap, const RCol& FieldMap, const RCol& ShotPhaseMap) {
+    pg_op h = nullptr;
+    check(pg_pcsense_create(&h, detail::ptr(kx), detail::ptr(ky), detail::ptr(kz), detail::len(kx), nx, ny, nz, nc,
+                            detail::ptr(t), reinterpret_cast<const float*>(detail::ptr(SENSEmap)),
+                            detail::ptr(FieldMap), detail::ptr(ShotPhaseMap), detail::len(ShotPhaseMap)));
+    adopt(h);
+  }
+};
+
+// calc3DDensityCompensation (reconSupport/directRecon.cpp:28-61).
+template <typename T1, typename RCol>
+RCol calc3DDensityCompensation(const RCol& kx, const RCol& ky, const RCol& kz, uword Ninplane, uword Nz) {
+  RCol dcf(detail::len(kx));
+  check(pg_density_compensation(detail::ptr(kx), detail::ptr(ky), detail::ptr(kz), detail::len(kx), Ninplane, Nz,
+                                detail::mptr(dcf)));
+  return dcf;
+}
+
+// Coil-major images G / (dcf .* data_c) (directRecon.cpp:108-133).
+template <typename T1, typename RCol, typename CxCol>
+CxCol gridCoilImages(const Gnufft<T1>& G, const RCol& dcf, const CxCol& data, uword Ncoils) {
+  CxCol out(G.n_image() * Ncoils);
+  check(pg_grid_coil_images(G.handle(), detail::ptr(dcf), reinterpret_cast<const float*>(detail::ptr(data)), Ncoils,
+                            reinterpret_cast<float*>(detail::mptr(out))));
+  return out;
+}
+
+// calcSumOfSquaresImage (directRecon.cpp:63-73): sqrt(sum_c |img_c|).
+template <typename T1, typename RCol, typename CxCol>
+RCol calcSumOfSquaresImage(const CxCol& coilImages, uword Ncoils) {
+  const uword n = detail::len(coilImages) / Ncoils;
+  RCol out(n);
+  check(pg_sum_of_squares_image(reinterpret_cast<const float*>(detail::ptr(coilImages)), n, Ncoils,
+                                detail::mptr(out)));
+  return out;
+}
 
 template <typename T1>
 struct QuadPenalty {

@@ -1,6 +1,7 @@
 // Drives the C++ operator API (include/powergrid/PowerGrid.hpp) the way the
 // reference's PowerGridIsmrmrd driver does (PowerGridIsmrmrd.cpp:244-264):
-// Gnufft -> TimeSegmentation -> SENSE -> operator*, operator/, reconSolve.
+// Gnufft -> TimeSegmentation -> SENSE -> operator*, operator/, reconSolve,
+// then the direct-reconstruction helpers and the spatial interpolation.
 // Inputs and outputs are raw little-endian files in the directory argv[1]
 // (written and checked by tests/test_cpp_api.py).
 #include <complex>
@@ -54,6 +55,18 @@ int main(int argc, char** argv) {
     save(d + "/y_out.bin", y);
     save(d + "/xadj_out.bin", xa);
     save(d + "/img_out.bin", img);
+    // direct reconstruction (reconSupport/directRecon.cpp): density
+    // compensation, per-coil gridded images, coil combination
+    pg::Col<float> dcf = pg::calc3DDensityCompensation<float>(kx, ky, kz, nx, nz);
+    pg::Col<cx> coil = pg::gridCoilImages<float>(G, dcf, data, nc);
+    pg::Col<float> sos = pg::calcSumOfSquaresImage<float, pg::Col<float>>(coil, nc);
+    save(d + "/dcf_out.bin", dcf);
+    save(d + "/sos_out.bin", sos);
+    // spatial interpolation round trip on the oversampled grid
+    pg::Col<cx> y0(M);  // the first coil's samples
+    for (pg::uword i = 0; i < M; ++i) y0.memptr()[i] = y.memptr()[i];
+    pg::Col<cx> grid = G.adjointSpatialInterp(y0);
+    save(d + "/interp_out.bin", G.forwardSpatialInterp(grid));
   } catch (const pg::Error& e) {
     std::fprintf(stderr, "pg error: %s\n", e.what());
     return 1;

@@ -45,3 +45,13 @@ def test_cpp_api_matches_reference_fixture(pg, tmp_path):
     t = np.load(os.path.join(ROOT, "tests", "golden", "tssense2d.npz"))
     assert rel_l2(y, t["y_f32"]) <= 1e-5          # same geometry and image as the tssense2d fixture
     assert rel_l2(img, c["x_pcg_f32"]) <= 1e-4    # reconSolve, 5 iterations
+    # the C++ helpers return what the Python API does (same library calls)
+    dcf = np.fromfile(os.path.join(out, "dcf_out.bin"), np.float32)
+    sos = np.fromfile(os.path.join(out, "sos_out.bin"), np.float32)
+    assert np.array_equal(dcf, pg.calc3DDensityCompensation(c["kx"], c["ky"], c["kz"], nx, nz))
+    G = pg.Gnufft(M, 2.0, nx, ny, nz, c["kx"], c["ky"], c["kz"])
+    coil = pg.gridCoilImages(G, dcf, c["y_f32"], nc)
+    assert rel_l2(sos, pg.calcSumOfSquaresImage(coil, nc)) <= 1e-6
+    rt = np.fromfile(os.path.join(out, "interp_out.bin"), np.complex64)
+    ysub = y[:M]
+    assert rt.size == M and rel_l2(rt, G.forwardSpatialInterp(G.adjointSpatialInterp(ysub))) <= 1e-6
