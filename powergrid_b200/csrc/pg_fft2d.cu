@@ -15,9 +15,20 @@
 //                columns, post-kernel weights (sign, deapodization, WoH,
 //                conj coil map, conj shot phase)               -> one image per grid
 //            sum the images of the batch's grids in a fixed order.
-// Transforms are unnormalised (FFTW/cuFFT conventions, forward sign -1) and
-// run in shared memory as Stockham radix-4 (+ one radix-2) passes over a
-// batch of rows; twiddles come from a table made in double precision.
+// Transforms are unnormalised (FFTW/cuFFT conventions, forward sign -1).
+//
+// Each length-n transform (n = R1 * R2) is two register passes with one
+// shared-memory transpose between them (the four-step form): with
+// m = R2*m1 + m2 and k = k1 + R1*k2,
+//   X[k] = sum_m2 W_R2^(m2 k2) * W_n^(m2 k1) * sum_m1 W_R1^(m1 k1) x[m].
+// Pass 1: a thread takes one m2, loads its R1 inputs straight from global
+// memory (consecutive threads: consecutive m2 or columns, so the loads
+// coalesce), does the R1-point DFT in registers and the twiddle W_n^(m2 k1),
+// and stores into shared memory.  Pass 2: a thread takes one k1, reads its R2
+// values, does the R2-point DFT and stores X[k1 + R1 k2] straight to global
+// memory.  Zero inputs (the padding) are never loaded and cropped outputs
+// never stored.  Twiddles W_n^(m2 k1) come from a table made in double
+// precision, laid out [k1][m2].
 #include <cmath>
 #include <vector>
 
@@ -26,34 +37,40 @@
 namespace pg {
 namespace {
 
-constexpr int kThreads = 256;
-constexpr int kElems = 2048;   // complex values per block and buffer
+constexpr int kT = 256;   // threads per block
 
 __device__ __forceinline__ float2 twiddle(float2 v, float2 w, bool inv) {
   const float wy = inv ? -w.y : w.y;
   return make_float2(v.x * w.x - v.y * wy, v.x * wy + v.y * w.x);
 }
 
-// Row layout in shared memory: one padding element after every 16 (the
-// radix-16 Stockham loads and stores then hit 16 distinct 8-byte bank pairs
-// per half-warp), and a row stride of 2 (mod 16) elements, so the column
-// kernels' transposed accesses (8 columns x 2 rows per half-warp at n = 256)
-// are conflict-free too.
-__host__ __device__ constexpr int pad16(int c) { return c + (c >> 4); }
-template <int LOGN>
-__host__ __device__ constexpr int row_stride() { return pad16(1 << LOGN) + 2; }
+// cos(2 pi m / 32), m = 0 .. 31 (points of the unit circle).
+__device__ constexpr float kC32[32] = {
+    1.f, 0.98078528040323044913f, 0.92387953251128675613f, 0.83146961230254523708f, 0.70710678118654752440f,
+    0.55557023301960222474f, 0.38268343236508977173f, 0.19509032201612826785f, 0.f, -0.19509032201612826785f,
+    -0.38268343236508977173f, -0.55557023301960222474f, -0.70710678118654752440f, -0.83146961230254523708f,
+    -0.92387953251128675613f, -0.98078528040323044913f, -1.f, -0.98078528040323044913f, -0.92387953251128675613f,
+    -0.83146961230254523708f, -0.70710678118654752440f, -0.55557023301960222474f, -0.38268343236508977173f,
+    -0.19509032201612826785f, 0.f, 0.19509032201612826785f, 0.38268343236508977173f, 0.55557023301960222474f,
+    0.70710678118654752440f, 0.83146961230254523708f, 0.92387953251128675613f, 0.98078528040323044913f};
 
-// exp(-/+ 2 pi i m / 16) * v for a compile-time m (constants of the unit circle).
+// exp(-/+ 2 pi i m / 32) * v for a compile-time m.
 template <int M>
-__device__ __forceinline__ float2 rot16(float2 v, bool inv) {
-  constexpr float kC[16] = {1.f, 0.92387953251128674f, 0.70710678118654752f, 0.38268343236508977f, 0.f,
-                            -0.38268343236508977f, -0.70710678118654752f, -0.92387953251128674f, -1.f,
-                            -0.92387953251128674f, -0.70710678118654752f, -0.38268343236508977f, 0.f,
-                            0.38268343236508977f, 0.70710678118654752f, 0.92387953251128674f};
-  constexpr float c = kC[M % 16];
-  constexpr float sn = kC[(M + 12) % 16];   // sin(2 pi m/16) = cos(2 pi (m - 4)/16)
-  const float sy = inv ? sn : -sn;
-  return make_float2(v.x * c - v.y * sy, v.x * sy + v.y * c);
+__device__ __forceinline__ float2 rot32(float2 v, bool inv) {
+  if constexpr (M % 32 == 0) {
+    return v;
+  } else {
+    constexpr float c = kC32[M % 32];
+    constexpr float sn = kC32[(M + 24) % 32];   // sin(2 pi m/32) = cos(2 pi (m - 8)/32)
+    const float sy = inv ? sn : -sn;
+    return make_float2(v.x * c - v.y * sy, v.x * sy + v.y * c);
+  }
+}
+
+__device__ __forceinline__ void dft2(float2& a, float2& b) {
+  const float2 t = a;
+  a = make_float2(t.x + b.x, t.y + b.y);
+  b = make_float2(t.x - b.x, t.y - b.y);
 }
 
 __device__ __forceinline__ void dft4(float2& v0, float2& v1, float2& v2, float2& v3, bool inv) {
@@ -67,17 +84,35 @@ __device__ __forceinline__ void dft4(float2& v0, float2& v1, float2& v2, float2&
   v3 = make_float2(t1.x - m3.x, t1.y - m3.y);
 }
 
-// 16-point DFT in registers as 4 x 4: y[k1 + 4 k2] = sum_n2 W4^(n2 k2) W16^(n2 k1)
-// sum_n1 W4^(n1 k1) v[4 n1 + n2].
+// 8-point DFT, natural order in and out: m = 2 m1 + m2, k = k1 + 4 k2.
+__device__ __forceinline__ void dft8(float2 (&v)[8], bool inv) {
+  dft4(v[0], v[2], v[4], v[6], inv);
+  dft4(v[1], v[3], v[5], v[7], inv);
+  v[3] = rot32<4>(v[3], inv);
+  v[5] = rot32<8>(v[5], inv);
+  v[7] = rot32<12>(v[7], inv);
+  float2 y[8];
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) {
+    float2 a = v[2 * k1], b = v[2 * k1 + 1];
+    dft2(a, b);
+    y[k1] = a;
+    y[k1 + 4] = b;
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = y[i];
+}
+
+// 16-point DFT as 4 x 4, natural order in and out.
 __device__ __forceinline__ void dft16(float2 (&v)[16], bool inv) {
   dft4(v[0], v[4], v[8], v[12], inv);
   dft4(v[1], v[5], v[9], v[13], inv);
   dft4(v[2], v[6], v[10], v[14], inv);
   dft4(v[3], v[7], v[11], v[15], inv);
   // v[4 k1 + n2] now holds u[n2][k1]
-  v[5] = rot16<1>(v[5], inv);   v[6] = rot16<2>(v[6], inv);   v[7] = rot16<3>(v[7], inv);
-  v[9] = rot16<2>(v[9], inv);   v[10] = rot16<4>(v[10], inv); v[11] = rot16<6>(v[11], inv);
-  v[13] = rot16<3>(v[13], inv); v[14] = rot16<6>(v[14], inv); v[15] = rot16<9>(v[15], inv);
+  v[5] = rot32<2>(v[5], inv);   v[6] = rot32<4>(v[6], inv);   v[7] = rot32<6>(v[7], inv);
+  v[9] = rot32<4>(v[9], inv);   v[10] = rot32<8>(v[10], inv); v[11] = rot32<12>(v[11], inv);
+  v[13] = rot32<6>(v[13], inv); v[14] = rot32<12>(v[14], inv); v[15] = rot32<18>(v[15], inv);
   dft4(v[0], v[1], v[2], v[3], inv);
   dft4(v[4], v[5], v[6], v[7], inv);
   dft4(v[8], v[9], v[10], v[11], inv);
@@ -92,249 +127,285 @@ __device__ __forceinline__ void dft16(float2 (&v)[16], bool inv) {
   t = v[11]; v[11] = v[14]; v[14] = t;
 }
 
-// One Stockham pass of radix R (16, 4 or 2) over ROWS rows of length n,
-// a -> b, after Ns = product of the earlier radices.
-template <int LOGN, int ROWS, int R>
-__device__ __forceinline__ void fft_stage(const float2* a, float2* b, int Ns, const float2* tw, bool inv) {
-  constexpr int n = 1 << LOGN, m = n / R, RS = row_stride<LOGN>();
-  constexpr int total = ROWS * m;
-  constexpr int per = (total + kThreads - 1) / kThreads;
-  const int step = n / (Ns * R);
-#pragma unroll
-  for (int it = 0; it < per; ++it) {
-    const int idx = it * kThreads + threadIdx.x;
-    if (total % kThreads != 0 && idx >= total) break;
-    const int row = idx / m, j = idx % m;
-    const float2* s = a + row * RS;
-    float2* d = b + row * RS;
-    float2 v[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = s[pad16(j + r * m)];
-    const int k = j & (Ns - 1);
-    if (Ns > 1) {
-#pragma unroll
-      for (int r = 1; r < R; ++r) v[r] = twiddle(v[r], tw[r * k * step], inv);
-    }
-    if constexpr (R == 16) {
-      dft16(v, inv);
-    } else if constexpr (R == 4) {
-      dft4(v[0], v[1], v[2], v[3], inv);
-    } else {
-      const float2 t = v[0];
-      v[0] = make_float2(t.x + v[1].x, t.y + v[1].y);
-      v[1] = make_float2(t.x - v[1].x, t.y - v[1].y);
-    }
-    const int o = (j / Ns) * Ns * R + k;
-#pragma unroll
-    for (int r = 0; r < R; ++r) d[pad16(o + r * Ns)] = v[r];
+template <int M>
+__device__ __forceinline__ void rot_odd32(float2 (&o)[16], bool inv) {
+  if constexpr (M < 16) {
+    o[M] = rot32<M>(o[M], inv);
+    rot_odd32<M + 1>(o, inv);
   }
-  __syncthreads();
 }
 
-// Batched in-shared-memory FFT of ROWS rows of length n = 2^LOGN (row r at
-// a + r*row_stride, padded by pad16); b is scratch of the same shape and tw
-// the twiddle table (in shared memory).  Radix-16 passes, then one radix-4
-// and/or radix-2 pass.  Returns the buffer that holds the result, in natural
-// order.
-template <int LOGN, int ROWS>
-__device__ float2* fft_rows(float2* a, float2* b, const float2* tw, bool inv) {
-  int Ns = 1;
+// 32-point DFT as 16 x 2, natural order in and out: m = 2 m1 + m2, k = k1 + 16 k2.
+__device__ __forceinline__ void dft32(float2 (&v)[32], bool inv) {
+  float2 e[16], o[16];
 #pragma unroll
-  for (int st = 0; st < LOGN / 4; ++st) {
-    fft_stage<LOGN, ROWS, 16>(a, b, Ns, tw, inv);
-    float2* t = a; a = b; b = t;
-    Ns *= 16;
+  for (int i = 0; i < 16; ++i) { e[i] = v[2 * i]; o[i] = v[2 * i + 1]; }
+  dft16(e, inv);
+  dft16(o, inv);
+  rot_odd32<1>(o, inv);
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    float2 a = e[k], b = o[k];
+    dft2(a, b);
+    v[k] = a;
+    v[k + 16] = b;
   }
-  if ((LOGN % 4) >= 2) {
-    fft_stage<LOGN, ROWS, 4>(a, b, Ns, tw, inv);
-    float2* t = a; a = b; b = t;
-    Ns *= 4;
-  }
-  if (LOGN % 2) {
-    fft_stage<LOGN, ROWS, 2>(a, b, Ns, tw, inv);
-    float2* t = a; a = b; b = t;
-  }
-  return a;
 }
 
-// Copy the n-entry twiddle table into shared memory.
+template <int R>
+__device__ __forceinline__ void dft(float2 (&v)[R], bool inv) {
+  if constexpr (R == 4) {
+    dft4(v[0], v[1], v[2], v[3], inv);
+  } else if constexpr (R == 8) {
+    dft8(v, inv);
+  } else if constexpr (R == 16) {
+    dft16(v, inv);
+  } else {
+    static_assert(R == 32, "radix");
+    dft32(v, inv);
+  }
+}
+
+// Factor n = R1 * R2 of each supported length.
+template <int LOGN> struct Split;
+template <> struct Split<6> { static constexpr int R1 = 16, R2 = 4; };
+template <> struct Split<7> { static constexpr int R1 = 16, R2 = 8; };
+template <> struct Split<8> { static constexpr int R1 = 16, R2 = 16; };
+template <> struct Split<9> { static constexpr int R1 = 16, R2 = 32; };
+template <> struct Split<10> { static constexpr int R1 = 32, R2 = 32; };
+
+// Row kernels: RB = kT / R2 rows per block.  Shared layout [row][k1][m2] with
+// m2 stride R2 + 1 (odd: pass 2's threads, one k1 each, hit distinct banks)
+// and a row stride = R2 (mod 16) (pass 1's half-warps span 16 / R2 rows).
 template <int LOGN>
-__device__ __forceinline__ void load_twiddles(float2* stw, const float2* __restrict__ tw) {
-  constexpr int n = 1 << LOGN;
-#pragma unroll
-  for (int it = 0; it < (n + kThreads - 1) / kThreads; ++it) {
-    const int k = it * kThreads + threadIdx.x;
-    if (k < n) stw[k] = tw[k];
-  }
-}
+struct RowGeo {
+  static constexpr int R1 = Split<LOGN>::R1, R2 = Split<LOGN>::R2, n = R1 * R2;
+  static constexpr int RB = kT / R2;
+  static constexpr int S2 = R2 + 1;
+  static constexpr int base = R1 * S2;
+  static constexpr int RS = base + (((R2 - base) % 16) + 16) % 16;
+  static constexpr size_t smem = (size_t)RB * RS * sizeof(float2);
+};
+
+// Column kernels: CB adjacent columns per block, shared layout [k1][m2][col].
+template <int LOGN>
+struct ColGeo {
+  static constexpr int R1 = Split<LOGN>::R1, R2 = Split<LOGN>::R2, n = R1 * R2;
+  static constexpr int CB = (4096 / n) > 8 ? (4096 / n) : 8;
+  static constexpr size_t smem = (size_t)n * CB * sizeof(float2);
+};
 
 __device__ __forceinline__ int parity2(int a, int b) { return (a + b) & 1; }
 
-// Shared memory per block: two R-row buffers and the twiddle table.
+// F1: pre-kernel values of image rows ix of grid b, zero padded to n, FFT
+// along y -> P[b][ix][0..n).
 template <int LOGN>
-constexpr size_t fft_smem_bytes() {
-  return (2ull * (kElems / (1 << LOGN)) * row_stride<LOGN>() + (1 << LOGN)) * sizeof(float2);
-}
-
-// F1: pre-kernel values of image rows ix (R rows per block) of grid b,
-// zero padded to n, FFT along y -> P[b][ix][0..n).
-template <int LOGN>
-__global__ void __launch_bounds__(kThreads) k_fft_fwd_rows(NufftGeom g, int L, const float2* __restrict__ x,
-                                                           const float2* __restrict__ S, int c0,
-                                                           const float2* __restrict__ E,
-                                                           const float2* __restrict__ Wo,
-                                                           const float* __restrict__ deapf,
-                                                           const float2* __restrict__ tw, float2* __restrict__ P) {
-  constexpr int n = 1 << LOGN, R = kElems / n, stride = row_stride<LOGN>(), PER = kElems / kThreads;
+__global__ void __launch_bounds__(kT) k_fft_fwd_rows(NufftGeom g, int L, const float2* __restrict__ x,
+                                                     const float2* __restrict__ S, int c0,
+                                                     const float2* __restrict__ E, const float2* __restrict__ Wo,
+                                                     const float* __restrict__ deapf, const float2* __restrict__ tw,
+                                                     float2* __restrict__ P) {
+  using RG = RowGeo<LOGN>;
+  constexpr int R1 = RG::R1, R2 = RG::R2, n = RG::n, RB = RG::RB, S2 = RG::S2, RS = RG::RS;
   extern __shared__ float2 sh[];
-  float2* a = sh;
-  float2* bb = sh + R * stride;
-  float2* stw = sh + 2 * R * stride;
-  load_twiddles<LOGN>(stw, tw);
   const int Nn = g.Ny, pad = g.pad_off[1];
   const uint64_t N = g.nimg();
   const int b = blockIdx.y, c = b / L, l = b - c * L;
-  const int ix0 = blockIdx.x * R;
-#pragma unroll
-  for (int it = 0; it < PER; ++it) {
-    const int e = it * kThreads + threadIdx.x;
-    const int r = e / n, gy = e % n;
+  const int ix0 = blockIdx.x * RB;
+  {
+    const int m2 = threadIdx.x % R2, r = threadIdx.x / R2;
     const int ix = ix0 + r;
-    float2 v = make_float2(0.f, 0.f);
-    const int iy = gy - pad;
-    if (ix < g.Nx && iy >= 0 && iy < Nn) {
-      const uint64_t p = (uint64_t)iy + (uint64_t)Nn * ix;
-      v = x[p];
-      if (S) {
-        const float2 sv = S[(uint64_t)(c0 + c) * N + p];
-        v = E ? cmul(v, cmul(sv, E[p])) : cmul(sv, v);
+    float2 v[R1];
+#pragma unroll
+    for (int m1 = 0; m1 < R1; ++m1) {
+      const int gy = R2 * m1 + m2;
+      const int iy = gy - pad;
+      float2 u = make_float2(0.f, 0.f);
+      if (ix < g.Nx && iy >= 0 && iy < Nn) {
+        const uint64_t p = (uint64_t)iy + (uint64_t)Nn * ix;
+        u = x[p];
+        if (S) {
+          const float2 sv = S[(uint64_t)(c0 + c) * N + p];
+          u = E ? cmul(u, cmul(sv, E[p])) : cmul(sv, u);
+        }
+        if (Wo) u = cmul(Wo[(uint64_t)l * N + p], u);
+        const float f = parity2(ix + g.pad_off[0], gy) ? -deapf[p] : deapf[p];
+        u = make_float2(u.x * f, u.y * f);
       }
-      if (Wo) v = cmul(Wo[(uint64_t)l * N + p], v);
-      const float f = parity2(ix + g.pad_off[0], gy) ? -deapf[p] : deapf[p];
-      v = make_float2(v.x * f, v.y * f);
+      v[m1] = u;
     }
-    a[r * stride + pad16(gy)] = v;
+    dft<R1>(v, false);
+    float2* d = sh + r * RS + m2;
+    d[0] = v[0];
+#pragma unroll
+    for (int k1 = 1; k1 < R1; ++k1) d[k1 * S2] = twiddle(v[k1], tw[k1 * R2 + m2], false);
   }
   __syncthreads();
-  const float2* res = fft_rows<LOGN, R>(a, bb, stw, false);
 #pragma unroll
-  for (int it = 0; it < PER; ++it) {
-    const int e = it * kThreads + threadIdx.x;
-    const int r = e / n, gy = e % n;
-    if (ix0 + r < g.Nx) P[((uint64_t)b * g.Nx + ix0 + r) * n + gy] = res[r * stride + pad16(gy)];
+  for (int it0 = 0; it0 < RB * R1; it0 += kT) {
+    const int it = it0 + threadIdx.x;
+    if ((RB * R1) % kT != 0 && it >= RB * R1) break;
+    const int k1 = it % R1, r = it / R1;
+    const int ix = ix0 + r;
+    float2 u[R2];
+    const float2* s = sh + r * RS + k1 * S2;
+#pragma unroll
+    for (int m2 = 0; m2 < R2; ++m2) u[m2] = s[m2];
+    dft<R2>(u, false);
+    if (ix < g.Nx) {
+      float2* o = P + ((uint64_t)b * g.Nx + ix) * n + k1;
+#pragma unroll
+      for (int k2 = 0; k2 < R2; ++k2) o[R1 * k2] = u[k2];
+    }
   }
 }
 
-// F2: columns gy (R per block) of grid b: the Nx rows of P at gx = pad + i,
-// zero padded to n, FFT along x -> grids[b][gx][gy] for every gx.
+// F2: columns gy of grid b: the Nx rows of P at gx = pad + i, zero padded to
+// n, FFT along x -> grids[b][gx][gy] for every gx.
 template <int LOGN>
-__global__ void __launch_bounds__(kThreads) k_fft_fwd_cols(NufftGeom g, const float2* __restrict__ P,
-                                                           const float2* __restrict__ tw,
-                                                           float2* __restrict__ grids) {
-  constexpr int n = 1 << LOGN, R = kElems / n, stride = row_stride<LOGN>(), PER = kElems / kThreads;
+__global__ void __launch_bounds__(kT) k_fft_fwd_cols(NufftGeom g, const float2* __restrict__ P,
+                                                     const float2* __restrict__ tw, float2* __restrict__ grids) {
+  using CG = ColGeo<LOGN>;
+  constexpr int R1 = CG::R1, R2 = CG::R2, n = CG::n, CB = CG::CB;
   extern __shared__ float2 sh[];
-  float2* a = sh;
-  float2* bb = sh + R * stride;
-  float2* stw = sh + 2 * R * stride;
-  load_twiddles<LOGN>(stw, tw);
   const int pad = g.pad_off[0];
-  const int b = blockIdx.y, gy0 = blockIdx.x * R;
+  const int b = blockIdx.y, gy0 = blockIdx.x * CB;
 #pragma unroll
-  for (int it = 0; it < PER; ++it) {
-    const int e = it * kThreads + threadIdx.x;
-    const int gx = e / R, cl = e % R;
-    const int i = gx - pad;
-    float2 v = make_float2(0.f, 0.f);
-    if (i >= 0 && i < g.Nx) v = P[((uint64_t)b * g.Nx + i) * n + gy0 + cl];
-    a[cl * stride + pad16(gx)] = v;
+  for (int it0 = 0; it0 < CB * R2; it0 += kT) {
+    const int it = it0 + threadIdx.x;
+    if ((CB * R2) % kT != 0 && it >= CB * R2) break;
+    const int col = it % CB, m2 = it / CB;
+    float2 v[R1];
+#pragma unroll
+    for (int m1 = 0; m1 < R1; ++m1) {
+      const int i = R2 * m1 + m2 - pad;
+      v[m1] = (i >= 0 && i < g.Nx) ? P[((uint64_t)b * g.Nx + i) * n + gy0 + col] : make_float2(0.f, 0.f);
+    }
+    dft<R1>(v, false);
+    float2* d = sh + m2 * CB + col;
+    d[0] = v[0];
+#pragma unroll
+    for (int k1 = 1; k1 < R1; ++k1) d[k1 * R2 * CB] = twiddle(v[k1], tw[k1 * R2 + m2], false);
   }
   __syncthreads();
-  const float2* res = fft_rows<LOGN, R>(a, bb, stw, false);
   const uint64_t G = (uint64_t)n * n;
 #pragma unroll
-  for (int it = 0; it < PER; ++it) {
-    const int e = it * kThreads + threadIdx.x;
-    const int gx = e / R, cl = e % R;
-    grids[(uint64_t)b * G + (uint64_t)gx * n + gy0 + cl] = res[cl * stride + pad16(gx)];
+  for (int it0 = 0; it0 < CB * R1; it0 += kT) {
+    const int it = it0 + threadIdx.x;
+    if ((CB * R1) % kT != 0 && it >= CB * R1) break;
+    const int col = it % CB, k1 = it / CB;
+    float2 u[R2];
+    const float2* s = sh + k1 * R2 * CB + col;
+#pragma unroll
+    for (int m2 = 0; m2 < R2; ++m2) u[m2] = s[m2 * CB];
+    dft<R2>(u, false);
+    float2* o = grids + (uint64_t)b * G + (uint64_t)k1 * n + gy0 + col;
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) o[(uint64_t)R1 * k2 * n] = u[k2];
   }
 }
 
 // A1: columns gy of grid b, inverse FFT along x, keep gx = crop + i -> Q[b][i][gy].
 template <int LOGN>
-__global__ void __launch_bounds__(kThreads) k_fft_inv_cols(NufftGeom g, const float2* __restrict__ grids,
-                                                           const float2* __restrict__ tw, float2* __restrict__ Q) {
-  constexpr int n = 1 << LOGN, R = kElems / n, stride = row_stride<LOGN>(), PER = kElems / kThreads;
+__global__ void __launch_bounds__(kT) k_fft_inv_cols(NufftGeom g, const float2* __restrict__ grids,
+                                                     const float2* __restrict__ tw, float2* __restrict__ Q) {
+  using CG = ColGeo<LOGN>;
+  constexpr int R1 = CG::R1, R2 = CG::R2, n = CG::n, CB = CG::CB;
   extern __shared__ float2 sh[];
-  float2* a = sh;
-  float2* bb = sh + R * stride;
-  float2* stw = sh + 2 * R * stride;
-  load_twiddles<LOGN>(stw, tw);
   const int crop = g.crop_off[0];
-  const int b = blockIdx.y, gy0 = blockIdx.x * R;
+  const int b = blockIdx.y, gy0 = blockIdx.x * CB;
   const uint64_t G = (uint64_t)n * n;
 #pragma unroll
-  for (int it = 0; it < PER; ++it) {
-    const int e = it * kThreads + threadIdx.x;
-    const int gx = e / R, cl = e % R;
-    a[cl * stride + pad16(gx)] = grids[(uint64_t)b * G + (uint64_t)gx * n + gy0 + cl];
+  for (int it0 = 0; it0 < CB * R2; it0 += kT) {
+    const int it = it0 + threadIdx.x;
+    if ((CB * R2) % kT != 0 && it >= CB * R2) break;
+    const int col = it % CB, m2 = it / CB;
+    float2 v[R1];
+    const float2* s = grids + (uint64_t)b * G + (uint64_t)m2 * n + gy0 + col;
+#pragma unroll
+    for (int m1 = 0; m1 < R1; ++m1) v[m1] = s[(uint64_t)R2 * m1 * n];
+    dft<R1>(v, true);
+    float2* d = sh + m2 * CB + col;
+    d[0] = v[0];
+#pragma unroll
+    for (int k1 = 1; k1 < R1; ++k1) d[k1 * R2 * CB] = twiddle(v[k1], tw[k1 * R2 + m2], true);
   }
   __syncthreads();
-  const float2* res = fft_rows<LOGN, R>(a, bb, stw, true);
 #pragma unroll
-  for (int it = 0; it < PER / 2; ++it) {    // the Nx = n/2 cropped rows
-    const int e = it * kThreads + threadIdx.x;
-    const int i = e / R, cl = e % R;
-    Q[((uint64_t)b * g.Nx + i) * n + gy0 + cl] = res[cl * stride + pad16(crop + i)];
+  for (int it0 = 0; it0 < CB * R1; it0 += kT) {
+    const int it = it0 + threadIdx.x;
+    if ((CB * R1) % kT != 0 && it >= CB * R1) break;
+    const int col = it % CB, k1 = it / CB;
+    float2 u[R2];
+    const float2* s = sh + k1 * R2 * CB + col;
+#pragma unroll
+    for (int m2 = 0; m2 < R2; ++m2) u[m2] = s[m2 * CB];
+    dft<R2>(u, true);
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) {
+      const int i = k1 + R1 * k2 - crop;
+      if (i >= 0 && i < g.Nx) Q[((uint64_t)b * g.Nx + i) * n + gy0 + col] = u[k2];
+    }
   }
 }
 
 // A2: cropped rows ix of grid b, inverse FFT along y, keep gy = crop + iy and
 // apply the post-kernel weights of grid b = (coil c, segment l) -> Rimg[b][p].
 template <int LOGN>
-__global__ void __launch_bounds__(kThreads) k_fft_inv_rows(NufftGeom g, int L, const float2* __restrict__ Q,
-                                                           const float2* __restrict__ S, int c0,
-                                                           const float2* __restrict__ E,
-                                                           const float2* __restrict__ WoH,
-                                                           const float* __restrict__ deapf,
-                                                           const float2* __restrict__ tw,
-                                                           float2* __restrict__ Rimg) {
-  constexpr int n = 1 << LOGN, R = kElems / n, stride = row_stride<LOGN>(), PER = kElems / kThreads;
+__global__ void __launch_bounds__(kT) k_fft_inv_rows(NufftGeom g, int L, const float2* __restrict__ Q,
+                                                     const float2* __restrict__ S, int c0,
+                                                     const float2* __restrict__ E, const float2* __restrict__ WoH,
+                                                     const float* __restrict__ deapf, const float2* __restrict__ tw,
+                                                     float2* __restrict__ Rimg) {
+  using RG = RowGeo<LOGN>;
+  constexpr int R1 = RG::R1, R2 = RG::R2, n = RG::n, RB = RG::RB, S2 = RG::S2, RS = RG::RS;
   extern __shared__ float2 sh[];
-  float2* a = sh;
-  float2* bb = sh + R * stride;
-  float2* stw = sh + 2 * R * stride;
-  load_twiddles<LOGN>(stw, tw);
   constexpr int Nn = n / 2;
   const int crop = g.crop_off[1];
   const uint64_t N = g.nimg();
   const int b = blockIdx.y, c = b / L, l = b - c * L;
-  const int ix0 = blockIdx.x * R;
+  const int ix0 = blockIdx.x * RB;
+  {
+    const int m2 = threadIdx.x % R2, r = threadIdx.x / R2;
+    const int ix = ix0 + r;
+    float2 v[R1];
+    const float2* s = Q + ((uint64_t)b * g.Nx + ix) * n + m2;
 #pragma unroll
-  for (int it = 0; it < PER; ++it) {
-    const int e = it * kThreads + threadIdx.x;
-    const int r = e / n, gy = e % n;
-    float2 v = make_float2(0.f, 0.f);
-    if (ix0 + r < g.Nx) v = Q[((uint64_t)b * g.Nx + ix0 + r) * n + gy];
-    a[r * stride + pad16(gy)] = v;
+    for (int m1 = 0; m1 < R1; ++m1) v[m1] = (ix < g.Nx) ? s[R2 * m1] : make_float2(0.f, 0.f);
+    dft<R1>(v, true);
+    float2* d = sh + r * RS + m2;
+    d[0] = v[0];
+#pragma unroll
+    for (int k1 = 1; k1 < R1; ++k1) d[k1 * S2] = twiddle(v[k1], tw[k1 * R2 + m2], true);
   }
   __syncthreads();
-  const float2* res = fft_rows<LOGN, R>(a, bb, stw, true);
 #pragma unroll
-  for (int it = 0; it < PER / 2; ++it) {    // the Ny = n/2 cropped columns of R rows
-    const int e = it * kThreads + threadIdx.x;
-    const int r = e / Nn, iy = e % Nn;
+  for (int it0 = 0; it0 < RB * R1; it0 += kT) {
+    const int it = it0 + threadIdx.x;
+    if ((RB * R1) % kT != 0 && it >= RB * R1) break;
+    const int k1 = it % R1, r = it / R1;
     const int ix = ix0 + r;
+    float2 u[R2];
+    const float2* s = sh + r * RS + k1 * S2;
+#pragma unroll
+    for (int m2 = 0; m2 < R2; ++m2) u[m2] = s[m2];
+    dft<R2>(u, true);
     if (ix >= g.Nx) continue;
-    const uint64_t p = (uint64_t)iy + (uint64_t)Nn * ix;
-    float2 v = res[r * stride + pad16(crop + iy)];
-    const float f = parity2(ix + g.crop_off[0], iy + crop) ? -deapf[p] : deapf[p];
-    v = make_float2(v.x * f, v.y * f);
-    if (WoH) v = cmul(v, WoH[(uint64_t)l * N + p]);
-    if (S) {
-      const float2 sv = S[(uint64_t)(c0 + c) * N + p];
-      v = E ? cmul(cmul(cconj(sv), cconj(E[p])), v) : cmul(v, cconj(sv));
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) {
+      const int iy = k1 + R1 * k2 - crop;
+      if (iy < 0 || iy >= Nn) continue;
+      const uint64_t p = (uint64_t)iy + (uint64_t)Nn * ix;
+      float2 v = u[k2];
+      const float f = parity2(ix + g.crop_off[0], iy + crop) ? -deapf[p] : deapf[p];
+      v = make_float2(v.x * f, v.y * f);
+      if (WoH) v = cmul(v, WoH[(uint64_t)l * N + p]);
+      if (S) {
+        const float2 sv = S[(uint64_t)(c0 + c) * N + p];
+        v = E ? cmul(cmul(cconj(sv), cconj(E[p])), v) : cmul(v, cconj(sv));
+      }
+      Rimg[(uint64_t)b * N + p] = v;
     }
-    Rimg[(uint64_t)b * N + p] = v;
   }
 }
 
@@ -360,12 +431,13 @@ template <int LOGN>
 pg_status forward_t(const NufftGeom& g, int B, int L, const float2* x, const float2* S, int c0, const float2* E,
                     const float2* Wo, const float* deapf, const float2* tw, float2* P, float2* grids,
                     cudaStream_t s) {
-  constexpr int n = 1 << LOGN, R = kElems / n;
-  const size_t smem = fft_smem_bytes<LOGN>();
-  PG_CUDA(cudaFuncSetAttribute(k_fft_fwd_rows<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  PG_CUDA(cudaFuncSetAttribute(k_fft_fwd_cols<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  PG_LAUNCH(k_fft_fwd_rows<LOGN>, dim3(ceil_div(g.Nx, R), B), kThreads, smem, s, g, L, x, S, c0, E, Wo, deapf, tw, P);
-  PG_LAUNCH(k_fft_fwd_cols<LOGN>, dim3(n / R, B), kThreads, smem, s, g, P, tw, grids);
+  using RG = RowGeo<LOGN>;
+  using CG = ColGeo<LOGN>;
+  PG_CUDA(cudaFuncSetAttribute(k_fft_fwd_rows<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RG::smem));
+  PG_CUDA(cudaFuncSetAttribute(k_fft_fwd_cols<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CG::smem));
+  PG_LAUNCH(k_fft_fwd_rows<LOGN>, dim3(ceil_div(g.Nx, RG::RB), B), kT, RG::smem, s, g, L, x, S, c0, E, Wo, deapf, tw,
+            P);
+  PG_LAUNCH(k_fft_fwd_cols<LOGN>, dim3(CG::n / CG::CB, B), kT, CG::smem, s, g, P, tw, grids);
   return PG_OK;
 }
 
@@ -373,13 +445,13 @@ template <int LOGN>
 pg_status adjoint_t(const NufftGeom& g, int B, int L, const float2* grids, const float2* S, int c0, const float2* E,
                     const float2* WoH, const float* deapf, const float2* tw, float2* Q, float2* Rimg,
                     cudaStream_t s) {
-  constexpr int n = 1 << LOGN, R = kElems / n;
-  const size_t smem = fft_smem_bytes<LOGN>();
-  PG_CUDA(cudaFuncSetAttribute(k_fft_inv_cols<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  PG_CUDA(cudaFuncSetAttribute(k_fft_inv_rows<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  PG_LAUNCH(k_fft_inv_cols<LOGN>, dim3(n / R, B), kThreads, smem, s, g, grids, tw, Q);
-  PG_LAUNCH(k_fft_inv_rows<LOGN>, dim3(ceil_div(g.Nx, R), B), kThreads, smem, s, g, L, Q, S, c0, E, WoH, deapf, tw,
-            Rimg);
+  using RG = RowGeo<LOGN>;
+  using CG = ColGeo<LOGN>;
+  PG_CUDA(cudaFuncSetAttribute(k_fft_inv_cols<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CG::smem));
+  PG_CUDA(cudaFuncSetAttribute(k_fft_inv_rows<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RG::smem));
+  PG_LAUNCH(k_fft_inv_cols<LOGN>, dim3(CG::n / CG::CB, B), kT, CG::smem, s, g, grids, tw, Q);
+  PG_LAUNCH(k_fft_inv_rows<LOGN>, dim3(ceil_div(g.Nx, RG::RB), B), kT, RG::smem, s, g, L, Q, S, c0, E, WoH, deapf,
+            tw, Rimg);
   return PG_OK;
 }
 
@@ -388,6 +460,9 @@ int log2_exact(int v) {
   while ((1 << l) < v) ++l;
   return ((1 << l) == v) ? l : -1;
 }
+
+// R2 of the factorisation n = R1 * R2 (Split above).
+int split_r2(int n) { return n == 1024 ? 32 : n / 16; }
 
 }  // namespace
 
@@ -398,13 +473,14 @@ bool fft2d_supported(const NufftGeom& g) {
 }
 
 pg_status fft2d_twiddles(const NufftGeom& g, DevBuf<float2>* tw, cudaStream_t s) {
-  const int n = g.Gx;
+  const int n = g.Gx, R2 = split_r2(n), R1 = n / R2;
   std::vector<float2> h(n);
   const double two_pi = 6.283185307179586476925286766559;
-  for (int k = 0; k < n; ++k) {
-    const double a = -two_pi * (double)k / (double)n;
-    h[k] = make_float2((float)std::cos(a), (float)std::sin(a));
-  }
+  for (int k1 = 0; k1 < R1; ++k1)
+    for (int m2 = 0; m2 < R2; ++m2) {
+      const double a = -two_pi * (double)(k1 * m2) / (double)n;
+      h[k1 * R2 + m2] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
   return tw->upload(h.data(), h.size(), s);
 }
 
