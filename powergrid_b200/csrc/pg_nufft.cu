@@ -229,69 +229,6 @@ __global__ void k_adjoint_prep(uint64_t n4, float4* __restrict__ grids, int nb, 
     }
 }
 
-// ---------------------------------------------------------------------------
-// Warp butterfly reduce-scatter of V = 2^p floats per lane: afterwards lane L
-// holds the warp-wide sum of value index (L >> (5 - p)) & (V - 1).
-// ---------------------------------------------------------------------------
-template <int V>
-__device__ __forceinline__ float warp_reduce_scatter(float (&v)[V], int lane) {
-  int n = V;
-#pragma unroll
-  for (int o = 16; o >= 1; o >>= 1) {
-    if (n > 1) {
-      const bool upper = (lane & o) != 0;
-#pragma unroll
-      for (int i = 0; i < V / 2; ++i) {
-        if (i < n / 2) {
-          const float send = upper ? v[i] : v[i + n / 2];
-          const float keep = upper ? v[i + n / 2] : v[i];
-          v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
-        }
-      }
-      n >>= 1;
-    } else {
-      v[0] += __shfl_xor_sync(0xffffffffu, v[0], o);
-    }
-  }
-  return v[0];
-}
-
-template <int V>
-__host__ __device__ constexpr int log2c() {
-  return V <= 1 ? 0 : V <= 2 ? 1 : V <= 4 ? 2 : V <= 8 ? 3 : V <= 16 ? 4 : 5;
-}
-
-// ---------------------------------------------------------------------------
-// Forward interpolation, tiled: one block per (subproblem, coil chunk).
-// The padded tiles of the subproblem's KP segment grids for CC coils are
-// staged in shared memory ([c][j][re|im][PZ][PX][PY], PY = 8 mod 32).  A
-// warp interpolates 4 samples at a time: lane = (y-tap, sample), each lane
-// walks its sample's 8 x-taps (x 8 z-taps in 3-D) for every (coil, segment)
-// plane, then the 8 lanes of a sample combine their partial sums with a
-// 3-level butterfly and the segment interpolator AA is applied per coil.
-// ---------------------------------------------------------------------------
-template <int V>
-__device__ __forceinline__ void group8_reduce_scatter(float (&v)[V], int lane) {
-  int n = V;
-#pragma unroll
-  for (int o = 4; o >= 1; o >>= 1) {
-    if (n > 1) {
-      const bool upper = (lane & o) != 0;
-#pragma unroll
-      for (int i = 0; i < V / 2; ++i) {
-        if (i < n / 2) {
-          const float send = upper ? v[i] : v[i + n / 2];
-          const float keep = upper ? v[i + n / 2] : v[i];
-          v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
-        }
-      }
-      n >>= 1;
-    } else {
-      v[0] += __shfl_xor_sync(0xffffffffu, v[0], o);
-    }
-  }
-}
-
 // Padded extent along y (the fastest axis) such that 4 x-rows of 8 y-taps
 // land in 32 distinct banks: PY = 8 or 24 (mod 32).
 __host__ __device__ constexpr int padded_y(int T) {
@@ -331,8 +268,19 @@ __device__ __forceinline__ int next_item(unsigned* q, int nitems) {
   return item;
 }
 
+// ---------------------------------------------------------------------------
+// Forward interpolation, tiled: one block per (subproblem, coil chunk).  The
+// padded tiles of the subproblem's KP segment grids for CC coils are staged in
+// shared memory as complex cells ([c][j][PZ][PX][PY]).  Then one thread per
+// sample reads its 8^d cells of every (coil, segment) plane and sums them in
+// the reference's order (x outer, y inner, gridding.cpp:275-289) with paired
+// fma; no cross-lane reduction is needed, and consecutive samples of a warp
+// often share their window (spiral readouts are oversampled along the arm),
+// so their shared-memory reads broadcast.  The segment interpolator AA is
+// applied per coil on the way out.
+// ---------------------------------------------------------------------------
 template <int DIM, int T, int CC, int KP>
-__global__ void __launch_bounds__(256) k_gather(NufftGeom g, TileShape t, const int4* __restrict__ sub,
+__global__ void __launch_bounds__(128) k_gather(NufftGeom g, TileShape t, const int4* __restrict__ sub,
                                                 const uint2* __restrict__ start, const float* __restrict__ wxy,
                                                 const float* __restrict__ wz, const uint32_t* __restrict__ perm,
                                                 const float2* __restrict__ aa, int K, int L,
@@ -340,10 +288,7 @@ __global__ void __launch_bounds__(256) k_gather(NufftGeom g, TileShape t, const 
                                                 float2* __restrict__ data, uint64_t dstride) {
   using TG = TileGeo<DIM, T>;
   constexpr int CELLS = TG::CELLS, PY = TG::PY, PX = TG::PX, PLANE = TG::PLANE;
-  constexpr int V = 2 * CC * KP;                 // accumulators per sample
-  constexpr int PER = (V >= 8) ? V / 8 : 1;      // values a lane holds after the group butterfly
   extern __shared__ __align__(16) float2 sm2[];   // [c*KP + j][PZ][PX][PY] complex cells
-  __shared__ float red[8][4][V];
   const int4 sp = sub[blockIdx.x];
   const int cfirst = blockIdx.y * CC;
   const int ncl = min(CC, Cb - cfirst);
@@ -371,74 +316,59 @@ __global__ void __launch_bounds__(256) k_gather(NufftGeom g, TileShape t, const 
       }
   }
   __syncthreads();
-
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  constexpr int NW = 8;
-  const int dy = lane & 7, grp = lane >> 3;
   const int end = first + count;
-  for (int s0 = first + 4 * warp; s0 < end; s0 += 4 * NW) {
-    const int s = s0 + grp;
-    float2 acc2[CC * KP];
+  for (int s = first + threadIdx.x; s < end; s += blockDim.x) {
+    const uint2 st = start[s];
+    const int ox = (int)(st.x & 0xffff) - x0, oy = (int)(st.x >> 16) - y0;
+    const float4* w4 = reinterpret_cast<const float4*>(wxy + (uint64_t)s * 16);
+    const float4 wa = w4[0], wb = w4[1], wc = w4[2], wd = w4[3];
+    const float wxr[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
+    const float wyr[8] = {wc.x, wc.y, wc.z, wc.w, wd.x, wd.y, wd.z, wd.w};
+    float2 acc[CC * KP];
 #pragma unroll
-    for (int i = 0; i < CC * KP; ++i) acc2[i] = make_float2(0.f, 0.f);
-    if (s < end) {
-      const uint2 st = start[s];
-      const int ox = (int)(st.x & 0xffff) - x0, oy = (int)(st.x >> 16) - y0;
-      const float4* w4 = reinterpret_cast<const float4*>(wxy + (uint64_t)s * 16);
-      const float4 wa = w4[0], wb = w4[1];
-      const float wxr[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
-      const float wyv = wxy[(uint64_t)s * 16 + 8 + dy];
-      const float2* base = sm2 + ox * PY + oy + dy;
-      if (DIM == 2) {
+    for (int i = 0; i < CC * KP; ++i) acc[i] = make_float2(0.f, 0.f);
+    const float2* base = sm2 + ox * PY + oy;
+    if (DIM == 2) {
 #pragma unroll
-        for (int r = 0; r < 8; ++r) {
-          const float wr = wxr[r] * wyv;
-          const float2 w2 = make_float2(wr, wr);
+      for (int r = 0; r < 8; ++r)
 #pragma unroll
-          for (int cj = 0; cj < CC * KP; ++cj) acc2[cj] = __ffma2_rn(w2, base[cj * CELLS + r * PY], acc2[cj]);
+        for (int d = 0; d < 8; ++d) {
+          const float w = wxr[r] * wyr[d];
+          const float2 w2 = make_float2(w, w);
+#pragma unroll
+          for (int cj = 0; cj < CC * KP; ++cj) acc[cj] = __ffma2_rn(w2, base[cj * CELLS + r * PY + d], acc[cj]);
         }
-      } else {
-        const int oz = (int)st.y - z0;
-        const float* wzz = wz + (uint64_t)s * 8;
-        const float2* bz = base + oz * PLANE;
-#pragma unroll 1
-        for (int e = 0; e < 8; ++e, bz += PLANE) {
-          const float wze = wzz[e];
-#pragma unroll
-          for (int r = 0; r < 8; ++r) {
-            const float wr = wxr[r] * wyv * wze;
-            const float2 w2 = make_float2(wr, wr);
-#pragma unroll
-            for (int cj = 0; cj < CC * KP; ++cj) acc2[cj] = __ffma2_rn(w2, bz[cj * CELLS + r * PY], acc2[cj]);
-          }
-        }
-      }
-    }
-    float acc[V];
-#pragma unroll
-    for (int i = 0; i < CC * KP; ++i) { acc[2 * i] = acc2[i].x; acc[2 * i + 1] = acc2[i].y; }
-    group8_reduce_scatter<V>(acc, lane);
-    // lane dy of a group now holds values [PER*dy', PER*dy'+PER) (dy' = dy for
-    // V >= 8; for V < 8 the low lanes hold the V values)
-    if (V >= 8) {
-#pragma unroll
-      for (int i = 0; i < PER; ++i) red[warp][grp][PER * dy + i] = acc[i];
     } else {
-      constexpr int sh = (V >= 8) ? 0 : 3 - log2c<V>();
-      if ((dy & ((1 << sh) - 1)) == 0) red[warp][grp][(dy >> sh) & (V - 1)] = acc[0];
-    }
-    __syncwarp();
-    const int og = lane >> 3, oc = lane & 7;
-    const int so = s0 + og;
-    if (oc < ncl && so < end) {
-      float2 out = make_float2(0.f, 0.f);
-      for (int j = 0; j < K; ++j) {
-        const float2 a = make_float2(red[warp][og][2 * (oc * KP + j)], red[warp][og][2 * (oc * KP + j) + 1]);
-        out = aa ? cadd(out, cmul(a, aa[(uint64_t)so * K + j])) : a;
+      const int oz = (int)st.y - z0;
+      const float* wzz = wz + (uint64_t)s * 8;
+      const float2* bz = base + oz * PLANE;
+#pragma unroll 1
+      for (int e = 0; e < 8; ++e, bz += PLANE) {
+        const float wze = wzz[e];
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+#pragma unroll
+          for (int d = 0; d < 8; ++d) {
+            const float w = wxr[r] * wyr[d] * wze;
+            const float2 w2 = make_float2(w, w);
+#pragma unroll
+            for (int cj = 0; cj < CC * KP; ++cj) acc[cj] = __ffma2_rn(w2, bz[cj * CELLS + r * PY + d], acc[cj]);
+          }
       }
-      data[(uint64_t)(cfirst + oc) * dstride + perm[so]] = out;
     }
-    __syncwarp();
+    const uint32_t o = perm[s];
+#pragma unroll
+    for (int c = 0; c < CC; ++c) {
+      if (c >= ncl) break;
+      float2 out = acc[c * KP];
+      if (aa) {
+        out = cmul(acc[c * KP], aa[(uint64_t)s * K]);
+#pragma unroll
+        for (int j = 1; j < KP; ++j)
+          if (j < K) out = cadd(out, cmul(acc[c * KP + j], aa[(uint64_t)s * K + j]));
+      }
+      data[(uint64_t)(cfirst + c) * dstride + o] = out;
+    }
   }
 }
 
@@ -1119,7 +1049,8 @@ static pg_status ensure_queue(NufftPlan* p, cudaStream_t s) {
 }
 
 // Tiled gather launch: choose the padded segment count KP and the coils per
-// block CC so that the staged tiles fit in shared memory and 2*CC*KP <= 32.
+// block CC so that the staged tiles fit in shared memory and the per-thread
+// accumulators (2*CC*KP floats) stay at most 32.
 template <int DIM, int T, int CC, int KP>
 static pg_status gather_launch_one(NufftPlan* p, const Binning* bin, const float2* aa, int nb, float2* y,
                                    uint64_t dstride, cudaStream_t s) {
@@ -1127,7 +1058,7 @@ static pg_status gather_launch_one(NufftPlan* p, const Binning* bin, const float
   PG_CUDA(cudaFuncSetAttribute(k_gather<DIM, T, CC, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   // a static grid: the persistent work-queue form measured ~4 % slower here
   dim3 grid(bin->nsub, ceil_div(nb, CC));
-  PG_LAUNCH((k_gather<DIM, T, CC, KP>), grid, 256, smem, s, p->g, bin->tile, bin->subprob.p, bin->start.p,
+  PG_LAUNCH((k_gather<DIM, T, CC, KP>), grid, 128, smem, s, p->g, bin->tile, bin->subprob.p, bin->start.p,
             bin->wxy.p, bin->wz.p, bin->perm.p, aa, bin->K, bin->L, p->work->grids.p, nb, y, dstride);
   return PG_OK;
 }
