@@ -159,6 +159,19 @@ class Gdft : public Operator {
   }
 };
 
+template <typename T1>
+class GdftR2 : public Operator {
+ public:
+  template <typename RCol>
+  GdftR2(uword nk, uword ni, const RCol& k1, const RCol& k2, const RCol& k3, const RCol& i1, const RCol& i2,
+         const RCol& i3, const RCol& FM, const RCol& t, int num_x, int num_y, int num_z) {
+    pg_op h = nullptr;
+    check(pg_gdftr2_create(&h, nk, ni, detail::ptr(k1), detail::ptr(k2), detail::ptr(k3), detail::ptr(i1),
+                           detail::ptr(i2), detail::ptr(i3), detail::ptr(FM), detail::ptr(t), num_x, num_y, num_z));
+    adopt(h);
+  }
+};
+
 template <typename T1, typename Tobj>
 class TimeSegmentation : public Operator {
  public:

@@ -71,6 +71,15 @@ pg_status pg_gdft_create(pg_op* out, uint64_t nk, uint64_t ni, const float* kx, 
                          const float* kz, const float* ix, const float* iy, const float* iz,
                          const float* field_map, const float* t);
 
+/* GdftR2(nk, ni, kx, ky, kz, ix, iy, iz, FM, t, num_x, num_y, num_z) replaces
+ * GdftR2<float>::GdftR2 (GdftR2.h, GdftR2.cpp:32-57): Gdft with each
+ * sample-voxel pair weighted by sinc(kx/Nx + Gx t) sinc(ky/Ny + Gy t)
+ * sinc(kz/Nz + Gz t), G* the field map's differences (GdftR2.cpp:62-110,
+ * ftCpuWithGrads.cpp:93-216).  nx*ny*nz must equal ni. */
+pg_status pg_gdftr2_create(pg_op* out, uint64_t nk, uint64_t ni, const float* kx, const float* ky, const float* kz,
+                           const float* ix, const float* iy, const float* iz, const float* field_map, const float* t,
+                           uint64_t nx, uint64_t ny, uint64_t nz);
+
 /* TimeSegmentation(G, fieldmap, tvec, n1 = data length, n2 = image length, L,
  * interptype, shots) replaces TimeSegmentation<float, Tobj>::TimeSegmentation
  * (TimeSegmentation.h:70-71, TimeSegmentation.cpp:37-221).  G is not owned

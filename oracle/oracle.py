@@ -44,6 +44,8 @@ def lib() -> C.CDLL:
         L.orc_gnufft_new.argtypes = [C.c_int, U64, C.c_float, U64, U64, U64, P, P, P]
         L.orc_gdft_new.restype = P
         L.orc_gdft_new.argtypes = [C.c_int, U64, U64] + [P] * 8
+        L.orc_gdftr2_new.restype = P
+        L.orc_gdftr2_new.argtypes = [C.c_int, U64, U64] + [P] * 8 + [U64, U64, U64]
         L.orc_timeseg_new.restype = P
         L.orc_timeseg_new.argtypes = [P, P, P, U64, U64, U64, U64, U64, C.c_int]
         L.orc_sense_new.restype = P
@@ -176,6 +178,12 @@ def gnufft(prec, M, nx, ny, nz, kx, ky, kz, gridos=2.0) -> Op:
 def gdft(prec, kx, ky, kz, ix, iy, iz, fm, t) -> Op:
     a = [_f32(v) for v in (kx, ky, kz, ix, iy, iz, fm, t)]
     return Op(lib().orc_gdft_new(prec, a[0].size, a[3].size, *[_p(v) for v in a]), prec)
+
+
+def gdftr2(prec, kx, ky, kz, ix, iy, iz, fm, t, nx, ny, nz) -> Op:
+    """GdftR2 (GdftR2.cpp:32-150); prec 2 = FP64 DFT and sinc."""
+    a = [_f32(v) for v in (kx, ky, kz, ix, iy, iz, fm, t)]
+    return Op(lib().orc_gdftr2_new(prec, a[0].size, a[3].size, *[_p(v) for v in a], nx, ny, nz), prec)
 
 
 def timeseg(G: Op, fm, t, n1, n2, L, interptype=1, shots=1, tables64=False) -> Op:

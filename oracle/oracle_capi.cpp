@@ -161,12 +161,14 @@ int orc_use_reference(const char* so_path) {
   kd.fh = (decltype(kd.fh))dlsym(h, "pgref_fh_d");
   kd.ft = (decltype(kd.ft))dlsym(h, "pgref_ft_d");
   kd.ift = (decltype(kd.ift))dlsym(h, "pgref_ift_d");
+  kf.ftg = (decltype(kf.ftg))dlsym(h, "pgref_ftg_f");
+  kf.iftg = (decltype(kf.iftg))dlsym(h, "pgref_iftg_f");
   kf.ifwd = (decltype(kf.ifwd))dlsym(h, "pgref_ifwd_f");
   kf.iadj = (decltype(kf.iadj))dlsym(h, "pgref_iadj_f");
   kd.ifwd = (decltype(kd.ifwd))dlsym(h, "pgref_ifwd_d");
   kd.iadj = (decltype(kd.iadj))dlsym(h, "pgref_iadj_d");
   if (!kf.fd || !kf.fh || !kf.ft || !kf.ift || !kd.fd || !kd.fh || !kd.ft || !kd.ift || !kf.ifwd || !kf.iadj ||
-      !kd.ifwd || !kd.iadj) {
+      !kd.ifwd || !kd.iadj || !kf.ftg || !kf.iftg) {
     g_err = "libpgref.so lacks an expected symbol";
     return -1;
   }
@@ -235,6 +237,29 @@ void* orc_gdft_new(int prec, u64 nk, u64 ni, const float* kx, const float* ky, c
 }
 
 // tables64: min-max / histogram tables built in double and rounded (float handles only)
+// prec: 0 float, 1 double (reference formula), 2 double with the FP64 DFT
+void* orc_gdftr2_new(int prec, u64 nk, u64 ni, const float* kx, const float* ky, const float* kz, const float* ix,
+                     const float* iy, const float* iz, const float* fm, const float* t, u64 nx, u64 ny, u64 nz) {
+  return guard([&]() -> void* {
+    auto* h = new Handle;
+    h->prec = prec;
+    if (prec == 0) {
+      auto* op = new pgo::GdftR2Op<float>(nk, ni, kx, ky, kz, ix, iy, iz, fm, t, (int)nx, (int)ny, (int)nz);
+      op->use_ref = g_use_ref;
+      h->f.reset(op);
+    } else {
+      auto a = widen<double>(kx, nk), b = widen<double>(ky, nk), c = widen<double>(kz, nk);
+      auto d = widen<double>(ix, ni), e = widen<double>(iy, ni), f = widen<double>(iz, ni);
+      auto g = widen<double>(fm, ni), tt = widen<double>(t, nk);
+      auto* op = new pgo::GdftR2Op<double>(nk, ni, a.data(), b.data(), c.data(), d.data(), e.data(), f.data(),
+                                           g.data(), tt.data(), (int)nx, (int)ny, (int)nz);
+      op->exact64 = (prec == 2);
+      h->d.reset(op);
+    }
+    return h;
+  });
+}
+
 void* orc_timeseg_new(void* G, const float* fieldmap, const float* tvec, u64 n1, u64 n2, u64 L, u64 type,
                       u64 shots, int tables64) {
   return guard([&]() -> void* {

@@ -11,6 +11,7 @@
 //   SENSE               SENSE.cpp:33-97
 //   pcSenseTimeSeg      pcSenseTimeSeg.cpp:41-171
 //   pcSENSE             pcSENSE.cpp:40-153
+//   GdftR2              GdftR2.cpp:32-150, ftCpuWithGrads.cpp:76-216
 //   spatial interpolation, density compensation   Gnufft.cpp:213-337, reconSupport/directRecon.cpp:28-73
 //   Robject/Quad/TV     Robject.cpp:49-193, QuadPenalty.cpp:45-64, TVPenalty.cpp:43-68
 //   solve_pwls_pcg      solve_pwls_pcg.hpp:34-167
@@ -377,6 +378,11 @@ struct RefKernels {
              const T*, const T*, int, int) = nullptr;
   void (*ift)(T*, T*, const T*, const T*, const T*, const T*, const T*, const T*, const T*, const T*,
               const T*, const T*, int, int) = nullptr;
+  // ftCpuWithGrads / iftCpuWithGrads wrappers
+  void (*ftg)(T*, T*, const T*, const T*, const T*, const T*, const T*, const T*, const T*, const T*, const T*,
+              const T*, const T*, const T*, const T*, int, int, int, int, int) = nullptr;
+  void (*iftg)(T*, T*, const T*, const T*, const T*, const T*, const T*, const T*, const T*, const T*, const T*,
+               const T*, const T*, const T*, const T*, int, int, int, int, int) = nullptr;
   // forwardSpatialInterp / adjointSpatialInterp bodies
   void (*ifwd)(int, const T*, const T*, const T*, const T*, u64, int, int, int, T, T, T, const T*, u64, T*) = nullptr;
   void (*iadj)(int, const T*, const T*, const T*, const T*, u64, int, int, int, T, T, T, const T*, u64, T*) = nullptr;
@@ -601,6 +607,133 @@ struct GdftOp : Op<T> {
           T co = cosf(e);
           sr += (co * yr[i]) - (s * yi[i]);
           si += (s * yr[i]) + (co * yi[i]);
+        }
+        xr[j] = sr; xi[j] = si;
+      }
+    }
+    for (u64 j = 0; j < ni; ++j) x[j] = C(xr[j], xi[j]);
+  }
+};
+
+// GdftR2 (GdftR2.cpp:32-150): Gdft with per-pair through-voxel dephasing
+// factors from the field map's differences (ftCpuWithGrads.cpp:76-216).
+template <typename T>
+struct GdftR2Op : GdftOp<T> {
+  using C = std::complex<T>;
+  std::vector<T> gx, gy, gz;
+  int nx, ny, nz;
+  // sincPG (ftCpuWithGrads.cpp:76-84): the product with the float MRI_PI and
+  // sin in T (the overload for T; checked bit for bit against the compiled
+  // reference)
+  static T sinc_pg(T x) {
+    if (std::fabs((double)x) < 0.0001) return (T)1.0;
+    return (T)(std::sin(kPiF * x) / (kPiF * x));
+  }
+  static double sinc64(double x) { return std::fabs(x) < 0.0001 ? 1.0 : std::sin(kPiD * x) / (kPiD * x); }
+  // Cd of GdftR2.cpp:72-110
+  std::vector<T> cd(u64 off) const {
+    const u64 N = (u64)nx * ny * nz;
+    std::vector<T> out(N, (T)0);
+    for (u64 ii = off; ii < N - off; ++ii) out[ii] = this->fm[ii + off] - this->fm[ii - off];
+    for (u64 ii = 0; ii < off; ++ii) out[ii] = this->fm[ii + off] - this->fm[ii];
+    for (u64 ii = N - off; ii < N; ++ii) out[ii] = this->fm[ii] - this->fm[ii - off];
+    return out;
+  }
+  GdftR2Op(u64 nk, u64 ni, const T* k1, const T* k2, const T* k3, const T* i1, const T* i2, const T* i3, const T* f,
+           const T* tt, int x, int y, int z)
+      : GdftOp<T>(nk, ni, k1, k2, k3, i1, i2, i3, f, tt), nx(x), ny(y), nz(z) {
+    gx = cd(1);
+    gy = cd((u64)ny);
+    gz = cd((u64)nx * ny);
+  }
+  void forward(const C* xin, C* y) const override {
+    const u64 nk = this->n1, ni = this->n2;
+    std::vector<T> xr(ni), xi(ni), yr(nk, 0), yi(nk, 0);
+    for (u64 j = 0; j < ni; ++j) { xr[j] = xin[j].real(); xi[j] = xin[j].imag(); }
+    const auto& kx = this->kx; const auto& ky = this->ky; const auto& kz = this->kz;
+    const auto& ix = this->ix; const auto& iy = this->iy; const auto& iz = this->iz;
+    const auto& fm = this->fm; const auto& t = this->t;
+    if (this->use_ref && ref_kernels<T>().ftg && !this->exact64) {
+      ref_kernels<T>().ftg(yr.data(), yi.data(), xr.data(), xi.data(), kx.data(), ky.data(), kz.data(), ix.data(),
+                           iy.data(), iz.data(), fm.data(), gx.data(), gy.data(), gz.data(), t.data(), (int)nk,
+                           (int)ni, nx, ny, nz);
+    } else if (this->exact64) {
+      const double tpi = 2.0 * kPiD;
+      for (u64 i = 0; i < nk; ++i) {
+        double sr = 0, si = 0;
+        for (u64 j = 0; j < ni; ++j) {
+          const double ph = tpi * ((double)kx[i] * ix[j] + (double)ky[i] * iy[j] + (double)kz[i] * iz[j]) +
+                            (double)fm[j] * t[i];
+          const double b = sinc64((double)kx[i] / nx + (double)gx[j] * t[i]) *
+                           sinc64((double)ky[i] / ny + (double)gy[j] * t[i]) *
+                           sinc64((double)kz[i] / nz + (double)gz[j] * t[i]);
+          const double s = std::sin(ph), c = std::cos(ph);
+          sr += b * (c * xr[j] + s * xi[j]);
+          si += b * (-s * xr[j] + c * xi[j]);
+        }
+        yr[i] = (T)sr; yi[i] = (T)si;
+      }
+    } else {
+      // ftCpuWithGrads.cpp:115-138
+      for (u64 i = 0; i < nk; ++i) {
+        T sr = 0.0, si = 0.0;
+        T a = kx[i] * 2 * kPiF, b = ky[i] * 2 * kPiF, c = kz[i] * 2 * kPiF;
+        T ti = t[i];
+        for (u64 j = 0; j < ni; ++j) {
+          T e = (a * ix[j] + b * iy[j] + c * iz[j] + (fm[j] * ti));
+          float s = sinf(e);
+          float co = cosf(e);
+          T bf = sinc_pg(kx[i] / nx + gx[j] * ti) * sinc_pg(ky[i] / ny + gy[j] * ti) * sinc_pg(kz[i] / nz + gz[j] * ti);
+          sr += bf * ((co * xr[j]) + (s * xi[j]));
+          si += bf * ((-s * xr[j]) + (co * xi[j]));
+        }
+        yr[i] = sr; yi[i] = si;
+      }
+    }
+    for (u64 i = 0; i < nk; ++i) y[i] = C(yr[i], yi[i]);
+  }
+  void adjoint(const C* yin, C* x) const override {
+    const u64 nk = this->n1, ni = this->n2;
+    std::vector<T> yr(nk), yi(nk), xr(ni, 0), xi(ni, 0);
+    for (u64 i = 0; i < nk; ++i) { yr[i] = yin[i].real(); yi[i] = yin[i].imag(); }
+    const auto& kx = this->kx; const auto& ky = this->ky; const auto& kz = this->kz;
+    const auto& ix = this->ix; const auto& iy = this->iy; const auto& iz = this->iz;
+    const auto& fm = this->fm; const auto& t = this->t;
+    if (this->use_ref && ref_kernels<T>().iftg && !this->exact64) {
+      ref_kernels<T>().iftg(xr.data(), xi.data(), yr.data(), yi.data(), kx.data(), ky.data(), kz.data(), ix.data(),
+                            iy.data(), iz.data(), fm.data(), gx.data(), gy.data(), gz.data(), t.data(), (int)nk,
+                            (int)ni, nx, ny, nz);
+    } else if (this->exact64) {
+      const double tpi = 2.0 * kPiD;
+      for (u64 j = 0; j < ni; ++j) {
+        double sr = 0, si = 0;
+        for (u64 i = 0; i < nk; ++i) {
+          const double ph = tpi * ((double)kx[i] * ix[j] + (double)ky[i] * iy[j] + (double)kz[i] * iz[j]) +
+                            (double)fm[j] * t[i];
+          const double b = sinc64((double)kx[i] / nx + (double)gx[j] * t[i]) *
+                           sinc64((double)ky[i] / ny + (double)gy[j] * t[i]) *
+                           sinc64((double)kz[i] / nz + (double)gz[j] * t[i]);
+          const double s = std::sin(ph), c = std::cos(ph);
+          sr += b * (c * yr[i] - s * yi[i]);
+          si += b * (s * yr[i] + c * yi[i]);
+        }
+        xr[j] = (T)sr; xi[j] = (T)si;
+      }
+    } else {
+      // ftCpuWithGrads.cpp:164-212
+      T tpi = kPiF * 2.0;
+      for (u64 j = 0; j < ni; ++j) {
+        T sr = 0.0, si = 0.0;
+        T ax = ix[j] * tpi, ay = iy[j] * tpi, az = iz[j] * tpi;
+        T f = fm[j];
+        for (u64 i = 0; i < nk; ++i) {
+          T e = (kx[i] * ax + ky[i] * ay + kz[i] * az + (f * t[i]));
+          T s = sinf(e);
+          T co = cosf(e);
+          T bf = sinc_pg(kx[i] / nx + gx[j] * t[i]) * sinc_pg(ky[i] / ny + gy[j] * t[i]) *
+                 sinc_pg(kz[i] / nz + gz[j] * t[i]);
+          sr += bf * ((co * yr[i]) - (s * yi[i]));
+          si += bf * ((s * yr[i]) + (co * yi[i]));
         }
         xr[j] = sr; xi[j] = si;
       }

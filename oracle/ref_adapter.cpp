@@ -10,6 +10,7 @@
 // Gdft does (Gdft.cpp:78-80, 120-122).  Nothing here re-implements the math.
 #include "gridding.h"
 #include "ftCpu.h"
+#include "ftCpuWithGrads.h"
 
 #include <cmath>
 #include <cstring>
@@ -185,6 +186,18 @@ void pgref_ift_d(double* ir, double* ii, const double* kr, const double* ki, con
                  const double* ky, const double* kz, const double* ix, const double* iy, const double* iz,
                  const double* fm, const double* t, int nk, int ni) {
   iftCpu<double>(ir, ii, kr, ki, kx, ky, kz, ix, iy, iz, fm, t, nk, ni);
+}
+
+// ftCpuWithGrads / iftCpuWithGrads (ftCpuWithGrads.cpp:93-216), planar like GdftR2.cpp:116-150.
+void pgref_ftg_f(float* kr, float* ki, const float* ir, const float* ii, const float* kx, const float* ky,
+                 const float* kz, const float* ix, const float* iy, const float* iz, const float* fm, const float* gx,
+                 const float* gy, const float* gz, const float* t, int nk, int ni, int nx, int ny, int nz) {
+  ftCpuWithGrads<float>(kr, ki, ir, ii, kx, ky, kz, ix, iy, iz, fm, gx, gy, gz, t, nk, ni, nx, ny, nz);
+}
+void pgref_iftg_f(float* ir, float* ii, const float* kr, const float* ki, const float* kx, const float* ky,
+                  const float* kz, const float* ix, const float* iy, const float* iz, const float* fm, const float* gx,
+                  const float* gy, const float* gz, const float* t, int nk, int ni, int nx, int ny, int nz) {
+  iftCpuWithGrads<float>(ir, ii, kr, ki, kx, ky, kz, ix, iy, iz, fm, gx, gy, gz, t, nk, ni, nx, ny, nz);
 }
 
 }  // extern "C"

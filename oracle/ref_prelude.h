@@ -1,8 +1,8 @@
 /* ORACLE / TEST INFRASTRUCTURE ONLY.
  *
  * Forced-include prelude (g++ -include) for compiling the reference's own
- * PowerGrid/gridding.cpp, griddingSupport.cpp, ftCpu.cpp and fftCPU.cpp in
- * place, unmodified, without Armadillo:
+ * PowerGrid/gridding.cpp, griddingSupport.cpp, ftCpu.cpp, fftCPU.cpp and
+ * ftCpuWithGrads.cpp in place, unmodified, without Armadillo:
  *   - PGINCLUDES_H is pre-defined so PGIncludes.h (which includes
  *     <armadillo>, PGIncludes.h:26-42) is skipped;
  *   - the few names those four files take from it are supplied here:

@@ -58,6 +58,7 @@ SIGNATURES = {
     "pg_kernel_launch_count": (U64, []),
     "pg_gnufft_create": (C.c_int, [C.POINTER(P), U64, F32, U64, U64, U64, P, P, P]),
     "pg_gdft_create": (C.c_int, [C.POINTER(P), U64, U64, P, P, P, P, P, P, P, P]),
+    "pg_gdftr2_create": (C.c_int, [C.POINTER(P), U64, U64, P, P, P, P, P, P, P, P, U64, U64, U64]),
     "pg_timeseg_create": (C.c_int, [C.POINTER(P), P, P, P, U64, U64, U64, U64, U64]),
     "pg_sense_create": (C.c_int, [C.POINTER(P), P, P, U64, U64, U64]),
     "pg_pcsense_timeseg_create": (C.c_int, [C.POINTER(P), P, P, P, U64, U64, U64, U64, U64, P, U64, U64, P, P, P,

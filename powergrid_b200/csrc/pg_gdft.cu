@@ -8,10 +8,17 @@
 // __sincosf serves every coil of the pair; the complex MACs are FP32 with a
 // two-level (per-tile, then running) sum.
 //
+// GdftR2 (ftCpuWithGrads.cpp:93-216) multiplies each pair by
+//   sinc(kx_i/Nx + Gx_j t_i) sinc(ky_i/Ny + Gy_j t_i) sinc(kz_i/Nz + Gz_j t_i),
+// sinc(a) = sin(pi a)/(pi a) (1 for |a| < 1e-4), Gx/Gy/Gz the field map's
+// differences (GdftR2.cpp:62-110): the same kernels with GRAD = true.
+//
 // Layout: one thread per output (sample for forward, voxel for adjoint);
 // the other side is staged in shared-memory tiles of 128 entries.  When the
 // outputs alone do not fill the GPU the inner sum is split over blockIdx.y
 // and the partial sums are combined in a fixed order (deterministic).
+#include <vector>
+
 #include "pg_gdft.cuh"
 #include "pg_profile.cuh"
 
@@ -20,6 +27,17 @@ namespace pg {
 namespace {
 constexpr int kTile = 128;
 constexpr int kCoilChunk = 8;
+
+// sincPG (ftCpuWithGrads.cpp:76-84)
+__device__ __forceinline__ float sinc_pg(float a) {
+  return fabsf(a) < 0.0001f ? 1.0f : sinpif(a) / (3.14159265358979323846f * a);
+}
+
+// The pair's through-voxel dephasing factor: kn = (kx/Nx, ky/Ny, kz/Nz, t),
+// gm = (Gx, Gy, Gz, -).
+__device__ __forceinline__ float grad_factor(float4 kn, float4 gm) {
+  return sinc_pg(kn.x + gm.x * kn.w) * sinc_pg(kn.y + gm.y * kn.w) * sinc_pg(kn.z + gm.z * kn.w);
+}
 
 __device__ __forceinline__ void phase_sincos(double ph, float* s, float* c) {
   const double inv2pi = 0.15915494309189533577;   // 1 / (2 pi)
@@ -32,18 +50,24 @@ __device__ __forceinline__ void phase_sincos(double ph, float* s, float* c) {
 
 // Forward partial sums.  ks[i] = (2pi kx, 2pi ky, 2pi kz, t); vs[j] = (ix, iy, iz, FM).
 // xin: nc x ni inputs (already multiplied by the coil maps).
-template <int NC>
+template <int NC, bool GRAD>
 __global__ void __launch_bounds__(kTile) k_dft_forward(uint64_t nk, uint64_t ni, const double4* __restrict__ ks,
                                                        const double4* __restrict__ vs,
+                                                       const float4* __restrict__ kns, const float4* __restrict__ gms,
                                                        const float2* __restrict__ xin, uint64_t jchunk,
                                                        float2* __restrict__ part) {
   __shared__ double4 sv[kTile];
   __shared__ float2 sx[NC][kTile];
+  __shared__ float4 sg[GRAD ? kTile : 1];
   const uint64_t i = (uint64_t)blockIdx.x * kTile + threadIdx.x;
   const uint64_t j0 = (uint64_t)blockIdx.y * jchunk;
   const uint64_t j1 = min(ni, j0 + jchunk);
   double4 k = make_double4(0, 0, 0, 0);
-  if (i < nk) k = ks[i];
+  float4 kn = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (i < nk) {
+    k = ks[i];
+    if (GRAD) kn = kns[i];
+  }
   float2 tot[NC];
 #pragma unroll
   for (int c = 0; c < NC; ++c) tot[c] = make_float2(0.f, 0.f);
@@ -52,6 +76,7 @@ __global__ void __launch_bounds__(kTile) k_dft_forward(uint64_t nk, uint64_t ni,
     __syncthreads();
     if (threadIdx.x < n) {
       sv[threadIdx.x] = vs[jt + threadIdx.x];
+      if (GRAD) sg[threadIdx.x] = gms[jt + threadIdx.x];
 #pragma unroll
       for (int c = 0; c < NC; ++c) sx[c][threadIdx.x] = xin[(uint64_t)c * ni + jt + threadIdx.x];
     }
@@ -64,6 +89,11 @@ __global__ void __launch_bounds__(kTile) k_dft_forward(uint64_t nk, uint64_t ni,
       const double ph = fma(k.x, v.x, fma(k.y, v.y, fma(k.z, v.z, v.w * k.w)));
       float s, co;
       phase_sincos(ph, &s, &co);
+      if (GRAD) {
+        const float b = grad_factor(kn, sg[j]);
+        s *= b;
+        co *= b;
+      }
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
         const float2 x = sx[c][j];
@@ -81,18 +111,24 @@ __global__ void __launch_bounds__(kTile) k_dft_forward(uint64_t nk, uint64_t ni,
 }
 
 // Adjoint partial sums.  yin: nc x nk data (coil-major, stride dstride).
-template <int NC>
+template <int NC, bool GRAD>
 __global__ void __launch_bounds__(kTile) k_dft_adjoint(uint64_t nk, uint64_t ni, const double4* __restrict__ ks,
                                                        const double4* __restrict__ vs,
+                                                       const float4* __restrict__ kns, const float4* __restrict__ gms,
                                                        const float2* __restrict__ yin, uint64_t dstride,
                                                        uint64_t ichunk, float2* __restrict__ part) {
   __shared__ double4 sk[kTile];
   __shared__ float2 sy[NC][kTile];
+  __shared__ float4 skn[GRAD ? kTile : 1];
   const uint64_t j = (uint64_t)blockIdx.x * kTile + threadIdx.x;
   const uint64_t i0 = (uint64_t)blockIdx.y * ichunk;
   const uint64_t i1 = min(nk, i0 + ichunk);
   double4 v = make_double4(0, 0, 0, 0);
-  if (j < ni) v = vs[j];
+  float4 gm = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (j < ni) {
+    v = vs[j];
+    if (GRAD) gm = gms[j];
+  }
   float2 tot[NC];
 #pragma unroll
   for (int c = 0; c < NC; ++c) tot[c] = make_float2(0.f, 0.f);
@@ -101,6 +137,7 @@ __global__ void __launch_bounds__(kTile) k_dft_adjoint(uint64_t nk, uint64_t ni,
     __syncthreads();
     if (threadIdx.x < n) {
       sk[threadIdx.x] = ks[it + threadIdx.x];
+      if (GRAD) skn[threadIdx.x] = kns[it + threadIdx.x];
 #pragma unroll
       for (int c = 0; c < NC; ++c) sy[c][threadIdx.x] = yin[(uint64_t)c * dstride + it + threadIdx.x];
     }
@@ -113,6 +150,11 @@ __global__ void __launch_bounds__(kTile) k_dft_adjoint(uint64_t nk, uint64_t ni,
       const double ph = fma(k.x, v.x, fma(k.y, v.y, fma(k.z, v.z, v.w * k.w)));
       float s, co;
       phase_sincos(ph, &s, &co);
+      if (GRAD) {
+        const float b = grad_factor(skn[q], gm);
+        s *= b;
+        co *= b;
+      }
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
         const float2 y = sy[c][q];
@@ -214,6 +256,35 @@ pg_status gdft_plan_same_voxels(std::unique_ptr<GdftPlan>* out, const GdftPlan& 
   return PG_OK;
 }
 
+pg_status gdft_plan_add_gradients(GdftPlan* p, const float* kx, const float* ky, const float* kz, const float* t,
+                                  const float* fm, int nx, int ny, int nz, cudaStream_t s) {
+  const uint64_t N = (uint64_t)nx * ny * nz;
+  if (nx < 1 || ny < 1 || nz < 1 || N != p->ni)
+    return set_error(PG_INVALID_ARG, "GdftR2: nx*ny*nz = %llu does not match %llu voxels", (unsigned long long)N,
+                     (unsigned long long)p->ni);
+  // field-map differences along y, x, z (GdftR2.cpp:62-110: central inside,
+  // one-sided over the first and last `offset` entries, no division)
+  auto cd = [&](uint64_t off, std::vector<float>* out) {
+    out->assign(N, 0.f);
+    if (off >= N) return;
+    for (uint64_t i = off; i < N - off; ++i) (*out)[i] = fm[i + off] - fm[i - off];
+    for (uint64_t i = 0; i < off && i < N; ++i) (*out)[i] = fm[i + off] - fm[i];
+    for (uint64_t i = N - off; i < N; ++i) (*out)[i] = fm[i] - fm[i - off];
+  };
+  std::vector<float> gx, gy, gz;
+  cd(1, &gx);
+  cd((uint64_t)ny, &gy);
+  cd((uint64_t)nx * ny, &gz);
+  std::vector<float4> gm(N), kn(p->nk);
+  for (uint64_t j = 0; j < N; ++j) gm[j] = make_float4(gx[j], gy[j], gz[j], 0.f);
+  for (uint64_t i = 0; i < p->nk; ++i)
+    kn[i] = make_float4(kx[i] / (float)nx, ky[i] / (float)ny, kz[i] / (float)nz, t[i]);
+  PG_TRY(p->gm.upload(gm.data(), N, s));
+  PG_TRY(p->kn.upload(kn.data(), p->nk, s));
+  PG_CUDA(cudaStreamSynchronize(s));
+  return PG_OK;
+}
+
 static int splits_for(uint64_t nout, uint64_t ninner) {
   const uint64_t blocks = (nout + kTile - 1) / kTile;
   const uint64_t want = (uint64_t)sm_count() * 8;
@@ -228,14 +299,24 @@ static int splits_for(uint64_t nout, uint64_t ninner) {
 template <int NC>
 static pg_status launch_fwd(GdftPlan* p, int nsplit, uint64_t jchunk, const float2* xin, float2* part, cudaStream_t s) {
   dim3 grid(ceil_div(p->nk, kTile), nsplit);
-  PG_LAUNCH(k_dft_forward<NC>, grid, kTile, 0, s, p->nk, p->ni, p->ks.p, p->vs.p, xin, jchunk, part);
+  if (p->kn.p)
+    PG_LAUNCH((k_dft_forward<NC, true>), grid, kTile, 0, s, p->nk, p->ni, p->ks.p, p->vs.p, p->kn.p, p->gm.p, xin,
+              jchunk, part);
+  else
+    PG_LAUNCH((k_dft_forward<NC, false>), grid, kTile, 0, s, p->nk, p->ni, p->ks.p, p->vs.p, nullptr, nullptr, xin,
+              jchunk, part);
   return PG_OK;
 }
 template <int NC>
 static pg_status launch_adj(GdftPlan* p, int nsplit, uint64_t ichunk, const float2* yin, uint64_t dstride,
                             float2* part, cudaStream_t s) {
   dim3 grid(ceil_div(p->ni, kTile), nsplit);
-  PG_LAUNCH(k_dft_adjoint<NC>, grid, kTile, 0, s, p->nk, p->ni, p->ks.p, p->vs.p, yin, dstride, ichunk, part);
+  if (p->kn.p)
+    PG_LAUNCH((k_dft_adjoint<NC, true>), grid, kTile, 0, s, p->nk, p->ni, p->ks.p, p->vs.p, p->kn.p, p->gm.p, yin,
+              dstride, ichunk, part);
+  else
+    PG_LAUNCH((k_dft_adjoint<NC, false>), grid, kTile, 0, s, p->nk, p->ni, p->ks.p, p->vs.p, nullptr, nullptr, yin,
+              dstride, ichunk, part);
   return PG_OK;
 }
 

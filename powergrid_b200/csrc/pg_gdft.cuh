@@ -20,6 +20,9 @@ struct GdftPlan {
   DevBuf<double4> ks;    // per sample (2pi kx, 2pi ky, 2pi kz, t)
   DevBuf<double4> vs;    // per voxel (ix, iy, iz, FM rad/s); may view another plan's
   std::shared_ptr<GdftWork> work = std::make_shared<GdftWork>();
+  // GdftR2 only: per sample (kx/Nx, ky/Ny, kz/Nz, t), per voxel (Gx, Gy, Gz, 0)
+  DevBuf<float4> kn;
+  DevBuf<float4> gm;
 };
 
 pg_status gdft_plan_create(std::unique_ptr<GdftPlan>* out, uint64_t nk, uint64_t ni, const float* kx, const float* ky,
@@ -30,6 +33,10 @@ pg_status gdft_plan_create(std::unique_ptr<GdftPlan>* out, uint64_t nk, uint64_t
 // both run on one stream).
 pg_status gdft_plan_same_voxels(std::unique_ptr<GdftPlan>* out, const GdftPlan& src, uint64_t nk, const float* kx,
                                 const float* ky, const float* kz, const float* t, cudaStream_t s);
+// Turn p into GdftR2 (GdftR2.cpp:32-110): field-map gradient maps of the
+// nx x ny x nz image and the per-pair through-voxel sinc factors.
+pg_status gdft_plan_add_gradients(GdftPlan* p, const float* kx, const float* ky, const float* kz, const float* t,
+                                  const float* fm, int nx, int ny, int nz, cudaStream_t s);
 // y_c = G (S_c x) for C coils; S may be null (C = 1).  y coil stride dstride.
 pg_status gdft_forward(GdftPlan* p, int C, const float2* S, const float2* x, float2* y, uint64_t dstride,
                        cudaStream_t s);

@@ -500,6 +500,23 @@ pg_status pg_gdft_create(pg_op* out, uint64_t nk, uint64_t ni, const float* kx, 
   return PG_OK;
 }
 
+pg_status pg_gdftr2_create(pg_op* out, uint64_t nk, uint64_t ni, const float* kx, const float* ky, const float* kz,
+                           const float* ix, const float* iy, const float* iz, const float* field_map, const float* t,
+                           uint64_t nx, uint64_t ny, uint64_t nz) {
+  if (!out || !kx || !ky || !kz || !ix || !iy || !iz || !field_map || !t)
+    return set_error(PG_INVALID_ARG, "GdftR2: null argument");
+  PG_TRY(ensure_init());
+  auto op = std::make_unique<GdftOp>();
+  op->kind = PG_OP_GDFT;
+  cudaStream_t s = default_stream();
+  PG_TRY(gdft_plan_create(&op->plan, nk, ni, kx, ky, kz, ix, iy, iz, field_map, t, s));
+  PG_TRY(gdft_plan_add_gradients(op->plan.get(), kx, ky, kz, t, field_map, (int)nx, (int)ny, (int)nz, s));
+  op->n_data = nk;
+  op->n_image = ni;
+  *out = op.release();
+  return PG_OK;
+}
+
 pg_status pg_timeseg_create(pg_op* out, pg_op G, const float* field_map, const float* tvec, uint64_t n1, uint64_t n2,
                             uint64_t L, uint64_t interptype, uint64_t shots) {
   if (!out) return set_error(PG_INVALID_ARG, "TimeSegmentation: null argument");

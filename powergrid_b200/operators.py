@@ -23,7 +23,7 @@ import numpy as np
 from . import _lib
 from ._lib import P, U64, Penalty, check
 
-__all__ = ["Gnufft", "Gdft", "TimeSegmentation", "SENSE", "pcSenseTimeSeg", "pcSENSE", "QuadPenalty", "TVPenalty",
+__all__ = ["Gnufft", "Gdft", "GdftR2", "TimeSegmentation", "SENSE", "pcSenseTimeSeg", "pcSENSE", "QuadPenalty", "TVPenalty",
            "calc3DDensityCompensation", "gridCoilImages", "calcSumOfSquaresImage", "solve_pwls_pcg", "reconSolve",
            "init"]
 
@@ -166,6 +166,18 @@ class Gdft(_Op):
         a = [_f32(v) for v in (kx, ky, kz, ix, iy, iz, FM, t)]
         h = P()
         check(_lib.load().pg_gdft_create(C.byref(h), int(nk), int(ni), *[_ptr(v) for v in a]))
+        super().__init__(h)
+
+
+class GdftR2(_Op):
+    """Field-corrected DFT with field-map gradient (through-voxel dephasing) factors
+    (GdftR2.cpp:32-150, ftCpuWithGrads.cpp:93-216); FM in rad/s, t in s."""
+
+    def __init__(self, nk, ni, kx, ky, kz, ix, iy, iz, FM, t, num_x, num_y, num_z):
+        a = [_f32(v) for v in (kx, ky, kz, ix, iy, iz, FM, t)]
+        h = P()
+        check(_lib.load().pg_gdftr2_create(C.byref(h), int(nk), int(ni), *[_ptr(v) for v in a], int(num_x),
+                                            int(num_y), int(num_z)))
         super().__init__(h)
 
 

@@ -2,7 +2,8 @@
 
 The outputs come from the reference's OWN kernels — PowerGrid/gridding.cpp,
 griddingSupport.cpp, ftCpu.cpp and fftCPU.cpp compiled unmodified from the
-reference tree into oracle/_ref/libpgref.so (oracle/Makefile, target `ref`),
+reference tree into oracle/_ref/libpgref.so (oracle/Makefile, target `ref`;
+ftCpuWithGrads.cpp too, for GdftR2),
 with the project FFT behind the FFTW API — driven by the oracle's restated
 Armadillo layers (TimeSegmentation, SENSE, pcSenseTimeSeg, PCG).  FP64
 outputs come from the reference's double instantiation (Gnufft) and the
@@ -67,6 +68,10 @@ def small_cases():
                                    fm=S.field_map(S.Rng(113), 8, 8, 4, 150.0),
                                    smap=S.coil_maps(S.Rng(114), 8, 8, 4, 2),
                                    pmap=S.shot_phase_maps(S.Rng(115), 8, 8, 4, 2), x=S.image(S.Rng(116), 256))
+    # 3-D SENSE<GdftR2>, 8x8x4 image, 512 samples, +-150 Hz, 2 coils
+    c = dict(cases["gdft3d"])
+    c["x"] = S.image(S.Rng(117), 256)
+    cases["gdftr2_3d"] = c
     # 2-D PCG: SENSE<TimeSegmentation<Gnufft>> + QuadPenalty, 5 iterations
     c = dict(cases["tssense2d"])
     c["beta"] = 1e-3
@@ -89,6 +94,10 @@ def build_op(name, c, prec):
     if name == "gdft3d":
         ix, iy, iz = S.image_coords(c["nx"], c["ny"], c["nz"])
         G = O.gdft(prec, c["kx"], c["ky"], c["kz"], ix, iy, iz, c["fm"], c["t"])
+        return O.sense(G, c["smap"], M, n, c["nc"])
+    if name == "gdftr2_3d":
+        ix, iy, iz = S.image_coords(c["nx"], c["ny"], c["nz"])
+        G = O.gdftr2(prec, c["kx"], c["ky"], c["kz"], ix, iy, iz, c["fm"], c["t"], c["nx"], c["ny"], c["nz"])
         return O.sense(G, c["smap"], M, n, c["nc"])
     if name == "pcsense3d":
         return O.pcsense_timeseg(prec, c["kx"], c["ky"], c["kz"], c["nx"], c["ny"], c["nz"], c["nc"], c["t"], c["L"],

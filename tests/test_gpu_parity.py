@@ -47,6 +47,10 @@ def _gpu_op(pg, name, c):
     if name == "pcsense3d":
         return pg.pcSenseTimeSeg(c["kx"], c["ky"], c["kz"], c["nx"], c["ny"], c["nz"], c["nc"], c["t"], c["L"], 1,
                                  c["smap"], c["fm"], c["pmap"])
+    if name == "gdftr2_3d":
+        ix, iy, iz = S.image_coords(c["nx"], c["ny"], c["nz"])
+        G = pg.GdftR2(M, n, c["kx"], c["ky"], c["kz"], ix, iy, iz, c["fm"], c["t"], c["nx"], c["ny"], c["nz"])
+        return pg.SENSE(G, c["smap"], M, n, c["nc"])
     if name == "pcsense_gdft3d":
         return pg.pcSENSE(c["kx"], c["ky"], c["kz"], c["nx"], c["ny"], c["nz"], c["nc"], c["t"], c["smap"], c["fm"],
                           c["pmap"])
@@ -55,7 +59,8 @@ def _gpu_op(pg, name, c):
     return pg.SENSE(A, c["smap"], M, n, c["nc"])
 
 
-@pytest.mark.parametrize("name", ["nufft2d", "nufft3d", "gdft3d", "tssense2d", "pcsense3d", "pcsense_gdft3d"])
+@pytest.mark.parametrize("name", ["nufft2d", "nufft3d", "gdft3d", "gdftr2_3d", "tssense2d", "pcsense3d",
+                                  "pcsense_gdft3d"])
 def test_operator_vs_reference_fixture(pg, name):
     c = _case(name)
     op = _gpu_op(pg, name, c)
@@ -268,6 +273,31 @@ def test_pcsense_gdft_at_size_vs_oracle(pg, oracle):
     xa64 = R64.adjoint(y32.astype(np.complex128))
     ef, ea = rel_l2(y, y32), rel_l2(xa, xa32)
     print(f"pcSENSE 16x16x8: fwd {ef:.2e} (fp64 {rel_l2(y, y64):.2e}, ref {rel_l2(y32, y64):.2e}); "
+          f"adj {ea:.2e} (fp64 {rel_l2(xa, xa64):.2e}, ref {rel_l2(xa32, xa64):.2e})")
+    assert ef <= OP_TOL and ea <= OP_TOL
+    assert rel_l2(y, y64) <= rel_l2(y32, y64) + OP_TOL
+
+
+def test_gdftr2_at_size_vs_oracle(pg, oracle):
+    """SENSE<GdftR2> 16x16x8, 2048 samples, 2 coils, against the restated reference
+    path (bit-exact to the compiled ftCpuWithGrads) and FP64."""
+    from powergrid_b200 import synthetic as S
+    nx = ny = 16
+    nz = 8
+    kx, ky, kz, t = S.stack_of_spirals(nx, nz, 2, 128, 20e-3)
+    ix, iy, iz = S.image_coords(nx, ny, nz)
+    fm = S.field_map(S.Rng(131), nx, ny, nz, 150.0)
+    sm = S.coil_maps(S.Rng(132), nx, ny, nz, 2)
+    M, n = kx.size, nx * ny * nz
+    x = S.image(S.Rng(133), n)
+    G = pg.GdftR2(M, n, kx, ky, kz, ix, iy, iz, fm, t, nx, ny, nz)
+    A = pg.SENSE(G, sm, M, n, 2)
+    R32 = oracle.sense(oracle.gdftr2(0, kx, ky, kz, ix, iy, iz, fm, t, nx, ny, nz), sm, M, n, 2)
+    R64 = oracle.sense(oracle.gdftr2(2, kx, ky, kz, ix, iy, iz, fm, t, nx, ny, nz), sm, M, n, 2)
+    y, y32, y64 = A * x, R32.forward(x), R64.forward(x.astype(np.complex128))
+    xa, xa32, xa64 = A / y32, R32.adjoint(y32), R64.adjoint(y32.astype(np.complex128))
+    ef, ea = rel_l2(y, y32), rel_l2(xa, xa32)
+    print(f"GdftR2 16x16x8: fwd {ef:.2e} (fp64 {rel_l2(y, y64):.2e}, ref {rel_l2(y32, y64):.2e}); "
           f"adj {ea:.2e} (fp64 {rel_l2(xa, xa64):.2e}, ref {rel_l2(xa32, xa64):.2e})")
     assert ef <= OP_TOL and ea <= OP_TOL
     assert rel_l2(y, y64) <= rel_l2(y32, y64) + OP_TOL

@@ -26,7 +26,8 @@ def _case(path):
 
 def test_fixtures_present():
     names = {os.path.basename(p)[:-4] for p in GOLDEN}
-    assert {"nufft2d", "nufft3d", "gdft3d", "tssense2d", "pcsense3d", "pcg2d", "pcgtv2d"} <= names
+    assert {"nufft2d", "nufft3d", "gdft3d", "gdftr2_3d", "tssense2d", "pcsense3d", "pcsense_gdft3d", "pcg2d",
+            "pcgtv2d"} <= names
 
 
 @pytest.mark.parametrize("shape", [(16,), (12,), (30,), (7,), (8, 6), (4, 6, 10), (64, 64)])
@@ -211,3 +212,21 @@ def test_minmax_interpolator_oracle_float_vs_fp64(oracle, typ):
         x = S.image(S.Rng(7), n * n)
         ys.append(T.forward(x.astype(np.complex64 if prec == 0 else np.complex128)))
     assert rel_l2(ys[0], ys[1]) < 1e-4
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(HERE), "oracle", "_ref", "libpgref.so")),
+                    reason="reference kernels are compiled only where the reference tree exists")
+def test_gdftr2_restatement_matches_reference_kernels(oracle):
+    """GdftR2 restated (gradient maps + ftCpuWithGrads / iftCpuWithGrads) == the compiled reference, bit for bit."""
+    from powergrid_b200 import synthetic as S
+    kx, ky, kz, t = S.stack_of_spirals(8, 4, 2, 64, 25e-3)
+    ix, iy, iz = S.image_coords(8, 8, 4)
+    fm = S.field_map(S.Rng(104), 8, 8, 4, 150.0)
+    x, y = S.image(S.Rng(1), 256), S.image(S.Rng(2), kx.size)
+    outs = []
+    for use_ref in (False, True):
+        oracle.use_reference(use_ref)
+        G = oracle.gdftr2(0, kx, ky, kz, ix, iy, iz, fm, t, 8, 8, 4)
+        outs.append((G.forward(x), G.adjoint(y)))
+    oracle.use_reference(False)
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
