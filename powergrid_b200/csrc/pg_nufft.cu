@@ -458,11 +458,17 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
     const float2* src = vs + ((uint64_t)(cfirst + c) * M + first) * K;
     for (int r = tid; r < nk; r += blockDim.x) {
       const int i = (K == 1) ? r : (K == 2) ? (r >> 1) : r / K;
-      const int pl = c * K + (r - i * K);
+      const int j = r - i * K;
       const float2 v = src[r];
-      sv[i * np + pl] = v;
-      // non-negative floats order like their bit patterns
-      atomicMax(&vmax[pl], __float_as_uint(fmaxf(fabsf(v.x), fabsf(v.y))));
+      sv[i * np + c * K + j] = v;
+      // non-negative floats order like their bit patterns; one shared atomic
+      // per warp and plane instead of one per value
+      const unsigned m = __float_as_uint(fmaxf(fabsf(v.x), fabsf(v.y)));
+      const unsigned act = __activemask();
+      for (int jj = 0; jj < K; ++jj) {
+        const unsigned wm = __reduce_max_sync(act, j == jj ? m : 0u);
+        if ((threadIdx.x & 31) == __ffs(act) - 1 && wm) atomicMax(&vmax[c * K + jj], wm);
+      }
     }
   }
   __syncthreads();
