@@ -394,6 +394,17 @@ __global__ void __launch_bounds__(128) k_gather(NufftGeom g, TileShape t, const 
 // Tile layout [coil][segment][re|im][PZ][PX][PY], PY = 8 (mod 32): a warp's
 // 32 lanes (8 y-taps x 4 x-taps) hit 32 distinct banks.
 // ---------------------------------------------------------------------------
+// Asynchronous global -> shared copies (cp.async; 16 bytes bypass L1).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 __device__ __forceinline__ int fixed_point(float w, float v) {
   constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23, float bits 0x4B400000
   return __float_as_int(__fmaf_rn(w, v, kMagic)) - 0x4B400000;
@@ -439,18 +450,16 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
   if (tid < 16) vmax[tid] = 0u;
   __syncthreads();
 
-  // 1. staging
+  // 1. staging: asynchronous copies straight into shared memory (no register
+  // round trip; every copy of the item is in flight before the one wait)
   constexpr int R4 = WROW / 4;
   for (int q = tid; q < count * R4; q += blockDim.x) {
     const int i = q / R4, a = q % R4;
-    float4 val;
-    if (a < 4)
-      val = reinterpret_cast<const float4*>(wxy + (uint64_t)(first + i) * 16)[a];
-    else
-      val = reinterpret_cast<const float4*>(wz + (uint64_t)(first + i) * 8)[a - 4];
-    reinterpret_cast<float4*>(sw + i * WROW)[a] = val;
+    const float4* src = (a < 4) ? reinterpret_cast<const float4*>(wxy + (uint64_t)(first + i) * 16) + a
+                                : reinterpret_cast<const float4*>(wz + (uint64_t)(first + i) * 8) + (a - 4);
+    cp_async16(reinterpret_cast<float4*>(sw + i * WROW) + a, src);
   }
-  for (int i = tid; i < count; i += blockDim.x) sst[i] = start[first + i];
+  for (int i = tid; i < count; i += blockDim.x) cp_async8(&sst[i], &start[first + i]);
   // sv[i][c*K + j] = vs[cfirst + c][first + i][j]: for each coil of the block
   // the block's samples are one contiguous run of count*K values
   const int nk = count * K;
@@ -458,18 +467,21 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
     const float2* src = vs + ((uint64_t)(cfirst + c) * M + first) * K;
     for (int r = tid; r < nk; r += blockDim.x) {
       const int i = (K == 1) ? r : (K == 2) ? (r >> 1) : r / K;
-      const int j = r - i * K;
-      const float2 v = src[r];
-      sv[i * np + c * K + j] = v;
-      // non-negative floats order like their bit patterns; one shared atomic
-      // per warp and plane instead of one per value
-      const unsigned m = __float_as_uint(fmaxf(fabsf(v.x), fabsf(v.y)));
-      const unsigned act = __activemask();
-      for (int jj = 0; jj < K; ++jj) {
-        const unsigned wm = __reduce_max_sync(act, j == jj ? m : 0u);
-        if ((threadIdx.x & 31) == __ffs(act) - 1 && wm) atomicMax(&vmax[c * K + jj], wm);
-      }
+      cp_async8(&sv[i * np + c * K + (r - i * K)], &src[r]);
     }
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  // largest |re| or |im| per plane (non-negative floats order like their bit
+  // patterns): a register maximum per thread, then one atomic per warp
+  for (int pl = 0; pl < np; ++pl) {
+    unsigned m = 0u;
+    for (int i = tid; i < count; i += blockDim.x) {
+      const float2 v = sv[i * np + pl];
+      m = max(m, __float_as_uint(fmaxf(fabsf(v.x), fabsf(v.y))));
+    }
+    m = __reduce_max_sync(0xffffffffu, m);
+    if ((tid & 31) == 0 && m) atomicMax(&vmax[pl], m);
   }
   __syncthreads();
 
