@@ -229,6 +229,17 @@ __global__ void k_adjoint_prep(uint64_t n4, float4* __restrict__ grids, int nb, 
     }
 }
 
+// Asynchronous global -> shared copies (cp.async; 16 bytes bypass L1).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // Padded extent along y (the fastest axis) such that 4 x-rows of 8 y-taps
 // land in 32 distinct banks: PY = 8 or 24 (mod 32).
 __host__ __device__ constexpr int padded_y(int T) {
@@ -299,7 +310,12 @@ __global__ void __launch_bounds__(128) k_gather(NufftGeom g, TileShape t, const 
   const int tz = txz / t.ntx;
   const int x0 = tx * T, y0 = ty * T, z0 = tz * TG::TZ;
   const uint64_t G = g.ngrid();
-  for (int q = threadIdx.x; q < CELLS; q += blockDim.x) {
+  // cell pairs (y, y+1) with asynchronous 16-byte copies: PY, y0 and Gy are
+  // even, so a pair is in the grid or outside it as a whole and both of its
+  // addresses are 16-byte aligned
+  static_assert(PY % 2 == 0 && CELLS % 2 == 0, "cell pairs");
+  for (int t2 = threadIdx.x; t2 < CELLS / 2; t2 += blockDim.x) {
+    const int q = 2 * t2;
     const int pyy = q % PY;
     const int pxx = (q / PY) % PX;
     const int pzz = q / PLANE;
@@ -310,11 +326,14 @@ __global__ void __launch_bounds__(128) k_gather(NufftGeom g, TileShape t, const 
     for (int c = 0; c < CC; ++c)
 #pragma unroll
       for (int j = 0; j < KP; ++j) {
-        float2 v = make_float2(0.f, 0.f);
-        if (in && c < ncl && j < K) v = grids[((uint64_t)(cfirst + c) * L + lseg + j) * G + idx];
-        sm2[(c * KP + j) * CELLS + q] = v;
+        float2* d = &sm2[(c * KP + j) * CELLS + q];
+        if (in && c < ncl && j < K)
+          cp_async16(d, &grids[((uint64_t)(cfirst + c) * L + lseg + j) * G + idx]);
+        else
+          *reinterpret_cast<float4*>(d) = make_float4(0.f, 0.f, 0.f, 0.f);
       }
   }
+  cp_async_wait_all();
   __syncthreads();
   const int end = first + count;
   for (int s = first + threadIdx.x; s < end; s += blockDim.x) {
@@ -394,17 +413,6 @@ __global__ void __launch_bounds__(128) k_gather(NufftGeom g, TileShape t, const 
 // Tile layout [coil][segment][re|im][PZ][PX][PY], PY = 8 (mod 32): a warp's
 // 32 lanes (8 y-taps x 4 x-taps) hit 32 distinct banks.
 // ---------------------------------------------------------------------------
-// Asynchronous global -> shared copies (cp.async; 16 bytes bypass L1).
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
 __device__ __forceinline__ int fixed_point(float w, float v) {
   constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23, float bits 0x4B400000
   return __float_as_int(__fmaf_rn(w, v, kMagic)) - 0x4B400000;
