@@ -301,3 +301,37 @@ def test_gdftr2_at_size_vs_oracle(pg, oracle):
           f"adj {ea:.2e} (fp64 {rel_l2(xa, xa64):.2e}, ref {rel_l2(xa32, xa64):.2e})")
     assert ef <= OP_TOL and ea <= OP_TOL
     assert rel_l2(y, y64) <= rel_l2(y32, y64) + OP_TOL
+
+
+def test_invalid_inputs_of_the_widened_api_are_rejected(pg):
+    """pcSENSE, GdftR2, the min-max interpolators, the spatial interpolation and
+    the direct-reconstruction helpers reject malformed input with INVALID_ARG."""
+    from powergrid_b200 import synthetic as S
+    from powergrid_b200._lib import PGError
+    kx, ky, kz, t = S.stack_of_spirals(8, 4, 2, 64, 20e-3)
+    fm = S.field_map(S.Rng(1), 8, 8, 4, 100.0)
+    sm = S.coil_maps(S.Rng(2), 8, 8, 4, 2)
+    pm = S.shot_phase_maps(S.Rng(3), 8, 8, 4, 2)
+    ix, iy, iz = S.image_coords(8, 8, 4)
+    with pytest.raises(PGError, match="INVALID_ARG"):      # phase maps not a multiple of the image
+        pg.pcSENSE(kx, ky, kz, 8, 8, 4, 2, t, sm, fm, pm[:-1])
+    with pytest.raises(PGError, match="INVALID_ARG"):      # samples not divisible by the shots
+        pg.pcSENSE(kx[:-1], ky[:-1], kz[:-1], 8, 8, 4, 2, t[:-1], sm, fm, pm)
+    with pytest.raises(PGError, match="INVALID_ARG"):      # nx*ny*nz != voxels
+        pg.GdftR2(kx.size, 256, kx, ky, kz, ix, iy, iz, fm, t, 8, 8, 2)
+    with pytest.raises(PGError, match="INVALID_ARG"):      # interpolator type out of range
+        G = pg.Gnufft(kx.size, 2.0, 8, 8, 4, kx, ky, kz)
+        pg.TimeSegmentation(G, fm, t, kx.size, 256, 4, 4, 1)
+    with pytest.raises(PGError, match="INVALID_ARG"):      # more than 16 taps per window axis
+        pg.Gnufft(kx.size, 4.0, 8, 8, 4, kx, ky, kz)
+    G3 = pg.Gnufft(kx.size, 3.0, 8, 8, 4, kx, ky, kz)       # interpolation only at gridos 3
+    with pytest.raises(PGError, match="INVALID_ARG"):
+        G3 * np.zeros(256, np.complex64)
+    with pytest.raises(ValueError):
+        G3.forwardSpatialInterp(np.zeros(10, np.complex64))
+    bad = kx.copy()
+    bad[5] = np.inf
+    with pytest.raises(PGError, match="INVALID_ARG"):
+        pg.calc3DDensityCompensation(bad, ky, kz, 8, 4)
+    with pytest.raises(ValueError):
+        pg.calcSumOfSquaresImage(np.zeros(10, np.complex64), 3)
