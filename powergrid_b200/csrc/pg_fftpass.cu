@@ -1,5 +1,6 @@
-// Oversampled 2-D FFTs for power-of-two grids (2N x 2N, N = 32 ... 512),
-// written as four pruned passes with the pre- and post-kernels fused in.
+// Oversampled 2-D and 3-D FFTs for power-of-two grids (2N per axis,
+// N = 16 ... 512), written as pruned passes with the pre- and post-kernels
+// fused in.
 //
 // The forward operator's input grid is zero outside the N x N image region
 // (zero_pad, griddingSupport.cpp:372-404) and the adjoint keeps only that
@@ -15,6 +16,10 @@
 //                columns, post-kernel weights (sign, deapodization, WoH,
 //                conj coil map, conj shot phase)               -> one image per grid
 //            sum the images of the batch's grids in a fixed order.
+// In 3-D the first pass runs over the Nx*Nz image lines along y, the second
+// along x over each of the Nz nonzero z-slabs, and a third along z over every
+// (x, y) column, reading only the Nz nonzero slabs; the adjoint mirrors it
+// (z, keeping Nz slabs; x per slab, keeping Nx rows; y with the post weights).
 // Transforms are unnormalised (FFTW/cuFFT conventions, forward sign -1).
 //
 // Each length-n transform (n = R1 * R2) is two register passes with one
@@ -29,15 +34,17 @@
 // memory.  Zero inputs (the padding) are never loaded and cropped outputs
 // never stored.  Twiddles W_n^(m2 k1) come from a table made in double
 // precision, laid out [k1][m2].
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
-#include "pg_fft2d.cuh"
+#include "pg_fftpass.cuh"
 
 namespace pg {
 namespace {
 
 constexpr int kT = 256;   // threads per block
+constexpr int kMaxGridY = 65535;
 
 __device__ __forceinline__ float2 twiddle(float2 v, float2 w, bool inv) {
   const float wy = inv ? -w.y : w.y;
@@ -168,6 +175,8 @@ __device__ __forceinline__ void dft(float2 (&v)[R], bool inv) {
 
 // Factor n = R1 * R2 of each supported length.
 template <int LOGN> struct Split;
+template <> struct Split<4> { static constexpr int R1 = 4, R2 = 4; };
+template <> struct Split<5> { static constexpr int R1 = 8, R2 = 4; };
 template <> struct Split<6> { static constexpr int R1 = 16, R2 = 4; };
 template <> struct Split<7> { static constexpr int R1 = 16, R2 = 8; };
 template <> struct Split<8> { static constexpr int R1 = 16, R2 = 16; };
@@ -187,7 +196,7 @@ struct RowGeo {
   static constexpr size_t smem = (size_t)RB * RS * sizeof(float2);
 };
 
-// Column kernels: CB adjacent columns per block, shared layout [k1][m2][col].
+// Strided-line kernels: CB adjacent columns per block, shared layout [k1][m2][col].
 template <int LOGN>
 struct ColGeo {
   static constexpr int R1 = Split<LOGN>::R1, R2 = Split<LOGN>::R2, n = R1 * R2;
@@ -195,10 +204,19 @@ struct ColGeo {
   static constexpr size_t smem = (size_t)n * CB * sizeof(float2);
 };
 
+// A batch of strided lines: grid (or slab) b holds ncols columns; element
+// m of column c sits at b * bstride + m * rstride + c.
+struct Lines {
+  uint64_t in_bstride, out_bstride, rstride;
+  int ncols;
+  int nio;      // nonzero input rows (forward) / kept output rows (inverse)
+  int off;      // their first index along the line (pad / crop offset)
+};
+
 __device__ __forceinline__ int parity2(int a, int b) { return (a + b) & 1; }
 
-// F1: pre-kernel values of image rows ix of grid b, zero padded to n, FFT
-// along y -> P[b][ix][0..n).
+// F1: pre-kernel values of the image lines (ix, iz) of grid b, zero padded
+// to n along y, FFT along y -> P[b][iz][ix][0..n).
 template <int LOGN>
 __global__ void __launch_bounds__(kT) k_fft_fwd_rows(NufftGeom g, int L, const float2* __restrict__ x,
                                                      const float2* __restrict__ S, int c0,
@@ -209,27 +227,30 @@ __global__ void __launch_bounds__(kT) k_fft_fwd_rows(NufftGeom g, int L, const f
   constexpr int R1 = RG::R1, R2 = RG::R2, n = RG::n, RB = RG::RB, S2 = RG::S2, RS = RG::RS;
   extern __shared__ float2 sh[];
   const int Nn = g.Ny, pad = g.pad_off[1];
+  const int nrows = g.Nx * g.Nz;
   const uint64_t N = g.nimg();
   const int b = blockIdx.y, c = b / L, l = b - c * L;
-  const int ix0 = blockIdx.x * RB;
+  const int r0 = blockIdx.x * RB;
   {
     const int m2 = threadIdx.x % R2, r = threadIdx.x / R2;
-    const int ix = ix0 + r;
+    const int rg = r0 + r;
+    const int ix = rg % g.Nx, iz = rg / g.Nx;
+    const int pxz = ix + g.pad_off[0] + iz + g.pad_off[2];
     float2 v[R1];
 #pragma unroll
     for (int m1 = 0; m1 < R1; ++m1) {
       const int gy = R2 * m1 + m2;
       const int iy = gy - pad;
       float2 u = make_float2(0.f, 0.f);
-      if (ix < g.Nx && iy >= 0 && iy < Nn) {
-        const uint64_t p = (uint64_t)iy + (uint64_t)Nn * ix;
+      if (rg < nrows && iy >= 0 && iy < Nn) {
+        const uint64_t p = (uint64_t)iy + (uint64_t)Nn * ((uint64_t)ix + (uint64_t)g.Nx * iz);
         u = x[p];
         if (S) {
           const float2 sv = S[(uint64_t)(c0 + c) * N + p];
           u = E ? cmul(u, cmul(sv, E[p])) : cmul(sv, u);
         }
         if (Wo) u = cmul(Wo[(uint64_t)l * N + p], u);
-        const float f = parity2(ix + g.pad_off[0], gy) ? -deapf[p] : deapf[p];
+        const float f = parity2(pxz, gy) ? -deapf[p] : deapf[p];
         u = make_float2(u.x * f, u.y * f);
       }
       v[m1] = u;
@@ -246,40 +267,41 @@ __global__ void __launch_bounds__(kT) k_fft_fwd_rows(NufftGeom g, int L, const f
     const int it = it0 + threadIdx.x;
     if ((RB * R1) % kT != 0 && it >= RB * R1) break;
     const int k1 = it % R1, r = it / R1;
-    const int ix = ix0 + r;
+    const int rg = r0 + r;
     float2 u[R2];
     const float2* s = sh + r * RS + k1 * S2;
 #pragma unroll
     for (int m2 = 0; m2 < R2; ++m2) u[m2] = s[m2];
     dft<R2>(u, false);
-    if (ix < g.Nx) {
-      float2* o = P + ((uint64_t)b * g.Nx + ix) * n + k1;
+    if (rg < nrows) {
+      float2* o = P + ((uint64_t)b * nrows + rg) * n + k1;
 #pragma unroll
       for (int k2 = 0; k2 < R2; ++k2) o[R1 * k2] = u[k2];
     }
   }
 }
 
-// F2: columns gy of grid b: the Nx rows of P at gx = pad + i, zero padded to
-// n, FFT along x -> grids[b][gx][gy] for every gx.
+// Forward strided lines: per column, the nio nonzero rows at off + i
+// (zero padded to n), FFT along the line -> all n rows of the output.
 template <int LOGN>
-__global__ void __launch_bounds__(kT) k_fft_fwd_cols(NufftGeom g, const float2* __restrict__ P,
-                                                     const float2* __restrict__ tw, float2* __restrict__ grids) {
+__global__ void __launch_bounds__(kT) k_fft_fwd_cols(Lines ln, const float2* __restrict__ P,
+                                                     const float2* __restrict__ tw, float2* __restrict__ out) {
   using CG = ColGeo<LOGN>;
-  constexpr int R1 = CG::R1, R2 = CG::R2, n = CG::n, CB = CG::CB;
+  constexpr int R1 = CG::R1, R2 = CG::R2, CB = CG::CB;
   extern __shared__ float2 sh[];
-  const int pad = g.pad_off[0];
-  const int b = blockIdx.y, gy0 = blockIdx.x * CB;
+  const int b = blockIdx.y, c0 = blockIdx.x * CB;
+  const float2* pin = P + (uint64_t)b * ln.in_bstride;
 #pragma unroll
   for (int it0 = 0; it0 < CB * R2; it0 += kT) {
     const int it = it0 + threadIdx.x;
     if ((CB * R2) % kT != 0 && it >= CB * R2) break;
     const int col = it % CB, m2 = it / CB;
+    const int cg = c0 + col;
     float2 v[R1];
 #pragma unroll
     for (int m1 = 0; m1 < R1; ++m1) {
-      const int i = R2 * m1 + m2 - pad;
-      v[m1] = (i >= 0 && i < g.Nx) ? P[((uint64_t)b * g.Nx + i) * n + gy0 + col] : make_float2(0.f, 0.f);
+      const int i = R2 * m1 + m2 - ln.off;
+      v[m1] = (cg < ln.ncols && i >= 0 && i < ln.nio) ? pin[(uint64_t)i * ln.rstride + cg] : make_float2(0.f, 0.f);
     }
     dft<R1>(v, false);
     float2* d = sh + m2 * CB + col;
@@ -288,42 +310,46 @@ __global__ void __launch_bounds__(kT) k_fft_fwd_cols(NufftGeom g, const float2* 
     for (int k1 = 1; k1 < R1; ++k1) d[k1 * R2 * CB] = twiddle(v[k1], tw[k1 * R2 + m2], false);
   }
   __syncthreads();
-  const uint64_t G = (uint64_t)n * n;
+  float2* pout = out + (uint64_t)b * ln.out_bstride;
 #pragma unroll
   for (int it0 = 0; it0 < CB * R1; it0 += kT) {
     const int it = it0 + threadIdx.x;
     if ((CB * R1) % kT != 0 && it >= CB * R1) break;
     const int col = it % CB, k1 = it / CB;
+    const int cg = c0 + col;
     float2 u[R2];
     const float2* s = sh + k1 * R2 * CB + col;
 #pragma unroll
     for (int m2 = 0; m2 < R2; ++m2) u[m2] = s[m2 * CB];
     dft<R2>(u, false);
-    float2* o = grids + (uint64_t)b * G + (uint64_t)k1 * n + gy0 + col;
+    if (cg < ln.ncols) {
+      float2* o = pout + (uint64_t)k1 * ln.rstride + cg;
 #pragma unroll
-    for (int k2 = 0; k2 < R2; ++k2) o[(uint64_t)R1 * k2 * n] = u[k2];
+      for (int k2 = 0; k2 < R2; ++k2) o[(uint64_t)R1 * k2 * ln.rstride] = u[k2];
+    }
   }
 }
 
-// A1: columns gy of grid b, inverse FFT along x, keep gx = crop + i -> Q[b][i][gy].
+// Inverse strided lines: per column, all n rows, inverse FFT along the line,
+// keep the nio rows at off + i -> row i of the output.
 template <int LOGN>
-__global__ void __launch_bounds__(kT) k_fft_inv_cols(NufftGeom g, const float2* __restrict__ grids,
+__global__ void __launch_bounds__(kT) k_fft_inv_cols(Lines ln, const float2* __restrict__ in,
                                                      const float2* __restrict__ tw, float2* __restrict__ Q) {
   using CG = ColGeo<LOGN>;
-  constexpr int R1 = CG::R1, R2 = CG::R2, n = CG::n, CB = CG::CB;
+  constexpr int R1 = CG::R1, R2 = CG::R2, CB = CG::CB;
   extern __shared__ float2 sh[];
-  const int crop = g.crop_off[0];
-  const int b = blockIdx.y, gy0 = blockIdx.x * CB;
-  const uint64_t G = (uint64_t)n * n;
+  const int b = blockIdx.y, c0 = blockIdx.x * CB;
+  const float2* pin = in + (uint64_t)b * ln.in_bstride;
 #pragma unroll
   for (int it0 = 0; it0 < CB * R2; it0 += kT) {
     const int it = it0 + threadIdx.x;
     if ((CB * R2) % kT != 0 && it >= CB * R2) break;
     const int col = it % CB, m2 = it / CB;
+    const int cg = c0 + col;
     float2 v[R1];
-    const float2* s = grids + (uint64_t)b * G + (uint64_t)m2 * n + gy0 + col;
+    const float2* s = pin + (uint64_t)m2 * ln.rstride + cg;
 #pragma unroll
-    for (int m1 = 0; m1 < R1; ++m1) v[m1] = s[(uint64_t)R2 * m1 * n];
+    for (int m1 = 0; m1 < R1; ++m1) v[m1] = (cg < ln.ncols) ? s[(uint64_t)R2 * m1 * ln.rstride] : make_float2(0.f, 0.f);
     dft<R1>(v, true);
     float2* d = sh + m2 * CB + col;
     d[0] = v[0];
@@ -331,26 +357,30 @@ __global__ void __launch_bounds__(kT) k_fft_inv_cols(NufftGeom g, const float2* 
     for (int k1 = 1; k1 < R1; ++k1) d[k1 * R2 * CB] = twiddle(v[k1], tw[k1 * R2 + m2], true);
   }
   __syncthreads();
+  float2* pout = Q + (uint64_t)b * ln.out_bstride;
 #pragma unroll
   for (int it0 = 0; it0 < CB * R1; it0 += kT) {
     const int it = it0 + threadIdx.x;
     if ((CB * R1) % kT != 0 && it >= CB * R1) break;
     const int col = it % CB, k1 = it / CB;
+    const int cg = c0 + col;
     float2 u[R2];
     const float2* s = sh + k1 * R2 * CB + col;
 #pragma unroll
     for (int m2 = 0; m2 < R2; ++m2) u[m2] = s[m2 * CB];
     dft<R2>(u, true);
+    if (cg >= ln.ncols) continue;
 #pragma unroll
     for (int k2 = 0; k2 < R2; ++k2) {
-      const int i = k1 + R1 * k2 - crop;
-      if (i >= 0 && i < g.Nx) Q[((uint64_t)b * g.Nx + i) * n + gy0 + col] = u[k2];
+      const int i = k1 + R1 * k2 - ln.off;
+      if (i >= 0 && i < ln.nio) pout[(uint64_t)i * ln.rstride + cg] = u[k2];
     }
   }
 }
 
-// A2: cropped rows ix of grid b, inverse FFT along y, keep gy = crop + iy and
-// apply the post-kernel weights of grid b = (coil c, segment l) -> Rimg[b][p].
+// Last inverse pass: cropped lines (ix, iz) of grid b, inverse FFT along y,
+// keep gy = crop + iy and apply the post-kernel weights of grid b = (coil c,
+// segment l) -> Rimg[b][p].
 template <int LOGN>
 __global__ void __launch_bounds__(kT) k_fft_inv_rows(NufftGeom g, int L, const float2* __restrict__ Q,
                                                      const float2* __restrict__ S, int c0,
@@ -362,16 +392,17 @@ __global__ void __launch_bounds__(kT) k_fft_inv_rows(NufftGeom g, int L, const f
   extern __shared__ float2 sh[];
   constexpr int Nn = n / 2;
   const int crop = g.crop_off[1];
+  const int nrows = g.Nx * g.Nz;
   const uint64_t N = g.nimg();
   const int b = blockIdx.y, c = b / L, l = b - c * L;
-  const int ix0 = blockIdx.x * RB;
+  const int r0 = blockIdx.x * RB;
   {
     const int m2 = threadIdx.x % R2, r = threadIdx.x / R2;
-    const int ix = ix0 + r;
+    const int rg = r0 + r;
     float2 v[R1];
-    const float2* s = Q + ((uint64_t)b * g.Nx + ix) * n + m2;
+    const float2* s = Q + ((uint64_t)b * nrows + rg) * n + m2;
 #pragma unroll
-    for (int m1 = 0; m1 < R1; ++m1) v[m1] = (ix < g.Nx) ? s[R2 * m1] : make_float2(0.f, 0.f);
+    for (int m1 = 0; m1 < R1; ++m1) v[m1] = (rg < nrows) ? s[R2 * m1] : make_float2(0.f, 0.f);
     dft<R1>(v, true);
     float2* d = sh + r * RS + m2;
     d[0] = v[0];
@@ -384,20 +415,22 @@ __global__ void __launch_bounds__(kT) k_fft_inv_rows(NufftGeom g, int L, const f
     const int it = it0 + threadIdx.x;
     if ((RB * R1) % kT != 0 && it >= RB * R1) break;
     const int k1 = it % R1, r = it / R1;
-    const int ix = ix0 + r;
+    const int rg = r0 + r;
     float2 u[R2];
     const float2* s = sh + r * RS + k1 * S2;
 #pragma unroll
     for (int m2 = 0; m2 < R2; ++m2) u[m2] = s[m2];
     dft<R2>(u, true);
-    if (ix >= g.Nx) continue;
+    if (rg >= nrows) continue;
+    const int ix = rg % g.Nx, iz = rg / g.Nx;
+    const int pxz = ix + g.crop_off[0] + iz + g.crop_off[2];
 #pragma unroll
     for (int k2 = 0; k2 < R2; ++k2) {
       const int iy = k1 + R1 * k2 - crop;
       if (iy < 0 || iy >= Nn) continue;
-      const uint64_t p = (uint64_t)iy + (uint64_t)Nn * ix;
+      const uint64_t p = (uint64_t)iy + (uint64_t)Nn * ((uint64_t)ix + (uint64_t)g.Nx * iz);
       float2 v = u[k2];
-      const float f = parity2(ix + g.crop_off[0], iy + crop) ? -deapf[p] : deapf[p];
+      const float f = parity2(pxz, iy + crop) ? -deapf[p] : deapf[p];
       v = make_float2(v.x * f, v.y * f);
       if (WoH) v = cmul(v, WoH[(uint64_t)l * N + p]);
       if (S) {
@@ -428,31 +461,68 @@ __global__ void k_sum_images(uint64_t N, int B, const float2* __restrict__ Rimg,
 }
 
 template <int LOGN>
-pg_status forward_t(const NufftGeom& g, int B, int L, const float2* x, const float2* S, int c0, const float2* E,
-                    const float2* Wo, const float* deapf, const float2* tw, float2* P, float2* grids,
-                    cudaStream_t s) {
+pg_status rows_fwd(const NufftGeom& g, int B, int L, const float2* x, const float2* S, int c0, const float2* E,
+                   const float2* Wo, const float* deapf, const float2* tw, float2* P, cudaStream_t s) {
   using RG = RowGeo<LOGN>;
-  using CG = ColGeo<LOGN>;
   PG_CUDA(cudaFuncSetAttribute(k_fft_fwd_rows<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RG::smem));
-  PG_CUDA(cudaFuncSetAttribute(k_fft_fwd_cols<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CG::smem));
-  PG_LAUNCH(k_fft_fwd_rows<LOGN>, dim3(ceil_div(g.Nx, RG::RB), B), kT, RG::smem, s, g, L, x, S, c0, E, Wo, deapf, tw,
-            P);
-  PG_LAUNCH(k_fft_fwd_cols<LOGN>, dim3(CG::n / CG::CB, B), kT, CG::smem, s, g, P, tw, grids);
+  PG_LAUNCH(k_fft_fwd_rows<LOGN>, dim3(ceil_div((uint64_t)g.Nx * g.Nz, RG::RB), B), kT, RG::smem, s, g, L, x, S, c0,
+            E, Wo, deapf, tw, P);
   return PG_OK;
 }
 
 template <int LOGN>
-pg_status adjoint_t(const NufftGeom& g, int B, int L, const float2* grids, const float2* S, int c0, const float2* E,
-                    const float2* WoH, const float* deapf, const float2* tw, float2* Q, float2* Rimg,
-                    cudaStream_t s) {
+pg_status rows_inv(const NufftGeom& g, int B, int L, const float2* Q, const float2* S, int c0, const float2* E,
+                   const float2* WoH, const float* deapf, const float2* tw, float2* Rimg, cudaStream_t s) {
   using RG = RowGeo<LOGN>;
+  PG_CUDA(cudaFuncSetAttribute(k_fft_inv_rows<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RG::smem));
+  PG_LAUNCH(k_fft_inv_rows<LOGN>, dim3(ceil_div((uint64_t)g.Nx * g.Nz, RG::RB), B), kT, RG::smem, s, g, L, Q, S, c0,
+            E, WoH, deapf, tw, Rimg);
+  return PG_OK;
+}
+
+template <int LOGN>
+pg_status cols_fwd(const Lines& ln, int B, const float2* P, const float2* tw, float2* out, cudaStream_t s) {
+  using CG = ColGeo<LOGN>;
+  PG_CUDA(cudaFuncSetAttribute(k_fft_fwd_cols<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CG::smem));
+  PG_LAUNCH(k_fft_fwd_cols<LOGN>, dim3(ceil_div(ln.ncols, CG::CB), B), kT, CG::smem, s, ln, P, tw, out);
+  return PG_OK;
+}
+
+template <int LOGN>
+pg_status cols_inv(const Lines& ln, int B, const float2* in, const float2* tw, float2* Q, cudaStream_t s) {
   using CG = ColGeo<LOGN>;
   PG_CUDA(cudaFuncSetAttribute(k_fft_inv_cols<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CG::smem));
-  PG_CUDA(cudaFuncSetAttribute(k_fft_inv_rows<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RG::smem));
-  PG_LAUNCH(k_fft_inv_cols<LOGN>, dim3(CG::n / CG::CB, B), kT, CG::smem, s, g, grids, tw, Q);
-  PG_LAUNCH(k_fft_inv_rows<LOGN>, dim3(ceil_div(g.Nx, RG::RB), B), kT, RG::smem, s, g, L, Q, S, c0, E, WoH, deapf,
-            tw, Rimg);
+  PG_LAUNCH(k_fft_inv_cols<LOGN>, dim3(ceil_div(ln.ncols, CG::CB), B), kT, CG::smem, s, ln, in, tw, Q);
   return PG_OK;
+}
+
+#define PG_FFT_DISPATCH(lg, fn, ...)                                           \
+  switch (lg) {                                                                \
+    case 4: return fn<4>(__VA_ARGS__);                                         \
+    case 5: return fn<5>(__VA_ARGS__);                                         \
+    case 6: return fn<6>(__VA_ARGS__);                                         \
+    case 7: return fn<7>(__VA_ARGS__);                                         \
+    case 8: return fn<8>(__VA_ARGS__);                                         \
+    case 9: return fn<9>(__VA_ARGS__);                                         \
+    case 10: return fn<10>(__VA_ARGS__);                                       \
+    default: return set_error(PG_INVALID_ARG, "fft passes: unsupported length 2^%d", lg); \
+  }
+
+pg_status d_rows_fwd(int lg, const NufftGeom& g, int B, int L, const float2* x, const float2* S, int c0,
+                     const float2* E, const float2* Wo, const float* deapf, const float2* tw, float2* P,
+                     cudaStream_t s) {
+  PG_FFT_DISPATCH(lg, rows_fwd, g, B, L, x, S, c0, E, Wo, deapf, tw, P, s)
+}
+pg_status d_rows_inv(int lg, const NufftGeom& g, int B, int L, const float2* Q, const float2* S, int c0,
+                     const float2* E, const float2* WoH, const float* deapf, const float2* tw, float2* Rimg,
+                     cudaStream_t s) {
+  PG_FFT_DISPATCH(lg, rows_inv, g, B, L, Q, S, c0, E, WoH, deapf, tw, Rimg, s)
+}
+pg_status d_cols_fwd(int lg, const Lines& ln, int B, const float2* P, const float2* tw, float2* out, cudaStream_t s) {
+  PG_FFT_DISPATCH(lg, cols_fwd, ln, B, P, tw, out, s)
+}
+pg_status d_cols_inv(int lg, const Lines& ln, int B, const float2* in, const float2* tw, float2* Q, cudaStream_t s) {
+  PG_FFT_DISPATCH(lg, cols_inv, ln, B, in, tw, Q, s)
 }
 
 int log2_exact(int v) {
@@ -462,54 +532,86 @@ int log2_exact(int v) {
 }
 
 // R2 of the factorisation n = R1 * R2 (Split above).
-int split_r2(int n) { return n == 1024 ? 32 : n / 16; }
+int split_r2(int n) { return n >= 1024 ? 32 : n <= 64 ? 4 : n / 16; }
 
-}  // namespace
-
-bool fft2d_supported(const NufftGeom& g) {
-  if (g.dim != 2 || g.Gx != g.Gy || g.Gx != 2 * g.Nx || g.Ny != g.Nx) return false;
-  const int l = log2_exact(g.Gx);
-  return l >= 6 && l <= 10;
-}
-
-pg_status fft2d_twiddles(const NufftGeom& g, DevBuf<float2>* tw, cudaStream_t s) {
-  const int n = g.Gx, R2 = split_r2(n), R1 = n / R2;
-  std::vector<float2> h(n);
+void twiddle_table(int n, std::vector<float2>* h) {
+  const int R2 = split_r2(n), R1 = n / R2;
   const double two_pi = 6.283185307179586476925286766559;
   for (int k1 = 0; k1 < R1; ++k1)
     for (int m2 = 0; m2 < R2; ++m2) {
       const double a = -two_pi * (double)(k1 * m2) / (double)n;
-      h[k1 * R2 + m2] = make_float2((float)std::cos(a), (float)std::sin(a));
+      h->push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
     }
+}
+
+}  // namespace
+
+bool fftpass_supported(const NufftGeom& g) {
+  if (g.Gx != g.Gy || g.Gx != 2 * g.Nx || g.Ny != g.Nx) return false;
+  const int l = log2_exact(g.Gx);
+  if (l < 4 || l > 10) return false;
+  if (g.dim == 2) return true;
+  const int lz = log2_exact(g.Gz);
+  return g.Gz == 2 * g.Nz && lz >= 4 && lz <= 10;
+}
+
+uint64_t fftpass_scratch(const NufftGeom& g, int B) {
+  // 2-D: Nx rows of Gy per grid.  3-D: Nz*Nx rows of Gy, then Nz slabs of Gx*Gy.
+  const uint64_t rows = (uint64_t)g.Nx * g.Nz * g.Gy;
+  return (uint64_t)B * (g.dim == 2 ? rows : rows + (uint64_t)g.Nz * g.Gx * g.Gy);
+}
+
+pg_status fftpass_twiddles(const NufftGeom& g, DevBuf<float2>* tw, cudaStream_t s) {
+  std::vector<float2> h;
+  twiddle_table(g.Gx, &h);
+  if (g.dim == 3) twiddle_table(g.Gz, &h);   // the z table follows the in-plane one
   return tw->upload(h.data(), h.size(), s);
 }
 
-pg_status fft2d_forward(const NufftGeom& g, int B, int L, const float2* x, const float2* S, int c0, const float2* E,
-                        const float2* Wo, const float* deapf, const float2* tw, float2* P, float2* grids,
-                        cudaStream_t s) {
-  switch (log2_exact(g.Gx)) {
-    case 6: return forward_t<6>(g, B, L, x, S, c0, E, Wo, deapf, tw, P, grids, s);
-    case 7: return forward_t<7>(g, B, L, x, S, c0, E, Wo, deapf, tw, P, grids, s);
-    case 8: return forward_t<8>(g, B, L, x, S, c0, E, Wo, deapf, tw, P, grids, s);
-    case 9: return forward_t<9>(g, B, L, x, S, c0, E, Wo, deapf, tw, P, grids, s);
-    case 10: return forward_t<10>(g, B, L, x, S, c0, E, Wo, deapf, tw, P, grids, s);
+pg_status fftpass_forward(const NufftGeom& g, int B, int L, const float2* x, const float2* S, int c0,
+                          const float2* E, const float2* Wo, const float* deapf, const float2* tw, float2* P,
+                          float2* grids, cudaStream_t s) {
+  if (B > kMaxGridY) return set_error(PG_INVALID_ARG, "fft passes: batch of %d grids", B);
+  const int lg = log2_exact(g.Gx);
+  const uint64_t plane = (uint64_t)g.Gx * g.Gy;
+  PG_TRY(d_rows_fwd(lg, g, B, L, x, S, c0, E, Wo, deapf, tw, P, s));
+  if (g.dim == 2) {
+    const Lines ln{(uint64_t)g.Nx * g.Gy, plane, (uint64_t)g.Gy, g.Gy, g.Nx, g.pad_off[0]};
+    return d_cols_fwd(lg, ln, B, P, tw, grids, s);
   }
-  return set_error(PG_INVALID_ARG, "fft2d: unsupported grid %d", g.Gx);
+  // x lines per nonzero z-slab, then z lines over every (x, y) column
+  float2* P2 = P + (uint64_t)B * g.Nz * g.Nx * g.Gy;
+  const Lines lx{(uint64_t)g.Nx * g.Gy, plane, (uint64_t)g.Gy, g.Gy, g.Nx, g.pad_off[0]};
+  const int slabs = B * g.Nz;
+  for (int s0 = 0; s0 < slabs; s0 += kMaxGridY)
+    PG_TRY(d_cols_fwd(lg, lx, std::min(kMaxGridY, slabs - s0), P + s0 * lx.in_bstride, tw,
+                      P2 + s0 * lx.out_bstride, s));
+  const Lines lz{(uint64_t)g.Nz * plane, g.ngrid(), plane, (int)plane, g.Nz, g.pad_off[2]};
+  return d_cols_fwd(log2_exact(g.Gz), lz, B, P2, tw + g.Gx, grids, s);
 }
 
-pg_status fft2d_adjoint(const NufftGeom& g, int B, int L, const float2* grids, const float2* S, int c0,
-                        const float2* E, const float2* WoH, const float* deapf, const float2* tw, float2* Q,
-                        float2* Rimg, int accumulate, float2* x, cudaStream_t s) {
-  pg_status st = PG_INVALID_ARG;
-  switch (log2_exact(g.Gx)) {
-    case 6: st = adjoint_t<6>(g, B, L, grids, S, c0, E, WoH, deapf, tw, Q, Rimg, s); break;
-    case 7: st = adjoint_t<7>(g, B, L, grids, S, c0, E, WoH, deapf, tw, Q, Rimg, s); break;
-    case 8: st = adjoint_t<8>(g, B, L, grids, S, c0, E, WoH, deapf, tw, Q, Rimg, s); break;
-    case 9: st = adjoint_t<9>(g, B, L, grids, S, c0, E, WoH, deapf, tw, Q, Rimg, s); break;
-    case 10: st = adjoint_t<10>(g, B, L, grids, S, c0, E, WoH, deapf, tw, Q, Rimg, s); break;
-    default: return set_error(PG_INVALID_ARG, "fft2d: unsupported grid %d", g.Gx);
+pg_status fftpass_adjoint(const NufftGeom& g, int B, int L, const float2* grids, const float2* S, int c0,
+                          const float2* E, const float2* WoH, const float* deapf, const float2* tw, float2* Q,
+                          float2* Rimg, int accumulate, float2* x, cudaStream_t s) {
+  if (B > kMaxGridY) return set_error(PG_INVALID_ARG, "fft passes: batch of %d grids", B);
+  const int lg = log2_exact(g.Gx);
+  const uint64_t plane = (uint64_t)g.Gx * g.Gy;
+  float2* Qr = Q;   // the rows the last pass reads
+  if (g.dim == 2) {
+    const Lines ln{plane, (uint64_t)g.Nx * g.Gy, (uint64_t)g.Gy, g.Gy, g.Nx, g.crop_off[0]};
+    PG_TRY(d_cols_inv(lg, ln, B, grids, tw, Q, s));
+  } else {
+    // z lines keeping the Nz cropped slabs, then x lines per slab keeping Nx rows
+    float2* Q1 = Q + (uint64_t)B * g.Nz * g.Nx * g.Gy;
+    const Lines lz{g.ngrid(), (uint64_t)g.Nz * plane, plane, (int)plane, g.Nz, g.crop_off[2]};
+    PG_TRY(d_cols_inv(log2_exact(g.Gz), lz, B, grids, tw + g.Gx, Q1, s));
+    const Lines lx{plane, (uint64_t)g.Nx * g.Gy, (uint64_t)g.Gy, g.Gy, g.Nx, g.crop_off[0]};
+    const int slabs = B * g.Nz;
+    for (int s0 = 0; s0 < slabs; s0 += kMaxGridY)
+      PG_TRY(d_cols_inv(lg, lx, std::min(kMaxGridY, slabs - s0), Q1 + s0 * lx.in_bstride, tw,
+                        Q + s0 * lx.out_bstride, s));
   }
-  if (st != PG_OK) return st;
+  PG_TRY(d_rows_inv(lg, g, B, L, Qr, S, c0, E, WoH, deapf, tw, Rimg, s));
   const uint64_t N = g.nimg();
   PG_LAUNCH(k_sum_images, ceil_div(N * 8, 256), 256, 0, s, N, B, Rimg, accumulate, x);
   return PG_OK;

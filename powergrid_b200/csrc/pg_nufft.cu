@@ -29,7 +29,7 @@
 #include <tuple>
 
 #include "pg_binsort.cuh"
-#include "pg_fft2d.cuh"
+#include "pg_fftpass.cuh"
 #include "pg_kb.cuh"
 #include "pg_nufft.cuh"
 #include "pg_profile.cuh"
@@ -790,11 +790,11 @@ pg_status nufft_plan_create(std::unique_ptr<NufftPlan>* out, uint64_t M, float g
   PG_TRY(p->lut.upload(lut.data(), lut.size(), s));
   p->lut_max = *std::max_element(lut.begin(), lut.end());
   PG_TRY(p->deap.upload(deap.data(), deap.size(), s));
-  // power-of-two 2-D grids run the pruned, fused FFT passes; PG_CUFFT=1 keeps cuFFT
+  // power-of-two 2N grids run the pruned, fused FFT passes; PG_CUFFT=1 keeps cuFFT
   {
     const char* e = getenv("PG_CUFFT");
-    p->own_fft = fft2d_supported(g) && !(e && e[0] == '1');
-    if (p->own_fft) PG_TRY(fft2d_twiddles(g, &p->tw2d, s));
+    p->own_fft = fftpass_supported(g) && !(e && e[0] == '1');
+    if (p->own_fft) PG_TRY(fftpass_twiddles(g, &p->tw2d, s));
   }
   // Per-voxel deapodization factor 1/(OS^d k), k the product of the axis
   // factors in float as the reference forms it; 0 where k is NaN (the
@@ -1204,9 +1204,9 @@ pg_status nufft_forward(NufftPlan* p, const NufftBatch& b, const float2* x, floa
     const int B = nb * L;
     if (p->own_fft) {
       PG_TRY(ensure_workspace(p, B, nullptr, s));
-      PG_TRY(grow(p->work->fin, (uint64_t)B * G / 2, s));
+      PG_TRY(grow(p->work->fin, fftpass_scratch(g, B), s));
       ProfScope ps("fft_fwd", s);
-      PG_TRY(fft2d_forward(g, B, L, x, b.S, c0, b.E, b.Wo, p->deapf.p, p->tw2d.p, p->work->fin.p,
+      PG_TRY(fftpass_forward(g, B, L, x, b.S, c0, b.E, b.Wo, p->deapf.p, p->tw2d.p, p->work->fin.p,
                            p->work->grids.p, s));
     } else {
     cufftHandle h;
@@ -1283,10 +1283,10 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
     }
     const int acc = (b.accumulate || c0 > 0) ? 1 : 0;
     if (p->own_fft) {
-      PG_TRY(grow(p->work->fin, (uint64_t)B * G / 2, s));
+      PG_TRY(grow(p->work->fin, fftpass_scratch(g, B), s));
       PG_TRY(grow(p->work->rimg, (uint64_t)B * g.nimg(), s));
       ProfScope ps("fft_adj", s);
-      PG_TRY(fft2d_adjoint(g, B, L, p->work->grids.p, b.S, c0, b.E, b.WoH, p->deapf.p, p->tw2d.p, p->work->fin.p,
+      PG_TRY(fftpass_adjoint(g, B, L, p->work->grids.p, b.S, c0, b.E, b.WoH, p->deapf.p, p->tw2d.p, p->work->fin.p,
                            p->work->rimg.p, acc, x, s));
       continue;
     }

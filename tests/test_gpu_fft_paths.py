@@ -1,9 +1,10 @@
 """The oversampled-FFT stage in both of its forms, and gridding edge cases.
 
-2-D operators on power-of-two grids run the library's own pruned FFT passes
-(with the pre/post kernels fused in); PG_CUFFT=1 at construction keeps the
-cuFFT form.  Both must agree with each other and with the reference CPU path
-at every supported grid size (64 ... 1024), and the gridding must handle the
+Operators on power-of-two 2N grids (2-D and 3-D) run the library's own
+pruned FFT passes (with the pre/post kernels fused in); PG_CUFFT=1 at
+construction keeps the cuFFT form.  Both must agree with each other and with
+the reference CPU path at the supported grid sizes (in-plane 64 ... 1024, z
+16 ... 128 here), and the gridding must handle the
 trajectory edges the reference's clamped windows define (samples on the
 -N/2 border, a single sample, all samples in one tile).
 
@@ -24,18 +25,34 @@ OP_TOL = 1e-5
 FORMS_TOL = 2e-6
 
 
-def _ts_sense(pg, n, M, L, nc, seed):
+def _ts_sense(pg, n, M, L, nc, seed, nz=1):
     from powergrid_b200 import synthetic as S
     rng = S.Rng(seed)
     inter = max(1, M // 2048)
-    kx, ky, t = S.spiral(n, inter, M // inter, 10e-3)
-    kz = np.zeros_like(kx)
-    fm = S.field_map(rng, n, n, 1, 80.0)
-    sm = S.coil_maps(rng, n, n, 1, nc)
-    G = pg.Gnufft(kx.size, 2.0, n, n, 1, kx, ky, kz)
-    A = pg.TimeSegmentation(G, fm, t, kx.size, n * n, L, 1, 1)
-    Sg = pg.SENSE(A, sm, kx.size, n * n, nc)
+    if nz == 1:
+        kx, ky, t = S.spiral(n, inter, M // inter, 10e-3)
+        kz = np.zeros_like(kx)
+    else:
+        kx, ky, kz, t = S.stack_of_spirals(n, nz, inter, M // inter, 10e-3)
+    fm = S.field_map(rng, n, n, nz, 80.0)
+    sm = S.coil_maps(rng, n, n, nz, nc)
+    N = n * n * nz
+    G = pg.Gnufft(kx.size, 2.0, n, n, nz, kx, ky, kz)
+    A = pg.TimeSegmentation(G, fm, t, kx.size, N, L, 1, 1)
+    Sg = pg.SENSE(A, sm, kx.size, N, nc)
     return (kx, ky, kz, t, fm, sm), (G, A, Sg)
+
+
+def _cufft_form(build):
+    old = os.environ.get("PG_CUFFT")
+    os.environ["PG_CUFFT"] = "1"
+    try:
+        return build()
+    finally:
+        if old is None:
+            del os.environ["PG_CUFFT"]
+        else:
+            os.environ["PG_CUFFT"] = old
 
 
 @pytest.mark.parametrize("n", [32, 64, 128, 256, 512])
@@ -45,15 +62,7 @@ def test_own_fft_passes_match_cufft(pg, n):
     from powergrid_b200 import synthetic as S
     M = 8192 if n <= 128 else 32768
     arrays, own = _ts_sense(pg, n, M, 4, 2, 40 + n)
-    old = os.environ.get("PG_CUFFT")
-    os.environ["PG_CUFFT"] = "1"
-    try:
-        _, ref = _ts_sense(pg, n, M, 4, 2, 40 + n)
-    finally:
-        if old is None:
-            del os.environ["PG_CUFFT"]
-        else:
-            os.environ["PG_CUFFT"] = old
+    _, ref = _cufft_form(lambda: _ts_sense(pg, n, M, 4, 2, 40 + n))
     x = S.image(S.Rng(7), n * n)
     y1, y2 = own[2] * x, ref[2] * x
     e_f = rel_l2(y1, y2)
@@ -77,6 +86,39 @@ def test_own_fft_passes_vs_reference(pg, oracle, n):
     e_f = rel_l2(G * x, ref.forward(x))
     e_a = rel_l2(G / y, ref.adjoint(y))
     print(f"n={n}: forward {e_f:.2e}, adjoint {e_a:.2e}")
+    assert e_f <= OP_TOL and e_a <= OP_TOL
+
+
+@pytest.mark.parametrize("n,nz", [(8, 8), (16, 32), (32, 16), (64, 8), (128, 64)])
+def test_own_fft_passes_3d_match_cufft(pg, n, nz):
+    """3-D SENSE<TS<Gnufft>> (L=3, 2 coils) with the own FFT passes and with
+    cuFFT, from 16 x 16 x 16 up to the 256 x 256 x 128 grid of a 128^2 x 64
+    volume; the z length differs from the in-plane one in most cases."""
+    from powergrid_b200 import synthetic as S
+    per_plane = 1024
+    _, own = _ts_sense(pg, n, per_plane, 3, 2, 70 + n + nz, nz=nz)
+    _, ref = _cufft_form(lambda: _ts_sense(pg, n, per_plane, 3, 2, 70 + n + nz, nz=nz))
+    x = S.image(S.Rng(9), n * n * nz)
+    y1, y2 = own[2] * x, ref[2] * x
+    e_f = rel_l2(y1, y2)
+    e_a = rel_l2(own[2] / y2, ref[2] / y2)
+    print(f"{n}x{n}x{nz}: forward {e_f:.2e}, adjoint {e_a:.2e}")
+    assert e_f <= FORMS_TOL and e_a <= FORMS_TOL
+
+
+@pytest.mark.parametrize("n,nz", [(16, 8), (32, 16)])
+def test_own_fft_passes_3d_vs_reference(pg, oracle, n, nz):
+    """Gnufft 3-D on the own FFT passes against the reference CPU path."""
+    from powergrid_b200 import synthetic as S
+    kx, ky, kz, t = S.stack_of_spirals(n, nz, 2, 256, 5e-3)
+    M = kx.size
+    G = pg.Gnufft(M, 2.0, n, n, nz, kx, ky, kz)
+    ref = oracle.gnufft(0, M, n, n, nz, kx, ky, kz)
+    x = S.image(S.Rng(13), n * n * nz)
+    y = S.image(S.Rng(14), M)
+    e_f = rel_l2(G * x, ref.forward(x))
+    e_a = rel_l2(G / y, ref.adjoint(y))
+    print(f"{n}x{n}x{nz}: forward {e_f:.2e}, adjoint {e_a:.2e}")
     assert e_f <= OP_TOL and e_a <= OP_TOL
 
 
