@@ -5,7 +5,10 @@
 //   TimeSegmentation<T1, Tobj>   TimeSegmentation.h:70-71
 //   SENSE<T1, Tobj>       SENSE.h:64
 //   pcSenseTimeSeg<T1>    pcSenseTimeSeg.h:80-82
+//   pcSENSE<T1>           pcSENSE.h:76-78
+//   LRobj<T1, Gobj>       lowRank/LRobj.h:55
 //   QuadPenalty<T1>, TVPenalty<T1>   QuadPenalty.h:43, TVPenalty.h:42
+//   R_lowRank<T1, Robj>   lowRank/R_lowRank.h:52
 //   solve_pwls_pcg        solve_pwls_pcg.hpp:48-51
 //   reconSolve            reconSolve.h:63-66
 // with T1 = float.  Column types: any type with memptr() (or data()),
@@ -226,6 +229,23 @@ class pcSENSE : public Operator {
   }
 };
 
+// LRobj(NimgSize, N_data, n_rank, n_img, vBasis, All) (lowRank/LRobj.h:55):
+// vBasis is n_rank x n_img (any column-major matrix with memptr()); All holds
+// n_img operators, borrowed as the reference's raw pointers are.
+template <typename T1, typename Gobj>
+class LRobj : public Operator {
+ public:
+  template <typename CxMat>
+  LRobj(uword NimgSize, uword N_data, uword n_rank, uword n_img, const CxMat& vBasis, Gobj** All) {
+    std::vector<pg_op> ops(n_img);
+    for (uword i = 0; i < n_img; ++i) ops[i] = All[i]->handle();
+    pg_op h = nullptr;
+    check(pg_lowrank_create(&h, NimgSize, N_data, n_rank, n_img,
+                            reinterpret_cast<const float*>(detail::ptr(vBasis)), ops.data()));
+    adopt(h);
+  }
+};
+
 // calc3DDensityCompensation (reconSupport/directRecon.cpp:28-61).
 template <typename T1, typename RCol>
 RCol calc3DDensityCompensation(const RCol& kx, const RCol& ky, const RCol& kz, uword Ninplane, uword Nz) {
@@ -268,15 +288,45 @@ struct TVPenalty {
       : p{PG_PENALTY_TV, nx, ny, nz, (float)beta, (float)delta, dims2penalize} {}
 };
 
-// solve_pwls_pcg(xInitial, A, W, yi, R, niter) on the device.
+// R_lowRank(R1, rank, nImages, vBasis) (lowRank/R_lowRank.h:52): R1 applied
+// to the columns of X * vBasis^H.  vBasis is rank x nImages; as in the
+// reference, a solve needs rank == nImages.
+template <typename T1, typename Robj>
+struct R_lowRank {
+  pg_penalty p;
+  uword Nrank, Nimg;
+  std::vector<std::complex<float>> v;
+  template <typename CxMat>
+  R_lowRank(const Robj& R1, uword rank, uword nImages, const CxMat& vBasis)
+      : p(R1.p), Nrank(rank), Nimg(nImages),
+        v(reinterpret_cast<const std::complex<float>*>(detail::ptr(vBasis)),
+          reinterpret_cast<const std::complex<float>*>(detail::ptr(vBasis)) + rank * nImages) {}
+};
+
+namespace detail {
+template <typename R>
+struct is_lowrank : std::false_type {};
+template <typename T1, typename Robj>
+struct is_lowrank<R_lowRank<T1, Robj>> : std::true_type {};
+}  // namespace detail
+
+// solve_pwls_pcg(xInitial, A, W, yi, R, niter) on the device (a QuadPenalty,
+// TVPenalty or R_lowRank R).
 template <typename T1, typename Tobj, typename Robj, typename CxCol, typename RCol>
 CxCol solve_pwls_pcg(const CxCol& xInitial, const Tobj& A, const RCol& W, const CxCol& yi, const Robj& R,
                      uword niter) {
   CxCol x(A.n_image());
   uint64_t done = 0;
-  check(pg_pcg_solve(A.handle(), reinterpret_cast<const float*>(detail::ptr(xInitial)), detail::ptr(W),
-                     reinterpret_cast<const float*>(detail::ptr(yi)), &R.p, niter,
-                     reinterpret_cast<float*>(detail::mptr(x)), &done));
+  if constexpr (detail::is_lowrank<Robj>::value) {
+    check(pg_pcg_solve_lowrank(A.handle(), reinterpret_cast<const float*>(detail::ptr(xInitial)), detail::ptr(W),
+                               reinterpret_cast<const float*>(detail::ptr(yi)), &R.p, R.Nrank, R.Nimg,
+                               reinterpret_cast<const float*>(R.v.data()), niter,
+                               reinterpret_cast<float*>(detail::mptr(x)), &done));
+  } else {
+    check(pg_pcg_solve(A.handle(), reinterpret_cast<const float*>(detail::ptr(xInitial)), detail::ptr(W),
+                       reinterpret_cast<const float*>(detail::ptr(yi)), &R.p, niter,
+                       reinterpret_cast<float*>(detail::mptr(x)), &done));
+  }
   return x;
 }
 

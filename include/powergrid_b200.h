@@ -111,6 +111,20 @@ pg_status pg_pcsense_create(pg_op* out, const float* kx, const float* ky, const 
                             uint64_t ny, uint64_t nz, uint64_t nc, const float* t, const float* sense_map,
                             const float* field_map, const float* shot_phase_map, uint64_t n_shot_phase);
 
+/* LRobj(NimgSize, N_data, n_rank, n_img, vBasis, All) replaces
+ * LRobj<float, Gobj>::LRobj (lowRank/LRobj.h:55, LRobj.cpp:27-35): the
+ * partial-separability model x = vec(X), X n_image x rank, whose image i is
+ * column i of X * vBasis and goes through ops[i] (operator*, LRobj.cpp:38-50);
+ * the adjoint applies ops[i]^H to data column i and multiplies the
+ * n_image x n_img stack by vBasis^H (LRobj.cpp:53-66).  v: rank x n_img
+ * complex, column-major (interleaved float pairs).  Every ops[i] must be
+ * n_data x n_image (a pcSENSE or pcSenseTimeSeg plan, or any operator of
+ * that shape); they are borrowed and must outlive the model, as the
+ * reference holds raw pointers.  The model is (n_data*n_img) x
+ * (n_image*rank). */
+pg_status pg_lowrank_create(pg_op* out, uint64_t n_image, uint64_t n_data, uint64_t rank, uint64_t n_img,
+                            const float* v, const pg_op* ops);
+
 pg_status pg_op_destroy(pg_op op);
 /* Lengths of the data vector (operator* output) and image vector. */
 pg_status pg_op_shape(pg_op op, uint64_t* n_data, uint64_t* n_image);
@@ -205,6 +219,30 @@ pg_status pg_recon_solve(pg_op Sg, const pg_penalty* R, const float* data, uint6
 /* Penalty pieces (Robject.cpp:143-193) on device buffers, for tests. */
 pg_status pg_penalty_gradient_device(const pg_penalty* R, const void* x_dev, void* g_dev, void* stream);
 pg_status pg_penalty_denom_device(const pg_penalty* R, const void* ddir_dev, const void* x_dev, double* out_host);
+
+/* solve_pwls_pcg(xInitial, A, W, yi, R_lr, niter) with
+ * R_lr = R_lowRank(R, rank, nImages, vBasis) (lowRank/R_lowRank.h:52,
+ * R_lowRank.cpp:27-95; composed so in lowRank/oscillateRecon.cpp:256-265):
+ * R (nx*ny*nz = the model's image length) applied to the columns of
+ * X * vBasis^H.  As in the reference, the wrapper's gradient is
+ * vectorise(strans(vBasis) * strans(Y)) -- stored rank-fastest -- which is
+ * defined only when rank == n_img (PG_INVALID_ARG otherwise), and its Denom
+ * is beta * sum_i R.Denom(...), R.Denom already carrying beta.  v: rank x
+ * n_img complex, column-major.  The step scalars are FP64 on the host (one
+ * synchronisation per inner product).  Host buffers. */
+pg_status pg_pcg_solve_lowrank(pg_op A, const float* x0, const float* W, const float* y, const pg_penalty* R,
+                               uint64_t rank, uint64_t n_img, const float* v, uint64_t niter, float* x_out,
+                               uint64_t* iters_done);
+/* The same on device buffers (v stays a host array); returns after the
+ * solve (iters_done is a host pointer, may be NULL). */
+pg_status pg_pcg_solve_lowrank_device(pg_op A, const void* x0_dev, const void* W_dev, const void* y_dev,
+                                      const pg_penalty* R, uint64_t rank, uint64_t n_img, const float* v,
+                                      uint64_t niter, void* x_out_dev, uint64_t* iters_done, void* stream);
+/* R_lowRank::Gradient and ::Denom (R_lowRank.cpp:50-87) on device buffers, for tests. */
+pg_status pg_lowrank_penalty_gradient_device(const pg_penalty* R, uint64_t rank, uint64_t n_img, const float* v,
+                                             const void* x_dev, void* g_dev, void* stream);
+pg_status pg_lowrank_penalty_denom_device(const pg_penalty* R, uint64_t rank, uint64_t n_img, const float* v,
+                                          const void* ddir_dev, const void* x_dev, double* out_host);
 
 /* ---- request server (continuous batching) ---------------------------- */
 typedef struct pg_server_config {

@@ -69,6 +69,14 @@ def lib() -> C.CDLL:
         L.orc_pcg.argtypes = [P, P, P, P, C.c_int, U64, U64, U64, C.c_double, C.c_double, U64, U64, P]
         L.orc_penalty_gradient.argtypes = [C.c_int, C.c_int, U64, U64, U64, C.c_double, C.c_double, U64, P, P]
         L.orc_penalty_denom.argtypes = [C.c_int, C.c_int, U64, U64, U64, C.c_double, C.c_double, U64, P, P, P]
+        L.orc_lowrank_new.restype = P
+        L.orc_lowrank_new.argtypes = [U64, U64, U64, U64, P, P]
+        L.orc_pcg_lowrank.argtypes = [P, P, P, P, C.c_int, U64, U64, U64, C.c_double, C.c_double, U64, U64, P, U64,
+                                      P]
+        L.orc_lowrank_gradient.argtypes = [C.c_int, C.c_int, U64, U64, U64, C.c_double, C.c_double, U64, U64, P, P,
+                                           P]
+        L.orc_lowrank_denom.argtypes = [C.c_int, C.c_int, U64, U64, U64, C.c_double, C.c_double, U64, U64, P, P, P,
+                                        P]
         L.orc_kb_lut.argtypes = [C.c_int, C.c_float, P, U64, P]
         L.orc_timeseg_tables.argtypes = [P, P, P, P, P]
         L.orc_fft.argtypes = [C.c_int, P, P, C.c_int, C.c_int]
@@ -279,6 +287,51 @@ def penalty_denom(prec, kind, nx, ny, nz, beta, delta, dims2pen, ddir, x):
     out = np.zeros(2)
     lib().orc_penalty_denom(prec, {"quad": 0, "tv": 1}[kind], nx, ny, nz, beta, delta, dims2pen, _p(d), _p(x),
                             _p(out))
+    return complex(out[0], out[1])
+
+
+def _basis(v, rank, nimg):
+    """rank x nimg complex basis, column-major, as interleaved float32 pairs."""
+    v = np.asarray(v, dtype=C64).reshape(rank, nimg, order="F")
+    return np.ascontiguousarray(v.reshape(-1, order="F")).view(F32)
+
+
+def lowrank(n_image, n_data, rank, nimg, v, ops) -> Op:
+    """LRobj (lowRank/LRobj.cpp:27-68) over oracle operators (borrowed: kept alive here)."""
+    vb = _basis(v, rank, nimg)
+    hs = (C.c_void_p * nimg)(*[o.h for o in ops])
+    h = lib().orc_lowrank_new(n_image, n_data, rank, nimg, _p(vb), C.cast(hs, C.c_void_p))
+    return Op(h, ops[0].prec, keep=list(ops))
+
+
+def pcg_lowrank(op: Op, y, penalty: str, nx, ny, nz, beta, rank, v, delta=1.0, dims2pen=3, niter=10, x0=None,
+                W=None):
+    """solve_pwls_pcg with R_lowRank (lowRank/R_lowRank.cpp:27-95); v: rank x rank basis."""
+    y = np.ascontiguousarray(y, dtype=op.cdtype)
+    x = np.zeros(op.n_image, dtype=op.cdtype)
+    x0p = None if x0 is None else _p(np.ascontiguousarray(x0, dtype=op.cdtype))
+    Wa = None if W is None else np.ascontiguousarray(W, dtype=op.rdtype)
+    vb = _basis(v, rank, rank)
+    n = lib().orc_pcg_lowrank(op.h, x0p, None if Wa is None else _p(Wa), _p(y), {"quad": 0, "tv": 1}[penalty], nx,
+                              ny, nz, beta, delta, dims2pen, rank, _p(vb), niter, _p(x))
+    return x, n
+
+
+def lowrank_gradient(prec, kind, nx, ny, nz, beta, delta, dims2pen, rank, v, x):
+    x = np.ascontiguousarray(x, dtype=C64 if prec == 0 else C128)
+    g = np.zeros_like(x)
+    lib().orc_lowrank_gradient(prec, {"quad": 0, "tv": 1}[kind], nx, ny, nz, beta, delta, dims2pen, rank,
+                               _p(_basis(v, rank, rank)), _p(x), _p(g))
+    return g
+
+
+def lowrank_denom(prec, kind, nx, ny, nz, beta, delta, dims2pen, rank, v, ddir, x):
+    ct = C64 if prec == 0 else C128
+    d = np.ascontiguousarray(ddir, dtype=ct)
+    x = np.ascontiguousarray(x, dtype=ct)
+    out = np.zeros(2)
+    lib().orc_lowrank_denom(prec, {"quad": 0, "tv": 1}[kind], nx, ny, nz, beta, delta, dims2pen, rank,
+                            _p(_basis(v, rank, rank)), _p(d), _p(x), _p(out))
     return complex(out[0], out[1])
 
 

@@ -142,6 +142,18 @@ void* guard(F fn) {
 
 }  // namespace
 
+namespace {
+template <typename T>
+pgo::LowRankPenalty<T> lowrank_penalty(const pgo::Penalty<T>& R, u64 rank, const float* v) {
+  pgo::LowRankPenalty<T> P;
+  P.R = &R;
+  P.K = rank;
+  P.v.resize(rank * rank);
+  for (u64 i = 0; i < rank * rank; ++i) P.v[i] = std::complex<T>((T)v[2 * i], (T)v[2 * i + 1]);
+  return P;
+}
+}  // namespace
+
 extern "C" {
 
 const char* orc_last_error() { return g_err.c_str(); }
@@ -429,6 +441,73 @@ int orc_pcg(void* h, const void* x0, const void* W, const void* y, int kind, u64
   };
   if (o->prec == 0) return run(o->f.get(), float());
   return run(o->d.get(), double());
+}
+
+// LRobj over oracle operators (lowRank/LRobj.cpp:27-68); the operators are
+// borrowed and must outlive it.  v: rank x n_img complex float, column-major.
+void* orc_lowrank_new(u64 n_image, u64 n_data, u64 rank, u64 n_img, const float* v, void* const* ops) {
+  return guard([&]() -> void* {
+    const int prec = ((Handle*)ops[0])->prec;
+    auto* h = new Handle;
+    h->prec = prec;
+    auto make = [&](auto tag) {
+      using T = decltype(tag);
+      std::vector<std::complex<T>> vb(rank * n_img);
+      for (u64 i = 0; i < rank * n_img; ++i) vb[i] = std::complex<T>((T)v[2 * i], (T)v[2 * i + 1]);
+      std::vector<const pgo::Op<T>*> A;
+      for (u64 i = 0; i < n_img; ++i) A.push_back(get<T>((Handle*)ops[i]));
+      set<T>(h, new pgo::LowRankOp<T>(n_image, n_data, rank, n_img, vb.data(), A));
+    };
+    if (prec == 0) make(float()); else make(double());
+    return h;
+  });
+}
+
+// solve_pwls_pcg<T1, LRobj, R_lowRank> (lowRank/oscillateRecon.cpp:260-265
+// composes it); R_lowRank's basis is rank x rank (rank == number of images).
+int orc_pcg_lowrank(void* h, const void* x0, const void* W, const void* y, int kind, u64 nx, u64 ny, u64 nz,
+                    double beta, double delta, u64 dims2pen, u64 rank, const float* v, u64 niter, void* xout) {
+  Handle* o = (Handle*)h;
+  auto run = [&](auto* op, auto tag) -> int {
+    using T = decltype(tag);
+    pgo::Penalty<T> R;
+    R.kind = kind; R.Nx = nx; R.Ny = ny; R.Nz = nz; R.beta = (T)beta; R.delta = (T)delta; R.dims2pen = dims2pen;
+    const pgo::LowRankPenalty<T> P = lowrank_penalty(R, rank, v);
+    const u64 nd = pgo::op_data_len(*op), ni = pgo::op_image_len(*op);
+    std::vector<T> w(nd, (T)1);
+    if (W) std::memcpy(w.data(), W, sizeof(T) * nd);
+    std::vector<std::complex<T>> xi(ni, std::complex<T>(0, 0));
+    if (x0) std::memcpy(xi.data(), x0, sizeof(std::complex<T>) * ni);
+    return pgo::pwls_pcg<T>(*op, xi.data(), w.data(), (const std::complex<T>*)y, P, niter,
+                            (std::complex<T>*)xout);
+  };
+  if (o->prec == 0) return run(o->f.get(), float());
+  return run(o->d.get(), double());
+}
+
+// R_lowRank pieces for unit tests (lowRank/R_lowRank.cpp:50-87).
+int orc_lowrank_gradient(int prec, int kind, u64 nx, u64 ny, u64 nz, double beta, double delta, u64 dims2pen,
+                         u64 rank, const float* v, const void* x, void* g) {
+  auto run = [&](auto tag) {
+    using T = decltype(tag);
+    pgo::Penalty<T> R;
+    R.kind = kind; R.Nx = nx; R.Ny = ny; R.Nz = nz; R.beta = (T)beta; R.delta = (T)delta; R.dims2pen = dims2pen;
+    lowrank_penalty(R, rank, v).Gradient((const std::complex<T>*)x, (std::complex<T>*)g);
+  };
+  if (prec == 0) run(float()); else run(double());
+  return 0;
+}
+int orc_lowrank_denom(int prec, int kind, u64 nx, u64 ny, u64 nz, double beta, double delta, u64 dims2pen,
+                      u64 rank, const float* v, const void* ddir, const void* x, double* out2) {
+  auto run = [&](auto tag) {
+    using T = decltype(tag);
+    pgo::Penalty<T> R;
+    R.kind = kind; R.Nx = nx; R.Ny = ny; R.Nz = nz; R.beta = (T)beta; R.delta = (T)delta; R.dims2pen = dims2pen;
+    auto d = lowrank_penalty(R, rank, v).Denom((const std::complex<T>*)ddir, (const std::complex<T>*)x);
+    out2[0] = d.real(); out2[1] = d.imag();
+  };
+  if (prec == 0) run(float()); else run(double());
+  return 0;
 }
 
 // Regularizer pieces for unit tests: Gradient and Denom (Robject.cpp:143-193).

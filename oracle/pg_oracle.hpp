@@ -14,6 +14,7 @@
 //   GdftR2              GdftR2.cpp:32-150, ftCpuWithGrads.cpp:76-216
 //   spatial interpolation, density compensation   Gnufft.cpp:213-337, reconSupport/directRecon.cpp:28-73
 //   Robject/Quad/TV     Robject.cpp:49-193, QuadPenalty.cpp:45-64, TVPenalty.cpp:43-68
+//   LRobj, R_lowRank    lowRank/LRobj.cpp:27-68, lowRank/R_lowRank.cpp:27-95
 //   solve_pwls_pcg      solve_pwls_pcg.hpp:34-167
 //
 // Expressions keep the reference's operand types and evaluation order, so
@@ -1222,6 +1223,50 @@ struct PcSenseOp : Op<T> {
   }
 };
 
+// LRobj (lowRank/LRobj.cpp:27-68): the partial-separability model.  x = vec(X)
+// with X N x K (K = rank); operator* forms the images X v (v: K x Nimg,
+// column-major) and sends image i through A_all[i] (:39-50); operator/ applies
+// A_all[i] / d_i and multiplies the N x Nimg stack by trans(v) (conjugate
+// transpose, :53-66).  The per-image operators are borrowed, as the reference
+// holds raw pointers.
+template <typename T>
+struct LowRankOp : Op<T> {
+  using C = std::complex<T>;
+  u64 N, Nd, K, Ni;
+  std::vector<C> v;
+  std::vector<const Op<T>*> A;
+  LowRankOp(u64 n, u64 nd, u64 k, u64 ni, const C* vb, std::vector<const Op<T>*> ops)
+      : N(n), Nd(nd), K(k), Ni(ni), v(vb, vb + k * ni), A(std::move(ops)) {
+    if (A.size() != Ni) throw std::runtime_error("LRobj: one operator per image");
+    for (const Op<T>* a : A)
+      if (op_image_len(*a) != N || op_data_len(*a) != Nd)
+        throw std::runtime_error("LRobj: operator sizes differ from NimgSize / N_data");
+    this->n1 = Nd * Ni;
+    this->n2 = N * K;
+  }
+  void forward(const C* x, C* y) const override {
+    std::vector<C> img(N);
+    for (u64 i = 0; i < Ni; ++i) {
+      std::fill(img.begin(), img.end(), C(0, 0));
+      for (u64 k = 0; k < K; ++k) {
+        const C c = v[k + K * i];
+        for (u64 p = 0; p < N; ++p) img[p] += x[p + N * k] * c;
+      }
+      A[i]->forward(img.data(), y + Nd * i);
+    }
+  }
+  void adjoint(const C* d, C* x) const override {
+    std::vector<C> img(N * Ni);
+    for (u64 i = 0; i < Ni; ++i) A[i]->adjoint(d + Nd * i, img.data() + N * i);
+    std::fill(x, x + N * K, C(0, 0));
+    for (u64 k = 0; k < K; ++k)
+      for (u64 i = 0; i < Ni; ++i) {
+        const C c = std::conj(v[k + K * i]);
+        for (u64 p = 0; p < N; ++p) x[p + N * k] += img[p + N * i] * c;
+      }
+  }
+};
+
 // ---------------------------------------------------------------------------
 // Regularizers (Robject.cpp:49-193, QuadPenalty.cpp:45-64, TVPenalty.cpp:43-68)
 // ---------------------------------------------------------------------------
@@ -1286,6 +1331,53 @@ struct Penalty {
   }
 };
 
+// R_lowRank (lowRank/R_lowRank.cpp:27-95) over a Robject R.  With x = vec(X),
+// X N x K, it penalises the columns of I = X * trans(v.cols(0, K-1)) (:42-44;
+// trans is the conjugate transpose, so I[n, j] = sum_k X[n, k] conj(v[j, k])).
+// Gradient (:50-64) returns vectorise(strans(v.cols(0, K-1)) * strans(Y)) with
+// Y_j = R.Gradient(I_j): a K x N matrix, element [k + K*n].  That product is
+// defined only when K == Nimg (K x K times Nimg x N), so v here is K x K.
+// Denom (:67-87) is R.Beta * sum_j R.Denom(D_j, I_j), D = Ddir * trans(v), and
+// R.Denom already carries one factor beta.
+template <typename T>
+struct LowRankPenalty {
+  using C = std::complex<T>;
+  const Penalty<T>* R = nullptr;
+  u64 K = 1;
+  std::vector<C> v;   // K x K, column-major
+  u64 n() const { return R->Nx * R->Ny * R->Nz; }
+  void mix(const C* x, C* I) const {
+    const u64 N = n();
+    std::fill(I, I + N * K, C(0, 0));
+    for (u64 j = 0; j < K; ++j)
+      for (u64 k = 0; k < K; ++k) {
+        const C c = std::conj(v[j + K * k]);
+        for (u64 p = 0; p < N; ++p) I[p + N * j] += x[p + N * k] * c;
+      }
+  }
+  void Gradient(const C* x, C* g) const {
+    const u64 N = n();
+    std::vector<C> I(N * K), Y(N * K);
+    mix(x, I.data());
+    for (u64 j = 0; j < K; ++j) R->Gradient(I.data() + N * j, Y.data() + N * j);
+    for (u64 p = 0; p < N; ++p)
+      for (u64 k = 0; k < K; ++k) {
+        C acc(0, 0);
+        for (u64 j = 0; j < K; ++j) acc += v[j + K * k] * Y[p + N * j];
+        g[k + K * p] = acc;
+      }
+  }
+  C Denom(const C* ddir, const C* x) const {
+    const u64 N = n();
+    std::vector<C> I(N * K), D(N * K);
+    mix(x, I.data());
+    mix(ddir, D.data());
+    C sum(0, 0);
+    for (u64 j = 0; j < K; ++j) sum += R->Denom(D.data() + N * j, I.data() + N * j);
+    return R->beta * sum;
+  }
+};
+
 template <typename T>
 inline std::complex<T> cdot(const std::complex<T>* a, const std::complex<T>* b, u64 n) {
   std::complex<T> s(0, 0);
@@ -1295,9 +1387,9 @@ inline std::complex<T> cdot(const std::complex<T>* a, const std::complex<T>* b, 
 
 // solve_pwls_pcg (solve_pwls_pcg.hpp:48-167), scalars complex<T> as in the reference.
 // Returns the number of completed iterations.
-template <typename T>
+template <typename T, typename Robj>
 int pwls_pcg(const Op<T>& A, const std::complex<T>* x0, const T* W, const std::complex<T>* y,
-             const Penalty<T>& R, u64 niter, std::complex<T>* xout) {
+             const Robj& R, u64 niter, std::complex<T>* xout) {
   using C = std::complex<T>;
   const u64 nd = op_data_len(A), ni = op_image_len(A);
   std::vector<C> x(x0, x0 + ni), Ax(nd), r(nd), ngrad(ni), ddir(ni, C(0, 0)), Adir(nd), pgrad(ni), xs(ni);

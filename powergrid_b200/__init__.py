@@ -4,10 +4,10 @@ The compute lives in libpowergrid_b200.so (CUDA C++, C ABI in
 include/powergrid_b200.h).  This package is the Python host mirror of the
 reference's operator interface; importing it does not touch the GPU.
 """
-from .operators import (SENSE, Gdft, GdftR2, Gnufft, QuadPenalty, TimeSegmentation, TVPenalty,
+from .operators import (SENSE, Gdft, GdftR2, Gnufft, LRobj, QuadPenalty, R_lowRank, TimeSegmentation, TVPenalty,
                         calc3DDensityCompensation, calcSumOfSquaresImage, gridCoilImages, init, pcSENSE,
                         pcSenseTimeSeg, reconSolve, solve_pwls_pcg, solve_pwls_pcg_device)
 
-__all__ = ["Gnufft", "Gdft", "GdftR2", "TimeSegmentation", "SENSE", "pcSenseTimeSeg", "pcSENSE", "QuadPenalty",
-           "calc3DDensityCompensation", "gridCoilImages", "calcSumOfSquaresImage", "TVPenalty",
+__all__ = ["Gnufft", "Gdft", "GdftR2", "TimeSegmentation", "SENSE", "pcSenseTimeSeg", "pcSENSE", "LRobj", "QuadPenalty",
+           "calc3DDensityCompensation", "gridCoilImages", "calcSumOfSquaresImage", "TVPenalty", "R_lowRank",
            "solve_pwls_pcg", "solve_pwls_pcg_device", "reconSolve", "init"]

@@ -64,6 +64,7 @@ SIGNATURES = {
     "pg_pcsense_timeseg_create": (C.c_int, [C.POINTER(P), P, P, P, U64, U64, U64, U64, U64, P, U64, U64, P, P, P,
                                             U64]),
     "pg_pcsense_create": (C.c_int, [C.POINTER(P), P, P, P, U64, U64, U64, U64, U64, P, P, P, P, U64]),
+    "pg_lowrank_create": (C.c_int, [C.POINTER(P), U64, U64, U64, U64, P, P]),
     "pg_gnufft_grid_length": (C.c_int, [P, C.POINTER(U64)]),
     "pg_gnufft_forward_spatial_interp": (C.c_int, [P, P, P]),
     "pg_gnufft_adjoint_spatial_interp": (C.c_int, [P, P, P]),
@@ -84,6 +85,11 @@ SIGNATURES = {
     "pg_recon_solve": (C.c_int, [P, C.POINTER(Penalty), P, U64, P]),
     "pg_penalty_gradient_device": (C.c_int, [C.POINTER(Penalty), P, P, P]),
     "pg_penalty_denom_device": (C.c_int, [C.POINTER(Penalty), P, P, C.POINTER(C.c_double)]),
+    "pg_pcg_solve_lowrank": (C.c_int, [P, P, P, P, C.POINTER(Penalty), U64, U64, P, U64, P, C.POINTER(U64)]),
+    "pg_pcg_solve_lowrank_device": (C.c_int, [P, P, P, P, C.POINTER(Penalty), U64, U64, P, U64, P, C.POINTER(U64),
+                                              P]),
+    "pg_lowrank_penalty_gradient_device": (C.c_int, [C.POINTER(Penalty), U64, U64, P, P, P, P]),
+    "pg_lowrank_penalty_denom_device": (C.c_int, [C.POINTER(Penalty), U64, U64, P, P, P, C.POINTER(C.c_double)]),
     "pg_server_create": (C.c_int, [C.POINTER(P), C.POINTER(ServerConfig)]),
     "pg_server_destroy": (C.c_int, [P]),
     "pg_submit": (C.c_int, [P, C.POINTER(Request), C.POINTER(U64)]),

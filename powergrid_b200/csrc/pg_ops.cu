@@ -341,6 +341,49 @@ uint64_t PcSenseOp::resident_bytes() const {
   return b;
 }
 
+// ---------------------------------------------------------------------------
+// LRobj (lowRank/LRobj.cpp:27-68)
+// ---------------------------------------------------------------------------
+namespace {
+// Thread per output element; a transposed output puts a fastest across the
+// threads (coalesced stores, the input reads broadcast within a pixel).
+__global__ void k_mix_columns(uint64_t N, int Kin, int Kout, const float2* __restrict__ in,
+                              const float2* __restrict__ C, int transposed_out, float2* __restrict__ out) {
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= N * (uint64_t)Kout) return;
+  uint64_t n;
+  int a;
+  if (transposed_out) { a = (int)(t % Kout); n = t / Kout; }
+  else { n = t % N; a = (int)(t / N); }
+  float2 acc = make_float2(0.f, 0.f);
+  for (int b = 0; b < Kin; ++b) acc = cadd(acc, cmul(in[n + N * b], C[a + (uint64_t)Kout * b]));
+  out[t] = acc;
+}
+}  // namespace
+
+pg_status mix_columns(uint64_t N, int Kin, int Kout, const float2* in, const float2* C, bool transposed_out,
+                      float2* out, cudaStream_t s) {
+  const uint64_t n = N * (uint64_t)Kout;
+  if (n == 0) return PG_OK;
+  PG_LAUNCH(k_mix_columns, ceil_div(n, 256), 256, 0, s, N, Kin, Kout, in, C, transposed_out ? 1 : 0, out);
+  return PG_OK;
+}
+
+pg_status LowRankOp::forward(const float2* x, float2* y, cudaStream_t s) {
+  PG_TRY(stack.alloc(N * Ni));
+  PG_TRY(mix_columns(N, (int)K, (int)Ni, x, cf.p, false, stack.p, s));
+  for (uint64_t i = 0; i < Ni; ++i) PG_TRY(ops[i]->forward(stack.p + N * i, y + Nd * i, s));
+  return PG_OK;
+}
+
+pg_status LowRankOp::adjoint(const float2* y, float2* x, cudaStream_t s) {
+  PG_TRY(stack.alloc(N * Ni));
+  for (uint64_t i = 0; i < Ni; ++i) PG_TRY(ops[i]->adjoint(y + Nd * i, stack.p + N * i, s));
+  return mix_columns(N, (int)Ni, (int)K, stack.p, ca.p, false, x, s);
+}
+
+uint64_t LowRankOp::resident_bytes() const { return cf.bytes() + ca.bytes() + N * Ni * sizeof(float2); }
+
 // The fused gridding stages K segment grids per tile in shared memory: up to
 // 8 in-plane (the forward's register budget), 3 in 3-D (8x8x8 tiles padded
 // to 16x24x16 complex cells, 48 KB each).  Wider windows (the dense min-max
@@ -636,6 +679,45 @@ pg_status pg_pcsense_create(pg_op* out, const float* kx, const float* ky, const 
     E[i] = make_float2(std::cos(ph), std::sin(ph));
   }
   PG_TRY(op->E.upload(E.data(), E.size(), s));
+  PG_CUDA(cudaStreamSynchronize(s));
+  *out = op.release();
+  return PG_OK;
+}
+
+pg_status pg_lowrank_create(pg_op* out, uint64_t n_image, uint64_t n_data, uint64_t rank, uint64_t n_img,
+                            const float* v, const pg_op* ops) {
+  if (!out || !v || !ops) return set_error(PG_INVALID_ARG, "LRobj: null argument");
+  if (rank == 0 || n_img == 0 || n_image == 0 || n_data == 0)
+    return set_error(PG_INVALID_ARG, "LRobj: empty model (rank %llu, %llu images)", (unsigned long long)rank,
+                     (unsigned long long)n_img);
+  if (rank > 1024 || n_img > 65536) return set_error(PG_INVALID_ARG, "LRobj: rank or image count too large");
+  for (uint64_t i = 0; i < n_img; ++i) {
+    if (!ops[i]) return set_error(PG_INVALID_ARG, "LRobj: operator %llu is null", (unsigned long long)i);
+    if (ops[i]->n_image != n_image || ops[i]->n_data != n_data)
+      return set_error(PG_INVALID_ARG, "LRobj: operator %llu is %llux%llu, the model needs %llux%llu",
+                       (unsigned long long)i, (unsigned long long)ops[i]->n_data,
+                       (unsigned long long)ops[i]->n_image, (unsigned long long)n_data,
+                       (unsigned long long)n_image);
+  }
+  PG_TRY(ensure_init());
+  auto op = std::make_unique<LowRankOp>();
+  op->kind = PG_OP_LOWRANK;
+  op->N = n_image; op->Nd = n_data; op->K = rank; op->Ni = n_img;
+  op->n_image = n_image * rank;   // LRobj.cpp:42 reshapes d to N x Nrank
+  op->n_data = n_data * n_img;    // :43 (Ndata x Nimg)
+  op->ops.assign(ops, ops + n_img);
+  const float2* vb = reinterpret_cast<const float2*>(v);
+  std::vector<float2> cf(n_img * rank), ca(rank * n_img);
+  for (uint64_t k = 0; k < rank; ++k)
+    for (uint64_t i = 0; i < n_img; ++i) {
+      const float2 e = vb[k + rank * i];
+      cf[i + n_img * k] = e;
+      ca[k + rank * i] = make_float2(e.x, -e.y);
+    }
+  cudaStream_t s = default_stream();
+  PG_TRY(op->cf.upload(cf.data(), cf.size(), s));
+  PG_TRY(op->ca.upload(ca.data(), ca.size(), s));
+  PG_TRY(op->stack.alloc(n_image * n_img));
   PG_CUDA(cudaStreamSynchronize(s));
   *out = op.release();
   return PG_OK;

@@ -10,7 +10,8 @@
 #include "pg_nufft.cuh"
 
 enum pg_op_kind {
-  PG_OP_GNUFFT = 1, PG_OP_GDFT = 2, PG_OP_TIMESEG = 3, PG_OP_SENSE = 4, PG_OP_PCSENSE_TS = 5, PG_OP_PCSENSE = 6
+  PG_OP_GNUFFT = 1, PG_OP_GDFT = 2, PG_OP_TIMESEG = 3, PG_OP_SENSE = 4, PG_OP_PCSENSE_TS = 5, PG_OP_PCSENSE = 6,
+  PG_OP_LOWRANK = 7
 };
 
 // Per-operator PWLS-PCG state kept between solves (buffers + the captured
@@ -117,6 +118,27 @@ struct PcSenseOp : pg_op_s {
   pg_status adjoint(const float2* y, float2* x, cudaStream_t s) override;
   uint64_t resident_bytes() const override;
 };
+
+// LRobj (lowRank/LRobj.cpp:27-68): x = vec(X), X N x K; forward sends the
+// columns of X v (v: K x Nimg) through the per-image operators, adjoint
+// applies their adjoints and multiplies the N x Nimg stack by v^H.  The
+// per-image operators are borrowed (the reference holds raw pointers).
+struct LowRankOp : pg_op_s {
+  uint64_t N = 0, Nd = 0, K = 0, Ni = 0;
+  std::vector<pg_op_s*> ops;
+  DevBuf<float2> cf;      // Nimg x K: cf[i + Nimg k] = v[k + K i]
+  DevBuf<float2> ca;      // K x Nimg: ca[k + K i] = conj(v[k + K i])
+  DevBuf<float2> stack;   // N x Nimg image stack
+  pg_status forward(const float2* x, float2* y, cudaStream_t s) override;
+  pg_status adjoint(const float2* y, float2* x, cudaStream_t s) override;
+  uint64_t resident_bytes() const override;
+};
+
+// out[:, a] = sum_b in[:, b] * C[a + Kout b] over columns of length N, the sum
+// in order of b; out is stored column-major N x Kout, or transposed (Kout x N,
+// out[a + Kout n]) when transposed_out.
+pg_status mix_columns(uint64_t N, int Kin, int Kout, const float2* in, const float2* C, bool transposed_out,
+                      float2* out, cudaStream_t s);
 
 pg_status make_gnufft(std::unique_ptr<GnufftOp>* out, uint64_t data_length, float gridos, uint64_t nx, uint64_t ny,
                       uint64_t nz, const float* kx, const float* ky, const float* kz, cudaStream_t s);

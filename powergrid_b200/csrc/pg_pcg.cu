@@ -653,6 +653,223 @@ __global__ void k_denom_only(PenDev R, const float2* __restrict__ ddir, const fl
   block_store2(a, 0.0, part, nb);
 }
 
+// ---------------------------------------------------------------------------
+// R_lowRank (lowRank/R_lowRank.cpp:27-95) and the PCG loop that carries it.
+//
+// With x = vec(X), X N x K, the wrapper penalises the columns of
+// I = X * trans(v.cols(0, K-1)) (:42-44; trans is the conjugate transpose, so
+// I[:, j] = sum_k X[:, k] conj(v[j + K k])).  Gradient (:50-64) returns
+// vectorise(strans(v.cols(0, K-1)) * strans(Y)), Y_j = R.Gradient(I_j): a
+// K x N matrix stored k fastest, g[k + K n] = sum_j v[j + K k] Y[n, j].  That
+// product is defined only when K == Nimg (a K x K matrix times an Nimg x N
+// one), so the wrapper takes a square basis.  Denom (:67-87) is
+// R.Beta * sum_j R.Denom(D_j, I_j) with D = Ddir * trans(v), R.Denom already
+// carrying one factor beta.
+// ---------------------------------------------------------------------------
+__global__ void k_grad_images(PenDev R, int K, const float2* __restrict__ x, float2* __restrict__ g) {
+  const uint64_t n = R.N * (uint64_t)K;
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t img = t / R.N, j = t - img * R.N;
+    g[t] = grad_at(R, x + img * R.N, nullptr, 0.f, j);
+  }
+}
+
+__global__ void k_denom_images(PenDev R, int K, const float2* __restrict__ ddir, const float2* __restrict__ x,
+                               double* part, int nb) {
+  double a = 0.0;
+  const uint64_t n = R.N * (uint64_t)K;
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t img = t / R.N, j = t - img * R.N;
+    const float2* di = ddir + img * R.N;
+    const float2* xi = x + img * R.N;
+    for (int dim = 0; dim < R.nd; ++dim) {
+      const uint64_t off = R.off[dim];
+      if (j < off || off >= R.N) continue;
+      const float2 cd = csub(di[j], di[j - off]);
+      const float2 cz = csub(xi[j], xi[j - off]);
+      a += (double)wpot(R, cz) * ((double)cd.x * cd.x + (double)cd.y * cd.y);
+    }
+  }
+  block_store2(a, 0.0, part, nb);
+}
+
+// Sums over n of (|a|^2 or Re conj(a) b) and, with W, of (W|a|^2, Re conj(a) b).
+__global__ void k_sums(uint64_t n, const float2* __restrict__ a, const float2* __restrict__ b,
+                       const float* __restrict__ W, double* part, int nb) {
+  double s0 = 0.0, s1 = 0.0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const float2 u = a[i];
+    const double nn = (double)u.x * u.x + (double)u.y * u.y;
+    s0 += W ? (double)W[i] * nn : nn;
+    if (b) {
+      const float2 v = b[i];
+      s1 += (double)u.x * v.x + (double)u.y * v.y;
+    }
+  }
+  block_store2(s0, s1, part, nb);
+}
+
+// out = a + alpha * b (out may alias a or b).
+__global__ void k_axpy(uint64_t n, const float2* a, double alpha, const float2* b, float2* out) {
+  const float al = (float)alpha;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const float2 u = a[i], v = b[i];
+    out[i] = make_float2(u.x + al * v.x, u.y + al * v.y);
+  }
+}
+
+struct HostSums {
+  DevBuf<double> part;
+  std::vector<double> h;
+  // Launch k_sums and add its block partials in block order.
+  pg_status run(uint64_t n, const float2* a, const float2* b, const float* W, double* s0, double* s1,
+                cudaStream_t s) {
+    const int nb = red_blocks(n);
+    PG_TRY(part.alloc(2 * (uint64_t)nb));
+    PG_LAUNCH(k_sums, (unsigned)nb, kRed, 0, s, n, a, b, W, part.p, nb);
+    return fetch(nb, s0, s1, s);
+  }
+  pg_status fetch(int nb, double* s0, double* s1, cudaStream_t s) {
+    h.resize(2 * (size_t)nb);
+    PG_CUDA(cudaMemcpyAsync(h.data(), part.p, 2 * (size_t)nb * sizeof(double), cudaMemcpyDeviceToHost, s));
+    PG_CUDA(cudaStreamSynchronize(s));
+    double a = 0.0, b = 0.0;
+    for (int i = 0; i < nb; ++i) { a += h[i]; b += h[nb + i]; }
+    if (s0) *s0 = a;
+    if (s1) *s1 = b;
+    return PG_OK;
+  }
+};
+
+struct LowRankPen {
+  PenDev R;
+  double beta = 0;
+  int K = 1;
+  DevBuf<float2> cr;    // K x K, cr[j + K k] = conj(v[j + K k]): the mixing into I
+  DevBuf<float2> cg;    // K x K, cg[k + K j] = v[j + K k]: the gradient's strans(v)
+  DevBuf<float2> I, D, Y;
+  HostSums sums;
+
+  pg_status init(const pg_penalty& Rh, uint64_t rank, const float* v, cudaStream_t s) {
+    R = make_pen(Rh);
+    beta = Rh.beta;
+    K = (int)rank;
+    const float2* vb = reinterpret_cast<const float2*>(v);
+    std::vector<float2> hr(rank * rank), hg(rank * rank);
+    for (uint64_t j = 0; j < rank; ++j)
+      for (uint64_t k = 0; k < rank; ++k) {
+        const float2 e = vb[j + rank * k];
+        hr[j + rank * k] = make_float2(e.x, -e.y);
+        hg[k + rank * j] = e;
+      }
+    PG_TRY(cr.upload(hr.data(), hr.size(), s));
+    PG_TRY(cg.upload(hg.data(), hg.size(), s));
+    PG_TRY(I.alloc(R.N * rank));
+    PG_TRY(D.alloc(R.N * rank));
+    PG_TRY(Y.alloc(R.N * rank));
+    return PG_OK;
+  }
+  pg_status gradient(const float2* x, float2* g, cudaStream_t s) {
+    PG_TRY(mix_columns(R.N, K, K, x, cr.p, false, I.p, s));
+    PG_LAUNCH(k_grad_images, (unsigned)red_blocks(R.N * K), kRed, 0, s, R, K, I.p, Y.p);
+    return mix_columns(R.N, K, K, Y.p, cg.p, true, g, s);
+  }
+  pg_status denom(const float2* ddir, const float2* x, double* out, cudaStream_t s) {
+    PG_TRY(mix_columns(R.N, K, K, x, cr.p, false, I.p, s));
+    PG_TRY(mix_columns(R.N, K, K, ddir, cr.p, false, D.p, s));
+    const int nb = red_blocks(R.N * K);
+    PG_TRY(sums.part.alloc(2 * (uint64_t)nb));
+    PG_LAUNCH(k_denom_images, (unsigned)nb, kRed, 0, s, R, K, D.p, I.p, sums.part.p, nb);
+    double a = 0.0;
+    PG_TRY(sums.fetch(nb, &a, nullptr, s));
+    *out = a * beta * beta;
+    return PG_OK;
+  }
+};
+
+pg_status lowrank_penalty_check(const pg_penalty& Rh, uint64_t rank, uint64_t n_img) {
+  if (rank == 0 || rank > 1024) return set_error(PG_INVALID_ARG, "R_lowRank: rank %llu", (unsigned long long)rank);
+  if (n_img != rank)
+    return set_error(PG_INVALID_ARG,
+                     "R_lowRank: the gradient multiplies strans(v.cols(0, rank-1)) (%llux%llu) by an %llu x N "
+                     "matrix, defined only when rank == the number of images",
+                     (unsigned long long)rank, (unsigned long long)rank, (unsigned long long)n_img);
+  if (Rh.kind != PG_PENALTY_QUAD && Rh.kind != PG_PENALTY_TV) return set_error(PG_INVALID_ARG, "unknown penalty");
+  if (Rh.kind == PG_PENALTY_TV && !(Rh.delta > 0)) return set_error(PG_INVALID_ARG, "TV penalty needs delta > 0");
+  return PG_OK;
+}
+
+// solve_pwls_pcg (solve_pwls_pcg.hpp:48-167) with the low-rank wrapper: the
+// same steps as the fused solver, with the scalars on the host (FP64) because
+// the wrapper's gradient is not a local stencil.
+pg_status pcg_solve_lowrank(pg_op_s* A, LowRankPen& P, const float2* x0, const float* W, const float2* y,
+                            uint64_t niter, float2* xout, uint64_t* iters, cudaStream_t s) {
+  const uint64_t ni = A->n_image, nd = A->n_data;
+  DevBuf<float2> x, Ax, r, ngrad, pgrad, ddir, Adir, xs;
+  DevBuf<float> ones;
+  PG_TRY(x.alloc(ni)); PG_TRY(ngrad.alloc(ni)); PG_TRY(pgrad.alloc(ni)); PG_TRY(ddir.alloc(ni));
+  PG_TRY(xs.alloc(ni)); PG_TRY(Ax.alloc(nd)); PG_TRY(r.alloc(nd)); PG_TRY(Adir.alloc(nd));
+  if (!W) {
+    PG_TRY(ones.alloc(nd));
+    PG_LAUNCH(k_fill_ones, ceil_div(nd, 256), 256, 0, s, nd, ones.p);
+    W = ones.p;
+  }
+  if (x0) PG_CUDA(cudaMemcpyAsync(x.p, x0, ni * sizeof(float2), cudaMemcpyDeviceToDevice, s));
+  else PG_CUDA(cudaMemsetAsync(x.p, 0, ni * sizeof(float2), s));
+  PG_TRY(A->forward(x.p, Ax.p, s));
+  HostSums hs;
+  double ywy = 0.0;
+  PG_TRY(hs.run(nd, y, nullptr, W, &ywy, nullptr, s));
+  const unsigned gd = (unsigned)red_blocks(nd), gi = (unsigned)red_blocks(ni);
+  double oldinprod = 0.0;
+  uint64_t done = 0;
+  for (uint64_t it = 0; it < niter; ++it) {
+    PG_LAUNCH(k_residual, gd, kRed, 0, s, nd, y, Ax.p, W, r.p);
+    PG_TRY(A->adjoint(r.p, ngrad.p, s));
+    double gn = 0.0;
+    PG_TRY(hs.run(ni, ngrad.p, nullptr, nullptr, &gn, nullptr, s));
+    if (std::sqrt(gn) / ywy < 1e-10) break;                       // :88-91
+    PG_TRY(P.gradient(x.p, pgrad.p, s));
+    PG_LAUNCH(k_axpy, gi, kRed, 0, s, ni, ngrad.p, -1.0, pgrad.p, ngrad.p);
+    double newinprod = 0.0;
+    PG_TRY(hs.run(ni, ngrad.p, nullptr, nullptr, &newinprod, nullptr, s));
+    if (it == 0) {
+      PG_CUDA(cudaMemcpyAsync(ddir.p, ngrad.p, ni * sizeof(float2), cudaMemcpyDeviceToDevice, s));
+    } else {
+      const double gamma = (std::fabs(oldinprod) < 1e-10) ? 0.0 : newinprod / oldinprod;
+      PG_LAUNCH(k_axpy, gi, kRed, 0, s, ni, ngrad.p, gamma, ddir.p, ddir.p);
+    }
+    oldinprod = newinprod;
+    double dn = 0.0;
+    PG_TRY(hs.run(ni, ddir.p, ngrad.p, nullptr, nullptr, &dn, s));
+    if (dn < 0) break;                                               // :113-116
+    PG_TRY(A->forward(ddir.p, Adir.p, s));
+    double dAWAd = 0.0, dAWr = 0.0;
+    PG_TRY(hs.run(nd, Adir.p, r.p, W, &dAWAd, &dAWr, s));
+    double step = 0.0;
+    bool stop = false;
+    for (int j = 0; j < 3; ++j) {                                    // :128-150
+      PG_LAUNCH(k_axpy, gi, kRed, 0, s, ni, x.p, step, ddir.p, xs.p);
+      double pdenom = 0.0;
+      PG_TRY(P.denom(ddir.p, xs.p, &pdenom, s));
+      const double denom = dAWAd + pdenom;
+      if (std::fabs(denom) < 1e-20 || std::fabs(denom) > 1e25) { stop = true; break; }
+      PG_TRY(P.gradient(xs.p, pgrad.p, s));
+      double pdot = 0.0;
+      PG_TRY(hs.run(ni, ddir.p, pgrad.p, nullptr, nullptr, &pdot, s));
+      step -= (-dAWr + step * dAWAd + pdot) / denom;
+    }
+    if (stop) break;
+    PG_LAUNCH(k_axpy, gd, kRed, 0, s, nd, Ax.p, step, Adir.p, Ax.p);
+    PG_LAUNCH(k_axpy, gi, kRed, 0, s, ni, x.p, step, ddir.p, x.p);
+    done = it + 1;
+  }
+  PG_CUDA(cudaMemcpyAsync(xout, x.p, ni * sizeof(float2), cudaMemcpyDeviceToDevice, s));
+  PG_CUDA(cudaStreamSynchronize(s));
+  if (iters) *iters = done;
+  return PG_OK;
+}
+
 }  // namespace pg
 
 using namespace pg;
@@ -701,6 +918,64 @@ pg_status pg_penalty_gradient_device(const pg_penalty* R, const void* x, void* g
   PenDev P = make_pen(*R);
   PG_LAUNCH(k_grad_only, (unsigned)red_blocks(P.N), kRed, 0, s, P, (const float2*)x, (float2*)g);
   return PG_OK;
+}
+
+pg_status pg_pcg_solve_lowrank_device(pg_op A, const void* x0, const void* W, const void* y, const pg_penalty* R,
+                                      uint64_t rank, uint64_t n_img, const float* v, uint64_t niter, void* x_out,
+                                      uint64_t* iters_done, void* stream) {
+  if (!A || !y || !R || !v || !x_out) return set_error(PG_INVALID_ARG, "low-rank pcg: null argument");
+  PG_TRY(lowrank_penalty_check(*R, rank, n_img));
+  if (R->nx * R->ny * R->nz * rank != A->n_image)
+    return set_error(PG_INVALID_ARG, "low-rank pcg: penalty %llux%llux%llu x rank %llu does not match the model's %llu",
+                     (unsigned long long)R->nx, (unsigned long long)R->ny, (unsigned long long)R->nz,
+                     (unsigned long long)rank, (unsigned long long)A->n_image);
+  PG_TRY(ensure_init());
+  cudaStream_t s = stream ? (cudaStream_t)stream : default_stream();
+  LowRankPen P;
+  PG_TRY(P.init(*R, rank, v, s));
+  return pcg_solve_lowrank(A, P, (const float2*)x0, (const float*)W, (const float2*)y, niter, (float2*)x_out,
+                           iters_done, s);
+}
+
+pg_status pg_pcg_solve_lowrank(pg_op A, const float* x0, const float* W, const float* y, const pg_penalty* R,
+                               uint64_t rank, uint64_t n_img, const float* v, uint64_t niter, float* x_out,
+                               uint64_t* iters_done) {
+  if (!A || !y || !R || !v || !x_out) return set_error(PG_INVALID_ARG, "low-rank pcg: null argument");
+  PG_TRY(ensure_init());
+  cudaStream_t s = default_stream();
+  PG_TRY(A->hy.upload(reinterpret_cast<const float2*>(y), A->n_data, s));
+  if (x0) PG_TRY(A->hx0.upload(reinterpret_cast<const float2*>(x0), A->n_image, s));
+  if (W) PG_TRY(A->hw.upload(W, A->n_data, s));
+  PG_TRY(A->hx.alloc(A->n_image));
+  PG_TRY(pg_pcg_solve_lowrank_device(A, x0 ? A->hx0.p : nullptr, W ? A->hw.p : nullptr, A->hy.p, R, rank, n_img, v,
+                                     niter, A->hx.p, iters_done, s));
+  PG_CUDA(cudaMemcpyAsync(x_out, A->hx.p, A->n_image * sizeof(float2), cudaMemcpyDeviceToHost, s));
+  PG_CUDA(cudaStreamSynchronize(s));
+  return PG_OK;
+}
+
+pg_status pg_lowrank_penalty_gradient_device(const pg_penalty* R, uint64_t rank, uint64_t n_img, const float* v,
+                                             const void* x, void* g, void* stream) {
+  if (!R || !v || !x || !g) return set_error(PG_INVALID_ARG, "R_lowRank: null argument");
+  PG_TRY(lowrank_penalty_check(*R, rank, n_img));
+  PG_TRY(ensure_init());
+  cudaStream_t s = stream ? (cudaStream_t)stream : default_stream();
+  LowRankPen P;
+  PG_TRY(P.init(*R, rank, v, s));
+  PG_TRY(P.gradient((const float2*)x, (float2*)g, s));
+  PG_CUDA(cudaStreamSynchronize(s));   // P's buffers are freed on return
+  return PG_OK;
+}
+
+pg_status pg_lowrank_penalty_denom_device(const pg_penalty* R, uint64_t rank, uint64_t n_img, const float* v,
+                                          const void* ddir, const void* x, double* out_host) {
+  if (!R || !v || !x || !ddir || !out_host) return set_error(PG_INVALID_ARG, "R_lowRank: null argument");
+  PG_TRY(lowrank_penalty_check(*R, rank, n_img));
+  PG_TRY(ensure_init());
+  cudaStream_t s = default_stream();
+  LowRankPen P;
+  PG_TRY(P.init(*R, rank, v, s));
+  return P.denom((const float2*)ddir, (const float2*)x, out_host, s);
 }
 
 pg_status pg_penalty_denom_device(const pg_penalty* R, const void* ddir, const void* x, double* out_host) {

@@ -23,7 +23,8 @@ import numpy as np
 from . import _lib
 from ._lib import P, U64, Penalty, check
 
-__all__ = ["Gnufft", "Gdft", "GdftR2", "TimeSegmentation", "SENSE", "pcSenseTimeSeg", "pcSENSE", "QuadPenalty", "TVPenalty",
+__all__ = ["Gnufft", "Gdft", "GdftR2", "TimeSegmentation", "SENSE", "pcSenseTimeSeg", "pcSENSE", "LRobj", "QuadPenalty",
+           "TVPenalty", "R_lowRank",
            "calc3DDensityCompensation", "gridCoilImages", "calcSumOfSquaresImage", "solve_pwls_pcg", "reconSolve",
            "init"]
 
@@ -233,6 +234,59 @@ class pcSENSE(_Op):
         super().__init__(h)
 
 
+def _basis(v, rank, n_img):
+    """A rank x n_img complex basis as a column-major complex64 array."""
+    v = np.asarray(v, dtype=np.complex64)
+    if v.shape != (rank, n_img):
+        v = v.reshape(rank, n_img, order="F")
+    return np.ascontiguousarray(v.reshape(-1, order="F"))
+
+
+class LRobj(_Op):
+    """Partial-separability model (lowRank/LRobj.cpp:27-68): x = vec(X) with X
+    NimgSize x n_rank; image i = column i of X * vBasis goes through All[i].
+    The per-image operators are borrowed (kept alive by this object)."""
+
+    def __init__(self, NimgSize, N_data, n_rank, n_img, vBasis, All):
+        ops = list(All)
+        if len(ops) != int(n_img):
+            raise ValueError(f"LRobj: {len(ops)} operators for {n_img} images")
+        self.v = _basis(vBasis, int(n_rank), int(n_img))
+        hs = (P * len(ops))(*[o.handle for o in ops])
+        h = P()
+        check(_lib.load().pg_lowrank_create(C.byref(h), int(NimgSize), int(N_data), int(n_rank), int(n_img),
+                                             _ptr(self.v), C.cast(hs, P)))
+        super().__init__(h, keep=ops)
+
+
+class R_lowRank:
+    """Low-rank wrapper of a QuadPenalty/TVPenalty (lowRank/R_lowRank.cpp:27-95):
+    R applied to the columns of X * vBasis^H.  As in the reference the
+    gradient is defined only for rank == nImages and comes back rank-fastest,
+    and Denom carries beta twice."""
+
+    def __init__(self, R1, rank, nImages, vBasis):
+        self.R, self.rank, self.n_img = R1, int(rank), int(nImages)
+        self.v = _basis(vBasis, self.rank, self.n_img)
+
+    def Gradient(self, x):
+        import torch
+        g = torch.empty_like(x)
+        pen = self.R._struct()
+        check(_lib.load().pg_lowrank_penalty_gradient_device(C.byref(pen), self.rank, self.n_img, _ptr(self.v),
+                                                              P(x.data_ptr()), P(g.data_ptr()), _stream_ptr(None)))
+        return g
+
+    def Denom(self, ddir, x) -> float:
+        import torch
+        torch.cuda.current_stream().synchronize()
+        out = C.c_double()
+        pen = self.R._struct()
+        check(_lib.load().pg_lowrank_penalty_denom_device(C.byref(pen), self.rank, self.n_img, _ptr(self.v),
+                                                           P(ddir.data_ptr()), P(x.data_ptr()), C.byref(out)))
+        return out.value
+
+
 def calc3DDensityCompensation(kx, ky, kz, Ninplane, Nz):
     """Sample density compensation (reconSupport/directRecon.cpp:28-61): two Pipe
     iterations on a 3x oversampled grid, |dcf| normalised to unit L2 norm."""
@@ -314,8 +368,14 @@ def solve_pwls_pcg(xInitial, A: _Op, W, yi, R: QuadPenalty, niter):
     x = np.empty(A.n_image, dtype=np.complex64)
     x0 = None if xInitial is None else _c64(xInitial)
     Wa = None if W is None else _f32(W)
-    pen = R._struct()
     it = U64()
+    if isinstance(R, R_lowRank):
+        pen = R.R._struct()
+        check(_lib.load().pg_pcg_solve_lowrank(A.handle, None if x0 is None else _ptr(x0),
+                                                None if Wa is None else _ptr(Wa), _ptr(yi), C.byref(pen), R.rank,
+                                                R.n_img, _ptr(R.v), int(niter), _ptr(x), C.byref(it)))
+        return x, int(it.value)
+    pen = R._struct()
     check(_lib.load().pg_pcg_solve(A.handle, None if x0 is None else _ptr(x0), None if Wa is None else _ptr(Wa),
                                     _ptr(yi), C.byref(pen), int(niter), _ptr(x), C.byref(it)))
     return x, int(it.value)

@@ -1,7 +1,8 @@
 // Drives the C++ operator API (include/powergrid/PowerGrid.hpp) the way the
 // reference's PowerGridIsmrmrd driver does (PowerGridIsmrmrd.cpp:244-264):
 // Gnufft -> TimeSegmentation -> SENSE -> operator*, operator/, reconSolve,
-// then the direct-reconstruction helpers and the spatial interpolation.
+// then the direct-reconstruction helpers, the spatial interpolation and a
+// low-rank model over the same operator.
 // Inputs and outputs are raw little-endian files in the directory argv[1]
 // (written and checked by tests/test_cpp_api.py).
 #include <complex>
@@ -67,6 +68,25 @@ int main(int argc, char** argv) {
     for (pg::uword i = 0; i < M; ++i) y0.memptr()[i] = y.memptr()[i];
     pg::Col<cx> grid = G.adjointSpatialInterp(y0);
     save(d + "/interp_out.bin", G.forwardSpatialInterp(grid));
+    // the low-rank model as lowRank/oscillateRecon.cpp:256-265 composes it:
+    // two repetitions through the same SENSE operator, identity basis
+    {
+      using Sop = pg::SENSE<float, pg::TimeSegmentation<float, pg::Gnufft<float>>>;
+      Sop* All[2] = {&S, &S};
+      pg::Col<cx> v(4, cx(0, 0));
+      v[0] = cx(1, 0);
+      v[3] = cx(1, 0);
+      pg::LRobj<float, Sop> Alr(N, M * nc, 2, 2, v, All);
+      pg::Col<cx> x2(2 * N), d2(2 * M * nc), x0(2 * N, cx(0, 0));
+      for (pg::uword i = 0; i < N; ++i) x2[i] = x2[N + i] = x[i];
+      for (pg::uword i = 0; i < M * nc; ++i) d2[i] = d2[M * nc + i] = data[i];
+      save(d + "/ylr_out.bin", Alr * x2);
+      pg::R_lowRank<float, pg::QuadPenalty<float>> Rlr(R, 2, 2, v);
+      pg::Col<float> W(2 * M * nc, 1.0f);
+      pg::Col<cx> xlr = pg::solve_pwls_pcg<float, pg::LRobj<float, Sop>, pg::R_lowRank<float, pg::QuadPenalty<float>>>(
+          x0, Alr, W, d2, Rlr, 3);
+      save(d + "/xlr_out.bin", xlr);
+    }
   } catch (const pg::Error& e) {
     std::fprintf(stderr, "pg error: %s\n", e.what());
     return 1;

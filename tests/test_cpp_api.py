@@ -55,3 +55,16 @@ def test_cpp_api_matches_reference_fixture(pg, tmp_path):
     rt = np.fromfile(os.path.join(out, "interp_out.bin"), np.complex64)
     ysub = y[:M]
     assert rt.size == M and rel_l2(rt, G.forwardSpatialInterp(G.adjointSpatialInterp(ysub))) <= 1e-6
+    # LRobj over two copies of the SENSE operator with an identity basis: each
+    # repetition's data is that operator's output; the solve runs the same
+    # library path as the Python API
+    ylr = np.fromfile(os.path.join(out, "ylr_out.bin"), np.complex64)
+    assert np.array_equal(ylr, np.concatenate([y, y]))
+    xlr = np.fromfile(os.path.join(out, "xlr_out.bin"), np.complex64)
+    A = pg.TimeSegmentation(G, c["fm"], c["t"], M, nx * ny * nz, L, 1, 1)
+    S = pg.SENSE(A, c["smap"], M, nx * ny * nz, nc)
+    v = np.eye(2, dtype=np.complex64)
+    Alr = pg.LRobj(nx * ny * nz, M * nc, 2, 2, v, [S, S])
+    xp, _ = pg.solve_pwls_pcg(None, Alr, None, np.concatenate([c["y_f32"]] * 2),
+                              pg.R_lowRank(pg.QuadPenalty(nx, ny, nz, float(c["beta"])), 2, 2, v), 3)
+    assert rel_l2(xlr, xp) <= 1e-6

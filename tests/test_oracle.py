@@ -230,3 +230,50 @@ def test_gdftr2_restatement_matches_reference_kernels(oracle):
         outs.append((G.forward(x), G.adjoint(y)))
     oracle.use_reference(False)
     assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+
+
+def test_lowrank_restatement_matches_dense_formulation(oracle):
+    """LRobj (lowRank/LRobj.cpp:38-66) and R_lowRank (lowRank/R_lowRank.cpp:50-87) restated,
+    against the same products written as dense numpy matrices: the reference has no
+    tests or fixtures for the low-rank model, so this pins the restatement's index
+    conventions (column-major reshapes, trans = conjugate transpose, the gradient's
+    rank-fastest strans product, beta twice in Denom)."""
+    from powergrid_b200 import synthetic as S
+    n = 8
+    N = n * n
+    rng = np.random.default_rng(0)
+    ix, iy, iz = S.image_coords(n, n, 1)
+    K, Ni, M = 2, 3, 40
+    ops = []
+    for _ in range(Ni):
+        kx = rng.uniform(-n / 2, n / 2, M).astype(np.float32)
+        ky = rng.uniform(-n / 2, n / 2, M).astype(np.float32)
+        t = np.linspace(0, 5e-3, M).astype(np.float32)
+        fm = rng.uniform(-50, 50, N).astype(np.float32)
+        ops.append(oracle.gdft(1, kx, ky, np.zeros(M, np.float32), ix, iy, iz, fm, t))
+    v = (rng.standard_normal((K, Ni)) + 1j * rng.standard_normal((K, Ni))).astype(np.complex64)
+    A = oracle.lowrank(N, M, K, Ni, v, ops)
+    x = rng.standard_normal(N * K) + 1j * rng.standard_normal(N * K)
+    y = rng.standard_normal(M * Ni) + 1j * rng.standard_normal(M * Ni)
+    vd = v.astype(np.complex128)
+    F = x.reshape(N, K, order="F") @ vd
+    assert rel_l2(A * x, np.concatenate([ops[i] * F[:, i] for i in range(Ni)])) < 1e-13
+    T = np.stack([ops[i] / y[M * i:M * (i + 1)] for i in range(Ni)], axis=1)
+    assert rel_l2(A / y, (T @ vd.conj().T).reshape(-1, order="F")) < 1e-13
+    assert abs(np.vdot(y, A * x) - np.vdot(A / y, x)) < 1e-10 * abs(np.vdot(y, A * x))
+
+    Kr, beta = 3, 0.5
+    vr = (rng.standard_normal((Kr, Kr)) + 1j * rng.standard_normal((Kr, Kr))).astype(np.complex64)
+    vrd = vr.astype(np.complex128)
+    xr = rng.standard_normal(N * Kr) + 1j * rng.standard_normal(N * Kr)
+    d = rng.standard_normal(N * Kr) + 1j * rng.standard_normal(N * Kr)
+    I = xr.reshape(N, Kr, order="F") @ vrd.conj().T
+    D = d.reshape(N, Kr, order="F") @ vrd.conj().T
+    for kind in ("quad", "tv"):
+        g = oracle.lowrank_gradient(1, kind, n, n, 1, beta, 0.1, 3, Kr, vr, xr)
+        Y = np.stack([oracle.penalty_gradient(1, kind, n, n, 1, beta, 0.1, 3, I[:, j]) for j in range(Kr)], axis=1)
+        assert rel_l2(g, (vrd.T @ Y.T).reshape(-1, order="F")) < 1e-13
+        den = oracle.lowrank_denom(1, kind, n, n, 1, beta, 0.1, 3, Kr, vr, d, xr)
+        den_dense = beta * sum(oracle.penalty_denom(1, kind, n, n, 1, beta, 0.1, 3, D[:, j], I[:, j])
+                               for j in range(Kr))
+        assert abs(den - den_dense) < 1e-12 * abs(den_dense)
