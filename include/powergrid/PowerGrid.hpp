@@ -11,6 +11,8 @@
 //   R_lowRank<T1, Robj>   lowRank/R_lowRank.h:52
 //   solve_pwls_pcg        solve_pwls_pcg.hpp:48-51
 //   reconSolve            reconSolve.h:63-66
+//   acqTracking, getCompleteISMRMRDAcqData   acqTracking.h:14, processIsmrmrd.hpp:361-471
+//   writeNiftiRealImage, writeNiftiMagPhsImage   processNIFTI.hpp:37-117
 // with T1 = float.  Column types: any type with memptr() (or data()),
 // n_elem (or size()) and a size constructor — arma::Col<std::complex<float>>
 // and arma::Col<float> work unchanged; pg::Col<T> is provided for callers
@@ -272,6 +274,59 @@ RCol calcSumOfSquaresImage(const CxCol& coilImages, uword Ncoils) {
   check(pg_sum_of_squares_image(reinterpret_cast<const float*>(detail::ptr(coilImages)), n, Ncoils,
                                 detail::mptr(out)));
   return out;
+}
+
+// writeNiftiRealImage / writeNiftiMagPhsImage (processNIFTI.hpp:37-117):
+// "<filename>.nii", or "<filename>_mag.nii" and "<filename>_phs.nii".
+template <typename T1, typename RCol>
+void writeNiftiRealImage(const std::string& filename, const RCol& imageData, uword Nx, uword Ny, uword Nz = 1,
+                         uword Nslab = 1, uword N_TR = 1) {
+  check(pg_write_nifti_real(filename.c_str(), detail::ptr(imageData), Nx, Ny, Nz, Nslab, N_TR));
+}
+template <typename T1, typename CxCol>
+void writeNiftiMagPhsImage(const std::string& filename, const CxCol& imageData, uword Nx, uword Ny, uword Nz,
+                           uword Nslab = 1, uword N_TR = 1) {
+  check(pg_write_nifti_mag_phs(filename.c_str(), reinterpret_cast<const float*>(detail::ptr(imageData)), Nx, Ny, Nz,
+                               Nslab, N_TR));
+}
+
+// acqTracking over an in-memory acquisition list (acqTracking.h:14); the
+// acquisitions' arrays are borrowed.
+class acqTracking {
+ public:
+  acqTracking(const std::vector<pg_acquisition>& acqs, const pg_encoding_limits& limits) {
+    check(pg_acq_index_create(&h_, acqs.data(), acqs.size(), &limits));
+  }
+  acqTracking(const acqTracking&) = delete;
+  acqTracking& operator=(const acqTracking&) = delete;
+  ~acqTracking() { pg_acq_index_destroy(h_); }
+  pg_acq_index handle() const { return h_; }
+  long long acqArray(uword shot, uword par, uword slice, uword rep, uword avg, uword echo, uword phase) const {
+    int64_t a = -1;
+    check(pg_acq_index_lookup(h_, (uint32_t)shot, (uint32_t)par, (uint32_t)slice, (uint32_t)rep, (uint32_t)avg,
+                              (uint32_t)echo, (uint32_t)phase, &a));
+    return a;
+  }
+
+ private:
+  pg_acq_index h_ = nullptr;
+};
+
+// getCompleteISMRMRDAcqData (processIsmrmrd.hpp:361-471) over the index.
+template <typename T1, typename CxCol, typename RCol>
+void getCompleteISMRMRDAcqData(const acqTracking& acqTrack, uword NSlice, uword NRep, uword NAve, uword NEcho,
+                               uword NPhase, CxCol& data, RCol& kx, RCol& ky, RCol& kz, RCol& tvec) {
+  uint64_t na = 0, nro = 0, nc = 0;
+  check(pg_acq_gather_size(acqTrack.handle(), (uint32_t)NSlice, (uint32_t)NRep, (uint32_t)NAve, (uint32_t)NEcho,
+                           (uint32_t)NPhase, &na, &nro, &nc));
+  data = CxCol(na * nro * nc);
+  kx = RCol(na * nro);
+  ky = RCol(na * nro);
+  kz = RCol(na * nro);
+  tvec = RCol(na * nro);
+  check(pg_acq_gather(acqTrack.handle(), (uint32_t)NSlice, (uint32_t)NRep, (uint32_t)NAve, (uint32_t)NEcho,
+                      (uint32_t)NPhase, reinterpret_cast<float*>(detail::mptr(data)), detail::mptr(kx),
+                      detail::mptr(ky), detail::mptr(kz), detail::mptr(tvec)));
 }
 
 template <typename T1>

@@ -244,6 +244,73 @@ pg_status pg_lowrank_penalty_gradient_device(const pg_penalty* R, uint64_t rank,
 pg_status pg_lowrank_penalty_denom_device(const pg_penalty* R, uint64_t rank, uint64_t n_img, const float* v,
                                           const void* ddir_dev, const void* x_dev, double* out_host);
 
+/* ---- ingest and output formats ---------------------------------------- */
+/* One acquisition as ISMRMRD::Acquisition presents it: the encoding counters
+ * the reference sorts by (acqTracking.cpp:64-75), the sample and channel
+ * counts, the samples channel-major (acq.data(sample, channel) =
+ * data[2*(channel*number_of_samples + sample)], complex) and the trajectory
+ * sample-major with kx, ky, kz, t as its first four rows (acq.traj(dim,
+ * sample) = traj[sample*trajectory_dimensions + dim]).  The arrays are
+ * borrowed by the index built over them. */
+typedef struct pg_acquisition {
+  uint32_t kspace_encode_step_1;   /* shot */
+  uint32_t kspace_encode_step_2;   /* partition */
+  uint32_t slice, repetition, average, contrast, phase;
+  uint32_t number_of_samples;
+  uint32_t active_channels;
+  uint32_t trajectory_dimensions;  /* >= 4 */
+  const float* data;
+  const float* traj;
+} pg_acquisition;
+
+/* encodingLimits.<counter>.maximum + 1 for each counter (acqTracking.cpp:17-26). */
+typedef struct pg_encoding_limits {
+  uint32_t shots, partitions, slices, repetitions, averages, contrasts, phases;
+} pg_encoding_limits;
+
+typedef struct pg_acq_index_s* pg_acq_index;
+
+/* acqTracking(d, hdr) (acqTracking.h:14, acqTracking.cpp:9-76): the table
+ * (shot, partition, slice, repetition, average, contrast, phase) ->
+ * acquisition number, -1 where none; a later acquisition with the same
+ * counters replaces an earlier one. */
+pg_status pg_acq_index_create(pg_acq_index* out, const pg_acquisition* acqs, uint64_t n_acq,
+                              const pg_encoding_limits* limits);
+pg_status pg_acq_index_destroy(pg_acq_index ix);
+/* acqArray(NShot, NPar, NSlice, NRep, NAvg, NEcho, NPhase) (acqTracking.cpp:73). */
+pg_status pg_acq_index_lookup(pg_acq_index ix, uint32_t shot, uint32_t partition, uint32_t slice, uint32_t repetition,
+                              uint32_t average, uint32_t contrast, uint32_t phase, int64_t* acq);
+/* getCompleteISMRMRDAcqData(d, acqTrack, NSlice, NRep, NAve, NEcho, NPhase,
+ * data, kx, ky, kz, tvec) (processIsmrmrd.hpp:361-471): the sizes first
+ * (acquisitions found, samples and channels of each; all must match), then
+ * the arrays: data complex n_channels x n_acq x n_samples (coil-major, the
+ * reference's permute + vectorise), kx/ky/kz/t n_acq x n_samples, the
+ * acquisitions in partition-major, shot-minor order.  Host buffers. */
+pg_status pg_acq_gather_size(pg_acq_index ix, uint32_t slice, uint32_t repetition, uint32_t average,
+                             uint32_t contrast, uint32_t phase, uint64_t* n_acq, uint64_t* n_samples,
+                             uint64_t* n_channels);
+pg_status pg_acq_gather(pg_acq_index ix, uint32_t slice, uint32_t repetition, uint32_t average, uint32_t contrast,
+                        uint32_t phase, float* data, float* kx, float* ky, float* kz, float* t);
+/* The same into DEVICE buffers: each acquisition's block is copied to the
+ * device once and the coil-major permutation runs on the GPU.  Stream-
+ * ordered; the host arrays must stay valid until the stream reaches the
+ * copies. */
+pg_status pg_acq_gather_device(pg_acq_index ix, uint32_t slice, uint32_t repetition, uint32_t average,
+                               uint32_t contrast, uint32_t phase, void* data_dev, void* kx_dev, void* ky_dev,
+                               void* kz_dev, void* t_dev, void* stream);
+
+/* writeNiftiRealImage(filename, imageData, Nx, Ny, Nz, Nslab, N_TR)
+ * (processNIFTI.hpp:37-99): "<filename>.nii", a NIfTI-1 header (dim[0] = 3,
+ * float32, vox_offset 352, scl_slope 100, mm units, magic "n+1"), a zero
+ * 4-byte extender and the voxels in the vector's own order.  Header fields
+ * the reference leaves unset are zero. */
+pg_status pg_write_nifti_real(const char* filename, const float* image, uint64_t nx, uint64_t ny, uint64_t nz,
+                              uint64_t nslab, uint64_t ntr);
+/* writeNiftiMagPhsImage (processNIFTI.hpp:103-117): "<filename>_mag.nii" and
+ * "<filename>_phs.nii" from a complex image (abs and arg in float). */
+pg_status pg_write_nifti_mag_phs(const char* filename, const float* image, uint64_t nx, uint64_t ny, uint64_t nz,
+                                 uint64_t nslab, uint64_t ntr);
+
 /* ---- request server (continuous batching) ---------------------------- */
 typedef struct pg_server_config {
   uint64_t hbm_budget_bytes;   /* admission limit on the summed footprint of resident jobs */

@@ -47,6 +47,19 @@ class RequestStats(C.Structure):
                 ("solve_ms", C.c_double)]
 
 
+class Acquisition(C.Structure):
+    _fields_ = [("kspace_encode_step_1", C.c_uint32), ("kspace_encode_step_2", C.c_uint32), ("slice", C.c_uint32),
+                ("repetition", C.c_uint32), ("average", C.c_uint32), ("contrast", C.c_uint32), ("phase", C.c_uint32),
+                ("number_of_samples", C.c_uint32), ("active_channels", C.c_uint32),
+                ("trajectory_dimensions", C.c_uint32), ("data", P), ("traj", P)]
+
+
+class EncodingLimits(C.Structure):
+    _fields_ = [("shots", C.c_uint32), ("partitions", C.c_uint32), ("slices", C.c_uint32),
+                ("repetitions", C.c_uint32), ("averages", C.c_uint32), ("contrasts", C.c_uint32),
+                ("phases", C.c_uint32)]
+
+
 _lib = None
 
 # Every symbol the header declares, with its ctypes signature.
@@ -90,6 +103,14 @@ SIGNATURES = {
                                               P]),
     "pg_lowrank_penalty_gradient_device": (C.c_int, [C.POINTER(Penalty), U64, U64, P, P, P, P]),
     "pg_lowrank_penalty_denom_device": (C.c_int, [C.POINTER(Penalty), U64, U64, P, P, P, C.POINTER(C.c_double)]),
+    "pg_acq_index_create": (C.c_int, [C.POINTER(P), C.POINTER(Acquisition), U64, C.POINTER(EncodingLimits)]),
+    "pg_acq_index_destroy": (C.c_int, [P]),
+    "pg_acq_index_lookup": (C.c_int, [P] + [C.c_uint32] * 7 + [C.POINTER(C.c_int64)]),
+    "pg_acq_gather_size": (C.c_int, [P] + [C.c_uint32] * 5 + [C.POINTER(U64)] * 3),
+    "pg_acq_gather": (C.c_int, [P] + [C.c_uint32] * 5 + [P] * 5),
+    "pg_acq_gather_device": (C.c_int, [P] + [C.c_uint32] * 5 + [P] * 6),
+    "pg_write_nifti_real": (C.c_int, [C.c_char_p, P, U64, U64, U64, U64, U64]),
+    "pg_write_nifti_mag_phs": (C.c_int, [C.c_char_p, P, U64, U64, U64, U64, U64]),
     "pg_server_create": (C.c_int, [C.POINTER(P), C.POINTER(ServerConfig)]),
     "pg_server_destroy": (C.c_int, [P]),
     "pg_submit": (C.c_int, [P, C.POINTER(Request), C.POINTER(U64)]),

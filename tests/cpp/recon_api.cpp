@@ -87,6 +87,33 @@ int main(int argc, char** argv) {
           x0, Alr, W, d2, Rlr, 3);
       save(d + "/xlr_out.bin", xlr);
     }
+    // the reconstructed image as NIfTI magnitude and phase (processNIFTI.hpp:103-117)
+    pg::writeNiftiMagPhsImage<float>(d + "/img", img, nx, ny, nz);
+    // an acquisition list of two shots, gathered back into one image's data
+    {
+      const pg::uword half = M / 2;
+      std::vector<float> tr(4 * M);
+      for (pg::uword s = 0; s < M; ++s) {
+        tr[4 * s] = kx[s]; tr[4 * s + 1] = ky[s]; tr[4 * s + 2] = kz[s]; tr[4 * s + 3] = t[s];
+      }
+      std::vector<cx> a0(nc * half), a1(nc * half);
+      for (pg::uword c = 0; c < nc; ++c)
+        for (pg::uword s = 0; s < half; ++s) {
+          a0[c * half + s] = data[c * M + s];
+          a1[c * half + s] = data[c * M + half + s];
+        }
+      std::vector<pg_acquisition> acqs(2);
+      for (int k = 0; k < 2; ++k) {
+        acqs[k] = pg_acquisition{(uint32_t)k, 0, 0, 0, 0, 0, 0, (uint32_t)half, (uint32_t)nc, 4,
+                                 reinterpret_cast<const float*>(k ? a1.data() : a0.data()), tr.data() + 4 * half * k};
+      }
+      pg::acqTracking track(acqs, pg_encoding_limits{2, 1, 1, 1, 1, 1, 1});
+      pg::Col<cx> gd;
+      pg::Col<float> gkx, gky, gkz, gt;
+      pg::getCompleteISMRMRDAcqData<float>(track, 0, 0, 0, 0, 0, gd, gkx, gky, gkz, gt);
+      save(d + "/gather_data.bin", gd);
+      save(d + "/gather_kx.bin", gkx);
+    }
   } catch (const pg::Error& e) {
     std::fprintf(stderr, "pg error: %s\n", e.what());
     return 1;

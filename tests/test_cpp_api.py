@@ -68,3 +68,13 @@ def test_cpp_api_matches_reference_fixture(pg, tmp_path):
     xp, _ = pg.solve_pwls_pcg(None, Alr, None, np.concatenate([c["y_f32"]] * 2),
                               pg.R_lowRank(pg.QuadPenalty(nx, ny, nz, float(c["beta"])), 2, 2, v), 3)
     assert rel_l2(xlr, xp) <= 1e-6
+    # NIfTI magnitude/phase of the solved image; the gathered acquisitions
+    # reproduce the data and trajectory they were cut from (M even here)
+    from powergrid_b200 import ingest
+    ingest.writeNiftiMagPhsImage(os.path.join(out, "py"), img, nx, ny, nz)
+    for part in ("_mag.nii", "_phs.nii"):
+        a = np.fromfile(os.path.join(out, "img" + part), np.uint8)
+        assert np.array_equal(a, np.fromfile(os.path.join(out, "py" + part), np.uint8))
+    gd = np.fromfile(os.path.join(out, "gather_data.bin"), np.complex64)
+    assert np.array_equal(gd, c["y_f32"].astype(np.complex64))
+    assert np.array_equal(np.fromfile(os.path.join(out, "gather_kx.bin"), np.float32), c["kx"].astype(np.float32))
