@@ -38,7 +38,11 @@
 #include <cmath>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "pg_fftpass.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace pg {
 namespace {
@@ -525,6 +529,274 @@ pg_status d_cols_inv(int lg, const Lines& ln, int B, const float2* in, const flo
   PG_FFT_DISPATCH(lg, cols_inv, ln, B, in, tw, Q, s)
 }
 
+// ---------------------------------------------------------------------------
+// Fused 2-D passes for 256 x 256 grids: one thread-block cluster of CL = 4
+// CTAs per grid.
+//   forward  CTA r transforms image rows [32r, 32r+32) along y (the F1
+//            arithmetic, pre weights included) into its own shared memory;
+//            after a cluster barrier it transforms grid columns [64r, 64r+64)
+//            along x, reading the 128 nonzero rows from the four CTAs'
+//            shared memory (distributed shared memory), and stores the full
+//            columns (the F2 arithmetic).
+//   adjoint  CTA r inverse-transforms grid columns [64r, 64r+64) along x and
+//            keeps the 128 cropped rows in its shared memory (A1); after a
+//            cluster barrier it inverse-transforms cropped rows [32r, 32r+32)
+//            along y, reading the 256 columns from the four CTAs, and applies
+//            the post weights (A2).
+// The transforms are the separate passes' code in the same order, so the
+// results are the same floats; the half-transformed grid never leaves the
+// SMs and one launch replaces two.  Every thread of every CTA reaches both
+// cluster barriers (no early exits); the second keeps each CTA's rows alive
+// until the other CTAs have read them.
+// ---------------------------------------------------------------------------
+namespace fused {
+constexpr int n = 256, Nn = 128, R = 16;   // n = R * R (Split<8>)
+constexpr int CL = 4;                      // CTAs per grid
+constexpr int kTF = 512;                   // threads per CTA
+constexpr int RPC = Nn / CL;               // image rows per CTA
+constexpr int CPC = n / CL;                // grid columns per CTA
+constexpr int S2 = RowGeo<8>::S2, RS = RowGeo<8>::RS;
+constexpr int kHeld = RPC * n;             // rows (forward) or cropped columns (adjoint) held for the cluster
+constexpr int kWork = (n * CPC > RPC * RS) ? n * CPC : RPC * RS;
+constexpr size_t smem = (size_t)(kHeld + kWork) * sizeof(float2);
+static_assert(RowGeo<8>::R1 == R && RowGeo<8>::R2 == R, "four-step split of 256");
+static_assert(kTF == RPC * R && CPC * R % kTF == 0, "thread mapping");
+static_assert(Nn * CPC == kHeld, "held block sizes");
+}  // namespace fused
+
+__global__ void __launch_bounds__(fused::kTF, 1)
+    k_fft2_fwd_fused(NufftGeom g, int L, const float2* __restrict__ x, const float2* __restrict__ S, int c0,
+                     const float2* __restrict__ E, const float2* __restrict__ Wo, const float* __restrict__ deapf,
+                     const float2* __restrict__ tw, float2* __restrict__ grids) {
+  using namespace fused;
+  extern __shared__ float2 sh[];
+  cg::cluster_group cluster = cg::this_cluster();
+  const int r = (int)cluster.block_rank();
+  float2* P = sh;               // [row][gy], this CTA's 32 image rows after the y transform
+  float2* W = sh + kHeld;       // work area
+  const int pad = g.pad_off[1];
+  const uint64_t N = g.nimg();
+  const int b = blockIdx.y, c = b / L, l = b - c * L;
+  {  // y transform, pass 1: one (row, m2) per thread
+    const int m2 = threadIdx.x % R, rl = threadIdx.x / R;
+    const int ix = r * RPC + rl;
+    const int px = ix + g.pad_off[0];
+    float2 v[R];
+#pragma unroll
+    for (int m1 = 0; m1 < R; ++m1) {
+      const int gy = R * m1 + m2;
+      const int iy = gy - pad;
+      float2 u = make_float2(0.f, 0.f);
+      if (iy >= 0 && iy < Nn) {
+        const uint64_t p = (uint64_t)iy + (uint64_t)Nn * ix;
+        u = x[p];
+        if (S) {
+          const float2 sv = S[(uint64_t)(c0 + c) * N + p];
+          u = E ? cmul(u, cmul(sv, E[p])) : cmul(sv, u);
+        }
+        if (Wo) u = cmul(Wo[(uint64_t)l * N + p], u);
+        const float f = parity2(px, gy) ? -deapf[p] : deapf[p];
+        u = make_float2(u.x * f, u.y * f);
+      }
+      v[m1] = u;
+    }
+    dft<R>(v, false);
+    float2* d = W + rl * RS + m2;
+    d[0] = v[0];
+#pragma unroll
+    for (int k1 = 1; k1 < R; ++k1) d[k1 * S2] = twiddle(v[k1], tw[k1 * R + m2], false);
+  }
+  __syncthreads();
+  {  // y transform, pass 2: one (row, k1) per thread
+    const int k1 = threadIdx.x % R, rl = threadIdx.x / R;
+    float2 u[R];
+    const float2* s = W + rl * RS + k1 * S2;
+#pragma unroll
+    for (int m2 = 0; m2 < R; ++m2) u[m2] = s[m2];
+    dft<R>(u, false);
+    float2* o = P + rl * n + k1;
+#pragma unroll
+    for (int k2 = 0; k2 < R; ++k2) o[R * k2] = u[k2];
+  }
+  cluster.sync();
+  const int padx = g.pad_off[0];
+  for (int it = threadIdx.x; it < CPC * R; it += kTF) {   // x transform, pass 1: (column, m2)
+    const int col = it % CPC, m2 = it / CPC;
+    const int gy = r * CPC + col;
+    float2 v[R];
+#pragma unroll
+    for (int m1 = 0; m1 < R; ++m1) {
+      const int ix = R * m1 + m2 - padx;
+      v[m1] = (ix >= 0 && ix < Nn) ? *cluster.map_shared_rank(P + (ix % RPC) * n + gy, ix / RPC)
+                                   : make_float2(0.f, 0.f);
+    }
+    dft<R>(v, false);
+    float2* d = W + m2 * CPC + col;
+    d[0] = v[0];
+#pragma unroll
+    for (int k1 = 1; k1 < R; ++k1) d[k1 * R * CPC] = twiddle(v[k1], tw[k1 * R + m2], false);
+  }
+  __syncthreads();
+  float2* out = grids + (uint64_t)b * n * n;
+  for (int it = threadIdx.x; it < CPC * R; it += kTF) {   // x transform, pass 2: (column, k1)
+    const int col = it % CPC, k1 = it / CPC;
+    float2 u[R];
+    const float2* s = W + k1 * R * CPC + col;
+#pragma unroll
+    for (int m2 = 0; m2 < R; ++m2) u[m2] = s[m2 * CPC];
+    dft<R>(u, false);
+    float2* o = out + (uint64_t)k1 * n + r * CPC + col;
+#pragma unroll
+    for (int k2 = 0; k2 < R; ++k2) o[(uint64_t)R * k2 * n] = u[k2];
+  }
+  cluster.sync();
+}
+
+__global__ void __launch_bounds__(fused::kTF, 1)
+    k_fft2_adj_fused(NufftGeom g, int L, const float2* __restrict__ grids, const float2* __restrict__ S, int c0,
+                     const float2* __restrict__ E, const float2* __restrict__ WoH, const float* __restrict__ deapf,
+                     const float2* __restrict__ tw, float2* __restrict__ Rimg) {
+  using namespace fused;
+  extern __shared__ float2 sh[];
+  cg::cluster_group cluster = cg::this_cluster();
+  const int r = (int)cluster.block_rank();
+  float2* Q = sh;               // [cropped row][column], this CTA's 64 columns after the x transform
+  float2* W = sh + kHeld;
+  const int crop0 = g.crop_off[0], crop1 = g.crop_off[1];
+  const uint64_t N = g.nimg();
+  const int b = blockIdx.y, c = b / L, l = b - c * L;
+  const float2* in = grids + (uint64_t)b * n * n;
+  for (int it = threadIdx.x; it < CPC * R; it += kTF) {   // x transform, pass 1: (column, m2)
+    const int col = it % CPC, m2 = it / CPC;
+    float2 v[R];
+    const float2* s = in + (uint64_t)m2 * n + r * CPC + col;
+#pragma unroll
+    for (int m1 = 0; m1 < R; ++m1) v[m1] = s[(uint64_t)R * m1 * n];
+    dft<R>(v, true);
+    float2* d = W + m2 * CPC + col;
+    d[0] = v[0];
+#pragma unroll
+    for (int k1 = 1; k1 < R; ++k1) d[k1 * R * CPC] = twiddle(v[k1], tw[k1 * R + m2], true);
+  }
+  __syncthreads();
+  for (int it = threadIdx.x; it < CPC * R; it += kTF) {   // x transform, pass 2: keep the cropped rows
+    const int col = it % CPC, k1 = it / CPC;
+    float2 u[R];
+    const float2* s = W + k1 * R * CPC + col;
+#pragma unroll
+    for (int m2 = 0; m2 < R; ++m2) u[m2] = s[m2 * CPC];
+    dft<R>(u, true);
+#pragma unroll
+    for (int k2 = 0; k2 < R; ++k2) {
+      const int i = k1 + R * k2 - crop0;
+      if (i >= 0 && i < Nn) Q[i * CPC + col] = u[k2];
+    }
+  }
+  cluster.sync();
+  {  // y transform, pass 1: one (cropped row, m2) per thread, columns from the four CTAs
+    const int m2 = threadIdx.x % R, rl = threadIdx.x / R;
+    const int ix = r * RPC + rl;
+    float2 v[R];
+#pragma unroll
+    for (int m1 = 0; m1 < R; ++m1) {
+      const int gy = R * m1 + m2;
+      v[m1] = *cluster.map_shared_rank(Q + ix * CPC + gy % CPC, gy / CPC);
+    }
+    dft<R>(v, true);
+    float2* d = W + rl * RS + m2;
+    d[0] = v[0];
+#pragma unroll
+    for (int k1 = 1; k1 < R; ++k1) d[k1 * S2] = twiddle(v[k1], tw[k1 * R + m2], true);
+  }
+  __syncthreads();
+  {  // y transform, pass 2: keep the cropped columns, post weights
+    const int k1 = threadIdx.x % R, rl = threadIdx.x / R;
+    const int ix = r * RPC + rl;
+    float2 u[R];
+    const float2* s = W + rl * RS + k1 * S2;
+#pragma unroll
+    for (int m2 = 0; m2 < R; ++m2) u[m2] = s[m2];
+    dft<R>(u, true);
+    const int px = ix + crop0;
+#pragma unroll
+    for (int k2 = 0; k2 < R; ++k2) {
+      const int iy = k1 + R * k2 - crop1;
+      if (iy < 0 || iy >= Nn) continue;
+      const uint64_t p = (uint64_t)iy + (uint64_t)Nn * ix;
+      float2 v = u[k2];
+      const float f = parity2(px, iy + crop1) ? -deapf[p] : deapf[p];
+      v = make_float2(v.x * f, v.y * f);
+      if (WoH) v = cmul(v, WoH[(uint64_t)l * N + p]);
+      if (S) {
+        const float2 sv = S[(uint64_t)(c0 + c) * N + p];
+        v = E ? cmul(cmul(cconj(sv), cconj(E[p])), v) : cmul(v, cconj(sv));
+      }
+      Rimg[(uint64_t)b * N + p] = v;
+    }
+  }
+  cluster.sync();
+}
+
+template <typename Kern, typename... Args>
+pg_status launch_fused(Kern kern, int B, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(fused::CL, (unsigned)B, 1);
+  cfg.blockDim = dim3(fused::kTF, 1, 1);
+  cfg.dynamicSmemBytes = fused::smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = fused::CL;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  PG_CUDA(cudaLaunchKernelEx(&cfg, kern, args...));
+  count_launch();
+  return PG_OK;
+}
+
+// The fused passes run where a cluster of four 192 KB CTAs can be resident.
+bool fused_available() {
+  static int ok = -1;
+  if (ok >= 0) return ok == 1;
+  ok = 0;
+  if (cudaFuncSetAttribute(k_fft2_fwd_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused::smem) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_fft2_adj_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused::smem) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(fused::CL, 1, 1);
+  cfg.blockDim = dim3(fused::kTF, 1, 1);
+  cfg.dynamicSmemBytes = fused::smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = fused::CL;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int nf = 0, na = 0;
+  if (cudaOccupancyMaxActiveClusters(&nf, k_fft2_fwd_fused, &cfg) != cudaSuccess ||
+      cudaOccupancyMaxActiveClusters(&na, k_fft2_adj_fused, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  ok = (nf >= 1 && na >= 1) ? 1 : 0;
+  return ok == 1;
+}
+
+// PG_FFT_FUSED=0 (read at each call) keeps the separate passes.
+bool use_fused(const NufftGeom& g) {
+  const char* e = getenv("PG_FFT_FUSED");
+  if (e && e[0] == '0') return false;
+  return g.dim == 2 && g.Gx == fused::n && g.Gy == fused::n && g.Nx == fused::Nn && g.Ny == fused::Nn &&
+         fused_available();
+}
+
 int log2_exact(int v) {
   int l = 0;
   while ((1 << l) < v) ++l;
@@ -565,6 +837,7 @@ pg_status fftpass_twiddles(const NufftGeom& g, DevBuf<float2>* tw, cudaStream_t 
   std::vector<float2> h;
   twiddle_table(g.Gx, &h);
   if (g.dim == 3) twiddle_table(g.Gz, &h);   // the z table follows the in-plane one
+  else (void)fused_available();              // occupancy query outside any stream capture
   return tw->upload(h.data(), h.size(), s);
 }
 
@@ -572,6 +845,7 @@ pg_status fftpass_forward(const NufftGeom& g, int B, int L, const float2* x, con
                           const float2* E, const float2* Wo, const float* deapf, const float2* tw, float2* P,
                           float2* grids, cudaStream_t s) {
   if (B > kMaxGridY) return set_error(PG_INVALID_ARG, "fft passes: batch of %d grids", B);
+  if (use_fused(g)) return launch_fused(k_fft2_fwd_fused, B, s, g, L, x, S, c0, E, Wo, deapf, tw, grids);
   const int lg = log2_exact(g.Gx);
   const uint64_t plane = (uint64_t)g.Gx * g.Gy;
   PG_TRY(d_rows_fwd(lg, g, B, L, x, S, c0, E, Wo, deapf, tw, P, s));
@@ -597,6 +871,12 @@ pg_status fftpass_adjoint(const NufftGeom& g, int B, int L, const float2* grids,
   const int lg = log2_exact(g.Gx);
   const uint64_t plane = (uint64_t)g.Gx * g.Gy;
   float2* Qr = Q;   // the rows the last pass reads
+  if (use_fused(g)) {
+    PG_TRY(launch_fused(k_fft2_adj_fused, B, s, g, L, grids, S, c0, E, WoH, deapf, tw, Rimg));
+    const uint64_t N = g.nimg();
+    PG_LAUNCH(k_sum_images, ceil_div(N * 8, 256), 256, 0, s, N, B, Rimg, accumulate, x);
+    return PG_OK;
+  }
   if (g.dim == 2) {
     const Lines ln{plane, (uint64_t)g.Nx * g.Gy, (uint64_t)g.Gy, g.Gy, g.Nx, g.crop_off[0]};
     PG_TRY(d_cols_inv(lg, ln, B, grids, tw, Q, s));
