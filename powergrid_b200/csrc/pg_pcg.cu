@@ -493,6 +493,11 @@ struct PcgCache : pg_pcg_cache_base {
   DevBuf<float> wbuf;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  // With stage timing on, `exec` is captured without stage events and
+  // `exec_timed` with them; a solve replays the timed copy for its last
+  // iteration only (event nodes in every iteration cost ~10 us each).
+  cudaGraph_t graph_timed = nullptr;
+  cudaGraphExec_t exec_timed = nullptr;
   uint64_t per_iter = 0;
   pg_penalty R{};
   uint64_t prof_epoch = 0;
@@ -500,6 +505,8 @@ struct PcgCache : pg_pcg_cache_base {
   ~PcgCache() override {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
+    if (exec_timed) cudaGraphExecDestroy(exec_timed);
+    if (graph_timed) cudaGraphDestroy(graph_timed);
   }
   bool matches(const pg_penalty& r, bool ones) const {
     return R.kind == r.kind && R.nx == r.nx && R.ny == r.ny && R.nz == r.nz && R.beta == r.beta &&
@@ -585,34 +592,43 @@ pg_status pcg_solve_device(pg_op_s* A, const float2* x0, const float* W, const f
     if (st != PG_OK) { A->pcg_cache.reset(); return st; }
     it = 1;
     if (graphs_enabled() && niter > 1) {
-      const uint64_t before = g_launches.load();
-      PG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-      st = S.iteration(s);
-      cudaGraph_t graph = nullptr;
-      cudaError_t ce = cudaStreamEndCapture(s, &graph);
-      // the capture pass counted launches that never ran
-      cache->per_iter = g_launches.load() - before;
-      g_launches.fetch_sub(cache->per_iter);
-      if (st != PG_OK || ce != cudaSuccess) {
-        if (graph) cudaGraphDestroy(graph);
-        cudaGetLastError();
-        A->pcg_cache.reset();
-        return st != PG_OK ? st : set_error(PG_CUDA_ERROR, "graph capture: %s", cudaGetErrorString(ce));
+      // one capture without stage events, and with stage timing on a second
+      // one with them
+      for (int timed = 0; timed < (g_profile ? 2 : 1); ++timed) {
+        const uint64_t before = g_launches.load();
+        g_profile_suppress = timed == 0;
+        PG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        st = S.iteration(s);
+        cudaGraph_t graph = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(s, &graph);
+        g_profile_suppress = false;
+        // the capture pass counted launches that never ran
+        cache->per_iter = g_launches.load() - before;
+        g_launches.fetch_sub(cache->per_iter);
+        if (st != PG_OK || ce != cudaSuccess) {
+          if (graph) cudaGraphDestroy(graph);
+          cudaGetLastError();
+          A->pcg_cache.reset();
+          return st != PG_OK ? st : set_error(PG_CUDA_ERROR, "graph capture: %s", cudaGetErrorString(ce));
+        }
+        cudaGraphExec_t exec = nullptr;
+        ce = cudaGraphInstantiate(&exec, graph, 0);
+        if (ce != cudaSuccess) {
+          cudaGraphDestroy(graph);
+          cudaGetLastError();
+          A->pcg_cache.reset();
+          return set_error(PG_CUDA_ERROR, "graph instantiate: %s", cudaGetErrorString(ce));
+        }
+        (timed ? cache->graph_timed : cache->graph) = graph;
+        (timed ? cache->exec_timed : cache->exec) = exec;
       }
-      ce = cudaGraphInstantiate(&cache->exec, graph, 0);
-      if (ce != cudaSuccess) {
-        cudaGraphDestroy(graph);
-        cudaGetLastError();
-        A->pcg_cache.reset();
-        return set_error(PG_CUDA_ERROR, "graph instantiate: %s", cudaGetErrorString(ce));
-      }
-      cache->graph = graph;
     }
   }
   for (; it < niter; ++it) {
     if (cancel && cancel->load()) break;
     if (cache->exec) {
-      cudaError_t ce = cudaGraphLaunch(cache->exec, s);
+      cudaGraphExec_t exec = (cache->exec_timed && it + 1 == niter) ? cache->exec_timed : cache->exec;
+      cudaError_t ce = cudaGraphLaunch(exec, s);
       if (ce != cudaSuccess) {
         cudaGetLastError();
         A->pcg_cache.reset();

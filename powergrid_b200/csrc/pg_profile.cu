@@ -8,6 +8,7 @@
 namespace pg {
 
 bool g_profile = false;
+thread_local bool g_profile_suppress = false;
 uint64_t g_profile_epoch = 0;
 
 namespace {

@@ -6,6 +6,8 @@
 namespace pg {
 
 extern bool g_profile;
+// Set while capturing a graph that must carry no stage events.
+extern thread_local bool g_profile_suppress;
 // Changes whenever the recording set changes (captured graphs embed it).
 extern uint64_t g_profile_epoch;
 // Record the start / stop event of `stage` on stream s (no-op unless enabled).
@@ -15,8 +17,11 @@ void prof_stop(const char* stage, cudaStream_t s);
 struct ProfScope {
   const char* name;
   cudaStream_t s;
-  ProfScope(const char* n, cudaStream_t st) : name(n), s(st) { if (g_profile) prof_start(name, s); }
-  ~ProfScope() { if (g_profile) prof_stop(name, s); }
+  bool on;
+  ProfScope(const char* n, cudaStream_t st) : name(n), s(st), on(g_profile && !g_profile_suppress) {
+    if (on) prof_start(name, s);
+  }
+  ~ProfScope() { if (on) prof_stop(name, s); }
 };
 
 }  // namespace pg

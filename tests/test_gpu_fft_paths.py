@@ -72,14 +72,15 @@ def test_own_fft_passes_match_cufft(pg, n):
     assert e_f <= FORMS_TOL and e_a <= FORMS_TOL
 
 
-def test_fused_cluster_passes_equal_separate_passes(pg):
+@pytest.mark.parametrize("L,nc", [(1, 1), (4, 3), (8, 8)])
+def test_fused_cluster_passes_equal_separate_passes(pg, L, nc):
     """The 256x256 grids' one-launch cluster form (rows in each CTA's shared
     memory, columns over distributed shared memory) against the separate
     passes: the same transforms in the same order (differences only from the
-    compiler's fma contraction in each kernel), SENSE<TS<Gnufft>> 128^2, L=4,
-    3 coils."""
+    compiler's fma contraction in each kernel), SENSE<TS<Gnufft>> 128^2 with
+    batches of 1, 12 and 64 grids (the last more clusters than fit at once)."""
     from powergrid_b200 import synthetic as S
-    _, own = _ts_sense(pg, 128, 8192, 4, 3, 77)
+    _, own = _ts_sense(pg, 128, 8192, L, nc, 77)
     x = S.image(S.Rng(78), 128 * 128)
     y = own[2] * x
     xa = own[2] / y
@@ -94,7 +95,7 @@ def test_fused_cluster_passes_equal_separate_passes(pg):
         else:
             os.environ["PG_FFT_FUSED"] = old
     e_f, e_a = rel_l2(y, y_sep), rel_l2(xa, xa_sep)
-    print(f"fused vs separate: forward {e_f:.2e}, adjoint {e_a:.2e}")
+    print(f"fused vs separate, L={L}, {nc} coils: forward {e_f:.2e}, adjoint {e_a:.2e}")
     assert e_f <= 1e-6 and e_a <= 1e-6
 
 
