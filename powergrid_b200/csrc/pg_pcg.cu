@@ -578,8 +578,12 @@ pg_status pcg_solve_device(pg_op_s* A, const float2* x0, const float* W, const f
   if (x0) PG_CUDA(cudaMemcpyAsync(S.x.p, x0, ni * sizeof(float2), cudaMemcpyDeviceToDevice, s));
   else PG_CUDA(cudaMemsetAsync(S.x.p, 0, ni * sizeof(float2), s));
   PG_CUDA(cudaMemsetAsync(S.ddir.p, 0, ni * sizeof(float2), s));
-  // Ax = A * xInitial (:55)
-  pg_status st = A->forward(S.x.p, S.Ax.p, s);
+  // Ax = A * xInitial (:55).  Without x0 the start is zero and so is A * 0,
+  // exactly (the operators are linear and their factors finite: the
+  // deapodization's NaNs are stored as 0), so Ax is cleared instead.
+  pg_status st = PG_OK;
+  if (x0) st = A->forward(S.x.p, S.Ax.p, s);
+  else PG_CUDA(cudaMemsetAsync(S.Ax.p, 0, nd * sizeof(float2), s));
   if (st != PG_OK) { A->pcg_cache.reset(); return st; }
   PG_LAUNCH(k_ywy, (unsigned)S.nbd, kRed, 0, s, nd, S.y, S.W, S.part.p, S.nbd);
   PG_LAUNCH(k_scalar_init, 1, 32, 0, s, S.part.p, S.nbd, S.sc.p, S.fl.p);
@@ -832,7 +836,8 @@ pg_status pcg_solve_lowrank(pg_op_s* A, LowRankPen& P, const float2* x0, const f
   }
   if (x0) PG_CUDA(cudaMemcpyAsync(x.p, x0, ni * sizeof(float2), cudaMemcpyDeviceToDevice, s));
   else PG_CUDA(cudaMemsetAsync(x.p, 0, ni * sizeof(float2), s));
-  PG_TRY(A->forward(x.p, Ax.p, s));
+  if (x0) PG_TRY(A->forward(x.p, Ax.p, s));
+  else PG_CUDA(cudaMemsetAsync(Ax.p, 0, nd * sizeof(float2), s));   // A * 0 = 0 exactly
   HostSums hs;
   double ywy = 0.0;
   PG_TRY(hs.run(nd, y, nullptr, W, &ywy, nullptr, s));
