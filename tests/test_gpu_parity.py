@@ -335,3 +335,27 @@ def test_invalid_inputs_of_the_widened_api_are_rejected(pg):
         pg.calc3DDensityCompensation(bad, ky, kz, 8, 4)
     with pytest.raises(ValueError):
         pg.calcSumOfSquaresImage(np.zeros(10, np.complex64), 3)
+
+
+def test_run_to_run_reproducibility(pg):
+    """Two applications of the same operator to the same input.  The forward
+    (gather, no atomics) and the spatial-interpolation adjoint (gather form,
+    ordered fix-up) are bitwise reproducible; the gridding adjoint adds each
+    work item's tile into the grid with float atomics, so only its tile sums
+    are order-independent and two runs may differ in the last bits."""
+    from powergrid_b200 import synthetic as S
+    p = S.config2()
+    M, n = p.kx.size, p.nimg
+    G = pg.Gnufft(M, 2.0, p.nx, p.ny, p.nz, p.kx, p.ky, p.kz)
+    A = pg.TimeSegmentation(G, p.fm, p.t, M, n, p.L, 1, 1)
+    Sg = pg.SENSE(A, p.smap, M, n, p.nc)
+    x = S.image(S.Rng(301), n)
+    y1, y2 = Sg * x, Sg * x
+    assert np.array_equal(y1, y2)
+    a1, a2 = Sg / y1, Sg / y1
+    e = rel_l2(a1, a2)
+    print(f"cfg2 adjoint run-to-run: rel {e:.2e}, bitwise equal: {np.array_equal(a1, a2)}")
+    assert e <= 1e-6
+    G3 = pg.Gnufft(M, 3.0, p.nx, p.ny, p.nz, p.kx, p.ky, p.kz)
+    ys = y1[:M]
+    assert np.array_equal(G3.adjointSpatialInterp(ys), G3.adjointSpatialInterp(ys))
