@@ -108,10 +108,8 @@ class ClockSampler:
 
 
 def _dist():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from powergrid_b200.replicas import rank_layout
+    return rank_layout()
 
 
 def _problem():
@@ -178,6 +176,7 @@ def run_reference_arm(args):
 # GPU arm
 # --------------------------------------------------------------------------------------------
 def run_gpu_arm(args):
+    from powergrid_b200.replicas import job_rate, max_over_ranks
     import ctypes as C
 
     import torch
@@ -273,11 +272,8 @@ def run_gpu_arm(args):
     check(L.pg_profile_enable(0))
     total_ms = sum(step_ms)
     done = int(iters.item())
-    if ws > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = ws * args.steps * NITER / (total_ms / 1000.0)
+    total_ms = max_over_ranks(total_ms, device=dev)
+    value = job_rate(args.steps * NITER, total_ms / 1000.0, ws)
 
     # end to end through the C ABI host entry point (pinned host buffers)
     yh = torch.empty(Sg.n_data, dtype=torch.complex64).pin_memory()
@@ -297,11 +293,8 @@ def run_gpu_arm(args):
         check(L.pg_pcg_solve(Sg.handle, None, None, P(yh.data_ptr()), C.byref(pen), NITER, P(xh.data_ptr()),
                              C.byref(itn)))
         e2e_s += time.perf_counter() - t0
-    if ws > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = ws * e2e_steps * NITER / e2e_s
+    e2e_s = max_over_ranks(e2e_s, device=dev)
+    e2e = job_rate(e2e_steps * NITER, e2e_s, ws)
 
     # roofline of the adjoint gridding kernel: algorithmic bytes per launch
     # = coils * (M * (4*d + 8 + 4) + L * G * 8), d = 2, G = 256^2
