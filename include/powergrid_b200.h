@@ -212,6 +212,24 @@ pg_status pg_pcg_solve_device(pg_op A, const void* x0_dev, const void* W_dev, co
                               const pg_penalty* R, uint64_t niter, void* x_out_dev, void* iters_done_dev,
                               void* stream);
 
+/* Checkpoint / resume of a solve (no counterpart in the reference, which
+ * keeps no state between calls).  The state the solver holds on the
+ * operator between iterations — x, Ax, the residual, the search direction
+ * (and the previous one for a QuadPenalty), the FP64 scalars and the
+ * iteration counters — is copied to a host blob of pg_pcg_state_size bytes
+ * after a solve (or a cancelled one: cancellation stops between
+ * iterations), and loaded onto an operator of the same shape, e.g. a new
+ * plan on another GPU.  pg_pcg_resume then runs niter more iterations from
+ * it, exactly as the uninterrupted solve would continue; iters_done counts
+ * from the original start. */
+pg_status pg_pcg_state_size(pg_op A, uint64_t* bytes);
+pg_status pg_pcg_state_save(pg_op A, void* host, uint64_t bytes);
+pg_status pg_pcg_state_load(pg_op A, const pg_penalty* R, const void* host, uint64_t bytes);
+pg_status pg_pcg_resume(pg_op A, const float* W, const float* y, const pg_penalty* R, uint64_t niter, float* x_out,
+                        uint64_t* iters_done);
+pg_status pg_pcg_resume_device(pg_op A, const void* W_dev, const void* y_dev, const pg_penalty* R, uint64_t niter,
+                               void* x_out_dev, void* iters_done_dev, void* stream);
+
 /* reconSolve(data, Sg, R, kx, ky, kz, Nx, Ny, Nz, tvec, niter)
  * (reconSolve.h:63-82): W = 1, x0 = 0. */
 pg_status pg_recon_solve(pg_op Sg, const pg_penalty* R, const float* data, uint64_t niter, float* image_out);

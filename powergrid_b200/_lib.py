@@ -96,6 +96,11 @@ SIGNATURES = {
     "pg_pcg_solve": (C.c_int, [P, P, P, P, C.POINTER(Penalty), U64, P, C.POINTER(U64)]),
     "pg_pcg_solve_device": (C.c_int, [P, P, P, P, C.POINTER(Penalty), U64, P, P, P]),
     "pg_recon_solve": (C.c_int, [P, C.POINTER(Penalty), P, U64, P]),
+    "pg_pcg_state_size": (C.c_int, [P, C.POINTER(U64)]),
+    "pg_pcg_state_save": (C.c_int, [P, P, U64]),
+    "pg_pcg_state_load": (C.c_int, [P, C.POINTER(Penalty), P, U64]),
+    "pg_pcg_resume": (C.c_int, [P, P, P, C.POINTER(Penalty), U64, P, C.POINTER(U64)]),
+    "pg_pcg_resume_device": (C.c_int, [P, P, P, C.POINTER(Penalty), U64, P, P, P]),
     "pg_penalty_gradient_device": (C.c_int, [C.POINTER(Penalty), P, P, P]),
     "pg_penalty_denom_device": (C.c_int, [C.POINTER(Penalty), P, P, C.POINTER(C.c_double)]),
     "pg_pcg_solve_lowrank": (C.c_int, [P, P, P, P, C.POINTER(Penalty), U64, U64, P, U64, P, C.POINTER(U64)]),

@@ -156,9 +156,11 @@ pg_status tune_for_coils(pg_op_s* G, int nc, bool search, cudaStream_t s);
 pg_status make_gnufft_shared(std::unique_ptr<GnufftOp>* out, const GnufftOp& src);
 pg_status make_timeseg_shared(std::unique_ptr<TimeSegOp>* out, pg_op_s* G, const TimeSegOp& src,
                               const float* field_map, cudaStream_t s);
-// Device PWLS-PCG (pg_pcg.cu).  cancel (may be null) is polled between iterations.
+// Device PWLS-PCG (pg_pcg.cu).  cancel (may be null) is polled between
+// iterations.  resume: continue from the solver state on the operator (x0
+// ignored) for niter more iterations.
 pg_status pcg_solve_device(pg_op_s* A, const float2* x0, const float* W, const float2* y, const pg_penalty& R,
                            uint64_t niter, float2* xout, uint32_t* iters_dev, cudaStream_t s,
-                           const std::atomic<bool>* cancel = nullptr);
+                           const std::atomic<bool>* cancel = nullptr, bool resume = false);
 
 }  // namespace pg

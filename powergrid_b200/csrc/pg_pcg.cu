@@ -17,6 +17,7 @@
 // d[j]-d[j+off] up to N-2-off, d[N-1-off] at N-1-off, zero above
 // (Robject.cpp:111-117).
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "pg_ops.cuh"
@@ -508,6 +509,10 @@ struct PcgCache : pg_pcg_cache_base {
     if (exec_timed) cudaGraphExecDestroy(exec_timed);
     if (graph_timed) cudaGraphDestroy(graph_timed);
   }
+  bool same_penalty(const pg_penalty& r) const {
+    return R.kind == r.kind && R.nx == r.nx && R.ny == r.ny && R.nz == r.nz && R.beta == r.beta &&
+           R.delta == r.delta && R.dims2penalize == r.dims2penalize;
+  }
   bool matches(const pg_penalty& r, bool ones) const {
     return R.kind == r.kind && R.nx == r.nx && R.ny == r.ny && R.nz == r.nz && R.beta == r.beta &&
            R.delta == r.delta && R.dims2penalize == r.dims2penalize && prof_epoch == g_profile_epoch &&
@@ -552,9 +557,12 @@ pg_status make_cache(pg_op_s* A, const pg_penalty& Rh, bool w_ones, std::unique_
 
 }  // namespace
 
+pg_status pcg_iterate(pg_op_s* A, PcgCache* cache, uint64_t niter, float2* xout, uint32_t* iters_dev,
+                      cudaStream_t s, const std::atomic<bool>* cancel);
+
 pg_status pcg_solve_device(pg_op_s* A, const float2* x0, const float* W, const float2* y, const pg_penalty& Rh,
                            uint64_t niter, float2* xout, uint32_t* iters_dev, cudaStream_t s,
-                           const std::atomic<bool>* cancel) {
+                           const std::atomic<bool>* cancel, bool resume) {
   const uint64_t ni = A->n_image, nd = A->n_data;
   if (Rh.nx * Rh.ny * Rh.nz != ni)
     return set_error(PG_INVALID_ARG, "penalty size %llux%llux%llu does not match the image length %llu",
@@ -564,6 +572,15 @@ pg_status pcg_solve_device(pg_op_s* A, const float2* x0, const float* W, const f
   if (Rh.kind == PG_PENALTY_TV && !(Rh.delta > 0)) return set_error(PG_INVALID_ARG, "TV penalty needs delta > 0");
 
   auto* cache = dynamic_cast<PcgCache*>(A->pcg_cache.get());
+  if (resume) {
+    // continue from the state on the operator (a solve or pg_pcg_state_load)
+    if (!cache || !cache->same_penalty(Rh))
+      return set_error(PG_INVALID_ARG, "pcg resume: no solver state for this penalty on the operator");
+    PG_CUDA(cudaMemcpyAsync(cache->ybuf.p, y, nd * sizeof(float2), cudaMemcpyDeviceToDevice, s));
+    if (W) PG_CUDA(cudaMemcpyAsync(cache->wbuf.p, W, nd * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    else PG_LAUNCH(k_fill_ones, ceil_div(nd, 256), 256, 0, s, nd, cache->wbuf.p);
+    return pcg_iterate(A, cache, niter, xout, iters_dev, s, cancel);
+  }
   if (!cache || !cache->matches(Rh, W == nullptr)) {
     A->pcg_cache.reset();
     std::unique_ptr<PcgCache> c;
@@ -588,7 +605,15 @@ pg_status pcg_solve_device(pg_op_s* A, const float2* x0, const float* W, const f
   PG_LAUNCH(k_ywy, (unsigned)S.nbd, kRed, 0, s, nd, S.y, S.W, S.part.p, S.nbd);
   PG_LAUNCH(k_scalar_init, 1, 32, 0, s, S.part.p, S.nbd, S.sc.p, S.fl.p);
   PG_LAUNCH(k_residual, (unsigned)S.nbd, kRed, 0, s, nd, S.y, S.Ax.p, S.W, S.r.p);
+  return pcg_iterate(A, cache, niter, xout, iters_dev, s, cancel);
+}
 
+// The iterations of a solve, from the state in the cache.
+pg_status pcg_iterate(pg_op_s* A, PcgCache* cache, uint64_t niter, float2* xout, uint32_t* iters_dev,
+                      cudaStream_t s, const std::atomic<bool>* cancel) {
+  Solver& S = cache->S;
+  const uint64_t ni = A->n_image;
+  pg_status st = PG_OK;
   uint64_t it = 0;
   if (!cache->exec && niter > 0) {
     // first iteration eagerly: allocates every workspace the graph will use
@@ -938,6 +963,128 @@ pg_status pg_penalty_gradient_device(const pg_penalty* R, const void* x, void* g
   cudaStream_t s = stream ? (cudaStream_t)stream : default_stream();
   PenDev P = make_pen(*R);
   PG_LAUNCH(k_grad_only, (unsigned)red_blocks(P.N), kRed, 0, s, P, (const float2*)x, (float2*)g);
+  return PG_OK;
+}
+
+// ---- checkpoint / resume ----------------------------------------------------
+// The solver state between iterations, as a host blob: a header, then x, Ax,
+// the residual r and the direction (ni, nd, nd, ni complex), the previous
+// direction for the quadratic penalty (ni), the FP64 scalars and the flags.
+struct PcgStateHeader {
+  char magic[8];
+  uint64_t ni, nd;
+  int32_t kind, has_prev;
+  uint64_t nscal, nflag;
+};
+
+static uint64_t state_bytes(uint64_t ni, uint64_t nd, bool prev) {
+  return sizeof(PcgStateHeader) + (2 * ni + 2 * nd + (prev ? ni : 0)) * sizeof(float2) + S_NSCAL * sizeof(double) +
+         F_NFLAG * sizeof(uint32_t);
+}
+
+pg_status pg_pcg_state_size(pg_op A, uint64_t* bytes) {
+  if (!A || !bytes) return set_error(PG_INVALID_ARG, "pcg state: null argument");
+  auto* c = dynamic_cast<PcgCache*>(A->pcg_cache.get());
+  if (!c) return set_error(PG_INVALID_ARG, "pcg state: no solve has run on this operator");
+  *bytes = state_bytes(A->n_image, A->n_data, c->S.ddir_prev.p != nullptr);
+  return PG_OK;
+}
+
+pg_status pg_pcg_state_save(pg_op A, void* host, uint64_t bytes) {
+  uint64_t need = 0;
+  PG_TRY(pg_pcg_state_size(A, &need));
+  if (!host || bytes < need) return set_error(PG_INVALID_ARG, "pcg state: buffer of %llu bytes, %llu needed",
+                                              (unsigned long long)bytes, (unsigned long long)need);
+  auto* c = dynamic_cast<PcgCache*>(A->pcg_cache.get());
+  Solver& S = c->S;
+  PG_CUDA(cudaDeviceSynchronize());   // the solve may have run on any stream
+  PcgStateHeader h{};
+  std::memcpy(h.magic, "PGPCGST1", 8);
+  h.ni = A->n_image;
+  h.nd = A->n_data;
+  h.kind = S.R.kind;
+  h.has_prev = S.ddir_prev.p ? 1 : 0;
+  h.nscal = S_NSCAL;
+  h.nflag = F_NFLAG;
+  char* o = static_cast<char*>(host);
+  std::memcpy(o, &h, sizeof(h));
+  o += sizeof(h);
+  auto take = [&](const void* d, uint64_t nb) -> pg_status {
+    PG_CUDA(cudaMemcpy(o, d, nb, cudaMemcpyDeviceToHost));
+    o += nb;
+    return PG_OK;
+  };
+  PG_TRY(take(S.x.p, h.ni * sizeof(float2)));
+  PG_TRY(take(S.Ax.p, h.nd * sizeof(float2)));
+  PG_TRY(take(S.r.p, h.nd * sizeof(float2)));
+  PG_TRY(take(S.ddir.p, h.ni * sizeof(float2)));
+  if (h.has_prev) PG_TRY(take(S.ddir_prev.p, h.ni * sizeof(float2)));
+  PG_TRY(take(S.sc.p, S_NSCAL * sizeof(double)));
+  PG_TRY(take(S.fl.p, F_NFLAG * sizeof(uint32_t)));
+  return PG_OK;
+}
+
+pg_status pg_pcg_state_load(pg_op A, const pg_penalty* R, const void* host, uint64_t bytes) {
+  if (!A || !R || !host) return set_error(PG_INVALID_ARG, "pcg state: null argument");
+  PcgStateHeader h{};
+  if (bytes < sizeof(h)) return set_error(PG_INVALID_ARG, "pcg state: %llu bytes", (unsigned long long)bytes);
+  std::memcpy(&h, host, sizeof(h));
+  if (std::memcmp(h.magic, "PGPCGST1", 8) != 0 || h.nscal != S_NSCAL || h.nflag != F_NFLAG)
+    return set_error(PG_INVALID_ARG, "pcg state: not a solver state of this library");
+  if (h.ni != A->n_image || h.nd != A->n_data || h.kind != R->kind ||
+      (h.has_prev != 0) != (R->kind == PG_PENALTY_QUAD) || bytes < state_bytes(h.ni, h.nd, h.has_prev != 0))
+    return set_error(PG_INVALID_ARG, "pcg state: saved for a %llux%llu operator with penalty %d",
+                     (unsigned long long)h.nd, (unsigned long long)h.ni, h.kind);
+  if (R->nx * R->ny * R->nz != A->n_image) return set_error(PG_INVALID_ARG, "pcg state: penalty size");
+  PG_TRY(ensure_init());
+  cudaStream_t s = default_stream();
+  A->pcg_cache.reset();
+  std::unique_ptr<PcgCache> c;
+  PG_TRY(make_cache(A, *R, true, &c, s));
+  Solver& S = c->S;
+  const char* i = static_cast<const char*>(host) + sizeof(h);
+  auto put = [&](void* d, uint64_t nb) -> pg_status {
+    PG_CUDA(cudaMemcpyAsync(d, i, nb, cudaMemcpyHostToDevice, s));
+    i += nb;
+    return PG_OK;
+  };
+  PG_TRY(put(S.x.p, h.ni * sizeof(float2)));
+  PG_TRY(put(S.Ax.p, h.nd * sizeof(float2)));
+  PG_TRY(put(S.r.p, h.nd * sizeof(float2)));
+  PG_TRY(put(S.ddir.p, h.ni * sizeof(float2)));
+  if (h.has_prev) PG_TRY(put(S.ddir_prev.p, h.ni * sizeof(float2)));
+  PG_TRY(put(S.sc.p, S_NSCAL * sizeof(double)));
+  PG_TRY(put(S.fl.p, F_NFLAG * sizeof(uint32_t)));
+  PG_CUDA(cudaStreamSynchronize(s));
+  A->pcg_cache = std::move(c);
+  return PG_OK;
+}
+
+pg_status pg_pcg_resume_device(pg_op A, const void* W, const void* y, const pg_penalty* R, uint64_t niter,
+                               void* x_out, void* iters_done_dev, void* stream) {
+  if (!A || !y || !R || !x_out) return set_error(PG_INVALID_ARG, "pcg resume: null argument");
+  PG_TRY(ensure_init());
+  cudaStream_t s = stream ? (cudaStream_t)stream : default_stream();
+  return pcg_solve_device(A, nullptr, (const float*)W, (const float2*)y, *R, niter, (float2*)x_out,
+                          (uint32_t*)iters_done_dev, s, nullptr, true);
+}
+
+pg_status pg_pcg_resume(pg_op A, const float* W, const float* y, const pg_penalty* R, uint64_t niter, float* x_out,
+                        uint64_t* iters_done) {
+  if (!A || !y || !R || !x_out) return set_error(PG_INVALID_ARG, "pcg resume: null argument");
+  PG_TRY(ensure_init());
+  cudaStream_t s = default_stream();
+  PG_TRY(A->hy.upload(reinterpret_cast<const float2*>(y), A->n_data, s));
+  if (W) PG_TRY(A->hw.upload(W, A->n_data, s));
+  PG_TRY(A->hx.alloc(A->n_image));
+  PG_TRY(A->hit.alloc(1));
+  PG_TRY(pcg_solve_device(A, nullptr, W ? A->hw.p : nullptr, A->hy.p, *R, niter, A->hx.p, A->hit.p, s, nullptr,
+                          true));
+  PG_CUDA(cudaMemcpyAsync(x_out, A->hx.p, A->n_image * sizeof(float2), cudaMemcpyDeviceToHost, s));
+  uint32_t n = 0;
+  PG_CUDA(cudaMemcpyAsync(&n, A->hit.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  PG_CUDA(cudaStreamSynchronize(s));
+  if (iters_done) *iters_done = n;
   return PG_OK;
 }
 

@@ -24,7 +24,7 @@ from . import _lib
 from ._lib import P, U64, Penalty, check
 
 __all__ = ["Gnufft", "Gdft", "GdftR2", "TimeSegmentation", "SENSE", "pcSenseTimeSeg", "pcSENSE", "LRobj", "QuadPenalty",
-           "TVPenalty", "R_lowRank",
+           "TVPenalty", "R_lowRank", "pcg_state_save", "pcg_resume",
            "calc3DDensityCompensation", "gridCoilImages", "calcSumOfSquaresImage", "solve_pwls_pcg", "reconSolve",
            "init"]
 
@@ -389,6 +389,29 @@ def solve_pwls_pcg_device(A: _Op, yi, R: QuadPenalty, niter, x_out, xInitial=Non
                                            int(niter), P(x_out.data_ptr()),
                                            None if iters is None else P(iters.data_ptr()), _stream_ptr(stream)))
     return x_out
+
+
+def pcg_state_save(A: _Op) -> bytes:
+    """The solver state on A after a solve (x, Ax, residual, direction(s), scalars, counters)."""
+    n = U64()
+    check(_lib.load().pg_pcg_state_size(A.handle, C.byref(n)))
+    buf = np.empty(n.value, np.uint8)
+    check(_lib.load().pg_pcg_state_save(A.handle, _ptr(buf), n.value))
+    return buf.tobytes()
+
+
+def pcg_resume(A: _Op, state: bytes, W, yi, R: QuadPenalty, niter):
+    """Load `state` onto A and run niter more PCG iterations; returns (x, iterations counted from the start)."""
+    buf = np.frombuffer(state, np.uint8).copy()
+    pen = R._struct()
+    check(_lib.load().pg_pcg_state_load(A.handle, C.byref(pen), _ptr(buf), buf.size))
+    yi = _c64(yi)
+    Wa = None if W is None else _f32(W)
+    x = np.empty(A.n_image, dtype=np.complex64)
+    it = U64()
+    check(_lib.load().pg_pcg_resume(A.handle, None if Wa is None else _ptr(Wa), _ptr(yi), C.byref(pen), int(niter),
+                                     _ptr(x), C.byref(it)))
+    return x, int(it.value)
 
 
 def reconSolve(data, Sg: _Op, R: QuadPenalty, kx=None, ky=None, kz=None, Nx=None, Ny=None, Nz=None, tvec=None,

@@ -359,3 +359,36 @@ def test_run_to_run_reproducibility(pg):
     G3 = pg.Gnufft(M, 3.0, p.nx, p.ny, p.nz, p.kx, p.ky, p.kz)
     ys = y1[:M]
     assert np.array_equal(G3.adjointSpatialInterp(ys), G3.adjointSpatialInterp(ys))
+
+
+@pytest.mark.parametrize("name", ["pcg2d", "pcgtv2d"])
+def test_pcg_checkpoint_resume(pg, name):
+    """2 iterations, the solver state saved to the host and loaded onto a new
+    plan, 3 more: the same image and count as 5 uninterrupted iterations, up
+    to the gridding adjoint's run-to-run rounding (these fixtures amplify it
+    past ~5 iterations: two uninterrupted 10-iteration solves differ by up to
+    2e-2, as the reference's float solve differs from FP64)."""
+    c = _case(name)
+    if name == "pcgtv2d":
+        R = pg.TVPenalty(c["nx"], c["ny"], c["nz"], c["beta"], c["delta"])
+    else:
+        R = pg.QuadPenalty(c["nx"], c["ny"], c["nz"], c["beta"])
+    y = c["y_f32"]
+    x5, it5 = pg.solve_pwls_pcg(None, _gpu_op(pg, name, c), None, y, R, 5)
+    x5b, _ = pg.solve_pwls_pcg(None, _gpu_op(pg, name, c), None, y, R, 5)
+    A = _gpu_op(pg, name, c)
+    pg.solve_pwls_pcg(None, A, None, y, R, 2)
+    state = pg.pcg_state_save(A)
+    B = _gpu_op(pg, name, c)
+    x, it = pg.pcg_resume(B, state, None, y, R, 3)
+    e, floor = rel_l2(x, x5), rel_l2(x5b, x5)
+    print(f"{name}: resumed vs uninterrupted {e:.2e} (two uninterrupted solves: {floor:.2e}), "
+          f"iterations {it} / {it5}")
+    assert it == it5 == 5 and e <= 1e-5
+    from powergrid_b200._lib import PGError
+    with pytest.raises(PGError, match="no solve has run"):
+        pg.pcg_state_save(_gpu_op(pg, name, c))
+    other = pg.TVPenalty(c["nx"], c["ny"], c["nz"], 1e-3, 0.1) if name == "pcg2d" else \
+        pg.QuadPenalty(c["nx"], c["ny"], c["nz"], 1e-3)
+    with pytest.raises(PGError, match="saved for"):
+        pg.pcg_resume(_gpu_op(pg, name, c), state, None, y, other, 2)
