@@ -756,11 +756,9 @@ pg_status launch_fused(Kern kern, int B, cudaStream_t s, Args... args) {
   return PG_OK;
 }
 
-// The fused passes run where a cluster of four 192 KB CTAs can be resident.
-bool fused_available() {
-  static int ok = -1;
-  if (ok >= 0) return ok == 1;
-  ok = 0;
+// The fused passes run where a cluster of four 192 KB CTAs can be resident
+// (queried once per process; plan creation may run on several threads).
+bool query_fused() {
   if (cudaFuncSetAttribute(k_fft2_fwd_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused::smem) !=
           cudaSuccess ||
       cudaFuncSetAttribute(k_fft2_adj_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused::smem) !=
@@ -785,8 +783,12 @@ bool fused_available() {
     cudaGetLastError();
     return false;
   }
-  ok = (nf >= 1 && na >= 1) ? 1 : 0;
-  return ok == 1;
+  return nf >= 1 && na >= 1;
+}
+
+bool fused_available() {
+  static const bool ok = query_fused();   // thread-safe one-time initialisation
+  return ok;
 }
 
 // PG_FFT_FUSED=0 (read at each call) keeps the separate passes.
