@@ -436,6 +436,14 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
   __shared__ float scale[16], inv_scale[16];
   // planes per block: NP when fixed at compile time, else cc x K
   const int np = (NP > 0) ? NP : cc * K;
+  // The tile planes are zeroed once here; afterwards each item's flush zeroes
+  // every cell as it reads it (one thread per cell), and the scale step
+  // resets the plane maxima it has read (next_item's barrier orders both).
+  {
+    int4* z = reinterpret_cast<int4*>(smi);
+    for (int q = threadIdx.x; q < (np * 2 * CELLS) / 4; q += blockDim.x) z[q] = make_int4(0, 0, 0, 0);
+  }
+  if (threadIdx.x < 16) vmax[threadIdx.x] = 0u;
   for (int item; (item = next_item(queue, nitems)) >= 0;) {
   const int4 sp = sub[item / nchunks];
   const int cfirst = c0 + (item % nchunks) * cc;
@@ -450,13 +458,6 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
   float* sw = reinterpret_cast<float*>(smi + (size_t)np * 2 * CELLS);
   float2* sv = reinterpret_cast<float2*>(sw + (size_t)smax * WROW);
   uint2* sst = reinterpret_cast<uint2*>(sv + (size_t)smax * np);
-
-  {
-    int4* z = reinterpret_cast<int4*>(smi);
-    for (int q = tid; q < (np * 2 * CELLS) / 4; q += blockDim.x) z[q] = make_int4(0, 0, 0, 0);
-  }
-  if (tid < 16) vmax[tid] = 0u;
-  __syncthreads();
 
   // 1. staging: asynchronous copies straight into shared memory (no register
   // round trip; every copy of the item is in flight before the one wait)
@@ -505,14 +506,10 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
     }
     scale[tid] = ldexpf(1.f, e);
     inv_scale[tid] = ldexpf(1.f, -e);
+    vmax[tid] = 0u;                        // for the next item
   }
   __syncthreads();
-  for (int q = tid; q < count * np; q += blockDim.x) {
-    const float sc = scale[q % np];
-    const float2 v = sv[q];
-    sv[q] = make_float2(v.x * sc, v.y * sc);
-  }
-  __syncthreads();
+  // the scale is applied to each value as the spread reads it (exact: a power of two)
 
   // 3. spread
   const int warp = tid >> 5, lane = tid & 31;
@@ -527,6 +524,9 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
     // to the integer grid.  Integer sums of the runs do not depend on the
     // order of the atomics, so the result is deterministic.
     constexpr int NPC = NP > 0 ? NP : 1;
+    float scp[NPC];
+#pragma unroll
+    for (int pl = 0; pl < NPC; ++pl) scp[pl] = scale[pl];
     const int per = (count + NW - 1) / NW;
     const int i0 = warp * per, i1 = min(count, i0 + per);
     float2 a0[NPC], a1[NPC];              // (re, im) at tap dx and dx + 4
@@ -560,7 +560,8 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
       const float2* vi = sv + i * NPC;
 #pragma unroll
       for (int pl = 0; pl < NPC; ++pl) {
-        const float2 v = vi[pl];
+        const float2 u = vi[pl];
+        const float2 v = make_float2(u.x * scp[pl], u.y * scp[pl]);
         a0[pl] = __ffma2_rn(w0v, v, a0[pl]);
         a1[pl] = __ffma2_rn(w1v, v, a1[pl]);
       }
@@ -578,7 +579,9 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
       if (DIM == 2) {
 #pragma unroll
         for (int pl = 0; pl < np; ++pl) {
-          const float2 v = vi[pl];
+          const float2 u = vi[pl];
+          const float sc = scale[pl];
+          const float2 v = make_float2(u.x * sc, u.y * sc);
           atomicAdd(b + (2 * pl) * CELLS, fixed_point(w0, v.x));
           atomicAdd(b + (2 * pl + 1) * CELLS, fixed_point(w0, v.y));
           atomicAdd(b + (2 * pl) * CELLS + 4 * PY, fixed_point(w1, v.x));
@@ -593,7 +596,9 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
           const float w0e = w0 * wzv, w1e = w1 * wzv;
 #pragma unroll
           for (int pl = 0; pl < np; ++pl) {
-            const float2 v = vi[pl];
+            const float2 u = vi[pl];
+            const float sc = scale[pl];
+            const float2 v = make_float2(u.x * sc, u.y * sc);
             atomicAdd(b + (2 * pl) * CELLS, fixed_point(w0e, v.x));
             atomicAdd(b + (2 * pl + 1) * CELLS, fixed_point(w0e, v.y));
             atomicAdd(b + (2 * pl) * CELLS + 4 * PY, fixed_point(w1e, v.x));
@@ -612,16 +617,20 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
     const int pxx = (q / PY) % PX;
     const int pzz = q / PLANE;
     const int gy = y0 + pyy, gx = x0 + pxx, gz = z0 + pzz;
-    if (gy >= g.Gy || gx >= g.Gx || gz >= g.Gz) continue;
+    const bool inside = gy < g.Gy && gx < g.Gx && gz < g.Gz;
     const uint64_t idx = (uint64_t)gy + (uint64_t)g.Gy * ((uint64_t)gx + (uint64_t)g.Gx * gz);
     int pl = 0;
     for (int c = 0; c < cc; ++c)
       for (int j = 0; j < K; ++j, ++pl) {
-        const int* pr = smi + (pl * 2) * CELLS;
+        int* pr = smi + (pl * 2) * CELLS;
         const int re = pr[q], im = pr[CELLS + q];
-        if (re != 0 || im != 0)
-          atomicAdd(grids + ((uint64_t)(cfirst + c) * L + lseg + j) * G + idx,
-                    make_float2((float)re * inv_scale[pl], (float)im * inv_scale[pl]));
+        if (re != 0 || im != 0) {
+          pr[q] = 0;                       // zero for the next item
+          pr[CELLS + q] = 0;
+          if (inside)
+            atomicAdd(grids + ((uint64_t)(cfirst + c) * L + lseg + j) * G + idx,
+                      make_float2((float)re * inv_scale[pl], (float)im * inv_scale[pl]));
+        }
       }
   }
   }
