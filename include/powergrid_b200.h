@@ -176,8 +176,10 @@ pg_status pg_sum_of_squares_image(const float* coil_images, uint64_t n, uint64_t
  * held by every GPU that loads the library until exit, so nk is limited to
  * 524288 samples (larger sizes return PG_INVALID_ARG).  The array is shared
  * by all calls: calls whose work overlaps on the GPU race and must be
- * ordered by the caller.  The first call on each device looks up the array's
- * device address; make that first call before any stream capture.
+ * ordered by the caller.  The call runs on the device given to pg_init (the
+ * library makes it current), so the buffers must live on that device.  The
+ * first call after pg_init looks up the array's device address; make that
+ * first call before any stream capture.
  * Stream-ordered on `stream` (NULL = the library's stream). */
 pg_status pg_gdft_forward_noalloc(uint64_t nk, uint64_t ni, const float* kx, const float* ky, const float* kz,
                                   const float* ix, const float* iy, const float* iz, const float* field_map,
@@ -221,7 +223,10 @@ pg_status pg_pcg_solve_device(pg_op A, const void* x0_dev, const void* W_dev, co
  * iterations), and loaded onto an operator of the same shape, e.g. a new
  * plan on another GPU.  pg_pcg_resume then runs niter more iterations from
  * it, exactly as the uninterrupted solve would continue; iters_done counts
- * from the original start. */
+ * from the original start.  The blob records the operator shape and the
+ * penalty (kind, size, beta, delta, dims2penalize) it was computed for;
+ * pg_pcg_state_load and pg_pcg_resume refuse another one with
+ * PG_INVALID_ARG. */
 pg_status pg_pcg_state_size(pg_op A, uint64_t* bytes);
 pg_status pg_pcg_state_save(pg_op A, void* host, uint64_t bytes);
 pg_status pg_pcg_state_load(pg_op A, const pg_penalty* R, const void* host, uint64_t bytes);

@@ -67,6 +67,7 @@ def lib() -> C.CDLL:
         L.orc_forward.argtypes = [P, P, P]
         L.orc_adjoint.argtypes = [P, P, P]
         L.orc_pcg.argtypes = [P, P, P, P, C.c_int, U64, U64, U64, C.c_double, C.c_double, U64, U64, P]
+        L.orc_pcg_fp64_over_f32.argtypes = [P, P, P, C.c_int, U64, U64, U64, C.c_double, C.c_double, U64, U64, P]
         L.orc_penalty_gradient.argtypes = [C.c_int, C.c_int, U64, U64, U64, C.c_double, C.c_double, U64, P, P]
         L.orc_penalty_denom.argtypes = [C.c_int, C.c_int, U64, U64, U64, C.c_double, C.c_double, U64, P, P, P]
         L.orc_lowrank_new.restype = P
@@ -158,6 +159,21 @@ class Op:
         kind = {"quad": 0, "tv": 1}[penalty]
         n = lib().orc_pcg(self.h, x0p, None if Wa is None else _p(Wa), _p(y), kind, nx, ny, nz, beta, delta,
                           dims2pen, niter, _p(x))
+        return x, n
+
+    def pcg_fp64_solver(self, y, penalty: str, nx, ny, nz, beta, delta=1.0, dims2pen=3, niter=10, W=None):
+        """PWLS-PCG with FP64 vectors, inner products and steps over this float
+        operator (inputs rounded to float, outputs widened): the operator's FP32
+        rounding is then the solve's only FP32 step.  Returns complex128."""
+        if self.prec != 0:
+            raise ValueError("pcg_fp64_solver needs a float (precision 0) operator")
+        y = np.ascontiguousarray(y, dtype=C128)
+        x = np.zeros(self.n_image, dtype=C128)
+        Wa = None if W is None else np.ascontiguousarray(W, dtype=F64)
+        n = lib().orc_pcg_fp64_over_f32(self.h, None if Wa is None else _p(Wa), _p(y), {"quad": 0, "tv": 1}[penalty],
+                                        nx, ny, nz, beta, delta, dims2pen, niter, _p(x))
+        if n < 0:
+            raise RuntimeError("oracle: " + lib().orc_last_error().decode())
         return x, n
 
     def timeseg_tables(self):

@@ -5,6 +5,9 @@
 //   0  float  — the reference CPU path (T1 = float)
 //   1  double — the reference's double instantiation (ftCpu<double> keeps sinf/cosf)
 //   2  FP64   — the FP64 oracle (as 1, but the DFT evaluates sin/cos in double)
+//   3  FP64 evaluation of the float Gnufft: window bounds, LUT index, LUT
+//      values and beta as the float instantiation computes them, every other
+//      step in double (the float operator without its rounding)
 // All geometry / map / time inputs arrive as float32 (what the product
 // receives) and are widened for precision 1/2.  Complex vectors are
 // interleaved complex64 for precision 0 and complex128 otherwise.
@@ -103,6 +106,59 @@ struct SenseParallel : pgo::SenseOp<T> {
   }
 };
 
+// pcSenseTimeSeg with its (coil, shot, segment) Gnufft calls spread over
+// threads.  Per-element arithmetic and summation order equal the serial
+// loops of PcSenseTimeSegOp and TimeSegOp (pcSenseTimeSeg.cpp:127-171,
+// TimeSegmentation.cpp:252-324).
+template <typename T>
+struct PcSenseTsParallel : pgo::PcSenseTimeSegOp<T> {
+  using C = std::complex<T>;
+  using pgo::PcSenseTimeSegOp<T>::PcSenseTimeSegOp;
+  void forward(const C* x, C* y) const override {
+    if (g_threads <= 1) return pgo::PcSenseTimeSegOp<T>::forward(x, y);
+    const u64 Ni = this->Ni, Nd = this->Nd, Ns = this->Ns, Nc = this->Nc, L = (u64)this->A[0]->L;
+    std::vector<C> out(Nd * L * Ns * Nc);
+    parallel_for(Nc * Ns * L, [&](u64 u) {
+      const u64 l = u % L, cs = u / L, s = cs % Ns;   // cs = s + c*Ns
+      const auto* ts = this->A[s].get();
+      const C* m = this->M.data() + Ni * cs;
+      std::vector<C> tmp(Ni);
+      for (u64 p = 0; p < Ni; ++p) tmp[p] = ts->Wo[p + Ni * l] * (x[p] * m[p]);
+      ts->G->forward(tmp.data(), out.data() + Nd * u);
+    });
+    for (u64 cs = 0; cs < Nc * Ns; ++cs) {
+      const auto* ts = this->A[cs % Ns].get();
+      C* yc = y + Nd * cs;
+      std::fill(yc, yc + Nd, C(0, 0));
+      for (u64 l = 0; l < L; ++l)
+        for (u64 q = 0; q < Nd; ++q) yc[q] += out[Nd * (cs * L + l) + q] * ts->AA[q + Nd * l];
+    }
+  }
+  void adjoint(const C* d, C* x) const override {
+    if (g_threads <= 1) return pgo::PcSenseTimeSegOp<T>::adjoint(d, x);
+    const u64 Ni = this->Ni, Nd = this->Nd, Ns = this->Ns, Nc = this->Nc, L = (u64)this->A[0]->L;
+    std::vector<C> img(Ni * L * Ns * Nc);
+    parallel_for(Nc * Ns * L, [&](u64 u) {
+      const u64 l = u % L, cs = u / L, s = cs % Ns;
+      const auto* ts = this->A[s].get();
+      const C* dc = d + Nd * cs;
+      std::vector<C> tmp(Nd);
+      for (u64 q = 0; q < Nd; ++q) tmp[q] = std::conj(ts->AA[q + Nd * l]) * dc[q];
+      ts->G->adjoint(tmp.data(), img.data() + Ni * u);
+    });
+    std::fill(x, x + Ni, C(0, 0));
+    std::vector<C> xs(Ni);
+    for (u64 cs = 0; cs < Nc * Ns; ++cs) {
+      const auto* ts = this->A[cs % Ns].get();
+      std::fill(xs.begin(), xs.end(), C(0, 0));
+      for (u64 l = 0; l < L; ++l)
+        for (u64 p = 0; p < Ni; ++p) xs[p] += img[Ni * (cs * L + l) + p] * ts->WoH[p + Ni * l];
+      const C* m = this->Mc.data() + Ni * cs;
+      for (u64 p = 0; p < Ni; ++p) x[p] += m[p] * xs[p];
+    }
+  }
+};
+
 struct Handle {
   int prec;
   std::unique_ptr<pgo::Op<float>> f;
@@ -129,6 +185,26 @@ template <>
 void set<float>(Handle* h, pgo::Op<float>* op) { h->f.reset(op); }
 template <>
 void set<double>(Handle* h, pgo::Op<double>* op) { h->d.reset(op); }
+
+// An FP64 view of a float operator: the input is rounded to float, the float
+// operator applied and its output widened.  Solving over it in FP64 leaves
+// the operator's FP32 rounding as the only FP32 step, which separates the
+// operator's share of a float solve's error from the solver's.
+struct WidenedOp : pgo::Op<double> {
+  const pgo::Op<float>* f = nullptr;
+  void forward(const std::complex<double>* x, std::complex<double>* y) const override {
+    std::vector<std::complex<float>> xf(n2), yf(n1);
+    for (u64 i = 0; i < n2; ++i) xf[i] = std::complex<float>((float)x[i].real(), (float)x[i].imag());
+    f->forward(xf.data(), yf.data());
+    for (u64 i = 0; i < n1; ++i) y[i] = std::complex<double>(yf[i].real(), yf[i].imag());
+  }
+  void adjoint(const std::complex<double>* y, std::complex<double>* x) const override {
+    std::vector<std::complex<float>> yf(n1), xf(n2);
+    for (u64 i = 0; i < n1; ++i) yf[i] = std::complex<float>((float)y[i].real(), (float)y[i].imag());
+    f->adjoint(yf.data(), xf.data());
+    for (u64 i = 0; i < n2; ++i) x[i] = std::complex<double>(xf[i].real(), xf[i].imag());
+  }
+};
 
 template <typename F>
 void* guard(F fn) {
@@ -218,7 +294,10 @@ void* orc_gnufft_new(int prec, u64 M, float gridos, u64 nx, u64 ny, u64 nz, cons
     } else {
       auto a = widen<double>(kx, M), b = widen<double>(ky, M), c = widen<double>(kz, M);
       auto* op = new pgo::GnufftOp<double>(M, gridos, (int)nx, (int)ny, (int)nz, a.data(), b.data(), c.data());
-      op->use_ref = g_use_ref;
+      if (prec == 3)
+        op->use_float_taps();
+      else
+        op->use_ref = g_use_ref;
       h->d.reset(op);
     }
     return h;
@@ -315,16 +394,19 @@ void* orc_pcsense_ts_new(int prec, const float* kx, const float* ky, const float
     const u64 ni = nx * ny * nz;
     const std::complex<float>* s = reinterpret_cast<const std::complex<float>*>(smap);
     if (prec == 0) {
-      h->f.reset(new pgo::PcSenseTimeSegOp<float>(kx, ky, kz, nk, (int)nx, (int)ny, (int)nz, nc, t, L, type, s,
-                                                  fmap, pmap, npmap, g_use_ref));
+      h->f.reset(new PcSenseTsParallel<float>(kx, ky, kz, nk, (int)nx, (int)ny, (int)nz, nc, t, L, type, s,
+                                              fmap, pmap, npmap, g_use_ref));
     } else {
       auto a = widen<double>(kx, nk), b = widen<double>(ky, nk), c = widen<double>(kz, nk);
       auto tt = widen<double>(t, nk), fm = widen<double>(fmap, ni), pm = widen<double>(pmap, npmap);
       std::vector<std::complex<double>> sd(ni * nc);
       for (u64 i = 0; i < ni * nc; ++i) sd[i] = std::complex<double>(s[i].real(), s[i].imag());
-      h->d.reset(new pgo::PcSenseTimeSegOp<double>(a.data(), b.data(), c.data(), nk, (int)nx, (int)ny, (int)nz,
-                                                   nc, tt.data(), L, type, sd.data(), fm.data(), pm.data(), npmap,
-                                                   g_use_ref));
+      auto* op = new PcSenseTsParallel<double>(a.data(), b.data(), c.data(), nk, (int)nx, (int)ny, (int)nz,
+                                               nc, tt.data(), L, type, sd.data(), fm.data(), pm.data(), npmap,
+                                               g_use_ref && prec != 3);
+      if (prec == 3)
+        for (auto& g : op->G) g->use_float_taps();
+      h->d.reset(op);
     }
     return h;
   });
@@ -441,6 +523,25 @@ int orc_pcg(void* h, const void* x0, const void* W, const void* y, int kind, u64
   };
   if (o->prec == 0) return run(o->f.get(), float());
   return run(o->d.get(), double());
+}
+
+// PWLS-PCG in FP64 (vectors, inner products, steps) over a float (precision 0)
+// operator.  y and xout are complex128; W, if given, double.
+int orc_pcg_fp64_over_f32(void* h, const void* W, const void* y, int kind, u64 nx, u64 ny, u64 nz, double beta,
+                          double delta, u64 dims2pen, u64 niter, void* xout) {
+  Handle* o = (Handle*)h;
+  if (o->prec != 0) { g_err = "orc_pcg_fp64_over_f32 needs a float operator"; return -1; }
+  WidenedOp A;
+  A.f = o->f.get();
+  A.n1 = pgo::op_data_len(*A.f);
+  A.n2 = pgo::op_image_len(*A.f);
+  pgo::Penalty<double> R;
+  R.kind = kind; R.Nx = nx; R.Ny = ny; R.Nz = nz; R.beta = beta; R.delta = delta; R.dims2pen = dims2pen;
+  std::vector<double> w(A.n1, 1.0);
+  if (W) std::memcpy(w.data(), W, sizeof(double) * A.n1);
+  std::vector<std::complex<double>> xi(A.n2, std::complex<double>(0, 0));
+  return pgo::pwls_pcg<double>(A, xi.data(), w.data(), (const std::complex<double>*)y, R, niter,
+                               (std::complex<double>*)xout);
 }
 
 // LRobj over oracle operators (lowRank/LRobj.cpp:27-68); the operators are

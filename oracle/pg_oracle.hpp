@@ -106,6 +106,13 @@ struct Geom {
   T kw = 4;                    // kernel width
   T beta = 0;
   std::vector<T> lut;
+  // FP64 evaluation of the float operator (double only): window bounds, LUT
+  // index and LUT values as the float instantiation computes them (lut32),
+  // every other step in T.  The float and double instantiations pick
+  // different LUT entries for some taps, which makes them two operators
+  // that differ by ~2e-5; this mode is the float operator without rounding.
+  bool float_taps = false;
+  std::vector<float> lut32;
   bool is3d() const { return Nz != 1; }
   u64 nimg() const { return (u64)Nx * Ny * Nz; }
   u64 ngrid() const { return (u64)Gx * Gy * Gz; }
@@ -141,25 +148,42 @@ inline T lut_weight(T s, int n, T os, T kw, const T* lut, u64 nlut) {
   return lut[k0];
 }
 
+// Sample position on the grid, window bounds and tap weight through the
+// geometry: with float_taps the float operator's values, widened.
+template <typename T>
+inline T grid_pos(const Geom<T>& g, T k, int n) {
+  if (g.float_taps) return (T)((float)g.os * ((float)k + ((float)n) / 2.0f));
+  return (g.os) * (k + ((T)n) / (T)2.0);
+}
+template <typename T>
+inline void win(const Geom<T>& g, T s, int n, int& lo, int& hi) {
+  if (g.float_taps) window<float>((float)s, (float)g.kw, (float)g.os, n, lo, hi);
+  else window(s, g.kw, g.os, n, lo, hi);
+}
+template <typename T>
+inline T tapw(const Geom<T>& g, T s, int c) {
+  if (g.float_taps)
+    return (T)lut_weight<float>((float)s, c, (float)g.os, (float)g.kw, g.lut32.data(), g.lut32.size());
+  return lut_weight(s, c, g.os, g.kw, g.lut.data(), g.lut.size());
+}
+
 // Forward interpolation: y_i = sum over the window of w * grid[ny + nx*Gy (+ nz*Gx*Gy)]
 // (gridding.cpp:217-415).
 template <typename T>
 void interp_forward(const Geom<T>& g, u64 M, const T* kx, const T* ky, const T* kz,
                     const std::complex<T>* grid, std::complex<T>* y) {
-  const T* lut = g.lut.data();
-  const u64 nl = g.lut.size();
   for (u64 i = 0; i < M; ++i) {
     T acc_r = 0, acc_i = 0;
-    T sx = (g.os) * (kx[i] + ((T)g.Nx) / (T)2.0);
-    T sy = (g.os) * (ky[i] + ((T)g.Ny) / (T)2.0);
+    T sx = grid_pos(g, kx[i], g.Nx);
+    T sy = grid_pos(g, ky[i], g.Ny);
     int xl, xh, yl, yh;
-    window(sx, g.kw, g.os, g.Nx, xl, xh);
-    window(sy, g.kw, g.os, g.Ny, yl, yh);
+    win(g, sx, g.Nx, xl, xh);
+    win(g, sy, g.Ny, yl, yh);
     if (!g.is3d()) {
       for (int nx = xl; nx <= xh; ++nx) {
-        T wx = lut_weight(sx, nx, g.os, g.kw, lut, nl);
+        T wx = tapw(g, sx, nx);
         for (int ny = yl; ny <= yh; ++ny) {
-          T wy = lut_weight(sy, ny, g.os, g.kw, lut, nl);
+          T wy = tapw(g, sy, ny);
           T w = wx * wy;
           const std::complex<T> v = grid[(u64)ny + (u64)nx * g.Gy];
           acc_r += w * v.real();
@@ -167,15 +191,15 @@ void interp_forward(const Geom<T>& g, u64 M, const T* kx, const T* ky, const T* 
         }
       }
     } else {
-      T sz = (g.os) * (kz[i] + ((T)g.Nz) / (T)2.0);
+      T sz = grid_pos(g, kz[i], g.Nz);
       int zl, zh;
-      window(sz, g.kw, g.os, g.Nz, zl, zh);
+      win(g, sz, g.Nz, zl, zh);
       for (int nz = zl; nz <= zh; ++nz) {
-        T wz = lut_weight(sz, nz, g.os, g.kw, lut, nl);
+        T wz = tapw(g, sz, nz);
         for (int nx = xl; nx <= xh; ++nx) {
-          T wx = lut_weight(sx, nx, g.os, g.kw, lut, nl);
+          T wx = tapw(g, sx, nx);
           for (int ny = yl; ny <= yh; ++ny) {
-            T wy = lut_weight(sy, ny, g.os, g.kw, lut, nl);
+            T wy = tapw(g, sy, ny);
             T w = wx * wy * wz;
             const std::complex<T> v = grid[(u64)ny + (u64)nx * g.Gy + (u64)nz * g.Gx * g.Gy];
             acc_r += w * v.real();
@@ -192,21 +216,19 @@ void interp_forward(const Geom<T>& g, u64 M, const T* kx, const T* ky, const T* 
 template <typename T>
 void spread_adjoint(const Geom<T>& g, u64 M, const T* kx, const T* ky, const T* kz,
                     const std::complex<T>* d, std::complex<T>* grid) {
-  const T* lut = g.lut.data();
-  const u64 nl = g.lut.size();
   T* gr = reinterpret_cast<T*>(grid);
   for (u64 i = 0; i < M; ++i) {
     const T dr = d[i].real(), di = d[i].imag();
-    T sx = (g.os) * (kx[i] + ((T)g.Nx) / (T)2.0);
-    T sy = (g.os) * (ky[i] + ((T)g.Ny) / (T)2.0);
+    T sx = grid_pos(g, kx[i], g.Nx);
+    T sy = grid_pos(g, ky[i], g.Ny);
     int xl, xh, yl, yh;
-    window(sx, g.kw, g.os, g.Nx, xl, xh);
-    window(sy, g.kw, g.os, g.Ny, yl, yh);
+    win(g, sx, g.Nx, xl, xh);
+    win(g, sy, g.Ny, yl, yh);
     if (!g.is3d()) {
       for (int nx = xl; nx <= xh; ++nx) {
-        T wx = lut_weight(sx, nx, g.os, g.kw, lut, nl);
+        T wx = tapw(g, sx, nx);
         for (int ny = yl; ny <= yh; ++ny) {
-          T wy = lut_weight(sy, ny, g.os, g.kw, lut, nl);
+          T wy = tapw(g, sy, ny);
           T w = wx * wy;
           const u64 idx = 2 * ((u64)ny + (u64)nx * g.Gy);
           gr[idx] += w * dr;
@@ -214,15 +236,15 @@ void spread_adjoint(const Geom<T>& g, u64 M, const T* kx, const T* ky, const T* 
         }
       }
     } else {
-      T sz = (g.os) * (kz[i] + ((T)g.Nz) / (T)2.0);
+      T sz = grid_pos(g, kz[i], g.Nz);
       int zl, zh;
-      window(sz, g.kw, g.os, g.Nz, zl, zh);
+      win(g, sz, g.Nz, zl, zh);
       for (int nz = zl; nz <= zh; ++nz) {
-        T wz = lut_weight(sz, nz, g.os, g.kw, lut, nl);
+        T wz = tapw(g, sz, nz);
         for (int nx = xl; nx <= xh; ++nx) {
-          T wx = lut_weight(sx, nx, g.os, g.kw, lut, nl);
+          T wx = tapw(g, sx, nx);
           for (int ny = yl; ny <= yh; ++ny) {
-            T wy = lut_weight(sy, ny, g.os, g.kw, lut, nl);
+            T wy = tapw(g, sy, ny);
             T w = wx * wy * wz;
             const u64 idx = (u64)ny + (u64)nx * g.Gy + (u64)nz * g.Gx * g.Gy;
             gr[2 * idx] += w * dr;
@@ -422,6 +444,13 @@ struct GnufftOp : Op<T> {
   }
   u64 data_len() const { return this->n2; }
   u64 image_len() const { return this->n1; }
+  // Evaluate the float operator's taps in this (double) instantiation.
+  void use_float_taps() {
+    const float beta32 = kb_beta<float>((float)g.os, 4.0f);
+    g.float_taps = true;
+    g.lut32 = kb_lut<float>(beta32, 4.0f);
+    g.beta = (T)beta32;   // the float operator's beta (deapodization), widened
+  }
 
   // computeFd_CPU_Grid restated (gridding.cpp:584-727)
   void forward(const C* x, C* y) const override {

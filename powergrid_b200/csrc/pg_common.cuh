@@ -18,6 +18,9 @@
 namespace pg {
 
 pg_status set_error(pg_status s, const char* fmt, ...);
+// Drops the cached device address of the allocation-free Gdft's scratch array
+// (pg_noalloc.cu); pg_shutdown calls it.
+void noalloc_forget_scratch();
 pg_status ensure_init();
 cudaStream_t default_stream();
 int sm_count();

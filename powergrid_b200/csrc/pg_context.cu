@@ -164,6 +164,7 @@ pg_status pg_shutdown(void) {
   cudaStreamSynchronize(pg::g_stream);
   cudaStreamDestroy(pg::g_stream);
   pg::g_stream = nullptr;
+  pg::noalloc_forget_scratch();
   pg::g_inited = false;
   return PG_OK;
 }

@@ -16,10 +16,13 @@
 // partial it later reads, so nothing from an earlier call carries over and
 // no clearing is needed.
 //
+// The call runs on the library's device (the one given to pg_init, which the
+// library makes current); the caller's buffers must live on that device.
 // In host code the array's name is only a host-side stand-in; the device
-// address is obtained with cudaGetSymbolAddress, once per device, with that
-// device current, on the first call on that device.  That first call should
-// therefore happen before any stream capture.
+// address is obtained with cudaGetSymbolAddress, with that device current,
+// on the first call after pg_init (pg_shutdown forgets it, so a call after
+// a later pg_init looks it up again).  That first call should therefore
+// happen before any stream capture.
 #include <mutex>
 
 #include "pg_gdft.cuh"
@@ -34,7 +37,8 @@ constexpr int kTileNA = 128;
 static __device__ __align__(256) float2 g_noalloc_partials[kNoAllocPartials];
 
 std::mutex g_na_mu;
-float2* g_na_addr[64] = {};  // per device
+float2* g_na_addr = nullptr;  // device address of g_noalloc_partials on g_na_dev
+int g_na_dev = -1;
 
 __device__ __forceinline__ void na_phase_sincos(double ph, float* s, float* c) {
   const double inv2pi = 0.15915494309189533577;   // 1 / (2 pi)
@@ -97,25 +101,33 @@ __global__ void k_dft_finish_noalloc(uint64_t nk, int nsplit, const float2* __re
   y[i] = s;
 }
 
+// The scratch array's device address on the current (library) device.
 pg_status noalloc_scratch(float2** out) {
   int dev = 0;
   PG_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) return set_error(PG_INVALID_ARG, "no-alloc Gdft: device index %d out of range", dev);
   std::lock_guard<std::mutex> lk(g_na_mu);
-  if (!g_na_addr[dev]) {
+  if (!g_na_addr || g_na_dev != dev) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
     if (e != cudaSuccess || !p) {
       cudaGetLastError();
       return set_error(PG_CUDA_ERROR, "no-alloc Gdft: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
     }
-    g_na_addr[dev] = static_cast<float2*>(p);
+    g_na_addr = static_cast<float2*>(p);
+    g_na_dev = dev;
   }
-  *out = g_na_addr[dev];
+  *out = g_na_addr;
   return PG_OK;
 }
 
 }  // namespace
+
+// Called by pg_shutdown: the cached address belongs to the context that ends.
+void noalloc_forget_scratch() {
+  std::lock_guard<std::mutex> lk(g_na_mu);
+  g_na_addr = nullptr;
+  g_na_dev = -1;
+}
 
 }  // namespace pg
 

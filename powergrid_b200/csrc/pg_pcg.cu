@@ -579,6 +579,8 @@ pg_status pcg_solve_device(pg_op_s* A, const float2* x0, const float* W, const f
     PG_CUDA(cudaMemcpyAsync(cache->ybuf.p, y, nd * sizeof(float2), cudaMemcpyDeviceToDevice, s));
     if (W) PG_CUDA(cudaMemcpyAsync(cache->wbuf.p, W, nd * sizeof(float), cudaMemcpyDeviceToDevice, s));
     else PG_LAUNCH(k_fill_ones, ceil_div(nd, 256), 256, 0, s, nd, cache->wbuf.p);
+    // what wbuf holds now: a later plain solve reuses the cache only if it is ones
+    cache->w_ones = (W == nullptr);
     return pcg_iterate(A, cache, niter, xout, iters_dev, s, cancel);
   }
   if (!cache || !cache->matches(Rh, W == nullptr)) {
@@ -970,12 +972,18 @@ pg_status pg_penalty_gradient_device(const pg_penalty* R, const void* x, void* g
 // The solver state between iterations, as a host blob: a header, then x, Ax,
 // the residual r and the direction (ni, nd, nd, ni complex), the previous
 // direction for the quadratic penalty (ni), the FP64 scalars and the flags.
+// The blob records the objective it was computed for (operator shape and
+// penalty parameters); loading it for another objective is refused, since the
+// saved direction and FP64 scalars belong to the saved one.
 struct PcgStateHeader {
   char magic[8];
   uint64_t ni, nd;
   int32_t kind, has_prev;
   uint64_t nscal, nflag;
+  uint64_t nx, ny, nz, dims2penalize;
+  float beta, delta;
 };
+constexpr char kStateMagic[9] = "PGPCGST2";
 
 static uint64_t state_bytes(uint64_t ni, uint64_t nd, bool prev) {
   return sizeof(PcgStateHeader) + (2 * ni + 2 * nd + (prev ? ni : 0)) * sizeof(float2) + S_NSCAL * sizeof(double) +
@@ -999,10 +1007,16 @@ pg_status pg_pcg_state_save(pg_op A, void* host, uint64_t bytes) {
   Solver& S = c->S;
   PG_CUDA(cudaDeviceSynchronize());   // the solve may have run on any stream
   PcgStateHeader h{};
-  std::memcpy(h.magic, "PGPCGST1", 8);
+  std::memcpy(h.magic, kStateMagic, 8);
   h.ni = A->n_image;
   h.nd = A->n_data;
   h.kind = S.R.kind;
+  h.nx = c->R.nx;
+  h.ny = c->R.ny;
+  h.nz = c->R.nz;
+  h.dims2penalize = c->R.dims2penalize;
+  h.beta = c->R.beta;
+  h.delta = c->R.delta;
   h.has_prev = S.ddir_prev.p ? 1 : 0;
   h.nscal = S_NSCAL;
   h.nflag = F_NFLAG;
@@ -1029,13 +1043,19 @@ pg_status pg_pcg_state_load(pg_op A, const pg_penalty* R, const void* host, uint
   PcgStateHeader h{};
   if (bytes < sizeof(h)) return set_error(PG_INVALID_ARG, "pcg state: %llu bytes", (unsigned long long)bytes);
   std::memcpy(&h, host, sizeof(h));
-  if (std::memcmp(h.magic, "PGPCGST1", 8) != 0 || h.nscal != S_NSCAL || h.nflag != F_NFLAG)
+  if (std::memcmp(h.magic, kStateMagic, 8) != 0 || h.nscal != S_NSCAL || h.nflag != F_NFLAG)
     return set_error(PG_INVALID_ARG, "pcg state: not a solver state of this library");
   if (h.ni != A->n_image || h.nd != A->n_data || h.kind != R->kind ||
       (h.has_prev != 0) != (R->kind == PG_PENALTY_QUAD) || bytes < state_bytes(h.ni, h.nd, h.has_prev != 0))
     return set_error(PG_INVALID_ARG, "pcg state: saved for a %llux%llu operator with penalty %d",
                      (unsigned long long)h.nd, (unsigned long long)h.ni, h.kind);
   if (R->nx * R->ny * R->nz != A->n_image) return set_error(PG_INVALID_ARG, "pcg state: penalty size");
+  if (h.nx != R->nx || h.ny != R->ny || h.nz != R->nz || h.dims2penalize != R->dims2penalize || h.beta != R->beta ||
+      (R->kind == PG_PENALTY_TV && h.delta != R->delta))
+    return set_error(PG_INVALID_ARG,
+                     "pcg state: saved for penalty %llux%llux%llu beta %g delta %g dims %llu, not this one",
+                     (unsigned long long)h.nx, (unsigned long long)h.ny, (unsigned long long)h.nz, (double)h.beta,
+                     (double)h.delta, (unsigned long long)h.dims2penalize);
   PG_TRY(ensure_init());
   cudaStream_t s = default_stream();
   A->pcg_cache.reset();

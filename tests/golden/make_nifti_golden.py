@@ -9,7 +9,9 @@ complex image as writeNiftiMagPhsImage does (processNIFTI.hpp:106-107) and
 writes header, 4-byte extender and float32 voxels (:88-99).  The resulting
 bytes pin the library's writer, which lays the header out by byte offset.
 
-Run where the reference tree exists:  python tests/golden/make_nifti_golden.py
+Run where the reference tree exists, with PG_REFERENCE_ROOT naming the
+reference project's root (the directory holding Support/ and PowerGrid/):
+    PG_REFERENCE_ROOT=<root> python tests/golden/make_nifti_golden.py
 """
 from __future__ import annotations
 
@@ -20,7 +22,13 @@ import tempfile
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_SUPPORT = "/root/reference/Support"
+
+
+def _ref_support() -> str:
+    root = os.environ.get("PG_REFERENCE_ROOT")
+    if not root:
+        raise SystemExit("set PG_REFERENCE_ROOT to the reference project's root (holding Support/nifti1.h)")
+    return os.path.join(root, "Support")
 
 PROGRAM = r'''
 #include <cmath>
@@ -85,7 +93,7 @@ def main():
         with open(src, "w") as f:
             f.write(PROGRAM)
         exe = os.path.join(d, "nifti_ref")
-        subprocess.run(["g++", "-std=c++17", "-O0", "-I" + REF_SUPPORT, src, "-o", exe], check=True)
+        subprocess.run(["g++", "-std=c++17", "-O0", "-I" + _ref_support(), src, "-o", exe], check=True)
         zin = os.path.join(d, "z.bin")
         z.tofile(zin)
         base = os.path.join(d, "img")

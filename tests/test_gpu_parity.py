@@ -144,8 +144,39 @@ def test_linearity_and_repeatability(pg):
     assert rel_l2(a1, a2) < 1e-6   # shared-memory atomics reorder sums only
 
 
+def _pcg_solves(oracle, p, y, niter, op32=None):
+    """The CPU solves a PCG image is compared with (quadratic penalty, W = 1, x0 = 0):
+    ref  the reference CPU path: its own compiled Gnufft kernels where built, the
+         restated composites, float inner products and steps (solve_pwls_pcg.hpp:48-167);
+    w64  an FP64 solve over the same float operator (FP64 vectors, inner products and
+         steps): the operator's FP32 rounding is its only FP32 step, which is the
+         arithmetic this library's solver follows (FP32 operator, FP64 scalars);
+    f64  the FP64 oracle (the reference's double instantiation)."""
+    ref_on = oracle.reference_available()
+    if ref_on:
+        oracle.use_reference(True)
+    try:
+        o32 = op32 if op32 is not None else oracle.build_problem_op(p, 0)
+        xr, nr = o32.pcg(y, "quad", p.nx, p.ny, p.nz, p.beta, niter=niter)
+        xw, nw = o32.pcg_fp64_solver(y, "quad", p.nx, p.ny, p.nz, p.beta, niter=niter)
+    finally:
+        if ref_on:
+            oracle.use_reference(False)
+    o64 = oracle.build_problem_op(p, 1)
+    x64, n64 = o64.pcg(np.asarray(y, np.complex128), "quad", p.nx, p.ny, p.nz, p.beta, niter=niter)
+    assert nr == nw == n64 == niter
+    return xr, xw, x64
+
+
 def test_config1_full_size_vs_oracle(pg, oracle):
-    """Config 1 (64x64, 4096 samples, SENSE with one coil): fwd, adj and 10 PCG iterations."""
+    """Config 1 (64x64, 4096 samples, SENSE with one coil): fwd, adj and PCG at 5 and 10 iterations.
+
+    On this problem CG amplifies the float operator's ~1e-6 rounding by up to 1e5 between
+    iterations 6 and 11: an FP64 solve over the reference's float operator is 5e-5 from
+    the FP64 oracle after 5 iterations and 4.5e-2 after 10, and so is every solve over a
+    float operator, the reference's own included.  At 5 iterations the GPU image is bounded
+    against all three CPU solves; at 10 against the reference CPU path at the measured
+    level (a 2x drift fails) and, against FP64, by the reference path's own distance."""
     from powergrid_b200 import synthetic as S
     p = S.config1()
     M, n = p.kx.size, p.nimg
@@ -159,22 +190,55 @@ def test_config1_full_size_vs_oracle(pg, oracle):
     xa = Sg / y64
     assert rel_l2(xa, o32.adjoint(y64)) <= OP_TOL
     R = pg.QuadPenalty(p.nx, p.ny, 1, p.beta)
-    # Config 1 has one sample per unknown and a white-noise image, so CG
-    # amplifies FP32 rounding: the reference CPU path itself drifts from FP64
-    # by ~3e-4 after 5 iterations and ~4e-2 after 10.  At 5 iterations every
-    # bound holds; at 10 the GPU path must stay within 1e-3 of the reference
-    # path and no further from FP64 than the reference path is.  (The GPU
-    # path, with FP64 inner products and step sizes, lands closer to FP64
-    # than the reference path does, so its distance to the reference is
-    # bounded by the reference's own FP32 drift plus the tolerance.)
+    bounds = {5: dict(ref=5e-4, w64=1e-4), 10: dict(ref=2.5e-4, w64=None)}
     for niter in (5, 10):
         x = pg.reconSolve(y64, Sg, R, niter=niter)
-        xr, _ = o32.pcg(y64, "quad", p.nx, p.ny, 1, p.beta, niter=niter)
-        x64, _ = o64.pcg(y64, "quad", p.nx, p.ny, 1, p.beta, niter=niter)
-        e, e64, r64 = rel_l2(x, xr), rel_l2(x, x64), rel_l2(xr, x64)
-        print(f"cfg1 pcg({niter}): {e:.2e} vs reference, {e64:.2e} vs fp64 (reference vs fp64 {r64:.2e})")
-        assert e <= PCG_TOL + r64
+        xr, xw, x64 = _pcg_solves(oracle, p, y64, niter)
+        e, ew, e64, r64 = rel_l2(x, xr), rel_l2(x, xw), rel_l2(x, x64), rel_l2(xr, x64)
+        print(f"cfg1 pcg({niter}): {e:.2e} vs reference, {ew:.2e} vs FP64 solve over the float operator, "
+              f"{e64:.2e} vs fp64 (reference vs fp64 {r64:.2e}, FP64 solve over the float operator vs fp64 "
+              f"{rel_l2(xw, x64):.2e})")
+        b = bounds[niter]
+        assert e <= b["ref"]
+        if b["w64"] is not None:
+            assert ew <= b["w64"] and e64 <= PCG_TOL
         assert e64 <= max(PCG_TOL, 1.1 * r64)
+
+
+def test_config2_pcg_full_size(pg, oracle):
+    """Config 2's timed reconstruction at full size (128x128, L=8, 4 coils, 131072 samples
+    per coil, QuadPenalty 1e-3): the PCG image after 3 and after 20 iterations against the
+    reference CPU path, an FP64 solve over the reference's float operator and the FP64
+    oracle.  At 3 iterations the image matches the FP64 solves within the PCG tolerance;
+    the reference path's float inner products (sums of 524288 products accumulated in
+    float) already put it 7e-4 from them, so the bound against it is that distance plus
+    the tolerance.  By 20 iterations CG has amplified operator rounding into ~1e-1
+    differences between any two solves whose operators round differently; the 20-iteration
+    errors are printed and bounded at twice the measured level."""
+    from powergrid_b200 import synthetic as S
+    p = S.config2()
+    M, n = p.kx.size, p.nimg
+    G = pg.Gnufft(M, 2.0, p.nx, p.ny, 1, p.kx, p.ky, p.kz)
+    A = pg.TimeSegmentation(G, p.fm, p.t, M, n, p.L, 1, 1)
+    Sg = pg.SENSE(A, p.smap, M, n, p.nc)
+    R = pg.QuadPenalty(p.nx, p.ny, 1, p.beta)
+    oracle.set_threads(os.cpu_count() or 1)
+    try:
+        y = oracle.build_problem_op(p, 0).forward(p.x_true)
+        for niter in (3, 20):
+            x = pg.reconSolve(y, Sg, R, niter=niter)
+            xr, xw, x64 = _pcg_solves(oracle, p, y, niter)
+            e, ew, e64, rw = rel_l2(x, xr), rel_l2(x, xw), rel_l2(x, x64), rel_l2(xr, xw)
+            print(f"cfg2 pcg({niter}): {e:.2e} vs reference, {ew:.2e} vs FP64 solve over the float operator, "
+                  f"{e64:.2e} vs fp64 (reference vs FP64 solve over the float operator {rw:.2e}, "
+                  f"reference vs fp64 {rel_l2(xr, x64):.2e})")
+            if niter == 3:
+                assert ew <= PCG_TOL and e64 <= PCG_TOL
+                assert e <= rw + PCG_TOL
+            else:
+                assert e <= 0.3 and ew <= 0.3 and e64 <= 0.3
+    finally:
+        oracle.set_threads(1)
 
 
 def test_config2_operator_full_size_vs_oracle(pg, oracle):
@@ -198,7 +262,11 @@ def test_config2_operator_full_size_vs_oracle(pg, oracle):
 
 
 def test_gdft_config3_sampled_outputs(pg, oracle):
-    """Config 3 at full size (64x64x32, 131072 samples, 8 coils): sampled outputs vs FP64 DFT."""
+    """Config 3 at full size (SENSE<Gdft>, 64x64x32, 131072 samples, 8 coils).  Forward:
+    48 sampled rows of every coil; adjoint (iftCpu, ftCpu.cpp:150-215, summed over the
+    coils with conj(S) as SENSE.cpp:84-96): 48 sampled voxels.  Both against the FP64 DFT
+    and against the reference's float formula (sinf/cosf of a float phase) on the same
+    rows and voxels."""
     from powergrid_b200 import synthetic as S
     p = S.config3()
     M, n = p.kx.size, p.nimg
@@ -206,17 +274,84 @@ def test_gdft_config3_sampled_outputs(pg, oracle):
     G = pg.Gdft(M, n, p.kx, p.ky, p.kz, ix, iy, iz, p.fm, p.t)
     Sg = pg.SENSE(G, p.smap, M, n, p.nc)
     y = Sg * p.x_true
+    xa = Sg / y
     rng = np.random.default_rng(0)
-    idx = np.sort(rng.choice(M, 48, replace=False))
-    # FP64 DFT of coil 0 and 5 at the sampled rows
+    rows = np.sort(rng.choice(M, 48, replace=False))
+    vox = np.sort(rng.choice(n, 48, replace=False))
     sm = p.smap.reshape(p.nc, n)
-    for c in (0, 5):
-        sub = oracle.gdft(2, p.kx[idx], p.ky[idx], p.kz[idx], ix, iy, iz, p.fm, p.t[idx])
-        ref = sub.forward((sm[c] * p.x_true).astype(np.complex128))
-        got = y[c * M + idx]
-        e = rel_l2(got, ref)
-        print(f"cfg3 coil {c}: sampled fwd vs fp64 {e:.2e}")
-        assert e <= OP_TOL
+    oracle.set_threads(os.cpu_count() or 1)
+    try:
+        fwd64 = oracle.gdft(2, p.kx[rows], p.ky[rows], p.kz[rows], ix, iy, iz, p.fm, p.t[rows])
+        fwd32 = oracle.gdft(0, p.kx[rows], p.ky[rows], p.kz[rows], ix, iy, iz, p.fm, p.t[rows])
+        adj64 = oracle.gdft(2, p.kx, p.ky, p.kz, ix[vox], iy[vox], iz[vox], p.fm[vox], p.t)
+        adj32 = oracle.gdft(0, p.kx, p.ky, p.kz, ix[vox], iy[vox], iz[vox], p.fm[vox], p.t)
+        ref64 = np.zeros(vox.size, np.complex128)
+        ref32 = np.zeros(vox.size, np.complex128)
+        for c in range(p.nc):
+            got = y[c * M + rows]
+            e64 = rel_l2(got, fwd64.forward((sm[c] * p.x_true).astype(np.complex128)))
+            e32 = rel_l2(got, fwd32.forward((sm[c] * p.x_true).astype(np.complex64)))
+            print(f"cfg3 coil {c}: sampled fwd {e64:.2e} vs fp64, {e32:.2e} vs the reference formula")
+            assert e64 <= OP_TOL and e32 <= OP_TOL
+            yc = y[c * M:(c + 1) * M]
+            ref64 += np.conj(sm[c, vox]).astype(np.complex128) * adj64.adjoint(yc.astype(np.complex128))
+            ref32 += np.conj(sm[c, vox]).astype(np.complex128) * adj32.adjoint(yc)
+    finally:
+        oracle.set_threads(1)
+    ea64, ea32 = rel_l2(xa[vox], ref64), rel_l2(xa[vox], ref32)
+    print(f"cfg3 sampled adjoint (8 coils): {ea64:.2e} vs fp64, {ea32:.2e} vs the reference formula "
+          f"(reference formula vs fp64 {rel_l2(ref32, ref64):.2e})")
+    assert ea64 <= OP_TOL and ea32 <= OP_TOL
+
+
+def test_config5_full_grid_vs_oracle(pg, oracle):
+    """Config 5's operator at its full grid: pcSenseTimeSeg 128x128x64, L = 12 Hanning
+    segments, +-200 Hz, per-shot phase maps, with 2 shots of 32768 samples and 1 coil
+    (the full 16 shots x 32 coils would keep the CPU path busy for hours).  Forward and
+    adjoint against the reference CPU path and FP64; the TVPenalty (delta 0.1) solve at
+    3 iterations against the reference CPU path and an FP64 solve over the float operator,
+    and at 30 iterations, the configuration's count, against the reference CPU path.
+    Data are scaled so that the first line-search denominator is 1 (the solver's 1e25
+    guard, solve_pwls_pcg.hpp:137, is scale-dependent)."""
+    from powergrid_b200 import synthetic as S
+    p = S.config5(shots=2, nc=1, per=512)
+    op = pg.pcSenseTimeSeg(p.kx, p.ky, p.kz, p.nx, p.ny, p.nz, p.nc, p.t, p.L, 1, p.smap, p.fm, p.pmap)
+    R = pg.TVPenalty(p.nx, p.ny, p.nz, p.beta, p.delta)
+    oracle.set_threads(os.cpu_count() or 1)
+    ref_on = oracle.reference_available()
+    try:
+        if ref_on:
+            oracle.use_reference(True)
+        o32 = oracle.build_problem_op(p, 0)
+        if ref_on:
+            oracle.use_reference(False)
+        o64 = oracle.build_problem_op(p, 1)
+        y = op * p.x_true
+        yr = o32.forward(p.x_true)
+        ef, ef64 = rel_l2(y, yr), rel_l2(y, o64.forward(p.x_true.astype(np.complex128)))
+        xa = op / yr
+        xar = o32.adjoint(yr)
+        ea, ea64 = rel_l2(xa, xar), rel_l2(xa, o64.adjoint(yr.astype(np.complex128)))
+        print(f"cfg5 grid, 2 shots x 1 coil, L=12: fwd {ef:.2e} (fp64 {ef64:.2e}), adj {ea:.2e} (fp64 {ea64:.2e})")
+        assert ef <= OP_TOL and ea <= OP_TOL
+        yr = (yr / np.linalg.norm((op * (op / yr)).astype(np.complex128))).astype(np.complex64)
+        for niter in (3, 30):
+            x, it = pg.solve_pwls_pcg(None, op, None, yr, R, niter)
+            xr, nr = o32.pcg(yr, "tv", p.nx, p.ny, p.nz, p.beta, delta=p.delta, niter=niter)
+            e = rel_l2(x, xr)
+            if niter == 3:
+                xw, nw = o32.pcg_fp64_solver(yr, "tv", p.nx, p.ny, p.nz, p.beta, delta=p.delta, niter=niter)
+                ew, rw = rel_l2(x, xw), rel_l2(xr, xw)
+                print(f"cfg5 TV pcg(3): {e:.2e} vs reference, {ew:.2e} vs FP64 solve over the float operator "
+                      f"(reference vs it {rw:.2e})")
+                assert it == nr == nw == 3 and ew <= PCG_TOL and e <= rw + PCG_TOL
+            else:
+                print(f"cfg5 TV pcg(30): {e:.2e} vs reference, iterations {it} / {nr}")
+                assert it == nr and e <= 0.3
+    finally:
+        if ref_on:
+            oracle.use_reference(False)
+        oracle.set_threads(1)
 
 
 def test_invalid_inputs_are_rejected(pg):
@@ -392,3 +527,28 @@ def test_pcg_checkpoint_resume(pg, name):
         pg.QuadPenalty(c["nx"], c["ny"], c["nz"], 1e-3)
     with pytest.raises(PGError, match="saved for"):
         pg.pcg_resume(_gpu_op(pg, name, c), state, None, y, other, 2)
+
+
+def test_pcg_weighted_resume_then_plain_solve(pg):
+    """A resume with data weights W leaves the weights it used in the solver
+    state; a later plain solve (W = ones) on the same operator must not reuse
+    them: it equals a plain solve on a fresh operator.  A state saved for one
+    penalty strength is refused for another."""
+    from powergrid_b200._lib import PGError
+    c = _case("pcg2d")
+    R = pg.QuadPenalty(c["nx"], c["ny"], c["nz"], c["beta"])
+    y = c["y_f32"]
+    A = _gpu_op(pg, "pcg2d", c)
+    pg.solve_pwls_pcg(None, A, None, y, R, 2)
+    state = pg.pcg_state_save(A)
+    W = np.full(A.n_data, 0.5, np.float32)
+    W[::3] = 2.0
+    pg.pcg_resume(A, state, W, y, R, 2)
+    x_after, it = pg.solve_pwls_pcg(None, A, None, y, R, 3)
+    x_fresh, it_f = pg.solve_pwls_pcg(None, _gpu_op(pg, "pcg2d", c), None, y, R, 3)
+    e = rel_l2(x_after, x_fresh)
+    print(f"plain solve after a weighted resume vs fresh: {e:.2e}")
+    assert it == it_f == 3 and e <= 1e-5
+    R2 = pg.QuadPenalty(c["nx"], c["ny"], c["nz"], 2.0 * c["beta"])
+    with pytest.raises(PGError, match="saved for penalty"):
+        pg.pcg_resume(_gpu_op(pg, "pcg2d", c), state, None, y, R2, 1)

@@ -5,7 +5,10 @@ avoid cudaMalloc's implicit synchronisation cannot use an entry point that
 allocates; this one keeps its scratch in a fixed device array.  The test
 calls it through the C ABI twice in a row on caller-owned device buffers and
 checks each result against the existing Gdft operator (pg_op_forward_device)
-within the operator tolerance.  This file is collected last on purpose.
+and against the oracle's restatement of the reference's float ftCpu, within
+the operator tolerance.  During those calls the library's allocation hook is
+armed to fail the next device allocation, so a call that allocated would
+return PG_OUT_OF_MEMORY.  This file is collected last on purpose.
 """
 import ctypes as C
 
@@ -22,7 +25,7 @@ def _dev(a, torch, dev):
 
 
 @pytest.mark.gpu
-def test_noalloc_gdft_matches_operator_twice(pg):
+def test_noalloc_gdft_matches_operator_twice(pg, oracle):
     import torch
 
     from powergrid_b200 import _lib
@@ -36,17 +39,27 @@ def test_noalloc_gdft_matches_operator_twice(pg):
     nk, ni = kx.size, ix.size
     G = pg.Gdft(nk, ni, kx, ky, kz, ix, iy, iz, fm, t)
     L = _lib.load()
+    R = oracle.gdft(0, kx, ky, kz, ix, iy, iz, fm, t)
     inputs = [_dev(v, torch, dev) for v in (kx, ky, kz, ix, iy, iz, fm, t)]
-    for seed in (31, 32):                        # two calls in a row, different images
-        x = _dev(S.image(S.Rng(seed), ni), torch, dev)
-        y_ref = G.forward(x)
-        y = torch.empty(nk, dtype=torch.complex64, device=dev)
-        stream = torch.cuda.current_stream()
-        check(L.pg_gdft_forward_noalloc(nk, ni, *[P(v.data_ptr()) for v in inputs], P(x.data_ptr()),
-                                        P(y.data_ptr()), P(stream.cuda_stream)))
-        torch.cuda.synchronize()
-        e = rel_l2(y.cpu().numpy(), y_ref.cpu().numpy())
-        assert e <= OP_TOL, e
+    stream = torch.cuda.current_stream()
+    y = torch.empty(nk, dtype=torch.complex64, device=dev)
+    images = [S.image(S.Rng(seed), ni) for seed in (31, 32)]
+    xs = [_dev(v, torch, dev) for v in images]
+    refs = [G.forward(x).cpu().numpy() for x in xs]
+    torch.cuda.synchronize()
+    try:
+        for x, img, y_op in zip(xs, images, refs):    # two calls in a row, different images
+            L.pg_debug_fail_allocation_after(1)       # any library allocation now fails
+            check(L.pg_gdft_forward_noalloc(nk, ni, *[P(v.data_ptr()) for v in inputs], P(x.data_ptr()),
+                                            P(y.data_ptr()), P(stream.cuda_stream)))
+            L.pg_debug_fail_allocation_after(0)
+            torch.cuda.synchronize()
+            got = y.cpu().numpy()
+            e_op, e_or = rel_l2(got, y_op), rel_l2(got, R.forward(img))
+            print(f"no-alloc Gdft: {e_op:.2e} vs the Gdft operator, {e_or:.2e} vs the oracle")
+            assert e_op <= OP_TOL and e_or <= OP_TOL, (e_op, e_or)
+    finally:
+        L.pg_debug_fail_allocation_after(0)
 
 
 @pytest.mark.gpu
