@@ -11,8 +11,9 @@ W = 1, x0 = 0).  Seeded synthetic inputs stand in for ISMRMRD data.
   e2e        the same metric through the C ABI's host-buffer entry point
              pg_pcg_solve (H2D of the coil data and D2H of the image inside
              the timed region)
-  roofline   the adjoint gridding kernel (k_spread), timed by a CUDA event
-             pair around its launch in the last PCG iteration of every timed
+  roofline   the adjoint gridding (the grids' clearing and the spread
+             kernel, as the reference's gridding_adjoint), timed by a CUDA
+             event pair around it in the last PCG iteration of every timed
              step (an instrumented copy of the iteration graph; the other
              iterations replay the plain one), against the measured HBM
              bandwidth; the other stages are timed on extra steps
@@ -255,11 +256,11 @@ def run_gpu_arm(args):
         check(L.pg_pcg_solve_device(Sg.handle, None, None, P(y.data_ptr()), C.byref(pen), NITER, P(x.data_ptr()),
                                     P(iters.data_ptr()), sp))
 
-    # Each timed step carries one CUDA event pair, around the spread kernel
-    # (the roofline kernel) of its last PCG iteration; the other stage times
+    # Each timed step carries one CUDA event pair, around the adjoint gridding
+    # (the roofline stage) of its last PCG iteration; the other stage times
     # come from extra profiled steps after the timed region.
     check(L.pg_profile_enable(1))
-    check(L.pg_profile_only(b"spread"))
+    check(L.pg_profile_only(b"adjoint_gridding"))
     sampler = ClockSampler(local)
     sampler.__enter__()
     for _ in range(max(3, args.warmup)):
@@ -284,13 +285,13 @@ def run_gpu_arm(args):
         stream.synchronize()
         step_ms.append(ev[i][0].elapsed_time(ev[i][1]))
         ms = C.c_float()
-        if L.pg_profile_stage_ms(b"spread", C.byref(ms)) == 0:
+        if L.pg_profile_stage_ms(b"adjoint_gridding", C.byref(ms)) == 0:
             spread_ms.append(ms.value)
     torch.cuda.synchronize()
     launches = _lib.launches() - launches0
     sampler.__exit__(None, None, None)
 
-    stages = ["pre", "fft_fwd", "gather", "prep", "spread", "fft_adj", "post"]
+    stages = ["pre", "fft_fwd", "gather", "adjoint_gridding", "prep", "spread", "fft_adj", "post"]
     stage_ms = {k: [] for k in stages}
     check(L.pg_profile_only(None))
     for i in range(4):
@@ -331,8 +332,8 @@ def run_gpu_arm(args):
     e2e_s = max_over_ranks(e2e_s, device=dev)
     e2e = job_rate(e2e_steps * NITER, e2e_s, ws)
 
-    # roofline of the adjoint gridding kernel: algorithmic bytes per launch
-    # = coils * (M * (4*d + 8 + 4) + L * G * 8), d = 2, G = 256^2
+    # roofline of the adjoint gridding (clearing + spread): algorithmic bytes
+    # per application = coils * (M * (4*d + 8 + 4) + L * G * 8), d = 2, G = 256^2
     G2 = (2 * p.nx) * (2 * p.ny)
     alg_bytes = p.nc * (M * (4 * 2 + 8 + 4) + p.L * G2 * 8)
     peak, peak_kind = _peaks()
@@ -368,7 +369,8 @@ def run_gpu_arm(args):
                         "d2h_bytes_per_step": int(n * 8), "l2": "flushed before each step, outside the timed call",
                         "timer": "host clock around the synchronous pg_pcg_solve call (copies included)"},
                 "stages_ms_per_launch": {k: (statistics.mean(v) if v else None) for k, v in stage_ms.items()},
-                "roofline": {"kernel": "k_spread<2> (adjoint gridding, TS-fused, 4 coils x 8 segments)",
+                "roofline": {"kernel": "adjoint gridding: grid clearing + k_spread2d (TS-fused, 4 coils x 8 "
+                                       "segments), one event pair around both",
                              "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                              "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_spread,

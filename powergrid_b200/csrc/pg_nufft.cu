@@ -238,6 +238,10 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // Padded extent along y (the fastest axis) such that 4 x-rows of 8 y-taps
@@ -633,6 +637,229 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
         }
       }
   }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 2-D adjoint spread with the adjoint preparation folded in, for segment
+// windows of KK <= 2 (Hanning time segmentation, or none).  Persistent like
+// k_spread: blocks take (subproblem, coil chunk of CC) items from the device
+// work queue, largest first.  Per item:
+//  1. staging: tap weights and window starts by cp.async; the values
+//     v = conj(AA(s, l0 + j)) * y_c[perm s] read straight from the data
+//     vector (no intermediate array), with their largest |re| or |im|
+//     reduced in registers, then per warp;
+//  2. the bounding box of the item's windows, and one power-of-two scale
+//     2^e for all of the item's planes, chosen as in k_spread so that every
+//     single contribution w * v * 2^e is below 2^22 and every cell sum below
+//     2^30; it multiplies the y weight of each sample (exact);
+//  3. the spread: each warp walks a contiguous run of samples, lane = (y tap,
+//     x-tap pair); runs of equal window start are summed in registers with
+//     paired fp32 fma (two planes per 16-byte value load) and rounded once to
+//     the integer grid, one int32 shared atomic per tap, plane and run;
+//  4. the flush: the bounding box only, two cells per 16-byte vector atomic;
+//     each cell is zeroed as it is read, so the tile is zero for the next item.
+// The grids are cleared before the launch (a memset).  Integer tile sums do
+// not depend on the order of the atomics; the flush into the grid is a float
+// vector atomic per cell pair.
+// Shared memory: tile planes [NP][re|im][PX][PY] int32, weights [smax][16]
+// f32, values [smax][NP2] float4 (two planes each), window starts [smax] u32.
+// ---------------------------------------------------------------------------
+template <int T, int CC, int KK>
+__global__ void __launch_bounds__(256) k_spread2d(NufftGeom g, TileShape t, const int4* __restrict__ sub,
+                                                  const uint2* __restrict__ start, const float* __restrict__ wxy,
+                                                  const uint32_t* __restrict__ perm, const float2* __restrict__ aa,
+                                                  const float2* __restrict__ y, uint64_t dstride, int nb, int L,
+                                                  int smax, float wmax, float2* __restrict__ grids,
+                                                  unsigned* __restrict__ queue, int nchunks, int nitems) {
+  using TG = TileGeo<2, T>;
+  constexpr int CELLS = TG::CELLS, PY = TG::PY;
+  constexpr int NP = CC * KK;          // planes per item
+  constexpr int NP2 = (NP + 1) / 2;    // 16-byte value slots per sample
+  static_assert(CC == 1 || CC == 2 || CC == 4, "coils per item: 1, 2 or 4");
+  static_assert(PY % 2 == 0 && CELLS % 2 == 0, "cell pairs");
+  extern __shared__ __align__(16) int smi[];
+  __shared__ unsigned vmax;
+  __shared__ int box[4];               // window starts: min x, max x, min y, max y (tile coordinates)
+  __shared__ int s_item;
+  const int tid = threadIdx.x;
+  int* tile = smi;
+  float* sw = reinterpret_cast<float*>(smi + NP * 2 * CELLS);
+  float4* sv = reinterpret_cast<float4*>(sw + (size_t)smax * 16);
+  float2* sv2 = reinterpret_cast<float2*>(sv);
+  uint32_t* sst = reinterpret_cast<uint32_t*>(sv + (size_t)smax * NP2);
+  for (int q = tid; q < NP * 2 * CELLS / 4; q += blockDim.x) reinterpret_cast<int4*>(tile)[q] = make_int4(0, 0, 0, 0);
+  for (;;) {
+    __syncthreads();                   // the previous item's shared memory is no longer in use
+    if (tid == 0) {
+      int it = (int)atomicAdd(&queue[0], 1u);
+      if (it >= nitems) {
+        it = -1;
+        if (atomicAdd(&queue[1], 1u) == gridDim.x - 1) { queue[0] = 0u; queue[1] = 0u; }
+      }
+      s_item = it;
+      vmax = 0u;
+      box[0] = box[2] = 0x7fffffff;
+      box[1] = box[3] = -1;
+    }
+    __syncthreads();
+    const int item = s_item;
+    if (item < 0) break;
+    const int4 sp = sub[item / nchunks];
+    const int cfirst = (item % nchunks) * CC;
+    const int ncl = min(CC, nb - cfirst);
+    const int tile_i = sp.x, lseg = sp.y, first = sp.z, count = sp.w;
+    const int x0 = (tile_i / t.nty) * T, y0 = (tile_i % t.nty) * T;
+
+    // 1. staging
+    for (int q = tid; q < count * 4; q += blockDim.x) {
+      const int i = q >> 2, a = q & 3;
+      cp_async16(reinterpret_cast<float4*>(sw + i * 16) + a,
+                 reinterpret_cast<const float4*>(wxy + (uint64_t)(first + i) * 16) + a);
+    }
+    for (int i = tid; i < count; i += blockDim.x) cp_async4(&sst[i], &start[first + i].x);
+    {
+      const int c = tid % CC;
+      float m = 0.f;
+      for (int i = tid / CC; i < count; i += blockDim.x / CC) {
+        const uint64_t s = (uint64_t)(first + i);
+        float2 d = make_float2(0.f, 0.f);
+        if (c < ncl) d = y[(uint64_t)(cfirst + c) * dstride + perm[s]];
+#pragma unroll
+        for (int j = 0; j < KK; ++j) {
+          const float2 v = aa ? cmul(cconj(aa[s * KK + j]), d) : d;
+          m = fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y)));
+          sv2[(size_t)i * 2 * NP2 + c * KK + j] = v;
+        }
+      }
+      const unsigned u = __reduce_max_sync(0xffffffffu, __float_as_uint(m));
+      if ((tid & 31) == 0 && u) atomicMax(&vmax, u);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+
+    // 2. bounding box of the windows and the item's scale
+    {
+      int xlo = 0x7fffffff, xhi = -1, ylo = 0x7fffffff, yhi = -1;
+      for (int i = tid; i < count; i += blockDim.x) {
+        const uint32_t st = sst[i];
+        const int ox = (int)(st & 0xffff) - x0, oy = (int)(st >> 16) - y0;
+        xlo = min(xlo, ox); xhi = max(xhi, ox);
+        ylo = min(ylo, oy); yhi = max(yhi, oy);
+      }
+      xlo = __reduce_min_sync(0xffffffffu, xlo);
+      xhi = __reduce_max_sync(0xffffffffu, xhi);
+      ylo = __reduce_min_sync(0xffffffffu, ylo);
+      yhi = __reduce_max_sync(0xffffffffu, yhi);
+      if ((tid & 31) == 0 && xhi >= 0) {
+        atomicMin(&box[0], xlo); atomicMax(&box[1], xhi);
+        atomicMin(&box[2], ylo); atomicMax(&box[3], yhi);
+      }
+    }
+    __syncthreads();
+    float sc, inv;
+    {
+      int extra = 0;
+      while (count > (256 << extra)) ++extra;
+      const float B = __uint_as_float(vmax) * wmax * 1.0001f;
+      int e = 0;
+      if (B > 0.f) {
+        frexpf(B, &e);                 // B < 2^e
+        e = 22 - e - extra;            // B * 2^e' < 2^(22 - extra)
+      }
+      sc = ldexpf(1.f, e);
+      inv = ldexpf(1.f, -e);
+    }
+
+    // 3. spread
+    {
+      const int warp = tid >> 5, lane = tid & 31;
+      constexpr int NW = 8;
+      const int dy = lane & 7, dx = lane >> 3;
+      const int per = (count + NW - 1) / NW;
+      const int i0 = warp * per, i1 = min(count, i0 + per);
+      float2 a0[NP], a1[NP];           // (re, im) at tap dx and dx + 4
+      uint32_t prev = 0xffffffffu;
+      int* b = tile;
+      bool open = false;
+      auto flush_run = [&]() {
+#pragma unroll
+        for (int pl = 0; pl < NP; ++pl) {
+          if (pl / KK >= ncl) break;
+          atomicAdd(b + (2 * pl) * CELLS, __float2int_rn(a0[pl].x));
+          atomicAdd(b + (2 * pl + 1) * CELLS, __float2int_rn(a0[pl].y));
+          atomicAdd(b + (2 * pl) * CELLS + 4 * PY, __float2int_rn(a1[pl].x));
+          atomicAdd(b + (2 * pl + 1) * CELLS + 4 * PY, __float2int_rn(a1[pl].y));
+        }
+      };
+      for (int i = i0; i < i1; ++i) {
+        const uint32_t st = sst[i];
+        if (st != prev) {              // uniform across the warp
+          if (open) flush_run();
+          open = true;
+          prev = st;
+          const int ox = (int)(st & 0xffff) - x0, oy = (int)(st >> 16) - y0;
+          b = tile + (ox + dx) * PY + oy + dy;
+#pragma unroll
+          for (int pl = 0; pl < NP; ++pl) a0[pl] = a1[pl] = make_float2(0.f, 0.f);
+        }
+        const float* w = sw + i * 16;
+        const float wyv = w[8 + dy] * sc;
+        const float w0 = w[dx] * wyv, w1 = w[dx + 4] * wyv;
+        const float2 w0v = make_float2(w0, w0), w1v = make_float2(w1, w1);
+        if constexpr (NP % 2 == 0) {
+          const float4* vi = sv + (size_t)i * NP2;
+#pragma unroll
+          for (int q = 0; q < NP2; ++q) {
+            const float4 u = vi[q];
+            const float2 ua = make_float2(u.x, u.y), ub = make_float2(u.z, u.w);
+            a0[2 * q] = __ffma2_rn(w0v, ua, a0[2 * q]);
+            a1[2 * q] = __ffma2_rn(w1v, ua, a1[2 * q]);
+            a0[2 * q + 1] = __ffma2_rn(w0v, ub, a0[2 * q + 1]);
+            a1[2 * q + 1] = __ffma2_rn(w1v, ub, a1[2 * q + 1]);
+          }
+        } else {
+          const float2* vi = sv2 + (size_t)i * 2 * NP2;
+#pragma unroll
+          for (int pl = 0; pl < NP; ++pl) {
+            const float2 u = vi[pl];
+            a0[pl] = __ffma2_rn(w0v, u, a0[pl]);
+            a1[pl] = __ffma2_rn(w1v, u, a1[pl]);
+          }
+        }
+      }
+      if (open) flush_run();
+    }
+    __syncthreads();
+
+    // 4. flush the bounding box, two cells (y, y + 1) per vector atomic
+    {
+      const int bx0 = box[0], by0 = box[2] & ~1;
+      const int nxb = box[1] + 8 - bx0, nyp = (box[3] + 8 - by0 + 1) >> 1;
+      const uint64_t G = g.ngrid();
+      for (int q = tid; q < nxb * nyp; q += blockDim.x) {
+        const int px = bx0 + q / nyp, py = by0 + 2 * (q % nyp);
+        const int cell = px * PY + py;
+        const int gx = x0 + px, gy = y0 + py;
+        const bool inside = gx < g.Gx && gy < g.Gy;
+        const uint64_t idx = (uint64_t)gy + (uint64_t)g.Gy * (uint64_t)gx;
+#pragma unroll
+        for (int pl = 0; pl < NP; ++pl) {
+          const int c = pl / KK, j = pl % KK;
+          if (c >= ncl) break;
+          int2* pr = reinterpret_cast<int2*>(tile + (2 * pl) * CELLS + cell);
+          int2* pi = reinterpret_cast<int2*>(tile + (2 * pl + 1) * CELLS + cell);
+          const int2 re = *pr, im = *pi;
+          if ((re.x | re.y | im.x | im.y) != 0) {
+            *pr = make_int2(0, 0);
+            *pi = make_int2(0, 0);
+            if (inside)
+              atomicAdd(reinterpret_cast<float4*>(grids + ((uint64_t)(cfirst + c) * L + lseg + j) * G + idx),
+                        make_float4((float)re.x * inv, (float)im.x * inv, (float)re.y * inv, (float)im.y * inv));
+          }
+        }
+      }
+    }
   }
 }
 
@@ -1173,6 +1400,42 @@ static pg_status launch_spread(NufftPlan* p, const Binning* bin, const SpreadArg
   return spread_launch_t<2, 16>(p, bin, a, s);
 }
 
+// Shared memory of k_spread2d: tile planes, staged weights, values and starts.
+static size_t spread2d_smem(int T, int np, int smax) {
+  const int px = T + 8, py = padded_y(T);
+  return (size_t)np * 2 * px * py * sizeof(int) +
+         (size_t)smax * (16 * sizeof(float) + (size_t)((np + 1) / 2) * sizeof(float4) + sizeof(uint32_t));
+}
+
+template <int T, int CC, int KK>
+static pg_status spread2d_launch(NufftPlan* p, const Binning* bin, const float2* aa, const float2* y,
+                                 uint64_t dstride, int nb, float wmax, cudaStream_t s) {
+  const size_t smem = spread2d_smem(T, CC * KK, bin->submax);
+  PG_CUDA(cudaFuncSetAttribute(k_spread2d<T, CC, KK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int nchunks = (nb + CC - 1) / CC;
+  const int nitems = bin->nsub * nchunks;
+  PG_TRY(ensure_queue(p, s));
+  const int blocks = persistent_blocks((const void*)k_spread2d<T, CC, KK>, smem, nitems);
+  PG_LAUNCH((k_spread2d<T, CC, KK>), blocks, 256, smem, s, p->g, bin->tile, bin->subprob.p, bin->start.p, bin->wxy.p,
+            bin->perm.p, aa, y, dstride, nb, bin->L, bin->submax, wmax, p->work->grids.p, p->work->queue.p, nchunks,
+            nitems);
+  return PG_OK;
+}
+
+template <int T>
+static pg_status spread2d_launch_t(NufftPlan* p, const Binning* bin, int cc, const float2* aa, const float2* y,
+                                   uint64_t dstride, int nb, float wmax, cudaStream_t s) {
+  switch (cc * 10 + bin->K) {
+    case 11: return spread2d_launch<T, 1, 1>(p, bin, aa, y, dstride, nb, wmax, s);
+    case 21: return spread2d_launch<T, 2, 1>(p, bin, aa, y, dstride, nb, wmax, s);
+    case 41: return spread2d_launch<T, 4, 1>(p, bin, aa, y, dstride, nb, wmax, s);
+    case 12: return spread2d_launch<T, 1, 2>(p, bin, aa, y, dstride, nb, wmax, s);
+    case 22: return spread2d_launch<T, 2, 2>(p, bin, aa, y, dstride, nb, wmax, s);
+    case 42: return spread2d_launch<T, 4, 2>(p, bin, aa, y, dstride, nb, wmax, s);
+  }
+  return set_error(PG_INVALID_ARG, "adjoint: no folded spread for %d coils x K=%d", cc, bin->K);
+}
+
 // Post-kernel launch: CP coil lanes x LP segment lanes per pixel (powers of
 // two, at most 8 lanes).
 template <int CP, int LP>
@@ -1256,10 +1519,20 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
     return plane_bytes * K * cc + (size_t)smax * (spread_wrow(g.dim) * sizeof(float) + sizeof(uint2) +
                                                   (size_t)K * cc * sizeof(float2));
   };
+  // 2-D with K <= 2 (Hanning segments or none): the folded spread reads the
+  // data vector itself; otherwise k_adjoint_prep forms the values first.
+  const bool folded = (g.dim == 2 && K <= 2 && (t.TX == 16 || t.TX == 32));
   int Cc = std::max(1, std::min(4, p->tune.spread_cc));
-  while (Cc > 1 && (Cc * K > 16 || smem_for(Cc) > smem_limit)) --Cc;
-  if (K > 16 || smem_for(1) > smem_limit)
-    return set_error(PG_INVALID_ARG, "adjoint: segment window K=%d too wide for shared memory", K);
+  if (folded) {
+    Cc = Cc >= 4 ? 4 : Cc >= 2 ? 2 : 1;
+    while (Cc > 1 && (Cc >= 2 * std::min(Cb, b.C) || spread2d_smem(t.TX, Cc * K, smax) > smem_limit)) Cc >>= 1;
+    if (spread2d_smem(t.TX, K, smax) > smem_limit)
+      return set_error(PG_INVALID_ARG, "adjoint: tile of %d cells too large for shared memory", t.TX);
+  } else {
+    while (Cc > 1 && (Cc * K > 16 || smem_for(Cc) > smem_limit)) --Cc;
+    if (K > 16 || smem_for(1) > smem_limit)
+      return set_error(PG_INVALID_ARG, "adjoint: segment window K=%d too wide for shared memory", K);
+  }
   const float w1 = p->lut_max;
   const float wmax = (g.dim == 2) ? w1 * w1 : w1 * w1 * w1;
   for (int c0 = 0; c0 < b.C; c0 += Cb) {
@@ -1269,6 +1542,21 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
     PG_TRY(ensure_workspace(p, B, p->own_fft ? nullptr : &h, s));
     const float2* yc = y + (uint64_t)c0 * b.data_stride;
     const float2* aa = (L > 1 || bin->aa.p) ? bin->aa.p : nullptr;
+    {
+    // the adjoint gridding as the reference's gridding_adjoint (gridding.cpp:31-214):
+    // the grids' clearing and the spread, timed together
+    ProfScope pag("adjoint_gridding", s);
+    if (folded) {
+      {
+        ProfScope ps("prep", s);
+        PG_CUDA(cudaMemsetAsync(p->work->grids.p, 0, (size_t)B * G * sizeof(float2), s));
+      }
+      if (bin->nsub > 0) {
+        ProfScope ps("spread", s);
+        if (t.TX == 32) PG_TRY(spread2d_launch_t<32>(p, bin, Cc, aa, yc, b.data_stride, nb, wmax, s));
+        else PG_TRY(spread2d_launch_t<16>(p, bin, Cc, aa, yc, b.data_stride, nb, wmax, s));
+      }
+    } else {
     PG_TRY(grow(p->work->vs, (uint64_t)nb * bin->M * K, s));
     {
       ProfScope ps("prep", s);
@@ -1289,6 +1577,8 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
         SpreadArgs r{p->work->vs.p, full * cc, rest, 1, wmax, smem_for(rest)};
         PG_TRY(launch_spread(p, bin, r, s));
       }
+    }
+    }
     }
     const int acc = (b.accumulate || c0 > 0) ? 1 : 0;
     if (p->own_fft) {

@@ -213,8 +213,11 @@ def test_config2_pcg_full_size(pg, oracle):
     the reference path's float inner products (sums of 524288 products accumulated in
     float) already put it 7e-4 from them, so the bound against it is that distance plus
     the tolerance.  By 20 iterations CG has amplified operator rounding into ~1e-1
-    differences between any two solves whose operators round differently; the 20-iteration
-    errors are printed and bounded at twice the measured level."""
+    differences between any two solves whose operators round differently (the reference
+    path is 1.4e-1 from the FP64 oracle and 5.5e-2 from the FP64 solve over its own float
+    operator); the GPU image must be no farther from the FP64 solves than the reference
+    path's image is (measured: 7.1e-2 from FP64, 3.0e-2 from the FP64 solve over the float
+    operator, 8.4e-2 from the reference path)."""
     from powergrid_b200 import synthetic as S
     p = S.config2()
     M, n = p.kx.size, p.nimg
@@ -232,11 +235,12 @@ def test_config2_pcg_full_size(pg, oracle):
             print(f"cfg2 pcg({niter}): {e:.2e} vs reference, {ew:.2e} vs FP64 solve over the float operator, "
                   f"{e64:.2e} vs fp64 (reference vs FP64 solve over the float operator {rw:.2e}, "
                   f"reference vs fp64 {rel_l2(xr, x64):.2e})")
+            r64 = rel_l2(xr, x64)
             if niter == 3:
                 assert ew <= PCG_TOL and e64 <= PCG_TOL
                 assert e <= rw + PCG_TOL
             else:
-                assert e <= 0.3 and ew <= 0.3 and e64 <= 0.3
+                assert ew <= rw and e64 <= r64 and e <= rw + r64
     finally:
         oracle.set_threads(1)
 
@@ -347,7 +351,7 @@ def test_config5_full_grid_vs_oracle(pg, oracle):
                 assert it == nr == nw == 3 and ew <= PCG_TOL and e <= rw + PCG_TOL
             else:
                 print(f"cfg5 TV pcg(30): {e:.2e} vs reference, iterations {it} / {nr}")
-                assert it == nr and e <= 0.3
+                assert it == nr and e <= PCG_TOL
     finally:
         if ref_on:
             oracle.use_reference(False)
@@ -552,3 +556,41 @@ def test_pcg_weighted_resume_then_plain_solve(pg):
     R2 = pg.QuadPenalty(c["nx"], c["ny"], c["nz"], 2.0 * c["beta"])
     with pytest.raises(PGError, match="saved for penalty"):
         pg.pcg_resume(_gpu_op(pg, "pcg2d", c), state, None, y, R2, 1)
+
+
+@pytest.mark.parametrize("tile", [16, 32])
+@pytest.mark.parametrize("cc", [1, 2, 4])
+@pytest.mark.parametrize("nc,L", [(3, 4), (4, 6), (3, 1)])
+def test_adjoint_spread_tilings_vs_oracle(pg, oracle, tile, cc, nc, L):
+    """The 2-D adjoint spread under every compiled tiling: tile edge 16 or 32, 1, 2 or 4
+    coils per work item (3 coils leave a partial last chunk), Hanning segments (two per
+    sample window) or none, against the reference CPU path (SENSE over TimeSegmentation
+    over Gnufft, or over Gnufft alone for L = 1)."""
+    from powergrid_b200 import synthetic as S
+    n = 32
+    kx, ky, t = S.spiral(n, 4, 1024, 10e-3)
+    kz = np.zeros_like(kx)
+    fm = S.field_map(S.Rng(141), n, n, 1, 100.0)
+    sm = S.coil_maps(S.Rng(142), n, n, 1, nc)
+    M = kx.size
+    y = S.image(S.Rng(143), M * nc)
+    keys = ("PG_AUTOTUNE", "PG_TILE2D", "PG_SPREAD_CC")
+    saved = {k: os.environ.get(k) for k in keys}
+    os.environ.update({"PG_AUTOTUNE": "0", "PG_TILE2D": str(tile), "PG_SPREAD_CC": str(cc)})
+    try:
+        G = pg.Gnufft(M, 2.0, n, n, 1, kx, ky, kz)
+        A = pg.TimeSegmentation(G, fm, t, M, n * n, L, 1, 1) if L > 1 else G
+        Sg = pg.SENSE(A, sm, M, n * n, nc)
+        x = Sg / y
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    Go = oracle.gnufft(0, M, n, n, 1, kx, ky, kz)
+    Ao = oracle.timeseg(Go, fm, t, M, n * n, L) if L > 1 else Go
+    xr = oracle.sense(Ao, sm, M, n * n, nc).adjoint(y)
+    e = rel_l2(x, xr)
+    print(f"adjoint tile {tile}, {cc} coils per item, {nc} coils, L={L}: {e:.2e}")
+    assert e <= OP_TOL

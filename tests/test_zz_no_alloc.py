@@ -43,18 +43,18 @@ def test_noalloc_gdft_matches_operator_twice(pg, oracle):
     inputs = [_dev(v, torch, dev) for v in (kx, ky, kz, ix, iy, iz, fm, t)]
     stream = torch.cuda.current_stream()
     y = torch.empty(nk, dtype=torch.complex64, device=dev)
-    images = [S.image(S.Rng(seed), ni) for seed in (31, 32)]
-    xs = [_dev(v, torch, dev) for v in images]
-    refs = [G.forward(x).cpu().numpy() for x in xs]
-    torch.cuda.synchronize()
     try:
-        for x, img, y_op in zip(xs, images, refs):    # two calls in a row, different images
+        for seed in (31, 32):                         # two calls in a row, different images
+            img = S.image(S.Rng(seed), ni)
+            x = _dev(img, torch, dev)
+            y_op = G.forward(x, stream=stream)        # the existing entry point
+            torch.cuda.synchronize()
             L.pg_debug_fail_allocation_after(1)       # any library allocation now fails
             check(L.pg_gdft_forward_noalloc(nk, ni, *[P(v.data_ptr()) for v in inputs], P(x.data_ptr()),
                                             P(y.data_ptr()), P(stream.cuda_stream)))
             L.pg_debug_fail_allocation_after(0)
             torch.cuda.synchronize()
-            got = y.cpu().numpy()
+            got, y_op = y.cpu().numpy(), y_op.cpu().numpy()
             e_op, e_or = rel_l2(got, y_op), rel_l2(got, R.forward(img))
             print(f"no-alloc Gdft: {e_op:.2e} vs the Gdft operator, {e_or:.2e} vs the oracle")
             assert e_op <= OP_TOL and e_or <= OP_TOL, (e_op, e_or)
