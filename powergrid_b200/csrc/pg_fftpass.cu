@@ -335,15 +335,17 @@ __global__ void __launch_bounds__(kT) k_fft_fwd_cols(Lines ln, const float2* __r
 }
 
 // Inverse strided lines: per column, all n rows, inverse FFT along the line,
-// keep the nio rows at off + i -> row i of the output.
+// keep the nio rows at off + i -> row i of the output.  Every input cell is
+// read exactly once; with clear set it is zeroed after that read, which
+// leaves the input grids zero for the next adjoint spread.
 template <int LOGN>
-__global__ void __launch_bounds__(kT) k_fft_inv_cols(Lines ln, const float2* __restrict__ in,
+__global__ void __launch_bounds__(kT) k_fft_inv_cols(Lines ln, float2* in, int clear,
                                                      const float2* __restrict__ tw, float2* __restrict__ Q) {
   using CG = ColGeo<LOGN>;
   constexpr int R1 = CG::R1, R2 = CG::R2, CB = CG::CB;
   extern __shared__ float2 sh[];
   const int b = blockIdx.y, c0 = blockIdx.x * CB;
-  const float2* pin = in + (uint64_t)b * ln.in_bstride;
+  float2* pin = in + (uint64_t)b * ln.in_bstride;
 #pragma unroll
   for (int it0 = 0; it0 < CB * R2; it0 += kT) {
     const int it = it0 + threadIdx.x;
@@ -351,7 +353,7 @@ __global__ void __launch_bounds__(kT) k_fft_inv_cols(Lines ln, const float2* __r
     const int col = it % CB, m2 = it / CB;
     const int cg = c0 + col;
     float2 v[R1];
-    const float2* s = pin + (uint64_t)m2 * ln.rstride + cg;
+    float2* s = pin + (uint64_t)m2 * ln.rstride + cg;
 #pragma unroll
     for (int m1 = 0; m1 < R1; ++m1) v[m1] = (cg < ln.ncols) ? s[(uint64_t)R2 * m1 * ln.rstride] : make_float2(0.f, 0.f);
     dft<R1>(v, true);
@@ -359,6 +361,10 @@ __global__ void __launch_bounds__(kT) k_fft_inv_cols(Lines ln, const float2* __r
     d[0] = v[0];
 #pragma unroll
     for (int k1 = 1; k1 < R1; ++k1) d[k1 * R2 * CB] = twiddle(v[k1], tw[k1 * R2 + m2], true);
+    if (clear && cg < ln.ncols) {
+#pragma unroll
+      for (int m1 = 0; m1 < R1; ++m1) s[(uint64_t)R2 * m1 * ln.rstride] = make_float2(0.f, 0.f);
+    }
   }
   __syncthreads();
   float2* pout = Q + (uint64_t)b * ln.out_bstride;
@@ -493,10 +499,10 @@ pg_status cols_fwd(const Lines& ln, int B, const float2* P, const float2* tw, fl
 }
 
 template <int LOGN>
-pg_status cols_inv(const Lines& ln, int B, const float2* in, const float2* tw, float2* Q, cudaStream_t s) {
+pg_status cols_inv(const Lines& ln, int B, float2* in, int clear, const float2* tw, float2* Q, cudaStream_t s) {
   using CG = ColGeo<LOGN>;
   PG_CUDA(cudaFuncSetAttribute(k_fft_inv_cols<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CG::smem));
-  PG_LAUNCH(k_fft_inv_cols<LOGN>, dim3(ceil_div(ln.ncols, CG::CB), B), kT, CG::smem, s, ln, in, tw, Q);
+  PG_LAUNCH(k_fft_inv_cols<LOGN>, dim3(ceil_div(ln.ncols, CG::CB), B), kT, CG::smem, s, ln, in, clear, tw, Q);
   return PG_OK;
 }
 
@@ -525,8 +531,9 @@ pg_status d_rows_inv(int lg, const NufftGeom& g, int B, int L, const float2* Q, 
 pg_status d_cols_fwd(int lg, const Lines& ln, int B, const float2* P, const float2* tw, float2* out, cudaStream_t s) {
   PG_FFT_DISPATCH(lg, cols_fwd, ln, B, P, tw, out, s)
 }
-pg_status d_cols_inv(int lg, const Lines& ln, int B, const float2* in, const float2* tw, float2* Q, cudaStream_t s) {
-  PG_FFT_DISPATCH(lg, cols_inv, ln, B, in, tw, Q, s)
+pg_status d_cols_inv(int lg, const Lines& ln, int B, float2* in, int clear, const float2* tw, float2* Q,
+                     cudaStream_t s) {
+  PG_FFT_DISPATCH(lg, cols_inv, ln, B, in, clear, tw, Q, s)
 }
 
 // ---------------------------------------------------------------------------
@@ -653,7 +660,7 @@ __global__ void __launch_bounds__(fused::kTF, 1)
 }
 
 __global__ void __launch_bounds__(fused::kTF, 1)
-    k_fft2_adj_fused(NufftGeom g, int L, const float2* __restrict__ grids, const float2* __restrict__ S, int c0,
+    k_fft2_adj_fused(NufftGeom g, int L, float2* grids, int clear, const float2* __restrict__ S, int c0,
                      const float2* __restrict__ E, const float2* __restrict__ WoH, const float* __restrict__ deapf,
                      const float2* __restrict__ tw, float2* __restrict__ Rimg) {
   using namespace fused;
@@ -665,11 +672,11 @@ __global__ void __launch_bounds__(fused::kTF, 1)
   const int crop0 = g.crop_off[0], crop1 = g.crop_off[1];
   const uint64_t N = g.nimg();
   const int b = blockIdx.y, c = b / L, l = b - c * L;
-  const float2* in = grids + (uint64_t)b * n * n;
+  float2* in = grids + (uint64_t)b * n * n;
   for (int it = threadIdx.x; it < CPC * R; it += kTF) {   // x transform, pass 1: (column, m2)
     const int col = it % CPC, m2 = it / CPC;
     float2 v[R];
-    const float2* s = in + (uint64_t)m2 * n + r * CPC + col;
+    float2* s = in + (uint64_t)m2 * n + r * CPC + col;
 #pragma unroll
     for (int m1 = 0; m1 < R; ++m1) v[m1] = s[(uint64_t)R * m1 * n];
     dft<R>(v, true);
@@ -677,6 +684,10 @@ __global__ void __launch_bounds__(fused::kTF, 1)
     d[0] = v[0];
 #pragma unroll
     for (int k1 = 1; k1 < R; ++k1) d[k1 * R * CPC] = twiddle(v[k1], tw[k1 * R + m2], true);
+    if (clear) {   // every grid cell is read once, here: zero it for the next adjoint spread
+#pragma unroll
+      for (int m1 = 0; m1 < R; ++m1) s[(uint64_t)R * m1 * n] = make_float2(0.f, 0.f);
+    }
   }
   __syncthreads();
   for (int it = threadIdx.x; it < CPC * R; it += kTF) {   // x transform, pass 2: keep the cropped rows
@@ -866,7 +877,7 @@ pg_status fftpass_forward(const NufftGeom& g, int B, int L, const float2* x, con
   return d_cols_fwd(log2_exact(g.Gz), lz, B, P2, tw + g.Gx, grids, s);
 }
 
-pg_status fftpass_adjoint(const NufftGeom& g, int B, int L, const float2* grids, const float2* S, int c0,
+pg_status fftpass_adjoint(const NufftGeom& g, int B, int L, float2* grids, int clear, const float2* S, int c0,
                           const float2* E, const float2* WoH, const float* deapf, const float2* tw, float2* Q,
                           float2* Rimg, int accumulate, float2* x, cudaStream_t s) {
   if (B > kMaxGridY) return set_error(PG_INVALID_ARG, "fft passes: batch of %d grids", B);
@@ -874,23 +885,23 @@ pg_status fftpass_adjoint(const NufftGeom& g, int B, int L, const float2* grids,
   const uint64_t plane = (uint64_t)g.Gx * g.Gy;
   float2* Qr = Q;   // the rows the last pass reads
   if (use_fused(g)) {
-    PG_TRY(launch_fused(k_fft2_adj_fused, B, s, g, L, grids, S, c0, E, WoH, deapf, tw, Rimg));
+    PG_TRY(launch_fused(k_fft2_adj_fused, B, s, g, L, grids, clear, S, c0, E, WoH, deapf, tw, Rimg));
     const uint64_t N = g.nimg();
     PG_LAUNCH(k_sum_images, ceil_div(N * 8, 256), 256, 0, s, N, B, Rimg, accumulate, x);
     return PG_OK;
   }
   if (g.dim == 2) {
     const Lines ln{plane, (uint64_t)g.Nx * g.Gy, (uint64_t)g.Gy, g.Gy, g.Nx, g.crop_off[0]};
-    PG_TRY(d_cols_inv(lg, ln, B, grids, tw, Q, s));
+    PG_TRY(d_cols_inv(lg, ln, B, grids, clear, tw, Q, s));
   } else {
     // z lines keeping the Nz cropped slabs, then x lines per slab keeping Nx rows
     float2* Q1 = Q + (uint64_t)B * g.Nz * g.Nx * g.Gy;
     const Lines lz{g.ngrid(), (uint64_t)g.Nz * plane, plane, (int)plane, g.Nz, g.crop_off[2]};
-    PG_TRY(d_cols_inv(log2_exact(g.Gz), lz, B, grids, tw + g.Gx, Q1, s));
+    PG_TRY(d_cols_inv(log2_exact(g.Gz), lz, B, grids, clear, tw + g.Gx, Q1, s));
     const Lines lx{plane, (uint64_t)g.Nx * g.Gy, (uint64_t)g.Gy, g.Gy, g.Nx, g.crop_off[0]};
     const int slabs = B * g.Nz;
     for (int s0 = 0; s0 < slabs; s0 += kMaxGridY)
-      PG_TRY(d_cols_inv(lg, lx, std::min(kMaxGridY, slabs - s0), Q1 + s0 * lx.in_bstride, tw,
+      PG_TRY(d_cols_inv(lg, lx, std::min(kMaxGridY, slabs - s0), Q1 + s0 * lx.in_bstride, 0, tw,
                         Q + s0 * lx.out_bstride, s));
   }
   PG_TRY(d_rows_inv(lg, g, B, L, Qr, S, c0, E, WoH, deapf, tw, Rimg, s));

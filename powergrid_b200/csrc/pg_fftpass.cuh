@@ -17,9 +17,10 @@ pg_status fftpass_twiddles(const NufftGeom& g, DevBuf<float2>* tw, cudaStream_t 
 pg_status fftpass_forward(const NufftGeom& g, int B, int L, const float2* x, const float2* S, int c0,
                           const float2* E, const float2* Wo, const float* deapf, const float2* tw, float2* P,
                           float2* grids, cudaStream_t s);
-// grids: B full grids in (after the spread).  Q: fftpass_scratch elements;
+// grids: B full grids in (after the spread); with clear set the first pass
+// zeroes every cell after reading it.  Q: fftpass_scratch elements;
 // Rimg: B images; x (+)= their sum in a fixed order.
-pg_status fftpass_adjoint(const NufftGeom& g, int B, int L, const float2* grids, const float2* S, int c0,
+pg_status fftpass_adjoint(const NufftGeom& g, int B, int L, float2* grids, int clear, const float2* S, int c0,
                           const float2* E, const float2* WoH, const float* deapf, const float2* tw, float2* Q,
                           float2* Rimg, int accumulate, float2* x, cudaStream_t s);
 

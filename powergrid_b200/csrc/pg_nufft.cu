@@ -665,8 +665,14 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
 // Shared memory: tile planes [NP][re|im][PX][PY] int32, weights [smax][16]
 // f32, values [smax][NP2] float4 (two planes each), window starts [smax] u32.
 // ---------------------------------------------------------------------------
+// Blocks per SM the folded spread's register budget is sized for: its shared
+// memory admits 5 items of up to 4 planes (44 KB each at 256 samples) and 3 of
+// 8 planes.
+__host__ __device__ constexpr int spread2d_min_blocks(int np) { return np <= 4 ? 5 : 3; }
+
 template <int T, int CC, int KK>
-__global__ void __launch_bounds__(256) k_spread2d(NufftGeom g, TileShape t, const int4* __restrict__ sub,
+__global__ void __launch_bounds__(256, spread2d_min_blocks(CC * KK))
+    k_spread2d(NufftGeom g, TileShape t, const int4* __restrict__ sub,
                                                   const uint2* __restrict__ start, const float* __restrict__ wxy,
                                                   const uint32_t* __restrict__ perm, const float2* __restrict__ aa,
                                                   const float2* __restrict__ y, uint64_t dstride, int nb, int L,
@@ -682,6 +688,7 @@ __global__ void __launch_bounds__(256) k_spread2d(NufftGeom g, TileShape t, cons
   __shared__ unsigned vmax;
   __shared__ int box[4];               // window starts: min x, max x, min y, max y (tile coordinates)
   __shared__ int s_item;
+  __shared__ float s_scale[2];         // 2^e and 2^-e of the current item
   const int tid = threadIdx.x;
   int* tile = smi;
   float* sw = reinterpret_cast<float*>(smi + NP * 2 * CELLS);
@@ -756,9 +763,7 @@ __global__ void __launch_bounds__(256) k_spread2d(NufftGeom g, TileShape t, cons
         atomicMin(&box[2], ylo); atomicMax(&box[3], yhi);
       }
     }
-    __syncthreads();
-    float sc, inv;
-    {
+    if (tid == 0) {
       int extra = 0;
       while (count > (256 << extra)) ++extra;
       const float B = __uint_as_float(vmax) * wmax * 1.0001f;
@@ -767,9 +772,11 @@ __global__ void __launch_bounds__(256) k_spread2d(NufftGeom g, TileShape t, cons
         frexpf(B, &e);                 // B < 2^e
         e = 22 - e - extra;            // B * 2^e' < 2^(22 - extra)
       }
-      sc = ldexpf(1.f, e);
-      inv = ldexpf(1.f, -e);
+      s_scale[0] = ldexpf(1.f, e);
+      s_scale[1] = ldexpf(1.f, -e);
     }
+    __syncthreads();
+    const float sc = s_scale[0], inv = s_scale[1];
 
     // 3. spread
     {
@@ -834,11 +841,13 @@ __global__ void __launch_bounds__(256) k_spread2d(NufftGeom g, TileShape t, cons
 
     // 4. flush the bounding box, two cells (y, y + 1) per vector atomic
     {
-      const int bx0 = box[0], by0 = box[2] & ~1;
-      const int nxb = box[1] + 8 - bx0, nyp = (box[3] + 8 - by0 + 1) >> 1;
+      constexpr int PX = TG::PX, PYP = PY / 2;   // cell pairs per padded row
+      const int bx0 = box[0], bx1 = box[1] + 7, by0 = box[2] >> 1, by1 = (box[3] + 7) >> 1;
       const uint64_t G = g.ngrid();
-      for (int q = tid; q < nxb * nyp; q += blockDim.x) {
-        const int px = bx0 + q / nyp, py = by0 + 2 * (q % nyp);
+      for (int q = tid; q < PX * PYP; q += blockDim.x) {
+        const int px = q / PYP, pp = q - px * PYP;
+        if (px < bx0 || px > bx1 || pp < by0 || pp > by1) continue;
+        const int py = 2 * pp;
         const int cell = px * PY + py;
         const int gx = x0 + px, gy = y0 + py;
         const bool inside = gx < g.Gx && gy < g.Gy;
@@ -1251,6 +1260,22 @@ static pg_status ensure_workspace(NufftPlan* p, int B, cufftHandle* h, cudaStrea
   return PG_OK;
 }
 
+// The adjoint's spread target on the own-FFT path: B zeroed grids.
+static pg_status ensure_adjoint_grids(NufftPlan* p, int B, cudaStream_t s) {
+  const uint64_t n = (uint64_t)B * p->g.ngrid();
+  NufftWork& w = *p->work;
+  if (w.agrids.n < n || !w.agrids.p) {
+    if (w.agrids.p) PG_CUDA(cudaStreamSynchronize(s));
+    PG_TRY(w.agrids.alloc(n));
+    w.agrids_clean = false;
+  }
+  if (!w.agrids_clean) {
+    PG_CUDA(cudaMemsetAsync(w.agrids.p, 0, w.agrids.n * sizeof(float2), s));
+    w.agrids_clean = true;
+  }
+  return PG_OK;
+}
+
 // Forward input grids: the image region is rewritten by every forward, the
 // zero-pad border only here, when the buffer is (re)allocated.  cuFFT's
 // out-of-place C2C transform leaves its input unchanged.
@@ -1264,7 +1289,8 @@ static pg_status ensure_forward_input(NufftPlan* p, int B, cudaStream_t s) {
 }
 
 static int batch_coils(const NufftPlan* p, int C, int L) {
-  const uint64_t per = (uint64_t)L * p->g.ngrid() * sizeof(float2);
+  // own FFT passes: forward grids and the adjoint's spread target
+  const uint64_t per = (uint64_t)L * p->g.ngrid() * sizeof(float2) * (p->own_fft ? 2 : 1);
   uint64_t cb = per ? p->budget_bytes / per : (uint64_t)C;
   if (cb < 1) cb = 1;
   return (int)std::min<uint64_t>(cb, (uint64_t)C);
@@ -1368,13 +1394,14 @@ struct SpreadArgs {
 };
 
 template <int DIM, int T, int NP>
-static pg_status spread_launch_np(NufftPlan* p, const Binning* bin, const SpreadArgs& a, cudaStream_t s) {
+static pg_status spread_launch_np(NufftPlan* p, const Binning* bin, const SpreadArgs& a, float2* target,
+                                  cudaStream_t s) {
   PG_CUDA(cudaFuncSetAttribute(k_spread<DIM, T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.smem));
   const int nitems = bin->nsub * a.nchunks;
   PG_TRY(ensure_queue(p, s));
   const int blocks = persistent_blocks((const void*)k_spread<DIM, T, NP>, a.smem, nitems);
   PG_LAUNCH((k_spread<DIM, T, NP>), blocks, 256, a.smem, s, p->g, bin->tile, bin->subprob.p, bin->start.p,
-            bin->wxy.p, bin->wz.p, a.vs, bin->M, bin->K, bin->L, a.c0, a.cc, bin->submax, a.wmax, p->work->grids.p,
+            bin->wxy.p, bin->wz.p, a.vs, bin->M, bin->K, bin->L, a.c0, a.cc, bin->submax, a.wmax, target,
             p->work->queue.p, a.nchunks, nitems);
   return PG_OK;
 }
@@ -1382,22 +1409,24 @@ static pg_status spread_launch_np(NufftPlan* p, const Binning* bin, const Spread
 // Planes per block (coils x segments) with an unrolled kernel; others use the
 // runtime-loop instantiation (NP = 0).
 template <int DIM, int T>
-static pg_status spread_launch_t(NufftPlan* p, const Binning* bin, const SpreadArgs& a, cudaStream_t s) {
+static pg_status spread_launch_t(NufftPlan* p, const Binning* bin, const SpreadArgs& a, float2* target,
+                                 cudaStream_t s) {
   switch (a.cc * bin->K) {
-    case 1: return spread_launch_np<DIM, T, 1>(p, bin, a, s);
-    case 2: return spread_launch_np<DIM, T, 2>(p, bin, a, s);
-    case 3: return spread_launch_np<DIM, T, 3>(p, bin, a, s);
-    case 4: return spread_launch_np<DIM, T, 4>(p, bin, a, s);
-    case 6: return spread_launch_np<DIM, T, 6>(p, bin, a, s);
-    case 8: return spread_launch_np<DIM, T, 8>(p, bin, a, s);
+    case 1: return spread_launch_np<DIM, T, 1>(p, bin, a, target, s);
+    case 2: return spread_launch_np<DIM, T, 2>(p, bin, a, target, s);
+    case 3: return spread_launch_np<DIM, T, 3>(p, bin, a, target, s);
+    case 4: return spread_launch_np<DIM, T, 4>(p, bin, a, target, s);
+    case 6: return spread_launch_np<DIM, T, 6>(p, bin, a, target, s);
+    case 8: return spread_launch_np<DIM, T, 8>(p, bin, a, target, s);
   }
-  return spread_launch_np<DIM, T, 0>(p, bin, a, s);
+  return spread_launch_np<DIM, T, 0>(p, bin, a, target, s);
 }
 
-static pg_status launch_spread(NufftPlan* p, const Binning* bin, const SpreadArgs& a, cudaStream_t s) {
-  if (p->g.dim == 3) return spread_launch_t<3, 8>(p, bin, a, s);
-  if (bin->tile.TX == 32) return spread_launch_t<2, 32>(p, bin, a, s);
-  return spread_launch_t<2, 16>(p, bin, a, s);
+static pg_status launch_spread(NufftPlan* p, const Binning* bin, const SpreadArgs& a, float2* target,
+                               cudaStream_t s) {
+  if (p->g.dim == 3) return spread_launch_t<3, 8>(p, bin, a, target, s);
+  if (bin->tile.TX == 32) return spread_launch_t<2, 32>(p, bin, a, target, s);
+  return spread_launch_t<2, 16>(p, bin, a, target, s);
 }
 
 // Shared memory of k_spread2d: tile planes, staged weights, values and starts.
@@ -1409,7 +1438,7 @@ static size_t spread2d_smem(int T, int np, int smax) {
 
 template <int T, int CC, int KK>
 static pg_status spread2d_launch(NufftPlan* p, const Binning* bin, const float2* aa, const float2* y,
-                                 uint64_t dstride, int nb, float wmax, cudaStream_t s) {
+                                 uint64_t dstride, int nb, float wmax, float2* target, cudaStream_t s) {
   const size_t smem = spread2d_smem(T, CC * KK, bin->submax);
   PG_CUDA(cudaFuncSetAttribute(k_spread2d<T, CC, KK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int nchunks = (nb + CC - 1) / CC;
@@ -1417,21 +1446,20 @@ static pg_status spread2d_launch(NufftPlan* p, const Binning* bin, const float2*
   PG_TRY(ensure_queue(p, s));
   const int blocks = persistent_blocks((const void*)k_spread2d<T, CC, KK>, smem, nitems);
   PG_LAUNCH((k_spread2d<T, CC, KK>), blocks, 256, smem, s, p->g, bin->tile, bin->subprob.p, bin->start.p, bin->wxy.p,
-            bin->perm.p, aa, y, dstride, nb, bin->L, bin->submax, wmax, p->work->grids.p, p->work->queue.p, nchunks,
-            nitems);
+            bin->perm.p, aa, y, dstride, nb, bin->L, bin->submax, wmax, target, p->work->queue.p, nchunks, nitems);
   return PG_OK;
 }
 
 template <int T>
 static pg_status spread2d_launch_t(NufftPlan* p, const Binning* bin, int cc, const float2* aa, const float2* y,
-                                   uint64_t dstride, int nb, float wmax, cudaStream_t s) {
+                                   uint64_t dstride, int nb, float wmax, float2* target, cudaStream_t s) {
   switch (cc * 10 + bin->K) {
-    case 11: return spread2d_launch<T, 1, 1>(p, bin, aa, y, dstride, nb, wmax, s);
-    case 21: return spread2d_launch<T, 2, 1>(p, bin, aa, y, dstride, nb, wmax, s);
-    case 41: return spread2d_launch<T, 4, 1>(p, bin, aa, y, dstride, nb, wmax, s);
-    case 12: return spread2d_launch<T, 1, 2>(p, bin, aa, y, dstride, nb, wmax, s);
-    case 22: return spread2d_launch<T, 2, 2>(p, bin, aa, y, dstride, nb, wmax, s);
-    case 42: return spread2d_launch<T, 4, 2>(p, bin, aa, y, dstride, nb, wmax, s);
+    case 11: return spread2d_launch<T, 1, 1>(p, bin, aa, y, dstride, nb, wmax, target, s);
+    case 21: return spread2d_launch<T, 2, 1>(p, bin, aa, y, dstride, nb, wmax, target, s);
+    case 41: return spread2d_launch<T, 4, 1>(p, bin, aa, y, dstride, nb, wmax, target, s);
+    case 12: return spread2d_launch<T, 1, 2>(p, bin, aa, y, dstride, nb, wmax, target, s);
+    case 22: return spread2d_launch<T, 2, 2>(p, bin, aa, y, dstride, nb, wmax, target, s);
+    case 42: return spread2d_launch<T, 4, 2>(p, bin, aa, y, dstride, nb, wmax, target, s);
   }
   return set_error(PG_INVALID_ARG, "adjoint: no folded spread for %d coils x K=%d", cc, bin->K);
 }
@@ -1542,40 +1570,51 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
     PG_TRY(ensure_workspace(p, B, p->own_fft ? nullptr : &h, s));
     const float2* yc = y + (uint64_t)c0 * b.data_stride;
     const float2* aa = (L > 1 || bin->aa.p) ? bin->aa.p : nullptr;
+    // spread target: on the own FFT passes a grid set kept zero between
+    // adjoints (its first inverse pass clears it); else the cuFFT grids,
+    // cleared here
+    float2* target = p->work->grids.p;
+    if (p->own_fft) {
+      PG_TRY(ensure_adjoint_grids(p, B, s));
+      target = p->work->agrids.p;
+    }
     {
-    // the adjoint gridding as the reference's gridding_adjoint (gridding.cpp:31-214):
-    // the grids' clearing and the spread, timed together
+    // the adjoint gridding as the reference's gridding_adjoint (gridding.cpp:31-214),
+    // timed as one stage (with the grids' clearing where it is a separate step)
     ProfScope pag("adjoint_gridding", s);
     if (folded) {
-      {
+      if (!p->own_fft) {
         ProfScope ps("prep", s);
-        PG_CUDA(cudaMemsetAsync(p->work->grids.p, 0, (size_t)B * G * sizeof(float2), s));
+        PG_CUDA(cudaMemsetAsync(target, 0, (size_t)B * G * sizeof(float2), s));
       }
+      p->work->agrids_clean = false;
       if (bin->nsub > 0) {
         ProfScope ps("spread", s);
-        if (t.TX == 32) PG_TRY(spread2d_launch_t<32>(p, bin, Cc, aa, yc, b.data_stride, nb, wmax, s));
-        else PG_TRY(spread2d_launch_t<16>(p, bin, Cc, aa, yc, b.data_stride, nb, wmax, s));
+        if (t.TX == 32) PG_TRY(spread2d_launch_t<32>(p, bin, Cc, aa, yc, b.data_stride, nb, wmax, target, s));
+        else PG_TRY(spread2d_launch_t<16>(p, bin, Cc, aa, yc, b.data_stride, nb, wmax, target, s));
       }
     } else {
     PG_TRY(grow(p->work->vs, (uint64_t)nb * bin->M * K, s));
     {
       ProfScope ps("prep", s);
-      const uint64_t n4 = (uint64_t)B * G / 2;   // G is even: float2 pairs -> float4 words
+      // the own-FFT target is already zero: only the values are formed
+      const uint64_t n4 = p->own_fft ? 0 : (uint64_t)B * G / 2;   // G is even: float2 pairs -> float4 words
       const uint64_t work = std::max<uint64_t>(n4, bin->M);
       PG_LAUNCH(k_adjoint_prep, (unsigned)std::min<uint64_t>(ceil_div(work, 256), 8ull * sm_count()), 256, 0, s, n4,
-                reinterpret_cast<float4*>(p->work->grids.p), nb, bin->M, K, bin->perm.p, aa, yc, b.data_stride,
+                reinterpret_cast<float4*>(target), nb, bin->M, K, bin->perm.p, aa, yc, b.data_stride,
                 p->work->vs.p);
     }
+    p->work->agrids_clean = false;
     if (bin->nsub > 0) {
       ProfScope ps("spread", s);
       // full chunks of cc coils, then the remaining coils in one chunk
       const int cc = std::min(Cc, nb);
       const int full = nb / cc, rest = nb - full * cc;
       SpreadArgs a{p->work->vs.p, 0, cc, full, wmax, smem_for(cc)};
-      PG_TRY(launch_spread(p, bin, a, s));
+      PG_TRY(launch_spread(p, bin, a, target, s));
       if (rest > 0) {
         SpreadArgs r{p->work->vs.p, full * cc, rest, 1, wmax, smem_for(rest)};
-        PG_TRY(launch_spread(p, bin, r, s));
+        PG_TRY(launch_spread(p, bin, r, target, s));
       }
     }
     }
@@ -1585,8 +1624,9 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
       PG_TRY(grow(p->work->fin, fftpass_scratch(g, B), s));
       PG_TRY(grow(p->work->rimg, (uint64_t)B * g.nimg(), s));
       ProfScope ps("fft_adj", s);
-      PG_TRY(fftpass_adjoint(g, B, L, p->work->grids.p, b.S, c0, b.E, b.WoH, p->deapf.p, p->tw2d.p, p->work->fin.p,
+      PG_TRY(fftpass_adjoint(g, B, L, target, 1, b.S, c0, b.E, b.WoH, p->deapf.p, p->tw2d.p, p->work->fin.p,
                            p->work->rimg.p, acc, x, s));
+      p->work->agrids_clean = true;   // the first inverse pass leaves the target zero
       continue;
     }
     {

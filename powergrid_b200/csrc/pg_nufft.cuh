@@ -67,7 +67,14 @@ struct Binning {
 // Grid workspace and cuFFT work area.  Plans of one geometry that run back
 // to back on one stream (the shots of pcSenseTimeSeg) share a single one.
 struct NufftWork {
-  DevBuf<float2> grids;     // FFT output (forward) / spread target (adjoint)
+  DevBuf<float2> grids;     // FFT output (forward) / spread target (adjoint, cuFFT path)
+  // Spread target of the adjoint on the plan's own FFT passes.  It is zero
+  // at the start of every adjoint: zeroed when allocated, and the first
+  // inverse FFT pass zeroes each cell after reading it.  agrids_clean is
+  // false from the spread until that pass is enqueued, so an adjoint that
+  // stops in between (an error) makes the next one clear it first.
+  DevBuf<float2> agrids;
+  bool agrids_clean = false;
   DevBuf<float2> fin;       // forward FFT input; its zero-pad border stays zero
   DevBuf<float2> vs;        // adjoint: per-sample segment values in binned order
   DevBuf<float2> rimg;      // adjoint with the plan's own FFT passes: one image per grid

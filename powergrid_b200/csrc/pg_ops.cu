@@ -159,7 +159,8 @@ pg_status GnufftOp::adjoint(const float2* y, float2* x, cudaStream_t s) {
 }
 uint64_t GnufftOp::resident_bytes() const {
   if (!plan) return interp ? interp->M * 16 + interp->lut.bytes() : 0;
-  return plan->M * (3 * 4 + 8 + 64 + 4 + 4) + plan->work->grids.bytes() + plan->work->fin.bytes();
+  return plan->M * (3 * 4 + 8 + 64 + 4 + 4) + plan->work->grids.bytes() + plan->work->agrids.bytes() +
+         plan->work->fin.bytes();
 }
 
 // ---- Gdft ------------------------------------------------------------------
@@ -310,7 +311,8 @@ uint64_t PcSenseTsOp::resident_bytes() const {
   uint64_t b = S.bytes() + E.bytes();
   for (auto& p : plans) b += p->M * 100;
   if (!plans.empty())
-    b += plans[0]->work->grids.bytes() + plans[0]->work->fin.bytes() + plans[0]->work->fft_work.bytes();
+    b += plans[0]->work->grids.bytes() + plans[0]->work->agrids.bytes() + plans[0]->work->fin.bytes() +
+         plans[0]->work->fft_work.bytes();
   return b;
 }
 
