@@ -14,7 +14,10 @@
 // differences (GdftR2.cpp:62-110): the same kernels with GRAD = true.
 //
 // Layout: one thread per output (sample for forward, voxel for adjoint);
-// the other side is staged in shared-memory tiles of 128 entries.  When the
+// the other side is staged in shared-memory tiles of 128 entries.  Within a
+// tile each coil keeps two complex sums, A = sum cos(ph) v and B = sum
+// sin(ph) v, each one paired fp32 fma per pair with v as loaded; they are
+// combined once per tile (forward A - iB, adjoint A + iB).  When the
 // outputs alone do not fill the GPU the inner sum is split over blockIdx.y
 // and the partial sums are combined in a fixed order (deterministic).
 #include <vector>
@@ -81,9 +84,9 @@ __global__ void __launch_bounds__(kTile) k_dft_forward(uint64_t nk, uint64_t ni,
       for (int c = 0; c < NC; ++c) sx[c][threadIdx.x] = xin[(uint64_t)c * ni + jt + threadIdx.x];
     }
     __syncthreads();
-    float2 acc[NC];
+    float2 acA[NC], acB[NC];
 #pragma unroll
-    for (int c = 0; c < NC; ++c) acc[c] = make_float2(0.f, 0.f);
+    for (int c = 0; c < NC; ++c) acA[c] = acB[c] = make_float2(0.f, 0.f);
     for (int j = 0; j < n; ++j) {
       const double4 v = sv[j];
       const double ph = fma(k.x, v.x, fma(k.y, v.y, fma(k.z, v.z, v.w * k.w)));
@@ -94,15 +97,17 @@ __global__ void __launch_bounds__(kTile) k_dft_forward(uint64_t nk, uint64_t ni,
         s *= b;
         co *= b;
       }
+      const float2 cp = make_float2(co, co), sp = make_float2(s, s);
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
         const float2 x = sx[c][j];
-        acc[c].x = fmaf(co, x.x, fmaf(s, x.y, acc[c].x));
-        acc[c].y = fmaf(co, x.y, fmaf(-s, x.x, acc[c].y));
+        acA[c] = __ffma2_rn(cp, x, acA[c]);
+        acB[c] = __ffma2_rn(sp, x, acB[c]);
       }
     }
+    // e^{-i ph} x = cos x - i sin x: re += A.x + B.y, im += A.y - B.x
 #pragma unroll
-    for (int c = 0; c < NC; ++c) { tot[c].x += acc[c].x; tot[c].y += acc[c].y; }
+    for (int c = 0; c < NC; ++c) { tot[c].x += acA[c].x + acB[c].y; tot[c].y += acA[c].y - acB[c].x; }
   }
   if (i < nk) {
 #pragma unroll
@@ -142,9 +147,9 @@ __global__ void __launch_bounds__(kTile) k_dft_adjoint(uint64_t nk, uint64_t ni,
       for (int c = 0; c < NC; ++c) sy[c][threadIdx.x] = yin[(uint64_t)c * dstride + it + threadIdx.x];
     }
     __syncthreads();
-    float2 acc[NC];
+    float2 acA[NC], acB[NC];
 #pragma unroll
-    for (int c = 0; c < NC; ++c) acc[c] = make_float2(0.f, 0.f);
+    for (int c = 0; c < NC; ++c) acA[c] = acB[c] = make_float2(0.f, 0.f);
     for (int q = 0; q < n; ++q) {
       const double4 k = sk[q];
       const double ph = fma(k.x, v.x, fma(k.y, v.y, fma(k.z, v.z, v.w * k.w)));
@@ -155,15 +160,17 @@ __global__ void __launch_bounds__(kTile) k_dft_adjoint(uint64_t nk, uint64_t ni,
         s *= b;
         co *= b;
       }
+      const float2 cp = make_float2(co, co), sp = make_float2(s, s);
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
         const float2 y = sy[c][q];
-        acc[c].x = fmaf(co, y.x, fmaf(-s, y.y, acc[c].x));
-        acc[c].y = fmaf(s, y.x, fmaf(co, y.y, acc[c].y));
+        acA[c] = __ffma2_rn(cp, y, acA[c]);
+        acB[c] = __ffma2_rn(sp, y, acB[c]);
       }
     }
+    // e^{+i ph} y = cos y + i sin y: re += A.x - B.y, im += A.y + B.x
 #pragma unroll
-    for (int c = 0; c < NC; ++c) { tot[c].x += acc[c].x; tot[c].y += acc[c].y; }
+    for (int c = 0; c < NC; ++c) { tot[c].x += acA[c].x - acB[c].y; tot[c].y += acA[c].y + acB[c].x; }
   }
   if (j < ni) {
 #pragma unroll
