@@ -1467,28 +1467,30 @@ static pg_status spread2d_launch_t(NufftPlan* p, const Binning* bin, int cc, con
 // Post-kernel launch: CP coil lanes x LP segment lanes per pixel (powers of
 // two, at most 8 lanes).
 template <int CP, int LP>
-static pg_status post_launch(NufftPlan* p, int nb, int L, const NufftBatch& b, int c0, int acc, float2* x,
-                             cudaStream_t s) {
+static pg_status post_launch(NufftPlan* p, int nb, int L, const NufftBatch& b, const float2* WoH,
+                             const float2* grids, int c0, int acc, float2* x, cudaStream_t s) {
   const uint64_t N = p->g.nimg();
-  PG_LAUNCH((k_post<CP, LP>), ceil_div(N * CP * LP, 256), 256, 0, s, p->g, nb, L, p->work->grids.p, b.S, c0, b.E,
-            b.WoH, p->deapf.p, acc, x);
+  PG_LAUNCH((k_post<CP, LP>), ceil_div(N * CP * LP, 256), 256, 0, s, p->g, nb, L, grids, b.S, c0, b.E, WoH,
+            p->deapf.p, acc, x);
   return PG_OK;
 }
 
-static pg_status launch_post(NufftPlan* p, int nb, int L, const NufftBatch& b, int c0, int acc, float2* x,
-                             cudaStream_t s) {
+// nb coils starting at coil c0 of the batch's maps, whose grids start at
+// `grids`; x (+)= their image.
+static pg_status launch_post(NufftPlan* p, int nb, int L, const NufftBatch& b, const float2* WoH,
+                             const float2* grids, int c0, int acc, float2* x, cudaStream_t s) {
   const int cp = nb >= 8 ? 8 : nb >= 4 ? 4 : nb >= 2 ? 2 : 1;
   const int lp = std::min(8 / cp, L >= 4 ? 4 : L >= 2 ? 2 : 1);
   switch (cp * 10 + lp) {
-    case 81: return post_launch<8, 1>(p, nb, L, b, c0, acc, x, s);
-    case 42: return post_launch<4, 2>(p, nb, L, b, c0, acc, x, s);
-    case 41: return post_launch<4, 1>(p, nb, L, b, c0, acc, x, s);
-    case 24: return post_launch<2, 4>(p, nb, L, b, c0, acc, x, s);
-    case 22: return post_launch<2, 2>(p, nb, L, b, c0, acc, x, s);
-    case 21: return post_launch<2, 1>(p, nb, L, b, c0, acc, x, s);
-    case 14: return post_launch<1, 4>(p, nb, L, b, c0, acc, x, s);
-    case 12: return post_launch<1, 2>(p, nb, L, b, c0, acc, x, s);
-    default: return post_launch<1, 1>(p, nb, L, b, c0, acc, x, s);
+    case 81: return post_launch<8, 1>(p, nb, L, b, WoH, grids, c0, acc, x, s);
+    case 42: return post_launch<4, 2>(p, nb, L, b, WoH, grids, c0, acc, x, s);
+    case 41: return post_launch<4, 1>(p, nb, L, b, WoH, grids, c0, acc, x, s);
+    case 24: return post_launch<2, 4>(p, nb, L, b, WoH, grids, c0, acc, x, s);
+    case 22: return post_launch<2, 2>(p, nb, L, b, WoH, grids, c0, acc, x, s);
+    case 21: return post_launch<2, 1>(p, nb, L, b, WoH, grids, c0, acc, x, s);
+    case 14: return post_launch<1, 4>(p, nb, L, b, WoH, grids, c0, acc, x, s);
+    case 12: return post_launch<1, 2>(p, nb, L, b, WoH, grids, c0, acc, x, s);
+    default: return post_launch<1, 1>(p, nb, L, b, WoH, grids, c0, acc, x, s);
   }
 }
 
@@ -1506,16 +1508,40 @@ pg_status nufft_forward(NufftPlan* p, const NufftBatch& b, const float2* x, floa
       PG_TRY(ensure_workspace(p, B, nullptr, s));
       PG_TRY(grow(p->work->fin, fftpass_scratch(g, B), s));
       ProfScope ps("fft_fwd", s);
-      PG_TRY(fftpass_forward(g, B, L, x, b.S, c0, b.E, b.Wo, p->deapf.p, p->tw2d.p, p->work->fin.p,
-                           p->work->grids.p, s));
+      if (b.cgroup > 0) {
+        // one pass per image over its coils of the batch, into their grids
+        for (int i0 = c0; i0 < c0 + nb;) {
+          const int img = i0 / b.cgroup;
+          const int i1 = std::min(c0 + nb, (img + 1) * b.cgroup);
+          PG_TRY(fftpass_forward(g, (i1 - i0) * L, L, x + (uint64_t)img * b.image_stride, b.S, i0, b.E,
+                                 b.Wo ? b.Wo + (uint64_t)img * b.phase_stride : nullptr, p->deapf.p, p->tw2d.p,
+                                 p->work->fin.p, p->work->grids.p + (uint64_t)(i0 - c0) * L * G, s));
+          i0 = i1;
+        }
+      } else {
+        PG_TRY(fftpass_forward(g, B, L, x, b.S, c0, b.E, b.Wo, p->deapf.p, p->tw2d.p, p->work->fin.p,
+                               p->work->grids.p, s));
+      }
     } else {
     cufftHandle h;
     PG_TRY(ensure_workspace(p, B, &h, s));
     PG_TRY(ensure_forward_input(p, B, s));
     {
       ProfScope ps("pre", s);
-      PG_LAUNCH(k_pre, dim3(ceil_div(g.nimg(), 256), B), 256, 0, s, g, L, x, b.S, c0, b.E, b.Wo, p->deapf.p,
-                p->work->fin.p);
+      if (b.cgroup > 0) {
+        for (int i0 = c0; i0 < c0 + nb;) {
+          const int img = i0 / b.cgroup;
+          const int i1 = std::min(c0 + nb, (img + 1) * b.cgroup);
+          PG_LAUNCH(k_pre, dim3(ceil_div(g.nimg(), 256), (i1 - i0) * L), 256, 0, s, g, L,
+                    x + (uint64_t)img * b.image_stride, b.S, i0, b.E,
+                    b.Wo ? b.Wo + (uint64_t)img * b.phase_stride : nullptr, p->deapf.p,
+                    p->work->fin.p + (uint64_t)(i0 - c0) * L * G);
+          i0 = i1;
+        }
+      } else {
+        PG_LAUNCH(k_pre, dim3(ceil_div(g.nimg(), 256), B), 256, 0, s, g, L, x, b.S, c0, b.E, b.Wo, p->deapf.p,
+                  p->work->fin.p);
+      }
     }
     {
       ProfScope ps("fft_fwd", s);
@@ -1624,8 +1650,22 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
       PG_TRY(grow(p->work->fin, fftpass_scratch(g, B), s));
       PG_TRY(grow(p->work->rimg, (uint64_t)B * g.nimg(), s));
       ProfScope ps("fft_adj", s);
-      PG_TRY(fftpass_adjoint(g, B, L, target, 1, b.S, c0, b.E, b.WoH, p->deapf.p, p->tw2d.p, p->work->fin.p,
-                           p->work->rimg.p, acc, x, s));
+      if (b.cgroup > 0) {
+        // one pass per image over its coils of the batch; an image whose
+        // coils began in an earlier batch adds to its sum
+        for (int i0 = c0; i0 < c0 + nb;) {
+          const int img = i0 / b.cgroup;
+          const int i1 = std::min(c0 + nb, (img + 1) * b.cgroup);
+          const int acc_img = (b.accumulate || i0 > img * b.cgroup) ? 1 : 0;
+          PG_TRY(fftpass_adjoint(g, (i1 - i0) * L, L, target + (uint64_t)(i0 - c0) * L * G, 1, b.S, i0, b.E,
+                                 b.WoH ? b.WoH + (uint64_t)img * b.phase_stride : nullptr, p->deapf.p, p->tw2d.p,
+                                 p->work->fin.p, p->work->rimg.p, acc_img, x + (uint64_t)img * b.image_stride, s));
+          i0 = i1;
+        }
+      } else {
+        PG_TRY(fftpass_adjoint(g, B, L, target, 1, b.S, c0, b.E, b.WoH, p->deapf.p, p->tw2d.p, p->work->fin.p,
+                               p->work->rimg.p, acc, x, s));
+      }
       p->work->agrids_clean = true;   // the first inverse pass leaves the target zero
       continue;
     }
@@ -1635,7 +1675,19 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
                             reinterpret_cast<cufftComplex*>(p->work->grids.p), CUFFT_INVERSE));
     }
     ProfScope ps("post", s);
-    PG_TRY(launch_post(p, nb, L, b, c0, acc, x, s));
+    if (b.cgroup > 0) {
+      for (int i0 = c0; i0 < c0 + nb;) {
+        const int img = i0 / b.cgroup;
+        const int i1 = std::min(c0 + nb, (img + 1) * b.cgroup);
+        const int acc_img = (b.accumulate || i0 > img * b.cgroup) ? 1 : 0;
+        PG_TRY(launch_post(p, i1 - i0, L, b, b.WoH ? b.WoH + (uint64_t)img * b.phase_stride : nullptr,
+                           p->work->grids.p + (uint64_t)(i0 - c0) * L * G, i0, acc_img,
+                           x + (uint64_t)img * b.image_stride, s));
+        i0 = i1;
+      }
+    } else {
+      PG_TRY(launch_post(p, nb, L, b, b.WoH, p->work->grids.p, c0, acc, x, s));
+    }
   }
   return PG_OK;
 }

@@ -111,6 +111,13 @@ struct NufftBatch {
   const Binning* bin = nullptr;  // segmentation binning (L, K, AA) or plan->plain
   uint64_t data_stride = 0;      // elements between coils in the data vector
   bool accumulate = false;       // adjoint: add into x instead of overwrite
+  // Several images in one call (the slices of a request): coil c belongs to
+  // image c / cgroup, whose x (forward input,
+  // adjoint output) starts image_stride elements after the previous one and
+  // whose Wo / WoH set phase_stride elements after the previous one.  S then
+  // holds C = images x cgroup coil maps.  0: one image.
+  int cgroup = 0;
+  uint64_t image_stride = 0, phase_stride = 0;
 };
 
 pg_status nufft_plan_create(std::unique_ptr<NufftPlan>* out, uint64_t M, float gridos, int nx, int ny, int nz,

@@ -479,6 +479,68 @@ pg_status make_timeseg_shared(std::unique_ptr<TimeSegOp>* out, pg_op_s* G, const
   return PG_OK;
 }
 
+// ---- the slices of a request as one operator ---------------------------------
+pg_status make_slice_batch(std::unique_ptr<SliceBatchOp>* out, GnufftOp* G, const TimeSegOp* ts, uint64_t ns,
+                           uint64_t nc, const float* field_maps, const float* sense_maps, cudaStream_t s) {
+  if (!G || !G->plan || !sense_maps || (ts && !field_maps) || ns == 0 || nc == 0)
+    return set_error(PG_INVALID_ARG, "slice batch: null argument");
+  const uint64_t N = G->n_image, M = G->n_data;
+  auto op = std::make_unique<SliceBatchOp>();
+  op->kind = PG_OP_SENSE;
+  op->G = G;
+  op->ts = (ts && ts->tab.L > 1) ? ts : nullptr;
+  op->ns = ns;
+  op->nc = nc;
+  op->N = N;
+  op->M = M;
+  op->L = op->ts ? op->ts->tab.L : 1;
+  op->n_image = ns * N;
+  op->n_data = ns * nc * M;
+  op->n_seg = ns;
+  if (op->ts) {
+    if (ts->n_image != N || ts->n_data != M || !ts->bin)
+      return set_error(PG_INVALID_ARG, "slice batch: segmentation does not match the Gnufft");
+    for (uint64_t p = 0; p < ns * N; ++p)
+      if (!std::isfinite(field_maps[p])) return set_error(PG_INVALID_ARG, "slice batch: non-finite field map");
+    DevBuf<float> fm;
+    PG_TRY(fm.upload(field_maps, ns * N, s));
+    const uint64_t LN = (uint64_t)op->L * N;
+    PG_TRY(op->Wo.alloc(ns * LN));
+    PG_TRY(op->WoH.alloc(ns * LN));
+    for (uint64_t sl = 0; sl < ns; ++sl)
+      PG_LAUNCH(k_ts_phases, ceil_div(LN, 256), 256, 0, s, N, op->L, ts->tab.tau, ts->tab.tmin, fm.p + sl * N,
+                op->Wo.p + sl * LN, op->WoH.p + sl * LN);
+    PG_CUDA(cudaStreamSynchronize(s));  // fm is released on return
+  }
+  PG_TRY(op->S.upload(reinterpret_cast<const float2*>(sense_maps), ns * nc * N, s));
+  *out = std::move(op);
+  return PG_OK;
+}
+
+pg_status SliceBatchOp::forward(const float2* x, float2* y, cudaStream_t s) {
+  NufftBatch b;
+  b.C = (int)(ns * nc);
+  b.S = S.p;
+  b.data_stride = M;
+  b.cgroup = (int)nc;
+  b.image_stride = N;
+  b.phase_stride = (uint64_t)L * N;
+  if (ts) { b.Wo = Wo.p; b.bin = ts->bin.get(); }
+  return nufft_forward(G->plan.get(), b, x, y, s);
+}
+
+pg_status SliceBatchOp::adjoint(const float2* y, float2* x, cudaStream_t s) {
+  NufftBatch b;
+  b.C = (int)(ns * nc);
+  b.S = S.p;
+  b.data_stride = M;
+  b.cgroup = (int)nc;
+  b.image_stride = N;
+  b.phase_stride = (uint64_t)L * N;
+  if (ts) { b.WoH = WoH.p; b.bin = ts->bin.get(); }
+  return nufft_adjoint(G->plan.get(), b, y, x, s);
+}
+
 pg_status tune_for_coils(pg_op_s* G, int nc, bool search, cudaStream_t s) {
   if (G->kind == PG_OP_GNUFFT) {
     NufftPlan* plan = static_cast<GnufftOp*>(G)->plan.get();

@@ -24,6 +24,9 @@ struct pg_op_s {
   int kind = 0;
   std::unique_ptr<pg_pcg_cache_base> pcg_cache;
   uint64_t n_data = 0, n_image = 0;
+  // independent problems of equal size stacked in x and y (the PCG solves each
+  // with its own scalars); 1 for every operator of the C ABI
+  uint64_t n_seg = 1;
   // staging for the host-buffer entry points (kept between calls)
   pg::DevBuf<float2> hx, hy, hx0;
   pg::DevBuf<float> hw;
@@ -133,6 +136,28 @@ struct LowRankOp : pg_op_s {
   pg_status adjoint(const float2* y, float2* x, cudaStream_t s) override;
   uint64_t resident_bytes() const override;
 };
+
+// The slices of a served request as one operator.  The reference's driver
+// builds SENSE over TimeSegmentation over Gnufft for each slice and solves them
+// one after another (PowerGridIsmrmrd.cpp:191-264); here the ns slices, which
+// share the trajectory, the segment windows and the sample binning, are
+// stacked, x = [x_0; ...; x_{ns-1}] (N each), y = [y_0; ...] (nc * M each,
+// coil-major), and one gridding launch carries every slice's coils (slice s,
+// coil c = virtual coil s * nc + c).  n_seg = ns: the PCG solves each slice
+// with its own FP64 scalars and early exits.
+struct SliceBatchOp : pg_op_s {
+  GnufftOp* G = nullptr;            // not owned: the job's plan (own workspace)
+  const TimeSegOp* ts = nullptr;    // not owned: segment windows and binning; null when L <= 1
+  uint64_t ns = 1, nc = 1, N = 0, M = 0;
+  int L = 1;
+  DevBuf<float2> S;                 // ns x nc x N coil maps
+  DevBuf<float2> Wo, WoH;           // ns x L x N segment phases
+  pg_status forward(const float2* x, float2* y, cudaStream_t s) override;
+  pg_status adjoint(const float2* y, float2* x, cudaStream_t s) override;
+};
+// field_maps: ns x N; sense_maps: ns x nc x N complex (interleaved floats).
+pg_status make_slice_batch(std::unique_ptr<SliceBatchOp>* out, GnufftOp* G, const TimeSegOp* ts, uint64_t ns,
+                           uint64_t nc, const float* field_maps, const float* sense_maps, cudaStream_t s);
 
 // out[:, a] = sum_b in[:, b] * C[a + Kout b] over columns of length N, the sum
 // in order of b; out is stored column-major N x Kout, or transposed (Kout x N,

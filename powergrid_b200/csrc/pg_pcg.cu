@@ -10,6 +10,14 @@
 // Early exits set a device flag that turns the remaining kernels into
 // no-ops, which returns the x of the exit point as the reference does.
 //
+// Segments: an operator may stack n_seg independent problems of equal size
+// (the slices of a served request), x = [x_0; ...], y = [y_0; ...].  Every
+// kernel then runs with blockIdx.y = segment over that segment's part of the
+// vectors, with its own partial sums, last-block counter, FP64 scalars and
+// flags, so each segment takes exactly the steps and early exits of its own
+// solve (solve_pwls_pcg is run per slice by the reference's drivers,
+// PowerGridIsmrmrd.cpp:191-264).  One segment is the plain solve.
+//
 // The regularizer is fused: Gradient = beta * sum_dims Ctd(dpot(Cd x)) is a
 // 3-point stencil per dimension evaluated on the fly (no Cd/Ctd vectors),
 // with the reference's boundary rules: Cd is zero below the offset and
@@ -140,7 +148,11 @@ __global__ void k_fill_ones(uint64_t n, float* w) {
 }
 
 // sum W |y|^2 (norm_grad denominator, solve_pwls_pcg.hpp:42-46)
-__global__ void k_ywy(uint64_t n, const float2* __restrict__ y, const float* __restrict__ W, double* part, int nb) {
+__global__ void k_ywy(uint64_t n, const float2* __restrict__ y, const float* __restrict__ W, double* part, int nb,
+                      int pstride) {
+  y += (uint64_t)blockIdx.y * n;
+  W += (uint64_t)blockIdx.y * n;
+  part += (size_t)blockIdx.y * pstride;
   double a = 0.0;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     const float2 v = y[i];
@@ -149,7 +161,10 @@ __global__ void k_ywy(uint64_t n, const float2* __restrict__ y, const float* __r
   block_store2(a, 0.0, part, nb);
 }
 
-__global__ void k_scalar_init(const double* part, int nb, double* sc, uint32_t* fl) {
+__global__ void k_scalar_init(const double* part, int nb, int pstride, double* sc, uint32_t* fl) {
+  part += (size_t)blockIdx.x * pstride;
+  sc += (size_t)blockIdx.x * S_NSCAL;
+  fl += (size_t)blockIdx.x * F_NFLAG;
   const double ywy = part_sum(part, nb, 0);
   if (threadIdx.x == 0) {
     for (int i = 0; i < S_NSCAL; ++i) sc[i] = 0.0;
@@ -198,6 +213,8 @@ __device__ __forceinline__ double block_part_sum(const double* part, int nb, int
 // r = W (.) (y - Ax): the residual before the first iteration.
 __global__ void k_residual(uint64_t n, const float2* __restrict__ y, const float2* __restrict__ Ax,
                            const float* __restrict__ W, float2* __restrict__ r) {
+  const uint64_t o = (uint64_t)blockIdx.y * n;
+  y += o; Ax += o; W += o; r += o;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     const float2 d = csub(y[i], Ax[i]);
     const float w = W[i];
@@ -211,7 +228,14 @@ __global__ void k_residual(uint64_t n, const float2* __restrict__ y, const float
 // quadratic k_ddir reads neighbours of the old direction while it rewrites it).
 __global__ void k_ngrad(PenDev R, const float2* __restrict__ x, float2* __restrict__ ngrad, double* part, int nb,
                         unsigned* counter, double* sc, uint32_t* fl, const float2* __restrict__ ddir,
-                        float2* __restrict__ ddir_prev) {
+                        float2* __restrict__ ddir_prev, int pstride) {
+  {
+    const uint64_t o = (uint64_t)blockIdx.y * R.N;
+    x += o; ngrad += o; ddir += o;
+    if (ddir_prev) ddir_prev += o;
+    part += (size_t)blockIdx.y * pstride; counter += blockIdx.y;
+    sc += (size_t)blockIdx.y * S_NSCAL; fl += (size_t)blockIdx.y * F_NFLAG;
+  }
   if (fl[F_DONE]) return;
   double a = 0.0, b = 0.0;
   for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < R.N; j += (uint64_t)gridDim.x * blockDim.x) {
@@ -238,7 +262,13 @@ __global__ void k_ngrad(PenDev R, const float2* __restrict__ x, float2* __restri
 
 // ddir = ngrad + gamma ddir; partial Re<ddir, ngrad>; then the descent check (:113-116).
 __global__ void k_ddir(uint64_t n, const float2* __restrict__ ngrad, float2* __restrict__ ddir, double* part, int nb,
-                       unsigned* counter, double* sc, uint32_t* fl) {
+                       unsigned* counter, double* sc, uint32_t* fl, int pstride) {
+  {
+    const uint64_t o = (uint64_t)blockIdx.y * n;
+    ngrad += o; ddir += o;
+    part += (size_t)blockIdx.y * pstride; counter += blockIdx.y;
+    sc += (size_t)blockIdx.y * S_NSCAL; fl += (size_t)blockIdx.y * F_NFLAG;
+  }
   if (fl[F_DONE]) return;
   const float gm = (float)sc[S_GAMMA];
   double a = 0.0;
@@ -264,7 +294,13 @@ __global__ void k_ddir(uint64_t n, const float2* __restrict__ ngrad, float2* __r
 // which this kernel does not write.
 __global__ void k_ddir_quad(PenDev R, const float2* __restrict__ ngrad, const float2* __restrict__ ddir_prev,
                             float2* __restrict__ ddir, const float2* __restrict__ x, double* part, int nb,
-                            unsigned* counter, double* sc, uint32_t* fl) {
+                            unsigned* counter, double* sc, uint32_t* fl, int pstride) {
+  {
+    const uint64_t o = (uint64_t)blockIdx.y * R.N;
+    ngrad += o; ddir_prev += o; ddir += o; x += o;
+    part += (size_t)blockIdx.y * pstride; counter += blockIdx.y;
+    sc += (size_t)blockIdx.y * S_NSCAL; fl += (size_t)blockIdx.y * F_NFLAG;
+  }
   if (fl[F_DONE]) return;
   const float gm = (float)sc[S_GAMMA];
   double v[4] = {0.0, 0.0, 0.0, 0.0};
@@ -321,7 +357,13 @@ __device__ __forceinline__ void newton_quad_steps(double beta, double* sc, uint3
 // dAWAd = Re<Adir, W Adir>, dAWr = Re(Adir' r) (:123-125).
 __global__ void k_daw(uint64_t n, const float2* __restrict__ Adir, const float* __restrict__ W,
                       const float2* __restrict__ r, double* part, int nb, unsigned* counter, double* sc,
-                      uint32_t* fl, int quad, double beta) {
+                      uint32_t* fl, int quad, double beta, int pstride) {
+  {
+    const uint64_t o = (uint64_t)blockIdx.y * n;
+    Adir += o; W += o; r += o;
+    part += (size_t)blockIdx.y * pstride; counter += blockIdx.y;
+    sc += (size_t)blockIdx.y * S_NSCAL; fl += (size_t)blockIdx.y * F_NFLAG;
+  }
   if (fl[F_DONE]) return;
   double a = 0.0, b = 0.0;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -359,7 +401,13 @@ __global__ void k_daw(uint64_t n, const float2* __restrict__ Adir, const float* 
 // One Newton step at z = x + step*ddir (:132-150): pdenom = sum_dims sum
 // wpot(Cd z) |Cd ddir|^2, pdot = Re<ddir, Gradient(z)>, then the step update.
 __global__ void k_newton(PenDev R, const float2* __restrict__ x, const float2* __restrict__ ddir, double beta,
-                         double* part, int nb, unsigned* counter, double* sc, uint32_t* fl) {
+                         double* part, int nb, unsigned* counter, double* sc, uint32_t* fl, int pstride) {
+  {
+    const uint64_t o = (uint64_t)blockIdx.y * R.N;
+    x += o; ddir += o;
+    part += (size_t)blockIdx.y * pstride; counter += blockIdx.y;
+    sc += (size_t)blockIdx.y * S_NSCAL; fl += (size_t)blockIdx.y * F_NFLAG;
+  }
   if (fl[F_DONE]) return;
   const float st = (float)sc[S_STEP];
   double a = 0.0, b = 0.0;
@@ -393,6 +441,12 @@ __global__ void k_newton(PenDev R, const float2* __restrict__ x, const float2* _
 __global__ void k_update(uint64_t ni, uint64_t nd, float2* __restrict__ x, const float2* __restrict__ ddir,
                          float2* __restrict__ Ax, const float2* __restrict__ Adir, const float2* __restrict__ y,
                          const float* __restrict__ W, float2* __restrict__ r, const double* sc, uint32_t* fl) {
+  {
+    const uint64_t oi = (uint64_t)blockIdx.y * ni, od = (uint64_t)blockIdx.y * nd;
+    x += oi; ddir += oi;
+    Ax += od; Adir += od; y += od; W += od; r += od;
+    sc += (size_t)blockIdx.y * S_NSCAL; fl += (size_t)blockIdx.y * F_NFLAG;
+  }
   if (fl[F_DONE]) return;
   const float st = (float)sc[S_STEP];
   const uint64_t n = ni > nd ? ni : nd;
@@ -415,7 +469,10 @@ __global__ void k_update(uint64_t ni, uint64_t nd, float2* __restrict__ x, const
   }
 }
 
-__global__ void k_copy_iters(const uint32_t* fl, uint32_t* out) { *out = fl[F_COMPLETED]; }
+// Completed iterations of each segment (out: nseg values).
+__global__ void k_copy_iters(const uint32_t* fl, int nseg, uint32_t* out) {
+  for (int g = threadIdx.x; g < nseg; g += blockDim.x) out[g] = fl[(size_t)g * F_NFLAG + F_COMPLETED];
+}
 
 // One element per thread up to 4 blocks per SM, then grid-stride: small
 // vectors still spread over many SMs, large ones keep the partial count low.
@@ -441,7 +498,9 @@ PenDev make_pen(const pg_penalty& R) {
 
 struct Solver {
   pg_op A;
-  uint64_t nd, ni;
+  uint64_t nd, ni;      // per-segment data and image lengths
+  int nseg = 1;         // independent problems stacked in the vectors
+  int pstride = 0;      // doubles of partial sums per segment
   PenDev R;
   double beta;
   DevBuf<float2> x, Ax, r, ngrad, ddir, Adir, ddir_prev;
@@ -455,23 +514,24 @@ struct Solver {
 
   // One PCG iteration; r = W (.) (y - Ax) holds on entry and on exit.
   pg_status iteration(cudaStream_t s) {
-    const unsigned gd = (unsigned)nbd, gi = (unsigned)nbi;
+    const dim3 gd((unsigned)nbd, (unsigned)nseg), gi((unsigned)nbi, (unsigned)nseg);
     const bool quad = R.kind == 0;
     PG_TRY(A->adjoint(r.p, ngrad.p, s));
     PG_LAUNCH(k_ngrad, gi, kRed, 0, s, R, x.p, ngrad.p, part.p, nbi, counter.p, sc.p, fl.p, ddir.p,
-              quad ? ddir_prev.p : nullptr);
+              quad ? ddir_prev.p : nullptr, pstride);
     if (quad)
       PG_LAUNCH(k_ddir_quad, gi, kRed, 0, s, R, ngrad.p, ddir_prev.p, ddir.p, x.p, part.p, nbi, counter.p, sc.p,
-                fl.p);
+                fl.p, pstride);
     else
-      PG_LAUNCH(k_ddir, gi, kRed, 0, s, ni, ngrad.p, ddir.p, part.p, nbi, counter.p, sc.p, fl.p);
+      PG_LAUNCH(k_ddir, gi, kRed, 0, s, ni, ngrad.p, ddir.p, part.p, nbi, counter.p, sc.p, fl.p, pstride);
     PG_TRY(A->forward(ddir.p, Adir.p, s));
-    PG_LAUNCH(k_daw, gd, kRed, 0, s, nd, Adir.p, W, r.p, part.p, nbd, counter.p, sc.p, fl.p, quad ? 1 : 0, beta);
+    PG_LAUNCH(k_daw, gd, kRed, 0, s, nd, Adir.p, W, r.p, part.p, nbd, counter.p, sc.p, fl.p, quad ? 1 : 0, beta,
+              pstride);
     if (!quad)
       for (int k = 0; k < 3; ++k)
-        PG_LAUNCH(k_newton, gi, kRed, 0, s, R, x.p, ddir.p, beta, part.p, nbi, counter.p, sc.p, fl.p);
-    PG_LAUNCH(k_update, (unsigned)red_blocks(std::max(nd, ni)), kRed, 0, s, ni, nd, x.p, ddir.p, Ax.p, Adir.p, y, W,
-              r.p, sc.p, fl.p);
+        PG_LAUNCH(k_newton, gi, kRed, 0, s, R, x.p, ddir.p, beta, part.p, nbi, counter.p, sc.p, fl.p, pstride);
+    PG_LAUNCH(k_update, dim3((unsigned)red_blocks(std::max(nd, ni)), (unsigned)nseg), kRed, 0, s, ni, nd, x.p,
+              ddir.p, Ax.p, Adir.p, y, W, r.p, sc.p, fl.p);
     return PG_OK;
   }
 };
@@ -523,29 +583,32 @@ struct PcgCache : pg_pcg_cache_base {
 pg_status make_cache(pg_op_s* A, const pg_penalty& Rh, bool w_ones, std::unique_ptr<PcgCache>* out, cudaStream_t s) {
   auto c = std::make_unique<PcgCache>();
   Solver& S = c->S;
+  const uint64_t g = A->n_seg ? A->n_seg : 1;
   S.A = A;
-  S.nd = A->n_data;
-  S.ni = A->n_image;
+  S.nseg = (int)g;
+  S.nd = A->n_data / g;
+  S.ni = A->n_image / g;
   S.R = make_pen(Rh);
   S.beta = Rh.beta;
   S.nbd = red_blocks(S.nd);
   S.nbi = red_blocks(S.ni);
   const int nb = std::max(S.nbd, S.nbi);
-  PG_TRY(S.x.alloc(S.ni));
-  PG_TRY(S.Ax.alloc(S.nd));
-  PG_TRY(S.r.alloc(S.nd));
-  PG_TRY(S.ngrad.alloc(S.ni));
-  PG_TRY(S.ddir.alloc(S.ni));
-  if (Rh.kind == PG_PENALTY_QUAD) PG_TRY(S.ddir_prev.alloc(S.ni));
-  PG_TRY(S.Adir.alloc(S.nd));
-  PG_TRY(S.part.alloc(4 * (uint64_t)nb));
-  PG_TRY(S.sc.alloc(S_NSCAL));
-  PG_TRY(S.fl.alloc(F_NFLAG));
-  PG_TRY(S.counter.alloc(1));
-  PG_CUDA(cudaMemsetAsync(S.counter.p, 0, sizeof(unsigned), s));
-  PG_TRY(c->ybuf.alloc(S.nd));
-  PG_TRY(c->wbuf.alloc(S.nd));
-  if (w_ones) PG_LAUNCH(k_fill_ones, ceil_div(S.nd, 256), 256, 0, s, S.nd, c->wbuf.p);
+  S.pstride = 4 * nb;
+  PG_TRY(S.x.alloc(A->n_image));
+  PG_TRY(S.Ax.alloc(A->n_data));
+  PG_TRY(S.r.alloc(A->n_data));
+  PG_TRY(S.ngrad.alloc(A->n_image));
+  PG_TRY(S.ddir.alloc(A->n_image));
+  if (Rh.kind == PG_PENALTY_QUAD) PG_TRY(S.ddir_prev.alloc(A->n_image));
+  PG_TRY(S.Adir.alloc(A->n_data));
+  PG_TRY(S.part.alloc((uint64_t)S.pstride * g));
+  PG_TRY(S.sc.alloc(S_NSCAL * g));
+  PG_TRY(S.fl.alloc(F_NFLAG * g));
+  PG_TRY(S.counter.alloc(g));
+  PG_CUDA(cudaMemsetAsync(S.counter.p, 0, g * sizeof(unsigned), s));
+  PG_TRY(c->ybuf.alloc(A->n_data));
+  PG_TRY(c->wbuf.alloc(A->n_data));
+  if (w_ones) PG_LAUNCH(k_fill_ones, ceil_div(A->n_data, 256), 256, 0, s, A->n_data, c->wbuf.p);
   S.y = c->ybuf.p;
   S.W = c->wbuf.p;
   c->R = Rh;
@@ -564,10 +627,11 @@ pg_status pcg_solve_device(pg_op_s* A, const float2* x0, const float* W, const f
                            uint64_t niter, float2* xout, uint32_t* iters_dev, cudaStream_t s,
                            const std::atomic<bool>* cancel, bool resume) {
   const uint64_t ni = A->n_image, nd = A->n_data;
-  if (Rh.nx * Rh.ny * Rh.nz != ni)
+  const uint64_t nseg = A->n_seg ? A->n_seg : 1;
+  if (Rh.nx * Rh.ny * Rh.nz * nseg != ni)
     return set_error(PG_INVALID_ARG, "penalty size %llux%llux%llu does not match the image length %llu",
                      (unsigned long long)Rh.nx, (unsigned long long)Rh.ny, (unsigned long long)Rh.nz,
-                     (unsigned long long)ni);
+                     (unsigned long long)(ni / nseg));
   if (Rh.kind != PG_PENALTY_QUAD && Rh.kind != PG_PENALTY_TV) return set_error(PG_INVALID_ARG, "unknown penalty");
   if (Rh.kind == PG_PENALTY_TV && !(Rh.delta > 0)) return set_error(PG_INVALID_ARG, "TV penalty needs delta > 0");
 
@@ -604,9 +668,9 @@ pg_status pcg_solve_device(pg_op_s* A, const float2* x0, const float* W, const f
   if (x0) st = A->forward(S.x.p, S.Ax.p, s);
   else PG_CUDA(cudaMemsetAsync(S.Ax.p, 0, nd * sizeof(float2), s));
   if (st != PG_OK) { A->pcg_cache.reset(); return st; }
-  PG_LAUNCH(k_ywy, (unsigned)S.nbd, kRed, 0, s, nd, S.y, S.W, S.part.p, S.nbd);
-  PG_LAUNCH(k_scalar_init, 1, 32, 0, s, S.part.p, S.nbd, S.sc.p, S.fl.p);
-  PG_LAUNCH(k_residual, (unsigned)S.nbd, kRed, 0, s, nd, S.y, S.Ax.p, S.W, S.r.p);
+  PG_LAUNCH(k_ywy, dim3((unsigned)S.nbd, (unsigned)S.nseg), kRed, 0, s, S.nd, S.y, S.W, S.part.p, S.nbd, S.pstride);
+  PG_LAUNCH(k_scalar_init, (unsigned)S.nseg, 32, 0, s, S.part.p, S.nbd, S.pstride, S.sc.p, S.fl.p);
+  PG_LAUNCH(k_residual, dim3((unsigned)S.nbd, (unsigned)S.nseg), kRed, 0, s, S.nd, S.y, S.Ax.p, S.W, S.r.p);
   return pcg_iterate(A, cache, niter, xout, iters_dev, s, cancel);
 }
 
@@ -672,7 +736,7 @@ pg_status pcg_iterate(pg_op_s* A, PcgCache* cache, uint64_t niter, float2* xout,
     }
   }
   PG_CUDA(cudaMemcpyAsync(xout, S.x.p, ni * sizeof(float2), cudaMemcpyDeviceToDevice, s));
-  if (iters_dev) PG_LAUNCH(k_copy_iters, 1, 1, 0, s, S.fl.p, iters_dev);
+  if (iters_dev) PG_LAUNCH(k_copy_iters, 1, 32, 0, s, S.fl.p, S.nseg, iters_dev);
   if (cancel && cancel->load()) {
     PG_CUDA(cudaStreamSynchronize(s));
     return set_error(PG_CANCELLED, "solve cancelled");
@@ -943,7 +1007,7 @@ pg_status pg_pcg_solve(pg_op A, const float* x0, const float* W, const float* y,
   if (x0) PG_TRY(A->hx0.upload(reinterpret_cast<const float2*>(x0), A->n_image, s));
   if (W) PG_TRY(A->hw.upload(W, A->n_data, s));
   PG_TRY(A->hx.alloc(A->n_image));
-  PG_TRY(A->hit.alloc(1));
+  PG_TRY(A->hit.alloc(A->n_seg ? A->n_seg : 1));   // one count per segment; the first is reported
   PG_TRY(pcg_solve_device(A, x0 ? A->hx0.p : nullptr, W ? A->hw.p : nullptr, A->hy.p, *R, niter, A->hx.p, A->hit.p,
                           s));
   PG_CUDA(cudaMemcpyAsync(x_out, A->hx.p, A->n_image * sizeof(float2), cudaMemcpyDeviceToHost, s));
@@ -994,6 +1058,7 @@ pg_status pg_pcg_state_size(pg_op A, uint64_t* bytes) {
   if (!A || !bytes) return set_error(PG_INVALID_ARG, "pcg state: null argument");
   auto* c = dynamic_cast<PcgCache*>(A->pcg_cache.get());
   if (!c) return set_error(PG_INVALID_ARG, "pcg state: no solve has run on this operator");
+  if (c->S.nseg > 1) return set_error(PG_INVALID_ARG, "pcg state: operators of several segments are not saved");
   *bytes = state_bytes(A->n_image, A->n_data, c->S.ddir_prev.p != nullptr);
   return PG_OK;
 }
@@ -1040,6 +1105,7 @@ pg_status pg_pcg_state_save(pg_op A, void* host, uint64_t bytes) {
 
 pg_status pg_pcg_state_load(pg_op A, const pg_penalty* R, const void* host, uint64_t bytes) {
   if (!A || !R || !host) return set_error(PG_INVALID_ARG, "pcg state: null argument");
+  if (A->n_seg > 1) return set_error(PG_INVALID_ARG, "pcg state: operators of several segments are not loaded");
   PcgStateHeader h{};
   if (bytes < sizeof(h)) return set_error(PG_INVALID_ARG, "pcg state: %llu bytes", (unsigned long long)bytes);
   std::memcpy(&h, host, sizeof(h));

@@ -2,14 +2,19 @@
 //
 // The reference drivers reconstruct one slice/echo/repetition after another
 // (PowerGridIsmrmrd.cpp:191-264), each with its own Gnufft, TimeSegmentation,
-// SENSE and reconSolve.  Here each slice of a request is a job; jobs are
-// admitted in FIFO order whenever a worker slot is free and the summed
-// device footprint of resident jobs stays within the HBM budget.  Every
-// worker owns a CUDA stream, so admitted jobs overlap on the GPU, and a job
-// that finishes frees its slot and memory for the next arrival.  A job keeps
-// its trajectory, maps and PCG state resident in a private device arena
-// (stream-ordered pool allocations, no cudaMalloc/cudaFree on the hot path)
-// until its image is copied out.
+// SENSE and reconSolve.  Here the slices of a request, which share the
+// trajectory, the segment windows and the sample binning, are batched: a job
+// is a run of a request's slices (all of them, or as many as fit the HBM
+// budget) solved as ONE stacked operator — every gridding launch carries the
+// coils of all its slices — and one PCG whose inner products, step sizes and
+// early exits are kept per slice (SliceBatchOp, pg_pcg.cu segments), so each
+// slice's image is the one its own solve gives.  Jobs are admitted in FIFO
+// order whenever a worker slot is free and the summed device footprint of
+// resident jobs stays within the budget.  Every worker owns a CUDA stream, so
+// admitted jobs overlap on the GPU, and a job that finishes frees its slot and
+// memory for the next arrival.  A job keeps its trajectory, maps and PCG state
+// resident in a private device arena (stream-ordered pool allocations, no
+// cudaMalloc/cudaFree on the hot path) until its images are copied out.
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -57,7 +62,8 @@ struct Ticket {
   pg_status shared_st = PG_OK;
   std::unique_ptr<SharedPlan> shared;
   pg_request req{};
-  uint64_t footprint = 0;
+  uint64_t footprint = 0;        // one slice (admission check at submit)
+  uint64_t slices_per_job = 1;
   int jobs_total = 0;
   int jobs_left = 0;
   int jobs_started = 0;
@@ -68,7 +74,9 @@ struct Ticket {
 
 struct Job {
   std::shared_ptr<Ticket> t;
-  uint64_t slice = 0;
+  uint64_t slice = 0;            // first slice
+  uint64_t count = 1;            // slices
+  uint64_t footprint = 0;
 };
 
 uint64_t grid_cells(const pg_request& r) {
@@ -98,7 +106,8 @@ void release_shared(std::unique_ptr<SharedPlan>& sp) { sp.reset(); }
 
 }  // namespace
 
-uint64_t request_footprint(const pg_request& r) {
+// Device bytes of a job of k slices of request r.
+uint64_t job_footprint(const pg_request& r, uint64_t k) {
   const uint64_t M = r.n_samples, N = r.nx * r.ny * r.nz, C = r.nc;
   const uint64_t L = r.L <= 1 ? 1 : r.L;
   const uint64_t G = grid_cells(r);
@@ -107,15 +116,17 @@ uint64_t request_footprint(const pg_request& r) {
   b += 3 * M * 4 + 40000 * 4 + (r.nx + r.ny + r.nz) * 4;          // trajectory, LUT, deapodization
   b += M * (8 + 64 + (d3 ? 32 : 0) + 4 + 4);                        // binning temporaries
   b += M * (4 + 8 + 64 + (d3 ? 32 : 0) + 4 + 3 * 8) + (M / 64 + 4096 * L) * 16;  // binning
-  uint64_t grids = C * L * G * 8;
+  uint64_t grids = k * C * L * G * 8;
   if (grids > kJobGridBytes) grids = std::max<uint64_t>(L * G * 8, (kJobGridBytes / (L * G * 8)) * L * G * 8);
-  b += 3 * grids;                                                   // grids, forward input, cuFFT work area
-  b += C * M * 8 * std::min<uint64_t>(L, 3);                        // adjoint segment values (Hanning: K <= 3)
-  b += 2 * L * N * 8 + C * N * 8;                                   // Wo, WoH, coil maps
-  b += 3 * N * 8 + 3 * C * M * 8 + C * M * 8 + C * M * 4 + 64 * 1024;  // PCG state
-  b += C * M * 8 + N * 8;                                           // job input / output
+  b += 3 * grids;                                                   // grids, FFT input / adjoint grids, cuFFT work area
+  b += k * C * M * 8 * std::min<uint64_t>(L, 3);                    // adjoint segment values (Hanning: K <= 3)
+  b += k * (2 * L * N * 8 + C * N * 8);                             // Wo, WoH, coil maps
+  b += k * (3 * N * 8 + 3 * C * M * 8 + C * M * 8 + C * M * 4) + 64 * 1024;  // PCG state
+  b += k * (C * M * 8 + N * 8);                                     // job input / output
   return b + b / 4 + (32ull << 20);
 }
+
+uint64_t request_footprint(const pg_request& r) { return job_footprint(r, 1); }
 
 }  // namespace pg
 
@@ -137,7 +148,7 @@ struct pg_server_s {
 
   bool head_fits() const {
     if (pending.empty()) return false;
-    const uint64_t f = pending.front().t->footprint;
+    const uint64_t f = pending.front().footprint;
     return used + f <= cfg.hbm_budget_bytes || running == 0;
   }
 
@@ -165,44 +176,47 @@ struct pg_server_s {
   pg_status run_job(const Job& j, cudaStream_t s, uint64_t* iters, double* setup_ms, double* solve_ms) {
     const pg_request& r = j.t->req;
     const uint64_t N = r.nx * r.ny * r.nz, M = r.n_samples, C = r.nc;
-    const uint64_t sl = j.slice;
+    const uint64_t sl = j.slice, ns = j.count;
     const double t0 = now_ms();
     double t1 = t0;
     Ticket& T = *j.t;
     std::call_once(T.shared_once, [&] { T.shared_st = build_shared(T, s); });
     if (T.shared_st != PG_OK) return T.shared_st;
     Arena arena;
-    PG_TRY(arena_open(&arena, j.t->footprint, s));
+    PG_TRY(arena_open(&arena, j.footprint, s));
     arena_install(&arena);
     pg_status st = PG_OK;
     {
       std::unique_ptr<GnufftOp> G;
-      std::unique_ptr<TimeSegOp> A;
-      std::unique_ptr<SenseOp> S;
+      std::unique_ptr<SliceBatchOp> A;
       DevBuf<float2> y, x;
       DevBuf<uint32_t> it;
+      std::vector<uint32_t> n(ns, 0);
       do {
         st = make_gnufft_shared(&G, *T.shared->G);
         if (st != PG_OK) break;
         G->plan->budget_bytes = kJobGridBytes;
-        st = make_timeseg_shared(&A, G.get(), *T.shared->A, r.field_map + sl * N, s);
+        // the job's slices as one operator: their coils share every gridding launch
+        st = make_slice_batch(&A, G.get(), T.shared->A.get(), ns, C, r.field_map + sl * N,
+                              r.sense_map + 2 * sl * N * C, s);
         if (st != PG_OK) break;
-        st = make_sense(&S, A.get(), r.sense_map + 2 * sl * N * C, M, N, C, s);
+        st = y.upload(reinterpret_cast<const float2*>(r.data) + sl * M * C, ns * M * C, s);
         if (st != PG_OK) break;
-        st = y.upload(reinterpret_cast<const float2*>(r.data) + sl * M * C, M * C, s);
-        if (st != PG_OK) break;
-        if ((st = x.alloc(N)) != PG_OK) break;
-        if ((st = it.alloc(1)) != PG_OK) break;
+        if ((st = x.alloc(ns * N)) != PG_OK) break;
+        if ((st = it.alloc(ns)) != PG_OK) break;
         pg_penalty R{PG_PENALTY_QUAD, r.nx, r.ny, r.nz, r.beta, 1.0f, 3};
         t1 = now_ms();
-        st = pcg_solve_device(S.get(), nullptr, nullptr, y.p, R, r.niter, x.p, it.p, s, &j.t->cancel);
+        // one PCG over the stack, inner products and steps per slice
+        st = pcg_solve_device(A.get(), nullptr, nullptr, y.p, R, r.niter, x.p, it.p, s, &j.t->cancel);
         if (st != PG_OK) break;
-        uint32_t n = 0;
-        cudaError_t e = cudaMemcpyAsync(r.image_out + 2 * sl * N, x.p, N * sizeof(float2), cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(&n, it.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+        cudaError_t e = cudaMemcpyAsync(r.image_out + 2 * sl * N, x.p, ns * N * sizeof(float2), cudaMemcpyDeviceToHost,
+                                        s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(n.data(), it.p, ns * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) { cudaGetLastError(); st = set_error(PG_CUDA_ERROR, "job copy-out: %s", cudaGetErrorString(e)); break; }
-        *iters = n;
+        uint64_t tot = 0;
+        for (uint32_t v : n) tot += v;
+        *iters = tot;
       } while (0);
       cudaStreamSynchronize(s);
       // operators and buffers release into the arena (no-ops) before it is returned
@@ -229,7 +243,7 @@ struct pg_server_s {
         if (stop) break;
         job = pending.front();
         pending.pop_front();
-        used += job.t->footprint;
+        used += job.footprint;
         ++running;
         if (job.t->jobs_started++ == 0) job.t->st.t_start_ms = now_ms();
       }
@@ -245,7 +259,7 @@ struct pg_server_s {
                      (unsigned long long)job.slice, pg_last_error());
       {
         std::lock_guard<std::mutex> lk(mu);
-        used -= job.t->footprint;
+        used -= job.footprint;
         --running;
         Ticket& t = *job.t;
         t.st.iters_done += iters;
@@ -329,14 +343,21 @@ pg_status pg_submit(pg_server sv, const pg_request* r, uint64_t* ticket) {
   if (t->footprint > sv->cfg.hbm_budget_bytes)
     return set_error(PG_REJECTED, "request needs %llu bytes per slice, budget is %llu",
                      (unsigned long long)t->footprint, (unsigned long long)sv->cfg.hbm_budget_bytes);
-  t->jobs_total = t->jobs_left = (int)t->req.n_slices;
+  // slices per job: all of the request's, or as many as fit the budget
+  uint64_t k = t->req.n_slices;
+  while (k > 1 && job_footprint(t->req, k) > sv->cfg.hbm_budget_bytes) k = (k + 1) / 2;
+  t->slices_per_job = k;
+  t->jobs_total = t->jobs_left = (int)((t->req.n_slices + k - 1) / k);
   {
     std::lock_guard<std::mutex> lk(sv->mu);
     if (sv->stop) return set_error(PG_CANCELLED, "server is shutting down");
     t->id = sv->next++;
     t->st.t_submit_ms = now_ms();
     sv->tickets[t->id] = t;
-    for (uint64_t sl = 0; sl < t->req.n_slices; ++sl) sv->pending.push_back(Job{t, sl});
+    for (uint64_t sl = 0; sl < t->req.n_slices; sl += k) {
+      const uint64_t cnt = std::min<uint64_t>(k, t->req.n_slices - sl);
+      sv->pending.push_back(Job{t, sl, cnt, job_footprint(t->req, cnt)});
+    }
     *ticket = t->id;
   }
   sv->cv_work.notify_all();
