@@ -344,8 +344,12 @@ typedef struct pg_server_config {
 /* A time-segmented SENSE reconstruction request:
  * SENSE<TimeSegmentation<Gnufft>> + QuadPenalty with reconSolve semantics
  * (reconSolve.h:63-82), for n_slices independent images that share one
- * trajectory (the slice loop of PowerGridIsmrmrd.cpp:191-264).  Each slice is
- * scheduled as its own job.  Arrays (host memory, valid until completion):
+ * trajectory (the slice loop of PowerGridIsmrmrd.cpp:191-264).  The slices
+ * are batched: a job is all of the request's slices (or as many as fit the
+ * HBM budget) solved as one stacked operator whose gridding launches carry
+ * every slice's coils, with one PCG that keeps its inner products, step sizes
+ * and early exits per slice, so each slice's image is that of its own solve.
+ * Arrays (host memory, valid until completion):
  *   kx, ky, kz, t   n_samples                  (k in cycles/FOV, t in s)
  *   field_map       n_slices * nx*ny*nz        (rad/s)
  *   sense_map       n_slices * nx*ny*nz*nc     (complex, coil-major per slice)
@@ -362,12 +366,13 @@ typedef struct pg_request {
 } pg_request;
 
 typedef struct pg_request_stats {
-  double t_submit_ms, t_start_ms, t_done_ms;   /* host steady clock; start = first slice admitted */
+  double t_submit_ms, t_start_ms, t_done_ms;   /* host steady clock; start = first job admitted */
   uint64_t iters_done;                         /* PCG iterations completed, all slices */
-  uint64_t bytes_resident;                     /* admission footprint of one slice job */
+  uint64_t bytes_resident;                     /* admission footprint of one slice */
   pg_status status;
-  double setup_ms;                             /* summed over slices: operator construction on the host */
-  double solve_ms;                             /* summed over slices: PCG solve and image copy-out */
+  double setup_ms;                             /* summed over jobs: operator construction */
+  double solve_ms;                             /* summed over jobs: PCG solve and image copy-out */
+  char error[160];                             /* the first failed job's message, or empty */
 } pg_request_stats;
 
 pg_status pg_server_create(pg_server* out, const pg_server_config* cfg);

@@ -44,7 +44,7 @@ class Request(C.Structure):
 class RequestStats(C.Structure):
     _fields_ = [("t_submit_ms", C.c_double), ("t_start_ms", C.c_double), ("t_done_ms", C.c_double),
                 ("iters_done", U64), ("bytes_resident", U64), ("status", C.c_int), ("setup_ms", C.c_double),
-                ("solve_ms", C.c_double)]
+                ("solve_ms", C.c_double), ("error", C.c_char * 160)]
 
 
 class Acquisition(C.Structure):

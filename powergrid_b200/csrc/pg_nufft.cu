@@ -1306,6 +1306,25 @@ static int smem_optin_bytes() {
   return v;
 }
 
+// The spread kernels' shared memory depends on the bin size, which differs
+// between plans; worker threads of the request server launch them
+// concurrently.  Raising the allowed dynamic shared memory per launch would
+// let one thread lower it between another thread's raise and launch, so it is
+// set once per kernel to the device's opt-in limit (less its static shared
+// memory), which covers every launch.
+static pg_status allow_full_dynamic_smem(const void* kernel) {
+  static std::mutex mu;
+  static std::map<const void*, bool> done;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count(kernel)) return PG_OK;
+  cudaFuncAttributes fa{};
+  PG_CUDA(cudaFuncGetAttributes(&fa, kernel));
+  const int dyn = smem_optin_bytes() - (int)fa.sharedSizeBytes;
+  PG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+  done[kernel] = true;
+  return PG_OK;
+}
+
 // Blocks of a persistent launch: as many as fit on the device at
 // once (cached per kernel and shared-memory size), at most one per item.
 static int persistent_blocks(const void* kernel, size_t smem, int nitems) {
@@ -1396,7 +1415,7 @@ struct SpreadArgs {
 template <int DIM, int T, int NP>
 static pg_status spread_launch_np(NufftPlan* p, const Binning* bin, const SpreadArgs& a, float2* target,
                                   cudaStream_t s) {
-  PG_CUDA(cudaFuncSetAttribute(k_spread<DIM, T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.smem));
+  PG_TRY(allow_full_dynamic_smem((const void*)k_spread<DIM, T, NP>));
   const int nitems = bin->nsub * a.nchunks;
   PG_TRY(ensure_queue(p, s));
   const int blocks = persistent_blocks((const void*)k_spread<DIM, T, NP>, a.smem, nitems);
@@ -1440,7 +1459,7 @@ template <int T, int CC, int KK>
 static pg_status spread2d_launch(NufftPlan* p, const Binning* bin, const float2* aa, const float2* y,
                                  uint64_t dstride, int nb, float wmax, float2* target, cudaStream_t s) {
   const size_t smem = spread2d_smem(T, CC * KK, bin->submax);
-  PG_CUDA(cudaFuncSetAttribute(k_spread2d<T, CC, KK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  PG_TRY(allow_full_dynamic_smem((const void*)k_spread2d<T, CC, KK>));
   const int nchunks = (nb + CC - 1) / CC;
   const int nitems = bin->nsub * nchunks;
   PG_TRY(ensure_queue(p, s));

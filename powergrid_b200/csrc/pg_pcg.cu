@@ -700,19 +700,24 @@ pg_status pcg_iterate(pg_op_s* A, PcgCache* cache, uint64_t niter, float2* xout,
         // the capture pass counted launches that never ran
         cache->per_iter = g_launches.load() - before;
         g_launches.fetch_sub(cache->per_iter);
-        if (st != PG_OK || ce != cudaSuccess) {
+        if (st != PG_OK) {
           if (graph) cudaGraphDestroy(graph);
           cudaGetLastError();
           A->pcg_cache.reset();
-          return st != PG_OK ? st : set_error(PG_CUDA_ERROR, "graph capture: %s", cudaGetErrorString(ce));
+          return st;
         }
         cudaGraphExec_t exec = nullptr;
-        ce = cudaGraphInstantiate(&exec, graph, 0);
+        if (ce == cudaSuccess) ce = cudaGraphInstantiate(&exec, graph, 0);
         if (ce != cudaSuccess) {
-          cudaGraphDestroy(graph);
+          // The capture or its instantiation failed; the captured work never
+          // ran, so the state is the one after the eager iteration: go on
+          // without graphs (same kernels, launched one by one).
+          if (graph) cudaGraphDestroy(graph);
           cudaGetLastError();
-          A->pcg_cache.reset();
-          return set_error(PG_CUDA_ERROR, "graph instantiate: %s", cudaGetErrorString(ce));
+          if (cache->exec) { cudaGraphExecDestroy(cache->exec); cache->exec = nullptr; }
+          if (cache->graph) { cudaGraphDestroy(cache->graph); cache->graph = nullptr; }
+          cache->per_iter = 0;
+          break;
         }
         (timed ? cache->graph_timed : cache->graph) = graph;
         (timed ? cache->exec_timed : cache->exec) = exec;

@@ -255,8 +255,9 @@ struct pg_server_s {
                                      cudaGetErrorString(stale));
       pg_status st = job.t->cancel.load() ? PG_CANCELLED : run_job(job, s, &iters, &setup_ms, &solve_ms);
       if (st != PG_OK && st != PG_CANCELLED && log_errors)
-        std::fprintf(stderr, "powergrid_b200 server: request %llu slice %llu: %s\n", (unsigned long long)job.t->id,
-                     (unsigned long long)job.slice, pg_last_error());
+        std::fprintf(stderr, "powergrid_b200 server: request %llu slices %llu-%llu: %s\n",
+                     (unsigned long long)job.t->id, (unsigned long long)job.slice,
+                     (unsigned long long)(job.slice + job.count - 1), pg_last_error());
       {
         std::lock_guard<std::mutex> lk(mu);
         used -= job.footprint;
@@ -265,7 +266,11 @@ struct pg_server_s {
         t.st.iters_done += iters;
         t.st.setup_ms += setup_ms;
         t.st.solve_ms += solve_ms;
-        if (st != PG_OK && t.st.status == PG_OK) t.st.status = st;
+        if (st != PG_OK && t.st.status == PG_OK) {
+          t.st.status = st;
+          std::snprintf(t.st.error, sizeof(t.st.error), "slices %llu-%llu: %s", (unsigned long long)job.slice,
+                        (unsigned long long)(job.slice + job.count - 1), pg_last_error());
+        }
         if (--t.jobs_left == 0) {
           t.st.t_done_ms = now_ms();
           if (t.cancel.load() && t.st.status == PG_OK) t.st.status = PG_CANCELLED;

@@ -106,7 +106,8 @@ class Server:
         keep, out, r = self._live[ticket]
         stats = {"t_submit_ms": st.t_submit_ms, "t_start_ms": st.t_start_ms, "t_done_ms": st.t_done_ms,
                  "iters_done": int(st.iters_done), "bytes_resident": int(st.bytes_resident),
-                 "status": _lib.STATUS.get(st.status, st.status), "setup_ms": st.setup_ms, "solve_ms": st.solve_ms}
+                 "status": _lib.STATUS.get(st.status, st.status), "setup_ms": st.setup_ms, "solve_ms": st.solve_ms,
+                 "error": st.error.decode(errors="replace")}
         return out.reshape(r.n_slices, r.nimg), stats
 
     def close(self):
