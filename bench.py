@@ -564,6 +564,96 @@ def gdft_block(steps: int, warmup: int, stream, with_error: bool = True):
     return res
 
 
+def cpu_table():
+    """The reference CPU path per configuration on this host: 1 thread and all
+    host threads (independent units on threads; ctypes releases the GIL).
+    Bounded samples, each stated: cfg1 a full 10-iteration solve; cfg2 a
+    3-iteration solve on 1 thread (the solve's start, one forward, included)
+    and a full 20-iteration solve on all threads; cfg3 the reference's float
+    ftCpu / iftCpu on 64 sample rows (forward) or 64 voxels (adjoint) of all 8
+    coils, as pairs/s; cfg5 one shot-coil-segment unit of the 3-D Gnufft
+    (forward + adjoint, 131072 samples, 256x256x128 grid) scaled to a PCG
+    iteration of 16 shots x 32 coils x 12 segments (two operator
+    applications)."""
+    import concurrent.futures as cf
+
+    import oracle as O
+    from powergrid_b200 import synthetic as S
+    nth = os.cpu_count() or 1
+    ref = O.reference_available()
+    if ref:
+        O.use_reference(True)
+    out = {"host_threads": nth, "kind": "reference" if ref else "port"}
+
+    def timed(fn):
+        t0 = time.perf_counter()
+        fn()
+        return time.perf_counter() - t0
+
+    p = S.config1()
+    o = O.build_problem_op(p, 0)
+    y = o.forward(p.x_true)
+    O.set_threads(1)
+    t1 = timed(lambda: o.pcg(y, "quad", p.nx, p.ny, 1, p.beta, niter=10))
+    out["cfg1"] = {"metric": "PCG iters/s (10 iterations)", "cpu_1thr": 10 / t1,
+                   "cpu_all": 10 / t1, "note": "one coil, no segments: no independent units to spread"}
+    p = S.config2()
+    o = O.build_problem_op(p, 0)
+    O.set_threads(nth)
+    y = o.forward(p.x_true)
+    O.set_threads(1)
+    t1 = timed(lambda: o.pcg(y, "quad", p.nx, p.ny, 1, p.beta, niter=3))
+    O.set_threads(nth)
+    ta = timed(lambda: o.pcg(y, "quad", p.nx, p.ny, 1, p.beta, niter=20))
+    out["cfg2"] = {"metric": "PCG iters/s", "cpu_1thr": 3 / t1, "cpu_all": 20 / ta,
+                   "sample": "1 thread: a 3-iteration solve; all threads: a 20-iteration solve"}
+    O.set_threads(1)
+    p = S.config3()
+    M, n = p.kx.size, p.nimg
+    ix, iy, iz = S.image_coords(p.nx, p.ny, p.nz)
+    sm = p.smap.reshape(p.nc, n)
+    rows = np.arange(0, M, M // 64)[:64]
+    vox = np.arange(0, n, n // 64)[:64]
+    fwd = O.gdft(0, p.kx[rows], p.ky[rows], p.kz[rows], ix, iy, iz, p.fm, p.t[rows])
+    adj = O.gdft(0, p.kx, p.ky, p.kz, ix[vox], iy[vox], iz[vox], p.fm[vox], p.t)
+    xs = [(sm[c] * p.x_true).astype(np.complex64) for c in range(p.nc)]
+    yv = S.image(S.Rng(7), M)
+
+    def fwd_all(pool):
+        list(pool.map(lambda c: fwd.forward(xs[c]), range(p.nc)))
+
+    def adj_all(pool):
+        list(pool.map(lambda c: adj.adjoint(yv), range(p.nc)))
+
+    g = {}
+    for label, workers in (("cpu_1thr", 1), ("cpu_all", nth)):
+        with cf.ThreadPoolExecutor(max_workers=workers) as pool:
+            tf = timed(lambda: fwd_all(pool))
+            ta = timed(lambda: adj_all(pool))
+        g[label] = {"forward_pairs_per_s": rows.size * n / tf, "adjoint_pairs_per_s": vox.size * M / ta}
+    out["cfg3"] = {"metric": "sample-voxel pairs/s per direction (8 coils per pair)", **g,
+                   "sample": "64 sample rows (forward) / 64 voxels (adjoint), all 8 coils; all threads: coils "
+                             "on threads (8 units)"}
+    p = S.config5(shots=16, nc=1, per=2048)
+    Mshot = p.kx.size // 16
+    unit = O.gnufft(0, Mshot, p.nx, p.ny, p.nz, p.kx[:Mshot], p.ky[:Mshot], p.kz[:Mshot])
+    xv = S.image(S.Rng(8), p.nimg)
+    yv = unit.forward(xv)
+    tu = timed(lambda: (unit.forward(xv), unit.adjoint(yv)))
+    units = 16 * 32 * 12
+    with cf.ThreadPoolExecutor(max_workers=nth) as pool:
+        tpar = timed(lambda: list(pool.map(lambda k: (unit.forward(xv), unit.adjoint(yv)), range(nth))))
+    out["cfg5"] = {"metric": "PCG iters/s (extrapolated)", "cpu_1thr": 1.0 / (units * tu),
+                   "cpu_all": 1.0 / (units * tpar / nth),
+                   "sample": f"one shot-coil-segment 3-D Gnufft forward+adjoint ({Mshot} samples, "
+                             f"{2 * p.nx}x{2 * p.ny}x{2 * p.nz} grid) "
+                             f"= {tu:.2f} s on 1 thread, {nth} such units concurrently in {tpar:.2f} s; x {units} "
+                             "units per iteration"}
+    if ref:
+        O.use_reference(False)
+    return out
+
+
 def run_workload(name: str, steps: int, warmup: int):
     """Secondary workloads, one JSON line each (parity cases elsewhere, measured here).
 
@@ -588,6 +678,32 @@ def run_workload(name: str, steps: int, warmup: int):
     L = _lib.load()
     stream = torch.cuda.Stream(device=dev)
     sampler = ClockSampler(0)
+    if name == "cfg1":
+        p = S.config1()
+        M, n = p.kx.size, p.nimg
+        G = pg.Gnufft(M, 2.0, p.nx, p.ny, 1, p.kx, p.ky, p.kz)
+        Sg = pg.SENSE(G, p.smap, M, n, 1)
+        R = pg.QuadPenalty(p.nx, p.ny, 1, p.beta)
+        x = torch.from_numpy(p.x_true).to(dev)
+        y = torch.empty(Sg.n_data, dtype=torch.complex64, device=dev)
+        Sg.forward(x, out=y, stream=stream)
+        xo = torch.empty(n, dtype=torch.complex64, device=dev)
+        it = torch.zeros(1, dtype=torch.int32, device=dev)
+        for _ in range(warmup):
+            pg.solve_pwls_pcg_device(Sg, y, R, p.niter, xo, iters=it, stream=stream)
+        stream.synchronize()
+        ms = []
+        with sampler:
+            for _ in range(steps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                pg.solve_pwls_pcg_device(Sg, y, R, p.niter, xo, iters=it, stream=stream)
+                e1.record(stream)
+                stream.synchronize()
+                ms.append(e0.elapsed_time(e1))
+        return {"workload": "cfg1 SENSE<Gnufft> 64x64, 1 coil, 4096 samples, QuadPenalty 1e-3, 10 PCG iterations",
+                "metric": METRIC, "unit": UNIT, "value": p.niter / (statistics.mean(ms) / 1e3),
+                "ms_per_solve": statistics.mean(ms), "steps": steps, "warmup": warmup, "clocks": sampler.summary()}
     if name == "cfg3":
         with sampler:
             res = gdft_block(steps, warmup, stream, with_error=True)
@@ -709,9 +825,12 @@ def main():
     ap.add_argument("--no-serving", action="store_true", help="skip the config-4 serving stream")
     ap.add_argument("--no-gdft", action="store_true", help="skip the config-3 Gdft block")
     ap.add_argument("--serving-only", action="store_true", help="only the config-4 serving stream")
-    ap.add_argument("--workload", default=None, choices=["cfg3", "cfg5", "direct"],
+    ap.add_argument("--workload", default=None, choices=["cfg1", "cfg3", "cfg5", "direct", "cpu"],
                     help="a secondary workload instead")
     args = ap.parse_args()
+    if args.workload == "cpu":
+        print(json.dumps(cpu_table()))
+        return 0
     if args.workload:
         print(json.dumps(run_workload(args.workload, args.steps, max(3, args.warmup))))
         return 0
