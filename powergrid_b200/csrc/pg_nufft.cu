@@ -1260,7 +1260,7 @@ static pg_status ensure_workspace(NufftPlan* p, int B, cufftHandle* h, cudaStrea
   return PG_OK;
 }
 
-// The adjoint's spread target on the own-FFT path: B zeroed grids.
+// The adjoint's spread target on the 2-D own-FFT path: B zeroed grids.
 static pg_status ensure_adjoint_grids(NufftPlan* p, int B, cudaStream_t s) {
   const uint64_t n = (uint64_t)B * p->g.ngrid();
   NufftWork& w = *p->work;
@@ -1288,9 +1288,16 @@ static pg_status ensure_forward_input(NufftPlan* p, int B, cudaStream_t s) {
   return PG_OK;
 }
 
+// The 2-D adjoint spreads into a grid set that its first inverse FFT pass
+// zeroes after reading (a full pass over contiguous rows, where the stores
+// are nearly free).  The 3-D first pass reads z columns across slabs, where
+// the same stores cost more than a separate clearing, so 3-D keeps clearing
+// the forward's grids in the adjoint preparation.
+static bool self_clearing(const NufftPlan& p) { return p.own_fft && p.g.dim == 2; }
+
 static int batch_coils(const NufftPlan* p, int C, int L) {
-  // own FFT passes: forward grids and the adjoint's spread target
-  const uint64_t per = (uint64_t)L * p->g.ngrid() * sizeof(float2) * (p->own_fft ? 2 : 1);
+  // 2-D own FFT passes: forward grids and the adjoint's self-clearing spread target
+  const uint64_t per = (uint64_t)L * p->g.ngrid() * sizeof(float2) * (self_clearing(*p) ? 2 : 1);
   uint64_t cb = per ? p->budget_bytes / per : (uint64_t)C;
   if (cb < 1) cb = 1;
   return (int)std::min<uint64_t>(cb, (uint64_t)C);
@@ -1615,11 +1622,12 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
     PG_TRY(ensure_workspace(p, B, p->own_fft ? nullptr : &h, s));
     const float2* yc = y + (uint64_t)c0 * b.data_stride;
     const float2* aa = (L > 1 || bin->aa.p) ? bin->aa.p : nullptr;
-    // spread target: on the own FFT passes a grid set kept zero between
-    // adjoints (its first inverse pass clears it); else the cuFFT grids,
+    // spread target: on the 2-D own FFT passes a grid set kept zero between
+    // adjoints (its first inverse pass clears it); else the forward's grids,
     // cleared here
+    const bool self_clear = self_clearing(*p);
     float2* target = p->work->grids.p;
-    if (p->own_fft) {
+    if (self_clear) {
       PG_TRY(ensure_adjoint_grids(p, B, s));
       target = p->work->agrids.p;
     }
@@ -1628,7 +1636,7 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
     // timed as one stage (with the grids' clearing where it is a separate step)
     ProfScope pag("adjoint_gridding", s);
     if (folded) {
-      if (!p->own_fft) {
+      if (!self_clear) {
         ProfScope ps("prep", s);
         PG_CUDA(cudaMemsetAsync(target, 0, (size_t)B * G * sizeof(float2), s));
       }
@@ -1642,8 +1650,8 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
     PG_TRY(grow(p->work->vs, (uint64_t)nb * bin->M * K, s));
     {
       ProfScope ps("prep", s);
-      // the own-FFT target is already zero: only the values are formed
-      const uint64_t n4 = p->own_fft ? 0 : (uint64_t)B * G / 2;   // G is even: float2 pairs -> float4 words
+      // a self-clearing target is already zero: only the values are formed
+      const uint64_t n4 = self_clear ? 0 : (uint64_t)B * G / 2;   // G is even: float2 pairs -> float4 words
       const uint64_t work = std::max<uint64_t>(n4, bin->M);
       PG_LAUNCH(k_adjoint_prep, (unsigned)std::min<uint64_t>(ceil_div(work, 256), 8ull * sm_count()), 256, 0, s, n4,
                 reinterpret_cast<float4*>(target), nb, bin->M, K, bin->perm.p, aa, yc, b.data_stride,
@@ -1676,16 +1684,16 @@ pg_status nufft_adjoint(NufftPlan* p, const NufftBatch& b, const float2* y, floa
           const int img = i0 / b.cgroup;
           const int i1 = std::min(c0 + nb, (img + 1) * b.cgroup);
           const int acc_img = (b.accumulate || i0 > img * b.cgroup) ? 1 : 0;
-          PG_TRY(fftpass_adjoint(g, (i1 - i0) * L, L, target + (uint64_t)(i0 - c0) * L * G, 1, b.S, i0, b.E,
+          PG_TRY(fftpass_adjoint(g, (i1 - i0) * L, L, target + (uint64_t)(i0 - c0) * L * G, self_clear, b.S, i0, b.E,
                                  b.WoH ? b.WoH + (uint64_t)img * b.phase_stride : nullptr, p->deapf.p, p->tw2d.p,
                                  p->work->fin.p, p->work->rimg.p, acc_img, x + (uint64_t)img * b.image_stride, s));
           i0 = i1;
         }
       } else {
-        PG_TRY(fftpass_adjoint(g, B, L, target, 1, b.S, c0, b.E, b.WoH, p->deapf.p, p->tw2d.p, p->work->fin.p,
-                               p->work->rimg.p, acc, x, s));
+        PG_TRY(fftpass_adjoint(g, B, L, target, self_clear, b.S, c0, b.E, b.WoH, p->deapf.p, p->tw2d.p,
+                               p->work->fin.p, p->work->rimg.p, acc, x, s));
       }
-      p->work->agrids_clean = true;   // the first inverse pass leaves the target zero
+      if (self_clear) p->work->agrids_clean = true;   // the first inverse pass leaves the target zero
       continue;
     }
     {

@@ -68,7 +68,7 @@ struct Binning {
 // to back on one stream (the shots of pcSenseTimeSeg) share a single one.
 struct NufftWork {
   DevBuf<float2> grids;     // FFT output (forward) / spread target (adjoint, cuFFT path)
-  // Spread target of the adjoint on the plan's own FFT passes.  It is zero
+  // Spread target of the 2-D adjoint on the plan's own FFT passes.  It is zero
   // at the start of every adjoint: zeroed when allocated, and the first
   // inverse FFT pass zeroes each cell after reading it.  agrids_clean is
   // false from the spread until that pass is enqueued, so an adjoint that
