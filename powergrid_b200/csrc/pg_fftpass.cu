@@ -336,34 +336,43 @@ __global__ void __launch_bounds__(kT) k_fft_fwd_cols(Lines ln, const float2* __r
 
 // Inverse strided lines: per column, all n rows, inverse FFT along the line,
 // keep the nio rows at off + i -> row i of the output.  Every input cell is
-// read exactly once; with clear set it is zeroed after that read, which
-// leaves the input grids zero for the next adjoint spread.
-template <int LOGN>
-__global__ void __launch_bounds__(kT) k_fft_inv_cols(Lines ln, float2* in, int clear,
+// read exactly once; with CLEAR it is zeroed after that read (through inw,
+// the same grids), which leaves them zero for the next adjoint spread;
+// without it the input is read-only (in).
+template <int LOGN, bool CLEAR>
+__global__ void __launch_bounds__(kT) k_fft_inv_cols(Lines ln, const float2* __restrict__ in, float2* inw,
                                                      const float2* __restrict__ tw, float2* __restrict__ Q) {
   using CG = ColGeo<LOGN>;
   constexpr int R1 = CG::R1, R2 = CG::R2, CB = CG::CB;
   extern __shared__ float2 sh[];
   const int b = blockIdx.y, c0 = blockIdx.x * CB;
-  float2* pin = in + (uint64_t)b * ln.in_bstride;
 #pragma unroll
   for (int it0 = 0; it0 < CB * R2; it0 += kT) {
     const int it = it0 + threadIdx.x;
     if ((CB * R2) % kT != 0 && it >= CB * R2) break;
     const int col = it % CB, m2 = it / CB;
     const int cg = c0 + col;
+    const uint64_t o = (uint64_t)b * ln.in_bstride + (uint64_t)m2 * ln.rstride + cg;
     float2 v[R1];
-    float2* s = pin + (uint64_t)m2 * ln.rstride + cg;
+    if constexpr (CLEAR) {
 #pragma unroll
-    for (int m1 = 0; m1 < R1; ++m1) v[m1] = (cg < ln.ncols) ? s[(uint64_t)R2 * m1 * ln.rstride] : make_float2(0.f, 0.f);
+      for (int m1 = 0; m1 < R1; ++m1)
+        v[m1] = (cg < ln.ncols) ? inw[o + (uint64_t)R2 * m1 * ln.rstride] : make_float2(0.f, 0.f);
+    } else {
+#pragma unroll
+      for (int m1 = 0; m1 < R1; ++m1)
+        v[m1] = (cg < ln.ncols) ? in[o + (uint64_t)R2 * m1 * ln.rstride] : make_float2(0.f, 0.f);
+    }
     dft<R1>(v, true);
     float2* d = sh + m2 * CB + col;
     d[0] = v[0];
 #pragma unroll
     for (int k1 = 1; k1 < R1; ++k1) d[k1 * R2 * CB] = twiddle(v[k1], tw[k1 * R2 + m2], true);
-    if (clear && cg < ln.ncols) {
+    if constexpr (CLEAR) {
+      if (cg < ln.ncols) {
 #pragma unroll
-      for (int m1 = 0; m1 < R1; ++m1) s[(uint64_t)R2 * m1 * ln.rstride] = make_float2(0.f, 0.f);
+        for (int m1 = 0; m1 < R1; ++m1) inw[o + (uint64_t)R2 * m1 * ln.rstride] = make_float2(0.f, 0.f);
+      }
     }
   }
   __syncthreads();
@@ -501,8 +510,16 @@ pg_status cols_fwd(const Lines& ln, int B, const float2* P, const float2* tw, fl
 template <int LOGN>
 pg_status cols_inv(const Lines& ln, int B, float2* in, int clear, const float2* tw, float2* Q, cudaStream_t s) {
   using CG = ColGeo<LOGN>;
-  PG_CUDA(cudaFuncSetAttribute(k_fft_inv_cols<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CG::smem));
-  PG_LAUNCH(k_fft_inv_cols<LOGN>, dim3(ceil_div(ln.ncols, CG::CB), B), kT, CG::smem, s, ln, in, clear, tw, Q);
+  if (clear) {
+    PG_CUDA(cudaFuncSetAttribute(k_fft_inv_cols<LOGN, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)CG::smem));
+    PG_LAUNCH((k_fft_inv_cols<LOGN, true>), dim3(ceil_div(ln.ncols, CG::CB), B), kT, CG::smem, s, ln, in, in, tw, Q);
+  } else {
+    PG_CUDA(cudaFuncSetAttribute(k_fft_inv_cols<LOGN, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)CG::smem));
+    PG_LAUNCH((k_fft_inv_cols<LOGN, false>), dim3(ceil_div(ln.ncols, CG::CB), B), kT, CG::smem, s, ln, in, nullptr,
+              tw, Q);
+  }
   return PG_OK;
 }
 
@@ -659,8 +676,10 @@ __global__ void __launch_bounds__(fused::kTF, 1)
   cluster.sync();
 }
 
+template <bool CLEAR>
 __global__ void __launch_bounds__(fused::kTF, 1)
-    k_fft2_adj_fused(NufftGeom g, int L, float2* grids, int clear, const float2* __restrict__ S, int c0,
+    k_fft2_adj_fused(NufftGeom g, int L, const float2* __restrict__ grids, float2* gridsw,
+                     const float2* __restrict__ S, int c0,
                      const float2* __restrict__ E, const float2* __restrict__ WoH, const float* __restrict__ deapf,
                      const float2* __restrict__ tw, float2* __restrict__ Rimg) {
   using namespace fused;
@@ -672,21 +691,25 @@ __global__ void __launch_bounds__(fused::kTF, 1)
   const int crop0 = g.crop_off[0], crop1 = g.crop_off[1];
   const uint64_t N = g.nimg();
   const int b = blockIdx.y, c = b / L, l = b - c * L;
-  float2* in = grids + (uint64_t)b * n * n;
   for (int it = threadIdx.x; it < CPC * R; it += kTF) {   // x transform, pass 1: (column, m2)
     const int col = it % CPC, m2 = it / CPC;
+    const uint64_t o = (uint64_t)b * n * n + (uint64_t)m2 * n + r * CPC + col;
     float2 v[R];
-    float2* s = in + (uint64_t)m2 * n + r * CPC + col;
+    if constexpr (CLEAR) {
 #pragma unroll
-    for (int m1 = 0; m1 < R; ++m1) v[m1] = s[(uint64_t)R * m1 * n];
+      for (int m1 = 0; m1 < R; ++m1) v[m1] = gridsw[o + (uint64_t)R * m1 * n];
+    } else {
+#pragma unroll
+      for (int m1 = 0; m1 < R; ++m1) v[m1] = grids[o + (uint64_t)R * m1 * n];
+    }
     dft<R>(v, true);
     float2* d = W + m2 * CPC + col;
     d[0] = v[0];
 #pragma unroll
     for (int k1 = 1; k1 < R; ++k1) d[k1 * R * CPC] = twiddle(v[k1], tw[k1 * R + m2], true);
-    if (clear) {   // every grid cell is read once, here: zero it for the next adjoint spread
+    if constexpr (CLEAR) {   // every grid cell is read once, here: zero it for the next adjoint spread
 #pragma unroll
-      for (int m1 = 0; m1 < R; ++m1) s[(uint64_t)R * m1 * n] = make_float2(0.f, 0.f);
+      for (int m1 = 0; m1 < R; ++m1) gridsw[o + (uint64_t)R * m1 * n] = make_float2(0.f, 0.f);
     }
   }
   __syncthreads();
@@ -772,7 +795,9 @@ pg_status launch_fused(Kern kern, int B, cudaStream_t s, Args... args) {
 bool query_fused() {
   if (cudaFuncSetAttribute(k_fft2_fwd_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused::smem) !=
           cudaSuccess ||
-      cudaFuncSetAttribute(k_fft2_adj_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused::smem) !=
+      cudaFuncSetAttribute(k_fft2_adj_fused<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused::smem) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_fft2_adj_fused<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused::smem) !=
           cudaSuccess) {
     cudaGetLastError();
     return false;
@@ -790,7 +815,7 @@ bool query_fused() {
   cfg.numAttrs = 1;
   int nf = 0, na = 0;
   if (cudaOccupancyMaxActiveClusters(&nf, k_fft2_fwd_fused, &cfg) != cudaSuccess ||
-      cudaOccupancyMaxActiveClusters(&na, k_fft2_adj_fused, &cfg) != cudaSuccess) {
+      cudaOccupancyMaxActiveClusters(&na, k_fft2_adj_fused<true>, &cfg) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
@@ -885,7 +910,12 @@ pg_status fftpass_adjoint(const NufftGeom& g, int B, int L, float2* grids, int c
   const uint64_t plane = (uint64_t)g.Gx * g.Gy;
   float2* Qr = Q;   // the rows the last pass reads
   if (use_fused(g)) {
-    PG_TRY(launch_fused(k_fft2_adj_fused, B, s, g, L, grids, clear, S, c0, E, WoH, deapf, tw, Rimg));
+    if (clear)
+      PG_TRY(launch_fused(k_fft2_adj_fused<true>, B, s, g, L, (const float2*)grids, grids, S, c0, E, WoH, deapf, tw,
+                          Rimg));
+    else
+      PG_TRY(launch_fused(k_fft2_adj_fused<false>, B, s, g, L, (const float2*)grids, (float2*)nullptr, S, c0, E,
+                          WoH, deapf, tw, Rimg));
     const uint64_t N = g.nimg();
     PG_LAUNCH(k_sum_images, ceil_div(N * 8, 256), 256, 0, s, N, B, Rimg, accumulate, x);
     return PG_OK;
