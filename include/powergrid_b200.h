@@ -303,6 +303,8 @@ pg_status pg_acq_index_destroy(pg_acq_index ix);
 /* acqArray(NShot, NPar, NSlice, NRep, NAvg, NEcho, NPhase) (acqTracking.cpp:73). */
 pg_status pg_acq_index_lookup(pg_acq_index ix, uint32_t shot, uint32_t partition, uint32_t slice, uint32_t repetition,
                               uint32_t average, uint32_t contrast, uint32_t phase, int64_t* acq);
+/* The encoding limits the index was built with. */
+pg_status pg_acq_index_limits(pg_acq_index ix, pg_encoding_limits* limits);
 /* getCompleteISMRMRDAcqData(d, acqTrack, NSlice, NRep, NAve, NEcho, NPhase,
  * data, kx, ky, kz, tvec) (processIsmrmrd.hpp:361-471): the sizes first
  * (acquisitions found, samples and channels of each; all must match), then
@@ -372,6 +374,7 @@ typedef struct pg_request_stats {
   pg_status status;
   double setup_ms;                             /* summed over jobs: operator construction */
   double solve_ms;                             /* summed over jobs: PCG solve and image copy-out */
+  uint64_t jobs;                               /* jobs the request was split into (batches of slices) */
   char error[160];                             /* the first failed job's message, or empty */
 } pg_request_stats;
 
@@ -386,6 +389,32 @@ pg_status pg_cancel(pg_server s, uint64_t ticket);
 /* Device bytes one slice job of the request holds while resident (the
  * admission metric; an upper bound of what the job allocates). */
 uint64_t pg_request_footprint(const pg_request* req);
+
+/* The reference ISMRMRD driver's image loop as one request
+ * (PowerGridIsmrmrd.cpp:191-264): every image of the acquisition index, in
+ * its loop order (slice outermost, then phase, contrast, average, and
+ * repetition innermost: image k = (((slice * phases + phase) * contrasts +
+ * contrast) * averages + average) * repetitions + repetition), each gathered
+ * as getCompleteISMRMRDAcqData does (pg_acq_gather), with its slice's field
+ * map and coil maps (getISMRMRDCompleteFieldMap / getISMRMRDCompleteSENSEMap,
+ * processIsmrmrd.hpp:196-266), reconstructed as
+ * SENSE<TimeSegmentation<Gnufft>> (Hanning interpolation, one shot) +
+ * QuadPenalty(beta, 3 dimensions) with reconSolve.  Images whose gathered
+ * trajectories are identical are batched as the slices of pg_submit are.
+ * The gather runs in pg_submit_acquisitions, so the acquisitions may be
+ * released on return; the maps and image_out must stay valid until
+ * completion.  Every image needs at least one acquisition and all the same
+ * channel count (the coil maps are sized by it); otherwise PG_INVALID_ARG. */
+typedef struct pg_acq_request {
+  uint64_t nx, ny, nz;
+  uint64_t L;               /* time segments; 0 = ceil((max t - min t) / 2 ms), the driver's default */
+  uint64_t niter;
+  float beta;
+  const float* field_map;   /* slices * nx*ny*nz (rad/s), slice-major */
+  const float* sense_map;   /* slices * nx*ny*nz*nc (complex, coil-major per slice) */
+  float* image_out;         /* images * nx*ny*nz (complex) */
+} pg_acq_request;
+pg_status pg_submit_acquisitions(pg_server s, pg_acq_index ix, const pg_acq_request* req, uint64_t* ticket);
 
 /* ---- instrumentation and fault injection (host-side only) ------------ */
 /* Stage timing: while enabled, the NUFFT and Gdft pipelines record a CUDA

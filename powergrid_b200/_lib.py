@@ -44,7 +44,7 @@ class Request(C.Structure):
 class RequestStats(C.Structure):
     _fields_ = [("t_submit_ms", C.c_double), ("t_start_ms", C.c_double), ("t_done_ms", C.c_double),
                 ("iters_done", U64), ("bytes_resident", U64), ("status", C.c_int), ("setup_ms", C.c_double),
-                ("solve_ms", C.c_double), ("error", C.c_char * 160)]
+                ("solve_ms", C.c_double), ("jobs", U64), ("error", C.c_char * 160)]
 
 
 class Acquisition(C.Structure):
@@ -58,6 +58,11 @@ class EncodingLimits(C.Structure):
     _fields_ = [("shots", C.c_uint32), ("partitions", C.c_uint32), ("slices", C.c_uint32),
                 ("repetitions", C.c_uint32), ("averages", C.c_uint32), ("contrasts", C.c_uint32),
                 ("phases", C.c_uint32)]
+
+
+class AcqRequest(C.Structure):
+    _fields_ = [("nx", U64), ("ny", U64), ("nz", U64), ("L", U64), ("niter", U64), ("beta", F32),
+                ("field_map", P), ("sense_map", P), ("image_out", P)]
 
 
 _lib = None
@@ -111,6 +116,7 @@ SIGNATURES = {
     "pg_acq_index_create": (C.c_int, [C.POINTER(P), C.POINTER(Acquisition), U64, C.POINTER(EncodingLimits)]),
     "pg_acq_index_destroy": (C.c_int, [P]),
     "pg_acq_index_lookup": (C.c_int, [P] + [C.c_uint32] * 7 + [C.POINTER(C.c_int64)]),
+    "pg_acq_index_limits": (C.c_int, [P, C.POINTER(EncodingLimits)]),
     "pg_acq_gather_size": (C.c_int, [P] + [C.c_uint32] * 5 + [C.POINTER(U64)] * 3),
     "pg_acq_gather": (C.c_int, [P] + [C.c_uint32] * 5 + [P] * 5),
     "pg_acq_gather_device": (C.c_int, [P] + [C.c_uint32] * 5 + [P] * 6),
@@ -119,6 +125,7 @@ SIGNATURES = {
     "pg_server_create": (C.c_int, [C.POINTER(P), C.POINTER(ServerConfig)]),
     "pg_server_destroy": (C.c_int, [P]),
     "pg_submit": (C.c_int, [P, C.POINTER(Request), C.POINTER(U64)]),
+    "pg_submit_acquisitions": (C.c_int, [P, P, C.POINTER(AcqRequest), C.POINTER(U64)]),
     "pg_poll": (C.c_int, [P, U64, C.POINTER(RequestStats)]),
     "pg_wait": (C.c_int, [P, U64, C.POINTER(RequestStats)]),
     "pg_cancel": (C.c_int, [P, U64]),

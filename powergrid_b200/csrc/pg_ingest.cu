@@ -205,6 +205,12 @@ pg_status pg_acq_index_lookup(pg_acq_index ix, uint32_t shot, uint32_t partition
   return PG_OK;
 }
 
+pg_status pg_acq_index_limits(pg_acq_index ix, pg_encoding_limits* limits) {
+  if (!ix || !limits) return set_error(PG_INVALID_ARG, "acquisition index: null argument");
+  *limits = ix->lim;
+  return PG_OK;
+}
+
 pg_status pg_acq_gather_size(pg_acq_index ix, uint32_t slice, uint32_t repetition, uint32_t average,
                              uint32_t contrast, uint32_t phase, uint64_t* n_acq, uint64_t* n_samples,
                              uint64_t* n_channels) {

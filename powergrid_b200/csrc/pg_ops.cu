@@ -481,7 +481,8 @@ pg_status make_timeseg_shared(std::unique_ptr<TimeSegOp>* out, pg_op_s* G, const
 
 // ---- the slices of a request as one operator ---------------------------------
 pg_status make_slice_batch(std::unique_ptr<SliceBatchOp>* out, GnufftOp* G, const TimeSegOp* ts, uint64_t ns,
-                           uint64_t nc, const float* field_maps, const float* sense_maps, cudaStream_t s) {
+                           uint64_t nc, const float* const* field_maps, const float* const* sense_maps,
+                           cudaStream_t s) {
   if (!G || !G->plan || !sense_maps || (ts && !field_maps) || ns == 0 || nc == 0)
     return set_error(PG_INVALID_ARG, "slice batch: null argument");
   const uint64_t N = G->n_image, M = G->n_data;
@@ -497,13 +498,18 @@ pg_status make_slice_batch(std::unique_ptr<SliceBatchOp>* out, GnufftOp* G, cons
   op->n_image = ns * N;
   op->n_data = ns * nc * M;
   op->n_seg = ns;
+  for (uint64_t sl = 0; sl < ns; ++sl)
+    if (!sense_maps[sl] || (op->ts && !field_maps[sl])) return set_error(PG_INVALID_ARG, "slice batch: null map");
   if (op->ts) {
     if (ts->n_image != N || ts->n_data != M || !ts->bin)
       return set_error(PG_INVALID_ARG, "slice batch: segmentation does not match the Gnufft");
-    for (uint64_t p = 0; p < ns * N; ++p)
-      if (!std::isfinite(field_maps[p])) return set_error(PG_INVALID_ARG, "slice batch: non-finite field map");
+    for (uint64_t sl = 0; sl < ns; ++sl)
+      for (uint64_t p = 0; p < N; ++p)
+        if (!std::isfinite(field_maps[sl][p])) return set_error(PG_INVALID_ARG, "slice batch: non-finite field map");
     DevBuf<float> fm;
-    PG_TRY(fm.upload(field_maps, ns * N, s));
+    PG_TRY(fm.alloc(ns * N));
+    for (uint64_t sl = 0; sl < ns; ++sl)
+      PG_CUDA(cudaMemcpyAsync(fm.p + sl * N, field_maps[sl], N * sizeof(float), cudaMemcpyHostToDevice, s));
     const uint64_t LN = (uint64_t)op->L * N;
     PG_TRY(op->Wo.alloc(ns * LN));
     PG_TRY(op->WoH.alloc(ns * LN));
@@ -512,7 +518,11 @@ pg_status make_slice_batch(std::unique_ptr<SliceBatchOp>* out, GnufftOp* G, cons
                 op->Wo.p + sl * LN, op->WoH.p + sl * LN);
     PG_CUDA(cudaStreamSynchronize(s));  // fm is released on return
   }
-  PG_TRY(op->S.upload(reinterpret_cast<const float2*>(sense_maps), ns * nc * N, s));
+  PG_TRY(op->S.alloc(ns * nc * N));
+  for (uint64_t sl = 0; sl < ns; ++sl)
+    PG_CUDA(cudaMemcpyAsync(op->S.p + sl * nc * N, sense_maps[sl], nc * N * sizeof(float2), cudaMemcpyHostToDevice,
+                            s));
+  PG_CUDA(cudaStreamSynchronize(s));  // the host maps may be released on return
   *out = std::move(op);
   return PG_OK;
 }

@@ -155,9 +155,11 @@ struct SliceBatchOp : pg_op_s {
   pg_status forward(const float2* x, float2* y, cudaStream_t s) override;
   pg_status adjoint(const float2* y, float2* x, cudaStream_t s) override;
 };
-// field_maps: ns x N; sense_maps: ns x nc x N complex (interleaved floats).
+// field_maps[sl]: slice sl's field map (N); sense_maps[sl]: its coil maps
+// (nc x N complex, interleaved floats).  Host memory, read before return.
 pg_status make_slice_batch(std::unique_ptr<SliceBatchOp>* out, GnufftOp* G, const TimeSegOp* ts, uint64_t ns,
-                           uint64_t nc, const float* field_maps, const float* sense_maps, cudaStream_t s);
+                           uint64_t nc, const float* const* field_maps, const float* const* sense_maps,
+                           cudaStream_t s);
 
 // out[:, a] = sum_b in[:, b] * C[a + Kout b] over columns of length N, the sum
 // in order of b; out is stored column-major N x Kout, or transposed (Kout x N,

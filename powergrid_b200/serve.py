@@ -4,8 +4,14 @@
     ticket = srv.submit(req)            # req: ReconRequest (host numpy arrays)
     image, stats = srv.wait(ticket)     # image: n_slices x (nx*ny*nz) complex64
 
-Each slice of a request runs as its own job; jobs are admitted FIFO while a
-worker slot is free and the summed device footprint stays within the budget.
+    # the ISMRMRD driver's image loop over an acquisition index
+    ticket = srv.submit_acquisitions(acq_track, nx, ny, nz, field_map, sense_map, niter=10, beta=...)
+    images, stats = srv.wait(ticket)    # images: (slice, phase, contrast, average, repetition) x N
+
+A request's slices (or an acquisition request's images of one trajectory)
+are batched into jobs of as many as fit the HBM budget; jobs are admitted
+FIFO while a worker slot is free and the summed device footprint stays within
+the budget.
 """
 from __future__ import annotations
 
@@ -16,6 +22,12 @@ import numpy as np
 
 from . import _lib
 from ._lib import P, U64, Request, RequestStats, ServerConfig, check
+
+
+@dataclasses.dataclass
+class _Shape:
+    n_slices: int
+    nimg: int
 
 
 @dataclasses.dataclass
@@ -86,6 +98,27 @@ class Server:
         self._live[t.value] = (keep, out, r)
         return int(t.value)
 
+    def submit_acquisitions(self, acq_track, nx: int, ny: int, nz: int, field_map, sense_map, L: int = 0,
+                            niter: int = 10, beta: float = 0.0) -> int:
+        """Every image of an acqTracking index (PowerGridIsmrmrd.cpp:191-264):
+        slice outermost, then phase, contrast, average, repetition; field_map
+        is slices x N and sense_map slices x nc x N, as the ISMRMRD file holds
+        them.  L = 0 takes the driver's default ceil((max t - min t) / 2 ms)."""
+        keep = [acq_track]
+        fm = np.ascontiguousarray(field_map, dtype=np.float32)
+        sm = np.ascontiguousarray(sense_map, dtype=np.complex64)
+        nimg = (acq_track.NSliceMax * acq_track.NPhaseMax * acq_track.NEchoMax * acq_track.NAvgMax *
+                acq_track.NRepMax)
+        out = np.zeros(nimg * nx * ny * nz, dtype=np.complex64)
+        keep += [fm, sm, out]
+        q = _lib.AcqRequest(nx, ny, nz, L, niter, beta, fm.ctypes.data_as(P), sm.ctypes.data_as(P),
+                            out.ctypes.data_as(P))
+        t = U64()
+        check(_lib.load().pg_submit_acquisitions(self._h, acq_track._h, C.byref(q), C.byref(t)))
+        shape = _Shape(nimg, nx * ny * nz)
+        self._live[t.value] = (keep, out, shape)
+        return int(t.value)
+
     def poll(self, ticket: int):
         st = RequestStats()
         rc = _lib.load().pg_poll(self._h, ticket, C.byref(st))
@@ -107,7 +140,7 @@ class Server:
         stats = {"t_submit_ms": st.t_submit_ms, "t_start_ms": st.t_start_ms, "t_done_ms": st.t_done_ms,
                  "iters_done": int(st.iters_done), "bytes_resident": int(st.bytes_resident),
                  "status": _lib.STATUS.get(st.status, st.status), "setup_ms": st.setup_ms, "solve_ms": st.solve_ms,
-                 "error": st.error.decode(errors="replace")}
+                 "jobs": int(st.jobs), "error": st.error.decode(errors="replace")}
         return out.reshape(r.n_slices, r.nimg), stats
 
     def close(self):

@@ -98,8 +98,8 @@ def test_batched_slices_match_per_slice_solves(pg, n):
     inner products and steps; each served slice equals the solve of that slice
     alone through the operator API (reconSolve over its own SENSE<TS<Gnufft>>),
     with slices that differ in field map, coil maps and data.  n = 32 runs the
-    own FFT passes, n = 40 the cuFFT path; a budget of one slice's footprint
-    splits the request into one job per slice."""
+    own FFT passes, n = 40 the cuFFT path; a budget just above one slice's
+    footprint splits the request into one job per slice."""
     from powergrid_b200 import synthetic as S
     from powergrid_b200.serve import ReconRequest, Server
     ns, nc, L, niter, beta = 3, 3, 4, 6, 1e-3
@@ -118,11 +118,11 @@ def test_batched_slices_match_per_slice_solves(pg, n):
     r = ReconRequest(n, n, 1, nc, L, niter, beta, kx, ky, kz, t, np.concatenate(fms), np.concatenate(sms),
                      np.concatenate(ys), ns)
     direct = [pg.reconSolve(ys[k], ops[k][2], pg.QuadPenalty(n, n, 1, beta), niter=niter) for k in range(ns)]
-    for budget in (8 << 30, int(1.5 * Server.footprint(r))):
+    for budget, jobs in ((8 << 30, 1), (Server.footprint(r) + (64 << 10), ns)):
         srv = Server(hbm_budget_bytes=budget, max_inflight=2)
         img, st = srv.wait(srv.submit(r))
         srv.close()
-        assert st["status"] == "PG_OK" and st["iters_done"] == ns * niter
+        assert st["status"] == "PG_OK" and st["iters_done"] == ns * niter and st["jobs"] == jobs
         for k in range(ns):
             e = rel_l2(img[k], direct[k])
             print(f"n={n} budget {budget >> 20} MiB slice {k}: served vs alone {e:.2e}")
@@ -153,4 +153,95 @@ def test_cancel_queued_request(pg):
     assert st2["status"] == "PG_CANCELLED"
     _, st0 = srv.wait(t[0])
     assert st0["status"] == "PG_OK"
+    srv.close()
+
+
+def _acquisition_dataset(pg_mod, n, nc, niter, beta, L):
+    """A dataset of 2 slices x 2 contrasts x 2 repetitions, each image 4 spiral
+    shots (one acquisition per shot), listed in a shuffled order.  Contrast 1
+    uses a rotated trajectory, so the images form two trajectory groups.
+    Returns the acquisitions, the limits, the maps, and per image (in the
+    driver's loop order) its direct reconSolve through the operator API."""
+    import math
+    from powergrid_b200 import ingest as I
+    from powergrid_b200 import synthetic as S
+    shots, per = 4, 768
+    N = n * n
+    fms = np.stack([S.field_map(S.Rng(300 + s), n, n, 1, 80.0) for s in range(2)])
+    sms = np.stack([S.coil_maps(S.Rng(310 + s), n, n, 1, nc) for s in range(2)])
+    trajs = []
+    for ec in range(2):
+        kx, ky, t = S.spiral(n, shots, per, 10e-3)
+        if ec == 1:
+            c, s_ = math.cos(0.3), math.sin(0.3)
+            kx, ky = (c * kx - s_ * ky).astype(np.float32), (s_ * kx + c * ky).astype(np.float32)
+        trajs.append((kx, ky, np.zeros_like(kx), t))
+    acqs, direct = [], []
+    for sl in range(2):
+        for ec in range(2):
+            for rp in range(2):
+                kx, ky, kz, t = trajs[ec]
+                M = kx.size
+                G = pg_mod.Gnufft(M, 2.0, n, n, 1, kx, ky, kz)
+                Lk = L if L else int(math.ceil(float(np.float32(t.max() - t.min())) / 2e-3))
+                A = pg_mod.TimeSegmentation(G, fms[sl], t, M, N, Lk, 1, 1)
+                Sg = pg_mod.SENSE(A, sms[sl].ravel(), M, N, nc)
+                y = (Sg * S.image(S.Rng(320 + 4 * sl + 2 * ec + rp), N)).astype(np.complex64)
+                direct.append(((sl, ec, rp), pg_mod.reconSolve(y, Sg, pg_mod.QuadPenalty(n, n, 1, beta),
+                                                                niter=niter)))
+                yc = y.reshape(nc, shots, per)
+                for sh in range(shots):
+                    sel = slice(sh * per, (sh + 1) * per)
+                    traj = np.stack([kx[sel], ky[sel], kz[sel], t[sel]], axis=1)
+                    acqs.append(I.Acquisition(sh, 0, sl, rp, 0, ec, 0, yc[:, sh, :], traj))
+    order = np.random.default_rng(5).permutation(len(acqs))
+    limits = (shots, 1, 2, 2, 1, 2, 1)
+    return [acqs[i] for i in order], limits, fms, sms, direct
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("L", [0, 3])
+def test_acquisition_request_matches_per_image_solves(pg, L):
+    """pg_submit_acquisitions: every image of the index, gathered as
+    getCompleteISMRMRDAcqData does, in the driver's loop order (slice,
+    phase, contrast, average, repetition), equals the solve of that image
+    alone; L = 0 takes the driver's default segment count."""
+    from powergrid_b200 import ingest as I
+    from powergrid_b200.serve import Server
+    n, nc, niter, beta = 32, 3, 5, 1e-3
+    from powergrid_b200.serve import ReconRequest
+    acqs, limits, fms, sms, direct = _acquisition_dataset(pg, n, nc, niter, beta, L)
+    track = I.acqTracking(acqs, limits)
+    z = np.zeros(4 * 768, np.float32)
+    one = ReconRequest(n, n, 1, nc, L or 5, niter, beta, z, z, z, z, fms[0], sms[0].ravel(),
+                       np.zeros(z.size * nc, np.complex64))
+    # two trajectory groups of 4 images: one job each, or one job per image
+    for budget, jobs in ((8 << 30, 2), (Server.footprint(one) + (64 << 10), 8)):
+        srv = Server(hbm_budget_bytes=budget, max_inflight=2)
+        t = srv.submit_acquisitions(track, n, n, 1, fms, sms, L=L, niter=niter, beta=beta)
+        img, st = srv.wait(t)
+        srv.close()
+        assert st["status"] == "PG_OK", st["error"]
+        assert img.shape == (8, n * n) and st["iters_done"] == 8 * niter and st["jobs"] == jobs
+        # loop order: slice, phase (1), contrast, average (1), repetition
+        for k, ((sl, ec, rp), x) in enumerate(direct):
+            assert k == (sl * 2 + ec) * 2 + rp
+            e = rel_l2(img[k], x)
+            print(f"L={L} budget {budget >> 20} MiB image {k}: served vs alone {e:.2e}")
+            assert e <= MIX_TOL
+
+
+@pytest.mark.gpu
+def test_acquisition_request_rejects_missing_image(pg):
+    from powergrid_b200 import ingest as I
+    from powergrid_b200._lib import PGError
+    from powergrid_b200.serve import Server
+    n, nc = 32, 3
+    acqs, limits, fms, sms, _ = _acquisition_dataset(pg, n, nc, 1, 1e-3, 3)
+    # drop every acquisition of slice 1, contrast 0, repetition 1
+    kept = [a for a in acqs if not (a.slice == 1 and a.contrast == 0 and a.repetition == 1)]
+    track = I.acqTracking(kept, limits)
+    srv = Server(hbm_budget_bytes=8 << 30, max_inflight=1)
+    with pytest.raises(PGError, match="no acquisitions"):
+        srv.submit_acquisitions(track, n, n, 1, fms, sms, L=3, niter=1, beta=1e-3)
     srv.close()
