@@ -809,42 +809,10 @@ __global__ void k_denom_images(PenDev R, int K, const float2* __restrict__ ddir,
   block_store2(a, 0.0, part, nb);
 }
 
-// Sums over n of (|a|^2 or Re conj(a) b) and, with W, of (W|a|^2, Re conj(a) b).
-__global__ void k_sums(uint64_t n, const float2* __restrict__ a, const float2* __restrict__ b,
-                       const float* __restrict__ W, double* part, int nb) {
-  double s0 = 0.0, s1 = 0.0;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-    const float2 u = a[i];
-    const double nn = (double)u.x * u.x + (double)u.y * u.y;
-    s0 += W ? (double)W[i] * nn : nn;
-    if (b) {
-      const float2 v = b[i];
-      s1 += (double)u.x * v.x + (double)u.y * v.y;
-    }
-  }
-  block_store2(s0, s1, part, nb);
-}
-
-// out = a + alpha * b (out may alias a or b).
-__global__ void k_axpy(uint64_t n, const float2* a, double alpha, const float2* b, float2* out) {
-  const float al = (float)alpha;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-    const float2 u = a[i], v = b[i];
-    out[i] = make_float2(u.x + al * v.x, u.y + al * v.y);
-  }
-}
-
+// Block partials of a stand-alone reduction, added on the host in block order.
 struct HostSums {
   DevBuf<double> part;
   std::vector<double> h;
-  // Launch k_sums and add its block partials in block order.
-  pg_status run(uint64_t n, const float2* a, const float2* b, const float* W, double* s0, double* s1,
-                cudaStream_t s) {
-    const int nb = red_blocks(n);
-    PG_TRY(part.alloc(2 * (uint64_t)nb));
-    PG_LAUNCH(k_sums, (unsigned)nb, kRed, 0, s, n, a, b, W, part.p, nb);
-    return fetch(nb, s0, s1, s);
-  }
   pg_status fetch(int nb, double* s0, double* s1, cudaStream_t s) {
     h.resize(2 * (size_t)nb);
     PG_CUDA(cudaMemcpyAsync(h.data(), part.p, 2 * (size_t)nb * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -915,73 +883,258 @@ pg_status lowrank_penalty_check(const pg_penalty& Rh, uint64_t rank, uint64_t n_
   return PG_OK;
 }
 
-// solve_pwls_pcg (solve_pwls_pcg.hpp:48-167) with the low-rank wrapper: the
-// same steps as the fused solver, with the scalars on the host (FP64) because
-// the wrapper's gradient is not a local stencil.
-pg_status pcg_solve_lowrank(pg_op_s* A, LowRankPen& P, const float2* x0, const float* W, const float2* y,
-                            uint64_t niter, float2* xout, uint64_t* iters, cudaStream_t s) {
-  const uint64_t ni = A->n_image, nd = A->n_data;
-  DevBuf<float2> x, Ax, r, ngrad, pgrad, ddir, Adir, xs;
-  DevBuf<float> ones;
-  PG_TRY(x.alloc(ni)); PG_TRY(ngrad.alloc(ni)); PG_TRY(pgrad.alloc(ni)); PG_TRY(ddir.alloc(ni));
-  PG_TRY(xs.alloc(ni)); PG_TRY(Ax.alloc(nd)); PG_TRY(r.alloc(nd)); PG_TRY(Adir.alloc(nd));
-  if (!W) {
-    PG_TRY(ones.alloc(nd));
-    PG_LAUNCH(k_fill_ones, ceil_div(nd, 256), 256, 0, s, nd, ones.p);
-    W = ones.p;
+// ---- the PCG loop with the low-rank wrapper ---------------------------------
+// solve_pwls_pcg (solve_pwls_pcg.hpp:48-167) over LRobj with R_lowRank.  The
+// wrapper's gradient mixes the K images (not a local stencil), so the
+// penalty terms are separate passes (mix, per-image stencil, mix); the
+// scalars stay on the device as in the fused solver (FP64 last-block sums,
+// early-exit flags), so an iteration has no host step and is replayed as
+// one CUDA graph.  The kernels shared with the fused solver run with one
+// segment.
+
+// ngrad = A'r - pgrad; partials |A'r|^2 and |ngrad|^2; then the early exit on
+// a vanishing gradient (:88-91) and the CG coefficient (:95-110).
+__global__ void k_lr_ngrad(uint64_t n, float2* __restrict__ ngrad, const float2* __restrict__ pgrad, double* part,
+                           int nb, unsigned* counter, double* sc, uint32_t* fl) {
+  if (fl[F_DONE]) return;
+  double a = 0.0, b = 0.0;
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x) {
+    const float2 raw = ngrad[j];
+    a += (double)raw.x * raw.x + (double)raw.y * raw.y;
+    const float2 v = csub(raw, pgrad[j]);
+    ngrad[j] = v;
+    b += (double)v.x * v.x + (double)v.y * v.y;
   }
-  if (x0) PG_CUDA(cudaMemcpyAsync(x.p, x0, ni * sizeof(float2), cudaMemcpyDeviceToDevice, s));
-  else PG_CUDA(cudaMemsetAsync(x.p, 0, ni * sizeof(float2), s));
-  if (x0) PG_TRY(A->forward(x.p, Ax.p, s));
-  else PG_CUDA(cudaMemsetAsync(Ax.p, 0, nd * sizeof(float2), s));   // A * 0 = 0 exactly
-  HostSums hs;
-  double ywy = 0.0;
-  PG_TRY(hs.run(nd, y, nullptr, W, &ywy, nullptr, s));
-  const unsigned gd = (unsigned)red_blocks(nd), gi = (unsigned)red_blocks(ni);
-  double oldinprod = 0.0;
-  uint64_t done = 0;
-  for (uint64_t it = 0; it < niter; ++it) {
-    PG_LAUNCH(k_residual, gd, kRed, 0, s, nd, y, Ax.p, W, r.p);
+  block_store2(a, b, part, nb);
+  if (!last_block(counter)) return;
+  const double gn = block_part_sum(part, nb, 0);
+  const double nw = block_part_sum(part, nb, 1);
+  if (threadIdx.x == 0) {
+    if (sqrt(gn) / sc[S_YWY] < 1e-10) { fl[F_DONE] = 1; fl[F_REASON] = 1; return; }
+    double gamma = 0.0;
+    if (fl[F_IT] > 0) gamma = (fabs(sc[S_OLD]) < 1e-10) ? 0.0 : nw / sc[S_OLD];
+    sc[S_GAMMA] = gamma;
+    sc[S_OLD] = nw;
+  }
+}
+
+// xs = x + step ddir: the point of a Newton step (:133).
+__global__ void k_lr_point(uint64_t n, const float2* __restrict__ x, const float2* __restrict__ ddir,
+                           float2* __restrict__ xs, const double* sc, const uint32_t* fl) {
+  if (fl[F_DONE]) return;
+  const float st = (float)sc[S_STEP];
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const float2 u = x[i], v = ddir[i];
+    xs[i] = make_float2(u.x + st * v.x, u.y + st * v.y);
+  }
+}
+
+// R_lowRank Denom (R_lowRank.cpp:67-87) over the mixed images D (of ddir) and
+// I (of xs): beta^2 sum_j sum_dims wpot(Cd I_j) |Cd D_j|^2; then the Newton
+// denominator dAWAd + pdenom and its range test (:136-140).
+__global__ void k_lr_denom(PenDev R, int K, const float2* __restrict__ D, const float2* __restrict__ I, double beta,
+                           double* part, int nb, unsigned* counter, double* sc, uint32_t* fl) {
+  if (fl[F_DONE]) return;
+  double a = 0.0;
+  const uint64_t n = R.N * (uint64_t)K;
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t img = t / R.N, j = t - img * R.N;
+    const float2* di = D + img * R.N;
+    const float2* xi = I + img * R.N;
+    for (int dim = 0; dim < R.nd; ++dim) {
+      const uint64_t off = R.off[dim];
+      if (j < off || off >= R.N) continue;
+      const float2 cd = csub(di[j], di[j - off]);
+      const float2 cz = csub(xi[j], xi[j - off]);
+      a += (double)wpot(R, cz) * ((double)cd.x * cd.x + (double)cd.y * cd.y);
+    }
+  }
+  block_store2(a, 0.0, part, nb);
+  if (!last_block(counter)) return;
+  const double pd = block_part_sum(part, nb, 0);
+  if (threadIdx.x == 0) {
+    const double denom = sc[S_DAWAD] + pd * beta * beta;
+    if (fabs(denom) < 1e-20 || fabs(denom) > 1e25) { fl[F_DONE] = 1; fl[F_REASON] = 3; return; }
+    sc[S_PDEN] = denom;
+  }
+}
+
+// pdot = Re<ddir, Gradient(xs)>; step -= (-dAWr + step dAWAd + pdot) / denom (:141-149).
+__global__ void k_lr_step(uint64_t n, const float2* __restrict__ ddir, const float2* __restrict__ pgrad, double* part,
+                          int nb, unsigned* counter, double* sc, uint32_t* fl) {
+  if (fl[F_DONE]) return;
+  double b = 0.0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const float2 u = ddir[i], v = pgrad[i];
+    b += (double)u.x * v.x + (double)u.y * v.y;
+  }
+  block_store2(b, 0.0, part, nb);
+  if (!last_block(counter)) return;
+  const double pdot = block_part_sum(part, nb, 0);
+  if (threadIdx.x == 0) {
+    const double step = sc[S_STEP];
+    sc[S_STEP] = step - (-sc[S_DAWR] + step * sc[S_DAWAD] + pdot) / sc[S_PDEN];
+  }
+}
+
+// Buffers, penalty and the captured iteration of low-rank solves, cached on
+// the LRobj operator.  A new solve with the same penalty shape re-uploads the
+// basis into the same device matrices and replays the graph.
+struct LowRankCache : pg_pcg_cache_base {
+  LowRankPen P;
+  pg_penalty R{};
+  uint64_t rank = 0;
+  bool w_ones = true;
+  uint64_t prof_epoch = 0;
+  DevBuf<float2> x, Ax, r, ngrad, pgrad, ddir, Adir, xs, ybuf;
+  DevBuf<float> wbuf;
+  DevBuf<double> part, sc;
+  DevBuf<uint32_t> fl;
+  DevBuf<unsigned> counter;
+  int nbd = 1, nbi = 1, nbk = 1;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint64_t per_iter = 0;
+  ~LowRankCache() override {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+  }
+  bool matches(const pg_penalty& q, uint64_t k, bool ones) const {
+    return R.kind == q.kind && R.nx == q.nx && R.ny == q.ny && R.nz == q.nz && R.beta == q.beta &&
+           R.delta == q.delta && R.dims2penalize == q.dims2penalize && rank == k && w_ones == ones &&
+           prof_epoch == g_profile_epoch;
+  }
+
+  // One iteration; r = W (.) (y - Ax) holds on entry and on exit.
+  pg_status iteration(pg_op_s* A, cudaStream_t s) {
+    const uint64_t ni = A->n_image, nd = A->n_data;
+    const int pst = 0;   // one segment
     PG_TRY(A->adjoint(r.p, ngrad.p, s));
-    double gn = 0.0;
-    PG_TRY(hs.run(ni, ngrad.p, nullptr, nullptr, &gn, nullptr, s));
-    if (std::sqrt(gn) / ywy < 1e-10) break;                       // :88-91
     PG_TRY(P.gradient(x.p, pgrad.p, s));
-    PG_LAUNCH(k_axpy, gi, kRed, 0, s, ni, ngrad.p, -1.0, pgrad.p, ngrad.p);
-    double newinprod = 0.0;
-    PG_TRY(hs.run(ni, ngrad.p, nullptr, nullptr, &newinprod, nullptr, s));
-    if (it == 0) {
-      PG_CUDA(cudaMemcpyAsync(ddir.p, ngrad.p, ni * sizeof(float2), cudaMemcpyDeviceToDevice, s));
-    } else {
-      const double gamma = (std::fabs(oldinprod) < 1e-10) ? 0.0 : newinprod / oldinprod;
-      PG_LAUNCH(k_axpy, gi, kRed, 0, s, ni, ngrad.p, gamma, ddir.p, ddir.p);
-    }
-    oldinprod = newinprod;
-    double dn = 0.0;
-    PG_TRY(hs.run(ni, ddir.p, ngrad.p, nullptr, nullptr, &dn, s));
-    if (dn < 0) break;                                               // :113-116
+    PG_LAUNCH(k_lr_ngrad, (unsigned)nbi, kRed, 0, s, ni, ngrad.p, pgrad.p, part.p, nbi, counter.p, sc.p, fl.p);
+    PG_LAUNCH(k_ddir, (unsigned)nbi, kRed, 0, s, ni, ngrad.p, ddir.p, part.p, nbi, counter.p, sc.p, fl.p, pst);
     PG_TRY(A->forward(ddir.p, Adir.p, s));
-    double dAWAd = 0.0, dAWr = 0.0;
-    PG_TRY(hs.run(nd, Adir.p, r.p, W, &dAWAd, &dAWr, s));
-    double step = 0.0;
-    bool stop = false;
-    for (int j = 0; j < 3; ++j) {                                    // :128-150
-      PG_LAUNCH(k_axpy, gi, kRed, 0, s, ni, x.p, step, ddir.p, xs.p);
-      double pdenom = 0.0;
-      PG_TRY(P.denom(ddir.p, xs.p, &pdenom, s));
-      const double denom = dAWAd + pdenom;
-      if (std::fabs(denom) < 1e-20 || std::fabs(denom) > 1e25) { stop = true; break; }
+    PG_LAUNCH(k_daw, (unsigned)nbd, kRed, 0, s, nd, Adir.p, wbuf.p, r.p, part.p, nbd, counter.p, sc.p, fl.p, 0, 0.0,
+              pst);
+    for (int k = 0; k < 3; ++k) {                                    // :128-150
+      PG_LAUNCH(k_lr_point, (unsigned)nbi, kRed, 0, s, ni, x.p, ddir.p, xs.p, sc.p, fl.p);
+      PG_TRY(mix_columns(P.R.N, P.K, P.K, xs.p, P.cr.p, false, P.I.p, s));
+      PG_TRY(mix_columns(P.R.N, P.K, P.K, ddir.p, P.cr.p, false, P.D.p, s));
+      PG_LAUNCH(k_lr_denom, (unsigned)nbk, kRed, 0, s, P.R, P.K, P.D.p, P.I.p, P.beta, part.p, nbk, counter.p, sc.p,
+                fl.p);
       PG_TRY(P.gradient(xs.p, pgrad.p, s));
-      double pdot = 0.0;
-      PG_TRY(hs.run(ni, ddir.p, pgrad.p, nullptr, nullptr, &pdot, s));
-      step -= (-dAWr + step * dAWAd + pdot) / denom;
+      PG_LAUNCH(k_lr_step, (unsigned)nbi, kRed, 0, s, ni, ddir.p, pgrad.p, part.p, nbi, counter.p, sc.p, fl.p);
     }
-    if (stop) break;
-    PG_LAUNCH(k_axpy, gd, kRed, 0, s, nd, Ax.p, step, Adir.p, Ax.p);
-    PG_LAUNCH(k_axpy, gi, kRed, 0, s, ni, x.p, step, ddir.p, x.p);
-    done = it + 1;
+    PG_LAUNCH(k_update, (unsigned)red_blocks(std::max(nd, ni)), kRed, 0, s, ni, nd, x.p, ddir.p, Ax.p, Adir.p, ybuf.p,
+              wbuf.p, r.p, sc.p, fl.p);
+    return PG_OK;
   }
-  PG_CUDA(cudaMemcpyAsync(xout, x.p, ni * sizeof(float2), cudaMemcpyDeviceToDevice, s));
+};
+
+pg_status make_lowrank_cache(pg_op_s* A, const pg_penalty& Rh, uint64_t rank, const float* v, bool w_ones,
+                             std::unique_ptr<LowRankCache>* out, cudaStream_t s) {
+  auto c = std::make_unique<LowRankCache>();
+  const uint64_t ni = A->n_image, nd = A->n_data;
+  PG_TRY(c->P.init(Rh, rank, v, s));
+  c->R = Rh;
+  c->rank = rank;
+  c->w_ones = w_ones;
+  c->prof_epoch = g_profile_epoch;
+  c->nbd = red_blocks(nd);
+  c->nbi = red_blocks(ni);
+  c->nbk = red_blocks(c->P.R.N * rank);
+  for (DevBuf<float2>* b : {&c->x, &c->ngrad, &c->pgrad, &c->ddir, &c->xs}) PG_TRY(b->alloc(ni));
+  for (DevBuf<float2>* b : {&c->Ax, &c->r, &c->Adir, &c->ybuf}) PG_TRY(b->alloc(nd));
+  PG_TRY(c->wbuf.alloc(nd));
+  if (w_ones) PG_LAUNCH(k_fill_ones, ceil_div(nd, 256), 256, 0, s, nd, c->wbuf.p);
+  PG_TRY(c->part.alloc(2 * (uint64_t)std::max(c->nbd, std::max(c->nbi, c->nbk))));
+  PG_TRY(c->sc.alloc(S_NSCAL));
+  PG_TRY(c->fl.alloc(F_NFLAG));
+  PG_TRY(c->counter.alloc(1));
+  PG_CUDA(cudaMemsetAsync(c->counter.p, 0, sizeof(unsigned), s));
+  *out = std::move(c);
+  return PG_OK;
+}
+
+pg_status pcg_solve_lowrank(pg_op_s* A, const pg_penalty& Rh, uint64_t rank, const float* v, const float2* x0,
+                            const float* W, const float2* y, uint64_t niter, float2* xout, uint64_t* iters,
+                            cudaStream_t s) {
+  const uint64_t ni = A->n_image, nd = A->n_data;
+  auto* c = dynamic_cast<LowRankCache*>(A->pcg_cache.get());
+  if (!c || !c->matches(Rh, rank, W == nullptr)) {
+    A->pcg_cache.reset();
+    std::unique_ptr<LowRankCache> nc;
+    PG_TRY(make_lowrank_cache(A, Rh, rank, v, W == nullptr, &nc, s));
+    c = nc.get();
+    A->pcg_cache = std::move(nc);
+  } else {
+    PG_TRY(c->P.init(Rh, rank, v, s));   // same shapes: the graph's matrices, rewritten in place
+  }
+  // inputs into the buffers the graph reads
+  PG_CUDA(cudaMemcpyAsync(c->ybuf.p, y, nd * sizeof(float2), cudaMemcpyDeviceToDevice, s));
+  if (W) PG_CUDA(cudaMemcpyAsync(c->wbuf.p, W, nd * sizeof(float), cudaMemcpyDeviceToDevice, s));
+  if (x0) PG_CUDA(cudaMemcpyAsync(c->x.p, x0, ni * sizeof(float2), cudaMemcpyDeviceToDevice, s));
+  else PG_CUDA(cudaMemsetAsync(c->x.p, 0, ni * sizeof(float2), s));
+  PG_CUDA(cudaMemsetAsync(c->ddir.p, 0, ni * sizeof(float2), s));
+  pg_status st = PG_OK;
+  if (x0) st = A->forward(c->x.p, c->Ax.p, s);                       // :55
+  else PG_CUDA(cudaMemsetAsync(c->Ax.p, 0, nd * sizeof(float2), s));   // A * 0 = 0 exactly
+  if (st != PG_OK) { A->pcg_cache.reset(); return st; }
+  PG_LAUNCH(k_ywy, (unsigned)c->nbd, kRed, 0, s, nd, c->ybuf.p, c->wbuf.p, c->part.p, c->nbd, 0);
+  PG_LAUNCH(k_scalar_init, 1, 32, 0, s, c->part.p, c->nbd, 0, c->sc.p, c->fl.p);
+  PG_LAUNCH(k_residual, (unsigned)c->nbd, kRed, 0, s, nd, c->ybuf.p, c->Ax.p, c->wbuf.p, c->r.p);
+  uint64_t it = 0;
+  if (!c->exec && niter > 0) {
+    // the first iteration eagerly (it sizes every workspace), then one capture
+    st = c->iteration(A, s);
+    if (st != PG_OK) { A->pcg_cache.reset(); return st; }
+    it = 1;
+    if (graphs_enabled() && niter > 1) {
+      const uint64_t before = g_launches.load();
+      g_profile_suppress = true;
+      PG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      st = c->iteration(A, s);
+      cudaGraph_t graph = nullptr;
+      cudaError_t ce = cudaStreamEndCapture(s, &graph);
+      g_profile_suppress = false;
+      c->per_iter = g_launches.load() - before;
+      g_launches.fetch_sub(c->per_iter);
+      if (st != PG_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        A->pcg_cache.reset();
+        return st;
+      }
+      cudaGraphExec_t exec = nullptr;
+      if (ce == cudaSuccess) ce = cudaGraphInstantiate(&exec, graph, 0);
+      if (ce == cudaSuccess) {
+        c->graph = graph;
+        c->exec = exec;
+      } else {
+        // nothing captured ran: continue from the eager iteration without graphs
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        c->per_iter = 0;
+      }
+    }
+  }
+  for (; it < niter; ++it) {
+    if (c->exec) {
+      cudaError_t ce = cudaGraphLaunch(c->exec, s);
+      if (ce != cudaSuccess) {
+        cudaGetLastError();
+        A->pcg_cache.reset();
+        return set_error(PG_CUDA_ERROR, "graph launch: %s", cudaGetErrorString(ce));
+      }
+      count_launch(c->per_iter);
+    } else {
+      st = c->iteration(A, s);
+      if (st != PG_OK) { A->pcg_cache.reset(); return st; }
+    }
+  }
+  PG_CUDA(cudaMemcpyAsync(xout, c->x.p, ni * sizeof(float2), cudaMemcpyDeviceToDevice, s));
+  uint32_t done = 0;
+  PG_CUDA(cudaMemcpyAsync(&done, c->fl.p + F_COMPLETED, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   PG_CUDA(cudaStreamSynchronize(s));
   if (iters) *iters = done;
   return PG_OK;
@@ -1190,10 +1343,8 @@ pg_status pg_pcg_solve_lowrank_device(pg_op A, const void* x0, const void* W, co
                      (unsigned long long)rank, (unsigned long long)A->n_image);
   PG_TRY(ensure_init());
   cudaStream_t s = stream ? (cudaStream_t)stream : default_stream();
-  LowRankPen P;
-  PG_TRY(P.init(*R, rank, v, s));
-  return pcg_solve_lowrank(A, P, (const float2*)x0, (const float*)W, (const float2*)y, niter, (float2*)x_out,
-                           iters_done, s);
+  return pcg_solve_lowrank(A, *R, rank, v, (const float2*)x0, (const float*)W, (const float2*)y, niter,
+                           (float2*)x_out, iters_done, s);
 }
 
 pg_status pg_pcg_solve_lowrank(pg_op A, const float* x0, const float* W, const float* y, const pg_penalty* R,

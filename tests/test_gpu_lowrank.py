@@ -146,6 +146,39 @@ def test_lowrank_pcg_vs_oracle(pg, oracle, kind):
     assert it == ito and e <= PCG_TOL
 
 
+def test_lowrank_pcg_graph_reuse_and_eager(pg, oracle, monkeypatch):
+    """The captured iteration stays cached on the LRobj: a second solve with
+    another penalty basis rewrites the graph's basis matrices in place and must
+    match the oracle's solve with that basis; the same solve with graphs off
+    (the same kernels launched one by one, on a fresh LRobj) gives the same
+    image up to the order of the gridding's float atomics."""
+    from powergrid_b200 import synthetic as S
+    n, nimg = 32, 3
+    rank, beta, niter = nimg, 1e-2, 6
+    dev, ref = _reps_timeseg(pg, oracle, n, nimg)
+    v, v2 = _basis(rank, nimg, 8), _basis(rank, nimg, 11)
+    N, Nd = n * n, dev[0].n_data
+    A = pg.LRobj(N, Nd, rank, nimg, v, dev)
+    Ao = oracle.lowrank(N, Nd, rank, nimg, v, ref)
+    y = Ao.forward(np.concatenate([S.image(S.Rng(300 + k), N) for k in range(rank)])).astype(np.complex64)
+
+    def pen(vb):
+        return pg.R_lowRank(pg.TVPenalty(n, n, 1, beta, 0.1), rank, nimg, vb)
+
+    for vb in (v, v2):
+        x, it = pg.solve_pwls_pcg(None, A, None, y, pen(vb), niter)
+        xo, ito = oracle.pcg_lowrank(Ao, y, "tv", n, n, 1, beta, rank, vb, delta=0.1, niter=niter)
+        e = rel_l2(x, xo)
+        print(f"cached low-rank PCG: {it} vs {ito} iterations, rel {e:.2e}")
+        assert it == ito and e <= PCG_TOL
+    monkeypatch.setenv("PG_NO_GRAPH", "1")
+    A2 = pg.LRobj(N, Nd, rank, nimg, v, dev)
+    x2, it2 = pg.solve_pwls_pcg(None, A2, None, y, pen(v2), niter)
+    e2 = rel_l2(x2, x)
+    print(f"eager vs graph: {e2:.2e}")
+    assert it2 == it and e2 <= OP_TOL
+
+
 def test_lowrank_invalid_inputs(pg, oracle):
     """The reference's R_lowRank gradient needs rank == images; LRobj needs one
     operator of the stated shape per image."""
