@@ -76,6 +76,38 @@ void arena_release(Arena* a);   // after all work on a->stream that uses it
     if (s_ != PG_OK) return s_;     \
   } while (0)
 
+// Programmatic dependent launch, for the kernels of a PCG iteration: the
+// launch of the next kernel overlaps the previous kernel's completion.  A
+// kernel launched this way calls pdl_wait() before it touches memory; the
+// wait returns once the previous kernel has completed and its writes are
+// visible (for a kernel launched without the attribute it returns at once).
+// No kernel triggers its dependents early: successors' blocks resident next
+// to a running kernel measured slower than the launch gap they hide.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// PG_NO_PDL=1 launches those kernels in plain stream order (read once).
+bool pdl_enabled();
+
+#define PG_LAUNCH_PDL(kernel, grid, block, smem, strm_, ...)                                       \
+  do {                                                                                             \
+    cudaLaunchConfig_t cfg_ = {};                                                                  \
+    cfg_.gridDim = dim3(grid);                                                                     \
+    cfg_.blockDim = dim3(block);                                                                   \
+    cfg_.dynamicSmemBytes = (smem);                                                                \
+    cfg_.stream = (strm_);                                                                         \
+    cudaLaunchAttribute at_[1];                                                                    \
+    at_[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;                                \
+    at_[0].val.programmaticStreamSerializationAllowed = ::pg::pdl_enabled() ? 1 : 0;               \
+    cfg_.attrs = at_;                                                                              \
+    cfg_.numAttrs = 1;                                                                             \
+    cudaError_t e_ = cudaLaunchKernelEx(&cfg_, kernel, __VA_ARGS__);                               \
+    ::pg::count_launch();                                                                          \
+    if (e_ != cudaSuccess) {                                                                       \
+      cudaGetLastError();                                                                          \
+      return ::pg::set_error(PG_CUDA_ERROR, "%s:%d launch %s: %s", __FILE__, __LINE__, #kernel,    \
+                             cudaGetErrorString(e_));                                              \
+    }                                                                                              \
+  } while (0)
+
 // Kernel launch followed by a launch-error check.
 #define PG_LAUNCH(kernel, grid, block, smem, stream, ...)                                          \
   do {                                                                                             \

@@ -1,5 +1,6 @@
 // Library context: device selection, default stream, error strings,
 // allocation (with a host-side failure hook) and launch counting.
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 
@@ -9,6 +10,14 @@ namespace pg {
 
 std::atomic<uint64_t> g_launches{0};
 std::atomic<uint64_t> g_fail_alloc_countdown{0};
+
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("PG_NO_PDL");
+    return !(e && e[0] == '1');
+  }();
+  return on;
+}
 
 namespace {
 thread_local std::string t_last_error;

@@ -465,6 +465,7 @@ __global__ void __launch_bounds__(kT) k_fft_inv_rows(NufftGeom g, int L, const f
 // k takes grids k, k+8, ..., added by a fixed xor butterfly.
 __global__ void k_sum_images(uint64_t N, int B, const float2* __restrict__ Rimg, int accumulate,
                              float2* __restrict__ x) {
+  pdl_wait();
   const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int k = (int)(t & 7);
   const uint64_t p = t >> 3;
@@ -592,6 +593,7 @@ __global__ void __launch_bounds__(fused::kTF, 1)
     k_fft2_fwd_fused(NufftGeom g, int L, const float2* __restrict__ x, const float2* __restrict__ S, int c0,
                      const float2* __restrict__ E, const float2* __restrict__ Wo, const float* __restrict__ deapf,
                      const float2* __restrict__ tw, float2* __restrict__ grids) {
+  pdl_wait();
   using namespace fused;
   extern __shared__ float2 sh[];
   cg::cluster_group cluster = cg::this_cluster();
@@ -682,6 +684,7 @@ __global__ void __launch_bounds__(fused::kTF, 1)
                      const float2* __restrict__ S, int c0,
                      const float2* __restrict__ E, const float2* __restrict__ WoH, const float* __restrict__ deapf,
                      const float2* __restrict__ tw, float2* __restrict__ Rimg) {
+  pdl_wait();
   using namespace fused;
   extern __shared__ float2 sh[];
   cg::cluster_group cluster = cg::this_cluster();
@@ -778,13 +781,15 @@ pg_status launch_fused(Kern kern, int B, cudaStream_t s, Args... args) {
   cfg.blockDim = dim3(fused::kTF, 1, 1);
   cfg.dynamicSmemBytes = fused::smem;
   cfg.stream = s;
-  cudaLaunchAttribute attr[1];
+  cudaLaunchAttribute attr[2];
   attr[0].id = cudaLaunchAttributeClusterDimension;
   attr[0].val.clusterDim.x = fused::CL;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
+  attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;   // the kernels call pdl_wait()
+  attr[1].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
   cfg.attrs = attr;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = 2;
   PG_CUDA(cudaLaunchKernelEx(&cfg, kern, args...));
   count_launch();
   return PG_OK;
@@ -806,13 +811,15 @@ bool query_fused() {
   cfg.gridDim = dim3(fused::CL, 1, 1);
   cfg.blockDim = dim3(fused::kTF, 1, 1);
   cfg.dynamicSmemBytes = fused::smem;
-  cudaLaunchAttribute attr[1];
+  cudaLaunchAttribute attr[2];
   attr[0].id = cudaLaunchAttributeClusterDimension;
   attr[0].val.clusterDim.x = fused::CL;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
+  attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;   // the kernels call pdl_wait()
+  attr[1].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
   cfg.attrs = attr;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = 2;
   int nf = 0, na = 0;
   if (cudaOccupancyMaxActiveClusters(&nf, k_fft2_fwd_fused, &cfg) != cudaSuccess ||
       cudaOccupancyMaxActiveClusters(&na, k_fft2_adj_fused<true>, &cfg) != cudaSuccess) {
@@ -917,7 +924,7 @@ pg_status fftpass_adjoint(const NufftGeom& g, int B, int L, float2* grids, int c
       PG_TRY(launch_fused(k_fft2_adj_fused<false>, B, s, g, L, (const float2*)grids, (float2*)nullptr, S, c0, E,
                           WoH, deapf, tw, Rimg));
     const uint64_t N = g.nimg();
-    PG_LAUNCH(k_sum_images, ceil_div(N * 8, 256), 256, 0, s, N, B, Rimg, accumulate, x);
+    PG_LAUNCH_PDL(k_sum_images, ceil_div(N * 8, 256), 256, 0, s, N, B, Rimg, accumulate, x);
     return PG_OK;
   }
   if (g.dim == 2) {
@@ -936,7 +943,7 @@ pg_status fftpass_adjoint(const NufftGeom& g, int B, int L, float2* grids, int c
   }
   PG_TRY(d_rows_inv(lg, g, B, L, Qr, S, c0, E, WoH, deapf, tw, Rimg, s));
   const uint64_t N = g.nimg();
-  PG_LAUNCH(k_sum_images, ceil_div(N * 8, 256), 256, 0, s, N, B, Rimg, accumulate, x);
+  PG_LAUNCH_PDL(k_sum_images, ceil_div(N * 8, 256), 256, 0, s, N, B, Rimg, accumulate, x);
   return PG_OK;
 }
 

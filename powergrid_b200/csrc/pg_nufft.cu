@@ -301,6 +301,7 @@ __global__ void __launch_bounds__(128) k_gather(NufftGeom g, TileShape t, const 
                                                 const float2* __restrict__ aa, int K, int L,
                                                 const float2* __restrict__ grids, int Cb,
                                                 float2* __restrict__ data, uint64_t dstride) {
+  pdl_wait();
   using TG = TileGeo<DIM, T>;
   constexpr int CELLS = TG::CELLS, PY = TG::PY, PX = TG::PX, PLANE = TG::PLANE;
   extern __shared__ __align__(16) float2 sm2[];   // [c*KP + j][PZ][PX][PY] complex cells
@@ -678,6 +679,7 @@ __global__ void __launch_bounds__(256, spread2d_min_blocks(CC * KK))
                                                   const float2* __restrict__ y, uint64_t dstride, int nb, int L,
                                                   int smax, float wmax, float2* __restrict__ grids,
                                                   unsigned* __restrict__ queue, int nchunks, int nitems) {
+  pdl_wait();
   using TG = TileGeo<2, T>;
   constexpr int CELLS = TG::CELLS, PY = TG::PY;
   constexpr int NP = CC * KK;          // planes per item
@@ -1372,7 +1374,7 @@ static pg_status gather_launch_one(NufftPlan* p, const Binning* bin, const float
   PG_CUDA(cudaFuncSetAttribute(k_gather<DIM, T, CC, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   // a static grid: the persistent work-queue form measured ~4 % slower here
   dim3 grid(bin->nsub, ceil_div(nb, CC));
-  PG_LAUNCH((k_gather<DIM, T, CC, KP>), grid, 128, smem, s, p->g, bin->tile, bin->subprob.p, bin->start.p,
+  PG_LAUNCH_PDL((k_gather<DIM, T, CC, KP>), grid, 128, smem, s, p->g, bin->tile, bin->subprob.p, bin->start.p,
             bin->wxy.p, bin->wz.p, bin->perm.p, aa, bin->K, bin->L, p->work->grids.p, nb, y, dstride);
   return PG_OK;
 }
@@ -1471,7 +1473,7 @@ static pg_status spread2d_launch(NufftPlan* p, const Binning* bin, const float2*
   const int nitems = bin->nsub * nchunks;
   PG_TRY(ensure_queue(p, s));
   const int blocks = persistent_blocks((const void*)k_spread2d<T, CC, KK>, smem, nitems);
-  PG_LAUNCH((k_spread2d<T, CC, KK>), blocks, 256, smem, s, p->g, bin->tile, bin->subprob.p, bin->start.p, bin->wxy.p,
+  PG_LAUNCH_PDL((k_spread2d<T, CC, KK>), blocks, 256, smem, s, p->g, bin->tile, bin->subprob.p, bin->start.p, bin->wxy.p,
             bin->perm.p, aa, y, dstride, nb, bin->L, bin->submax, wmax, target, p->work->queue.p, nchunks, nitems);
   return PG_OK;
 }
