@@ -416,6 +416,20 @@ typedef struct pg_acq_request {
 } pg_acq_request;
 pg_status pg_submit_acquisitions(pg_server s, pg_acq_index ix, const pg_acq_request* req, uint64_t* ticket);
 
+/* ---- device-side index checks ------------------------------------------ */
+/* In the PG_CHECKS build (libpowergrid_b200_checks.so, build(checks=True))
+ * the gridding kernels check every index they derive from the sample binning
+ * (window start inside the tile, sample count within the staging area,
+ * permutation entry inside the data) and record the first failed check
+ * instead of making the access: *record = (site << 48) | (low 48 bits of the
+ * offending value), sites 1 spread sample count, 2 / 3 spread window start
+ * (3-D or generic / 2-D), 4 spread permutation entry, 5 gather window start,
+ * 6 gather permutation entry; 0 if no check failed since the last call.
+ * Reading clears the record and synchronises the device.  *enabled = 1 in
+ * the checks build; the product build has no checks (*enabled = 0, *record =
+ * 0). */
+pg_status pg_checks_read(uint64_t* record, int* enabled);
+
 /* ---- instrumentation and fault injection (host-side only) ------------ */
 /* Stage timing: while enabled, the NUFFT and Gdft pipelines record a CUDA
  * event pair around each stage kernel on the stream they run on (also inside

@@ -9,7 +9,10 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libpowergrid_b200.so")
+# PG_LIBRARY=checks loads the PG_CHECKS build (device-side index checks,
+# reported by pg_checks_read) instead of the product library.
+LIB_PATH = os.path.join(HERE, "lib", "libpowergrid_b200_checks.so" if os.environ.get("PG_LIBRARY") == "checks"
+                        else "libpowergrid_b200.so")
 
 P = C.c_void_p
 U64 = C.c_uint64
@@ -130,6 +133,7 @@ SIGNATURES = {
     "pg_wait": (C.c_int, [P, U64, C.POINTER(RequestStats)]),
     "pg_cancel": (C.c_int, [P, U64]),
     "pg_request_footprint": (U64, [C.POINTER(Request)]),
+    "pg_checks_read": (C.c_int, [C.POINTER(U64), C.POINTER(C.c_int)]),
     "pg_debug_fail_allocation_after": (None, [U64]),
     "pg_util_kb_lut": (U64, [F32, P, U64, C.POINTER(F32)]),
     "pg_profile_enable": (C.c_int, [C.c_int]),

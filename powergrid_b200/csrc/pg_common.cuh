@@ -108,6 +108,49 @@ bool pdl_enabled();
     }                                                                                              \
   } while (0)
 
+// ---- device-side index checks (PG_CHECKS builds) --------------------------
+// Built with -DPG_CHECKS (libpowergrid_b200_checks.so), the gridding kernels
+// check the indices their shared-memory and global accesses derive from the
+// binning — window starts inside the tile, sample counts within the staging
+// size, permutation entries inside the data — and, instead of accessing out of
+// bounds or trapping, record the first failure in a device word of their
+// translation unit and skip the access.  The record is (site << 48) | (low 48
+// bits of the offending value); pg_checks_read returns and clears it.  In the
+// product build PG_CHECK(...) is the constant true and the checks vanish.
+enum pg_check_site {
+  PG_SITE_SPREAD_COUNT = 1,    // item sample count > staging size
+  PG_SITE_SPREAD_WINDOW = 2,   // sample window start outside its tile (k_spread)
+  PG_SITE_SPREAD2D_WINDOW = 3, // run window start outside its tile (k_spread2d)
+  PG_SITE_SPREAD2D_PERM = 4,   // permutation entry outside the data (k_spread2d)
+  PG_SITE_GATHER_WINDOW = 5,   // sample window start outside its tile (k_gather)
+  PG_SITE_GATHER_PERM = 6,     // permutation entry outside the data (k_gather)
+};
+// Host side: every translation unit with checks registers a reader of its word.
+int register_check_reader(bool (*reader)(uint64_t* record));
+#ifdef PG_CHECKS
+__device__ __forceinline__ bool check_fail(unsigned long long* word, int site, long long v) {
+  atomicCAS(word, 0ull, ((unsigned long long)site << 48) | ((unsigned long long)v & 0xffffffffffffull));
+  return false;
+}
+#define PG_DEFINE_CHECK_WORD()                                                                     \
+  static __device__ unsigned long long pg_check_word_;                                             \
+  static bool pg_check_reader_(uint64_t* record) {                                                 \
+    unsigned long long v = 0, zero = 0;                                                            \
+    if (cudaMemcpyFromSymbol(&v, pg_check_word_, sizeof(v)) != cudaSuccess ||                      \
+        cudaMemcpyToSymbol(pg_check_word_, &zero, sizeof(zero)) != cudaSuccess) {                  \
+      cudaGetLastError();                                                                          \
+      return false;                                                                                \
+    }                                                                                              \
+    *record = v;                                                                                   \
+    return true;                                                                                   \
+  }                                                                                                \
+  static const int pg_check_registered_ = ::pg::register_check_reader(&pg_check_reader_);
+#define PG_CHECK(cond, site, val) ((cond) || ::pg::check_fail(&pg_check_word_, (site), (long long)(val)))
+#else
+#define PG_DEFINE_CHECK_WORD()
+#define PG_CHECK(cond, site, val) true
+#endif
+
 // Kernel launch followed by a launch-error check.
 #define PG_LAUNCH(kernel, grid, block, smem, stream, ...)                                          \
   do {                                                                                             \

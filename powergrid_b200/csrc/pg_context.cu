@@ -3,6 +3,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "pg_common.cuh"
 
@@ -10,6 +11,18 @@ namespace pg {
 
 std::atomic<uint64_t> g_launches{0};
 std::atomic<uint64_t> g_fail_alloc_countdown{0};
+
+namespace {
+std::vector<bool (*)(uint64_t*)>& check_readers() {
+  static std::vector<bool (*)(uint64_t*)> r;
+  return r;
+}
+}  // namespace
+
+int register_check_reader(bool (*reader)(uint64_t* record)) {
+  check_readers().push_back(reader);
+  return 0;
+}
 
 bool pdl_enabled() {
   static const bool on = [] {
@@ -197,6 +210,24 @@ const char* pg_status_string(pg_status s) {
 const char* pg_last_error(void) { return pg::t_last_error.c_str(); }
 
 uint64_t pg_kernel_launch_count(void) { return pg::g_launches.load(); }
+
+pg_status pg_checks_read(uint64_t* record, int* enabled) {
+  if (!record || !enabled) return pg::set_error(PG_INVALID_ARG, "checks: null argument");
+#ifdef PG_CHECKS
+  *enabled = 1;
+#else
+  *enabled = 0;
+#endif
+  *record = 0;
+  PG_TRY(pg::ensure_init());
+  PG_CUDA(cudaDeviceSynchronize());
+  for (auto* rd : pg::check_readers()) {
+    uint64_t v = 0;
+    if (!rd(&v)) return pg::set_error(PG_CUDA_ERROR, "checks: reading the device record failed");
+    if (*record == 0) *record = v;
+  }
+  return PG_OK;
+}
 
 void pg_debug_fail_allocation_after(uint64_t n) { pg::g_fail_alloc_countdown.store(n); }
 

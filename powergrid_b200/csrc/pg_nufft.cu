@@ -36,6 +36,9 @@
 
 namespace pg {
 
+PG_DEFINE_CHECK_WORD()
+
+
 // ---------------------------------------------------------------------------
 // Host tables, with the operand types of the reference so the values agree.
 // ---------------------------------------------------------------------------
@@ -344,6 +347,10 @@ __global__ void __launch_bounds__(128) k_gather(NufftGeom g, TileShape t, const 
   for (int s = first + threadIdx.x; s < end; s += blockDim.x) {
     const uint2 st = start[s];
     const int ox = (int)(st.x & 0xffff) - x0, oy = (int)(st.x >> 16) - y0;
+    if (!PG_CHECK(ox >= 0 && ox < T && oy >= 0 && oy < T &&
+                      (DIM == 2 || ((int)st.y - z0 >= 0 && (int)st.y - z0 < TG::TZ)),
+                  PG_SITE_GATHER_WINDOW, ox * 65536 + oy))
+      continue;
     const float4* w4 = reinterpret_cast<const float4*>(wxy + (uint64_t)s * 16);
     const float4 wa = w4[0], wb = w4[1], wc = w4[2], wd = w4[3];
     const float wxr[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
@@ -381,6 +388,7 @@ __global__ void __launch_bounds__(128) k_gather(NufftGeom g, TileShape t, const 
       }
     }
     const uint32_t o = perm[s];
+    if (!PG_CHECK(o < dstride, PG_SITE_GATHER_PERM, o)) continue;
 #pragma unroll
     for (int c = 0; c < CC; ++c) {
       if (c >= ncl) break;
@@ -454,6 +462,7 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
   const int cfirst = c0 + (item % nchunks) * cc;
   const int tile = sp.x, first = sp.z, count = sp.w;
   const int lseg = sp.y;
+  if (!PG_CHECK(count <= smax, PG_SITE_SPREAD_COUNT, count)) continue;   // uniform across the block
   const int ty = tile % t.nty;
   const int txz = tile / t.nty;
   const int tx = txz % t.ntx;
@@ -551,9 +560,14 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
       const uint2 st = sst[i];
       if (st.x != prev) {                  // uniform across the warp
         if (open) flush_run();
-        open = true;
+        open = false;
         prev = st.x;
         const int ox = (int)(st.x & 0xffff) - x0, oy = (int)(st.x >> 16) - y0;
+        if (!PG_CHECK(ox >= 0 && ox < T && oy >= 0 && oy < T, PG_SITE_SPREAD_WINDOW, ox * 65536 + oy)) {
+          prev = 0xffffffffu;
+          continue;
+        }
+        open = true;
         b = smi + (ox + dx) * PY + oy + dy;
 #pragma unroll
         for (int pl = 0; pl < NPC; ++pl) a0[pl] = a1[pl] = make_float2(0.f, 0.f);
@@ -576,6 +590,10 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
     for (int i = warp; i < count; i += NW) {
       const uint2 st = sst[i];
       const int ox = (int)(st.x & 0xffff) - x0, oy = (int)(st.x >> 16) - y0;
+      if (!PG_CHECK(ox >= 0 && ox < T && oy >= 0 && oy < T &&
+                        (DIM == 2 || ((int)st.y - z0 >= 0 && (int)st.y - z0 < TG::TZ)),
+                    PG_SITE_SPREAD_WINDOW, ox * 65536 + oy))
+        continue;                          // uniform across the warp
       const float* w = sw + i * WROW;
       const float wyv = w[8 + dy];
       const float w0 = w[dx] * wyv, w1 = w[dx + 4] * wyv;
@@ -718,6 +736,7 @@ __global__ void __launch_bounds__(256, spread2d_min_blocks(CC * KK))
     const int cfirst = (item % nchunks) * CC;
     const int ncl = min(CC, nb - cfirst);
     const int tile_i = sp.x, lseg = sp.y, first = sp.z, count = sp.w;
+    if (!PG_CHECK(count <= smax, PG_SITE_SPREAD_COUNT, count)) continue;   // uniform across the block
     const int x0 = (tile_i / t.nty) * T, y0 = (tile_i % t.nty) * T;
 
     // 1. staging
@@ -733,7 +752,10 @@ __global__ void __launch_bounds__(256, spread2d_min_blocks(CC * KK))
       for (int i = tid / CC; i < count; i += blockDim.x / CC) {
         const uint64_t s = (uint64_t)(first + i);
         float2 d = make_float2(0.f, 0.f);
-        if (c < ncl) d = y[(uint64_t)(cfirst + c) * dstride + perm[s]];
+        if (c < ncl) {
+          const uint32_t ps = perm[s];
+          if (PG_CHECK(ps < dstride, PG_SITE_SPREAD2D_PERM, ps)) d = y[(uint64_t)(cfirst + c) * dstride + ps];
+        }
 #pragma unroll
         for (int j = 0; j < KK; ++j) {
           const float2 v = aa ? cmul(cconj(aa[s * KK + j]), d) : d;
@@ -805,9 +827,14 @@ __global__ void __launch_bounds__(256, spread2d_min_blocks(CC * KK))
         const uint32_t st = sst[i];
         if (st != prev) {              // uniform across the warp
           if (open) flush_run();
-          open = true;
+          open = false;
           prev = st;
           const int ox = (int)(st & 0xffff) - x0, oy = (int)(st >> 16) - y0;
+          if (!PG_CHECK(ox >= 0 && ox < T && oy >= 0 && oy < T, PG_SITE_SPREAD2D_WINDOW, ox * 65536 + oy)) {
+            prev = 0xffffffffu;
+            continue;
+          }
+          open = true;
           b = tile + (ox + dx) * PY + oy + dy;
 #pragma unroll
           for (int pl = 0; pl < NP; ++pl) a0[pl] = a1[pl] = make_float2(0.f, 0.f);
