@@ -287,7 +287,8 @@ __device__ __forceinline__ int next_item(unsigned* q, int nitems) {
 }
 
 // ---------------------------------------------------------------------------
-// Forward interpolation, tiled: one block per (subproblem, coil chunk).  The
+// Forward interpolation, tiled: one block per (subproblem, coil chunk), in 2-D
+// two for subproblems of more than kGatherHalf samples.  The
 // padded tiles of the subproblem's KP segment grids for CC coils are staged in
 // shared memory as complex cells ([c][j][PZ][PX][PY]).  Then one thread per
 // sample reads its 8^d cells of every (coil, segment) plane and sums them in
@@ -297,6 +298,8 @@ __device__ __forceinline__ int next_item(unsigned* q, int nitems) {
 // so their shared-memory reads broadcast.  The segment interpolator AA is
 // applied per coil on the way out.
 // ---------------------------------------------------------------------------
+constexpr int kGatherHalf = 128;   // 2-D subproblems above this are gathered by two blocks
+
 template <int DIM, int T, int CC, int KP>
 __global__ void __launch_bounds__(128) k_gather(NufftGeom g, TileShape t, const int4* __restrict__ sub,
                                                 const uint2* __restrict__ start, const float* __restrict__ wxy,
@@ -308,10 +311,18 @@ __global__ void __launch_bounds__(128) k_gather(NufftGeom g, TileShape t, const 
   using TG = TileGeo<DIM, T>;
   constexpr int CELLS = TG::CELLS, PY = TG::PY, PX = TG::PX, PLANE = TG::PLANE;
   extern __shared__ __align__(16) float2 sm2[];   // [c*KP + j][PZ][PX][PY] complex cells
-  const int4 sp = sub[blockIdx.x];
+  // In 2-D two blocks share a subproblem of more than kGatherHalf samples,
+  // one per half (more blocks to cover the staging latency; each stages the
+  // tile); the second block of a smaller subproblem has nothing to do.
+  constexpr int SPLIT = (DIM == 2) ? 2 : 1;
+  const int4 sp = sub[blockIdx.x / SPLIT];
+  const int part = blockIdx.x % SPLIT;
+  const int head = (SPLIT == 2 && sp.w > kGatherHalf) ? (sp.w + 1) / 2 : sp.w;
+  const int first = sp.z + part * head, count = part ? sp.w - head : head;
+  if (count <= 0) return;
   const int cfirst = blockIdx.y * CC;
   const int ncl = min(CC, Cb - cfirst);
-  const int tile = sp.x, lseg = sp.y, first = sp.z, count = sp.w;
+  const int tile = sp.x, lseg = sp.y;
   const int ty = tile % t.nty;
   const int txz = tile / t.nty;
   const int tx = txz % t.ntx;
@@ -1400,7 +1411,7 @@ static pg_status gather_launch_one(NufftPlan* p, const Binning* bin, const float
   const size_t smem = (size_t)CC * KP * 2 * TileGeo<DIM, T>::CELLS * sizeof(float);
   PG_CUDA(cudaFuncSetAttribute(k_gather<DIM, T, CC, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   // a static grid: the persistent work-queue form measured ~4 % slower here
-  dim3 grid(bin->nsub, ceil_div(nb, CC));
+  dim3 grid(bin->nsub * (DIM == 2 ? 2 : 1), ceil_div(nb, CC));
   PG_LAUNCH_PDL((k_gather<DIM, T, CC, KP>), grid, 128, smem, s, p->g, bin->tile, bin->subprob.p, bin->start.p,
             bin->wxy.p, bin->wz.p, bin->perm.p, aa, bin->K, bin->L, p->work->grids.p, nb, y, dstride);
   return PG_OK;
