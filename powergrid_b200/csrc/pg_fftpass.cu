@@ -227,6 +227,7 @@ __global__ void __launch_bounds__(kT) k_fft_fwd_rows(NufftGeom g, int L, const f
                                                      const float2* __restrict__ E, const float2* __restrict__ Wo,
                                                      const float* __restrict__ deapf, const float2* __restrict__ tw,
                                                      float2* __restrict__ P) {
+  pdl_wait();
   using RG = RowGeo<LOGN>;
   constexpr int R1 = RG::R1, R2 = RG::R2, n = RG::n, RB = RG::RB, S2 = RG::S2, RS = RG::RS;
   extern __shared__ float2 sh[];
@@ -290,6 +291,7 @@ __global__ void __launch_bounds__(kT) k_fft_fwd_rows(NufftGeom g, int L, const f
 template <int LOGN>
 __global__ void __launch_bounds__(kT) k_fft_fwd_cols(Lines ln, const float2* __restrict__ P,
                                                      const float2* __restrict__ tw, float2* __restrict__ out) {
+  pdl_wait();
   using CG = ColGeo<LOGN>;
   constexpr int R1 = CG::R1, R2 = CG::R2, CB = CG::CB;
   extern __shared__ float2 sh[];
@@ -342,6 +344,7 @@ __global__ void __launch_bounds__(kT) k_fft_fwd_cols(Lines ln, const float2* __r
 template <int LOGN, bool CLEAR>
 __global__ void __launch_bounds__(kT) k_fft_inv_cols(Lines ln, const float2* __restrict__ in, float2* inw,
                                                      const float2* __restrict__ tw, float2* __restrict__ Q) {
+  pdl_wait();
   using CG = ColGeo<LOGN>;
   constexpr int R1 = CG::R1, R2 = CG::R2, CB = CG::CB;
   extern __shared__ float2 sh[];
@@ -406,6 +409,7 @@ __global__ void __launch_bounds__(kT) k_fft_inv_rows(NufftGeom g, int L, const f
                                                      const float2* __restrict__ E, const float2* __restrict__ WoH,
                                                      const float* __restrict__ deapf, const float2* __restrict__ tw,
                                                      float2* __restrict__ Rimg) {
+  pdl_wait();
   using RG = RowGeo<LOGN>;
   constexpr int R1 = RG::R1, R2 = RG::R2, n = RG::n, RB = RG::RB, S2 = RG::S2, RS = RG::RS;
   extern __shared__ float2 sh[];
@@ -485,7 +489,7 @@ pg_status rows_fwd(const NufftGeom& g, int B, int L, const float2* x, const floa
                    const float2* Wo, const float* deapf, const float2* tw, float2* P, cudaStream_t s) {
   using RG = RowGeo<LOGN>;
   PG_CUDA(cudaFuncSetAttribute(k_fft_fwd_rows<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RG::smem));
-  PG_LAUNCH(k_fft_fwd_rows<LOGN>, dim3(ceil_div((uint64_t)g.Nx * g.Nz, RG::RB), B), kT, RG::smem, s, g, L, x, S, c0,
+  PG_LAUNCH_PDL(k_fft_fwd_rows<LOGN>, dim3(ceil_div((uint64_t)g.Nx * g.Nz, RG::RB), B), kT, RG::smem, s, g, L, x, S, c0,
             E, Wo, deapf, tw, P);
   return PG_OK;
 }
@@ -495,7 +499,7 @@ pg_status rows_inv(const NufftGeom& g, int B, int L, const float2* Q, const floa
                    const float2* WoH, const float* deapf, const float2* tw, float2* Rimg, cudaStream_t s) {
   using RG = RowGeo<LOGN>;
   PG_CUDA(cudaFuncSetAttribute(k_fft_inv_rows<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RG::smem));
-  PG_LAUNCH(k_fft_inv_rows<LOGN>, dim3(ceil_div((uint64_t)g.Nx * g.Nz, RG::RB), B), kT, RG::smem, s, g, L, Q, S, c0,
+  PG_LAUNCH_PDL(k_fft_inv_rows<LOGN>, dim3(ceil_div((uint64_t)g.Nx * g.Nz, RG::RB), B), kT, RG::smem, s, g, L, Q, S, c0,
             E, WoH, deapf, tw, Rimg);
   return PG_OK;
 }
@@ -504,7 +508,7 @@ template <int LOGN>
 pg_status cols_fwd(const Lines& ln, int B, const float2* P, const float2* tw, float2* out, cudaStream_t s) {
   using CG = ColGeo<LOGN>;
   PG_CUDA(cudaFuncSetAttribute(k_fft_fwd_cols<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CG::smem));
-  PG_LAUNCH(k_fft_fwd_cols<LOGN>, dim3(ceil_div(ln.ncols, CG::CB), B), kT, CG::smem, s, ln, P, tw, out);
+  PG_LAUNCH_PDL(k_fft_fwd_cols<LOGN>, dim3(ceil_div(ln.ncols, CG::CB), B), kT, CG::smem, s, ln, P, tw, out);
   return PG_OK;
 }
 
@@ -514,11 +518,11 @@ pg_status cols_inv(const Lines& ln, int B, float2* in, int clear, const float2* 
   if (clear) {
     PG_CUDA(cudaFuncSetAttribute(k_fft_inv_cols<LOGN, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)CG::smem));
-    PG_LAUNCH((k_fft_inv_cols<LOGN, true>), dim3(ceil_div(ln.ncols, CG::CB), B), kT, CG::smem, s, ln, in, in, tw, Q);
+    PG_LAUNCH_PDL((k_fft_inv_cols<LOGN, true>), dim3(ceil_div(ln.ncols, CG::CB), B), kT, CG::smem, s, ln, in, in, tw, Q);
   } else {
     PG_CUDA(cudaFuncSetAttribute(k_fft_inv_cols<LOGN, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)CG::smem));
-    PG_LAUNCH((k_fft_inv_cols<LOGN, false>), dim3(ceil_div(ln.ncols, CG::CB), B), kT, CG::smem, s, ln, in, nullptr,
+    PG_LAUNCH_PDL((k_fft_inv_cols<LOGN, false>), dim3(ceil_div(ln.ncols, CG::CB), B), kT, CG::smem, s, ln, in, nullptr,
               tw, Q);
   }
   return PG_OK;

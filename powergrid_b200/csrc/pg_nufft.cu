@@ -189,6 +189,7 @@ __device__ __forceinline__ int parity3(int a, int b, int c) { return (a + b + c)
 __global__ void k_pre(NufftGeom g, int L, const float2* __restrict__ x, const float2* __restrict__ S, int c0,
                       const float2* __restrict__ E, const float2* __restrict__ Wo, const float* __restrict__ deapf,
                       float2* __restrict__ grids) {
+  pdl_wait();
   const uint64_t N = g.nimg();
   const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= N) return;
@@ -452,6 +453,7 @@ __global__ void __launch_bounds__(256) k_spread(NufftGeom g, TileShape t, const 
                                                 uint64_t M, int K, int L, int c0, int cc, int smax, float wmax,
                                                 float2* __restrict__ grids, unsigned* __restrict__ queue,
                                                 int nchunks, int nitems) {
+  pdl_wait();
   using TG = TileGeo<DIM, T>;
   constexpr int CELLS = TG::CELLS, PY = TG::PY, PX = TG::PX, PLANE = TG::PLANE;
   constexpr int WROW = spread_wrow(DIM);   // staged weights per sample: wx[8] wy[8] (wz[8])
@@ -922,6 +924,7 @@ template <int CP, int LP>
 __global__ void k_post(NufftGeom g, int Cb, int L, const float2* __restrict__ grids, const float2* __restrict__ S,
                        int c0, const float2* __restrict__ E, const float2* __restrict__ WoH,
                        const float* __restrict__ deapf, int accumulate, float2* __restrict__ x) {
+  pdl_wait();
   constexpr int LN = CP * LP;
   const uint64_t N = g.nimg();
   const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1466,7 +1469,7 @@ static pg_status spread_launch_np(NufftPlan* p, const Binning* bin, const Spread
   const int nitems = bin->nsub * a.nchunks;
   PG_TRY(ensure_queue(p, s));
   const int blocks = persistent_blocks((const void*)k_spread<DIM, T, NP>, a.smem, nitems);
-  PG_LAUNCH((k_spread<DIM, T, NP>), blocks, 256, a.smem, s, p->g, bin->tile, bin->subprob.p, bin->start.p,
+  PG_LAUNCH_PDL((k_spread<DIM, T, NP>), blocks, 256, a.smem, s, p->g, bin->tile, bin->subprob.p, bin->start.p,
             bin->wxy.p, bin->wz.p, a.vs, bin->M, bin->K, bin->L, a.c0, a.cc, bin->submax, a.wmax, target,
             p->work->queue.p, a.nchunks, nitems);
   return PG_OK;
@@ -1536,7 +1539,7 @@ template <int CP, int LP>
 static pg_status post_launch(NufftPlan* p, int nb, int L, const NufftBatch& b, const float2* WoH,
                              const float2* grids, int c0, int acc, float2* x, cudaStream_t s) {
   const uint64_t N = p->g.nimg();
-  PG_LAUNCH((k_post<CP, LP>), ceil_div(N * CP * LP, 256), 256, 0, s, p->g, nb, L, grids, b.S, c0, b.E, WoH,
+  PG_LAUNCH_PDL((k_post<CP, LP>), ceil_div(N * CP * LP, 256), 256, 0, s, p->g, nb, L, grids, b.S, c0, b.E, WoH,
             p->deapf.p, acc, x);
   return PG_OK;
 }
@@ -1598,14 +1601,14 @@ pg_status nufft_forward(NufftPlan* p, const NufftBatch& b, const float2* x, floa
         for (int i0 = c0; i0 < c0 + nb;) {
           const int img = i0 / b.cgroup;
           const int i1 = std::min(c0 + nb, (img + 1) * b.cgroup);
-          PG_LAUNCH(k_pre, dim3(ceil_div(g.nimg(), 256), (i1 - i0) * L), 256, 0, s, g, L,
+          PG_LAUNCH_PDL(k_pre, dim3(ceil_div(g.nimg(), 256), (i1 - i0) * L), 256, 0, s, g, L,
                     x + (uint64_t)img * b.image_stride, b.S, i0, b.E,
                     b.Wo ? b.Wo + (uint64_t)img * b.phase_stride : nullptr, p->deapf.p,
                     p->work->fin.p + (uint64_t)(i0 - c0) * L * G);
           i0 = i1;
         }
       } else {
-        PG_LAUNCH(k_pre, dim3(ceil_div(g.nimg(), 256), B), 256, 0, s, g, L, x, b.S, c0, b.E, b.Wo, p->deapf.p,
+        PG_LAUNCH_PDL(k_pre, dim3(ceil_div(g.nimg(), 256), B), 256, 0, s, g, L, x, b.S, c0, b.E, b.Wo, p->deapf.p,
                   p->work->fin.p);
       }
     }
