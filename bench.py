@@ -382,6 +382,10 @@ def run_gpu_arm(args):
             line["serving"] = run_serving()
         if ws == 1 and not args.no_gdft:
             line["gdft"] = gdft_block(5, 3, stream, with_error=not args.no_cpu_baseline)
+        if ws == 1 and not args.no_secondary:
+            # the other configurations' solve rates, measured in the same run: cfg1 (10-iteration 2-D
+            # solves, launch-bound) and cfg5 (one 30-iteration 3-D pcSenseTimeSeg TV solve, ~20 s)
+            line["secondary"] = {"cfg1": run_workload("cfg1", 20, 5), "cfg5": run_workload("cfg5", 1, 3)}
         print(json.dumps(line))
     if ws > 1:
         torch.distributed.barrier()
@@ -824,6 +828,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the config-4 serving stream")
     ap.add_argument("--no-gdft", action="store_true", help="skip the config-3 Gdft block")
+    ap.add_argument("--no-secondary", action="store_true", help="skip the cfg1 and cfg5 solve-rate blocks")
     ap.add_argument("--serving-only", action="store_true", help="only the config-4 serving stream")
     ap.add_argument("--workload", default=None, choices=["cfg1", "cfg3", "cfg5", "direct", "cpu"],
                     help="a secondary workload instead")
