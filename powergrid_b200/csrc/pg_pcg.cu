@@ -28,6 +28,8 @@
 #include <cstring>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "pg_ops.cuh"
 #include "pg_profile.cuh"
 
@@ -60,28 +62,38 @@ __device__ __forceinline__ float wpot(const PenDev& R, float2 d) {
   return 1.f / sqrtf(1.f + a * a);
 }
 
+// Loads of the stencil helpers: plain, or through L2 only (CG) for data that
+// other CTAs of the same launch wrote.
+template <bool CG>
+__device__ __forceinline__ float2 ldv(const float2* p, uint64_t i) {
+  if constexpr (CG) return __ldcg(p + i);
+  else return p[i];
+}
+
+template <bool CG = false>
 __device__ __forceinline__ float2 zval(const float2* __restrict__ x, const float2* __restrict__ d, float st,
                                        uint64_t i) {
-  const float2 a = x[i];
+  const float2 a = ldv<CG>(x, i);
   if (!d) return a;
-  const float2 b = d[i];
+  const float2 b = ldv<CG>(d, i);
   return make_float2(a.x + st * b.x, a.y + st * b.y);
 }
 
 // beta * sum_dims Ctd(dpot(Cd z))[j], z = x + st*d.
+template <bool CG = false>
 __device__ __forceinline__ float2 grad_at(const PenDev& R, const float2* __restrict__ x, const float2* __restrict__ d,
                                           float st, uint64_t j) {
   float2 g = make_float2(0.f, 0.f);
-  const float2 zj = zval(x, d, st, j);
+  const float2 zj = zval<CG>(x, d, st, j);
   for (int dim = 0; dim < R.nd; ++dim) {
     const uint64_t off = R.off[dim];
     if (off >= R.N) continue;
     const uint64_t last = R.N - 1 - off;
     if (j > last) continue;
     float2 vj = make_float2(0.f, 0.f);
-    if (j >= off) vj = dpot(R, csub(zj, zval(x, d, st, j - off)));
+    if (j >= off) vj = dpot(R, csub(zj, zval<CG>(x, d, st, j - off)));
     if (j < last) {
-      const float2 vn = dpot(R, csub(zval(x, d, st, j + off), zj));
+      const float2 vn = dpot(R, csub(zval<CG>(x, d, st, j + off), zj));
       g = cadd(g, csub(vj, vn));
     } else {
       g = cadd(g, vj);
@@ -338,6 +350,132 @@ __global__ void k_ddir_quad(PenDev R, const float2* __restrict__ ngrad, const fl
   }
 }
 
+// k_ngrad followed by k_ddir_quad in one launch, for images of at most
+// kImgMax voxels and one segment: one cluster of kImgCL CTAs covers the whole
+// image, so the grid-wide step between the two (the CG coefficient needs the
+// sum over all voxels) is a cluster barrier instead of a kernel boundary and a
+// last-block reduction.  It pays while the image fits one voxel per thread:
+// at 64x64 a solve runs 4.4 % faster (19.7k vs 18.9k iterations/s), while at
+// 128x128 (two voxels per thread on 8 SMs) the two kernels over 64 SMs win
+// (8.77k vs 8.55k).  Each CTA sums the CTAs' partials itself, in rank
+// order, so every CTA holds the same FP64 totals and the same coefficient.
+// Same per-voxel arithmetic as the two kernels; the FP64 sums are added in a
+// different (fixed) order.
+namespace cgx = cooperative_groups;
+constexpr int kImgCL = 8, kImgT = 1024, kImgPer = 1;
+constexpr uint64_t kImgMax = (uint64_t)kImgCL * kImgT * kImgPer;
+
+// Sum of NV doubles over the CTA into red[0..NV) (thread 0 writes; all threads
+// must call it; ends with a barrier).
+template <int NV>
+__device__ __forceinline__ void cta_sum(double (&v)[NV], double* red) {
+  __shared__ double sw[NV][kImgT / 32];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    const double t = warp_sum(v[k]);
+    if (l == 0) sw[k][w] = t;
+  }
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double t = sw[k][l];   // kImgT / 32 == 32 warps
+      t = warp_sum(t);
+      if (l == 0) red[k] = t;
+    }
+  }
+  __syncthreads();
+}
+
+// Totals over the cluster's CTAs, added in rank order (identical in every CTA).
+template <int NV>
+__device__ __forceinline__ void cluster_totals(cgx::cluster_group& cl, double* red, double (&tot)[NV]) {
+#pragma unroll
+  for (int k = 0; k < NV; ++k) tot[k] = 0.0;
+  for (int q = 0; q < kImgCL; ++q) {
+    const double* rq = cl.map_shared_rank(red, q);
+#pragma unroll
+    for (int k = 0; k < NV; ++k) tot[k] += rq[k];
+  }
+}
+
+__global__ void __launch_bounds__(kImgT, 1)
+    k_image_step_quad(PenDev R, const float2* __restrict__ x, float2* ngrad, float2* ddir, float2* ddir_prev,
+                      double* sc, uint32_t* fl) {
+  pdl_wait();
+  cgx::cluster_group cl = cgx::this_cluster();
+  __shared__ double redA[2], redB[4];
+  const bool done0 = fl[F_DONE] != 0;     // the same value in every CTA
+  const uint64_t stride = (uint64_t)kImgCL * kImgT;
+  const uint64_t t0 = (uint64_t)cl.block_rank() * kImgT + threadIdx.x;
+  if (!done0) {
+    // gradient: ngrad = A'r - R.Gradient(x), the previous direction kept (k_ngrad)
+    double v[2] = {0.0, 0.0};
+    for (uint64_t j = t0; j < R.N; j += stride) {
+      ddir_prev[j] = ddir[j];
+      const float2 raw = ngrad[j];
+      v[0] += (double)raw.x * raw.x + (double)raw.y * raw.y;
+      const float2 g = grad_at(R, x, nullptr, 0.f, j);
+      const float2 u = csub(raw, g);
+      ngrad[j] = u;
+      v[1] += (double)u.x * u.x + (double)u.y * u.y;
+    }
+    cta_sum<2>(v, redA);
+  }
+  cl.sync();   // every CTA's ngrad / ddir_prev writes and partials are visible cluster-wide
+  bool done = done0;
+  float gm = 0.f;
+  if (!done) {
+    double tot[2];
+    cluster_totals<2>(cl, redA, tot);
+    const double gn = tot[0], nw = tot[1];
+    if (sqrt(gn) / sc[S_YWY] < 1e-10) {
+      done = true;
+      if (cl.block_rank() == 0 && threadIdx.x == 0) { fl[F_DONE] = 1; fl[F_REASON] = 1; }
+    } else {
+      double gamma = 0.0;
+      if (fl[F_IT] > 0) gamma = (fabs(sc[S_OLD]) < 1e-10) ? 0.0 : nw / sc[S_OLD];
+      gm = (float)gamma;
+      cl.sync();   // every CTA has read sc[S_OLD] before rank 0 replaces it
+      if (cl.block_rank() == 0 && threadIdx.x == 0) { sc[S_GAMMA] = gamma; sc[S_OLD] = nw; }
+    }
+  }
+  if (!done) {
+    // direction and the quadratic line-search sums (k_ddir_quad)
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    // ngrad and ddir_prev at neighbouring voxels come from other CTAs: L2 loads
+    for (uint64_t j = t0; j < R.N; j += stride) {
+      const float2 g = ldv<true>(ngrad, j);
+      const float2 dj = zval<true>(ngrad, ddir_prev, gm, j);
+      ddir[j] = dj;
+      v[0] += (double)dj.x * g.x + (double)dj.y * g.y;
+      for (int dim = 0; dim < R.nd; ++dim) {
+        const uint64_t off = R.off[dim];
+        if (j < off || off >= R.N) continue;
+        const float2 cd = csub(dj, zval<true>(ngrad, ddir_prev, gm, j - off));
+        v[1] += (double)cd.x * cd.x + (double)cd.y * cd.y;
+      }
+      const float2 gx = grad_at(R, x, nullptr, 0.f, j);
+      const float2 gd = grad_at<true>(R, ngrad, ddir_prev, gm, j);
+      v[2] += (double)dj.x * gx.x + (double)dj.y * gx.y;
+      v[3] += (double)dj.x * gd.x + (double)dj.y * gd.y;
+    }
+    cta_sum<4>(v, redB);
+    cl.sync();
+    double tot[4];
+    cluster_totals<4>(cl, redB, tot);
+    if (cl.block_rank() == 0 && threadIdx.x == 0) {
+      sc[S_DIRDOT] = tot[0];
+      sc[S_PDEN] = tot[1];
+      sc[S_PDOT0] = tot[2];
+      sc[S_Q1] = tot[3];
+      if (tot[0] < 0) { fl[F_DONE] = 1; fl[F_REASON] = 2; }
+    }
+  }
+  cl.sync();   // no CTA leaves while another reads its shared memory
+}
+
 // The three Newton steps of the quadratic penalty (:132-150) from the sums
 // k_ddir_quad stored: Gradient is linear and wpot = 1, so pdenom is fixed and
 // pdot(s) = pdot(0) + s Re<ddir, Gradient(ddir)>.
@@ -502,6 +640,52 @@ PenDev make_pen(const pg_penalty& R) {
   return p;
 }
 
+// Whether k_image_step_quad can run: one cluster of kImgCL CTAs of kImgT
+// threads must fit (checked once); PG_IMAGE_STEP=0 keeps the two kernels.
+bool image_step_ok() {
+  static const bool ok = [] {
+    const char* e = getenv("PG_IMAGE_STEP");
+    if (e && e[0] == '0') return false;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kImgCL, 1, 1);
+    cfg.blockDim = dim3(kImgT, 1, 1);
+    cudaLaunchAttribute a[1];
+    a[0].id = cudaLaunchAttributeClusterDimension;
+    a[0].val.clusterDim.x = kImgCL;
+    a[0].val.clusterDim.y = 1;
+    a[0].val.clusterDim.z = 1;
+    cfg.attrs = a;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k_image_step_quad, &cfg) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    return n >= 1;
+  }();
+  return ok;
+}
+
+pg_status launch_image_step(const PenDev& R, const float2* x, float2* ngrad, float2* ddir, float2* ddir_prev,
+                            double* sc, uint32_t* fl, cudaStream_t s) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(kImgCL, 1, 1);
+  cfg.blockDim = dim3(kImgT, 1, 1);
+  cfg.stream = s;
+  cudaLaunchAttribute a[2];
+  a[0].id = cudaLaunchAttributeClusterDimension;
+  a[0].val.clusterDim.x = kImgCL;
+  a[0].val.clusterDim.y = 1;
+  a[0].val.clusterDim.z = 1;
+  a[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;   // the kernel calls pdl_wait()
+  a[1].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+  cfg.attrs = a;
+  cfg.numAttrs = 2;
+  PG_CUDA(cudaLaunchKernelEx(&cfg, k_image_step_quad, R, x, ngrad, ddir, ddir_prev, sc, fl));
+  count_launch();
+  return PG_OK;
+}
+
 struct Solver {
   pg_op A;
   uint64_t nd, ni;      // per-segment data and image lengths
@@ -523,13 +707,18 @@ struct Solver {
     const dim3 gd((unsigned)nbd, (unsigned)nseg), gi((unsigned)nbi, (unsigned)nseg);
     const bool quad = R.kind == 0;
     PG_TRY(A->adjoint(r.p, ngrad.p, s));
-    PG_LAUNCH_PDL(k_ngrad, gi, kRed, 0, s, R, x.p, ngrad.p, part.p, nbi, counter.p, sc.p, fl.p, ddir.p,
-              quad ? ddir_prev.p : nullptr, pstride);
-    if (quad)
-      PG_LAUNCH_PDL(k_ddir_quad, gi, kRed, 0, s, R, ngrad.p, ddir_prev.p, ddir.p, x.p, part.p, nbi, counter.p, sc.p,
-                fl.p, pstride);
-    else
-      PG_LAUNCH_PDL(k_ddir, gi, kRed, 0, s, ni, ngrad.p, ddir.p, part.p, nbi, counter.p, sc.p, fl.p, pstride);
+    if (quad && nseg == 1 && R.N <= kImgMax && image_step_ok()) {
+      // gradient and direction of a small image in one cluster launch
+      PG_TRY(launch_image_step(R, x.p, ngrad.p, ddir.p, ddir_prev.p, sc.p, fl.p, s));
+    } else {
+      PG_LAUNCH_PDL(k_ngrad, gi, kRed, 0, s, R, x.p, ngrad.p, part.p, nbi, counter.p, sc.p, fl.p, ddir.p,
+                    quad ? ddir_prev.p : nullptr, pstride);
+      if (quad)
+        PG_LAUNCH_PDL(k_ddir_quad, gi, kRed, 0, s, R, ngrad.p, ddir_prev.p, ddir.p, x.p, part.p, nbi, counter.p,
+                      sc.p, fl.p, pstride);
+      else
+        PG_LAUNCH_PDL(k_ddir, gi, kRed, 0, s, ni, ngrad.p, ddir.p, part.p, nbi, counter.p, sc.p, fl.p, pstride);
+    }
     PG_TRY(A->forward(ddir.p, Adir.p, s));
     PG_LAUNCH_PDL(k_daw, gd, kRed, 0, s, nd, Adir.p, W, r.p, part.p, nbd, counter.p, sc.p, fl.p, quad ? 1 : 0, beta,
               pstride);
