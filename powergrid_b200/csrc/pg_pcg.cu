@@ -476,6 +476,79 @@ __global__ void __launch_bounds__(kImgT, 1)
   cl.sync();   // no CTA leaves while another reads its shared memory
 }
 
+// k_daw followed by k_update in one launch, for data and images of at most
+// kImgMax entries and one segment (quadratic penalty): the line-search sums,
+// the three Newton steps (newton_quad_steps, evaluated by every CTA from the
+// same rank-ordered totals) and the update of x, Ax and the residual, with a
+// cluster barrier where the two kernels had a launch boundary.
+__global__ void __launch_bounds__(kImgT, 1)
+    k_data_step_quad(uint64_t ni, uint64_t nd, float2* x, const float2* __restrict__ ddir, float2* Ax,
+                     const float2* __restrict__ Adir, const float2* __restrict__ y, const float* __restrict__ W,
+                     float2* r, double beta, double* sc, uint32_t* fl) {
+  pdl_wait();
+  cgx::cluster_group cl = cgx::this_cluster();
+  __shared__ double red[2];
+  const bool done0 = fl[F_DONE] != 0;     // the same value in every CTA
+  const uint64_t stride = (uint64_t)kImgCL * kImgT;
+  const uint64_t t0 = (uint64_t)cl.block_rank() * kImgT + threadIdx.x;
+  if (!done0) {
+    // dAWAd = Re<Adir, W Adir>, dAWr = Re(Adir' r) (k_daw)
+    double v[2] = {0.0, 0.0};
+    for (uint64_t i = t0; i < nd; i += stride) {
+      const float2 a = Adir[i];
+      const float2 q = r[i];
+      v[0] += (double)W[i] * ((double)a.x * a.x + (double)a.y * a.y);
+      v[1] += (double)a.x * q.x + (double)a.y * q.y;
+    }
+    cta_sum<2>(v, red);
+  }
+  cl.sync();
+  bool done = done0;
+  float st = 0.f;
+  if (!done) {
+    double tot[2];
+    cluster_totals<2>(cl, red, tot);
+    const double dawad = tot[0], dawr = tot[1];
+    const double denom = dawad + beta * sc[S_PDEN];
+    double step = 0.0;
+    bool bad = false;
+    for (int k = 0; k < 3; ++k) {                 // newton_quad_steps
+      if (fabs(denom) < 1e-20 || fabs(denom) > 1e25 || denom != denom) { bad = true; break; }
+      const double pdot = sc[S_PDOT0] + step * sc[S_Q1];
+      step = step - (-dawr + step * dawad + pdot) / denom;
+    }
+    if (cl.block_rank() == 0 && threadIdx.x == 0) {
+      sc[S_DAWAD] = dawad;
+      sc[S_DAWR] = dawr;
+      sc[S_STEP] = step;
+      if (bad) { fl[F_DONE] = 1; fl[F_REASON] = 3; }
+    }
+    done = bad;
+    st = (float)step;
+  }
+  if (!done) {
+    // x += step ddir; Ax += step Adir; r = W (.) (y - Ax) (k_update)
+    const uint64_t n = ni > nd ? ni : nd;
+    for (uint64_t i = t0; i < n; i += stride) {
+      if (i < ni) { const float2 d = ddir[i]; float2 v = x[i]; v.x += st * d.x; v.y += st * d.y; x[i] = v; }
+      if (i < nd) {
+        const float2 d = Adir[i];
+        float2 v = Ax[i];
+        v.x += st * d.x; v.y += st * d.y;
+        Ax[i] = v;
+        const float2 e = csub(y[i], v);
+        const float w = W[i];
+        r[i] = make_float2(w * e.x, w * e.y);
+      }
+    }
+    if (cl.block_rank() == 0 && threadIdx.x == 0) {
+      fl[F_IT] += 1;
+      fl[F_COMPLETED] = fl[F_IT];
+    }
+  }
+  cl.sync();   // no CTA leaves while another reads its shared memory
+}
+
 // The three Newton steps of the quadratic penalty (:132-150) from the sums
 // k_ddir_quad stored: Gradient is linear and wpot = 1, so pdenom is fixed and
 // pdot(s) = pdot(0) + s Re<ddir, Gradient(ddir)>.
@@ -666,6 +739,27 @@ bool image_step_ok() {
   return ok;
 }
 
+pg_status launch_data_step(uint64_t ni, uint64_t nd, float2* x, const float2* ddir, float2* Ax, const float2* Adir,
+                           const float2* y, const float* W, float2* r, double beta, double* sc, uint32_t* fl,
+                           cudaStream_t s) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(kImgCL, 1, 1);
+  cfg.blockDim = dim3(kImgT, 1, 1);
+  cfg.stream = s;
+  cudaLaunchAttribute a[2];
+  a[0].id = cudaLaunchAttributeClusterDimension;
+  a[0].val.clusterDim.x = kImgCL;
+  a[0].val.clusterDim.y = 1;
+  a[0].val.clusterDim.z = 1;
+  a[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;   // the kernel calls pdl_wait()
+  a[1].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+  cfg.attrs = a;
+  cfg.numAttrs = 2;
+  PG_CUDA(cudaLaunchKernelEx(&cfg, k_data_step_quad, ni, nd, x, ddir, Ax, Adir, y, W, r, beta, sc, fl));
+  count_launch();
+  return PG_OK;
+}
+
 pg_status launch_image_step(const PenDev& R, const float2* x, float2* ngrad, float2* ddir, float2* ddir_prev,
                             double* sc, uint32_t* fl, cudaStream_t s) {
   cudaLaunchConfig_t cfg = {};
@@ -720,6 +814,10 @@ struct Solver {
         PG_LAUNCH_PDL(k_ddir, gi, kRed, 0, s, ni, ngrad.p, ddir.p, part.p, nbi, counter.p, sc.p, fl.p, pstride);
     }
     PG_TRY(A->forward(ddir.p, Adir.p, s));
+    if (quad && nseg == 1 && nd <= kImgMax && ni <= kImgMax && image_step_ok()) {
+      // line search and update of a small problem in one cluster launch
+      return launch_data_step(ni, nd, x.p, ddir.p, Ax.p, Adir.p, y, W, r.p, beta, sc.p, fl.p, s);
+    }
     PG_LAUNCH_PDL(k_daw, gd, kRed, 0, s, nd, Adir.p, W, r.p, part.p, nbd, counter.p, sc.p, fl.p, quad ? 1 : 0, beta,
               pstride);
     if (!quad)
