@@ -13,6 +13,7 @@
 //   reconSolve            reconSolve.h:63-66
 //   acqTracking, getCompleteISMRMRDAcqData   acqTracking.h:14, processIsmrmrd.hpp:361-471
 //   writeNiftiRealImage, writeNiftiMagPhsImage   processNIFTI.hpp:37-117
+//   Server                (no counterpart: the request server over pg_server_*)
 // with T1 = float.  Column types: any type with memptr() (or data()),
 // n_elem (or size()) and a size constructor — arma::Col<std::complex<float>>
 // and arma::Col<float> work unchanged; pg::Col<T> is provided for callers
@@ -328,6 +329,49 @@ void getCompleteISMRMRDAcqData(const acqTracking& acqTrack, uword NSlice, uword 
                       (uint32_t)NPhase, reinterpret_cast<float*>(detail::mptr(data)), detail::mptr(kx),
                       detail::mptr(ky), detail::mptr(kz), detail::mptr(tvec)));
 }
+
+// The request server (pg_server_*).  The reference has no server: its
+// ISMRMRD driver reconstructs one image after another
+// (PowerGridIsmrmrd.cpp:191-264).  Here requests are batched, admitted by HBM
+// footprint and overlapped on the device; submit(acqTracking, ...) runs that
+// driver's whole image loop over an acquisition index.
+class Server {
+ public:
+  Server(uint64_t hbm_budget_bytes, uint32_t max_inflight) {
+    const pg_server_config c{hbm_budget_bytes, max_inflight, 0};
+    check(pg_server_create(&h_, &c));
+  }
+  Server(const Server&) = delete;
+  Server& operator=(const Server&) = delete;
+  ~Server() { pg_server_destroy(h_); }
+  // A request's arrays must stay valid until wait() (or poll()) reports it done.
+  uint64_t submit(const pg_request& r) {
+    uint64_t t = 0;
+    check(pg_submit(h_, &r, &t));
+    return t;
+  }
+  uint64_t submit(const acqTracking& acqs, const pg_acq_request& q) {
+    uint64_t t = 0;
+    check(pg_submit_acquisitions(h_, acqs.handle(), &q, &t));
+    return t;
+  }
+  pg_request_stats wait(uint64_t ticket) {
+    pg_request_stats st{};
+    check(pg_wait(h_, ticket, &st));
+    return st;
+  }
+  // true (stats filled) once the request is done
+  bool poll(uint64_t ticket, pg_request_stats* st) {
+    const pg_status s = pg_poll(h_, ticket, st);
+    if (s == PG_NOT_READY) return false;
+    check(s);
+    return true;
+  }
+  void cancel(uint64_t ticket) { check(pg_cancel(h_, ticket)); }
+
+ private:
+  pg_server h_ = nullptr;
+};
 
 template <typename T1>
 struct QuadPenalty {

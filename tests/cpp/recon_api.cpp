@@ -2,7 +2,8 @@
 // reference's PowerGridIsmrmrd driver does (PowerGridIsmrmrd.cpp:244-264):
 // Gnufft -> TimeSegmentation -> SENSE -> operator*, operator/, reconSolve,
 // then the direct-reconstruction helpers, the spatial interpolation and a
-// low-rank model over the same operator.
+// low-rank model over the same operator, and the same image through the
+// request server.
 // Inputs and outputs are raw little-endian files in the directory argv[1]
 // (written and checked by tests/test_cpp_api.py).
 #include <complex>
@@ -113,6 +114,21 @@ int main(int argc, char** argv) {
       pg::getCompleteISMRMRDAcqData<float>(track, 0, 0, 0, 0, 0, gd, gkx, gky, gkz, gt);
       save(d + "/gather_data.bin", gd);
       save(d + "/gather_kx.bin", gkx);
+      // the same image served: as a request, and as the driver's loop over the index
+      pg::Server srv(8ull << 30, 2);
+      pg::Col<cx> sreq(N), sacq(N);
+      const pg_request rq{nx, ny, nz, 1, nc, M, L, niter, beta, kx.memptr(), ky.memptr(), kz.memptr(), t.memptr(),
+                          fm.memptr(), reinterpret_cast<const float*>(sm.memptr()),
+                          reinterpret_cast<const float*>(data.memptr()), reinterpret_cast<float*>(sreq.memptr())};
+      const pg_acq_request aq{nx, ny, nz, L, niter, beta, fm.memptr(), reinterpret_cast<const float*>(sm.memptr()),
+                              reinterpret_cast<float*>(sacq.memptr())};
+      const uint64_t t1 = srv.submit(rq), t2 = srv.submit(track, aq);
+      for (const uint64_t tk : {t1, t2}) {
+        const pg_request_stats st = srv.wait(tk);
+        if (st.status != PG_OK) throw pg::Error(st.status, st.error);
+      }
+      save(d + "/served_req.bin", sreq);
+      save(d + "/served_acq.bin", sacq);
     }
   } catch (const pg::Error& e) {
     std::fprintf(stderr, "pg error: %s\n", e.what());

@@ -78,3 +78,8 @@ def test_cpp_api_matches_reference_fixture(pg, tmp_path):
     gd = np.fromfile(os.path.join(out, "gather_data.bin"), np.complex64)
     assert np.array_equal(gd, c["y_f32"].astype(np.complex64))
     assert np.array_equal(np.fromfile(os.path.join(out, "gather_kx.bin"), np.float32), c["kx"].astype(np.float32))
+    # pg::Server: the image as a request and as the driver's loop over the index equals reconSolve's
+    for name in ("served_req.bin", "served_acq.bin"):
+        e = rel_l2(np.fromfile(os.path.join(out, name), np.complex64), img)
+        print(f"{name}: vs reconSolve {e:.2e}")
+        assert e <= 1e-5
