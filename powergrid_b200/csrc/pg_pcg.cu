@@ -351,8 +351,8 @@ __global__ void k_ddir_quad(PenDev R, const float2* __restrict__ ngrad, const fl
 }
 
 // k_ngrad followed by k_ddir_quad in one launch, for images of at most
-// kImgMax voxels and one segment: one cluster of kImgCL CTAs covers the whole
-// image, so the grid-wide step between the two (the CG coefficient needs the
+// kImgMax voxels: one cluster of kImgCL CTAs covers a whole image (one cluster
+// per segment of a stacked solve), so the grid-wide step between the two (the CG coefficient needs the
 // sum over all voxels) is a cluster barrier instead of a kernel boundary and a
 // last-block reduction.  It pays while the image fits one voxel per thread:
 // at 64x64 a solve runs 4.4 % faster (19.7k vs 18.9k iterations/s), while at
@@ -404,6 +404,11 @@ __global__ void __launch_bounds__(kImgT, 1)
     k_image_step_quad(PenDev R, const float2* __restrict__ x, float2* ngrad, float2* ddir, float2* ddir_prev,
                       double* sc, uint32_t* fl) {
   pdl_wait();
+  {  // cluster blockIdx.y solves segment blockIdx.y: its part of the vectors, its scalars and flags
+    const uint64_t o = (uint64_t)blockIdx.y * R.N;
+    x += o; ngrad += o; ddir += o; ddir_prev += o;
+    sc += (size_t)blockIdx.y * S_NSCAL; fl += (size_t)blockIdx.y * F_NFLAG;
+  }
   cgx::cluster_group cl = cgx::this_cluster();
   __shared__ double redA[2], redB[4];
   const bool done0 = fl[F_DONE] != 0;     // the same value in every CTA
@@ -477,7 +482,7 @@ __global__ void __launch_bounds__(kImgT, 1)
 }
 
 // k_daw followed by k_update in one launch, for data and images of at most
-// kImgMax entries and one segment (quadratic penalty): the line-search sums,
+// kImgMax entries per segment (quadratic penalty; one cluster per segment): the line-search sums,
 // the three Newton steps (newton_quad_steps, evaluated by every CTA from the
 // same rank-ordered totals) and the update of x, Ax and the residual, with a
 // cluster barrier where the two kernels had a launch boundary.
@@ -486,6 +491,12 @@ __global__ void __launch_bounds__(kImgT, 1)
                      const float2* __restrict__ Adir, const float2* __restrict__ y, const float* __restrict__ W,
                      float2* r, double beta, double* sc, uint32_t* fl) {
   pdl_wait();
+  {  // cluster blockIdx.y solves segment blockIdx.y
+    const uint64_t oi = (uint64_t)blockIdx.y * ni, od = (uint64_t)blockIdx.y * nd;
+    x += oi; ddir += oi;
+    Ax += od; Adir += od; y += od; W += od; r += od;
+    sc += (size_t)blockIdx.y * S_NSCAL; fl += (size_t)blockIdx.y * F_NFLAG;
+  }
   cgx::cluster_group cl = cgx::this_cluster();
   __shared__ double red[2];
   const bool done0 = fl[F_DONE] != 0;     // the same value in every CTA
@@ -739,11 +750,11 @@ bool image_step_ok() {
   return ok;
 }
 
-pg_status launch_data_step(uint64_t ni, uint64_t nd, float2* x, const float2* ddir, float2* Ax, const float2* Adir,
-                           const float2* y, const float* W, float2* r, double beta, double* sc, uint32_t* fl,
-                           cudaStream_t s) {
+pg_status launch_data_step(int nseg, uint64_t ni, uint64_t nd, float2* x, const float2* ddir, float2* Ax,
+                           const float2* Adir, const float2* y, const float* W, float2* r, double beta, double* sc,
+                           uint32_t* fl, cudaStream_t s) {
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(kImgCL, 1, 1);
+  cfg.gridDim = dim3(kImgCL, (unsigned)nseg, 1);   // one cluster per segment
   cfg.blockDim = dim3(kImgT, 1, 1);
   cfg.stream = s;
   cudaLaunchAttribute a[2];
@@ -760,10 +771,10 @@ pg_status launch_data_step(uint64_t ni, uint64_t nd, float2* x, const float2* dd
   return PG_OK;
 }
 
-pg_status launch_image_step(const PenDev& R, const float2* x, float2* ngrad, float2* ddir, float2* ddir_prev,
-                            double* sc, uint32_t* fl, cudaStream_t s) {
+pg_status launch_image_step(int nseg, const PenDev& R, const float2* x, float2* ngrad, float2* ddir,
+                            float2* ddir_prev, double* sc, uint32_t* fl, cudaStream_t s) {
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(kImgCL, 1, 1);
+  cfg.gridDim = dim3(kImgCL, (unsigned)nseg, 1);   // one cluster per segment
   cfg.blockDim = dim3(kImgT, 1, 1);
   cfg.stream = s;
   cudaLaunchAttribute a[2];
@@ -801,9 +812,9 @@ struct Solver {
     const dim3 gd((unsigned)nbd, (unsigned)nseg), gi((unsigned)nbi, (unsigned)nseg);
     const bool quad = R.kind == 0;
     PG_TRY(A->adjoint(r.p, ngrad.p, s));
-    if (quad && nseg == 1 && R.N <= kImgMax && image_step_ok()) {
-      // gradient and direction of a small image in one cluster launch
-      PG_TRY(launch_image_step(R, x.p, ngrad.p, ddir.p, ddir_prev.p, sc.p, fl.p, s));
+    if (quad && R.N <= kImgMax && image_step_ok()) {
+      // gradient and direction of small images in one launch, one cluster per segment
+      PG_TRY(launch_image_step(nseg, R, x.p, ngrad.p, ddir.p, ddir_prev.p, sc.p, fl.p, s));
     } else {
       PG_LAUNCH_PDL(k_ngrad, gi, kRed, 0, s, R, x.p, ngrad.p, part.p, nbi, counter.p, sc.p, fl.p, ddir.p,
                     quad ? ddir_prev.p : nullptr, pstride);
@@ -814,9 +825,9 @@ struct Solver {
         PG_LAUNCH_PDL(k_ddir, gi, kRed, 0, s, ni, ngrad.p, ddir.p, part.p, nbi, counter.p, sc.p, fl.p, pstride);
     }
     PG_TRY(A->forward(ddir.p, Adir.p, s));
-    if (quad && nseg == 1 && nd <= kImgMax && ni <= kImgMax && image_step_ok()) {
-      // line search and update of a small problem in one cluster launch
-      return launch_data_step(ni, nd, x.p, ddir.p, Ax.p, Adir.p, y, W, r.p, beta, sc.p, fl.p, s);
+    if (quad && nd <= kImgMax && ni <= kImgMax && image_step_ok()) {
+      // line search and update of small problems in one launch, one cluster per segment
+      return launch_data_step(nseg, ni, nd, x.p, ddir.p, Ax.p, Adir.p, y, W, r.p, beta, sc.p, fl.p, s);
     }
     PG_LAUNCH_PDL(k_daw, gd, kRed, 0, s, nd, Adir.p, W, r.p, part.p, nbd, counter.p, sc.p, fl.p, quad ? 1 : 0, beta,
               pstride);
