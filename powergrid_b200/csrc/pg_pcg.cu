@@ -355,14 +355,16 @@ __global__ void k_ddir_quad(PenDev R, const float2* __restrict__ ngrad, const fl
 // per segment of a stacked solve), so the grid-wide step between the two (the CG coefficient needs the
 // sum over all voxels) is a cluster barrier instead of a kernel boundary and a
 // last-block reduction.  It pays while the image fits one voxel per thread:
-// at 64x64 a solve runs 4.4 % faster (19.7k vs 18.9k iterations/s), while at
-// 128x128 (two voxels per thread on 8 SMs) the two kernels over 64 SMs win
-// (8.77k vs 8.55k).  Each CTA sums the CTAs' partials itself, in rank
+// at 64x64 a solve ran 4.4 % faster (19.7k vs 18.9k iterations/s, measured
+// with 1024-thread CTAs), while at 128x128 the two kernels over 64 SMs won
+// (8.77k vs 8.55k with two voxels per thread, 8.61k with a 16-CTA cluster).  Each CTA sums the CTAs' partials itself, in rank
 // order, so every CTA holds the same FP64 totals and the same coefficient.
 // Same per-voxel arithmetic as the two kernels; the FP64 sums are added in a
 // different (fixed) order.
 namespace cgx = cooperative_groups;
-constexpr int kImgCL = 8, kImgT = 1024, kImgPer = 1;
+// 512-thread CTAs (32K registers, half an SM) so that a cluster never needs
+// whole idle SMs while other streams' kernels run.
+constexpr int kImgCL = 8, kImgT = 512, kImgPer = 1;
 constexpr uint64_t kImgMax = (uint64_t)kImgCL * kImgT * kImgPer;
 
 // Sum of NV doubles over the CTA into red[0..NV) (thread 0 writes; all threads
@@ -380,7 +382,7 @@ __device__ __forceinline__ void cta_sum(double (&v)[NV], double* red) {
   if (w == 0) {
 #pragma unroll
     for (int k = 0; k < NV; ++k) {
-      double t = sw[k][l];   // kImgT / 32 == 32 warps
+      double t = (l < kImgT / 32) ? sw[k][l] : 0.0;
       t = warp_sum(t);
       if (l == 0) red[k] = t;
     }
@@ -400,7 +402,7 @@ __device__ __forceinline__ void cluster_totals(cgx::cluster_group& cl, double* r
   }
 }
 
-__global__ void __launch_bounds__(kImgT, 1)
+__global__ void __launch_bounds__(kImgT, 2)
     k_image_step_quad(PenDev R, const float2* __restrict__ x, float2* ngrad, float2* ddir, float2* ddir_prev,
                       double* sc, uint32_t* fl) {
   pdl_wait();
@@ -486,7 +488,7 @@ __global__ void __launch_bounds__(kImgT, 1)
 // the three Newton steps (newton_quad_steps, evaluated by every CTA from the
 // same rank-ordered totals) and the update of x, Ax and the residual, with a
 // cluster barrier where the two kernels had a launch boundary.
-__global__ void __launch_bounds__(kImgT, 1)
+__global__ void __launch_bounds__(kImgT, 2)
     k_data_step_quad(uint64_t ni, uint64_t nd, float2* x, const float2* __restrict__ ddir, float2* Ax,
                      const float2* __restrict__ Adir, const float2* __restrict__ y, const float* __restrict__ W,
                      float2* r, double beta, double* sc, uint32_t* fl) {

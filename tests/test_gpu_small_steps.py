@@ -1,4 +1,4 @@
-"""The one-cluster PCG steps of small problems (image and data of at most 8192
+"""The one-cluster PCG steps of small problems (image and data of at most 4096
 entries per slice, quadratic penalty; one cluster per slice of a stacked
 solve): k_image_step_quad does the work of k_ngrad + k_ddir_quad and
 k_data_step_quad that of k_daw + k_update, with cluster barriers where the
